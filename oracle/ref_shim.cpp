@@ -1,0 +1,184 @@
+// Test infrastructure only: a C entry layer over HornSculpt's own CPU
+// galerkin code (space.cpp, pair_quadrature.cpp, interaction_plan.cpp),
+// compiled from the reference tree by oracle/Makefile into oracle/_ref/.
+// It exposes the reference's interaction plan and patch estimator with the
+// same flat layout as the restated oracle so tests can compare them exactly.
+#include "galerkin/interaction_plan.hpp"
+#include "galerkin/pair_quadrature.hpp"
+#include "galerkin/space.hpp"
+
+#include <cstring>
+#include <string>
+
+using namespace hornsculpt;
+using namespace hornsculpt::galerkin;
+
+namespace {
+thread_local std::string lastError;
+struct Handle {
+    InteractionPlan plan;
+};
+SurfaceMesh makeMesh(const double *verts, size_t nv, const uint32_t *tris, size_t nt) {
+    SurfaceMesh m;
+    // The solver session centres the mesh on vertex 0 before planning
+    // (cuda_solver.cu:771-781); do the same so plans are comparable.
+    const Vec3 origin{verts[0], verts[1], verts[2]};
+    for (size_t i = 0; i < nv; ++i)
+        m.vertices.push_back({verts[3 * i] - origin.x, verts[3 * i + 1] - origin.y, verts[3 * i + 2] - origin.z});
+    for (size_t i = 0; i < nt; ++i)
+        m.triangles.push_back({{tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]}, 0, BoundaryCondition::wall});
+    return m;
+}
+}  // namespace
+
+extern "C" {
+struct ref_numerics {
+    unsigned quadrature_order, singular_order;
+    double near_ratio, near_tol;
+    unsigned near_depth;
+    double residual_tol;
+    unsigned max_refine;
+};
+const char *ref_last_error() { return lastError.c_str(); }
+
+int ref_plan_build(const double *verts, size_t nv, const uint32_t *tris, size_t nt, const ref_numerics *nm,
+                   double maxK, unsigned threads, void **out) {
+    try {
+        const Space space = buildSpace(makeMesh(verts, nv, tris, nt));
+        PairQuadratureSettings st;
+        st.regularOrder = nm->quadrature_order;
+        st.singularOrder = nm->singular_order;
+        st.nearDistanceRatio = nm->near_ratio;
+        st.relativeTolerance = nm->near_tol;
+        st.maximumSubdivisionDepth = nm->near_depth;
+        auto *h = new Handle{makeInteractionPlan(space, st, maxK, {}, threads)};
+        *out = h;
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return 2;
+    }
+}
+void ref_plan_sizes(void *h, size_t *out) {
+    const auto &p = static_cast<Handle *>(h)->plan;
+    out[0] = p.touching.size();
+    out[1] = p.near.size();
+    out[2] = p.patches.size();
+    out[3] = p.wholePanelDegrees.size();
+    out[4] = p.nearTrials.size();
+    out[5] = p.maximumDepth;
+}
+void ref_plan_touching(void *h, uint32_t *out) {
+    for (const auto &j : static_cast<Handle *>(h)->plan.touching) {
+        *out++ = j.test;
+        *out++ = j.trial;
+        *out++ = static_cast<uint32_t>(j.permutation.topology);
+        for (int i = 0; i < 3; ++i)
+            *out++ = j.permutation.test[i];
+        for (int i = 0; i < 3; ++i)
+            *out++ = j.permutation.trial[i];
+    }
+}
+void ref_plan_near(void *h, uint32_t *out) {
+    for (const auto &j : static_cast<Handle *>(h)->plan.near) {
+        *out++ = j.test;
+        *out++ = j.trial;
+        *out++ = j.firstPatch;
+        *out++ = j.patchCount;
+        *out++ = j.swapBarycentric;
+    }
+}
+void ref_plan_patches(void *h, double *out) {
+    for (const auto &p : static_cast<Handle *>(h)->plan.patches) {
+        for (int i = 0; i < 9; ++i)
+            *out++ = p.test[i];
+        for (int i = 0; i < 9; ++i)
+            *out++ = p.trial[i];
+        *out++ = p.areaFraction;
+        *out++ = p.degree;
+        *out++ = p.projection;
+        *out++ = p.projectionIntervals;
+    }
+}
+void ref_plan_whole(void *h, uint8_t *out) {
+    const auto &w = static_cast<Handle *>(h)->plan.wholePanelDegrees;
+    if (!w.empty())
+        std::memcpy(out, w.data(), w.size());
+}
+void ref_plan_offsets(void *h, uint32_t *offsets, uint32_t *trials) {
+    const auto &p = static_cast<Handle *>(h)->plan;
+    std::memcpy(offsets, p.nearOffsets.data(), p.nearOffsets.size() * 4);
+    if (!p.nearTrials.empty())
+        std::memcpy(trials, p.nearTrials.data(), p.nearTrials.size() * 4);
+}
+void ref_plan_free(void *h) { delete static_cast<Handle *>(h); }
+
+int ref_triangle_rule(unsigned degree, double *out, size_t *count) {
+    try {
+        const auto r = triangleRule(degree);
+        *count = r.size();
+        if (out)
+            for (const auto &p : r) {
+                *out++ = p.barycentric[0];
+                *out++ = p.barycentric[1];
+                *out++ = p.barycentric[2];
+                *out++ = p.weight;
+            }
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return 1;
+    }
+}
+int ref_gauss(unsigned order, double *out) {
+    try {
+        for (const auto &g : gaussLegendre01(order)) {
+            *out++ = g.position;
+            *out++ = g.weight;
+        }
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return 1;
+    }
+}
+int ref_estimate_patch(const double *tri9a, const double *tri9b, const uint32_t *nodesA, const uint32_t *nodesB,
+                       const double *patch22, double k, double *moments72, double *errors3) {
+    try {
+        SurfaceMesh m;
+        for (int i = 0; i < 3; ++i)
+            m.vertices.push_back({tri9a[3 * i], tri9a[3 * i + 1], tri9a[3 * i + 2]});
+        for (int i = 0; i < 3; ++i)
+            m.vertices.push_back({tri9b[3 * i], tri9b[3 * i + 1], tri9b[3 * i + 2]});
+        m.triangles.push_back({{0, 1, 2}, 0, BoundaryCondition::wall});
+        m.triangles.push_back({{3, 4, 5}, 0, BoundaryCondition::wall});
+        const Space space = buildSpace(m);
+        Panel a = space.panels[0], b = space.panels[1];
+        for (int i = 0; i < 3; ++i) {
+            a.nodes[i] = nodesA[i];
+            b.nodes[i] = nodesB[i];
+        }
+        PairQuadraturePatch p;
+        for (int i = 0; i < 9; ++i) {
+            p.test[i] = patch22[i];
+            p.trial[i] = patch22[9 + i];
+        }
+        p.areaFraction = patch22[18];
+        p.degree = unsigned(patch22[19]);
+        p.projection = unsigned(patch22[20]);
+        p.projectionIntervals = unsigned(patch22[21]);
+        const auto e = estimatePairPatchCpu(a, b, p, k);
+        for (int i = 0; i < 36; ++i) {
+            moments72[2 * i] = e.integral[i].real();
+            moments72[2 * i + 1] = e.integral[i].imag();
+        }
+        errors3[0] = e.absoluteError;
+        errors3[1] = e.innerError;
+        errors3[2] = e.outerError;
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return 2;
+    }
+}
+}
