@@ -1,0 +1,352 @@
+"""Python mirror of HornSculpt's BEM solver interface
+(``modules/bem/include/hornsculpt/bem.hpp:27-388``) over the C ABI of
+libhs_bem.so. Names, defaults, units and error classes follow the reference:
+invalid meshes and requests raise ValueError (std::invalid_argument), device,
+numerical and convergence failures raise BemError (std::runtime_error).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import BemCancelled, BemError, BemUnsupported  # noqa: F401  (re-exported)
+from .meshes import SurfaceMesh
+
+
+@dataclasses.dataclass
+class AcousticMedium:
+    density: float = 1.21
+    sound_speed: float = 343.0
+
+
+@dataclasses.dataclass
+class FaceVelocity:
+    face_id: int
+    normal_velocity: complex = 1.0 + 0.0j  # RMS m/s, out of the solid
+
+
+@dataclasses.dataclass
+class BemExcitation:
+    name: str
+    faces: list
+
+
+@dataclasses.dataclass
+class FastMultipoleSettings:
+    leaf_support_capacity: int = 16
+    separation_ratio: float = 1.5
+    maximum_iterations: int = 300
+    restart_length: int = 40
+    preconditioner_block_width: int = 32
+
+
+@dataclasses.dataclass
+class BemNumerics:
+    quadrature_order: int = 4
+    singular_order: int = 4
+    near_distance_ratio: float = 1.0
+    near_relative_tolerance: float = 1e-4
+    near_maximum_depth: int = 6
+    relative_residual_tolerance: float = 5e-5
+    maximum_refinement_steps: int = 3
+    acceleration: str = "dense"  # "dense" | "fast_multipole"
+    precision: str = "fp64"      # the plain form
+    fast_multipole: FastMultipoleSettings = dataclasses.field(default_factory=FastMultipoleSettings)
+
+    def to_c(self) -> _lib.hs_numerics:
+        n = _lib.hs_numerics()
+        n.quadrature_order = self.quadrature_order
+        n.singular_order = self.singular_order
+        n.near_distance_ratio = self.near_distance_ratio
+        n.near_relative_tolerance = self.near_relative_tolerance
+        n.near_maximum_depth = self.near_maximum_depth
+        n.relative_residual_tolerance = self.relative_residual_tolerance
+        n.maximum_refinement_steps = self.maximum_refinement_steps
+        n.acceleration = {"dense": 0, "fast_multipole": 1}.get(self.acceleration, 99)
+        n.precision = {"fp64": 0}.get(self.precision, 99)
+        f = self.fast_multipole
+        n.fmm_leaf_support_capacity = f.leaf_support_capacity
+        n.fmm_separation_ratio = f.separation_ratio
+        n.fmm_maximum_iterations = f.maximum_iterations
+        n.fmm_restart_length = f.restart_length
+        n.fmm_preconditioner_block_width = f.preconditioner_block_width
+        return n
+
+
+@dataclasses.dataclass
+class FarFieldObservation:
+    origin: tuple = (0.0, 0.0, 0.0)
+    reference_distance: float = 1.0
+
+
+@dataclasses.dataclass
+class BemRequest:
+    frequencies: Sequence[float]
+    excitations: Sequence[BemExcitation]
+    observers: Sequence[Sequence[float]] = ()
+    medium: AcousticMedium = dataclasses.field(default_factory=AcousticMedium)
+    numerics: BemNumerics = dataclasses.field(default_factory=BemNumerics)
+    far_field: Optional[FarFieldObservation] = None
+    interaction_plan_frequencies: Sequence[float] = ()
+
+
+@dataclasses.dataclass
+class FaceImpedance:
+    face_id: int
+    area: float
+    mean_pressure: complex
+    volume_velocity: complex
+    volume_impedance: complex
+
+
+@dataclasses.dataclass
+class BemBoundaryData:
+    surface_pressure: np.ndarray   # DP0 mean pressure per triangle
+    pressure_trace: np.ndarray     # P1 pressure per vertex
+    normal_derivative: np.ndarray  # DP0 q = -i rho omega v per triangle
+
+
+@dataclasses.dataclass
+class BemExcitationResult:
+    name: str
+    observer_pressure: np.ndarray
+    impedances: list
+    refinement_steps: int
+    boundary_residual: float
+    field_quadrature_comparison_degree: int
+    field_quadrature_verification_degree: int
+    field_quadrature_discrepancy: float
+    boundary: BemBoundaryData
+    iterations: int = 0
+
+
+@dataclasses.dataclass
+class BemFrequencyResult:
+    frequency: float
+    excitations: list
+    assembly_milliseconds: float
+    solve_milliseconds: float
+    factorization_milliseconds: float
+    triangular_solve_milliseconds: float
+    field_milliseconds: float
+    residual_check_milliseconds: float
+    interaction_plan_milliseconds: float
+    interaction_plan_reused: bool
+
+
+@dataclasses.dataclass
+class BemResult:
+    device: str
+    triangle_count: int
+    pressure_dof_count: int
+    peak_device_bytes: int
+    frequencies: list
+    acceleration: str = "dense"
+
+
+class StopToken:
+    """Cooperative cancellation flag polled by the solver between device batches."""
+
+    def __init__(self):
+        self._flag = C.c_int32(0)
+
+    def request_stop(self):
+        self._flag.value = 1
+
+    @property
+    def stop_requested(self) -> bool:
+        return bool(self._flag.value)
+
+
+@dataclasses.dataclass
+class CudaStorageOptions:
+    quadrature_patches: str = "automatic"  # "automatic" | "device" | "mapped_host"
+
+
+def _cplx(buf: np.ndarray) -> np.ndarray:
+    return buf[0::2] + 1j * buf[1::2]
+
+
+class CudaBemSolver:
+    """One closed exterior surface mesh resident on the current CUDA device."""
+
+    def __init__(self, mesh: SurfaceMesh, storage: CudaStorageOptions = CudaStorageOptions()):
+        lib = _lib.load()
+        residency = {"automatic": 0, "device": 1, "mapped_host": 2}.get(storage.quadrature_patches, 99)
+        self._mesh = mesh
+        handle = C.c_void_p()
+        _lib.check(lib.hs_bem_session_create(mesh.vertices.ctypes.data, mesh.vertex_count, mesh.triangles.ctypes.data,
+                                             mesh.face_ids.ctypes.data, mesh.boundary.ctypes.data,
+                                             mesh.triangle_count, residency, C.byref(handle)))
+        self._handle = handle
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.hs_bem_session_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @staticmethod
+    def device_description() -> str:
+        buf = C.create_string_buffer(256)
+        _lib.check(_lib.load().hs_device_description(buf, 256))
+        return buf.value.decode()
+
+    def set_stream(self, cuda_stream: int | None) -> None:
+        _lib.check(self._lib.hs_bem_session_set_stream(self._handle, C.c_void_p(cuda_stream or 0)))
+
+    def set_profiling(self, enabled: bool) -> None:
+        _lib.check(self._lib.hs_bem_session_set_profiling(self._handle, int(enabled)))
+
+    def profile(self) -> dict:
+        """{kernel family: (milliseconds, launches)} of the CUDA events recorded so far."""
+        cap = 64
+        names = C.create_string_buffer(4096)
+        ms = (C.c_double * cap)()
+        launches = (C.c_uint64 * cap)()
+        count = C.c_size_t()
+        _lib.check(self._lib.hs_bem_session_profile(self._handle, names, 4096, ms, launches, cap, C.byref(count)))
+        keys = names.value.decode().split(",") if count.value else []
+        return {k: (ms[i], launches[i]) for i, k in enumerate(keys)}
+
+    WORK_KEYS = ("pairs_q6", "pairs_q12", "pairs_q16", "pairs_q64", "regular_samples", "singular_samples",
+                 "near_samples", "frequencies")
+
+    def work(self) -> dict:
+        """Work counters (pairs per regular rule, samples per pair class) since profiling was enabled."""
+        buf = (C.c_uint64 * 8)()
+        count = C.c_size_t()
+        _lib.check(self._lib.hs_bem_session_work(self._handle, buf, 8, C.byref(count)))
+        return {k: int(buf[i]) for i, k in enumerate(self.WORK_KEYS[: count.value])}
+
+    def solve(self, request: BemRequest, stop: StopToken | None = None,
+              progress: Callable | None = None) -> BemResult:
+        req, keep = self._c_request(request)
+        out = C.c_void_p()
+        cb = _lib.PROGRESS_FN(lambda p, _u: progress(p.contents) if progress else None) if progress else \
+            _lib.PROGRESS_FN()
+        flag = C.byref(stop._flag) if stop is not None else None
+        _lib.check(self._lib.hs_bem_solve(self._handle, C.byref(req), flag, cb, None, C.byref(out)))
+        try:
+            return self._read(out, request)
+        finally:
+            self._lib.hs_result_free(out)
+            del keep
+
+    # -- marshalling --------------------------------------------------------
+    def _c_request(self, r: BemRequest):
+        freqs = np.ascontiguousarray(r.frequencies, np.float64)
+        plan = np.ascontiguousarray(r.interaction_plan_frequencies, np.float64)
+        offsets = [0]
+        face_ids, vel = [], []
+        for ex in r.excitations:
+            for fv in ex.faces:
+                face_ids.append(fv.face_id)
+                v = complex(fv.normal_velocity)
+                vel += [v.real, v.imag]
+            offsets.append(len(face_ids))
+        offsets = np.asarray(offsets, np.uintp)
+        face_ids = np.asarray(face_ids or [0], np.uint32)
+        vel = np.asarray(vel or [0.0, 0.0], np.float64)
+        obs = np.ascontiguousarray(np.asarray(r.observers, np.float64).reshape(-1, 3))
+        c = _lib.hs_request()
+        c.density = r.medium.density
+        c.sound_speed = r.medium.sound_speed
+        dp = C.POINTER(C.c_double)
+        c.frequencies = freqs.ctypes.data_as(dp)
+        c.frequency_count = len(freqs)
+        c.plan_frequencies = plan.ctypes.data_as(dp) if len(plan) else None
+        c.plan_frequency_count = len(plan)
+        c.excitation_count = len(r.excitations)
+        c.excitation_face_offsets = offsets.ctypes.data_as(C.POINTER(C.c_size_t))
+        c.excitation_face_ids = face_ids.ctypes.data_as(C.POINTER(C.c_uint32))
+        c.excitation_velocities = vel.ctypes.data_as(dp)
+        c.observers = obs.ctypes.data_as(dp) if len(obs) else None
+        c.observer_count = len(obs)
+        if r.far_field is not None:
+            c.far_field = 1
+            for i in range(3):
+                c.far_origin[i] = float(r.far_field.origin[i])
+            c.far_reference_distance = r.far_field.reference_distance
+        c.numerics = r.numerics.to_c()
+        return c, (freqs, plan, offsets, face_ids, vel, obs)
+
+    def _read(self, out, request: BemRequest) -> BemResult:
+        lib = self._lib
+        F = lib.hs_result_frequency_count(out)
+        E = lib.hs_result_excitation_count(out)
+        T = lib.hs_result_triangle_count(out)
+        N = lib.hs_result_pressure_dof_count(out)
+        O = lib.hs_result_observer_count(out)
+        frames = []
+        for f in range(F):
+            fi = _lib.hs_frequency_info()
+            _lib.check(lib.hs_result_frequency_info(out, f, C.byref(fi)))
+            excs = []
+            for e in range(E):
+                info = _lib.hs_excitation_info()
+                _lib.check(lib.hs_result_excitation_info(out, f, e, C.byref(info)))
+                tr, sp, nd, ob = np.zeros(2 * N), np.zeros(2 * T), np.zeros(2 * T), np.zeros(max(2 * O, 2))
+                _lib.check(lib.hs_result_pressure_trace(out, f, e, tr.ctypes.data))
+                _lib.check(lib.hs_result_surface_pressure(out, f, e, sp.ctypes.data))
+                _lib.check(lib.hs_result_normal_derivative(out, f, e, nd.ctypes.data))
+                _lib.check(lib.hs_result_observer_pressure(out, f, e, ob.ctypes.data))
+                imp = (_lib.hs_face_impedance * max(info.impedance_count, 1))()
+                _lib.check(lib.hs_result_impedances(out, f, e, imp))
+                impedances = [FaceImpedance(x.face_id, x.area, complex(*x.mean_pressure), complex(*x.volume_velocity),
+                                            complex(*x.volume_impedance)) for x in imp[: info.impedance_count]]
+                excs.append(BemExcitationResult(
+                    name=request.excitations[e].name, observer_pressure=_cplx(ob[: 2 * O]), impedances=impedances,
+                    refinement_steps=info.refinement_steps, boundary_residual=info.boundary_residual,
+                    field_quadrature_comparison_degree=info.field_comparison_degree,
+                    field_quadrature_verification_degree=info.field_verification_degree,
+                    field_quadrature_discrepancy=info.field_discrepancy,
+                    boundary=BemBoundaryData(_cplx(sp), _cplx(tr), _cplx(nd))))
+            frames.append(BemFrequencyResult(fi.frequency, excs, fi.assembly_ms, fi.solve_ms, fi.factorization_ms,
+                                             fi.triangular_solve_ms, fi.field_ms, fi.residual_check_ms,
+                                             fi.interaction_plan_ms, bool(fi.interaction_plan_reused)))
+        return BemResult(self.device_description(), T, N, lib.hs_result_peak_device_bytes(out), frames)
+
+    # -- test hooks ---------------------------------------------------------
+    def debug_assemble(self, numerics: BemNumerics, plan_k: float, k: float, flux: np.ndarray):
+        """Row-equilibrated matrix (N x N, complex) and right-hand side for per-triangle flux."""
+        N, T = self._mesh.vertex_count, self._mesh.triangle_count
+        q = np.zeros(2 * T)
+        q[0::2], q[1::2] = np.real(flux), np.imag(flux)
+        A = np.zeros(2 * N * N)
+        b = np.zeros(2 * N)
+        n = numerics.to_c()
+        _lib.check(self._lib.hs_bem_debug_assemble(self._handle, C.byref(n), plan_k, k, q.ctypes.data, A.ctypes.data,
+                                                   b.ctypes.data))
+        return _cplx(A).reshape(N, N).T, _cplx(b)  # column-major -> [row, col]
+
+
+def host_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float) -> dict:
+    """The library's host interaction plan of a mesh (no device needed)."""
+    lib = _lib.load()
+    n = numerics.to_c()
+    sizes = (C.c_size_t * 6)()
+    args = (mesh.vertices.ctypes.data, mesh.vertex_count, mesh.triangles.ctypes.data, mesh.triangle_count, C.byref(n),
+            max_k, sizes)
+    _lib.check(lib.hs_bem_debug_plan(*args, None, None, None, None, None, None))
+    nt, nn, npch, nw, ntr, depth = list(sizes)
+    out = dict(touching=np.zeros((nt, 9), np.uint32), near=np.zeros((nn, 5), np.uint32),
+               patches=np.zeros((npch, 22)), whole=np.zeros(nw, np.uint8),
+               offsets=np.zeros(mesh.triangle_count + 1, np.uint32), trials=np.zeros(ntr, np.uint32), depth=depth)
+    _lib.check(lib.hs_bem_debug_plan(*args, out["touching"].ctypes.data, out["near"].ctypes.data,
+                                     out["patches"].ctypes.data, out["whole"].ctypes.data, out["offsets"].ctypes.data,
+                                     out["trials"].ctypes.data))
+    return out

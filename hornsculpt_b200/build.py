@@ -1,0 +1,63 @@
+"""Builds libhs_bem.so in-tree: host C++20 (mesh validation, planner, session,
+C ABI) and the sm_100a CUDA kernels, linked against the static CUDA runtime.
+
+    python -m hornsculpt_b200.build        # or hornsculpt_b200.build.build()
+"""
+from __future__ import annotations
+
+import concurrent.futures
+import os
+import pathlib
+import shutil
+import subprocess
+import sys
+
+PKG = pathlib.Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = PKG / "_build"
+LIBRARY = PKG / "libhs_bem.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    path = shutil.which("nvcc") or os.path.join(cuda, "bin", "nvcc")
+    if not os.path.exists(path):
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libhs_bem.so")
+    return path
+
+
+def _sources():
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+
+
+def _compile(src: pathlib.Path, verbose_ptxas: bool) -> pathlib.Path:
+    obj = BUILD / (src.name + ".o")
+    deps = [src] + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    if obj.exists() and obj.stat().st_mtime > max(d.stat().st_mtime for d in deps) and not verbose_ptxas:
+        return obj
+    cmd = [_nvcc(), "-std=c++20", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I", str(INCLUDE), "-I",
+           str(CSRC), "-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cu":
+        cmd += ["--use_fast_math"] if False else []
+        if verbose_ptxas:
+            cmd += ["-Xptxas", "-v"]
+    subprocess.run(cmd, check=True)
+    return obj
+
+
+def build(verbose_ptxas: bool = False) -> pathlib.Path:
+    BUILD.mkdir(exist_ok=True)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as pool:
+        objs = list(pool.map(lambda s: _compile(s, verbose_ptxas), _sources()))
+    if not LIBRARY.exists() or LIBRARY.stat().st_mtime < max(o.stat().st_mtime for o in objs):
+        tmp = LIBRARY.with_suffix(".so.tmp")
+        subprocess.run([_nvcc(), "-shared", *ARCH, "-o", str(tmp), *map(str, objs), "-lpthread"], check=True)
+        tmp.replace(LIBRARY)
+    return LIBRARY
+
+
+if __name__ == "__main__":
+    print(build(verbose_ptxas="-v" in sys.argv))

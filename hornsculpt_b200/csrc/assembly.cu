@@ -1,0 +1,754 @@
+// FP64 Burton-Miller Galerkin assembly for sm_100a (the plain form).
+//
+// Method: modules/bem/cuda/cuda_solver.cu:266-540 with the FP64 sample of
+// panel_integrals.cuh:166-198 — regular disjoint pairs with the qualified
+// Dunavant 4/6/8 rule (or an accepted whole-panel 8/14 rule), touching pairs
+// with Sauter-Schwab sectors, near pairs with their plan patches, plus half
+// the P1 mass, rows equilibrated by the reciprocal lumped mass.
+//
+// B200 layout: a batch of frequencies runs in one launch (blockIdx.y). Each
+// unordered regular or near pair is integrated once and yields both ordered
+// blocks, because the reverse direction's double-layer kernel is the forward
+// adjoint kernel at the same points. Pair blocks are written to per-pair
+// records (no atomics) and reduced to the matrix by two deterministic
+// gathers (trial vertex, then test vertex), so results are bit-reproducible.
+#include "device_types.cuh"
+#include "host_mesh.hpp"
+#include "kernel_timer.hpp"
+
+#include <algorithm>
+#include <stdexcept>
+#include <string>
+
+namespace hsb {
+namespace {
+
+constexpr double kInvFourPi = 0.07957747154594766788;
+
+// Rule points (b0, b1, b2, w) of the four regular bins, in bin order
+// (offsets 0, 6, 18, 34).
+constexpr int kRulePoints = 98;
+__constant__ double cRule[kRulePoints * 4];
+__constant__ double cGauss20[40];
+
+template <int NP> __device__ constexpr int ruleOffset() {
+    return NP == 6 ? 0 : NP == 12 ? 6 : NP == 16 ? 18 : 34;
+}
+
+void cudaCheck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess)
+        throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+__device__ __forceinline__ void flagError(int *error, int code) { atomicExch(error, code); }
+
+// Moment accumulators of one ordered pair: MG = sum g bt bs, MP = sum P bt bs,
+// MQ = sum Q bt bs (3x3 complex each) where, for delta = x_test - y_trial,
+// g = w exp(-ikr)/(4 pi r), P = g (1+ikr) (delta.n_trial)/r^2 (double layer),
+// Q = -g (1+ikr) (delta.n_test)/r^2 (adjoint double layer).
+struct PairMoments {
+    double g[18], p[18], q[18];
+};
+
+// Record entry o (0..11 forward block (test t, trial s); 12..23 reverse
+// block (test s, trial t)) of an unordered pair from its moments. Forward:
+// A_ij = -MP_ij + i k (n_t.n_s) MG_ij + alpha G (curl_ti . curl_sj),
+// b_i = sum_j (-MG_ij + (i/k) MQ_ij); reverse swaps P and Q and transposes.
+__device__ __forceinline__ void pairRecordValue(int o, const double *MG, const double *MP, const double *MQ,
+                                                const DPanel &t, const DPanel &s, double k, double invk,
+                                                double &re, double &im) {
+    const double nn = t.n[0] * s.n[0] + t.n[1] * s.n[1] + t.n[2] * s.n[2];
+    const bool reverse = o >= 12;
+    const int e = reverse ? o - 12 : o;
+    const double *X = reverse ? MQ : MP;  // double-layer moments of this direction
+    const double *Y = reverse ? MP : MQ;  // adjoint moments of this direction
+    if (e < 9) {
+        // forward element (i, j); reverse element (row j of s, col i of t) = moments (i, j)
+        const int row = e / 3, col = e % 3;
+        const int i = reverse ? col : row, j = reverse ? row : col;
+        const int m = 2 * (3 * i + j);
+        double gre = 0, gim = 0;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            gre += MG[2 * c];
+            gim += MG[2 * c + 1];
+        }
+        const double curl = t.curl[3 * i] * s.curl[3 * j] + t.curl[3 * i + 1] * s.curl[3 * j + 1] +
+                            t.curl[3 * i + 2] * s.curl[3 * j + 2];
+        re = -X[m] - k * nn * MG[m + 1] + gim * curl * invk;
+        im = -X[m + 1] + k * nn * MG[m] - gre * curl * invk;
+    } else {
+        const int a = e - 9;  // local row of this direction's test panel
+        double sg_re = 0, sg_im = 0, sy_re = 0, sy_im = 0;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const int m = reverse ? 2 * (3 * b + a) : 2 * (3 * a + b);
+            sg_re += MG[m];
+            sg_im += MG[m + 1];
+            sy_re += Y[m];
+            sy_im += Y[m + 1];
+        }
+        re = -sg_re - sy_im * invk;
+        im = -sg_im + sy_re * invk;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Regular pairs: one unordered pair per NP threads, thread x owns test point x
+// and sweeps the NP trial points, contracting trial bases on the fly.
+// ---------------------------------------------------------------------------
+template <int NP>
+__global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restrict__ panels, uint32_t T,
+                                                          const double *__restrict__ ks,
+                                                          const uint2 *__restrict__ bins,
+                                                          const uint32_t *__restrict__ binCounts, size_t binCapacity,
+                                                          int bin, double *__restrict__ records, int *error) {
+    constexpr int PPC = 192 / NP;
+    constexpr int RO = ruleOffset<NP>();
+    __shared__ double sS[192][18];
+    __shared__ double sL[192][3];
+    __shared__ double sM[PPC][54];
+    const int f = blockIdx.y;
+    const double k = ks[f], invk = 1.0 / k;
+    const uint32_t count = binCounts[f * kBins + bin];
+    const uint2 *list = bins + (size_t(f) * kBins + bin) * binCapacity;
+    double *rec = records + size_t(f) * T * T * kRecordDoubles;
+    const int l = threadIdx.x / NP, x = threadIdx.x % NP;
+    for (uint32_t base = blockIdx.x * PPC; base < count; base += gridDim.x * PPC) {
+        const uint32_t p = base + l;
+        if (p < count) {
+            const uint2 pr = list[p];
+            const DPanel &A = panels[pr.x];
+            const DPanel &S = panels[pr.y];
+            const double bx1 = cRule[4 * (RO + x) + 1], bx2 = cRule[4 * (RO + x) + 2];
+            const double X0 = A.e1[0] * bx1 + A.e2[0] * bx2, X1 = A.e1[1] * bx1 + A.e2[1] * bx2,
+                         X2 = A.e1[2] * bx1 + A.e2[2] * bx2;
+            const double d0 = A.v0[0] - S.v0[0], d1 = A.v0[1] - S.v0[1], d2 = A.v0[2] - S.v0[2];
+            const double w0 = cRule[4 * (RO + x) + 3] * 4.0 * A.area * S.area * kInvFourPi;
+            const double nt0 = A.n[0], nt1 = A.n[1], nt2 = A.n[2], ns0 = S.n[0], ns1 = S.n[1], ns2 = S.n[2];
+            const double se10 = S.e1[0], se11 = S.e1[1], se12 = S.e1[2], se20 = S.e2[0], se21 = S.e2[1],
+                         se22 = S.e2[2];
+            double sp[6] = {0, 0, 0, 0, 0, 0}, sq[6] = {0, 0, 0, 0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0};
+            bool bad = false;
+#pragma unroll 4
+            for (int y = 0; y < NP; ++y) {
+                const double b0 = cRule[4 * (RO + y)], b1 = cRule[4 * (RO + y) + 1], b2 = cRule[4 * (RO + y) + 2];
+                const double wy = cRule[4 * (RO + y) + 3];
+                const double dx = d0 + (X0 - (se10 * b1 + se20 * b2));
+                const double dy = d1 + (X1 - (se11 * b1 + se21 * b2));
+                const double dz = d2 + (X2 - (se12 * b1 + se22 * b2));
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                bad |= !(r2 > 0) || !isfinite(r2);
+                const double rinv = rsqrt(r2);
+                const double r = r2 * rinv, kr = k * r;
+                double sn, cs;
+                sincos(kr, &sn, &cs);
+                const double sc = w0 * wy * rinv;
+                const double gr = cs * sc, gi = -sn * sc;
+                const double rr = gr - gi * kr, ri = gi + gr * kr;
+                const double rinv2 = rinv * rinv;
+                const double ps = (dx * ns0 + dy * ns1 + dz * ns2) * rinv2;
+                const double qt = -(dx * nt0 + dy * nt1 + dz * nt2) * rinv2;
+                const double Pr = rr * ps, Pi = ri * ps, Qr = rr * qt, Qi = ri * qt;
+                const double bb[3] = {b0, b1, b2};
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    sp[2 * j] += Pr * bb[j];
+                    sp[2 * j + 1] += Pi * bb[j];
+                    sq[2 * j] += Qr * bb[j];
+                    sq[2 * j + 1] += Qi * bb[j];
+                    sg[2 * j] += gr * bb[j];
+                    sg[2 * j + 1] += gi * bb[j];
+                }
+            }
+            if (bad)
+                flagError(error, kErrDistance);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) {
+                sS[threadIdx.x][c] = sg[c];
+                sS[threadIdx.x][6 + c] = sp[c];
+                sS[threadIdx.x][12 + c] = sq[c];
+            }
+            sL[threadIdx.x][0] = cRule[4 * (RO + x)];
+            sL[threadIdx.x][1] = bx1;
+            sL[threadIdx.x][2] = bx2;
+        }
+        __syncthreads();
+        // Test-side contraction: M[kind][i][j] = sum_x bt_i(x) S_kind,j(x).
+        for (int item = threadIdx.x; item < PPC * 27; item += 192) {
+            const int pl = item / 27, e = item % 27, kind = e / 9, i = (e % 9) / 3, j = e % 3;
+            if (base + pl >= count)
+                continue;
+            double re = 0, im = 0;
+            for (int xx = 0; xx < NP; ++xx) {
+                const int th = pl * NP + xx;
+                re += sL[th][i] * sS[th][kind * 6 + 2 * j];
+                im += sL[th][i] * sS[th][kind * 6 + 2 * j + 1];
+            }
+            sM[pl][kind * 18 + 2 * (3 * i + j)] = re;
+            sM[pl][kind * 18 + 2 * (3 * i + j) + 1] = im;
+        }
+        __syncthreads();
+        for (int item = threadIdx.x; item < PPC * 24; item += 192) {
+            const int pl = item / 24, o = item % 24;
+            if (base + pl >= count)
+                continue;
+            const uint2 pr = list[base + pl];
+            double re, im;
+            pairRecordValue(o, &sM[pl][0], &sM[pl][18], &sM[pl][36], panels[pr.x], panels[pr.y], k, invk, re, im);
+            const size_t slot = o < 12 ? size_t(pr.y) * T + pr.x : size_t(pr.x) * T + pr.y;
+            const int e = o < 12 ? o : o - 12;
+            double *dst = rec + slot * kRecordDoubles + 2 * e;
+            if (!isfinite(re) || !isfinite(im))
+                flagError(error, kErrNonFinite);
+            dst[0] = re;
+            dst[1] = im;
+        }
+        __syncthreads();
+    }
+}
+
+// Sorts unordered regular pairs of each frequency into rule bins.
+__global__ void classifyPairsKernel(const uint8_t *__restrict__ pairCode, const Bounds *__restrict__ bounds,
+                                    uint64_t pairs, const double *__restrict__ ks, double tol, uint32_t minDegree,
+                                    uint2 *bins, uint32_t *binCounts, size_t binCapacity, int *error) {
+    const int f = blockIdx.y;
+    const double k = ks[f];
+    const unsigned lane = threadIdx.x & 31;
+    for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < pairs; base += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t u = base + threadIdx.x;
+        int bin = -1;
+        uint32_t i = 0, j = 0;
+        if (u < pairs) {
+            uint64_t hi = uint64_t((1.0 + sqrt(1.0 + 8.0 * double(u))) * 0.5);
+            while (hi * (hi - 1) / 2 > u)
+                --hi;
+            while ((hi + 1) * hi / 2 <= u)
+                ++hi;
+            i = uint32_t(u - hi * (hi - 1) / 2);
+            j = uint32_t(hi);
+            const uint8_t code = pairCode[u];
+            if (code == kPairWhole8)
+                bin = 2;
+            else if (code == kPairWhole14)
+                bin = 3;
+            else if (code == kPairRegular) {
+                const unsigned d = qualifiedDegree(bounds[i], bounds[j], k, tol, minDegree);
+                if (d == 4)
+                    bin = 0;
+                else if (d == 6)
+                    bin = 1;
+                else if (d == 8)
+                    bin = 2;
+                else
+                    flagError(error, kErrEscapedPlan);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kBins; ++b) {
+            const unsigned mask = __ballot_sync(0xffffffffu, bin == b);
+            if (!mask)
+                continue;
+            uint32_t start = 0;
+            if (lane == unsigned(__ffs(mask) - 1))
+                start = atomicAdd(&binCounts[f * kBins + b], uint32_t(__popc(mask)));
+            start = __shfl_sync(0xffffffffu, start, __ffs(mask) - 1);
+            if (bin == b)
+                bins[(size_t(f) * kBins + b) * binCapacity + start + __popc(mask & ((1u << lane) - 1))] = make_uint2(i, j);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Touching pairs (cuda_solver.cu:382-429): one CTA per ordered job, threads
+// over (sector, u, v, w), the radial Gauss variable factored out because
+// every sector map is linear in r about the shared vertex.
+// ---------------------------------------------------------------------------
+struct Moments13 {
+    double m[18], b[6], g[2];
+};
+
+__device__ __forceinline__ void sampleFp64(Moments13 &acc, const DPanel &t, const DPanel &s, double dx, double dy,
+                                           double dz, const double *bt, const double *bs, double w, double k,
+                                           double invk, bool coincident, bool &bad) {
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    bad |= !(r2 > 0) || !isfinite(r2);
+    const double rinv = rsqrt(r2);
+    const double r = r2 * rinv, kr = k * r;
+    double sn, cs;
+    sincos(kr, &sn, &cs);
+    const double sc = w * rinv;
+    const double gr = cs * sc, gi = -sn * sc;
+    acc.g[0] += gr;
+    acc.g[1] += gi;
+    const double rr = gr - gi * kr, ri = gi + gr * kr;
+    const double rinv2 = rinv * rinv;
+    const double ps = coincident ? 0.0 : (dx * s.n[0] + dy * s.n[1] + dz * s.n[2]) * rinv2;
+    const double qt = coincident ? 0.0 : -(dx * t.n[0] + dy * t.n[1] + dz * t.n[2]) * rinv2;
+    const double nn = t.n[0] * s.n[0] + t.n[1] * s.n[1] + t.n[2] * s.n[2];
+    const double ar = -rr * ps - k * nn * gi, ai = -ri * ps + k * nn * gr;
+    const double br = -gr - ri * qt * invk, bi = -gi + rr * qt * invk;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        acc.b[2 * i] += br * bt[i];
+        acc.b[2 * i + 1] += bi * bt[i];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double bij = bt[i] * bs[j];
+            acc.m[2 * (3 * i + j)] += ar * bij;
+            acc.m[2 * (3 * i + j) + 1] += ai * bij;
+        }
+    }
+}
+
+template <int N>
+__device__ __forceinline__ void blockReduce(double (&v)[N], double (*smem)[N]) {
+#pragma unroll
+    for (int c = 0; c < N; ++c)
+        for (int off = 16; off > 0; off >>= 1)
+            v[c] += __shfl_down_sync(0xffffffffu, v[c], off);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+#pragma unroll
+        for (int c = 0; c < N; ++c)
+            smem[warp][c] = v[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int warps = blockDim.x >> 5;
+        for (int w = 1; w < warps; ++w)
+#pragma unroll
+            for (int c = 0; c < N; ++c)
+                smem[0][c] += smem[w][c];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(128) singularKernel(const DPanel *__restrict__ panels, uint32_t T,
+                                                      const TouchingJob *__restrict__ jobs,
+                                                      const double *__restrict__ ks,
+                                                      const double *__restrict__ gauss, uint32_t order,
+                                                      double *__restrict__ records, int *error) {
+    __shared__ double red[4][26];
+    const TouchingJob job = jobs[blockIdx.x];
+    const int f = blockIdx.y;
+    const double k = ks[f], invk = 1.0 / k;
+    const DPanel &t = panels[job.test];
+    const DPanel &s = panels[job.trial];
+    const bool coincident = job.topology == kCoincident;
+    Permutation perm;
+    perm.topology = job.topology;
+    for (int i = 0; i < 3; ++i) {
+        perm.test[i] = job.permTest[i];
+        perm.trial[i] = job.permTrial[i];
+    }
+    const double w4 = 4.0 * t.area * s.area * kInvFourPi;
+    const uint32_t per = order * order * order;
+    const uint32_t count = sectorCount(job.topology) * per;
+    Moments13 acc;
+#pragma unroll
+    for (int c = 0; c < 18; ++c)
+        acc.m[c] = 0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        acc.b[c] = 0;
+    acc.g[0] = acc.g[1] = 0;
+    bool bad = false;
+    for (uint32_t idx = threadIdx.x; idx < count; idx += blockDim.x) {
+        uint32_t tuple = idx % per;
+        const uint32_t w = tuple % order;
+        tuple /= order;
+        const uint32_t v = tuple % order;
+        const uint32_t u = tuple / order;
+        PairPoint p = sauterSchwab(job.topology, idx / per, 1.0, gauss[2 * u], gauss[2 * v], gauss[2 * w]);
+        p.w *= gauss[2 * u + 1] * gauss[2 * v + 1] * gauss[2 * w + 1];
+        p = permutePoint(p, perm);
+        const double lx = (t.v0[0] - s.v0[0]) + ((t.e1[0] * p.t[1] + t.e2[0] * p.t[2]) - (s.e1[0] * p.s[1] + s.e2[0] * p.s[2]));
+        const double ly = (t.v0[1] - s.v0[1]) + ((t.e1[1] * p.t[1] + t.e2[1] * p.t[2]) - (s.e1[1] * p.s[1] + s.e2[1] * p.s[2]));
+        const double lz = (t.v0[2] - s.v0[2]) + ((t.e1[2] * p.t[1] + t.e2[2] * p.t[2]) - (s.e1[2] * p.s[1] + s.e2[2] * p.s[2]));
+        for (uint32_t ri = 0; ri < order; ++ri) {
+            const double r = gauss[2 * ri];
+            double bt[3], bs[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                bt[i] = r * p.t[i];
+                bs[i] = r * p.s[i];
+            }
+            bt[perm.test[0]] += 1 - r;
+            bs[perm.trial[0]] += 1 - r;
+            sampleFp64(acc, t, s, lx * r, ly * r, lz * r, bt, bs, p.w * r * r * r * gauss[2 * ri + 1] * w4, k, invk,
+                       coincident, bad);
+        }
+    }
+    if (bad)
+        flagError(error, kErrDistance);
+    double v[26];
+#pragma unroll
+    for (int c = 0; c < 18; ++c)
+        v[c] = acc.m[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        v[18 + c] = acc.b[c];
+    v[24] = acc.g[0];
+    v[25] = acc.g[1];
+    blockReduce<26>(v, red);
+    if (threadIdx.x < 12) {
+        const int o = threadIdx.x;
+        double re, im;
+        if (o < 9) {
+            const int i = o / 3, j = o % 3;
+            const double curl = t.curl[3 * i] * s.curl[3 * j] + t.curl[3 * i + 1] * s.curl[3 * j + 1] +
+                                t.curl[3 * i + 2] * s.curl[3 * j + 2];
+            re = red[0][2 * o] + red[0][25] * curl * invk;
+            im = red[0][2 * o + 1] - red[0][24] * curl * invk;
+        } else {
+            re = red[0][18 + 2 * (o - 9)];
+            im = red[0][18 + 2 * (o - 9) + 1] + (coincident ? t.area / (6.0 * k) : 0.0);
+        }
+        if (!isfinite(re) || !isfinite(im))
+            flagError(error, kErrNonFinite);
+        double *dst = records + size_t(f) * T * T * kRecordDoubles + (size_t(job.trial) * T + job.test) * kRecordDoubles;
+        dst[2 * o] = re;
+        dst[2 * o + 1] = im;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Near pairs (cuda_solver.cu:430-518, near_projection.hpp:228-254): one CTA
+// per unordered pair, both directions from the shared patch samples.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void nearSample(double (&acc)[54], const DPanel &t, const DPanel &s, const double *bt,
+                                           const double *bs, double w, double k, bool &bad) {
+    const double dx = (t.v0[0] - s.v0[0]) + ((t.e1[0] * bt[1] + t.e2[0] * bt[2]) - (s.e1[0] * bs[1] + s.e2[0] * bs[2]));
+    const double dy = (t.v0[1] - s.v0[1]) + ((t.e1[1] * bt[1] + t.e2[1] * bt[2]) - (s.e1[1] * bs[1] + s.e2[1] * bs[2]));
+    const double dz = (t.v0[2] - s.v0[2]) + ((t.e1[2] * bt[1] + t.e2[2] * bt[2]) - (s.e1[2] * bs[1] + s.e2[2] * bs[2]));
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    bad |= !(r2 > 0) || !isfinite(r2);
+    const double rinv = rsqrt(r2);
+    const double r = r2 * rinv, kr = k * r;
+    double sn, cs;
+    sincos(kr, &sn, &cs);
+    const double sc = w * rinv;
+    const double gr = cs * sc, gi = -sn * sc;
+    const double rr = gr - gi * kr, ri = gi + gr * kr;
+    const double rinv2 = rinv * rinv;
+    const double ps = (dx * s.n[0] + dy * s.n[1] + dz * s.n[2]) * rinv2;
+    const double qt = -(dx * t.n[0] + dy * t.n[1] + dz * t.n[2]) * rinv2;
+    const double val[6] = {gr, gi, rr * ps, ri * ps, rr * qt, ri * qt};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double bij = bt[i] * bs[j];
+#pragma unroll
+            for (int kind = 0; kind < 3; ++kind) {
+                acc[kind * 18 + 2 * (3 * i + j)] += val[2 * kind] * bij;
+                acc[kind * 18 + 2 * (3 * i + j) + 1] += val[2 * kind + 1] * bij;
+            }
+        }
+}
+
+__global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ panels, uint32_t T,
+                                                  const NearPairJob *__restrict__ jobs,
+                                                  const Patch *__restrict__ patches, const double *__restrict__ ks,
+                                                  double *__restrict__ records, int *error) {
+    __shared__ double red[4][54];
+    __shared__ double pts[2][64][3];
+    const NearPairJob job = jobs[blockIdx.x];
+    const int f = blockIdx.y;
+    const double k = ks[f], invk = 1.0 / k;
+    const DPanel &t = panels[job.first];
+    const DPanel &s = panels[job.second];
+    const double w4 = 4.0 * t.area * s.area * kInvFourPi;
+    double acc[54];
+#pragma unroll
+    for (int c = 0; c < 54; ++c)
+        acc[c] = 0;
+    bool bad = false;
+    FanPanel ft, fs;
+    for (int i = 0; i < 3; ++i) {
+        ft.v[i] = V3{t.v0[0] + (i == 1 ? t.e1[0] : i == 2 ? t.e2[0] : 0.0), t.v0[1] + (i == 1 ? t.e1[1] : i == 2 ? t.e2[1] : 0.0),
+                     t.v0[2] + (i == 1 ? t.e1[2] : i == 2 ? t.e2[2] : 0.0)};
+        fs.v[i] = V3{s.v0[0] + (i == 1 ? s.e1[0] : i == 2 ? s.e2[0] : 0.0), s.v0[1] + (i == 1 ? s.e1[1] : i == 2 ? s.e2[1] : 0.0),
+                     s.v0[2] + (i == 1 ? s.e1[2] : i == 2 ? s.e2[2] : 0.0)};
+    }
+    ft.n = V3{t.n[0], t.n[1], t.n[2]};
+    fs.n = V3{s.n[0], s.n[1], s.n[2]};
+    ft.area = t.area;
+    fs.area = s.area;
+    for (uint32_t q = 0; q < job.patchCount; ++q) {
+        const Patch &patch = patches[job.firstPatch + q];
+        const int n = patch.degree == 14 ? 64 : 16;
+        const int ro = patch.degree == 14 ? 34 : 18;  // rule offsets of the 16- and 64-point bins
+        if (!patch.projection) {
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < 2 * n; idx += blockDim.x) {
+                const int side = idx / n, x = idx % n;
+                const double *pv = side ? patch.trial : patch.test;
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    pts[side][x][i] = cRule[4 * (ro + x)] * pv[i] + cRule[4 * (ro + x) + 1] * pv[3 + i] +
+                                      cRule[4 * (ro + x) + 2] * pv[6 + i];
+            }
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+                const int x = idx / n, y = idx % n;
+                const double w = cRule[4 * (ro + x) + 3] * cRule[4 * (ro + y) + 3] * patch.areaFraction * w4;
+                nearSample(acc, t, s, pts[0][x], pts[1][y], w, k, bad);
+            }
+            continue;
+        }
+        const uint32_t order = 20 * patch.intervals;
+        const uint32_t points = uint32_t(n) * 3 * order * order;
+        for (uint32_t idx = threadIdx.x; idx < points; idx += blockDim.x) {
+            uint32_t rest = idx;
+            const uint32_t radial = rest % order;
+            rest /= order;
+            const uint32_t angular = rest % order;
+            rest /= order;
+            const uint32_t edge = rest % 3, outer = rest / 3;
+            GaussPoint u{cGauss20[2 * (angular % 20)], cGauss20[2 * (angular % 20) + 1]};
+            GaussPoint v{cGauss20[2 * (radial % 20)], cGauss20[2 * (radial % 20) + 1]};
+            u.x = (angular / 20 + u.x) / patch.intervals;
+            v.x = (radial / 20 + v.x) / patch.intervals;
+            u.w /= patch.intervals;
+            v.w /= patch.intervals;
+            const double ob[3] = {cRule[4 * (ro + outer)], cRule[4 * (ro + outer) + 1], cRule[4 * (ro + outer) + 2]};
+            const ProjOuter po = projOuter(ob, cRule[4 * (ro + outer) + 3], patch, ft, fs);
+            const PairPoint pp = projPoint(po, projRay(po, projEdge(po, edge, fs), u), v);
+            nearSample(acc, t, s, pp.t, pp.s, pp.w * w4, k, bad);
+        }
+    }
+    if (bad)
+        flagError(error, kErrDistance);
+    __syncthreads();
+    blockReduce<54>(acc, red);
+    if (threadIdx.x < 24) {
+        const int o = threadIdx.x;
+        double re, im;
+        pairRecordValue(o, &red[0][0], &red[0][18], &red[0][36], t, s, k, invk, re, im);
+        if (!isfinite(re) || !isfinite(im))
+            flagError(error, kErrNonFinite);
+        const size_t slot = o < 12 ? size_t(job.second) * T + job.first : size_t(job.first) * T + job.second;
+        const int e = o < 12 ? o : o - 12;
+        double *dst = records + size_t(f) * T * T * kRecordDoubles + slot * kRecordDoubles + 2 * e;
+        dst[0] = re;
+        dst[1] = im;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Deterministic gathers: records -> per-(test panel, trial vertex) columns ->
+// matrix entries, and records x flux -> right-hand side.
+// ---------------------------------------------------------------------------
+__global__ void gatherTrialKernel(const double *__restrict__ records, const uint32_t *__restrict__ incOffsets,
+                                  const uint32_t *__restrict__ incPanel, const uint8_t *__restrict__ incLocal,
+                                  uint32_t T, uint32_t N, double *__restrict__ columns) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t b = blockIdx.y;
+    const int f = blockIdx.z;
+    if (t >= T)
+        return;
+    const double *rec = records + size_t(f) * T * T * kRecordDoubles;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t o = incOffsets[b]; o < incOffsets[b + 1]; ++o) {
+        const uint32_t s = incPanel[o];
+        const int lb = incLocal[o];
+        const double *r = rec + (size_t(s) * T + t) * kRecordDoubles;
+#pragma unroll
+        for (int la = 0; la < 3; ++la) {
+            acc[2 * la] += r[2 * (3 * la + lb)];
+            acc[2 * la + 1] += r[2 * (3 * la + lb) + 1];
+        }
+    }
+    double *dst = columns + (size_t(f) * N + b) * 6 * T + 6 * size_t(t);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        dst[c] = acc[c];
+}
+
+__global__ void gatherTestKernel(const double *__restrict__ columns, const DPanel *__restrict__ panels,
+                                 const uint32_t *__restrict__ incOffsets, const uint32_t *__restrict__ incPanel,
+                                 const uint8_t *__restrict__ incLocal, const double *__restrict__ rowScale, uint32_t T,
+                                 uint32_t N, double *__restrict__ A) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t b = blockIdx.y;
+    const int f = blockIdx.z;
+    if (a >= N)
+        return;
+    const double *col = columns + (size_t(f) * N + b) * 6 * T;
+    double re = 0, im = 0;
+    for (uint32_t o = incOffsets[a]; o < incOffsets[a + 1]; ++o) {
+        const uint32_t t = incPanel[o];
+        const int la = incLocal[o];
+        re += col[6 * size_t(t) + 2 * la];
+        im += col[6 * size_t(t) + 2 * la + 1];
+        const DPanel &p = panels[t];
+        if (p.nodes[0] == b || p.nodes[1] == b || p.nodes[2] == b)
+            re += p.area * (a == b ? 2.0 : 1.0) / 24.0;
+    }
+    const double sc = rowScale[a];
+    double *dst = A + (size_t(f) * N * N + size_t(b) * N + a) * 2;
+    dst[0] = re * sc;
+    dst[1] = im * sc;
+}
+
+__global__ void rhsPanelKernel(const double *__restrict__ records, const double *__restrict__ flux, uint32_t T,
+                               uint32_t E, double *__restrict__ panelRhs) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t e = blockIdx.y;
+    const int f = blockIdx.z;
+    if (t >= T)
+        return;
+    const double *rec = records + size_t(f) * T * T * kRecordDoubles;
+    const double *q = flux + (size_t(f) * E + e) * 2 * T;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t s = 0; s < T; ++s) {
+        const double qr = q[2 * s], qi = q[2 * s + 1];
+        if (qr == 0 && qi == 0)
+            continue;
+        const double *r = rec + (size_t(s) * T + t) * kRecordDoubles + 18;
+#pragma unroll
+        for (int la = 0; la < 3; ++la) {
+            acc[2 * la] += r[2 * la] * qr - r[2 * la + 1] * qi;
+            acc[2 * la + 1] += r[2 * la] * qi + r[2 * la + 1] * qr;
+        }
+    }
+    double *dst = panelRhs + (size_t(f) * E + e) * 6 * T + 6 * size_t(t);
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        dst[c] = acc[c];
+}
+
+__global__ void rhsVertexKernel(const double *__restrict__ panelRhs, const uint32_t *__restrict__ incOffsets,
+                                const uint32_t *__restrict__ incPanel, const uint8_t *__restrict__ incLocal,
+                                const double *__restrict__ rowScale, uint32_t T, uint32_t N, uint32_t E,
+                                double *__restrict__ rhs) {
+    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t e = blockIdx.y;
+    const int f = blockIdx.z;
+    if (a >= N)
+        return;
+    const double *src = panelRhs + (size_t(f) * E + e) * 6 * T;
+    double re = 0, im = 0;
+    for (uint32_t o = incOffsets[a]; o < incOffsets[a + 1]; ++o) {
+        re += src[6 * size_t(incPanel[o]) + 2 * incLocal[o]];
+        im += src[6 * size_t(incPanel[o]) + 2 * incLocal[o] + 1];
+    }
+    double *dst = rhs + ((size_t(f) * E + e) * N + a) * 2;
+    dst[0] = re * rowScale[a];
+    dst[1] = im * rowScale[a];
+}
+
+int smCount() {
+    static int count = 0;
+    if (!count) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        if (count <= 0)
+            count = 148;
+    }
+    return count;
+}
+
+template <int NP>
+void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, const AssemblyWorkspace &ws, int bin,
+                   int *error, cudaStream_t stream, KernelTimer *timer) {
+    const char *names[kBins] = {"regular_q6", "regular_q12", "regular_q16", "regular_q64"};
+    TimedScope scope(timer, names[bin], stream);
+    const dim3 grid(unsigned(smCount() * 6), B);
+    regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity, bin,
+                                                     ws.records, error);
+    cudaCheck(cudaGetLastError(), "regular pair assembly launch");
+}
+
+}  // namespace
+
+void uploadRuleTables(cudaStream_t stream) {
+    static bool done = false;
+    if (done)
+        return;
+    double table[kRulePoints * 4];
+    const unsigned degrees[kBins] = {4, 6, 8, 14};
+    int o = 0;
+    for (int b = 0; b < kBins; ++b) {
+        const auto r = triangleRule(degrees[b]);
+        for (const auto &p : r) {
+            table[4 * o] = p.b[0];
+            table[4 * o + 1] = p.b[1];
+            table[4 * o + 2] = p.b[2];
+            table[4 * o + 3] = p.w;
+            ++o;
+        }
+    }
+    cudaCheck(cudaMemcpyToSymbolAsync(cRule, table, sizeof(table), 0, cudaMemcpyHostToDevice, stream), "rule upload");
+    double g20[40];
+    const auto g = gaussLegendre01(20);
+    for (int i = 0; i < 20; ++i) {
+        g20[2 * i] = g[i].x;
+        g20[2 * i + 1] = g[i].w;
+    }
+    cudaCheck(cudaMemcpyToSymbolAsync(cGauss20, g20, sizeof(g20), 0, cudaMemcpyHostToDevice, stream), "gauss upload");
+    cudaCheck(cudaStreamSynchronize(stream), "rule upload sync");
+    done = true;
+}
+
+size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B) {
+    const size_t pairs = size_t(T) * (T - 1) / 2;
+    return size_t(B) * (size_t(T) * T * kRecordDoubles * 8 + size_t(N) * 6 * T * 8 + size_t(E) * 6 * T * 8 +
+                        kBins * pairs * sizeof(uint2) + kBins * sizeof(uint32_t));
+}
+
+void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *gaussSingular, const double *flux,
+                   uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
+                   cudaStream_t stream, KernelTimer *timer) {
+    const uint64_t pairs = uint64_t(g.T) * (g.T - 1) / 2;
+    if (g.N > 65535 || B > 65535 || E > 65535)
+        throw std::runtime_error("Dense assembly grid limits exceeded (more than 65535 vertices, frequencies or excitations).");
+    cudaCheck(cudaMemsetAsync(ws.binCounts, 0, sizeof(uint32_t) * kBins * B, stream), "bin reset");
+    if (pairs) {
+        TimedScope scope(timer, "classify_pairs", stream);
+        const unsigned blocks = unsigned(std::min<uint64_t>((pairs + 255) / 256, uint64_t(smCount()) * 16));
+        classifyPairsKernel<<<dim3(blocks, B), 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, g.nearTolerance,
+                                                                 g.minimumDegree, ws.bins, ws.binCounts,
+                                                                 ws.binCapacity, error);
+        cudaCheck(cudaGetLastError(), "pair classification launch");
+    }
+    launchRegular<6>(g, ks, B, ws, 0, error, stream, timer);
+    launchRegular<12>(g, ks, B, ws, 1, error, stream, timer);
+    launchRegular<16>(g, ks, B, ws, 2, error, stream, timer);
+    launchRegular<64>(g, ks, B, ws, 3, error, stream, timer);
+    if (g.touchingCount) {
+        TimedScope scope(timer, "singular", stream);
+        singularKernel<<<dim3(g.touchingCount, B), 128, 0, stream>>>(g.panels, g.T, g.touching, ks, gaussSingular,
+                                                                     g.singularOrder, ws.records, error);
+        cudaCheck(cudaGetLastError(), "singular assembly launch");
+    }
+    if (g.nearPairCount) {
+        TimedScope scope(timer, "near", stream);
+        nearKernel<<<dim3(g.nearPairCount, B), 128, 0, stream>>>(g.panels, g.T, g.nearPairs, g.patches, ks,
+                                                                 ws.records, error);
+        cudaCheck(cudaGetLastError(), "near assembly launch");
+    }
+    {
+        TimedScope scope(timer, "gather_trial", stream);
+        gatherTrialKernel<<<dim3((g.T + 127) / 128, g.N, B), 128, 0, stream>>>(ws.records, g.incOffsets, g.incPanel,
+                                                                               g.incLocal, g.T, g.N, ws.columns);
+        cudaCheck(cudaGetLastError(), "trial gather launch");
+    }
+    {
+        TimedScope scope(timer, "gather_test", stream);
+        gatherTestKernel<<<dim3((g.N + 127) / 128, g.N, B), 128, 0, stream>>>(
+            ws.columns, g.panels, g.incOffsets, g.incPanel, g.incLocal, g.rowScale, g.T, g.N, A);
+        cudaCheck(cudaGetLastError(), "test gather launch");
+    }
+    {
+        TimedScope scope(timer, "rhs", stream);
+        rhsPanelKernel<<<dim3((g.T + 127) / 128, E, B), 128, 0, stream>>>(ws.records, flux, g.T, E, ws.panelRhs);
+        rhsVertexKernel<<<dim3((g.N + 127) / 128, E, B), 128, 0, stream>>>(ws.panelRhs, g.incOffsets, g.incPanel,
+                                                                           g.incLocal, g.rowScale, g.T, g.N, E, rhs);
+        cudaCheck(cudaGetLastError(), "rhs gather launch");
+    }
+}
+
+}  // namespace hsb

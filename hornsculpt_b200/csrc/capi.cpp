@@ -1,0 +1,345 @@
+// extern "C" entry points of include/hs_bem.h: exceptions of the session
+// layer become hs_status codes plus a thread-local message.
+#include "hs_bem.h"
+#include "session.hpp"
+
+#include <cstring>
+#include <string>
+
+using namespace hsb;
+
+struct hs_bem_session {
+    std::unique_ptr<Session> impl;
+};
+struct hs_result {
+    std::unique_ptr<Result> impl;
+};
+
+namespace {
+thread_local std::string lastError;
+
+hs_status fail(hs_status code, const char *message) {
+    lastError = message;
+    return code;
+}
+
+template <class F> hs_status guarded(F &&f) {
+    try {
+        f();
+        return HS_OK;
+    } catch (const InvalidArgument &e) {
+        return fail(HS_E_INVALID, e.what());
+    } catch (const std::invalid_argument &e) {
+        return fail(HS_E_INVALID, e.what());
+    } catch (const Cancelled &e) {
+        return fail(HS_E_CANCELLED, e.what());
+    } catch (const NoConvergence &e) {
+        return fail(HS_E_NOCONVERGE, e.what());
+    } catch (const OutOfMemory &e) {
+        return fail(HS_E_NOMEM, e.what());
+    } catch (const Unsupported &e) {
+        return fail(HS_E_UNSUPPORTED, e.what());
+    } catch (const NumericError &e) {
+        return fail(HS_E_NUMERIC, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(HS_E_NOMEM, "Host allocation failed.");
+    } catch (const std::exception &e) {
+        return fail(HS_E_CUDA, e.what());
+    }
+}
+
+const ExcitationResult *excitation(const hs_result *r, size_t f, size_t e) {
+    if (!r || !r->impl || f >= r->impl->frequencies.size() || e >= r->impl->frequencies[f].excitations.size())
+        return nullptr;
+    return &r->impl->frequencies[f].excitations[e];
+}
+hs_status copyComplex(const std::vector<cplx> &v, double *out) {
+    if (!out && !v.empty())
+        return fail(HS_E_INVALID, "Output buffer is null.");
+    if (!v.empty())
+        std::memcpy(out, v.data(), v.size() * sizeof(cplx));
+    return HS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+void hs_numerics_default(hs_numerics *o) {
+    if (!o)
+        return;
+    *o = hs_numerics{};
+    o->quadrature_order = 4;
+    o->singular_order = 4;
+    o->near_distance_ratio = 1.0;
+    o->near_relative_tolerance = 1e-4;
+    o->near_maximum_depth = 6;
+    o->relative_residual_tolerance = 5e-5;
+    o->maximum_refinement_steps = 3;
+    o->acceleration = HS_DENSE;
+    o->precision = HS_PRECISION_FP64;
+    o->fmm_leaf_support_capacity = 16;
+    o->fmm_separation_ratio = 1.5;
+    o->fmm_maximum_iterations = 300;
+    o->fmm_restart_length = 40;
+    o->fmm_preconditioner_block_width = 32;
+}
+
+hs_status hs_bem_session_create(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                const uint32_t *face_ids, const uint8_t *boundary, size_t triangle_count,
+                                uint32_t residency, hs_bem_session **out) {
+    if (!out)
+        return fail(HS_E_INVALID, "Session output pointer is null.");
+    *out = nullptr;
+    if ((!vertices && vertex_count) || (!triangle_count || !triangles || !face_ids || !boundary))
+        return fail(HS_E_INVALID, "BEM mesh has no vertices.");
+    return guarded([&]() {
+        MeshInput mesh;
+        mesh.vertices.resize(vertex_count);
+        for (size_t i = 0; i < vertex_count; ++i)
+            mesh.vertices[i] = V3{vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]};
+        mesh.triangles.assign(triangles, triangles + 3 * triangle_count);
+        mesh.faces.assign(face_ids, face_ids + triangle_count);
+        mesh.driven.resize(triangle_count);
+        for (size_t t = 0; t < triangle_count; ++t) {
+            if (boundary[t] > HS_DRIVEN)
+                throw InvalidArgument("Triangle boundary must be wall (0) or driven (1).");
+            mesh.driven[t] = boundary[t];
+        }
+        auto s = std::make_unique<hs_bem_session>();
+        s->impl = std::make_unique<Session>(mesh, residency);
+        *out = s.release();
+    });
+}
+
+void hs_bem_session_destroy(hs_bem_session *s) { delete s; }
+
+hs_status hs_bem_session_set_stream(hs_bem_session *s, void *stream) {
+    if (!s)
+        return fail(HS_E_INVALID, "Session is null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->setStream(static_cast<cudaStream_t>(stream));
+    });
+}
+
+hs_status hs_bem_solve(hs_bem_session *s, const hs_request *request, const volatile int32_t *cancel,
+                       hs_progress_fn progress, void *user, hs_result **out) {
+    if (!s || !request || !out)
+        return fail(HS_E_INVALID, "Session, request and result pointers must be non-null.");
+    *out = nullptr;
+    if ((request->frequency_count && !request->frequencies) ||
+        (request->plan_frequency_count && !request->plan_frequencies) ||
+        (request->excitation_count && !request->excitation_face_offsets) ||
+        (request->observer_count && !request->observers))
+        return fail(HS_E_INVALID, "Invalid BEM medium, frequencies, excitation or Galerkin settings.");
+    if (request->excitation_count) {
+        const size_t faces = request->excitation_face_offsets[request->excitation_count];
+        if (faces && (!request->excitation_face_ids || !request->excitation_velocities))
+            return fail(HS_E_INVALID, "Excitation must assign each known Driven face at most once.");
+        for (size_t e = 0; e < request->excitation_count; ++e)
+            if (request->excitation_face_offsets[e] > request->excitation_face_offsets[e + 1])
+                return fail(HS_E_INVALID, "Excitation face offsets must be nondecreasing.");
+    }
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        auto r = std::make_unique<hs_result>();
+        r->impl = s->impl->solve(*request, cancel, progress, user);
+        *out = r.release();
+    });
+}
+
+size_t hs_result_frequency_count(const hs_result *r) { return r && r->impl ? r->impl->frequencies.size() : 0; }
+size_t hs_result_excitation_count(const hs_result *r) { return r && r->impl ? r->impl->E : 0; }
+size_t hs_result_triangle_count(const hs_result *r) { return r && r->impl ? r->impl->T : 0; }
+size_t hs_result_pressure_dof_count(const hs_result *r) { return r && r->impl ? r->impl->N : 0; }
+size_t hs_result_observer_count(const hs_result *r) { return r && r->impl ? r->impl->O : 0; }
+size_t hs_result_peak_device_bytes(const hs_result *r) { return r && r->impl ? r->impl->peakDeviceBytes : 0; }
+
+hs_status hs_result_frequency_info(const hs_result *r, size_t f, hs_frequency_info *out) {
+    if (!r || !r->impl || !out || f >= r->impl->frequencies.size())
+        return fail(HS_E_INVALID, "Result index out of range.");
+    *out = r->impl->frequencies[f].info;
+    return HS_OK;
+}
+hs_status hs_result_excitation_info(const hs_result *r, size_t f, size_t e, hs_excitation_info *out) {
+    const ExcitationResult *x = excitation(r, f, e);
+    if (!x || !out)
+        return fail(HS_E_INVALID, "Result index out of range.");
+    out->boundary_residual = x->residual;
+    out->refinement_steps = x->refinements;
+    out->iterations = 0;
+    out->field_comparison_degree = x->fieldDegree;
+    out->field_verification_degree = x->fieldNext;
+    out->field_discrepancy = x->fieldDiscrepancy;
+    out->impedance_count = x->impedances.size();
+    return HS_OK;
+}
+hs_status hs_result_pressure_trace(const hs_result *r, size_t f, size_t e, double *out) {
+    const ExcitationResult *x = excitation(r, f, e);
+    return x ? copyComplex(x->trace, out) : fail(HS_E_INVALID, "Result index out of range.");
+}
+hs_status hs_result_surface_pressure(const hs_result *r, size_t f, size_t e, double *out) {
+    const ExcitationResult *x = excitation(r, f, e);
+    return x ? copyComplex(x->surface, out) : fail(HS_E_INVALID, "Result index out of range.");
+}
+hs_status hs_result_normal_derivative(const hs_result *r, size_t f, size_t e, double *out) {
+    const ExcitationResult *x = excitation(r, f, e);
+    return x ? copyComplex(x->normalDerivative, out) : fail(HS_E_INVALID, "Result index out of range.");
+}
+hs_status hs_result_observer_pressure(const hs_result *r, size_t f, size_t e, double *out) {
+    const ExcitationResult *x = excitation(r, f, e);
+    return x ? copyComplex(x->observer, out) : fail(HS_E_INVALID, "Result index out of range.");
+}
+hs_status hs_result_impedances(const hs_result *r, size_t f, size_t e, hs_face_impedance *out) {
+    const ExcitationResult *x = excitation(r, f, e);
+    if (!x || (!out && !x->impedances.empty()))
+        return fail(HS_E_INVALID, "Result index out of range.");
+    if (!x->impedances.empty())
+        std::memcpy(out, x->impedances.data(), x->impedances.size() * sizeof(hs_face_impedance));
+    return HS_OK;
+}
+void hs_result_free(hs_result *r) { delete r; }
+
+const char *hs_last_error(void) { return lastError.c_str(); }
+
+hs_status hs_device_description(char *buffer, size_t size) {
+    int count = 0, dev = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || !count)
+        return fail(HS_E_CUDA, "No CUDA device is available.");
+    cudaDeviceProp prop{};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess)
+        return fail(HS_E_CUDA, "CUDA device properties");
+    if (buffer && size) {
+        std::strncpy(buffer, prop.name, size - 1);
+        buffer[size - 1] = 0;
+    }
+    return HS_OK;
+}
+
+hs_status hs_bem_session_set_profiling(hs_bem_session *s, int32_t enabled) {
+    if (!s)
+        return fail(HS_E_INVALID, "Session is null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->timer().reset();
+        s->impl->timer().enable(enabled != 0);
+        std::fill(s->impl->work.begin(), s->impl->work.end(), 0);
+    });
+}
+
+hs_status hs_bem_session_work(const hs_bem_session *s, uint64_t *counters, size_t capacity, size_t *count) {
+    if (!s || !count)
+        return fail(HS_E_INVALID, "Session is null.");
+    std::lock_guard<std::mutex> lock(s->impl->mutex);
+    const auto &w = s->impl->work;
+    *count = std::min(capacity, w.size());
+    for (size_t i = 0; i < *count && counters; ++i)
+        counters[i] = w[i];
+    return HS_OK;
+}
+
+hs_status hs_bem_session_profile(const hs_bem_session *s, char *names, size_t namesSize, double *ms,
+                                 uint64_t *launches, size_t capacity, size_t *count) {
+    if (!s || !count)
+        return fail(HS_E_INVALID, "Session is null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        auto &timer = s->impl->timer();
+        timer.collect();
+        std::string joined;
+        size_t i = 0;
+        for (const auto &[name, total] : timer.totals()) {
+            if (i < capacity) {
+                if (ms)
+                    ms[i] = total.ms;
+                if (launches)
+                    launches[i] = total.launches;
+                joined += (i ? "," : "") + name;
+            }
+            ++i;
+        }
+        *count = std::min(i, capacity);
+        if (names && namesSize) {
+            std::strncpy(names, joined.c_str(), namesSize - 1);
+            names[namesSize - 1] = 0;
+        }
+    });
+}
+
+hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                            size_t triangle_count, const hs_numerics *numerics, double max_k, size_t *sizes,
+                            uint32_t *touching, uint32_t *near, double *patches, uint8_t *whole,
+                            uint32_t *near_offsets, uint32_t *near_trials) {
+    if (!vertices || !vertex_count || !triangles || !triangle_count || !numerics || !sizes)
+        return fail(HS_E_INVALID, "Mesh, numerics and sizes must be non-null.");
+    return guarded([&]() {
+        MeshInput mesh;
+        const V3 origin{vertices[0], vertices[1], vertices[2]};
+        for (size_t i = 0; i < vertex_count; ++i)
+            mesh.vertices.push_back(V3{vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]} - origin);
+        mesh.triangles.assign(triangles, triangles + 3 * triangle_count);
+        mesh.faces.assign(triangle_count, 0);
+        mesh.driven.assign(triangle_count, 0);
+        const Space space = buildSpace(mesh);
+        const Plan p = makePlan(space,
+                                PlanSettings{numerics->quadrature_order, numerics->singular_order,
+                                             numerics->near_distance_ratio, numerics->near_relative_tolerance,
+                                             numerics->near_maximum_depth},
+                                max_k, 0, nullptr);
+        sizes[0] = p.touching.size();
+        sizes[1] = p.near.size();
+        sizes[2] = p.patches.size();
+        sizes[3] = p.wholePanelDegrees.size();
+        sizes[4] = p.nearTrials.size();
+        sizes[5] = p.maxDepth;
+        if (touching)
+            for (const auto &j : p.touching) {
+                *touching++ = j.test;
+                *touching++ = j.trial;
+                *touching++ = j.perm.topology;
+                for (int i = 0; i < 3; ++i)
+                    *touching++ = j.perm.test[i];
+                for (int i = 0; i < 3; ++i)
+                    *touching++ = j.perm.trial[i];
+            }
+        if (near)
+            for (const auto &j : p.near) {
+                *near++ = j.test;
+                *near++ = j.trial;
+                *near++ = j.first;
+                *near++ = j.count;
+                *near++ = j.swap;
+            }
+        if (patches)
+            for (const auto &q : p.patches) {
+                for (int i = 0; i < 9; ++i)
+                    *patches++ = q.test[i];
+                for (int i = 0; i < 9; ++i)
+                    *patches++ = q.trial[i];
+                *patches++ = q.areaFraction;
+                *patches++ = q.degree;
+                *patches++ = q.projection;
+                *patches++ = q.intervals;
+            }
+        if (whole && !p.wholePanelDegrees.empty())
+            std::memcpy(whole, p.wholePanelDegrees.data(), p.wholePanelDegrees.size());
+        if (near_offsets)
+            std::memcpy(near_offsets, p.nearOffsets.data(), p.nearOffsets.size() * 4);
+        if (near_trials && !p.nearTrials.empty())
+            std::memcpy(near_trials, p.nearTrials.data(), p.nearTrials.size() * 4);
+    });
+}
+
+hs_status hs_bem_debug_assemble(hs_bem_session *s, const hs_numerics *numerics, double plan_k, double k,
+                                const double *flux, double *matrix, double *rhs) {
+    if (!s || !numerics || !flux || !matrix || !rhs)
+        return fail(HS_E_INVALID, "Debug assembly pointers must be non-null.");
+    if (!std::isfinite(k) || k <= 0 || !std::isfinite(plan_k) || plan_k < k)
+        return fail(HS_E_INVALID, "Debug assembly needs 0 < k <= plan_k.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->debugAssemble(*numerics, plan_k, k, flux, matrix, rhs);
+    });
+}
+
+}  // extern "C"

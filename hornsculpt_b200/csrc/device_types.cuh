@@ -1,0 +1,118 @@
+// Device-resident data layout of a solver session and the launch interface
+// of the sm_100a kernels (assembly.cu, dense_lu.cu, field.cu).
+#pragma once
+
+#include "pair_rules.cuh"
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hsb {
+
+// One flat panel in HBM (200 B): local-origin vertex 0, edge vectors, unit
+// normal, P1 surface curls, area, longest edge and node ids.
+struct DPanel {
+    double v0[3], e1[3], e2[3], n[3];
+    double curl[9];
+    double area, maxEdge;
+    uint32_t nodes[3], pad;
+};
+
+// Pair-block record of one ordered (test, trial) panel pair: the 3x3 P1xP1
+// Burton-Miller block (curl term included) and the 3 P1xDP0 right-hand-side
+// moments, complex FP64 (24 doubles = 192 B). Records live at
+// slot = trial * T + test so that consecutive test panels are adjacent.
+constexpr int kRecordDoubles = 24;
+
+// Device error word codes (cuda_solver.cu:705-715).
+enum DeviceError : int {
+    kErrDistance = 1,      // zero or invalid source distance
+    kErrNonFinite = 2,     // non-finite assembled value
+    kErrFieldDepth = 3,    // observer near field missed its tolerance
+    kErrEscapedPlan = 4,   // regular pair without a qualified rule
+};
+
+// Unordered-pair codes of the session plan.
+enum PairCode : uint8_t { kPairRegular = 0, kPairTouching = 1, kPairNear = 2, kPairWhole8 = 8, kPairWhole14 = 14 };
+
+// Regular-rule bins: Dunavant degree 4 (6 pts), 6 (12), 8 (16) and the
+// collapsed tensor degree-14 rule (64 pts) of accepted whole-panel pairs.
+constexpr int kBins = 4;
+constexpr int kBinPoints[kBins] = {6, 12, 16, 64};
+
+struct NearPairJob {
+    uint32_t first, second, firstPatch, patchCount;
+};
+struct TouchingJob {
+    uint32_t test, trial;
+    uint32_t topology;
+    uint8_t permTest[3], permTrial[3], pad[2];
+};
+
+struct AssemblyGeometry {
+    const DPanel *panels;
+    const Bounds *bounds;
+    const uint8_t *pairCode;        // T(T-1)/2 unordered pair codes
+    const TouchingJob *touching;
+    const NearPairJob *nearPairs;
+    const Patch *patches;
+    const uint32_t *incOffsets;     // vertex -> (panel, local) incidence
+    const uint32_t *incPanel;
+    const uint8_t *incLocal;
+    const double *rowScale;         // 1 / lumped mass
+    uint32_t T, N;
+    uint32_t touchingCount, nearPairCount;
+    double nearTolerance;
+    uint32_t minimumDegree, singularOrder;
+};
+
+// Quadrature tables copied to __constant__ memory at first use.
+void uploadRuleTables(cudaStream_t stream);
+
+// Per-batch assembly of B frequencies. ks[B]; flux q[B][E][T] complex;
+// outputs A[B][N*N] (column-major) and rhs[B][E][N] complex. Workspace:
+// records [B][T*T][24], gathered columns C[B][N][3T] complex, per-panel rhs
+// partials R[B][E][3T] complex, pair bins [B][4][pairs] and counters.
+struct AssemblyWorkspace {
+    double *records;
+    double *columns;
+    double *panelRhs;
+    uint2 *bins;
+    uint32_t *binCounts;
+    size_t binCapacity;
+};
+size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B);
+void assembleBatch(const AssemblyGeometry &geo, const double *ks, const double *gaussSingular, const double *flux,
+                   uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
+                   cudaStream_t stream, class KernelTimer *timer);
+
+// Batched dense LU (partial pivoting) and solves, complex FP64 column-major.
+size_t luWorkspaceBytes(uint32_t N, uint32_t B);
+void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
+                   class KernelTimer *timer);
+void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
+                  cudaStream_t stream, class KernelTimer *timer);
+// r = b - A x (FP64); writes the correction rhs into `correction` and the
+// mass-scaled residual norm and rhs norm per (batch, excitation) into norms[2].
+void residualBatch(const double *A, const double *b, const double *x, const double *mass, uint32_t N, uint32_t B,
+                   uint32_t E, double *correction, double *norms, cudaStream_t stream, class KernelTimer *timer);
+void addCorrectionBatch(double *x, const double *correction, size_t count, cudaStream_t stream);
+
+// Observer fields of one rule degree for every (batch, excitation, observer).
+struct FieldRequest {
+    const DPanel *panels;
+    uint32_t T, N, E, O, B;
+    const double *observers;     // O x 3 local points or unit directions
+    int farField;
+    double farOrigin[3];
+    double farDistance;
+    double tolerance;
+    uint32_t maximumDepth;
+};
+void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double *pressure, const double *flux,
+                        const uint32_t *batchDegree, double *partials, double *out, int *error,
+                        cudaStream_t stream, class KernelTimer *timer);
+size_t fieldPartialsBytes(uint32_t T, uint32_t E, uint32_t O, uint32_t B);
+
+}  // namespace hsb

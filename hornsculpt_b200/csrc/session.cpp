@@ -1,0 +1,716 @@
+// Solver session orchestration (cuda_solver.cu:1021-1853, dense form).
+#include "session.hpp"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <iomanip>
+#include <limits>
+#include <map>
+#include <set>
+#include <sstream>
+
+namespace hsb {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+double msSince(Clock::time_point t) { return std::chrono::duration<double, std::milli>(Clock::now() - t).count(); }
+
+void cuda(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation)
+        throw OutOfMemory(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess)
+        throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T> void upload(DeviceBuffer &buf, const std::vector<T> &v, cudaStream_t s) {
+    buf.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (!v.empty())
+        cuda(cudaMemcpyAsync(buf.as<void>(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+}
+
+bool sameNumerics(const hs_numerics &a, const hs_numerics &b) {
+    return a.quadrature_order == b.quadrature_order && a.singular_order == b.singular_order &&
+           a.near_distance_ratio == b.near_distance_ratio && a.near_relative_tolerance == b.near_relative_tolerance &&
+           a.near_maximum_depth == b.near_maximum_depth;
+}
+
+// cuda_solver.cu:679-704: solid-angle inside test of a finite observer.
+bool insideSolid(const Space &sp, V3 x) {
+    double angle = 0;
+    for (const auto &pn : sp.panels) {
+        const V3 e0 = pn.v[1] - pn.v[0], e1 = pn.v[2] - pn.v[0], rel = x - pn.v[0];
+        const double scale = std::max(std::sqrt(norm2(x)), std::sqrt(norm2(pn.v[0])));
+        const double tol = std::max(pn.maxEdge * 1e-10, scale * 32 * std::numeric_limits<double>::epsilon());
+        if (std::abs(dot(rel, pn.n)) <= tol) {
+            const double aa = dot(e0, e0), ab = dot(e0, e1), bb = dot(e1, e1), pa = dot(rel, e0), pb = dot(rel, e1);
+            const double det = aa * bb - ab * ab, u = (bb * pa - ab * pb) / det, v = (aa * pb - ab * pa) / det;
+            if (u >= -1e-10 && v >= -1e-10 && u + v <= 1 + 1e-10)
+                return true;
+        }
+        const V3 a = pn.v[0] - x, b = pn.v[1] - x, c = pn.v[2] - x;
+        const double la = std::sqrt(norm2(a)), lb = std::sqrt(norm2(b)), lc = std::sqrt(norm2(c));
+        const double den = la * lb * lc + dot(a, b) * lc + dot(b, c) * la + dot(c, a) * lb;
+        angle += 2 * std::atan2(dot(a, cross(b, c)), den);
+    }
+    return std::abs(angle) > 2 * M_PI;
+}
+
+// regular_qualification.hpp:370-377
+uint32_t refinedDegreeOf(uint32_t d) { return d < 4 ? 4 : d < 6 ? 6 : d < 8 ? 8 : d < 12 ? 12 : d < 14 ? 14 : 0; }
+
+// planning_frequencies.hpp:14-38
+double planningWavenumber(const hs_request &r) {
+    if (!r.frequency_count || !std::isfinite(r.sound_speed) || r.sound_speed <= 0)
+        throw InvalidArgument("Interaction planning requires frequencies and sound speed.");
+    std::set<double> raster;
+    double maximum = 0;
+    for (size_t i = 0; i < r.plan_frequency_count; ++i) {
+        const double f = r.plan_frequencies[i];
+        if (!std::isfinite(f) || f <= 0 || !raster.insert(f).second)
+            throw InvalidArgument("Interaction planning frequencies must be finite, positive and unique.");
+        maximum = std::max(maximum, f);
+    }
+    for (size_t i = 0; i < r.frequency_count; ++i) {
+        const double f = r.frequencies[i];
+        if (!std::isfinite(f) || f <= 0 || (r.plan_frequency_count && !raster.count(f)))
+            throw InvalidArgument("Solved frequency is invalid or absent from its interaction planning raster.");
+        if (!r.plan_frequency_count)
+            maximum = std::max(maximum, f);
+    }
+    const double k = 2 * M_PI * maximum / r.sound_speed;
+    if (!std::isfinite(k))
+        throw InvalidArgument("Interaction planning wavenumber overflows.");
+    return k;
+}
+
+void validateRequest(const hs_request &r) {
+    const hs_numerics &o = r.numerics;
+    const bool fmm = o.acceleration == HS_FAST_MULTIPOLE;
+    const unsigned w = o.fmm_preconditioner_block_width;
+    if ((o.acceleration != HS_DENSE && !fmm) ||
+        (fmm && (o.fmm_leaf_support_capacity < 4 || o.fmm_leaf_support_capacity > 256 ||
+                 !std::isfinite(o.fmm_separation_ratio) || o.fmm_separation_ratio < 1.5 || o.fmm_separation_ratio > 10 ||
+                 o.fmm_maximum_iterations < 1 || o.fmm_maximum_iterations > 10000 || o.fmm_restart_length < 2 ||
+                 o.fmm_restart_length > 300 ||
+                 (w != 32 && w != 64 && w != 128 && w != 256 && w != 512 && w != 1024 && w != 2048))))
+        throw InvalidArgument("Invalid Fast Multipole or GMRES settings.");
+    if (!std::isfinite(r.density) || r.density <= 0 || !std::isfinite(r.sound_speed) || r.sound_speed <= 0 ||
+        !r.frequency_count || !r.excitation_count || (o.quadrature_order != 2 && o.quadrature_order != 4) ||
+        o.singular_order < 2 || o.singular_order > 20 || !std::isfinite(o.near_distance_ratio) ||
+        o.near_distance_ratio < 0 || o.near_distance_ratio > 10 || !std::isfinite(o.near_relative_tolerance) ||
+        o.near_relative_tolerance < 1e-10 || o.near_relative_tolerance > .01 || o.near_maximum_depth > 10 ||
+        !std::isfinite(o.relative_residual_tolerance) || o.relative_residual_tolerance < 1e-7 ||
+        o.relative_residual_tolerance > .01 || o.maximum_refinement_steps > 10)
+        throw InvalidArgument("Invalid BEM medium, frequencies, excitation or Galerkin settings.");
+    if (fmm)
+        throw Unsupported("The fast-multipole acceleration is not part of this build; use the dense form.");
+    if (o.precision != HS_PRECISION_FP64)
+        throw Unsupported("Only the plain FP64 precision form is available in this build.");
+    if (r.excitation_count > 1024 || r.observer_count > 100000)
+        throw InvalidArgument("BEM request exceeds indexing limits.");
+}
+
+}  // namespace
+
+void *DeviceBuffer::ensure(size_t bytes) {
+    if (bytes <= bytes_)
+        return ptr_;
+    release();
+    void *p = nullptr;
+    cuda(cudaMalloc(&p, bytes), "CUDA allocation");
+    ptr_ = p;
+    bytes_ = bytes;
+    return ptr_;
+}
+void DeviceBuffer::release() {
+    if (ptr_)
+        cudaFree(ptr_);
+    ptr_ = nullptr;
+    bytes_ = 0;
+}
+
+Session::Session(const MeshInput &mesh, uint32_t residency) : mesh_(mesh), residency_(residency) {
+    if (residency > HS_RESIDENCY_MAPPED_HOST)
+        throw InvalidArgument("Invalid CUDA quadrature storage policy.");
+    if (mesh_.vertices.empty())
+        throw InvalidArgument("BEM mesh has no vertices.");
+    origin_ = mesh_.vertices.front();
+    for (auto &v : mesh_.vertices) {
+        v = v - origin_;
+        if (!std::isfinite(v.x) || !std::isfinite(v.y) || !std::isfinite(v.z))
+            throw InvalidArgument("BEM mesh coordinates are not finite.");
+    }
+    validateExteriorSurface(mesh_);
+    space_ = buildSpace(mesh_);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        throw CudaError("No CUDA device is available.");
+    cuda(cudaStreamCreateWithFlags(&own_, cudaStreamNonBlocking), "CUDA stream");
+    uploadGeometry();
+}
+
+Session::~Session() {
+    if (own_) {
+        cudaStreamSynchronize(own_);
+        cudaStreamDestroy(own_);
+    }
+}
+
+void Session::setStream(cudaStream_t s) {
+    cuda(cudaStreamSynchronize(stream()), "CUDA synchronization");
+    external_ = s;
+}
+
+void Session::uploadGeometry() {
+    const size_t T = space_.panels.size(), N = space_.vertices.size();
+    std::vector<DPanel> panels(T);
+    std::vector<Bounds> bounds(T);
+    for (size_t t = 0; t < T; ++t) {
+        const HostPanel &p = space_.panels[t];
+        DPanel &d = panels[t];
+        const V3 e1 = p.v[1] - p.v[0], e2 = p.v[2] - p.v[0];
+        const double v0[3] = {p.v[0].x, p.v[0].y, p.v[0].z}, a[3] = {e1.x, e1.y, e1.z}, b[3] = {e2.x, e2.y, e2.z},
+                     n[3] = {p.n.x, p.n.y, p.n.z};
+        for (int i = 0; i < 3; ++i) {
+            d.v0[i] = v0[i];
+            d.e1[i] = a[i];
+            d.e2[i] = b[i];
+            d.n[i] = n[i];
+            d.curl[3 * i] = p.curl[i].x;
+            d.curl[3 * i + 1] = p.curl[i].y;
+            d.curl[3 * i + 2] = p.curl[i].z;
+            d.nodes[i] = p.nodes[i];
+        }
+        d.area = p.area;
+        d.maxEdge = p.maxEdge;
+        d.pad = 0;
+        bounds[t] = makeBounds(p);
+    }
+    std::vector<double> scale(N);
+    for (size_t v = 0; v < N; ++v)
+        scale[v] = 1.0 / space_.lumpedMass[v];
+    const cudaStream_t s = stream();
+    upload(dPanels_, panels, s);
+    upload(dBounds_, bounds, s);
+    upload(dIncOffsets_, space_.incOffsets, s);
+    upload(dIncPanel_, space_.incPanel, s);
+    upload(dIncLocal_, space_.incLocal, s);
+    upload(dRowScale_, scale, s);
+    upload(dMass_, space_.lumpedMass, s);
+    dError_.ensure(16);
+    cuda(cudaMemsetAsync(dError_.as<void>(), 0, 16, s), "error reset");
+    uploadRuleTables(s);
+    cuda(cudaStreamSynchronize(s), "CUDA synchronization");
+}
+
+const Plan &Session::plan(const hs_numerics &numerics, double maxK, const volatile int32_t *cancel) {
+    preparePlan(numerics, maxK, cancel);
+    return plan_;
+}
+
+// cuda_solver.cu:800-940: the plan is rebuilt only when its settings or the
+// planning wavenumber change; otherwise the session's device copy is reused.
+void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int32_t *cancel) {
+    if (planValid_ && sameNumerics(planNumerics_, o) && planK_ == maxK) {
+        planMs_ = 0;
+        return;
+    }
+    planValid_ = false;
+    const auto start = Clock::now();
+    PlanSettings st{o.quadrature_order, o.singular_order, o.near_distance_ratio, o.near_relative_tolerance,
+                    o.near_maximum_depth};
+    plan_ = makePlan(space_, st, maxK, 0, cancel);
+    const uint32_t T = uint32_t(space_.panels.size());
+    const size_t pairs = size_t(T) * (T - 1) / 2;
+    std::vector<uint8_t> code(pairs, kPairRegular);
+    for (const auto &j : plan_.touching)
+        if (j.test != j.trial)
+            code[unorderedPairIndex(j.test, j.trial)] = kPairTouching;
+    std::vector<NearPairJob> nearPairs;
+    for (const auto &j : plan_.near) {
+        code[unorderedPairIndex(j.test, j.trial)] = kPairNear;
+        if (!j.swap)
+            nearPairs.push_back({j.test, j.trial, j.first, j.count});
+    }
+    if (!plan_.wholePanelDegrees.empty())
+        for (size_t u = 0; u < pairs; ++u)
+            if (code[u] == kPairRegular && plan_.wholePanelDegrees[u])
+                code[u] = plan_.wholePanelDegrees[u] == 14 ? kPairWhole14 : kPairWhole8;
+    std::vector<TouchingJob> touching(plan_.touching.size());
+    for (size_t i = 0; i < touching.size(); ++i) {
+        const auto &j = plan_.touching[i];
+        TouchingJob &d = touching[i];
+        d.test = j.test;
+        d.trial = j.trial;
+        d.topology = j.perm.topology;
+        for (int c = 0; c < 3; ++c) {
+            d.permTest[c] = j.perm.test[c];
+            d.permTrial[c] = j.perm.trial[c];
+        }
+        d.pad[0] = d.pad[1] = 0;
+    }
+    const auto gauss = gaussLegendre01(o.singular_order);
+    std::vector<double> g(2 * gauss.size());
+    for (size_t i = 0; i < gauss.size(); ++i) {
+        g[2 * i] = gauss[i].x;
+        g[2 * i + 1] = gauss[i].w;
+    }
+    const cudaStream_t s = stream();
+    upload(dPairCode_, code, s);
+    upload(dTouching_, touching, s);
+    upload(dNearPairs_, nearPairs, s);
+    upload(dPatches_, plan_.patches, s);
+    upload(dGauss_, g, s);
+    cuda(cudaStreamSynchronize(s), "CUDA synchronization");
+    singularSamples_ = 0;
+    for (const auto &j : plan_.touching)
+        singularSamples_ += uint64_t(sectorCount(j.perm.topology)) * o.singular_order * o.singular_order *
+                            o.singular_order * o.singular_order;
+    nearSamples_ = 0;
+    for (const auto &j : nearPairs)
+        for (uint32_t q = 0; q < j.patchCount; ++q) {
+            const Patch &p = plan_.patches[j.firstPatch + q];
+            const uint64_t n = p.degree == 14 ? 64 : 16, inner = 20ull * p.intervals;
+            nearSamples_ += p.projection ? n * 3 * inner * inner : n * n;
+        }
+    touchingCount_ = uint32_t(touching.size());
+    nearPairCount_ = uint32_t(nearPairs.size());
+    planNumerics_ = o;
+    planK_ = maxK;
+    planValid_ = true;
+    planMs_ = msSince(start);
+}
+
+uint32_t Session::chooseBatch(uint32_t F, uint32_t E, uint32_t O) const {
+    const uint64_t T = space_.panels.size(), N = space_.vertices.size();
+    const uint64_t perFrequency = assemblyWorkspaceBytes(uint32_t(T), uint32_t(N), E, 1) + 2 * N * N * 16 +
+                                  4 * E * N * 16 + E * T * 16 + fieldPartialsBytes(uint32_t(T), E, O, 1) + 64;
+    size_t free = 0, total = 0;
+    cuda(cudaMemGetInfo(&free, &total), "CUDA memory query");
+    const uint64_t budget = uint64_t(double(free) * .6);
+    if (perFrequency > budget)
+        throw OutOfMemory("BEM dense workspace of " + std::to_string(perFrequency >> 20) + " MiB per frequency exceeds the " +
+                          std::to_string(budget >> 20) + " MiB device budget.");
+    return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>({uint64_t(F), budget / perFrequency, 32})));
+}
+
+void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O) {
+    const size_t T = space_.panels.size(), N = space_.vertices.size();
+    const size_t pairs = T * (T - 1) / 2;
+    dRecords_.ensure(std::max<size_t>(B * T * T * kRecordDoubles * 8, 16));
+    dColumns_.ensure(B * N * 6 * T * 8);
+    dPanelRhs_.ensure(B * E * 6 * T * 8);
+    dBins_.ensure(std::max<size_t>(B * kBins * pairs * sizeof(uint2), 16));
+    dBinCounts_.ensure(B * kBins * sizeof(uint32_t));
+    dA_.ensure(B * N * N * 16);
+    dLU_.ensure(B * N * N * 16);
+    dRhs_.ensure(B * E * N * 16);
+    dX_.ensure(B * E * N * 16);
+    dCorr_.ensure(B * E * N * 16);
+    dNorms_.ensure(2 * B * E * 8 + 2 * B * E * N * 8);
+    dPivots_.ensure(B * N * sizeof(int));
+    dInfo_.ensure(16);
+    dKs_.ensure(B * 8);
+    dFlux_.ensure(B * E * T * 16);
+    dObservers_.ensure(std::max<size_t>(O * 3 * 8, 16));
+    dPartials_.ensure(std::max<size_t>(fieldPartialsBytes(uint32_t(T), E, O, B), 16));
+    dField_.ensure(std::max<size_t>(B * E * O * 16, 16));
+    dDegrees_.ensure(B * 4);
+    size_t bytes = 0;
+    for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_, &dMass_,
+                                  &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dRecords_, &dColumns_,
+                                  &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
+                                  &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_})
+        bytes += b->bytes();
+    peakBytes_ = std::max(peakBytes_, bytes);
+}
+
+void Session::checkDeviceError(const char *where) {
+    int code = 0;
+    cuda(cudaMemcpyAsync(&code, dError_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, stream()), where);
+    cuda(cudaStreamSynchronize(stream()), where);
+    if (!code)
+        return;
+    cuda(cudaMemsetAsync(dError_.as<int>(), 0, sizeof(int), stream()), "error reset");
+    if (code == kErrDistance)
+        throw NumericError("BEM quadrature encountered zero or invalid source distance.");
+    if (code == kErrNonFinite)
+        throw NumericError("BEM calculation produced a non-finite value.");
+    if (code == kErrFieldDepth)
+        throw NumericError("BEM field integration did not reach its near-field tolerance.");
+    if (code == kErrEscapedPlan)
+        throw NumericError("BEM dense regular pair escaped its qualified adaptive plan.");
+    throw NumericError("BEM device error code " + std::to_string(code));
+}
+
+std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32_t *cancel, hs_progress_fn progress,
+                                       void *user) {
+    const auto checkCancel = [&]() {
+        if (cancel && *cancel)
+            throw Cancelled();
+    };
+    checkCancel();
+    validateRequest(r);
+    const hs_numerics &o = r.numerics;
+    const double maxK = planningWavenumber(r);
+    const uint32_t T = uint32_t(space_.panels.size()), N = uint32_t(space_.vertices.size());
+    const uint32_t E = uint32_t(r.excitation_count), O = uint32_t(r.observer_count);
+    const uint32_t F = uint32_t(r.frequency_count);
+    // Far-field origin and observers in session coordinates (cuda_solver.cu:1087-1137).
+    V3 farOrigin{0, 0, 0};
+    if (r.far_field) {
+        const V3 fo{r.far_origin[0], r.far_origin[1], r.far_origin[2]};
+        farOrigin = fo - origin_;
+        if (!std::isfinite(fo.x) || !std::isfinite(fo.y) || !std::isfinite(fo.z) || !std::isfinite(farOrigin.x) ||
+            !std::isfinite(farOrigin.y) || !std::isfinite(farOrigin.z) || !std::isfinite(r.far_reference_distance) ||
+            r.far_reference_distance <= 0 || !std::isfinite(maxK * r.far_reference_distance))
+            throw InvalidArgument("Far-field origin and positive reference distance must be finite.");
+    }
+    std::vector<double> observers(3 * size_t(O));
+    for (uint32_t i = 0; i < O; ++i) {
+        const V3 w{r.observers[3 * i], r.observers[3 * i + 1], r.observers[3 * i + 2]};
+        V3 p = w - (r.far_field ? V3{r.far_origin[0], r.far_origin[1], r.far_origin[2]} : origin_);
+        if (!std::isfinite(w.x) || !std::isfinite(w.y) || !std::isfinite(w.z) || !std::isfinite(p.x) ||
+            !std::isfinite(p.y) || !std::isfinite(p.z))
+            throw InvalidArgument("BEM observation coordinates must be finite.");
+        if (r.far_field) {
+            const double d = std::hypot(p.x, p.y, p.z);
+            if (!(d > 0) || !std::isfinite(d))
+                throw InvalidArgument("A far-field direction must differ from its origin.");
+            p = V3{p.x / d, p.y / d, p.z / d};
+        } else if (insideSolid(space_, p))
+            throw InvalidArgument("BEM observation points must be finite and outside the solid.");
+        observers[3 * i] = p.x;
+        observers[3 * i + 1] = p.y;
+        observers[3 * i + 2] = p.z;
+    }
+    // Per-face boundary conditions and per-panel velocities (cuda_solver.cu:1165-1212).
+    std::map<uint32_t, uint8_t> conditions;
+    for (const auto &p : space_.panels) {
+        const auto [it, inserted] = conditions.emplace(p.face, p.driven);
+        if (!inserted && it->second != p.driven)
+            throw InvalidArgument("Conflicting boundary conditions on one face.");
+    }
+    std::vector<cplx> velocity(size_t(E) * T);
+    std::vector<std::map<uint32_t, cplx>> faceVelocity(E);
+    bool nonzero = false;
+    for (uint32_t e = 0; e < E; ++e) {
+        for (size_t i = r.excitation_face_offsets[e]; i < r.excitation_face_offsets[e + 1]; ++i) {
+            const uint32_t face = r.excitation_face_ids[i];
+            const cplx v(r.excitation_velocities[2 * i], r.excitation_velocities[2 * i + 1]);
+            const auto c = conditions.find(face);
+            if (c == conditions.end() || c->second != HS_DRIVEN || !std::isfinite(v.real()) || !std::isfinite(v.imag()) ||
+                !faceVelocity[e].emplace(face, v).second)
+                throw InvalidArgument("Excitation must assign each known Driven face at most once.");
+            nonzero = nonzero || v != cplx(0);
+        }
+        if (faceVelocity[e].empty())
+            throw InvalidArgument("Each excitation needs at least one assigned Driven face.");
+        for (uint32_t t = 0; t < T; ++t) {
+            const auto it = faceVelocity[e].find(space_.panels[t].face);
+            if (it != faceVelocity[e].end())
+                velocity[size_t(e) * T + t] = it->second;
+        }
+    }
+    if (progress) {
+        hs_progress p{0, F, r.frequencies[0], HS_PHASE_PREPARING};
+        progress(&p, user);
+    }
+    preparePlan(o, maxK, cancel);
+    const double planMs = planMs_;
+    checkCancel();
+    const cudaStream_t s = stream();
+    const uint32_t Bmax = chooseBatch(F, E, O);
+    ensureWorkspace(Bmax, E, O);
+    if (O)
+        cuda(cudaMemcpyAsync(dObservers_.as<void>(), observers.data(), observers.size() * 8, cudaMemcpyHostToDevice, s),
+             "observer upload");
+    auto result = std::make_unique<Result>();
+    result->T = T;
+    result->N = N;
+    result->O = O;
+    result->E = E;
+    result->frequencies.resize(F);
+    AssemblyGeometry geo{dPanels_.as<DPanel>(), dBounds_.as<Bounds>(), dPairCode_.as<uint8_t>(),
+                         dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), dPatches_.as<Patch>(),
+                         dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
+                         dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, o.near_relative_tolerance,
+                         o.quadrature_order, o.singular_order};
+    double maxEdge = 0;
+    for (const auto &p : space_.panels)
+        maxEdge = std::max(maxEdge, p.maxEdge);
+    for (uint32_t f0 = 0; f0 < F; f0 += Bmax) {
+        checkCancel();
+        const uint32_t B = std::min(Bmax, F - f0);
+        const auto batchStart = Clock::now();
+        std::vector<double> ks(B);
+        std::vector<cplx> flux(size_t(B) * E * T);
+        for (uint32_t b = 0; b < B; ++b) {
+            const double omega = 2 * M_PI * r.frequencies[f0 + b];
+            ks[b] = omega / r.sound_speed;
+            for (size_t i = 0; i < size_t(E) * T; ++i)
+                flux[size_t(b) * E * T + i] = cplx(0, -r.density * omega) * velocity[i];
+        }
+        cuda(cudaMemcpyAsync(dKs_.as<void>(), ks.data(), B * 8, cudaMemcpyHostToDevice, s), "k upload");
+        cuda(cudaMemcpyAsync(dFlux_.as<void>(), flux.data(), flux.size() * 16, cudaMemcpyHostToDevice, s), "flux upload");
+        AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
+                             dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
+        assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws, dA_.as<double>(),
+                      dRhs_.as<double>(), dError_.as<int>(), s, &timer_);
+        checkDeviceError("CUDA Galerkin assembly");
+        if (timer_.enabled()) {
+            std::vector<uint32_t> counts(size_t(B) * kBins);
+            cuda(cudaMemcpy(counts.data(), dBinCounts_.as<void>(), counts.size() * 4, cudaMemcpyDeviceToHost),
+                 "bin counts");
+            for (uint32_t b = 0; b < B; ++b)
+                for (int bin = 0; bin < kBins; ++bin) {
+                    const uint64_t c = counts[size_t(b) * kBins + bin];
+                    work[bin] += c;
+                    work[4] += c * uint64_t(kBinPoints[bin]) * kBinPoints[bin];
+                }
+            work[5] += uint64_t(B) * singularSamples_;
+            work[6] += uint64_t(B) * nearSamples_;
+            work[7] += B;
+        }
+        const double assemblyMs = msSince(batchStart);
+        checkCancel();
+        // LU of every matrix of the batch, then the initial solves.
+        const auto factorStart = Clock::now();
+        cuda(cudaMemcpyAsync(dLU_.as<void>(), dA_.as<void>(), size_t(B) * N * N * 16, cudaMemcpyDeviceToDevice, s),
+             "factorization copy");
+        luFactorBatch(dLU_.as<double>(), N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_);
+        int info = 0;
+        cuda(cudaMemcpyAsync(&info, dInfo_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, s), "LU info");
+        cuda(cudaStreamSynchronize(s), "CUDA pivoted LU");
+        if (info)
+            throw NumericError("CUDA Burton-Miller factorization failed at pivot " + std::to_string(info));
+        const double factorMs = msSince(factorStart);
+        const auto triStart = Clock::now();
+        cuda(cudaMemcpyAsync(dX_.as<void>(), dRhs_.as<void>(), size_t(B) * E * N * 16, cudaMemcpyDeviceToDevice, s),
+             "rhs copy");
+        luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), s, &timer_);
+        cuda(cudaStreamSynchronize(s), "CUDA multi-RHS solve");
+        double triMs = msSince(triStart);
+        // FP64 refinement (cuda_solver.cu:1519-1581), per frequency.
+        const auto residualStart = Clock::now();
+        std::vector<uint32_t> steps(B, 0);
+        std::vector<double> relative(size_t(B) * E, 0);
+        std::vector<double> norms(2 * size_t(B) * E);
+        for (;;) {
+            checkCancel();
+            residualBatch(dA_.as<double>(), dRhs_.as<double>(), dX_.as<double>(), dMass_.as<double>(), N, B, E,
+                          dCorr_.as<double>(), dNorms_.as<double>(), s, &timer_);
+            cuda(cudaMemcpyAsync(norms.data(), dNorms_.as<void>(), norms.size() * 8, cudaMemcpyDeviceToHost, s),
+                 "residual norms");
+            cuda(cudaStreamSynchronize(s), "CUDA FP64 physical residual");
+            bool any = false;
+            for (uint32_t b = 0; b < B; ++b) {
+                double largest = 0;
+                for (uint32_t e = 0; e < E; ++e) {
+                    const double res = norms[2 * (size_t(b) * E + e)], rhs = norms[2 * (size_t(b) * E + e) + 1];
+                    const double rel = rhs > 0 ? res / rhs : (res == 0 ? 0 : std::numeric_limits<double>::infinity());
+                    if (!std::isfinite(rel))
+                        throw NumericError("Burton-Miller residual is not finite.");
+                    relative[size_t(b) * E + e] = rel;
+                    largest = std::max(largest, rel);
+                }
+                const bool need = largest > o.relative_residual_tolerance;
+                if (need && steps[b] >= o.maximum_refinement_steps) {
+                    std::ostringstream msg;
+                    msg << std::setprecision(9) << "Burton-Miller residual " << largest << " exceeds tolerance "
+                        << o.relative_residual_tolerance << " at " << r.frequencies[f0 + b] << " Hz after " << steps[b]
+                        << " refinement steps.";
+                    throw NoConvergence(msg.str());
+                }
+                if (need) {
+                    ++steps[b];
+                    any = true;
+                } else
+                    cuda(cudaMemsetAsync(dCorr_.as<char>() + size_t(b) * E * N * 16, 0, size_t(E) * N * 16, s),
+                         "converged correction");
+            }
+            if (!any)
+                break;
+            const auto t0 = Clock::now();
+            luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dCorr_.as<double>(), s, &timer_);
+            addCorrectionBatch(dX_.as<double>(), dCorr_.as<double>(), size_t(B) * E * N * 2, s);
+            cuda(cudaStreamSynchronize(s), "CUDA refinement solve");
+            triMs += msSince(t0);
+        }
+        const double residualMs = msSince(residualStart);
+        // Observer fields with the degree-comparison loop (cuda_solver.cu:1717-1799).
+        const auto fieldStart = Clock::now();
+        std::vector<cplx> field(size_t(B) * E * O, 0);
+        std::vector<uint32_t> degree(B), fieldDeg(size_t(B) * E), fieldNext(size_t(B) * E);
+        std::vector<double> fieldDisc(size_t(B) * E, 0);
+        if (O && nonzero) {
+            if (progress)
+                for (uint32_t b = 0; b < B; ++b) {
+                    hs_progress p{f0 + b, F, r.frequencies[f0 + b], HS_PHASE_FIELD_EVALUATION};
+                    progress(&p, user);
+                }
+            for (uint32_t b = 0; b < B; ++b) {
+                const double kh = ks[b] * maxEdge;
+                if (kh > 3.25) {
+                    std::ostringstream msg;
+                    msg << "BEM panel quadrature: maximum k*h=" << kh
+                        << " exceeds the qualified electrical range 3.25; refine the mesh.";
+                    throw NumericError(msg.str());
+                }
+                const unsigned electrical = kh <= .25 ? 4 : kh <= 1 ? 6 : kh <= 2 ? 8 : 12;
+                degree[b] = std::max(electrical, o.quadrature_order);
+            }
+            FieldRequest fr{dPanels_.as<DPanel>(), T, N, E, O, B, dObservers_.as<double>(), r.far_field,
+                            {farOrigin.x, farOrigin.y, farOrigin.z}, r.far_field ? r.far_reference_distance : 1.0,
+                            std::min(o.near_relative_tolerance, .025 * o.relative_residual_tolerance),
+                            o.near_maximum_depth};
+            const auto evaluate = [&](const std::vector<uint32_t> &deg) {
+                cuda(cudaMemcpyAsync(dDegrees_.as<void>(), deg.data(), B * 4, cudaMemcpyHostToDevice, s), "degrees");
+                evaluateFieldBatch(fr, dKs_.as<double>(), dX_.as<double>(), dFlux_.as<double>(), dDegrees_.as<uint32_t>(),
+                                   dPartials_.as<double>(), dField_.as<double>(), dError_.as<int>(), s, &timer_);
+                std::vector<cplx> out(size_t(B) * E * O);
+                cuda(cudaMemcpyAsync(out.data(), dField_.as<void>(), out.size() * 16, cudaMemcpyDeviceToHost, s),
+                     "field download");
+                checkDeviceError("CUDA P1 field evaluation");
+                return out;
+            };
+            std::vector<cplx> current = evaluate(degree);
+            std::vector<bool> done(B, false);
+            for (;;) {
+                checkCancel();
+                std::vector<uint32_t> next(B);
+                for (uint32_t b = 0; b < B; ++b)
+                    next[b] = done[b] ? degree[b] : refinedDegreeOf(degree[b]);
+                const std::vector<cplx> refined = evaluate(next);
+                bool all = true;
+                for (uint32_t b = 0; b < B; ++b) {
+                    if (done[b])
+                        continue;
+                    bool passed = true;
+                    for (uint32_t e = 0; e < E; ++e) {
+                        double d2 = 0, n2 = 0;
+                        for (uint32_t q = 0; q < O; ++q) {
+                            const size_t i = (size_t(b) * E + e) * O + q;
+                            d2 += std::norm(refined[i] - current[i]);
+                            n2 += std::norm(refined[i]);
+                        }
+                        const double ind = n2 > 0 ? std::sqrt(d2 / n2) : (d2 == 0 ? 0 : std::numeric_limits<double>::infinity());
+                        fieldDeg[size_t(b) * E + e] = degree[b];
+                        fieldNext[size_t(b) * E + e] = next[b];
+                        fieldDisc[size_t(b) * E + e] = ind;
+                        passed = passed && ind <= .025 * o.relative_residual_tolerance;
+                    }
+                    for (uint32_t e = 0; e < E; ++e)
+                        for (uint32_t q = 0; q < O; ++q) {
+                            const size_t i = (size_t(b) * E + e) * O + q;
+                            field[i] = refined[i];
+                        }
+                    if (passed)
+                        done[b] = true;
+                    else if (degree[b] == 12)
+                        throw NoConvergence("BEM complex observer-field quadrature 12/14 did not converge within "
+                                            "0.025*residualTolerance; refine the mesh or observer separation. "
+                                            "Equation residuals do not bound field quadrature.");
+                    else
+                        degree[b] = next[b];
+                    all = all && done[b];
+                }
+                current = refined;
+                if (all)
+                    break;
+            }
+        }
+        const double fieldMs = msSince(fieldStart);
+        // Boundary data and impedances (cuda_solver.cu:1800-1846).
+        std::vector<cplx> x(size_t(B) * E * N);
+        cuda(cudaMemcpyAsync(x.data(), dX_.as<void>(), x.size() * 16, cudaMemcpyDeviceToHost, s), "trace download");
+        cuda(cudaStreamSynchronize(s), "CUDA synchronization");
+        for (uint32_t b = 0; b < B; ++b) {
+            FrequencyResult &fr = result->frequencies[f0 + b];
+            const double omega = 2 * M_PI * r.frequencies[f0 + b];
+            fr.frequency = r.frequencies[f0 + b];
+            fr.info.frequency = fr.frequency;
+            fr.info.assembly_ms = assemblyMs / B;
+            fr.info.factorization_ms = factorMs / B;
+            fr.info.triangular_solve_ms = triMs / B;
+            fr.info.residual_check_ms = residualMs / B;
+            fr.info.solve_ms = (factorMs + triMs + residualMs) / B;
+            fr.info.field_ms = fieldMs / B;
+            fr.info.interaction_plan_ms = (f0 + b == 0) ? planMs : 0;
+            fr.info.interaction_plan_reused = planMs == 0;
+            fr.excitations.resize(E);
+            for (uint32_t e = 0; e < E; ++e) {
+                ExcitationResult &er = fr.excitations[e];
+                er.trace.assign(x.begin() + (size_t(b) * E + e) * N, x.begin() + (size_t(b) * E + e + 1) * N);
+                er.residual = relative[size_t(b) * E + e];
+                er.refinements = steps[b];
+                er.fieldDegree = fieldDeg[size_t(b) * E + e];
+                er.fieldNext = fieldNext[size_t(b) * E + e];
+                er.fieldDiscrepancy = fieldDisc[size_t(b) * E + e];
+                er.surface.resize(T);
+                er.normalDerivative.resize(T);
+                for (uint32_t t = 0; t < T; ++t) {
+                    const HostPanel &p = space_.panels[t];
+                    cplx avg = 0;
+                    for (int i = 0; i < 3; ++i)
+                        avg += er.trace[p.nodes[i]] / 3.0;
+                    if (!std::isfinite(avg.real()) || !std::isfinite(avg.imag()))
+                        throw NumericError("Burton-Miller pressure is not finite.");
+                    er.surface[t] = avg;
+                    const auto it = faceVelocity[e].find(p.face);
+                    er.normalDerivative[t] = it == faceVelocity[e].end() ? cplx(0) : cplx(0, -r.density * omega) * it->second;
+                }
+                er.observer.assign(field.begin() + (size_t(b) * E + e) * O, field.begin() + (size_t(b) * E + e + 1) * O);
+                for (size_t i = r.excitation_face_offsets[e]; i < r.excitation_face_offsets[e + 1]; ++i) {
+                    const uint32_t face = r.excitation_face_ids[i];
+                    const cplx v(r.excitation_velocities[2 * i], r.excitation_velocities[2 * i + 1]);
+                    if (std::abs(v) == 0)
+                        continue;
+                    double area = 0;
+                    cplx integrated = 0;
+                    for (uint32_t t = 0; t < T; ++t)
+                        if (space_.panels[t].face == face) {
+                            area += space_.panels[t].area;
+                            integrated += er.surface[t] * space_.panels[t].area;
+                        }
+                    const cplx mean = integrated / area, volume = v * area, z = mean / volume;
+                    er.impedances.push_back(
+                        {face, area, {mean.real(), mean.imag()}, {volume.real(), volume.imag()}, {z.real(), z.imag()}});
+                }
+            }
+            if (progress) {
+                hs_progress p{f0 + b + 1, F, fr.frequency, HS_PHASE_FREQUENCY_COMPLETE};
+                progress(&p, user);
+            }
+        }
+    }
+    result->peakDeviceBytes = peakBytes_;
+    return result;
+}
+
+void Session::debugAssemble(const hs_numerics &o, double planK, double k, const double *flux, double *matrix,
+                            double *rhs) {
+    preparePlan(o, planK, nullptr);
+    const uint32_t T = uint32_t(space_.panels.size()), N = uint32_t(space_.vertices.size());
+    ensureWorkspace(1, 1, 0);
+    const cudaStream_t s = stream();
+    cuda(cudaMemcpyAsync(dKs_.as<void>(), &k, 8, cudaMemcpyHostToDevice, s), "k upload");
+    cuda(cudaMemcpyAsync(dFlux_.as<void>(), flux, size_t(T) * 16, cudaMemcpyHostToDevice, s), "flux upload");
+    AssemblyGeometry geo{dPanels_.as<DPanel>(), dBounds_.as<Bounds>(), dPairCode_.as<uint8_t>(),
+                         dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), dPatches_.as<Patch>(),
+                         dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
+                         dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, o.near_relative_tolerance,
+                         o.quadrature_order, o.singular_order};
+    AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
+                         dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
+    assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), 1, 1, ws, dA_.as<double>(),
+                  dRhs_.as<double>(), dError_.as<int>(), s, &timer_);
+    checkDeviceError("CUDA Galerkin assembly");
+    cuda(cudaMemcpyAsync(matrix, dA_.as<void>(), size_t(N) * N * 16, cudaMemcpyDeviceToHost, s), "matrix download");
+    cuda(cudaMemcpyAsync(rhs, dRhs_.as<void>(), size_t(N) * 16, cudaMemcpyDeviceToHost, s), "rhs download");
+    cuda(cudaStreamSynchronize(s), "CUDA synchronization");
+}
+
+}  // namespace hsb

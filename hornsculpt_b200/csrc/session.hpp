@@ -1,0 +1,102 @@
+// Solver session: one validated mesh with its device geometry, cached
+// interaction plan and reusable device workspaces
+// (CudaBemSolver::Implementation, cuda_solver.cu:742-987).
+#pragma once
+
+#include "device_types.cuh"
+#include "hs_bem.h"
+#include "kernel_timer.hpp"
+#include "planner.hpp"
+
+#include <complex>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace hsb {
+
+class DeviceBuffer {
+  public:
+    DeviceBuffer() = default;
+    ~DeviceBuffer() { release(); }
+    DeviceBuffer(const DeviceBuffer &) = delete;
+    DeviceBuffer &operator=(const DeviceBuffer &) = delete;
+    void *ensure(size_t bytes);  // grows (never shrinks) the allocation
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(ptr_); }
+    size_t bytes() const { return bytes_; }
+
+  private:
+    void *ptr_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+using cplx = std::complex<double>;
+
+struct ExcitationResult {
+    std::vector<cplx> trace, surface, normalDerivative, observer;
+    double residual{};
+    uint32_t refinements{}, fieldDegree{}, fieldNext{};
+    double fieldDiscrepancy{};
+    std::vector<hs_face_impedance> impedances;
+};
+struct FrequencyResult {
+    double frequency{};
+    hs_frequency_info info{};
+    std::vector<ExcitationResult> excitations;
+};
+struct Result {
+    size_t T{}, N{}, O{}, E{}, peakDeviceBytes{};
+    std::vector<FrequencyResult> frequencies;
+};
+
+class Session {
+  public:
+    Session(const MeshInput &mesh, uint32_t residency);
+    ~Session();
+    void setStream(cudaStream_t stream);
+    std::unique_ptr<Result> solve(const hs_request &request, const volatile int32_t *cancel, hs_progress_fn progress,
+                                  void *user);
+    const Plan &plan(const hs_numerics &numerics, double maxK, const volatile int32_t *cancel);
+    void debugAssemble(const hs_numerics &numerics, double planK, double k, const double *flux, double *matrix,
+                       double *rhs);
+    KernelTimer &timer() { return timer_; }
+    // regular pairs per bin (4), regular samples, touching samples, near samples, frequencies
+    std::vector<uint64_t> work = std::vector<uint64_t>(8, 0);
+    std::mutex mutex;
+
+  private:
+    struct Batch;
+    void uploadGeometry();
+    void preparePlan(const hs_numerics &numerics, double maxK, const volatile int32_t *cancel);
+    void ensureWorkspace(uint32_t B, uint32_t E, uint32_t O);
+    uint32_t chooseBatch(uint32_t F, uint32_t E, uint32_t O) const;
+    void checkDeviceError(const char *where);
+    cudaStream_t stream() const { return external_ ? external_ : own_; }
+
+    MeshInput mesh_;
+    V3 origin_{};
+    Space space_;
+    uint32_t residency_;
+    cudaStream_t own_ = nullptr, external_ = nullptr;
+    KernelTimer timer_;
+
+    // geometry (frequency independent)
+    DeviceBuffer dPanels_, dBounds_, dIncOffsets_, dIncPanel_, dIncLocal_, dRowScale_, dMass_, dError_;
+    // plan cache
+    bool planValid_ = false;
+    hs_numerics planNumerics_{};
+    double planK_ = -1;
+    Plan plan_;
+    double planMs_ = 0;
+    DeviceBuffer dPairCode_, dTouching_, dNearPairs_, dPatches_, dGauss_;
+    uint32_t touchingCount_ = 0, nearPairCount_ = 0;
+    uint64_t singularSamples_ = 0, nearSamples_ = 0;
+    // workspaces (grow only)
+    DeviceBuffer dRecords_, dColumns_, dPanelRhs_, dBins_, dBinCounts_, dA_, dLU_, dRhs_, dX_, dCorr_, dNorms_,
+        dPivots_, dInfo_, dKs_, dFlux_, dObservers_, dPartials_, dField_, dDegrees_;
+    size_t peakBytes_ = 0;
+};
+
+}  // namespace hsb

@@ -1,0 +1,223 @@
+/*
+ * hs_bem.h — C ABI of the B200-native exterior Burton-Miller solve.
+ *
+ * Drop-in boundary for HornSculpt's `hornsculpt::CudaBemSolver`
+ * (modules/bem/include/hornsculpt/bem.hpp:367-388; implementation
+ * modules/bem/cuda/cuda_solver.cu:1021-1853). Plain pointers and sizes only.
+ * A session holds one closed surface mesh (its geometry, interaction plan and
+ * device workspaces) across calls, like the reference solver object; a solve
+ * call takes a request (medium, frequencies, excitations, observers,
+ * numerics) and returns a host-owned result.
+ *
+ * Conventions follow the reference (bem.hpp:357-360): exp(+i omega t) RMS
+ * phasors, outgoing exp(-ikr), flux q = dp/dn = -i rho omega v on Driven
+ * faces, Burton-Miller coupling alpha = -i/k, P1 pressure per mesh vertex,
+ * DP0 flux per triangle. Complex arrays are interleaved (re, im) doubles.
+ *
+ * Every function returns an hs_status; on failure hs_last_error() holds the
+ * message of the calling thread's last failure. Invalid inputs that the
+ * reference rejects with std::invalid_argument return HS_E_INVALID; device,
+ * numerical and convergence failures that it reports with
+ * std::runtime_error return HS_E_CUDA / HS_E_NUMERIC / HS_E_NOCONVERGE /
+ * HS_E_NOMEM / HS_E_CANCELLED.
+ */
+#ifndef HS_BEM_H
+#define HS_BEM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hs_status {
+    HS_OK = 0,
+    HS_E_INVALID = 1,     /* std::invalid_argument in the reference */
+    HS_E_CUDA = 2,        /* CUDA runtime failure (cuda_solver.cu:35-38) */
+    HS_E_NUMERIC = 3,     /* quadrature / non-finite codes (cuda_solver.cu:705-715) */
+    HS_E_NOCONVERGE = 4,  /* refinement or field-degree loop exhausted (cuda_solver.cu:1559-1565, 1792-1796) */
+    HS_E_NOMEM = 5,       /* memory preflight (cuda_solver.cu:1161-1163, 1261-1264) */
+    HS_E_CANCELLED = 6,   /* "BEM calculation cancelled." (cuda_solver.cu:49-52) */
+    HS_E_UNSUPPORTED = 7  /* sub-domain, baffle, axisymmetric or fast-multipole requests */
+} hs_status;
+
+typedef enum hs_boundary { HS_WALL = 0, HS_DRIVEN = 1 } hs_boundary;   /* mesh.hpp:17 */
+typedef enum hs_acceleration { HS_DENSE = 0, HS_FAST_MULTIPOLE = 1 } hs_acceleration; /* bem.hpp:38 */
+typedef enum hs_precision {
+    HS_PRECISION_FP64 = 0 /* plain form: the reference method evaluated entirely in FP64 */
+} hs_precision;
+typedef enum hs_residency { HS_RESIDENCY_AUTOMATIC = 0, HS_RESIDENCY_DEVICE = 1, HS_RESIDENCY_MAPPED_HOST = 2 } hs_residency; /* bem.hpp:361-365 */
+
+/* BemNumerics + FastMultipoleSettings (bem.hpp:61-72, 113-123). */
+typedef struct hs_numerics {
+    uint32_t quadrature_order;            /* 2 or 4 (default 4) */
+    uint32_t singular_order;              /* 2..20 (default 4) */
+    double near_distance_ratio;           /* [0, 10] (default 1) */
+    double near_relative_tolerance;       /* [1e-10, 1e-2] (default 1e-4) */
+    uint32_t near_maximum_depth;          /* <= 10 (default 6) */
+    double relative_residual_tolerance;   /* [1e-7, 1e-2] (default 5e-5) */
+    uint32_t maximum_refinement_steps;    /* <= 10 (default 3) */
+    uint32_t acceleration;                /* hs_acceleration */
+    uint32_t precision;                   /* hs_precision */
+    uint32_t fmm_leaf_support_capacity;   /* 16 */
+    double fmm_separation_ratio;          /* 1.5 */
+    uint32_t fmm_maximum_iterations;      /* 300 */
+    uint32_t fmm_restart_length;          /* 40 */
+    uint32_t fmm_preconditioner_block_width; /* 32 */
+} hs_numerics;
+
+/* BemRequest (bem.hpp:163-191), exterior single-domain subset. Excitation e
+ * assigns velocities to Driven faces excitation_face_ids[o] for
+ * o in [excitation_face_offsets[e], excitation_face_offsets[e+1]). */
+typedef struct hs_request {
+    double density;                       /* kg/m^3 (AcousticMedium, default 1.21) */
+    double sound_speed;                   /* m/s (default 343) */
+    const double *frequencies;            /* Hz, finite, > 0 */
+    size_t frequency_count;
+    const double *plan_frequencies;       /* interactionPlanFrequencies; may be NULL */
+    size_t plan_frequency_count;
+    size_t excitation_count;              /* 1..1024 */
+    const size_t *excitation_face_offsets;/* excitation_count + 1 */
+    const uint32_t *excitation_face_ids;
+    const double *excitation_velocities;  /* complex RMS normal velocity per face entry */
+    const double *observers;              /* xyz world points, or far-field directions */
+    size_t observer_count;
+    int32_t far_field;                    /* nonzero: FarFieldObservation */
+    double far_origin[3];
+    double far_reference_distance;        /* metres; result includes exp(-ik R)/R */
+    hs_numerics numerics;
+} hs_request;
+
+/* BemProgress (bem.hpp:334-355). */
+typedef enum hs_phase {
+    HS_PHASE_PREPARING = 0,
+    HS_PHASE_NEAR_CONSTRUCTION = 1,
+    HS_PHASE_FAR_PREPARATION = 2,
+    HS_PHASE_KRYLOV_SOLVE = 3,
+    HS_PHASE_RESIDUAL_AUDIT = 4,
+    HS_PHASE_FIELD_EVALUATION = 5,
+    HS_PHASE_FREQUENCY_COMPLETE = 6
+} hs_phase;
+typedef struct hs_progress {
+    size_t completed_frequencies, total_frequencies;
+    double frequency;
+    uint32_t phase;
+} hs_progress;
+typedef void (*hs_progress_fn)(const hs_progress *progress, void *user);
+
+typedef struct hs_bem_session hs_bem_session;
+typedef struct hs_result hs_result;
+
+/* Per-excitation result scalars (BemExcitationResult, bem.hpp:231-301). */
+typedef struct hs_excitation_info {
+    double boundary_residual;             /* relative L2 residual of the unscaled equation */
+    uint32_t refinement_steps;
+    uint32_t iterations;                  /* 0 for dense LU */
+    uint32_t field_comparison_degree, field_verification_degree;
+    double field_discrepancy;
+    size_t impedance_count;
+} hs_excitation_info;
+
+/* FaceImpedance (bem.hpp:193-199). */
+typedef struct hs_face_impedance {
+    uint32_t face_id;
+    double area;
+    double mean_pressure[2];
+    double volume_velocity[2];
+    double volume_impedance[2];
+} hs_face_impedance;
+
+/* BemFrequencyResult timings (bem.hpp:303-317), milliseconds. */
+typedef struct hs_frequency_info {
+    double frequency;
+    double assembly_ms, factorization_ms, triangular_solve_ms, solve_ms, field_ms, residual_check_ms;
+    double interaction_plan_ms;
+    int32_t interaction_plan_reused;
+} hs_frequency_info;
+
+/* ---- numerics ---- */
+void hs_numerics_default(hs_numerics *out);                 /* BemNumerics{} defaults */
+
+/* ---- session (CudaBemSolver ctor / dtor, bem.hpp:369-378) ----
+ * vertices: vertex_count x 3 doubles; triangles: triangle_count x 3 vertex
+ * indices; face_ids, boundary (hs_boundary) one per triangle. The mesh is
+ * copied and centred on vertex 0 (cuda_solver.cu:771-781) and validated as a
+ * closed, outward-oriented exterior surface (cuda_solver.cu:782-789). */
+hs_status hs_bem_session_create(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                const uint32_t *face_ids, const uint8_t *boundary, size_t triangle_count,
+                                uint32_t residency, hs_bem_session **out);
+void hs_bem_session_destroy(hs_bem_session *session);
+
+/* Optional: run the session's device work on a caller-owned cudaStream_t
+ * (passed as void*). NULL restores the session's own non-blocking stream. */
+hs_status hs_bem_session_set_stream(hs_bem_session *session, void *cuda_stream);
+
+/* ---- solve (CudaBemSolver::solve, bem.hpp:381-382) ----
+ * cancel: optional flag polled between device batches (std::stop_token);
+ * progress: optional callback. Calls on one session are serialised. */
+hs_status hs_bem_solve(hs_bem_session *session, const hs_request *request, const volatile int32_t *cancel,
+                       hs_progress_fn progress, void *user, hs_result **out);
+
+/* ---- results (BemResult, bem.hpp:319-332) ---- */
+size_t hs_result_frequency_count(const hs_result *r);
+size_t hs_result_excitation_count(const hs_result *r);
+size_t hs_result_triangle_count(const hs_result *r);
+size_t hs_result_pressure_dof_count(const hs_result *r);
+size_t hs_result_observer_count(const hs_result *r);
+size_t hs_result_peak_device_bytes(const hs_result *r);
+hs_status hs_result_frequency_info(const hs_result *r, size_t f, hs_frequency_info *out);
+hs_status hs_result_excitation_info(const hs_result *r, size_t f, size_t e, hs_excitation_info *out);
+/* BemBoundaryData (bem.hpp:203-214): P1 trace [N], DP0 mean surface pressure
+ * [T], DP0 normal derivative [T]; observer pressure [O]. */
+hs_status hs_result_pressure_trace(const hs_result *r, size_t f, size_t e, double *out);
+hs_status hs_result_surface_pressure(const hs_result *r, size_t f, size_t e, double *out);
+hs_status hs_result_normal_derivative(const hs_result *r, size_t f, size_t e, double *out);
+hs_status hs_result_observer_pressure(const hs_result *r, size_t f, size_t e, double *out);
+hs_status hs_result_impedances(const hs_result *r, size_t f, size_t e, hs_face_impedance *out);
+void hs_result_free(hs_result *r);
+
+/* ---- diagnostics ---- */
+const char *hs_last_error(void);
+/* CudaBemSolver::deviceDescription (bem.hpp:383, cuda_solver.cu:1010-1020). */
+hs_status hs_device_description(char *buffer, size_t size);
+
+/* Device work of the last solve on this session, summed per kernel family
+ * from CUDA events recorded on the session stream when profiling is on.
+ * names: comma-separated family names written to names_buffer; ms/launches:
+ * one entry per family (capacity entries at most). */
+hs_status hs_bem_session_set_profiling(hs_bem_session *session, int32_t enabled);
+hs_status hs_bem_session_profile(const hs_bem_session *session, char *names_buffer, size_t names_size,
+                                 double *ms, uint64_t *launches, size_t capacity, size_t *count);
+
+/* Work counters of the solves since profiling was last enabled, in this
+ * order: regular unordered pairs with the 6/12/16/64-point rules (4 values),
+ * regular pair samples, touching-pair samples, near-pair samples (each
+ * sample evaluates the Green kernel once for both orientations of an
+ * unordered pair where applicable), solved frequency points. */
+hs_status hs_bem_session_work(const hs_bem_session *session, uint64_t *counters, size_t capacity, size_t *count);
+
+/* Test hooks: the host interaction plan of a mesh (no device needed) and a
+ * session's assembled system. hs_bem_debug_plan centres the mesh on vertex 0
+ * like a session, plans at wavenumber max_k and writes sizes = {touching,
+ * near, patches, whole-panel bytes, near-trial entries, maximum depth}; any
+ * array pointer may be NULL to query sizes first. Layouts match the
+ * reference's InteractionPlan (interaction_plan.hpp:25-53): touching 9 u32
+ * per job (test, trial, topology, test perm[3], trial perm[3]), near 5 u32
+ * (test, trial, first patch, count, swap), patches 22 doubles (test[9],
+ * trial[9], area fraction, degree, projection, intervals), near offsets
+ * triangle_count + 1 u32. hs_bem_debug_assemble writes the row-equilibrated
+ * matrix (column-major N x N complex) and right-hand side (N complex) of one
+ * excitation with per-triangle flux q (T complex) at wavenumber k, planned
+ * at plan_k >= k. */
+hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                            size_t triangle_count, const hs_numerics *numerics, double max_k, size_t *sizes,
+                            uint32_t *touching, uint32_t *near, double *patches, uint8_t *whole,
+                            uint32_t *near_offsets, uint32_t *near_trials);
+hs_status hs_bem_debug_assemble(hs_bem_session *session, const hs_numerics *numerics, double plan_k, double k,
+                                const double *flux, double *matrix, double *rhs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HS_BEM_H */

@@ -1,0 +1,88 @@
+"""Request validation, error classes and cancellation of the CUDA solver,
+matching the reference's behaviour (cuda_solver.cu:1054-1137, 1165-1212)."""
+import numpy as np
+import pytest
+
+import hornsculpt_b200 as hs
+from hornsculpt_b200 import meshes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def solver():
+    s = hs.CudaBemSolver(meshes.octahedral_sphere(2))
+    yield s
+    s.close()
+
+
+def req(**kw):
+    base = dict(frequencies=[500.0], excitations=[hs.BemExcitation("u", [hs.FaceVelocity(1, 1.0)])],
+                observers=[(0, 0, .5)])
+    base.update(kw)
+    return hs.BemRequest(**base)
+
+
+def test_device_description():
+    assert "B200" in hs.CudaBemSolver.device_description()
+
+
+@pytest.mark.parametrize("kw,match", [
+    (dict(frequencies=[]), "Invalid BEM medium"),
+    (dict(frequencies=[-5.0]), "Invalid BEM medium|Solved frequency is invalid"),
+    (dict(medium=hs.AcousticMedium(-1.0, 343.0)), "Invalid BEM medium"),
+    (dict(numerics=hs.BemNumerics(quadrature_order=3)), "Invalid BEM medium"),
+    (dict(numerics=hs.BemNumerics(singular_order=21)), "Invalid BEM medium"),
+    (dict(numerics=hs.BemNumerics(relative_residual_tolerance=1e-9)), "Invalid BEM medium"),
+    (dict(excitations=[hs.BemExcitation("x", [hs.FaceVelocity(7, 1.0)])]), "known Driven face"),
+    (dict(excitations=[hs.BemExcitation("x", [hs.FaceVelocity(1, 1.0), hs.FaceVelocity(1, 2.0)])]),
+     "known Driven face"),
+    (dict(excitations=[hs.BemExcitation("x", [])]), "at least one assigned Driven face"),
+    (dict(observers=[(0, 0, 0.01)]), "outside the solid"),
+    (dict(frequencies=[500.0], interaction_plan_frequencies=[400.0, 600.0]), "planning raster"),
+    (dict(far_field=hs.FarFieldObservation((0, 0, 0), 1.0), observers=[(0, 0, 0)]), "differ from its origin"),
+])
+def test_invalid_requests(solver, kw, match):
+    with pytest.raises(ValueError, match=match):
+        solver.solve(req(**kw))
+
+
+def test_fast_multipole_is_reported_unsupported(solver):
+    with pytest.raises(hs.BemUnsupported):
+        solver.solve(req(numerics=hs.BemNumerics(acceleration="fast_multipole")))
+
+
+def test_electrically_coarse_mesh_rejected():
+    """k*h > 3.25 (regular_qualification.hpp:360-368) stops the observer field
+    (tetrahedron: every pair touches, so planning is trivial)."""
+    with hs.CudaBemSolver(meshes.scalene_tetrahedron()) as tetra:
+        with pytest.raises(hs.BemError, match="qualified electrical range"):
+            tetra.solve(req(frequencies=[2000.0], excitations=[hs.BemExcitation("u", [hs.FaceVelocity(50, 1.0)])],
+                            observers=[(0, 0, 1.0)]))
+
+
+def test_cancellation(solver):
+    stop = hs.StopToken()
+    stop.request_stop()
+    with pytest.raises(hs.BemCancelled, match="BEM calculation cancelled."):
+        solver.solve(req(), stop=stop)
+    # the session stays usable after a cancelled call
+    assert solver.solve(req()).frequencies[0].excitations[0].boundary_residual < 1e-12
+
+
+def test_zero_excitation_gives_zero_field(solver):
+    res = solver.solve(req(excitations=[hs.BemExcitation("z", [hs.FaceVelocity(1, 0.0)])]))
+    ex = res.frequencies[0].excitations[0]
+    assert np.all(ex.observer_pressure == 0) and np.all(ex.boundary.pressure_trace == 0)
+    assert ex.impedances == []
+
+
+def test_progress_and_plan_reuse(solver):
+    phases = []
+    r1 = solver.solve(req(frequencies=[300.0, 500.0], interaction_plan_frequencies=[300.0, 500.0]),
+                      progress=lambda p: phases.append(p.phase))
+    r2 = solver.solve(req(frequencies=[300.0], interaction_plan_frequencies=[300.0, 500.0]))
+    assert phases[0] == 0 and phases.count(6) == 2
+    assert r2.frequencies[0].interaction_plan_reused
+    a, b = r1.frequencies[0].excitations[0], r2.frequencies[0].excitations[0]
+    assert np.array_equal(a.boundary.pressure_trace, b.boundary.pressure_trace)
