@@ -105,6 +105,9 @@ def load():
         "hs_bem_session_work": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
         "hs_bem_debug_plan": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, C.POINTER(hs_numerics), C.c_double, _P, _P,
                                         _P, _P, _P, _P, _P]),
+        "hs_bem_observer_field_noalloc": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, _P, _P, _P, C.c_size_t, C.c_double,
+                                                    C.c_uint32, C.c_int32, _P, C.c_double, C.c_double, C.c_uint32,
+                                                    _P, _P]),
         "hs_bem_debug_assemble": (C.c_int, [_P, C.POINTER(hs_numerics), C.c_double, C.c_double, _P, _P, _P]),
     }
     for name, (res, args) in sig.items():

@@ -342,4 +342,17 @@ hs_status hs_bem_debug_assemble(hs_bem_session *s, const hs_numerics *numerics, 
     });
 }
 
+hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                        size_t triangle_count, const double *pressure_trace, const double *flux,
+                                        const double *observers, size_t observer_count, double wavenumber,
+                                        uint32_t degree, int32_t far_field, const double *far_origin,
+                                        double far_reference_distance, double tolerance, uint32_t maximum_depth,
+                                        void *cuda_stream, double *observer_pressure) {
+    return guarded([&]() {
+        observerFieldNoAlloc(vertices, vertex_count, triangles, triangle_count, pressure_trace, flux, observers,
+                             observer_count, wavenumber, degree, far_field, far_origin, far_reference_distance,
+                             tolerance, maximum_depth, static_cast<cudaStream_t>(cuda_stream), observer_pressure);
+    });
+}
+
 }  // extern "C"

@@ -115,4 +115,12 @@ void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double 
                         cudaStream_t stream, class KernelTimer *timer);
 size_t fieldPartialsBytes(uint32_t T, uint32_t E, uint32_t O, uint32_t B);
 
+// Allocation-free observer field (field.cu): all inputs/outputs are caller
+// device memory, scratch is a fixed static device array.
+void observerFieldNoAlloc(const double *vertices, size_t vertexCount, const uint32_t *triangles, size_t triangleCount,
+                          const double *pressure, const double *flux, const double *observers, size_t observerCount,
+                          double k, uint32_t degree, int farField, const double *farOrigin, double farDistance,
+                          double tolerance, uint32_t maximumDepth, cudaStream_t stream, double *out);
+size_t noAllocScratchBytes();
+
 }  // namespace hsb

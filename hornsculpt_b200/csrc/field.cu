@@ -8,6 +8,9 @@
 #include "host_mesh.hpp"
 #include "kernel_timer.hpp"
 
+#include <algorithm>
+#include <cmath>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -268,6 +271,210 @@ void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double 
     fieldKernel<<<unsigned(outputs * tiles), 128, 0, stream>>>(req, ks, pressure, flux, batchDegree, partials, error);
     finishKernel<<<unsigned((outputs + 127) / 128), 128, 0, stream>>>(partials, tiles, outputs, out, error);
     check(cudaGetLastError(), "field launch");
+}
+
+namespace {
+// ---------------------------------------------------------------------------
+// Allocation-free observer field.
+//
+// Some callers cannot allocate device memory at the time they need an
+// observer field: an interactive sweep that must not stall on the device-wide
+// synchronisation cudaMalloc/cudaFree imply, a host application that hands the
+// solver only memory from its own pre-sized arena, or a process that has
+// already committed all device memory it may use. This entry point serves
+// them: the caller passes every input and output as device memory it already
+// owns, and the only extra device memory is the fixed scratch array below,
+// which is part of the library's device image (loaded with the module, held
+// by every GPU that loads the library until the process exits).
+//
+// The scratch holds, per call: the panel table built from the caller's raw
+// mesh, observers in session coordinates, the wavenumber and rule degree, the
+// device error word and the per-tile partial sums. Its maximum is 4 MiB:
+// T * 200 B + O * 24 B + O * ceil(T / 256) * 16 B + 256 B must fit.
+// Every call reuses the same array and leaves its contents behind; the error
+// word is cleared at the start of each call and all other entries are fully
+// rewritten. Calls that overlap on the GPU (from several host threads or on
+// several streams) race on the array and must be serialised by the caller.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;
+static __device__ __align__(256) double gNoAllocScratch[kNoAllocScratchBytes / sizeof(double)];
+constexpr int kErrDegenerate = 5;
+constexpr int kErrIndex = 6;
+
+// Panel table and observers from the caller's raw arrays, in the session's
+// coordinates (centred on vertex 0) and with the session's panel arithmetic.
+__global__ void noAllocPrepareKernel(const double *vertices, uint32_t N, const uint32_t *triangles, uint32_t T,
+                                     const double *observers, uint32_t O, int farField, double k, uint32_t degree,
+                                     DPanel *panels, double *localObservers, double *ks, uint32_t *degrees,
+                                     int *error) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const double ox = vertices[0], oy = vertices[1], oz = vertices[2];
+    if (i < T) {
+        V3 v[3];
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t n = triangles[3 * i + c];
+            if (n >= N) {  // invalid vertex index: flag it and leave the panel unread
+                atomicExch(error, kErrIndex);
+                return;
+            }
+            v[c] = V3{vertices[3 * n] - ox, vertices[3 * n + 1] - oy, vertices[3 * n + 2] - oz};
+        }
+        const V3 ab = v[1] - v[0], ac = v[2] - v[0], bc = v[2] - v[1];
+        const V3 av = cross(ab, ac);
+        const double twice = norm3d(av.x, av.y, av.z);
+        const double maxEdge = fmax(fmax(norm3d(ab.x, ab.y, ab.z), norm3d(ac.x, ac.y, ac.z)), norm3d(bc.x, bc.y, bc.z));
+        if (!(twice > 128.0 * 2.220446049250313e-16 * maxEdge * maxEdge))
+            atomicExch(error, kErrDegenerate);
+        DPanel d;
+        const double e1[3] = {ab.x, ab.y, ab.z}, e2[3] = {ac.x, ac.y, ac.z}, v0[3] = {v[0].x, v[0].y, v[0].z};
+        for (int c = 0; c < 3; ++c) {
+            d.v0[c] = v0[c];
+            d.e1[c] = e1[c];
+            d.e2[c] = e2[c];
+            d.nodes[c] = triangles[3 * i + c];
+        }
+        d.n[0] = av.x / twice;
+        d.n[1] = av.y / twice;
+        d.n[2] = av.z / twice;
+        for (int c = 0; c < 9; ++c)
+            d.curl[c] = 0;  // the field does not use the surface curls
+        d.area = 0.5 * twice;
+        d.maxEdge = maxEdge;
+        d.pad = 0;
+        panels[i] = d;
+    }
+    if (i < O && !farField) {
+        localObservers[3 * i] = observers[3 * i] - ox;
+        localObservers[3 * i + 1] = observers[3 * i + 1] - oy;
+        localObservers[3 * i + 2] = observers[3 * i + 2] - oz;
+    }
+    if (i == 0) {
+        ks[0] = k;
+        degrees[0] = degree;
+    }
+}
+
+// Far-field directions (x - origin)/|x - origin|, origin given in world coordinates.
+__global__ void noAllocDirectionsKernel(const double *observers, uint32_t O, double fx, double fy, double fz,
+                                        double *directions, int *error) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= O)
+        return;
+    const double x = observers[3 * i] - fx, y = observers[3 * i + 1] - fy, z = observers[3 * i + 2] - fz;
+    const double d = norm3d(x, y, z);
+    if (!(d > 0) || !isfinite(d)) {
+        atomicExch(error, kErrDistance);
+        return;
+    }
+    directions[3 * i] = x / d;
+    directions[3 * i + 1] = y / d;
+    directions[3 * i + 2] = z / d;
+}
+
+std::mutex gNoAllocMutex;
+void *gNoAllocAddress[256] = {};
+
+}  // namespace
+
+// Set-up once per device, with that device current: the host name of the
+// array is only a stand-in, so its device address is looked up here and
+// passed to the kernels. The first call on a device does this look-up and
+// should therefore come before any stream capture on that device.
+static double *noAllocScratch(int device) {
+    std::lock_guard<std::mutex> lock(gNoAllocMutex);
+    if (device < 0 || device >= 256)
+        throw std::runtime_error("CUDA device ordinal out of range for the no-allocation scratch.");
+    if (!gNoAllocAddress[device]) {
+        void *address = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&address, gNoAllocScratch);
+        if (e != cudaSuccess || !address)
+            throw std::runtime_error(std::string("no-allocation scratch address: ") + cudaGetErrorString(e));
+        gNoAllocAddress[device] = address;
+    }
+    return static_cast<double *>(gNoAllocAddress[device]);
+}
+
+size_t noAllocScratchBytes() { return kNoAllocScratchBytes; }
+
+// Observer pressure of one solved frequency without device allocation; see
+// hs_bem_observer_field_noalloc in include/hs_bem.h. Throws on invalid sizes
+// before any device work, and on device error codes after the field.
+void observerFieldNoAlloc(const double *vertices, size_t vertexCount, const uint32_t *triangles, size_t triangleCount,
+                          const double *pressure, const double *flux, const double *observers, size_t observerCount,
+                          double k, uint32_t degree, int farField, const double *farOrigin, double farDistance,
+                          double tolerance, uint32_t maximumDepth, cudaStream_t stream, double *out) {
+    if (!vertices || !triangles || !pressure || !flux || !out || !vertexCount || !triangleCount)
+        throw std::invalid_argument("No-allocation field: device inputs and output must be non-null and nonempty.");
+    if (observerCount && !observers)
+        throw std::invalid_argument("No-allocation field: observers are null.");
+    if (degree != 4 && degree != 6 && degree != 8 && degree != 12 && degree != 14)
+        throw std::invalid_argument("No-allocation field: rule degree must be 4, 6, 8, 12 or 14.");
+    if (!std::isfinite(k) || k <= 0 || !std::isfinite(tolerance) || tolerance <= 0 || maximumDepth > 10 ||
+        (farField && (!farOrigin || !std::isfinite(farDistance) || farDistance <= 0)))
+        throw std::invalid_argument("No-allocation field: wavenumber, tolerance, depth or far-field settings invalid.");
+    if (vertexCount > 0xffffffffu || triangleCount > 0xffffffffu || observerCount > 0xffffffffu)
+        throw std::invalid_argument("No-allocation field: sizes exceed 32-bit indexing.");
+    if (!observerCount)
+        return;
+    const uint32_t T = uint32_t(triangleCount), O = uint32_t(observerCount), N = uint32_t(vertexCount);
+    const size_t tiles = (T + kTile - 1) / kTile;
+    // Scratch layout (doubles): panels | observers | k, degree | error | partials
+    const size_t panelDoubles = size_t(T) * (sizeof(DPanel) / sizeof(double));
+    const size_t obsOffset = panelDoubles, parOffset = obsOffset + 3 * size_t(O) + 4;
+    const size_t needed = (parOffset + 2 * size_t(O) * tiles) * sizeof(double);
+    if (needed > kNoAllocScratchBytes)
+        throw std::invalid_argument("No-allocation field needs " + std::to_string(needed) + " bytes of scratch for " +
+                                    std::to_string(T) + " triangles and " + std::to_string(O) +
+                                    " observers; its fixed maximum is " + std::to_string(kNoAllocScratchBytes) +
+                                    " bytes (4 MiB).");
+    int device = 0;
+    check(cudaGetDevice(&device), "no-allocation field device");
+    double *scratch = noAllocScratch(device);
+    DPanel *panels = reinterpret_cast<DPanel *>(scratch);
+    double *localObservers = scratch + obsOffset;
+    double *ks = scratch + obsOffset + 3 * size_t(O);
+    uint32_t *degrees = reinterpret_cast<uint32_t *>(ks + 1);
+    int *error = reinterpret_cast<int *>(ks + 2);
+    double *partials = scratch + parOffset;
+    check(cudaMemsetAsync(error, 0, sizeof(int), stream), "no-allocation field error reset");
+    double origin[3];
+    check(cudaMemcpyAsync(origin, vertices, sizeof(origin), cudaMemcpyDeviceToHost, stream), "mesh origin");
+    check(cudaStreamSynchronize(stream), "mesh origin");
+    const uint32_t threads = std::max(T, O);
+    noAllocPrepareKernel<<<(threads + 127) / 128, 128, 0, stream>>>(vertices, N, triangles, T, observers, O, farField,
+                                                                   k, degree, panels, localObservers, ks, degrees,
+                                                                   error);
+    if (farField)
+        noAllocDirectionsKernel<<<(O + 127) / 128, 128, 0, stream>>>(observers, O, farOrigin[0], farOrigin[1],
+                                                                     farOrigin[2], localObservers, error);
+    check(cudaGetLastError(), "no-allocation field preparation");
+    // The field kernel indexes the trace through the panel table: stop here on
+    // invalid indices or degenerate panels.
+    int prepared = 0;
+    check(cudaMemcpyAsync(&prepared, error, sizeof(int), cudaMemcpyDeviceToHost, stream), "no-allocation field status");
+    check(cudaStreamSynchronize(stream), "no-allocation field preparation");
+    if (prepared == kErrIndex)
+        throw std::invalid_argument("No-allocation field: a triangle has an invalid vertex index.");
+    if (prepared == kErrDegenerate)
+        throw NumericError("Galerkin triangle is degenerate or numerically unresolved.");
+    if (prepared == kErrDistance)
+        throw std::invalid_argument("A far-field direction must differ from its origin.");
+    FieldRequest req{panels, T, N, 1, O, 1, localObservers, farField,
+                     {farField ? farOrigin[0] - origin[0] : 0.0, farField ? farOrigin[1] - origin[1] : 0.0,
+                      farField ? farOrigin[2] - origin[2] : 0.0},
+                     farField ? farDistance : 1.0, tolerance, maximumDepth};
+    evaluateFieldBatch(req, ks, pressure, flux, degrees, partials, out, error, stream, nullptr);
+    int code = 0;
+    check(cudaMemcpyAsync(&code, error, sizeof(int), cudaMemcpyDeviceToHost, stream), "no-allocation field status");
+    check(cudaStreamSynchronize(stream), "no-allocation field");
+    if (code == kErrDegenerate)
+        throw NumericError("Galerkin triangle is degenerate or numerically unresolved.");
+    if (code == kErrDistance)
+        throw NumericError("BEM quadrature encountered zero or invalid source distance.");
+    if (code == kErrFieldDepth)
+        throw NumericError("BEM field integration did not reach its near-field tolerance.");
+    if (code)
+        throw NumericError("BEM calculation produced a non-finite value.");
 }
 
 }  // namespace hsb

@@ -217,6 +217,33 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
 hs_status hs_bem_debug_assemble(hs_bem_session *session, const hs_numerics *numerics, double plan_k, double k,
                                 const double *flux, double *matrix, double *rhs);
 
+/* Allocation-free observer field. No counterpart in the reference: it is an
+ * addition for callers that cannot allocate device memory when they need a
+ * field — an interactive sweep that must not stall on the device-wide
+ * synchronisation of cudaMalloc/cudaFree, or a host that gives the solver only
+ * memory from its own pre-sized arena. All pointers except far_origin are
+ * DEVICE memory the caller owns: vertices (vertex_count x 3), triangles
+ * (triangle_count x 3), the solved P1 trace (vertex_count complex), the DP0
+ * flux q = -i rho omega v (triangle_count complex), observers
+ * (observer_count x 3 world points, or far-field points when far_field is
+ * nonzero), and the output (observer_count complex). The same quantity as a
+ * solve's observer pressure at rule degree `degree` (4, 6, 8, 12 or 14) with
+ * near-field tolerance `tolerance` and depth `maximum_depth`. The function
+ * calls no cudaMalloc, cudaFree or allocating library routine; its scratch is
+ * a fixed 4 MiB static device array of the library, which limits
+ * triangle_count * 200 + observer_count * 24 +
+ * observer_count * ceil(triangle_count / 256) * 16 + 256 bytes to 4 MiB (larger
+ * requests return HS_E_INVALID). The first call on a device looks up that
+ * array's device address, so make it before any stream capture on that device.
+ * All calls share the array: calls that overlap on the GPU race and must be
+ * serialised. The call returns after the work on `cuda_stream` has finished. */
+hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                        size_t triangle_count, const double *pressure_trace, const double *flux,
+                                        const double *observers, size_t observer_count, double wavenumber,
+                                        uint32_t degree, int32_t far_field, const double *far_origin,
+                                        double far_reference_distance, double tolerance, uint32_t maximum_depth,
+                                        void *cuda_stream, double *observer_pressure);
+
 #ifdef __cplusplus
 }
 #endif
