@@ -1,12 +1,14 @@
 """Benchmark of the exterior Burton-Miller solve on B200.
 
-Workload (dense plain FP64 form): pulsating rigid sphere of radius 0.1 m as an
+Workload (dense form): pulsating rigid sphere of radius 0.1 m as an
 icosphere with 3 subdivisions (642 vertices / 1280 triangles), uniform normal
 velocity 1 m/s, c = 343 m/s, rho = 1.205 kg/m^3, 32 log-spaced frequencies
 100 Hz - 5 kHz, observers (0,0,.3), (1,0,0), (0,0,3). One step = one sweep of
 the 32 frequency points through a solver session whose interaction plan is
 cached across steps (the reference's sweep usage). Metric: frequency-point
-solves per second (higher is better).
+solves per second (higher is better) of the mixed-precision form, whose
+surface-pressure error against the plain FP64 form is measured in the same
+run; the plain FP64 form is timed beside it.
 
 Multi-GPU: one process per GPU, each rank solves its own replica of the sweep
 (frequency points are independent; no collective on the data path); value is
@@ -33,14 +35,22 @@ sys.path.insert(0, str(ROOT))
 FREQUENCIES = [float(f) for f in __import__("numpy").geomspace(100.0, 5000.0, 32)]
 OBSERVERS = [(0.0, 0.0, 0.3), (1.0, 0.0, 0.0), (0.0, 0.0, 3.0)]
 DENSITY, SOUND_SPEED = 1.205, 343.0
-METRIC = "freq-point solves/s (dense plain FP64 form, C1 sphere sweep)"
+METRIC = "freq-point solves/s (dense mixed-precision form at <=1e-5 surface-pressure error vs the plain FP64 form, C1 sphere sweep)"
 # Algorithmic FP64 operations per regular-pair sample (one Green-kernel
 # evaluation shared by both orientations of an unordered pair), counted from
 # the regular-pair kernel source: displacement 15, |d|^2 5, 1/r 1, r and kr 2,
 # sincos 1, weight 2, g 2, g(1+ikr) 4, 1/r^2 1, two normal projections 12,
 # P and Q 4, three basis contractions 36.
 FLOPS_PER_REGULAR_SAMPLE = 85
-CONFIG = {"workload": "C1 icosphere s3 (642 v / 1280 t), 32 log freqs 100 Hz-5 kHz, 3 observers, dense FP64",
+# Mixed-form regular sample, counted from its kernel source: FP64 trial point
+# 9 + displacement 3 + |d|^2 5 + Newton root 5 + r and k*r 2 + turns 2 +
+# reduction 4; FP32 |d|^2 5, 1/r 1, sincos 1, weights 3, g 2, g(1+ikr) 4,
+# 1/r^2 1, normal projections 12, P and Q 4, trial contractions 36, test
+# contraction amortised over the rule (108/NP, taken at NP = 12) 9.
+MIXED_FP64_FLOPS_PER_SAMPLE = 30
+MIXED_FP32_FLOPS_PER_SAMPLE = 78
+CONFIG = {"workload": "C1 icosphere s3 (642 v / 1280 t), 32 log freqs 100 Hz-5 kHz, 3 observers, dense; "
+                      "mixed form timed, plain FP64 form timed beside it",
           "mesh": "icosphere-3 r=0.1 m", "frequencies": 32, "observers": 3, "excitations": 1,
           "l2": "per-sweep working set 10 GB (pair records) > 126 MB L2; L2 also flushed between steps"}
 
@@ -74,47 +84,78 @@ def cpu_reference(samples: int, frequencies_per_sample: int):
 
 
 class ClockSampler:
-    """nvidia-smi clock and throttle-reason samples during the timed region."""
+    """SM clock, power and throttle reasons sampled during the timed region by
+    an in-process NVML thread (read-only queries; one light query set per
+    period, which perturbs the host's CUDA calls far less than a polling
+    nvidia-smi process). Falls back to `nvidia-smi -lms` when NVML is absent."""
 
-    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
-             "clocks_event_reasons.sw_power_cap"
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, device_index: int):
-        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    def __init__(self, device_index: int, enabled: bool = True, period_s: float = 0.25):
         self.device = device_index
+        self.enabled = enabled
+        self.period = period_s
+        self.samples = []
+        self.thread = None
+        self.stop = None
         self.proc = None
+        self.file = None
 
     def __enter__(self):
+        if not self.enabled:
+            return self
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+            import pynvml
+            pynvml.nvmlInit()
+            handle = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+        except Exception:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            fields = "clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active"
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={fields}",
+                                          "--format=csv,noheader,nounits", "-lms", "500"], stdout=self.file,
                                          stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            return self
+        self.stop = threading.Event()
+
+        def run():
+            while True:
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(handle, pynvml.NVML_CLOCK_SM)
+                    mx = pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM)
+                    reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                    self.samples.append((sm, mx, reasons))
+                except Exception:
+                    pass
+                if self.stop.wait(self.period):
+                    return
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
         return self
 
     def __exit__(self, *exc):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             self.proc.wait(timeout=10)
 
     def summary(self):
-        self.file.flush()
-        rows = [line.split(",") for line in open(self.file.name).read().splitlines() if line.strip()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        sm, mx, reasons = [], 0.0, set()
-        for r in rows:
-            try:
-                sm.append(float(r[1]))
-                mx = max(mx, float(r[2]))
-                for name, v in zip(names, r[5:9]):
-                    if v.strip() == "Active":
-                        reasons.add(name)
-            except (ValueError, IndexError):
-                continue
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.file is not None:
+            self.file.flush()
+            for line in open(self.file.name).read().splitlines():
+                parts = line.split(",")
+                try:
+                    self.samples.append((float(parts[0]), float(parts[1]), int(parts[3], 16)))
+                except (ValueError, IndexError):
+                    continue
+        sm = [x[0] for x in self.samples]
+        reasons = sorted({name for _, _, bits in self.samples for name, mask in self.REASONS.items() if bits & mask})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max((x[1] for x in self.samples), default=None), "reasons": reasons,
+                "samples": len(sm), "source": "nvml" if self.file is None else "nvidia-smi"}
 
 
 def measured_peaks():
@@ -138,6 +179,29 @@ def fp64_peak_tflops(torch):
         e.synchronize()
         best = min(best, s.elapsed_time(e) / 1e3)
     return 2 * n ** 3 / best / 1e12
+
+
+def fp32_peak_tflops(torch):
+    """FP32 dense throughput of cuBLAS SGEMM with TF32 disabled (4096^3, best of 5)."""
+    previous = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        n = 4096
+        a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = math.inf
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e) / 1e3)
+        return 2 * n ** 3 / best / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = previous
 
 
 def run_reference(args, rank, world):
@@ -172,6 +236,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)  # >= 3 for reported numbers
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-clock-sampler", action="store_true", help="skip nvidia-smi sampling (diagnostics)")
     ap.add_argument("--sweep-frequencies", type=int, default=32,
                     help="solve only the first n sweep frequencies (small profiling cases)")
     args = ap.parse_args()
@@ -202,58 +267,119 @@ def main():
         if world > 1:
             dist.barrier()
 
-    for _ in range(args.warmup):
-        solver.solve(req)
     peaks = measured_peaks()
     fp64 = fp64_peak_tflops(torch)
-    solver.set_profiling(True)
-    device_s, wall_s = 0.0, 0.0
-    barrier()
-    with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            start.record(stream)
-            t0 = time.perf_counter()
-            result = solver.solve(req)
-            wall_s += time.perf_counter() - t0
-            end.record(stream)
-            end.synchronize()
-            device_s += start.elapsed_time(end) / 1e3
-    barrier()
-    times = torch.tensor([device_s, wall_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    device_s, wall_s = times.tolist()
-    profile, work = solver.profile(), solver.work()
+    fp32 = fp32_peak_tflops(torch)
+
+    def run_form(precision):
+        """Warm-up, then the timed steps of one precision form; device and wall seconds (max over ranks)."""
+        req.numerics = hs.BemNumerics(precision=precision)
+        for _ in range(args.warmup):
+            solver.solve(req)
+        solver.set_profiling(True)
+        device_s, wall_s, result = 0.0, 0.0, None
+        step_ms, phase_ms = [], []
+        barrier()
+        with ClockSampler(local, enabled=not args.no_clock_sampler) as clocks:
+            for _ in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                t0 = time.perf_counter()
+                result = solver.solve(req)
+                wall_s += time.perf_counter() - t0
+                end.record(stream)
+                end.synchronize()
+                device_s += start.elapsed_time(end) / 1e3
+                step_ms.append(round(start.elapsed_time(end), 2))
+                phase_ms.append(round(sum(f.assembly_milliseconds + f.solve_milliseconds + f.field_milliseconds
+                                          for f in result.frequencies), 2))
+        barrier()
+        times = torch.tensor([device_s, wall_s], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(times, op=dist.ReduceOp.MAX)
+        device_s, wall_s = times.tolist()
+        profile, work = solver.profile(), solver.work()
+        solver.set_profiling(False)
+        span = profile.pop("solve_span", (0.0, 0))[0] / 1e3
+        span_t = torch.tensor([span], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(span_t, op=dist.ReduceOp.MAX)
+        span = span_t.item()
+        return dict(device_s=device_s, wall_s=wall_s, span_s=span, result=result, profile=profile, work=work,
+                    clocks=clocks.summary(), step_ms=step_ms, phase_ms=phase_ms)
+
+    plain = run_form("fp64")
+    mixed = run_form("mixed")
     points = len(req.frequencies) * args.steps * world
     if rank == 0:
-        regular = [k for k in profile if k.startswith("regular_")]
-        regular_ms = sum(profile[k][0] for k in regular)
-        regular_launches = sum(profile[k][1] for k in regular)
-        total_ms = sum(v[0] for v in profile.values())
-        flops = work["regular_samples"] * FLOPS_PER_REGULAR_SAMPLE
-        achieved = flops / (regular_ms / 1e3) / 1e12
-        ex = result.frequencies[0].excitations[0]
+        def regular_stats(form, prefix):
+            prof = form["profile"]
+            keys = [k for k in prof if k.startswith(prefix)]
+            ms = sum(prof[k][0] for k in keys)
+            return ms, sum(v[0] for v in prof.values())
+
+        p_ms, p_total = regular_stats(plain, "regular_q")
+        m_ms, m_total = regular_stats(mixed, "regular_mixed_q")
+        p_samples, m_samples = plain["work"]["regular_samples"], mixed["work"]["regular_samples"]
+        p_achieved = p_samples * FLOPS_PER_REGULAR_SAMPLE / (p_ms / 1e3) / 1e12
+        m64 = m_samples * MIXED_FP64_FLOPS_PER_SAMPLE / (m_ms / 1e3) / 1e12
+        m32 = m_samples * MIXED_FP32_FLOPS_PER_SAMPLE / (m_ms / 1e3) / 1e12
+        # area-weighted relative L2 of DP0 surface pressure, mixed vs plain, worst frequency
+        v = mesh.vertices[mesh.triangles]
+        area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+        err = 0.0
+        for fp, fm in zip(plain["result"].frequencies, mixed["result"].frequencies):
+            a, b = fp.excitations[0].boundary.surface_pressure, fm.excitations[0].boundary.surface_pressure
+            err = max(err, float(np.sqrt((area * np.abs(b - a) ** 2).sum() / (area * np.abs(a) ** 2).sum())))
         T, N, O = mesh.triangle_count, mesh.vertex_count, len(OBSERVERS)
-        h2d = len(FREQUENCIES) * (T * 16 + 8) + O * 24
-        d2h = len(FREQUENCIES) * (N * 16 + O * 16 + 32)
+        F = len(req.frequencies)
+        h2d = F * (T * 16 + 8) + O * 24
+        d2h = F * (N * 16 + O * 16 + 32)
+        value = points / mixed["span_s"]
         line = {
-            "metric": METRIC, "value": points / device_s, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * device_s / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
-            "e2e": {"value": points / wall_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * mixed["span_s"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed form)", "data": "synthetic",
+            "config": CONFIG,
+            "e2e": {"value": points / mixed["wall_s"], "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
-            "gpu_launches": int(sum(v[1] for v in profile.values())),
-            "roofline": {"kernel": "regularPairsKernel (4 rule sizes)", "bound": "fp64", "achieved": achieved,
-                         "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
-                         "peak_source": "cuBLAS DGEMM 4096^3 measured in this run (MEASURED_PEAKS.json has no FP64 figure)",
-                         "traffic": None, "share_of_device_time": regular_ms / total_ms,
-                         "algorithmic": f"{work['regular_samples']} regular samples x {FLOPS_PER_REGULAR_SAMPLE} FLOP"},
-            "kernel_ms": {k: round(v[0] / args.steps, 4) for k, v in sorted(profile.items())},
-            "clocks": clocks.summary(), "peaks": {"hbm_gbs": peaks.get("hbm_gbs"), "fp64_tflops_dgemm": fp64},
-            "residual_max": max(e.boundary_residual for f in result.frequencies for e in f.excitations),
+            "gpu_launches": int(sum(v[1] for v in mixed["profile"].values())),
+            "forms": {
+                "fp64_plain": {"value": points / plain["span_s"], "e2e": points / plain["wall_s"],
+                               "ms_per_step": 1e3 * plain["span_s"] / args.steps,
+                               "step_ms": plain["step_ms"], "phase_ms": plain["phase_ms"],
+                               "residual_max": max(e.boundary_residual for f in plain["result"].frequencies
+                                                   for e in f.excitations)},
+                "mixed": {"value": value, "e2e": points / mixed["wall_s"],
+                          "ms_per_step": 1e3 * mixed["span_s"] / args.steps,
+                          "step_ms": mixed["step_ms"], "phase_ms": mixed["phase_ms"],
+                          "residual_max": max(e.boundary_residual for f in mixed["result"].frequencies
+                                              for e in f.excitations),
+                          "max_rel_err_surface_vs_fp64": err},
+                "mixed_over_fp64": plain["span_s"] / mixed["span_s"],
+                "timing": "value: CUDA events on the session stream around each sweep inside the library "
+                          "(first upload to last result download, host control included); e2e: wall clock of "
+                          "the Python API call with host request and result buffers",
+            },
+            "roofline": {"kernel": "regularMixedKernel (4 rule sizes), the mixed form's dominant kernel",
+                         "bound": "fp64+fp32 pipes", "unit": "TFLOP/s",
+                         "achieved": {"fp64": m64, "fp32": m32}, "peak": {"fp64": fp64, "fp32": fp32},
+                         "frac": max(m64 / fp64, m32 / fp32),
+                         "peak_source": "cuBLAS DGEMM and SGEMM (TF32 off) 4096^3 measured in this run; "
+                                        "MEASURED_PEAKS.json has no FP32/FP64 figures",
+                         "traffic": None, "share_of_device_time": m_ms / m_total,
+                         "algorithmic": f"{m_samples} samples x ({MIXED_FP64_FLOPS_PER_SAMPLE} FP64 + "
+                                        f"{MIXED_FP32_FLOPS_PER_SAMPLE} FP32 FLOP)"},
+            "roofline_fp64_plain": {"kernel": "regularPairsKernel (4 rule sizes)", "bound": "fp64",
+                                    "achieved": p_achieved, "peak": fp64, "unit": "TFLOP/s", "frac": p_achieved / fp64,
+                                    "share_of_device_time": p_ms / p_total,
+                                    "algorithmic": f"{p_samples} samples x {FLOPS_PER_REGULAR_SAMPLE} FLOP"},
+            "kernel_ms": {"mixed": {k: round(v[0] / args.steps, 4) for k, v in sorted(mixed["profile"].items())},
+                          "fp64_plain": {k: round(v[0] / args.steps, 4) for k, v in sorted(plain["profile"].items())}},
+            "clocks": mixed["clocks"], "clocks_fp64_plain": plain["clocks"],
+            "peaks": {"hbm_gbs": peaks.get("hbm_gbs"), "fp64_tflops_dgemm": fp64, "fp32_tflops_sgemm": fp32},
         }
         if world == 1 and not args.no_cpu_baseline:
             times_cpu, picks = cpu_reference(1, 2)

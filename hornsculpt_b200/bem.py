@@ -54,7 +54,7 @@ class BemNumerics:
     relative_residual_tolerance: float = 5e-5
     maximum_refinement_steps: int = 3
     acceleration: str = "dense"  # "dense" | "fast_multipole"
-    precision: str = "fp64"      # the plain form
+    precision: str = "fp64"      # "fp64" (plain form) | "mixed" (FP32 samples and LU, FP64 refinement)
     fast_multipole: FastMultipoleSettings = dataclasses.field(default_factory=FastMultipoleSettings)
 
     def to_c(self) -> _lib.hs_numerics:
@@ -67,7 +67,7 @@ class BemNumerics:
         n.relative_residual_tolerance = self.relative_residual_tolerance
         n.maximum_refinement_steps = self.maximum_refinement_steps
         n.acceleration = {"dense": 0, "fast_multipole": 1}.get(self.acceleration, 99)
-        n.precision = {"fp64": 0}.get(self.precision, 99)
+        n.precision = {"fp64": 0, "mixed": 1}.get(self.precision, 99)
         f = self.fast_multipole
         n.fmm_leaf_support_capacity = f.leaf_support_capacity
         n.fmm_separation_ratio = f.separation_ratio

@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 
 namespace hsb {
 namespace {
@@ -54,14 +55,15 @@ struct PairMoments {
 // block (test s, trial t)) of an unordered pair from its moments. Forward:
 // A_ij = -MP_ij + i k (n_t.n_s) MG_ij + alpha G (curl_ti . curl_sj),
 // b_i = sum_j (-MG_ij + (i/k) MQ_ij); reverse swaps P and Q and transposes.
-__device__ __forceinline__ void pairRecordValue(int o, const double *MG, const double *MP, const double *MQ,
+template <class Real>
+__device__ __forceinline__ void pairRecordValue(int o, const Real *MG, const Real *MP, const Real *MQ,
                                                 const DPanel &t, const DPanel &s, double k, double invk,
                                                 double &re, double &im) {
     const double nn = t.n[0] * s.n[0] + t.n[1] * s.n[1] + t.n[2] * s.n[2];
     const bool reverse = o >= 12;
     const int e = reverse ? o - 12 : o;
-    const double *X = reverse ? MQ : MP;  // double-layer moments of this direction
-    const double *Y = reverse ? MP : MQ;  // adjoint moments of this direction
+    const Real *X = reverse ? MQ : MP;  // double-layer moments of this direction
+    const Real *Y = reverse ? MP : MQ;  // adjoint moments of this direction
     if (e < 9) {
         // forward element (i, j); reverse element (row j of s, col i of t) = moments (i, j)
         const int row = e / 3, col = e % 3;
@@ -205,6 +207,128 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
             dst[1] = im;
         }
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Mixed form: the Green-kernel sample with FP32 arithmetic. The displacement
+// and the phase k*r stay in FP64 (the phase reduced modulo 2 pi before the
+// FP32 sine/cosine), because rounding r or k*r to FP32 leaves an
+// O(eps_fp32 * k*r) phase error that no quadrature refinement removes
+// (panel_integrals.cuh:91-142 keeps FP64 for k*r > 1 for the same reason).
+// Returns g, P and Q (see PairMoments) as (re, im) pairs.
+// ---------------------------------------------------------------------------
+constexpr double kTwoPiHi = 6.283185307179586, kTwoPiLo = 2.4492935982947064e-16, kInvTwoPi = 0.15915494309189535;
+
+__device__ __forceinline__ void mixedValues(double dx, double dy, double dz, float w, double k, const float *ns,
+                                            const float *nt, float (&val)[6], bool &bad) {
+    const float fx = float(dx), fy = float(dy), fz = float(dz);
+    const float r2 = fx * fx + fy * fy + fz * fz;
+    bad |= !(r2 > 0.f) || !isfinite(r2);
+    const float rinv = rsqrtf(r2);
+    // r in FP64 from one Newton step on the FP32 reciprocal root
+    const double r2d = dx * dx + dy * dy + dz * dz;
+    double y = double(rinv);
+    y = y * (1.5 - 0.5 * r2d * y * y);
+    const double ph = k * (r2d * y);
+    const double turns = rint(ph * kInvTwoPi);
+    const double th = fma(-turns, kTwoPiLo, fma(-turns, kTwoPiHi, ph));
+    float sn, cs;
+    sincosf(float(th), &sn, &cs);
+    const float kr = float(ph);
+    const float sc = w * rinv;
+    const float gr = cs * sc, gi = -sn * sc;
+    const float rr = gr - gi * kr, ri = gi + gr * kr;
+    const float rinv2 = rinv * rinv;
+    const float ps = (fx * ns[0] + fy * ns[1] + fz * ns[2]) * rinv2;
+    const float qt = -(fx * nt[0] + fy * nt[1] + fz * nt[2]) * rinv2;
+    val[0] = gr;
+    val[1] = gi;
+    val[2] = rr * ps;
+    val[3] = ri * ps;
+    val[4] = rr * qt;
+    val[5] = ri * qt;
+}
+
+// Regular pairs in the mixed form: one unordered pair per thread, NP x NP
+// samples, trial bases contracted per test point (FP32), no shared memory.
+template <int NP>
+__global__ void __launch_bounds__(256, 2) regularMixedKernel(const DPanel *__restrict__ panels, uint32_t T,
+                                                          const double *__restrict__ ks,
+                                                          const uint2 *__restrict__ bins,
+                                                          const uint32_t *__restrict__ binCounts, size_t binCapacity,
+                                                          int bin, double *__restrict__ records, int *error) {
+    constexpr int RO = ruleOffset<NP>();
+    const int f = blockIdx.y;
+    const double k = ks[f], invk = 1.0 / k;
+    const uint32_t count = binCounts[f * kBins + bin];
+    const uint2 *list = bins + (size_t(f) * kBins + bin) * binCapacity;
+    double *rec = records + size_t(f) * T * T * kRecordDoubles;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+        const uint2 pr = list[p];
+        const DPanel &A = panels[pr.x];
+        const DPanel &S = panels[pr.y];
+        const double d0 = A.v0[0] - S.v0[0], d1 = A.v0[1] - S.v0[1], d2 = A.v0[2] - S.v0[2];
+        const float w4 = float(4.0 * A.area * S.area * kInvFourPi);
+        const float ns[3] = {float(S.n[0]), float(S.n[1]), float(S.n[2])};
+        const float nt[3] = {float(A.n[0]), float(A.n[1]), float(A.n[2])};
+        float M[54];
+#pragma unroll
+        for (int c = 0; c < 54; ++c)
+            M[c] = 0.f;
+        bool bad = false;
+        for (int x = 0; x < NP; ++x) {
+            const double bx1 = cRule[4 * (RO + x) + 1], bx2 = cRule[4 * (RO + x) + 2];
+            const double D0 = d0 + (A.e1[0] * bx1 + A.e2[0] * bx2), D1 = d1 + (A.e1[1] * bx1 + A.e2[1] * bx2),
+                         D2 = d2 + (A.e1[2] * bx1 + A.e2[2] * bx2);
+            const float wx = float(cRule[4 * (RO + x) + 3]) * w4;
+            float Sv[18];
+#pragma unroll
+            for (int c = 0; c < 18; ++c)
+                Sv[c] = 0.f;
+#pragma unroll 2
+            for (int y = 0; y < NP; ++y) {
+                const double b1 = cRule[4 * (RO + y) + 1], b2 = cRule[4 * (RO + y) + 2];
+                const float bs[3] = {float(cRule[4 * (RO + y)]), float(b1), float(b2)};
+                float val[6];
+                mixedValues(D0 - (S.e1[0] * b1 + S.e2[0] * b2), D1 - (S.e1[1] * b1 + S.e2[1] * b2),
+                            D2 - (S.e1[2] * b1 + S.e2[2] * b2), wx * float(cRule[4 * (RO + y) + 3]), k, ns, nt,
+                            val, bad);
+#pragma unroll
+                for (int kind = 0; kind < 3; ++kind)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        Sv[kind * 6 + 2 * j] += val[2 * kind] * bs[j];
+                        Sv[kind * 6 + 2 * j + 1] += val[2 * kind + 1] * bs[j];
+                    }
+            }
+            const float bt[3] = {float(cRule[4 * (RO + x)]), float(bx1), float(bx2)};
+#pragma unroll
+            for (int kind = 0; kind < 3; ++kind)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        M[kind * 18 + 2 * (3 * i + j)] += bt[i] * Sv[kind * 6 + 2 * j];
+                        M[kind * 18 + 2 * (3 * i + j) + 1] += bt[i] * Sv[kind * 6 + 2 * j + 1];
+                    }
+        }
+        if (bad)
+            flagError(error, kErrDistance);
+        double *fwd = rec + (size_t(pr.y) * T + pr.x) * kRecordDoubles;
+        double *rev = rec + (size_t(pr.x) * T + pr.y) * kRecordDoubles;
+        bool nonFinite = false;
+#pragma unroll 1
+        for (int o = 0; o < 24; ++o) {
+            double re, im;
+            pairRecordValue(o, M, M + 18, M + 36, A, S, k, invk, re, im);
+            nonFinite |= !isfinite(re) || !isfinite(im);
+            double *dst = (o < 12 ? fwd : rev) + 2 * (o < 12 ? o : o - 12);
+            dst[0] = re;
+            dst[1] = im;
+        }
+        if (nonFinite)
+            flagError(error, kErrNonFinite);
     }
 }
 
@@ -447,10 +571,36 @@ __device__ __forceinline__ void nearSample(double (&acc)[54], const DPanel &t, c
         }
 }
 
+// Mixed-form near sample: FP64 displacement and phase, FP32 kernel values
+// and accumulation.
+__device__ __forceinline__ void nearSample(float (&acc)[54], const DPanel &t, const DPanel &s, const double *bt,
+                                           const double *bs, double w, double k, bool &bad) {
+    const double dx = (t.v0[0] - s.v0[0]) + ((t.e1[0] * bt[1] + t.e2[0] * bt[2]) - (s.e1[0] * bs[1] + s.e2[0] * bs[2]));
+    const double dy = (t.v0[1] - s.v0[1]) + ((t.e1[1] * bt[1] + t.e2[1] * bt[2]) - (s.e1[1] * bs[1] + s.e2[1] * bs[2]));
+    const double dz = (t.v0[2] - s.v0[2]) + ((t.e1[2] * bt[1] + t.e2[2] * bt[2]) - (s.e1[2] * bs[1] + s.e2[2] * bs[2]));
+    const float ns[3] = {float(s.n[0]), float(s.n[1]), float(s.n[2])};
+    const float nt[3] = {float(t.n[0]), float(t.n[1]), float(t.n[2])};
+    float val[6];
+    mixedValues(dx, dy, dz, float(w), k, ns, nt, val, bad);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const float bij = float(bt[i] * bs[j]);
+#pragma unroll
+            for (int kind = 0; kind < 3; ++kind) {
+                acc[kind * 18 + 2 * (3 * i + j)] += val[2 * kind] * bij;
+                acc[kind * 18 + 2 * (3 * i + j) + 1] += val[2 * kind + 1] * bij;
+            }
+        }
+}
+
+template <bool Mixed>
 __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                   const NearPairJob *__restrict__ jobs,
                                                   const Patch *__restrict__ patches, const double *__restrict__ ks,
                                                   double *__restrict__ records, int *error) {
+    using Acc = std::conditional_t<Mixed, float, double>;
     __shared__ double red[4][54];
     __shared__ double pts[2][64][3];
     const NearPairJob job = jobs[blockIdx.x];
@@ -459,7 +609,7 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
     const DPanel &t = panels[job.first];
     const DPanel &s = panels[job.second];
     const double w4 = 4.0 * t.area * s.area * kInvFourPi;
-    double acc[54];
+    Acc acc[54];
 #pragma unroll
     for (int c = 0; c < 54; ++c)
         acc[c] = 0;
@@ -521,7 +671,11 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
     if (bad)
         flagError(error, kErrDistance);
     __syncthreads();
-    blockReduce<54>(acc, red);
+    double accd[54];
+#pragma unroll
+    for (int c = 0; c < 54; ++c)
+        accd[c] = acc[c];
+    blockReduce<54>(accd, red);
     if (threadIdx.x < 24) {
         const int o = threadIdx.x;
         double re, im;
@@ -653,12 +807,20 @@ int smCount() {
 
 template <int NP>
 void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, const AssemblyWorkspace &ws, int bin,
-                   int *error, cudaStream_t stream, KernelTimer *timer) {
+                   int *error, cudaStream_t stream, KernelTimer *timer, bool mixed) {
     const char *names[kBins] = {"regular_q6", "regular_q12", "regular_q16", "regular_q64"};
-    TimedScope scope(timer, names[bin], stream);
-    const dim3 grid(unsigned(smCount() * 6), B);
-    regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity, bin,
-                                                     ws.records, error);
+    const char *mixedNames[kBins] = {"regular_mixed_q6", "regular_mixed_q12", "regular_mixed_q16",
+                                     "regular_mixed_q64"};
+    TimedScope scope(timer, mixed ? mixedNames[bin] : names[bin], stream);
+    if (mixed) {
+        const dim3 grid(unsigned(smCount() * 8), B);
+        regularMixedKernel<NP><<<grid, 256, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
+                                                         bin, ws.records, error);
+    } else {
+        const dim3 grid(unsigned(smCount() * 6), B);
+        regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
+                                                         bin, ws.records, error);
+    }
     cudaCheck(cudaGetLastError(), "regular pair assembly launch");
 }
 
@@ -701,7 +863,7 @@ size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B) {
 
 void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *gaussSingular, const double *flux,
                    uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
-                   cudaStream_t stream, KernelTimer *timer) {
+                   cudaStream_t stream, KernelTimer *timer, bool mixed) {
     const uint64_t pairs = uint64_t(g.T) * (g.T - 1) / 2;
     if (g.N > 65535 || B > 65535 || E > 65535)
         throw std::runtime_error("Dense assembly grid limits exceeded (more than 65535 vertices, frequencies or excitations).");
@@ -714,10 +876,10 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
                                                                  ws.binCapacity, error);
         cudaCheck(cudaGetLastError(), "pair classification launch");
     }
-    launchRegular<6>(g, ks, B, ws, 0, error, stream, timer);
-    launchRegular<12>(g, ks, B, ws, 1, error, stream, timer);
-    launchRegular<16>(g, ks, B, ws, 2, error, stream, timer);
-    launchRegular<64>(g, ks, B, ws, 3, error, stream, timer);
+    launchRegular<6>(g, ks, B, ws, 0, error, stream, timer, mixed);
+    launchRegular<12>(g, ks, B, ws, 1, error, stream, timer, mixed);
+    launchRegular<16>(g, ks, B, ws, 2, error, stream, timer, mixed);
+    launchRegular<64>(g, ks, B, ws, 3, error, stream, timer, mixed);
     if (g.touchingCount) {
         TimedScope scope(timer, "singular", stream);
         singularKernel<<<dim3(g.touchingCount, B), 128, 0, stream>>>(g.panels, g.T, g.touching, ks, gaussSingular,
@@ -726,8 +888,12 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
     }
     if (g.nearPairCount) {
         TimedScope scope(timer, "near", stream);
-        nearKernel<<<dim3(g.nearPairCount, B), 128, 0, stream>>>(g.panels, g.T, g.nearPairs, g.patches, ks,
-                                                                 ws.records, error);
+        if (mixed)
+            nearKernel<true><<<dim3(g.nearPairCount, B), 128, 0, stream>>>(g.panels, g.T, g.nearPairs, g.patches, ks,
+                                                                           ws.records, error);
+        else
+            nearKernel<false><<<dim3(g.nearPairCount, B), 128, 0, stream>>>(g.panels, g.T, g.nearPairs, g.patches,
+                                                                            ks, ws.records, error);
         cudaCheck(cudaGetLastError(), "near assembly launch");
     }
     {
@@ -743,12 +909,15 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         cudaCheck(cudaGetLastError(), "test gather launch");
     }
     {
-        TimedScope scope(timer, "rhs", stream);
+        TimedScope scope(timer, "rhs_panel", stream);
         rhsPanelKernel<<<dim3((g.T + 127) / 128, E, B), 128, 0, stream>>>(ws.records, flux, g.T, E, ws.panelRhs);
+    }
+    {
+        TimedScope scope(timer, "rhs_vertex", stream);
         rhsVertexKernel<<<dim3((g.N + 127) / 128, E, B), 128, 0, stream>>>(ws.panelRhs, g.incOffsets, g.incPanel,
                                                                            g.incLocal, g.rowScale, g.T, g.N, E, rhs);
-        cudaCheck(cudaGetLastError(), "rhs gather launch");
     }
+    cudaCheck(cudaGetLastError(), "rhs gather launch");
 }
 
 }  // namespace hsb

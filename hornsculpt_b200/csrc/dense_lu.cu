@@ -1,10 +1,11 @@
-// Batched dense complex FP64 LU with partial pivoting, triangular solves and
-// the FP64 refinement residual (cuda_solver.cu:1485-1581, plain form: the
-// factor is FP64 instead of the reference's FP32 cuSOLVER getrf/getrs).
+// Batched dense complex LU with partial pivoting, triangular solves and the
+// FP64 refinement residual (cuda_solver.cu:1485-1581). The plain form
+// factors in FP64; the mixed form factors an FP32 copy and refines in FP64
+// (the reference factors in FP32 with cuSOLVER getrf/getrs).
 //
-// Matrices are column-major N x N complex (interleaved doubles), one per
-// frequency of the batch (blockIdx.y / blockIdx.z). Right-looking blocked
-// LU with panel width 32: a single-CTA panel factorisation per matrix, row
+// Matrices are column-major N x N complex (interleaved reals), one per
+// frequency of the batch (blockIdx.y / blockIdx.z). Right-looking blocked LU
+// with panel width 32: a single-CTA panel factorisation per matrix, row
 // interchanges outside the panel, a unit-lower triangular solve for the U
 // block row and a shared-memory tiled complex GEMM for the trailing update.
 #include "device_types.cuh"
@@ -23,37 +24,58 @@ void check(cudaError_t e, const char *what) {
         throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-__device__ __forceinline__ double2 ld2(const double *p) { return *reinterpret_cast<const double2 *>(p); }
-__device__ __forceinline__ void st2(double *p, double2 v) { *reinterpret_cast<double2 *>(p) = v; }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// complex element type of a real type
+template <class R> struct Cx;
+template <> struct Cx<double> {
+    using type = double2;
+};
+template <> struct Cx<float> {
+    using type = float2;
+};
+template <class R> using C2 = typename Cx<R>::type;
+template <class R> __device__ __forceinline__ C2<R> mk(R x, R y) {
+    C2<R> v;
+    v.x = x;
+    v.y = y;
+    return v;
+}
+template <class R> __device__ __forceinline__ C2<R> ld2(const R *p) { return *reinterpret_cast<const C2<R> *>(p); }
+template <class R> __device__ __forceinline__ void st2(R *p, C2<R> v) { *reinterpret_cast<C2<R> *>(p) = v; }
+template <class R> __device__ __forceinline__ C2<R> cmul(C2<R> a, C2<R> b) {
+    return mk<R>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// v -= a * b
+template <class R> __device__ __forceinline__ void csub(C2<R> &v, C2<R> a, C2<R> b) {
+    v.x -= a.x * b.x - a.y * b.y;
+    v.y -= a.x * b.y + a.y * b.x;
 }
 
 // Panel factorisation of columns [k0, k0+jb) over rows [k0, N) of one matrix.
-__global__ void __launch_bounds__(512) panelKernel(double *LU, uint32_t N, uint32_t k0, uint32_t jb, int *pivots,
+template <class R>
+__global__ void __launch_bounds__(512) panelKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb, int *pivots,
                                                    int *info) {
-    double *M = LU + size_t(blockIdx.x) * N * N * 2;
+    R *M = LU + size_t(blockIdx.x) * N * N * 2;
     int *piv = pivots + size_t(blockIdx.x) * N;
-    __shared__ double sVal[16];
+    __shared__ R sVal[16];
     __shared__ int sIdx[16];
-    __shared__ double2 sRow[kPanel];
+    __shared__ C2<R> sRow[kPanel];
     __shared__ int sPivot;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     for (uint32_t j = 0; j < jb; ++j) {
         const uint32_t c = k0 + j;
         // argmax |re|+|im| over rows [c, N), first index on ties
-        double best = -1;
+        R best = -1;
         int bestRow = int(c);
         for (uint32_t i = c + threadIdx.x; i < N; i += blockDim.x) {
-            const double2 v = ld2(M + 2 * (size_t(c) * N + i));
-            const double a = fabs(v.x) + fabs(v.y);
+            const C2<R> v = ld2(M + 2 * (size_t(c) * N + i));
+            const R a = fabs(v.x) + fabs(v.y);
             if (a > best) {
                 best = a;
                 bestRow = int(i);
             }
         }
         for (int off = 16; off > 0; off >>= 1) {
-            const double ob = __shfl_down_sync(0xffffffffu, best, off);
+            const R ob = __shfl_down_sync(0xffffffffu, best, off);
             const int oi = __shfl_down_sync(0xffffffffu, bestRow, off);
             if (ob > best || (ob == best && oi < bestRow)) {
                 best = ob;
@@ -66,7 +88,7 @@ __global__ void __launch_bounds__(512) panelKernel(double *LU, uint32_t N, uint3
         }
         __syncthreads();
         if (threadIdx.x == 0) {
-            double b = sVal[0];
+            R b = sVal[0];
             int bi = sIdx[0];
             for (int w = 1; w < warps; ++w)
                 if (sVal[w] > b || (sVal[w] == b && sIdx[w] < bi)) {
@@ -81,9 +103,9 @@ __global__ void __launch_bounds__(512) panelKernel(double *LU, uint32_t N, uint3
         __syncthreads();
         const int p = sPivot;
         if (threadIdx.x < jb && p != int(c)) {
-            double *a = M + 2 * (size_t(k0 + threadIdx.x) * N + c);
-            double *b = M + 2 * (size_t(k0 + threadIdx.x) * N + p);
-            const double2 va = ld2(a), vb = ld2(b);
+            R *a = M + 2 * (size_t(k0 + threadIdx.x) * N + c);
+            R *b = M + 2 * (size_t(k0 + threadIdx.x) * N + p);
+            const C2<R> va = ld2(a), vb = ld2(b);
             st2(a, vb);
             st2(b, va);
         }
@@ -91,19 +113,17 @@ __global__ void __launch_bounds__(512) panelKernel(double *LU, uint32_t N, uint3
         if (threadIdx.x < jb)
             sRow[threadIdx.x] = ld2(M + 2 * (size_t(k0 + threadIdx.x) * N + c));
         __syncthreads();
-        const double2 d = sRow[j];
-        const double den = d.x * d.x + d.y * d.y;
-        const double2 inv = den > 0 ? make_double2(d.x / den, -d.y / den) : make_double2(0, 0);
+        const C2<R> d = sRow[j];
+        const R den = d.x * d.x + d.y * d.y;
+        const C2<R> inv = den > 0 ? mk<R>(d.x / den, -d.y / den) : mk<R>(0, 0);
         for (uint32_t i = c + 1 + threadIdx.x; i < N; i += blockDim.x) {
-            double *col = M + 2 * (size_t(c) * N + i);
-            const double2 l = cmul(ld2(col), inv);
+            R *col = M + 2 * (size_t(c) * N + i);
+            const C2<R> l = cmul<R>(ld2(col), inv);
             st2(col, l);
             for (uint32_t q = j + 1; q < jb; ++q) {
-                double *e = M + 2 * (size_t(k0 + q) * N + i);
-                const double2 u = sRow[q];
-                double2 v = ld2(e);
-                v.x -= l.x * u.x - l.y * u.y;
-                v.y -= l.x * u.y + l.y * u.x;
+                R *e = M + 2 * (size_t(k0 + q) * N + i);
+                C2<R> v = ld2(e);
+                csub<R>(v, l, sRow[q]);
                 st2(e, v);
             }
         }
@@ -112,16 +132,16 @@ __global__ void __launch_bounds__(512) panelKernel(double *LU, uint32_t N, uint3
 }
 
 // Row interchanges of the panel applied to columns outside it.
-__global__ void swapKernel(double *LU, uint32_t N, uint32_t k0, uint32_t jb, const int *pivots) {
+template <class R> __global__ void swapKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb, const int *pivots) {
     const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= N || (col >= k0 && col < k0 + jb))
         return;
-    double *M = LU + size_t(blockIdx.y) * N * N * 2 + 2 * size_t(col) * N;
+    R *M = LU + size_t(blockIdx.y) * N * N * 2 + 2 * size_t(col) * N;
     const int *piv = pivots + size_t(blockIdx.y) * N;
     for (uint32_t c = k0; c < k0 + jb; ++c) {
         const int p = piv[c];
         if (p != int(c)) {
-            const double2 a = ld2(M + 2 * c), b = ld2(M + 2 * p);
+            const C2<R> a = ld2(M + 2 * c), b = ld2(M + 2 * p);
             st2(M + 2 * c, b);
             st2(M + 2 * p, a);
         }
@@ -129,9 +149,9 @@ __global__ void swapKernel(double *LU, uint32_t N, uint32_t k0, uint32_t jb, con
 }
 
 // U12 = L11^{-1} A12 (unit lower L11 of the panel), one thread per column.
-__global__ void trsmKernel(double *LU, uint32_t N, uint32_t k0, uint32_t jb) {
-    __shared__ double2 L[kPanel][kPanel];
-    double *M = LU + size_t(blockIdx.y) * N * N * 2;
+template <class R> __global__ void trsmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb) {
+    __shared__ C2<R> L[kPanel][kPanel];
+    R *M = LU + size_t(blockIdx.y) * N * N * 2;
     for (uint32_t e = threadIdx.x; e < jb * jb; e += blockDim.x) {
         const uint32_t r = e % jb, c = e / jb;
         L[r][c] = ld2(M + 2 * (size_t(k0 + c) * N + k0 + r));
@@ -140,43 +160,40 @@ __global__ void trsmKernel(double *LU, uint32_t N, uint32_t k0, uint32_t jb) {
     const uint32_t col = k0 + jb + blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= N)
         return;
-    double *C = M + 2 * size_t(col) * N;
-    double2 x[kPanel];
+    R *C = M + 2 * size_t(col) * N;
+    C2<R> x[kPanel];
     for (uint32_t i = 0; i < jb; ++i) {
-        double2 v = ld2(C + 2 * (k0 + i));
-        for (uint32_t m = 0; m < i; ++m) {
-            const double2 l = L[i][m];
-            v.x -= l.x * x[m].x - l.y * x[m].y;
-            v.y -= l.x * x[m].y + l.y * x[m].x;
-        }
+        C2<R> v = ld2(C + 2 * (k0 + i));
+        for (uint32_t m = 0; m < i; ++m)
+            csub<R>(v, L[i][m], x[m]);
         x[i] = v;
         st2(C + 2 * (k0 + i), v);
     }
 }
 
 // A22 -= L21 * U12 with 64x64 output tiles, K = jb <= 32.
-__global__ void __launch_bounds__(256) gemmKernel(double *LU, uint32_t N, uint32_t k0, uint32_t jb) {
-    extern __shared__ double2 smem[];
-    double2 *sA = smem;                 // [kPanel][64]  L21 tile, k-major
-    double2 *sB = smem + kPanel * 64;   // [kPanel][64]  U12 tile, k-major
-    double *M = LU + size_t(blockIdx.z) * N * N * 2;
+template <class R> __global__ void __launch_bounds__(256) gemmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb) {
+    extern __shared__ __align__(16) unsigned char rawSmem[];
+    C2<R> *sA = reinterpret_cast<C2<R> *>(rawSmem);  // [kPanel][64]  L21 tile, k-major
+    C2<R> *sB = sA + kPanel * 64;                      // [kPanel][64]  U12 tile, k-major
+    R *M = LU + size_t(blockIdx.z) * N * N * 2;
     const uint32_t r0 = k0 + jb + blockIdx.x * 64, c0 = k0 + jb + blockIdx.y * 64;
     for (uint32_t e = threadIdx.x; e < jb * 64; e += blockDim.x) {
         const uint32_t kk = e / 64, x = e % 64;
         const uint32_t r = r0 + x, c = c0 + x;
-        sA[kk * 64 + x] = r < N ? ld2(M + 2 * (size_t(k0 + kk) * N + r)) : make_double2(0, 0);
-        sB[kk * 64 + x] = c < N ? ld2(M + 2 * (size_t(c) * N + k0 + kk)) : make_double2(0, 0);
+        sA[kk * 64 + x] = r < N ? ld2(M + 2 * (size_t(k0 + kk) * N + r)) : mk<R>(0, 0);
+        sB[kk * 64 + x] = c < N ? ld2(M + 2 * (size_t(c) * N + k0 + kk)) : mk<R>(0, 0);
     }
     __syncthreads();
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    double2 acc[4][4];
+    C2<R> acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-            acc[i][j] = make_double2(0, 0);
+            acc[i][j] = mk<R>(0, 0);
     for (uint32_t kk = 0; kk < jb; ++kk) {
-        double2 a[4], b[4];
+        C2<R> a[4], b[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             a[i] = sA[kk * 64 + tx + 16 * i];
@@ -200,8 +217,8 @@ __global__ void __launch_bounds__(256) gemmKernel(double *LU, uint32_t N, uint32
             const uint32_t r = r0 + tx + 16 * i;
             if (r >= N)
                 continue;
-            double *e = M + 2 * (size_t(c) * N + r);
-            double2 v = ld2(e);
+            R *e = M + 2 * (size_t(c) * N + r);
+            C2<R> v = ld2(e);
             v.x -= acc[i][j].x;
             v.y -= acc[i][j].y;
             st2(e, v);
@@ -210,14 +227,15 @@ __global__ void __launch_bounds__(256) gemmKernel(double *LU, uint32_t N, uint32
 }
 
 // Forward / back substitution of one right-hand side per CTA, with the
-// vector staged in shared memory (N <= 13000).
-__global__ void __launch_bounds__(256) solveKernel(const double *LU, const int *pivots, uint32_t N, uint32_t E,
-                                                   double *X) {
-    extern __shared__ double2 x[];
+// vector staged in shared memory.
+template <class R>
+__global__ void __launch_bounds__(256) solveKernel(const R *LU, const int *pivots, uint32_t N, uint32_t E, R *X) {
+    extern __shared__ __align__(16) unsigned char rawSmem[];
+    C2<R> *x = reinterpret_cast<C2<R> *>(rawSmem);
     const uint32_t e = blockIdx.x, f = blockIdx.y;
-    const double *M = LU + size_t(f) * N * N * 2;
+    const R *M = LU + size_t(f) * N * N * 2;
     const int *piv = pivots + size_t(f) * N;
-    double *out = X + (size_t(f) * E + e) * N * 2;
+    R *out = X + (size_t(f) * E + e) * N * 2;
     for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
         x[i] = ld2(out + 2 * i);
     __syncthreads();
@@ -225,7 +243,7 @@ __global__ void __launch_bounds__(256) solveKernel(const double *LU, const int *
         for (uint32_t c = 0; c < N; ++c) {
             const int p = piv[c];
             if (p != int(c)) {
-                const double2 t = x[c];
+                const C2<R> t = x[c];
                 x[c] = x[p];
                 x[p] = t;
             }
@@ -235,27 +253,20 @@ __global__ void __launch_bounds__(256) solveKernel(const double *LU, const int *
     for (uint32_t k = 0; k < N; k += 32) {
         const uint32_t kb = min(32u, N - k);
         if (warp == 0) {
-            double2 mine = lane < int(kb) ? x[k + lane] : make_double2(0, 0);
+            C2<R> mine = lane < int(kb) ? x[k + lane] : mk<R>(0, 0);
             for (uint32_t m = 0; m < kb; ++m) {
-                const double2 xm = make_double2(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
-                if (lane > int(m) && lane < int(kb)) {
-                    const double2 l = ld2(M + 2 * (size_t(k + m) * N + k + lane));
-                    mine.x -= l.x * xm.x - l.y * xm.y;
-                    mine.y -= l.x * xm.y + l.y * xm.x;
-                }
+                const C2<R> xm = mk<R>(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
+                if (lane > int(m) && lane < int(kb))
+                    csub<R>(mine, ld2(M + 2 * (size_t(k + m) * N + k + lane)), xm);
             }
             if (lane < int(kb))
                 x[k + lane] = mine;
         }
         __syncthreads();
         for (uint32_t i = k + kb + threadIdx.x; i < N; i += blockDim.x) {
-            double2 v = x[i];
-            for (uint32_t m = 0; m < kb; ++m) {
-                const double2 l = ld2(M + 2 * (size_t(k + m) * N + i));
-                const double2 xm = x[k + m];
-                v.x -= l.x * xm.x - l.y * xm.y;
-                v.y -= l.x * xm.y + l.y * xm.x;
-            }
+            C2<R> v = x[i];
+            for (uint32_t m = 0; m < kb; ++m)
+                csub<R>(v, ld2(M + 2 * (size_t(k + m) * N + i)), x[k + m]);
             x[i] = v;
         }
         __syncthreads();
@@ -264,32 +275,25 @@ __global__ void __launch_bounds__(256) solveKernel(const double *LU, const int *
     for (uint32_t bi = blocks; bi-- > 0;) {
         const uint32_t k = bi * 32, kb = min(32u, N - k);
         if (warp == 0) {
-            double2 mine = lane < int(kb) ? x[k + lane] : make_double2(0, 0);
+            C2<R> mine = lane < int(kb) ? x[k + lane] : mk<R>(0, 0);
             for (int m = int(kb) - 1; m >= 0; --m) {
                 if (lane == m) {
-                    const double2 d = ld2(M + 2 * (size_t(k + m) * N + k + m));
-                    const double den = d.x * d.x + d.y * d.y;
-                    mine = make_double2((mine.x * d.x + mine.y * d.y) / den, (mine.y * d.x - mine.x * d.y) / den);
+                    const C2<R> d = ld2(M + 2 * (size_t(k + m) * N + k + m));
+                    const R den = d.x * d.x + d.y * d.y;
+                    mine = mk<R>((mine.x * d.x + mine.y * d.y) / den, (mine.y * d.x - mine.x * d.y) / den);
                 }
-                const double2 xm = make_double2(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
-                if (lane < m) {
-                    const double2 u = ld2(M + 2 * (size_t(k + m) * N + k + lane));
-                    mine.x -= u.x * xm.x - u.y * xm.y;
-                    mine.y -= u.x * xm.y + u.y * xm.x;
-                }
+                const C2<R> xm = mk<R>(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
+                if (lane < m)
+                    csub<R>(mine, ld2(M + 2 * (size_t(k + m) * N + k + lane)), xm);
             }
             if (lane < int(kb))
                 x[k + lane] = mine;
         }
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < k; i += blockDim.x) {
-            double2 v = x[i];
-            for (uint32_t m = 0; m < kb; ++m) {
-                const double2 u = ld2(M + 2 * (size_t(k + m) * N + i));
-                const double2 xm = x[k + m];
-                v.x -= u.x * xm.x - u.y * xm.y;
-                v.y -= u.x * xm.y + u.y * xm.x;
-            }
+            C2<R> v = x[i];
+            for (uint32_t m = 0; m < kb; ++m)
+                csub<R>(v, ld2(M + 2 * (size_t(k + m) * N + i)), x[k + m]);
             x[i] = v;
         }
         __syncthreads();
@@ -298,7 +302,7 @@ __global__ void __launch_bounds__(256) solveKernel(const double *LU, const int *
         st2(out + 2 * i, x[i]);
 }
 
-// r = b - A x per row (FP64), plus mass-scaled squares for the norms.
+// r = b - A x per row (FP64 accumulation), plus mass-scaled squares for the norms.
 __global__ void residualKernel(const double *A, const double *b, const double *x, const double *mass, uint32_t N,
                                uint32_t E, double *correction, double *squares) {
     const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -318,7 +322,7 @@ __global__ void residualKernel(const double *A, const double *b, const double *x
     const double2 bb = ld2(b + 2 * idx);
     re = bb.x - re;
     im = bb.y - im;
-    st2(correction + 2 * idx, make_double2(re, im));
+    st2(correction + 2 * idx, mk<double>(re, im));
     const double s = mass[a];
     squares[2 * idx] = (re * s) * (re * s) + (im * s) * (im * s);
     squares[2 * idx + 1] = (bb.x * s) * (bb.x * s) + (bb.y * s) * (bb.y * s);
@@ -354,16 +358,24 @@ __global__ void addKernel(double *x, const double *c, size_t count) {
     if (i < count)
         x[i] += c[i];
 }
+__global__ void addFromFloatKernel(double *x, const float *c, size_t count) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count)
+        x[i] += double(c[i]);
+}
+__global__ void toFloatKernel(const double *in, float *out, size_t count) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count)
+        out[i] = float(in[i]);
+}
 
-}  // namespace
-
-void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
-                   KernelTimer *timer) {
+template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
+                               KernelTimer *timer) {
     check(cudaMemsetAsync(info, 0, sizeof(int), stream), "LU info reset");
-    const size_t gemmSmem = 2 * kPanel * 64 * sizeof(double2);
+    const size_t gemmSmem = 2 * kPanel * 64 * sizeof(C2<R>);
     static bool attr = false;
     if (!attr) {
-        check(cudaFuncSetAttribute(gemmKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gemmSmem)),
+        check(cudaFuncSetAttribute(gemmKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gemmSmem)),
               "gemm smem attribute");
         attr = true;
     }
@@ -371,53 +383,85 @@ void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, c
         const uint32_t jb = min(uint32_t(kPanel), N - k0);
         {
             TimedScope s(timer, "lu_panel", stream);
-            panelKernel<<<B, 512, 0, stream>>>(LU, N, k0, jb, pivots, info);
+            panelKernel<R><<<B, 512, 0, stream>>>(LU, N, k0, jb, pivots, info);
         }
         {
             TimedScope s(timer, "lu_swap", stream);
-            swapKernel<<<dim3((N + 127) / 128, B), 128, 0, stream>>>(LU, N, k0, jb, pivots);
+            swapKernel<R><<<dim3((N + 127) / 128, B), 128, 0, stream>>>(LU, N, k0, jb, pivots);
         }
         const uint32_t rest = N - k0 - jb;
         if (rest) {
             {
                 TimedScope s(timer, "lu_trsm", stream);
-                trsmKernel<<<dim3((rest + 127) / 128, B), 128, 0, stream>>>(LU, N, k0, jb);
+                trsmKernel<R><<<dim3((rest + 127) / 128, B), 128, 0, stream>>>(LU, N, k0, jb);
             }
             TimedScope s(timer, "lu_gemm", stream);
-            gemmKernel<<<dim3((rest + 63) / 64, (rest + 63) / 64, B), 256, gemmSmem, stream>>>(LU, N, k0, jb);
+            gemmKernel<R><<<dim3((rest + 63) / 64, (rest + 63) / 64, B), 256, gemmSmem, stream>>>(LU, N, k0, jb);
         }
         check(cudaGetLastError(), "LU launch");
     }
 }
 
-void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
-                  cudaStream_t stream, KernelTimer *timer) {
-    const size_t smem = size_t(N) * sizeof(double2);
+template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, R *x,
+                              cudaStream_t stream, KernelTimer *timer) {
+    const size_t smem = size_t(N) * sizeof(C2<R>);
     if (smem > 227 * 1024)
         throw std::runtime_error("Dense solve vector exceeds shared memory (N too large for the dense form).");
     static size_t attr = 0;
     if (smem > 48 * 1024 && smem > attr) {
-        check(cudaFuncSetAttribute(solveKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+        check(cudaFuncSetAttribute(solveKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
               "solve smem attribute");
         attr = smem;
     }
     TimedScope s(timer, "lu_solve", stream);
-    solveKernel<<<dim3(E, B), 256, smem, stream>>>(LU, pivots, N, E, x);
+    solveKernel<R><<<dim3(E, B), 256, smem, stream>>>(LU, pivots, N, E, x);
     check(cudaGetLastError(), "triangular solve launch");
+}
+
+}  // namespace
+
+void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
+                   KernelTimer *timer) {
+    factor<double>(LU, N, B, pivots, info, stream, timer);
+}
+void luFactorBatch(float *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
+                   KernelTimer *timer) {
+    factor<float>(LU, N, B, pivots, info, stream, timer);
+}
+void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
+                  cudaStream_t stream, KernelTimer *timer) {
+    solve<double>(LU, pivots, N, B, E, x, stream, timer);
+}
+void luSolveBatch(const float *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, float *x,
+                  cudaStream_t stream, KernelTimer *timer) {
+    solve<float>(LU, pivots, N, B, E, x, stream, timer);
 }
 
 void residualBatch(const double *A, const double *b, const double *x, const double *mass, uint32_t N, uint32_t B,
                    uint32_t E, double *correction, double *norms, cudaStream_t stream, KernelTimer *timer) {
-    TimedScope s(timer, "residual", stream);
     double *squares = norms + 2 * size_t(B) * E;  // scratch after the norms
-    residualKernel<<<dim3((N + 127) / 128, E, B), 128, 0, stream>>>(A, b, x, mass, N, E, correction, squares);
-    normKernel<<<unsigned(B * E), 256, 0, stream>>>(squares, N, norms);
+    {
+        TimedScope s(timer, "residual", stream);
+        residualKernel<<<dim3((N + 127) / 128, E, B), 128, 0, stream>>>(A, b, x, mass, N, E, correction, squares);
+    }
+    {
+        TimedScope s(timer, "residual_norm", stream);
+        normKernel<<<unsigned(B * E), 256, 0, stream>>>(squares, N, norms);
+    }
     check(cudaGetLastError(), "residual launch");
 }
 
 void addCorrectionBatch(double *x, const double *correction, size_t count, cudaStream_t stream) {
     addKernel<<<unsigned((count + 255) / 256), 256, 0, stream>>>(x, correction, count);
     check(cudaGetLastError(), "refinement update launch");
+}
+void addCorrectionBatch(double *x, const float *correction, size_t count, cudaStream_t stream) {
+    addFromFloatKernel<<<unsigned((count + 255) / 256), 256, 0, stream>>>(x, correction, count);
+    check(cudaGetLastError(), "refinement update launch");
+}
+void roundToFloat(const double *in, float *out, size_t count, cudaStream_t stream) {
+    toFloatKernel<<<unsigned((count + 255) / 256), 256, 0, stream>>>(in, out, count);
+    check(cudaGetLastError(), "FP32 rounding launch");
 }
 
 size_t luWorkspaceBytes(uint32_t N, uint32_t B) { return size_t(B) * N * sizeof(int); }

@@ -83,21 +83,29 @@ struct AssemblyWorkspace {
     size_t binCapacity;
 };
 size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B);
+// mixed: regular and near pairs with FP32 kernel arithmetic (displacement and
+// phase k*r in FP64), touching pairs in FP64 either way.
 void assembleBatch(const AssemblyGeometry &geo, const double *ks, const double *gaussSingular, const double *flux,
                    uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
-                   cudaStream_t stream, class KernelTimer *timer);
+                   cudaStream_t stream, class KernelTimer *timer, bool mixed = false);
 
 // Batched dense LU (partial pivoting) and solves, complex FP64 column-major.
 size_t luWorkspaceBytes(uint32_t N, uint32_t B);
 void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                    class KernelTimer *timer);
+void luFactorBatch(float *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
+                   class KernelTimer *timer);
 void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
+                  cudaStream_t stream, class KernelTimer *timer);
+void luSolveBatch(const float *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, float *x,
                   cudaStream_t stream, class KernelTimer *timer);
 // r = b - A x (FP64); writes the correction rhs into `correction` and the
 // mass-scaled residual norm and rhs norm per (batch, excitation) into norms[2].
 void residualBatch(const double *A, const double *b, const double *x, const double *mass, uint32_t N, uint32_t B,
                    uint32_t E, double *correction, double *norms, cudaStream_t stream, class KernelTimer *timer);
 void addCorrectionBatch(double *x, const double *correction, size_t count, cudaStream_t stream);
+void addCorrectionBatch(double *x, const float *correction, size_t count, cudaStream_t stream);
+void roundToFloat(const double *in, float *out, size_t count, cudaStream_t stream);
 
 // Observer fields of one rule degree for every (batch, excitation, observer).
 struct FieldRequest {

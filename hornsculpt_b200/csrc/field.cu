@@ -267,9 +267,15 @@ void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double 
     const size_t outputs = size_t(req.B) * req.E * req.O;
     if (!outputs)
         return;
-    TimedScope s(timer, "field", stream);
-    fieldKernel<<<unsigned(outputs * tiles), 128, 0, stream>>>(req, ks, pressure, flux, batchDegree, partials, error);
-    finishKernel<<<unsigned((outputs + 127) / 128), 128, 0, stream>>>(partials, tiles, outputs, out, error);
+    {
+        TimedScope s(timer, "field", stream);
+        fieldKernel<<<unsigned(outputs * tiles), 128, 0, stream>>>(req, ks, pressure, flux, batchDegree, partials,
+                                                                  error);
+    }
+    {
+        TimedScope s(timer, "field_finish", stream);
+        finishKernel<<<unsigned((outputs + 127) / 128), 128, 0, stream>>>(partials, tiles, outputs, out, error);
+    }
     check(cudaGetLastError(), "field launch");
 }
 

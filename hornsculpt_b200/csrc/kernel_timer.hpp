@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <map>
 #include <string>
 #include <vector>
@@ -26,18 +27,19 @@ class KernelTimer {
         collect();
         totals_.clear();
     }
-    // Records a start event; the matching stop() closes the interval.
-    void start(const char *family, cudaStream_t stream) {
+    // Records a start event and returns its interval; stop() closes it.
+    size_t start(const char *family, cudaStream_t stream) {
         if (!enabled_)
-            return;
+            return SIZE_MAX;
         Pending p{family, event(), event()};
         cudaEventRecord(p.start, stream);
         pending_.push_back(p);
+        return pending_.size() - 1;
     }
-    void stop(cudaStream_t stream) {
-        if (!enabled_ || pending_.empty())
+    void stop(size_t interval, cudaStream_t stream) {
+        if (!enabled_ || interval >= pending_.size())
             return;
-        cudaEventRecord(pending_.back().stop, stream);
+        cudaEventRecord(pending_[interval].stop, stream);
     }
     // Synchronises on recorded events and folds them into per-family totals.
     void collect() {
@@ -84,14 +86,15 @@ class KernelTimer {
 struct TimedScope {
     TimedScope(KernelTimer *t, const char *family, cudaStream_t s) : timer(t), stream(s) {
         if (timer)
-            timer->start(family, stream);
+            interval = timer->start(family, stream);
     }
     ~TimedScope() {
         if (timer)
-            timer->stop(stream);
+            timer->stop(interval, stream);
     }
     KernelTimer *timer;
     cudaStream_t stream;
+    size_t interval = SIZE_MAX;
 };
 
 }  // namespace hsb

@@ -106,8 +106,8 @@ void validateRequest(const hs_request &r) {
         throw InvalidArgument("Invalid BEM medium, frequencies, excitation or Galerkin settings.");
     if (fmm)
         throw Unsupported("The fast-multipole acceleration is not part of this build; use the dense form.");
-    if (o.precision != HS_PRECISION_FP64)
-        throw Unsupported("Only the plain FP64 precision form is available in this build.");
+    if (o.precision != HS_PRECISION_FP64 && o.precision != HS_PRECISION_MIXED)
+        throw InvalidArgument("Invalid BEM precision form.");
     if (r.excitation_count > 1024 || r.observer_count > 100000)
         throw InvalidArgument("BEM request exceeds indexing limits.");
 }
@@ -318,11 +318,13 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O) {
     dPartials_.ensure(std::max<size_t>(fieldPartialsBytes(uint32_t(T), E, O, B), 16));
     dField_.ensure(std::max<size_t>(B * E * O * 16, 16));
     dDegrees_.ensure(B * 4);
+    dWork32_.ensure(B * E * N * 8);
     size_t bytes = 0;
     for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_, &dMass_,
                                   &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dRecords_, &dColumns_,
                                   &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
-                                  &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_})
+                                  &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_,
+                                  &dWork32_})
         bytes += b->bytes();
     peakBytes_ = std::max(peakBytes_, bytes);
 }
@@ -441,6 +443,9 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     double maxEdge = 0;
     for (const auto &p : space_.panels)
         maxEdge = std::max(maxEdge, p.maxEdge);
+    // Device span of the whole sweep (profiling on): from the first upload to
+    // the last result download, host-side control included.
+    const size_t span = timer_.start("solve_span", s);
     for (uint32_t f0 = 0; f0 < F; f0 += Bmax) {
         checkCancel();
         const uint32_t B = std::min(Bmax, F - f0);
@@ -457,8 +462,9 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         cuda(cudaMemcpyAsync(dFlux_.as<void>(), flux.data(), flux.size() * 16, cudaMemcpyHostToDevice, s), "flux upload");
         AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
                              dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
+        const bool mixed = o.precision == HS_PRECISION_MIXED;
         assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws, dA_.as<double>(),
-                      dRhs_.as<double>(), dError_.as<int>(), s, &timer_);
+                      dRhs_.as<double>(), dError_.as<int>(), s, &timer_, mixed);
         checkDeviceError("CUDA Galerkin assembly");
         if (timer_.enabled()) {
             std::vector<uint32_t> counts(size_t(B) * kBins);
@@ -476,11 +482,22 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         }
         const double assemblyMs = msSince(batchStart);
         checkCancel();
-        // LU of every matrix of the batch, then the initial solves.
+        // LU of every matrix of the batch (FP64, or an FP32 copy in the mixed
+        // form), then the initial solves.
         const auto factorStart = Clock::now();
-        cuda(cudaMemcpyAsync(dLU_.as<void>(), dA_.as<void>(), size_t(B) * N * N * 16, cudaMemcpyDeviceToDevice, s),
-             "factorization copy");
-        luFactorBatch(dLU_.as<double>(), N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_);
+        const size_t matrixReals = size_t(B) * N * N * 2, vectorReals = size_t(B) * E * N * 2;
+        float *LU32 = dLU_.as<float>(), *work32 = dWork32_.as<float>();
+        if (mixed) {
+            {
+                TimedScope scope(&timer_, "round_fp32", s);
+                roundToFloat(dA_.as<double>(), LU32, matrixReals, s);
+            }
+            luFactorBatch(LU32, N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_);
+        } else {
+            cuda(cudaMemcpyAsync(dLU_.as<void>(), dA_.as<void>(), matrixReals * 8, cudaMemcpyDeviceToDevice, s),
+                 "factorization copy");
+            luFactorBatch(dLU_.as<double>(), N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_);
+        }
         int info = 0;
         cuda(cudaMemcpyAsync(&info, dInfo_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, s), "LU info");
         cuda(cudaStreamSynchronize(s), "CUDA pivoted LU");
@@ -488,12 +505,26 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             throw NumericError("CUDA Burton-Miller factorization failed at pivot " + std::to_string(info));
         const double factorMs = msSince(factorStart);
         const auto triStart = Clock::now();
-        cuda(cudaMemcpyAsync(dX_.as<void>(), dRhs_.as<void>(), size_t(B) * E * N * 16, cudaMemcpyDeviceToDevice, s),
-             "rhs copy");
-        luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), s, &timer_);
+        if (mixed) {
+            {
+                TimedScope scope(&timer_, "round_fp32", s);
+                roundToFloat(dRhs_.as<double>(), work32, vectorReals, s);
+            }
+            luSolveBatch(LU32, dPivots_.as<int>(), N, B, E, work32, s, &timer_);
+            cuda(cudaMemsetAsync(dX_.as<void>(), 0, vectorReals * 8, s), "solution reset");
+            TimedScope scope(&timer_, "add_correction", s);
+            addCorrectionBatch(dX_.as<double>(), work32, vectorReals, s);
+        } else {
+            cuda(cudaMemcpyAsync(dX_.as<void>(), dRhs_.as<void>(), vectorReals * 8, cudaMemcpyDeviceToDevice, s),
+                 "rhs copy");
+            luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), s, &timer_);
+        }
         cuda(cudaStreamSynchronize(s), "CUDA multi-RHS solve");
         double triMs = msSince(triStart);
-        // FP64 refinement (cuda_solver.cu:1519-1581), per frequency.
+        // FP64 refinement (cuda_solver.cu:1519-1581), per frequency. The mixed
+        // form refines against the FP64 residual to min(tolerance, 1e-10).
+        const double target = mixed ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
+        const uint32_t maxSteps = mixed ? std::max<uint32_t>(o.maximum_refinement_steps, 10) : o.maximum_refinement_steps;
         const auto residualStart = Clock::now();
         std::vector<uint32_t> steps(B, 0);
         std::vector<double> relative(size_t(B) * E, 0);
@@ -516,11 +547,11 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                     relative[size_t(b) * E + e] = rel;
                     largest = std::max(largest, rel);
                 }
-                const bool need = largest > o.relative_residual_tolerance;
-                if (need && steps[b] >= o.maximum_refinement_steps) {
+                const bool need = largest > target;
+                if (need && steps[b] >= maxSteps) {
                     std::ostringstream msg;
                     msg << std::setprecision(9) << "Burton-Miller residual " << largest << " exceeds tolerance "
-                        << o.relative_residual_tolerance << " at " << r.frequencies[f0 + b] << " Hz after " << steps[b]
+                        << target << " at " << r.frequencies[f0 + b] << " Hz after " << steps[b]
                         << " refinement steps.";
                     throw NoConvergence(msg.str());
                 }
@@ -534,8 +565,19 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             if (!any)
                 break;
             const auto t0 = Clock::now();
-            luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dCorr_.as<double>(), s, &timer_);
-            addCorrectionBatch(dX_.as<double>(), dCorr_.as<double>(), size_t(B) * E * N * 2, s);
+            if (mixed) {
+                {
+                    TimedScope scope(&timer_, "round_fp32", s);
+                    roundToFloat(dCorr_.as<double>(), work32, vectorReals, s);
+                }
+                luSolveBatch(LU32, dPivots_.as<int>(), N, B, E, work32, s, &timer_);
+                TimedScope scope(&timer_, "add_correction", s);
+                addCorrectionBatch(dX_.as<double>(), work32, vectorReals, s);
+            } else {
+                luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dCorr_.as<double>(), s, &timer_);
+                TimedScope scope(&timer_, "add_correction", s);
+                addCorrectionBatch(dX_.as<double>(), dCorr_.as<double>(), vectorReals, s);
+            }
             cuda(cudaStreamSynchronize(s), "CUDA refinement solve");
             triMs += msSince(t0);
         }
@@ -686,6 +728,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             }
         }
     }
+    timer_.stop(span, s);
     result->peakDeviceBytes = peakBytes_;
     return result;
 }
@@ -706,7 +749,7 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
     AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
                          dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
     assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), 1, 1, ws, dA_.as<double>(),
-                  dRhs_.as<double>(), dError_.as<int>(), s, &timer_);
+                  dRhs_.as<double>(), dError_.as<int>(), s, &timer_, o.precision == HS_PRECISION_MIXED);
     checkDeviceError("CUDA Galerkin assembly");
     cuda(cudaMemcpyAsync(matrix, dA_.as<void>(), size_t(N) * N * 16, cudaMemcpyDeviceToHost, s), "matrix download");
     cuda(cudaMemcpyAsync(rhs, dRhs_.as<void>(), size_t(N) * 16, cudaMemcpyDeviceToHost, s), "rhs download");

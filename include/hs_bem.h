@@ -45,7 +45,9 @@ typedef enum hs_status {
 typedef enum hs_boundary { HS_WALL = 0, HS_DRIVEN = 1 } hs_boundary;   /* mesh.hpp:17 */
 typedef enum hs_acceleration { HS_DENSE = 0, HS_FAST_MULTIPOLE = 1 } hs_acceleration; /* bem.hpp:38 */
 typedef enum hs_precision {
-    HS_PRECISION_FP64 = 0 /* plain form: the reference method evaluated entirely in FP64 */
+    HS_PRECISION_FP64 = 0,  /* plain form: the reference method evaluated entirely in FP64 */
+    HS_PRECISION_MIXED = 1  /* FP32 regular/near samples (FP64 displacement and phase), FP64 touching
+                               pairs, FP32 LU, FP64 iterative refinement to min(tolerance, 1e-10) */
 } hs_precision;
 typedef enum hs_residency { HS_RESIDENCY_AUTOMATIC = 0, HS_RESIDENCY_DEVICE = 1, HS_RESIDENCY_MAPPED_HOST = 2 } hs_residency; /* bem.hpp:361-365 */
 

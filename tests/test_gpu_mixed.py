@@ -1,0 +1,54 @@
+"""Mixed-precision form (FP32 regular/near samples with FP64 displacement and
+phase, FP64 touching pairs, FP32 LU, FP64 refinement) against the FP64
+oracle and the plain FP64 form (needs a B200). Contract: relative surface
+pressure error <= 1e-5 and relative residual <= 1e-10."""
+import numpy as np
+import pytest
+
+import hornsculpt_b200 as hs
+from conftest import rel_l2
+from hornsculpt_b200 import meshes
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-5
+MIXED = hs.BemNumerics(precision="mixed")
+
+
+def test_mixed_assembly_against_oracle():
+    """Entry-wise error of the mixed-form matrix: FP32 sample arithmetic only
+    (a few 1e-7 of the largest entry), well inside the 1e-5 budget."""
+    mesh = meshes.octahedral_sphere(3)
+    rng = np.random.default_rng(3)
+    q = rng.standard_normal(mesh.triangle_count) + 1j * rng.standard_normal(mesh.triangle_count)
+    plan_k = 2 * np.pi * 1715 / 343
+    with hs.CudaBemSolver(mesh) as solver:
+        for f in (150.0, 1715.0):
+            k = 2 * np.pi * f / 343
+            A, b = solver.debug_assemble(MIXED, plan_k, k, q)
+            Ao, bo = O.assemble(mesh, O.Numerics.default(), plan_k, k, q)
+            assert np.max(np.abs(A - Ao)) <= 1e-6 * np.max(np.abs(Ao))
+            assert np.max(np.abs(b - bo)) <= 1e-6 * np.max(np.abs(bo))
+
+
+@pytest.mark.parametrize("make,freqs", [(lambda: meshes.octahedral_sphere(3), [100.0, 500.0, 1000.0, 1715.0]),
+                                        (lambda: meshes.icosphere(3), list(np.geomspace(100, 5000, 32)))],
+                         ids=["sphere512", "c1_sweep"])
+def test_mixed_solve_matches_plain_form(make, freqs):
+    mesh = make()
+    obs = [(0, 0, .3), (1, 0, 0), (0, 0, 3)]
+    exc = [hs.BemExcitation("unit", [hs.FaceVelocity(1, 1.0)])]
+    with hs.CudaBemSolver(mesh) as solver:
+        plain = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc, observers=obs))
+        mixed = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc, observers=obs, numerics=MIXED))
+    v = mesh.vertices[mesh.triangles]
+    area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+    for fp, fm in zip(plain.frequencies, mixed.frequencies):
+        p, m = fp.excitations[0], fm.excitations[0]
+        # area-weighted relative L2 of DP0 surface pressure (tests/bem_small_mesh_parity_tests.cpp:60-76)
+        err = np.sqrt((area * np.abs(m.boundary.surface_pressure - p.boundary.surface_pressure) ** 2).sum() /
+                      (area * np.abs(p.boundary.surface_pressure) ** 2).sum())
+        assert err <= MIXED_TOL
+        assert m.boundary_residual <= 1e-10
+        assert rel_l2(m.observer_pressure, p.observer_pressure) <= MIXED_TOL
