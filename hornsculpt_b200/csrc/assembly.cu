@@ -231,7 +231,7 @@ __device__ __forceinline__ void mixedValues(double dx, double dy, double dz, flo
     double y = double(rinv);
     y = y * (1.5 - 0.5 * r2d * y * y);
     const double ph = k * (r2d * y);
-    const double turns = rint(ph * kInvTwoPi);
+    const double turns = (ph * kInvTwoPi + 6755399441055744.0) - 6755399441055744.0;  // round to nearest
     const double th = fma(-turns, kTwoPiLo, fma(-turns, kTwoPiHi, ph));
     float sn, cs;
     sincosf(float(th), &sn, &cs);
@@ -252,15 +252,23 @@ __device__ __forceinline__ void mixedValues(double dx, double dy, double dz, flo
 
 // Regular pairs in the mixed form: one unordered pair per thread, NP x NP
 // samples, trial bases contracted per test point (FP32), no shared memory.
+// The displacement used for amplitudes and normal projections is FP32
+// (test point converted once, trial point formed in FP32: relative error
+// ~eps_fp32, as for the reference's mixed sample); pairs whose k*r can
+// exceed 1 also form the FP64 displacement for the phase.
+__constant__ float cRuleF[kRulePoints * 4];
+
 template <int NP>
-__global__ void __launch_bounds__(256, 2) regularMixedKernel(const DPanel *__restrict__ panels, uint32_t T,
-                                                          const double *__restrict__ ks,
-                                                          const uint2 *__restrict__ bins,
-                                                          const uint32_t *__restrict__ binCounts, size_t binCapacity,
-                                                          int bin, double *__restrict__ records, int *error) {
+__global__ void __launch_bounds__(256, 2) regularMixedKernel(const DPanel *__restrict__ panels, const Bounds *__restrict__ bounds,
+                                                             uint32_t T, const double *__restrict__ ks,
+                                                             const uint2 *__restrict__ bins,
+                                                             const uint32_t *__restrict__ binCounts, size_t binCapacity,
+                                                             int bin, double *__restrict__ records, int *error) {
     constexpr int RO = ruleOffset<NP>();
+    constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52: adding and subtracting rounds to an integer
     const int f = blockIdx.y;
     const double k = ks[f], invk = 1.0 / k;
+    const float kf = float(k);
     const uint32_t count = binCounts[f * kBins + bin];
     const uint2 *list = bins + (size_t(f) * kBins + bin) * binCapacity;
     double *rec = records + size_t(f) * T * T * kRecordDoubles;
@@ -268,10 +276,16 @@ __global__ void __launch_bounds__(256, 2) regularMixedKernel(const DPanel *__res
         const uint2 pr = list[p];
         const DPanel &A = panels[pr.x];
         const DPanel &S = panels[pr.y];
+        const Bounds &ba = bounds[pr.x], &bb = bounds[pr.y];
+        // k times the largest point distance of the pair, from the enclosing balls
+        const double cx = ba.center.x - bb.center.x, cy = ba.center.y - bb.center.y, cz = ba.center.z - bb.center.z;
+        const bool exactPhase = k * (sqrt(cx * cx + cy * cy + cz * cz) + ba.radius + bb.radius) > 1.0;
         const double d0 = A.v0[0] - S.v0[0], d1 = A.v0[1] - S.v0[1], d2 = A.v0[2] - S.v0[2];
         const float w4 = float(4.0 * A.area * S.area * kInvFourPi);
         const float ns[3] = {float(S.n[0]), float(S.n[1]), float(S.n[2])};
         const float nt[3] = {float(A.n[0]), float(A.n[1]), float(A.n[2])};
+        const float se1[3] = {float(S.e1[0]), float(S.e1[1]), float(S.e1[2])};
+        const float se2[3] = {float(S.e2[0]), float(S.e2[1]), float(S.e2[2])};
         float M[54];
 #pragma unroll
         for (int c = 0; c < 54; ++c)
@@ -281,19 +295,44 @@ __global__ void __launch_bounds__(256, 2) regularMixedKernel(const DPanel *__res
             const double bx1 = cRule[4 * (RO + x) + 1], bx2 = cRule[4 * (RO + x) + 2];
             const double D0 = d0 + (A.e1[0] * bx1 + A.e2[0] * bx2), D1 = d1 + (A.e1[1] * bx1 + A.e2[1] * bx2),
                          D2 = d2 + (A.e1[2] * bx1 + A.e2[2] * bx2);
-            const float wx = float(cRule[4 * (RO + x) + 3]) * w4;
+            const float Df[3] = {float(D0), float(D1), float(D2)};
+            const float wx = cRuleF[4 * (RO + x) + 3] * w4;
             float Sv[18];
 #pragma unroll
             for (int c = 0; c < 18; ++c)
                 Sv[c] = 0.f;
 #pragma unroll 2
             for (int y = 0; y < NP; ++y) {
-                const double b1 = cRule[4 * (RO + y) + 1], b2 = cRule[4 * (RO + y) + 2];
-                const float bs[3] = {float(cRule[4 * (RO + y)]), float(b1), float(b2)};
-                float val[6];
-                mixedValues(D0 - (S.e1[0] * b1 + S.e2[0] * b2), D1 - (S.e1[1] * b1 + S.e2[1] * b2),
-                            D2 - (S.e1[2] * b1 + S.e2[2] * b2), wx * float(cRule[4 * (RO + y) + 3]), k, ns, nt,
-                            val, bad);
+                const float b0 = cRuleF[4 * (RO + y)], b1 = cRuleF[4 * (RO + y) + 1], b2 = cRuleF[4 * (RO + y) + 2];
+                const float fx = Df[0] - (se1[0] * b1 + se2[0] * b2), fy = Df[1] - (se1[1] * b1 + se2[1] * b2),
+                            fz = Df[2] - (se1[2] * b1 + se2[2] * b2);
+                const float r2 = fx * fx + fy * fy + fz * fz;
+                bad |= !(r2 > 0.f) || !isfinite(r2);
+                const float rinv = rsqrtf(r2);
+                const float r = r2 * rinv;
+                float sn, cs;
+                if (exactPhase) {
+                    const double yb1 = cRule[4 * (RO + y) + 1], yb2 = cRule[4 * (RO + y) + 2];
+                    const double ex = D0 - (S.e1[0] * yb1 + S.e2[0] * yb2), ey = D1 - (S.e1[1] * yb1 + S.e2[1] * yb2),
+                                 ez = D2 - (S.e1[2] * yb1 + S.e2[2] * yb2);
+                    const double r2d = ex * ex + ey * ey + ez * ez;
+                    double q = double(rinv);
+                    q = q * (1.5 - 0.5 * r2d * q * q);  // one Newton step of 1/sqrt in FP64
+                    const double ph = k * (r2d * q);
+                    const double turns = (ph * kInvTwoPi + kRound) - kRound;
+                    sincosf(float(fma(-turns, kTwoPiLo, fma(-turns, kTwoPiHi, ph))), &sn, &cs);
+                } else {
+                    sincosf(kf * r, &sn, &cs);
+                }
+                const float kr = kf * r;
+                const float sc = wx * cRuleF[4 * (RO + y) + 3] * rinv;
+                const float gr = cs * sc, gi = -sn * sc;
+                const float rr = gr - gi * kr, ri = gi + gr * kr;
+                const float rinv2 = rinv * rinv;
+                const float ps = (fx * ns[0] + fy * ns[1] + fz * ns[2]) * rinv2;
+                const float qt = -(fx * nt[0] + fy * nt[1] + fz * nt[2]) * rinv2;
+                const float val[6] = {gr, gi, rr * ps, ri * ps, rr * qt, ri * qt};
+                const float bs[3] = {b0, b1, b2};
 #pragma unroll
                 for (int kind = 0; kind < 3; ++kind)
 #pragma unroll
@@ -302,7 +341,7 @@ __global__ void __launch_bounds__(256, 2) regularMixedKernel(const DPanel *__res
                         Sv[kind * 6 + 2 * j + 1] += val[2 * kind + 1] * bs[j];
                     }
             }
-            const float bt[3] = {float(cRule[4 * (RO + x)]), float(bx1), float(bx2)};
+            const float bt[3] = {cRuleF[4 * (RO + x)], cRuleF[4 * (RO + x) + 1], cRuleF[4 * (RO + x) + 2]};
 #pragma unroll
             for (int kind = 0; kind < 3; ++kind)
 #pragma unroll
@@ -595,6 +634,159 @@ __device__ __forceinline__ void nearSample(float (&acc)[54], const DPanel &t, co
         }
 }
 
+// Green values (g, P, Q as re/im pairs) of one sample of a near pair in the
+// plain form, FP64.
+__device__ __forceinline__ void plainValues(double dx, double dy, double dz, double w, double k, const DPanel &t,
+                                            const DPanel &s, double (&val)[6], bool &bad) {
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    bad |= !(r2 > 0) || !isfinite(r2);
+    const double rinv = rsqrt(r2);
+    const double r = r2 * rinv, kr = k * r;
+    double sn, cs;
+    sincos(kr, &sn, &cs);
+    const double sc = w * rinv;
+    const double gr = cs * sc, gi = -sn * sc;
+    const double rr = gr - gi * kr, ri = gi + gr * kr;
+    const double rinv2 = rinv * rinv;
+    const double ps = (dx * s.n[0] + dy * s.n[1] + dz * s.n[2]) * rinv2;
+    const double qt = -(dx * t.n[0] + dy * t.n[1] + dz * t.n[2]) * rinv2;
+    val[0] = gr;
+    val[1] = gi;
+    val[2] = rr * ps;
+    val[3] = ri * ps;
+    val[4] = rr * qt;
+    val[5] = ri * qt;
+}
+
+// Near pairs whose patches are all tensor patches: one warp per unordered
+// pair. Lane (x, half) owns test point x of the patch rule and half of the
+// trial points; trial bases are contracted in registers, test bases through
+// shared memory by the 27 lanes that own a (kind, i, j) moment. Pairs with
+// projected patches go to nearKernel.
+template <bool Mixed>
+__global__ void __launch_bounds__(64) nearWarpKernel(const DPanel *__restrict__ panels, uint32_t T,
+                                                      const NearPairJob *__restrict__ jobs, uint32_t jobCount,
+                                                      const Patch *__restrict__ patches, const double *__restrict__ ks,
+                                                      double *__restrict__ records, int *error) {
+    using Acc = std::conditional_t<Mixed, float, double>;
+    __shared__ Acc sS[2][64][18];     // per warp: trial-contracted values S(x)
+    __shared__ double sB[2][64][3];   // per warp: mapped test barycentrics
+    __shared__ double sY[2][64][3];   // per warp: mapped trial barycentrics
+    __shared__ double sM[2][54];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t pairIndex = blockIdx.x * 2 + warp;
+    if (pairIndex >= jobCount)
+        return;
+    const NearPairJob job = jobs[pairIndex];
+    const int f = blockIdx.y;
+    const double k = ks[f], invk = 1.0 / k;
+    const DPanel &t = panels[job.first];
+    const DPanel &s = panels[job.second];
+    const double w4 = 4.0 * t.area * s.area * kInvFourPi;
+    bool bad = false;
+    double own[2] = {0, 0};  // lanes 0..26: accumulated moment (kind, i, j) of this pair
+    const double d0[3] = {t.v0[0] - s.v0[0], t.v0[1] - s.v0[1], t.v0[2] - s.v0[2]};
+    for (uint32_t q = 0; q < job.patchCount; ++q) {
+        const Patch &patch = patches[job.firstPatch + q];
+        const int n = patch.degree == 14 ? 64 : 16;
+        const int ro = patch.degree == 14 ? 34 : 18;  // rule offsets of the 16- and 64-point bins
+        // mapped rule points of this patch (test from patch.test, trial from patch.trial)
+        for (int idx = lane; idx < n; idx += 32) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                sB[warp][idx][i] = cRule[4 * (ro + idx)] * patch.test[i] + cRule[4 * (ro + idx) + 1] * patch.test[3 + i] +
+                                   cRule[4 * (ro + idx) + 2] * patch.test[6 + i];
+                sY[warp][idx][i] = cRule[4 * (ro + idx)] * patch.trial[i] + cRule[4 * (ro + idx) + 1] * patch.trial[3 + i] +
+                                   cRule[4 * (ro + idx) + 2] * patch.trial[6 + i];
+            }
+        }
+        __syncwarp();
+        const double wpatch = patch.areaFraction * w4;
+        // lane -> test points x = lane (+32) ; for n = 16, lanes 16..31 take the second half of the trial points
+        const int xCount = n == 16 ? 1 : 2;
+        for (int xi = 0; xi < xCount; ++xi) {
+            const int x = n == 16 ? (lane & 15) : lane + 32 * xi;
+            const int y0 = n == 16 ? (lane >> 4) * 8 : 0, y1 = n == 16 ? y0 + 8 : n;
+            const double *bt = sB[warp][x];
+            const double Dx = d0[0] + (t.e1[0] * bt[1] + t.e2[0] * bt[2]);
+            const double Dy = d0[1] + (t.e1[1] * bt[1] + t.e2[1] * bt[2]);
+            const double Dz = d0[2] + (t.e1[2] * bt[1] + t.e2[2] * bt[2]);
+            const double wx = cRule[4 * (ro + x) + 3] * wpatch;
+            Acc S[18];
+#pragma unroll
+            for (int c = 0; c < 18; ++c)
+                S[c] = 0;
+            for (int y = y0; y < y1; ++y) {
+                const double *bs = sY[warp][y];
+                const double dx = Dx - (s.e1[0] * bs[1] + s.e2[0] * bs[2]);
+                const double dy = Dy - (s.e1[1] * bs[1] + s.e2[1] * bs[2]);
+                const double dz = Dz - (s.e1[2] * bs[1] + s.e2[2] * bs[2]);
+                const double w = wx * cRule[4 * (ro + y) + 3];
+                Acc val[6];
+                if constexpr (Mixed) {
+                    const float ns[3] = {float(s.n[0]), float(s.n[1]), float(s.n[2])};
+                    const float nt[3] = {float(t.n[0]), float(t.n[1]), float(t.n[2])};
+                    mixedValues(dx, dy, dz, float(w), k, ns, nt, val, bad);
+                } else {
+                    plainValues(dx, dy, dz, w, k, t, s, val, bad);
+                }
+#pragma unroll
+                for (int kind = 0; kind < 3; ++kind)
+#pragma unroll
+                    for (int j = 0; j < 3; ++j) {
+                        S[kind * 6 + 2 * j] += val[2 * kind] * Acc(bs[j]);
+                        S[kind * 6 + 2 * j + 1] += val[2 * kind + 1] * Acc(bs[j]);
+                    }
+            }
+            if (n == 16) {
+#pragma unroll
+                for (int c = 0; c < 18; ++c)
+                    S[c] += __shfl_xor_sync(0xffffffffu, S[c], 16);
+                if (lane < 16)
+#pragma unroll
+                    for (int c = 0; c < 18; ++c)
+                        sS[warp][x][c] = S[c];
+            } else {
+#pragma unroll
+                for (int c = 0; c < 18; ++c)
+                    sS[warp][x][c] = S[c];
+            }
+        }
+        __syncwarp();
+        if (lane < 27) {
+            const int kind = lane / 9, i = (lane % 9) / 3, j = lane % 3;
+            double re = 0, im = 0;
+            for (int x = 0; x < n; ++x) {
+                re += sB[warp][x][i] * sS[warp][x][kind * 6 + 2 * j];
+                im += sB[warp][x][i] * sS[warp][x][kind * 6 + 2 * j + 1];
+            }
+            own[0] += re;
+            own[1] += im;
+        }
+        __syncwarp();
+    }
+    if (lane < 27) {
+        const int kind = lane / 9, e = lane % 9;
+        sM[warp][kind * 18 + 2 * e] = own[0];
+        sM[warp][kind * 18 + 2 * e + 1] = own[1];
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0)
+        flagError(error, kErrDistance);
+    __syncwarp();
+    if (lane < 24) {
+        const int o = lane;
+        double re, im;
+        pairRecordValue(o, &sM[warp][0], &sM[warp][18], &sM[warp][36], t, s, k, invk, re, im);
+        if (!isfinite(re) || !isfinite(im))
+            flagError(error, kErrNonFinite);
+        const size_t slot = o < 12 ? size_t(job.second) * T + job.first : size_t(job.first) * T + job.second;
+        const int e = o < 12 ? o : o - 12;
+        double *dst = records + size_t(f) * T * T * kRecordDoubles + slot * kRecordDoubles + 2 * e;
+        dst[0] = re;
+        dst[1] = im;
+    }
+}
+
 template <bool Mixed>
 __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                   const NearPairJob *__restrict__ jobs,
@@ -814,8 +1006,8 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
     TimedScope scope(timer, mixed ? mixedNames[bin] : names[bin], stream);
     if (mixed) {
         const dim3 grid(unsigned(smCount() * 8), B);
-        regularMixedKernel<NP><<<grid, 256, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
-                                                         bin, ws.records, error);
+        regularMixedKernel<NP><<<grid, 256, 0, stream>>>(g.panels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
+                                                         ws.binCapacity, bin, ws.records, error);
     } else {
         const dim3 grid(unsigned(smCount() * 6), B);
         regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
@@ -844,6 +1036,11 @@ void uploadRuleTables(cudaStream_t stream) {
         }
     }
     cudaCheck(cudaMemcpyToSymbolAsync(cRule, table, sizeof(table), 0, cudaMemcpyHostToDevice, stream), "rule upload");
+    static float tableF[kRulePoints * 4];
+    for (int i = 0; i < kRulePoints * 4; ++i)
+        tableF[i] = float(table[i]);
+    cudaCheck(cudaMemcpyToSymbolAsync(cRuleF, tableF, sizeof(tableF), 0, cudaMemcpyHostToDevice, stream),
+              "rule upload");
     double g20[40];
     const auto g = gaussLegendre01(20);
     for (int i = 0; i < 20; ++i) {
@@ -886,15 +1083,28 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
                                                                      g.singularOrder, ws.records, error);
         cudaCheck(cudaGetLastError(), "singular assembly launch");
     }
-    if (g.nearPairCount) {
+    if (g.nearPairCount - g.projectedPairCount) {
         TimedScope scope(timer, "near", stream);
+        const uint32_t tensorPairs = g.nearPairCount - g.projectedPairCount;
+        const dim3 grid((tensorPairs + 1) / 2, B);
         if (mixed)
-            nearKernel<true><<<dim3(g.nearPairCount, B), 128, 0, stream>>>(g.panels, g.T, g.nearPairs, g.patches, ks,
-                                                                           ws.records, error);
+            nearWarpKernel<true><<<grid, 64, 0, stream>>>(g.panels, g.T, g.nearPairs, tensorPairs, g.patches, ks,
+                                                          ws.records, error);
         else
-            nearKernel<false><<<dim3(g.nearPairCount, B), 128, 0, stream>>>(g.panels, g.T, g.nearPairs, g.patches,
-                                                                            ks, ws.records, error);
+            nearWarpKernel<false><<<grid, 64, 0, stream>>>(g.panels, g.T, g.nearPairs, tensorPairs, g.patches, ks,
+                                                           ws.records, error);
         cudaCheck(cudaGetLastError(), "near assembly launch");
+    }
+    if (g.projectedPairCount) {
+        TimedScope scope(timer, "near_projected", stream);
+        const NearPairJob *projected = g.nearPairs + (g.nearPairCount - g.projectedPairCount);
+        if (mixed)
+            nearKernel<true><<<dim3(g.projectedPairCount, B), 128, 0, stream>>>(g.panels, g.T, projected, g.patches,
+                                                                                ks, ws.records, error);
+        else
+            nearKernel<false><<<dim3(g.projectedPairCount, B), 128, 0, stream>>>(g.panels, g.T, projected, g.patches,
+                                                                                 ks, ws.records, error);
+        cudaCheck(cudaGetLastError(), "projected near assembly launch");
     }
     {
         TimedScope scope(timer, "gather_trial", stream);

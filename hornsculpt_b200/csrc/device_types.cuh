@@ -63,6 +63,7 @@ struct AssemblyGeometry {
     const double *rowScale;         // 1 / lumped mass
     uint32_t T, N;
     uint32_t touchingCount, nearPairCount;
+    uint32_t projectedPairCount;    // the last near pairs, those with projected patches
     double nearTolerance;
     uint32_t minimumDegree, singularOrder;
 };

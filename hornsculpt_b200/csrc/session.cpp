@@ -228,12 +228,19 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
     for (const auto &j : plan_.touching)
         if (j.test != j.trial)
             code[unorderedPairIndex(j.test, j.trial)] = kPairTouching;
-    std::vector<NearPairJob> nearPairs;
+    // Near pairs with only tensor patches first, those with projected patches last.
+    std::vector<NearPairJob> nearPairs, projectedPairs;
     for (const auto &j : plan_.near) {
         code[unorderedPairIndex(j.test, j.trial)] = kPairNear;
-        if (!j.swap)
-            nearPairs.push_back({j.test, j.trial, j.first, j.count});
+        if (j.swap)
+            continue;
+        bool projected = false;
+        for (uint32_t q = 0; q < j.count; ++q)
+            projected = projected || plan_.patches[j.first + q].projection;
+        (projected ? projectedPairs : nearPairs).push_back({j.test, j.trial, j.first, j.count});
     }
+    projectedPairCount_ = uint32_t(projectedPairs.size());
+    nearPairs.insert(nearPairs.end(), projectedPairs.begin(), projectedPairs.end());
     if (!plan_.wholePanelDegrees.empty())
         for (size_t u = 0; u < pairs; ++u)
             if (code[u] == kPairRegular && plan_.wholePanelDegrees[u])
@@ -438,7 +445,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     AssemblyGeometry geo{dPanels_.as<DPanel>(), dBounds_.as<Bounds>(), dPairCode_.as<uint8_t>(),
                          dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), dPatches_.as<Patch>(),
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
-                         dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, o.near_relative_tolerance,
+                         dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
+                         o.near_relative_tolerance,
                          o.quadrature_order, o.singular_order};
     double maxEdge = 0;
     for (const auto &p : space_.panels)
@@ -744,7 +752,8 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
     AssemblyGeometry geo{dPanels_.as<DPanel>(), dBounds_.as<Bounds>(), dPairCode_.as<uint8_t>(),
                          dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), dPatches_.as<Patch>(),
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
-                         dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, o.near_relative_tolerance,
+                         dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
+                         o.near_relative_tolerance,
                          o.quadrature_order, o.singular_order};
     AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
                          dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};

@@ -91,7 +91,7 @@ class Session {
     Plan plan_;
     double planMs_ = 0;
     DeviceBuffer dPairCode_, dTouching_, dNearPairs_, dPatches_, dGauss_;
-    uint32_t touchingCount_ = 0, nearPairCount_ = 0;
+    uint32_t touchingCount_ = 0, nearPairCount_ = 0, projectedPairCount_ = 0;
     uint64_t singularSamples_ = 0, nearSamples_ = 0;
     // workspaces (grow only)
     DeviceBuffer dRecords_, dColumns_, dPanelRhs_, dBins_, dBinCounts_, dA_, dLU_, dRhs_, dX_, dCorr_, dNorms_,
