@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
             pairRecordValue(o, &sM[pl][0], &sM[pl][18], &sM[pl][36], panels[pr.x], panels[pr.y], k, invk, re, im);
             const size_t slot = o < 12 ? size_t(pr.y) * T + pr.x : size_t(pr.x) * T + pr.y;
             const int e = o < 12 ? o : o - 12;
-            double *dst = rec + slot * kRecordDoubles + 2 * e;
+            double *dst = rec + recordOffset(T, slot, e);
             if (!isfinite(re) || !isfinite(im))
                 flagError(error, kErrNonFinite);
             dst[0] = re;
@@ -251,123 +251,235 @@ __device__ __forceinline__ void mixedValues(double dx, double dy, double dz, flo
 }
 
 // Regular pairs in the mixed form: one unordered pair per thread, NP x NP
-// samples, trial bases contracted per test point (FP32), no shared memory.
-// The displacement used for amplitudes and normal projections is FP32
-// (test point converted once, trial point formed in FP32: relative error
-// ~eps_fp32, as for the reference's mixed sample); pairs whose k*r can
-// exceed 1 also form the FP64 displacement for the phase.
+// samples, trial bases contracted per test point, no shared memory and no
+// FP64 arithmetic per sample.
+//
+// Phase. Rounding r or k*r to FP32 leaves an O(eps_fp32 * k*r) phase error
+// that no quadrature refinement removes (panel_integrals.cuh:91-142 keeps
+// FP64 for k*r > 1 for that reason). Here the pair's centre distance r0 and
+// its phase k*r0 are FP64 (reduced modulo pi/2 once per pair) and each sample
+// adds k*(r - r0) = k*Delta/(r + r0) with Delta = r^2 - r0^2 = d.(2c + d),
+// c the centre displacement and d the small point offset; Delta comes from
+// products with d only, so its FP32 error is O(eps * |d| * r0) and the phase
+// error O(eps * k * |d|), independent of k*r0. sin/cos are Taylor
+// polynomials on [-pi/4, pi/4] (truncation below 2e-9) with the quadrant
+// carried as an integer.
+// Amplitude. The displacement c + d is FP32 (relative error ~eps_fp32, as
+// for the reference's mixed sample); the normal projections use that the
+// trial edges are orthogonal to the trial normal.
 __constant__ float cRuleF[kRulePoints * 4];
 
+// (sin, cos) of x + q*pi/2 for |x| <= pi/4 (plus a small margin).
+__device__ __forceinline__ void sinCosQuadrant(float x, int q, float &sn, float &cs) {
+    const float x2 = x * x;
+    // Taylor series of sin and cos truncated after x^9 and x^10
+    const float ps = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.75573192e-6f, -1.98412698e-4f), 8.33333333e-3f),
+                                   -1.66666667e-1f), 1.f);
+    const float pc = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, -2.75573192e-7f, 2.48015873e-5f),
+                                                     -1.38888889e-3f), 4.16666667e-2f), -0.5f), 1.f);
+    const float s = x * ps;
+    const bool odd = q & 1;
+    const float a = odd ? pc : s, b = odd ? s : pc;
+    sn = __int_as_float(__float_as_int(a) ^ ((q & 2) << 30));
+    cs = __int_as_float(__float_as_int(b) ^ (((q + 1) & 2) << 30));
+}
+
+constexpr double kHalfPiHi = 1.5707963267948966, kHalfPiLo = 6.123233995736766e-17, kTwoOverPi = 0.6366197723675814;
+
+// Record element o of an unordered pair (0..11 forward block, 12..23
+// reverse block; see pairRecordValue) from its staged FP32 row: moments
+// MG, MP, MQ (54), sum of MG (2), k n_t.n_s (1), curl_ti.curl_sj (9).
+constexpr int kStageMG = 0, kStageMP = 18, kStageMQ = 36, kStageGsum = 54, kStageKnn = 56, kStageCurl = 57,
+              kStageStride = 67;  // 66 values, odd stride: conflict-free rows
+
+__device__ __forceinline__ void stagedRecordValue(int o, const float *m, float invk, float &re, float &im) {
+    const bool reverse = o >= 12;
+    const int e = reverse ? o - 12 : o;
+    const float *MG = m + kStageMG;
+    const float *X = m + (reverse ? kStageMQ : kStageMP);
+    const float *Y = m + (reverse ? kStageMP : kStageMQ);
+    if (e < 9) {
+        const int row = e / 3, col = e % 3;
+        const int i = reverse ? col : row, j = reverse ? row : col, c = 2 * (3 * i + j);
+        const float knn = m[kStageKnn], curl = m[kStageCurl + 3 * i + j] * invk;
+        re = fmaf(m[kStageGsum + 1], curl, fmaf(-knn, MG[c + 1], -X[c]));
+        im = fmaf(-m[kStageGsum], curl, fmaf(knn, MG[c], -X[c + 1]));
+    } else {
+        const int a = e - 9;
+        float sgr = 0.f, sgi = 0.f, syr = 0.f, syi = 0.f;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const int c = reverse ? 2 * (3 * b + a) : 2 * (3 * a + b);
+            sgr += MG[c];
+            sgi += MG[c + 1];
+            syr += Y[c];
+            syi += Y[c + 1];
+        }
+        re = fmaf(-syi, invk, -sgr);
+        im = fmaf(syr, invk, -sgi);
+    }
+}
+
 template <int NP>
-__global__ void __launch_bounds__(256, 2) regularMixedKernel(const DPanel *__restrict__ panels, const Bounds *__restrict__ bounds,
+__global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__restrict__ panels, const Bounds *__restrict__ bounds,
                                                              uint32_t T, const double *__restrict__ ks,
                                                              const uint2 *__restrict__ bins,
                                                              const uint32_t *__restrict__ binCounts, size_t binCapacity,
-                                                             int bin, double *__restrict__ records, int *error) {
+                                                             int bin, float *__restrict__ records, int *error) {
+    __shared__ float sStage[4][32][kStageStride];
+    __shared__ uint2 sPair[4][32];
     constexpr int RO = ruleOffset<NP>();
     constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52: adding and subtracting rounds to an integer
+    constexpr float kRoundF = 12582912.f;          // 1.5 * 2^23, the same for FP32
+    constexpr float kHalfPiHiF = 1.57079637f, kHalfPiLoF = -4.37113883e-8f, kTwoOverPiF = 0.636619772f;
     const int f = blockIdx.y;
     const double k = ks[f], invk = 1.0 / k;
-    const float kf = float(k);
+    const float kf = float(k), invkf = float(invk);
     const uint32_t count = binCounts[f * kBins + bin];
     const uint2 *list = bins + (size_t(f) * kBins + bin) * binCapacity;
-    double *rec = records + size_t(f) * T * T * kRecordDoubles;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+    float *rec = records + size_t(f) * T * T * kRecordDoubles;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x + warp * 32; base < count; base += gridDim.x * blockDim.x) {
+      const uint32_t p = base + lane;
+      if (p < count) {
         const uint2 pr = list[p];
         const DPanel &A = panels[pr.x];
         const DPanel &S = panels[pr.y];
-        const Bounds &ba = bounds[pr.x], &bb = bounds[pr.y];
-        // k times the largest point distance of the pair, from the enclosing balls
-        const double cx = ba.center.x - bb.center.x, cy = ba.center.y - bb.center.y, cz = ba.center.z - bb.center.z;
-        const bool exactPhase = k * (sqrt(cx * cx + cy * cy + cz * cz) + ba.radius + bb.radius) > 1.0;
-        const double d0 = A.v0[0] - S.v0[0], d1 = A.v0[1] - S.v0[1], d2 = A.v0[2] - S.v0[2];
-        const float w4 = float(4.0 * A.area * S.area * kInvFourPi);
-        const float ns[3] = {float(S.n[0]), float(S.n[1]), float(S.n[2])};
-        const float nt[3] = {float(A.n[0]), float(A.n[1]), float(A.n[2])};
+        const V3 ca = bounds[pr.x].center, cb = bounds[pr.y].center;
+        // centre displacement, distance and phase in FP64; phase = theta0 + q0 pi/2
+        const double cx = ca.x - cb.x, cy = ca.y - cb.y, cz = ca.z - cb.z;
+        const double r0 = sqrt(cx * cx + cy * cy + cz * cz);
+        const double ph0 = k * r0;
+        const double q0d = (ph0 * kTwoOverPi + kRound) - kRound;
+        const float theta0 = float(fma(-q0d, kHalfPiLo, fma(-q0d, kHalfPiHi, ph0)));
+        const int q0 = int(q0d - 4.0 * floor(q0d * 0.25));  // q0 mod 4, exact for |q0d| < 2^50
+        const float c[3] = {float(cx), float(cy), float(cz)};
+        const float r0f = float(r0);
+        // offset of the test panel's first vertex from the trial panel's, both about the centres
+        const float o0[3] = {float((A.v0[0] - ca.x) - (S.v0[0] - cb.x)), float((A.v0[1] - ca.y) - (S.v0[1] - cb.y)),
+                             float((A.v0[2] - ca.z) - (S.v0[2] - cb.z))};
+        const float ae1[3] = {float(A.e1[0]), float(A.e1[1]), float(A.e1[2])};
+        const float ae2[3] = {float(A.e2[0]), float(A.e2[1]), float(A.e2[2])};
         const float se1[3] = {float(S.e1[0]), float(S.e1[1]), float(S.e1[2])};
         const float se2[3] = {float(S.e2[0]), float(S.e2[1]), float(S.e2[2])};
+        const float ns[3] = {float(S.n[0]), float(S.n[1]), float(S.n[2])};
+        const float nt[3] = {float(A.n[0]), float(A.n[1]), float(A.n[2])};
+        // trial edges against the test normal (the trial normal sees none of them)
+        const float t1 = float(S.e1[0] * A.n[0] + S.e1[1] * A.n[1] + S.e1[2] * A.n[2]);
+        const float t2 = float(S.e2[0] * A.n[0] + S.e2[1] * A.n[1] + S.e2[2] * A.n[2]);
+        const float w4 = float(4.0 * A.area * S.area * kInvFourPi);
         float M[54];
 #pragma unroll
-        for (int c = 0; c < 54; ++c)
-            M[c] = 0.f;
+        for (int i = 0; i < 54; ++i)
+            M[i] = 0.f;
         bool bad = false;
+#pragma unroll 1
         for (int x = 0; x < NP; ++x) {
-            const double bx1 = cRule[4 * (RO + x) + 1], bx2 = cRule[4 * (RO + x) + 2];
-            const double D0 = d0 + (A.e1[0] * bx1 + A.e2[0] * bx2), D1 = d1 + (A.e1[1] * bx1 + A.e2[1] * bx2),
-                         D2 = d2 + (A.e1[2] * bx1 + A.e2[2] * bx2);
-            const float Df[3] = {float(D0), float(D1), float(D2)};
+            const float bx1 = cRuleF[4 * (RO + x) + 1], bx2 = cRuleF[4 * (RO + x) + 2];
+            // offset of test point x from the trial panel's first vertex, about the centres
+            float P[3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                P[i] = fmaf(ae1[i], bx1, fmaf(ae2[i], bx2, o0[i]));
+            const float CP[3] = {c[0] + P[0], c[1] + P[1], c[2] + P[2]};
+            const float psx = CP[0] * ns[0] + CP[1] * ns[1] + CP[2] * ns[2];
+            const float qtx = -(CP[0] * nt[0] + CP[1] * nt[1] + CP[2] * nt[2]);
             const float wx = cRuleF[4 * (RO + x) + 3] * w4;
             float Sv[18];
 #pragma unroll
-            for (int c = 0; c < 18; ++c)
-                Sv[c] = 0.f;
-#pragma unroll 2
+            for (int i = 0; i < 18; ++i)
+                Sv[i] = 0.f;
+#pragma unroll(NP <= 16 ? NP : 4)
             for (int y = 0; y < NP; ++y) {
                 const float b0 = cRuleF[4 * (RO + y)], b1 = cRuleF[4 * (RO + y) + 1], b2 = cRuleF[4 * (RO + y) + 2];
-                const float fx = Df[0] - (se1[0] * b1 + se2[0] * b2), fy = Df[1] - (se1[1] * b1 + se2[1] * b2),
-                            fz = Df[2] - (se1[2] * b1 + se2[2] * b2);
-                const float r2 = fx * fx + fy * fy + fz * fz;
+                float d[3], fx[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    d[i] = fmaf(-se1[i], b1, fmaf(-se2[i], b2, P[i]));
+                    fx[i] = c[i] + d[i];
+                }
+                const float r2 = fmaf(fx[0], fx[0], fmaf(fx[1], fx[1], fx[2] * fx[2]));
                 bad |= !(r2 > 0.f) || !isfinite(r2);
                 const float rinv = rsqrtf(r2);
                 const float r = r2 * rinv;
+                const float delta = fmaf(d[0], fx[0] + c[0], fmaf(d[1], fx[1] + c[1], d[2] * (fx[2] + c[2])));
+                const float theta = fmaf(kf, __fdividef(delta, r + r0f), theta0);
+                const float qf = fmaf(theta, kTwoOverPiF, kRoundF);
+                const int q = q0 + __float_as_int(qf);
+                const float qn = qf - kRoundF;
+                const float th = fmaf(-qn, kHalfPiLoF, fmaf(-qn, kHalfPiHiF, theta));
                 float sn, cs;
-                if (exactPhase) {
-                    const double yb1 = cRule[4 * (RO + y) + 1], yb2 = cRule[4 * (RO + y) + 2];
-                    const double ex = D0 - (S.e1[0] * yb1 + S.e2[0] * yb2), ey = D1 - (S.e1[1] * yb1 + S.e2[1] * yb2),
-                                 ez = D2 - (S.e1[2] * yb1 + S.e2[2] * yb2);
-                    const double r2d = ex * ex + ey * ey + ez * ez;
-                    double q = double(rinv);
-                    q = q * (1.5 - 0.5 * r2d * q * q);  // one Newton step of 1/sqrt in FP64
-                    const double ph = k * (r2d * q);
-                    const double turns = (ph * kInvTwoPi + kRound) - kRound;
-                    sincosf(float(fma(-turns, kTwoPiLo, fma(-turns, kTwoPiHi, ph))), &sn, &cs);
-                } else {
-                    sincosf(kf * r, &sn, &cs);
-                }
+                sinCosQuadrant(th, q, sn, cs);
                 const float kr = kf * r;
                 const float sc = wx * cRuleF[4 * (RO + y) + 3] * rinv;
                 const float gr = cs * sc, gi = -sn * sc;
-                const float rr = gr - gi * kr, ri = gi + gr * kr;
+                const float rr = fmaf(-gi, kr, gr), ri = fmaf(gr, kr, gi);
                 const float rinv2 = rinv * rinv;
-                const float ps = (fx * ns[0] + fy * ns[1] + fz * ns[2]) * rinv2;
-                const float qt = -(fx * nt[0] + fy * nt[1] + fz * nt[2]) * rinv2;
+                const float ps = psx * rinv2;
+                const float qt = fmaf(t1, b1, fmaf(t2, b2, qtx)) * rinv2;
                 const float val[6] = {gr, gi, rr * ps, ri * ps, rr * qt, ri * qt};
                 const float bs[3] = {b0, b1, b2};
 #pragma unroll
                 for (int kind = 0; kind < 3; ++kind)
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
-                        Sv[kind * 6 + 2 * j] += val[2 * kind] * bs[j];
-                        Sv[kind * 6 + 2 * j + 1] += val[2 * kind + 1] * bs[j];
+                        Sv[kind * 6 + 2 * j] = fmaf(val[2 * kind], bs[j], Sv[kind * 6 + 2 * j]);
+                        Sv[kind * 6 + 2 * j + 1] = fmaf(val[2 * kind + 1], bs[j], Sv[kind * 6 + 2 * j + 1]);
                     }
             }
-            const float bt[3] = {cRuleF[4 * (RO + x)], cRuleF[4 * (RO + x) + 1], cRuleF[4 * (RO + x) + 2]};
+            const float bt[3] = {cRuleF[4 * (RO + x)], bx1, bx2};
 #pragma unroll
             for (int kind = 0; kind < 3; ++kind)
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
 #pragma unroll
                     for (int j = 0; j < 3; ++j) {
-                        M[kind * 18 + 2 * (3 * i + j)] += bt[i] * Sv[kind * 6 + 2 * j];
-                        M[kind * 18 + 2 * (3 * i + j) + 1] += bt[i] * Sv[kind * 6 + 2 * j + 1];
+                        M[kind * 18 + 2 * (3 * i + j)] = fmaf(bt[i], Sv[kind * 6 + 2 * j], M[kind * 18 + 2 * (3 * i + j)]);
+                        M[kind * 18 + 2 * (3 * i + j) + 1] =
+                            fmaf(bt[i], Sv[kind * 6 + 2 * j + 1], M[kind * 18 + 2 * (3 * i + j) + 1]);
                     }
         }
         if (bad)
             flagError(error, kErrDistance);
-        double *fwd = rec + (size_t(pr.y) * T + pr.x) * kRecordDoubles;
-        double *rev = rec + (size_t(pr.x) * T + pr.y) * kRecordDoubles;
-        bool nonFinite = false;
-#pragma unroll 1
-        for (int o = 0; o < 24; ++o) {
-            double re, im;
-            pairRecordValue(o, M, M + 18, M + 36, A, S, k, invk, re, im);
-            nonFinite |= !isfinite(re) || !isfinite(im);
-            double *dst = (o < 12 ? fwd : rev) + 2 * (o < 12 ? o : o - 12);
-            dst[0] = re;
-            dst[1] = im;
+        // stage this pair's moments and per-pair factors for the warp's record writes
+        float *row = sStage[warp][lane];
+        float gre = 0.f, gim = 0.f;
+#pragma unroll
+        for (int c = 0; c < 54; ++c)
+            row[c] = M[c];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            gre += M[2 * c];
+            gim += M[2 * c + 1];
         }
-        if (nonFinite)
-            flagError(error, kErrNonFinite);
+        row[kStageGsum] = gre;
+        row[kStageGsum + 1] = gim;
+        row[kStageKnn] = float(k * (A.n[0] * S.n[0] + A.n[1] * S.n[1] + A.n[2] * S.n[2]));
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                row[kStageCurl + 3 * i + j] = float(A.curl[3 * i] * S.curl[3 * j] + A.curl[3 * i + 1] * S.curl[3 * j + 1] +
+                                                    A.curl[3 * i + 2] * S.curl[3 * j + 2]);
+        sPair[warp][lane] = pr;
+      }
+      __syncwarp();
+      // 24 record elements per pair, written by consecutive lanes (contiguous columns)
+      const uint32_t valid = min(32u, count - base);
+      bool nonFinite = false;
+      for (uint32_t idx = lane; idx < valid * 24; idx += 32) {
+          const uint32_t j = idx / 24;
+          const int o = int(idx % 24);
+          const uint2 pr = sPair[warp][j];
+          float re, im;
+          stagedRecordValue(o, sStage[warp][j], invkf, re, im);
+          nonFinite |= !isfinite(re) || !isfinite(im);
+          const size_t slot = o < 12 ? size_t(pr.y) * T + pr.x : size_t(pr.x) * T + pr.y;
+          *reinterpret_cast<float2 *>(rec + recordOffset(T, slot, o < 12 ? o : o - 12)) = make_float2(re, im);
+      }
+      if (nonFinite)
+          flagError(error, kErrNonFinite);
+      __syncwarp();
     }
 }
 
@@ -569,9 +681,170 @@ __global__ void __launch_bounds__(128) singularKernel(const DPanel *__restrict__
         }
         if (!isfinite(re) || !isfinite(im))
             flagError(error, kErrNonFinite);
-        double *dst = records + size_t(f) * T * T * kRecordDoubles + (size_t(job.trial) * T + job.test) * kRecordDoubles;
-        dst[2 * o] = re;
-        dst[2 * o + 1] = im;
+        double *dst = records + size_t(f) * T * T * kRecordDoubles + recordOffset(T, size_t(job.trial) * T + job.test, o);
+        dst[0] = re;
+        dst[1] = im;
+    }
+}
+
+// Mixed form of the touching pairs: one warp per ordered job, FP32 samples.
+// The sector maps do not depend on the job, so the (sector, u, v, w) tuples
+// come from a table built once per singular order in FP64
+// (buildSingularTable): canonical-order barycentrics at radius 1, the
+// weight, and coefficients (a1, a2, b1, b2) of the displacement
+// l = A1 a1 + A2 a2 - B1 b1 - B2 b2 over the canonical edges A (test) and B
+// (trial) from the first shared vertex. For shared edges and coincident
+// panels the shared edges are merged and their coefficients are differences
+// formed in FP64, so l keeps FP32 relative accuracy where the two points
+// nearly meet. Touching pairs have k*r <= 2 k h, so the FP32 phase needs no
+// FP64 help. Moments accumulate in canonical order and are permuted back to
+// local order once per job.
+__global__ void __launch_bounds__(128) singularMixedKernel(const DPanel *__restrict__ panels, uint32_t T,
+                                                           const TouchingJob *__restrict__ jobs, uint32_t jobCount,
+                                                           const double *__restrict__ ks,
+                                                           const float4 *__restrict__ table, uint32_t order,
+                                                           float *__restrict__ records, int *error) {
+    constexpr float kRoundF = 12582912.f, kHalfPiHiF = 1.57079637f, kHalfPiLoF = -4.37113883e-8f,
+                    kTwoOverPiF = 0.636619772f;
+    const uint32_t jobIndex = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const unsigned lane = threadIdx.x & 31;
+    if (jobIndex >= jobCount)
+        return;  // warp-uniform
+    const TouchingJob job = jobs[jobIndex];
+    const int f = blockIdx.y;
+    const double k = ks[f], invk = 1.0 / k;
+    const float kf = float(k), invkf = float(invk);
+    const DPanel &t = panels[job.test];
+    const DPanel &s = panels[job.trial];
+    const bool coincident = job.topology == kCoincident;
+    // canonical edges from the first shared vertex, in FP64 then rounded
+    float A1[3], A2[3], B1[3], B2[3];
+    {
+        const int ta = job.permTest[0], tb = job.permTest[1], tc = job.permTest[2];
+        const int sa = job.permTrial[0], sb = job.permTrial[1], sc = job.permTrial[2];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const double te[3] = {0.0, t.e1[i], t.e2[i]}, se[3] = {0.0, s.e1[i], s.e2[i]};
+            A1[i] = float(te[tb] - te[ta]);
+            A2[i] = float(te[tc] - te[ta]);
+            B1[i] = float(se[sb] - se[sa]);
+            B2[i] = float(se[sc] - se[sa]);
+        }
+    }
+    const float w4 = float(4.0 * t.area * s.area * kInvFourPi);
+    const float tn[3] = {float(t.n[0]), float(t.n[1]), float(t.n[2])};
+    const float sn3[3] = {float(s.n[0]), float(s.n[1]), float(s.n[2])};
+    const float knn = kf * float(t.n[0] * s.n[0] + t.n[1] * s.n[1] + t.n[2] * s.n[2]);
+    const uint32_t per = order * order * order;
+    const uint32_t count = sectorCount(job.topology) * per;
+    const uint32_t base = job.topology == kSharedVertex ? 0u : job.topology == kSharedEdge ? 2u * per : 7u * per;
+    const float4 *tuples = table + 3 * size_t(base);
+    const float4 *radial = table + 3 * size_t(13 * per);
+    float m[18], b[6], g[2] = {0.f, 0.f};
+#pragma unroll
+    for (int c = 0; c < 18; ++c)
+        m[c] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        b[c] = 0.f;
+    bool bad = false;
+    for (uint32_t idx = lane; idx < count; idx += 32) {
+        const float4 q0 = tuples[3 * idx], q1 = tuples[3 * idx + 1], q2 = tuples[3 * idx + 2];
+        const float pt[3] = {q0.x, q0.y, q0.z}, pq[3] = {q0.w, q1.x, q1.y};
+        float l[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+            l[i] = fmaf(A1[i], q1.z, fmaf(A2[i], q1.w, fmaf(-B1[i], q2.x, -B2[i] * q2.y)));
+        const float ps1 = coincident ? 0.f : l[0] * sn3[0] + l[1] * sn3[1] + l[2] * sn3[2];
+        const float qt1 = coincident ? 0.f : -(l[0] * tn[0] + l[1] * tn[1] + l[2] * tn[2]);
+        const float lr2 = l[0] * l[0] + l[1] * l[1] + l[2] * l[2];
+        bad |= !(lr2 > 0.f) || !isfinite(lr2);
+        const float linv = rsqrtf(lr2), llen = lr2 * linv;
+        const float pw = q2.z * w4;
+        for (uint32_t ri = 0; ri < order; ++ri) {
+            const float4 rad = radial[ri];  // (r, r^3 w_r)
+            const float r = rad.x;
+            // sample at radial fraction r: displacement r*l, distance r*|l|
+            const float rinv = linv * __frcp_rn(r), kr = kf * (llen * r);
+            const float qf = fmaf(kr, kTwoOverPiF, kRoundF);
+            const float qn = qf - kRoundF;
+            float sn, cs;
+            sinCosQuadrant(fmaf(-qn, kHalfPiLoF, fmaf(-qn, kHalfPiHiF, kr)), __float_as_int(qf), sn, cs);
+            const float sc = pw * rad.y * rinv;
+            const float gr = cs * sc, gi = -sn * sc;
+            g[0] += gr;
+            g[1] += gi;
+            const float rr = fmaf(-gi, kr, gr), ri2 = fmaf(gr, kr, gi);
+            // (r l).n / (r |l|)^2 = (l.n) / (r |l|^2)
+            const float inv = rinv * linv;
+            const float ps = ps1 * inv, qt = qt1 * inv;
+            const float ar = fmaf(-rr, ps, -knn * gi), ai = fmaf(-ri2, ps, knn * gr);
+            const float br = fmaf(-ri2 * qt, invkf, -gr), bi = fmaf(rr * qt, invkf, -gi);
+            const float bt[3] = {fmaf(r, pt[0], 1.f - r), r * pt[1], r * pt[2]};
+            const float bs[3] = {fmaf(r, pq[0], 1.f - r), r * pq[1], r * pq[2]};
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                b[2 * i] = fmaf(br, bt[i], b[2 * i]);
+                b[2 * i + 1] = fmaf(bi, bt[i], b[2 * i + 1]);
+                const float ari = ar * bt[i], aii = ai * bt[i];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    m[2 * (3 * i + j)] = fmaf(ari, bs[j], m[2 * (3 * i + j)]);
+                    m[2 * (3 * i + j) + 1] = fmaf(aii, bs[j], m[2 * (3 * i + j) + 1]);
+                }
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0)
+        flagError(error, kErrDistance);
+    float v[26];
+#pragma unroll
+    for (int c = 0; c < 18; ++c)
+        v[c] = m[c];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        v[18 + c] = b[c];
+    v[24] = g[0];
+    v[25] = g[1];
+#pragma unroll
+    for (int c = 0; c < 26; ++c)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            v[c] += __shfl_xor_sync(0xffffffffu, v[c], off);
+    if (lane < 12) {
+        const int o = lane;
+        // canonical index of each local vertex
+        int invT[3], invS[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            invT[job.permTest[c]] = c;
+            invS[job.permTrial[c]] = c;
+        }
+        const int i = o < 9 ? o / 3 : o - 9, j = o % 3;
+        const int src = o < 9 ? 2 * (3 * invT[i] + invS[j]) : 18 + 2 * invT[i];
+        float vre = 0.f, vim = 0.f;
+#pragma unroll
+        for (int c = 0; c < 12; ++c) {
+            const int cand = c < 9 ? 2 * c : 18 + 2 * (c - 9);
+            if (cand == src) {
+                vre = v[cand];
+                vim = v[cand + 1];
+            }
+        }
+        double re, im;
+        if (o < 9) {
+            const double curl = t.curl[3 * i] * s.curl[3 * j] + t.curl[3 * i + 1] * s.curl[3 * j + 1] +
+                                t.curl[3 * i + 2] * s.curl[3 * j + 2];
+            re = double(vre) + double(v[25]) * curl * invk;
+            im = double(vim) - double(v[24]) * curl * invk;
+        } else {
+            re = vre;
+            im = double(vim) + (coincident ? t.area / (6.0 * k) : 0.0);
+        }
+        if (!isfinite(re) || !isfinite(im))
+            flagError(error, kErrNonFinite);
+        float *dst = records + size_t(f) * T * T * kRecordDoubles + recordOffset(T, size_t(job.trial) * T + job.test, o);
+        *reinterpret_cast<float2 *>(dst) = make_float2(float(re), float(im));
     }
 }
 
@@ -667,7 +940,8 @@ template <bool Mixed>
 __global__ void __launch_bounds__(64) nearWarpKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                       const NearPairJob *__restrict__ jobs, uint32_t jobCount,
                                                       const Patch *__restrict__ patches, const double *__restrict__ ks,
-                                                      double *__restrict__ records, int *error) {
+                                                      std::conditional_t<Mixed, float, double> *__restrict__ records,
+                                                      int *error) {
     using Acc = std::conditional_t<Mixed, float, double>;
     __shared__ Acc sS[2][64][18];     // per warp: trial-contracted values S(x)
     __shared__ double sB[2][64][3];   // per warp: mapped test barycentrics
@@ -781,9 +1055,9 @@ __global__ void __launch_bounds__(64) nearWarpKernel(const DPanel *__restrict__ 
             flagError(error, kErrNonFinite);
         const size_t slot = o < 12 ? size_t(job.second) * T + job.first : size_t(job.first) * T + job.second;
         const int e = o < 12 ? o : o - 12;
-        double *dst = records + size_t(f) * T * T * kRecordDoubles + slot * kRecordDoubles + 2 * e;
-        dst[0] = re;
-        dst[1] = im;
+        Acc *dst = records + size_t(f) * T * T * kRecordDoubles + recordOffset(T, slot, e);
+        dst[0] = Acc(re);
+        dst[1] = Acc(im);
     }
 }
 
@@ -791,7 +1065,8 @@ template <bool Mixed>
 __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                   const NearPairJob *__restrict__ jobs,
                                                   const Patch *__restrict__ patches, const double *__restrict__ ks,
-                                                  double *__restrict__ records, int *error) {
+                                                  std::conditional_t<Mixed, float, double> *__restrict__ records,
+                                                  int *error) {
     using Acc = std::conditional_t<Mixed, float, double>;
     __shared__ double red[4][54];
     __shared__ double pts[2][64][3];
@@ -876,9 +1151,9 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
             flagError(error, kErrNonFinite);
         const size_t slot = o < 12 ? size_t(job.second) * T + job.first : size_t(job.first) * T + job.second;
         const int e = o < 12 ? o : o - 12;
-        double *dst = records + size_t(f) * T * T * kRecordDoubles + slot * kRecordDoubles + 2 * e;
-        dst[0] = re;
-        dst[1] = im;
+        Acc *dst = records + size_t(f) * T * T * kRecordDoubles + recordOffset(T, slot, e);
+        dst[0] = Acc(re);
+        dst[1] = Acc(im);
     }
 }
 
@@ -886,7 +1161,8 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
 // Deterministic gathers: records -> per-(test panel, trial vertex) columns ->
 // matrix entries, and records x flux -> right-hand side.
 // ---------------------------------------------------------------------------
-__global__ void gatherTrialKernel(const double *__restrict__ records, const uint32_t *__restrict__ incOffsets,
+template <class Rec>
+__global__ void gatherTrialKernel(const Rec *__restrict__ records, const uint32_t *__restrict__ incOffsets,
                                   const uint32_t *__restrict__ incPanel, const uint8_t *__restrict__ incLocal,
                                   uint32_t T, uint32_t N, double *__restrict__ columns) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -894,17 +1170,16 @@ __global__ void gatherTrialKernel(const double *__restrict__ records, const uint
     const int f = blockIdx.z;
     if (t >= T)
         return;
-    const double *rec = records + size_t(f) * T * T * kRecordDoubles;
+    const Rec *rec = records + size_t(f) * T * T * kRecordDoubles;
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (uint32_t o = incOffsets[b]; o < incOffsets[b + 1]; ++o) {
         const uint32_t s = incPanel[o];
         const int lb = incLocal[o];
-        const double *r = rec + (size_t(s) * T + t) * kRecordDoubles;
+        // column lb of the (trial s, test t) block: 3 contiguous complex values
+        const Rec *r = rec + recordOffset(T, size_t(s) * T + t, lb);
 #pragma unroll
-        for (int la = 0; la < 3; ++la) {
-            acc[2 * la] += r[2 * (3 * la + lb)];
-            acc[2 * la + 1] += r[2 * (3 * la + lb) + 1];
-        }
+        for (int c = 0; c < 6; ++c)
+            acc[c] += double(r[c]);
     }
     double *dst = columns + (size_t(f) * N + b) * 6 * T + 6 * size_t(t);
 #pragma unroll
@@ -938,25 +1213,27 @@ __global__ void gatherTestKernel(const double *__restrict__ columns, const DPane
     dst[1] = im * sc;
 }
 
-__global__ void rhsPanelKernel(const double *__restrict__ records, const double *__restrict__ flux, uint32_t T,
+template <class Rec>
+__global__ void rhsPanelKernel(const Rec *__restrict__ records, const double *__restrict__ flux, uint32_t T,
                                uint32_t E, double *__restrict__ panelRhs) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t e = blockIdx.y;
     const int f = blockIdx.z;
     if (t >= T)
         return;
-    const double *rec = records + size_t(f) * T * T * kRecordDoubles;
+    const Rec *rec = records + size_t(f) * T * T * kRecordDoubles;
     const double *q = flux + (size_t(f) * E + e) * 2 * T;
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (uint32_t s = 0; s < T; ++s) {
         const double qr = q[2 * s], qi = q[2 * s + 1];
         if (qr == 0 && qi == 0)
             continue;
-        const double *r = rec + (size_t(s) * T + t) * kRecordDoubles + 18;
+        const Rec *r = rec + recordOffset(T, size_t(s) * T + t, 9);
 #pragma unroll
         for (int la = 0; la < 3; ++la) {
-            acc[2 * la] += r[2 * la] * qr - r[2 * la + 1] * qi;
-            acc[2 * la + 1] += r[2 * la] * qi + r[2 * la + 1] * qr;
+            const double rr = r[2 * la], ri = r[2 * la + 1];
+            acc[2 * la] += rr * qr - ri * qi;
+            acc[2 * la + 1] += rr * qi + ri * qr;
         }
     }
     double *dst = panelRhs + (size_t(f) * E + e) * 6 * T + 6 * size_t(t);
@@ -1005,18 +1282,54 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
                                      "regular_mixed_q64"};
     TimedScope scope(timer, mixed ? mixedNames[bin] : names[bin], stream);
     if (mixed) {
-        const dim3 grid(unsigned(smCount() * 8), B);
-        regularMixedKernel<NP><<<grid, 256, 0, stream>>>(g.panels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
-                                                         ws.binCapacity, bin, ws.records, error);
+        const dim3 grid(unsigned(smCount() * 16), B);
+        regularMixedKernel<NP><<<grid, 128, 0, stream>>>(g.panels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
+                                                         ws.binCapacity, bin, static_cast<float *>(ws.records),
+                                                         error);
     } else {
         const dim3 grid(unsigned(smCount() * 6), B);
         regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
-                                                         bin, ws.records, error);
+                                                         bin, static_cast<double *>(ws.records), error);
     }
     cudaCheck(cudaGetLastError(), "regular pair assembly launch");
 }
 
 }  // namespace
+
+std::vector<float> buildSingularTable(unsigned order) {
+    const auto gauss = gaussLegendre01(order);
+    const size_t per = size_t(order) * order * order;
+    std::vector<float> out((13 * per) * 12 + order * 4, 0.f);
+    const uint32_t topologies[3] = {kSharedVertex, kSharedEdge, kCoincident};
+    size_t row = 0;
+    for (uint32_t topo : topologies)
+        for (unsigned sector = 0; sector < sectorCount(topo); ++sector)
+            for (size_t tuple = 0; tuple < per; ++tuple, ++row) {
+                const size_t wi = tuple % order, vi = (tuple / order) % order, ui = tuple / (size_t(order) * order);
+                const PairPoint p = sauterSchwab(topo, sector, 1.0, gauss[ui].x, gauss[vi].x, gauss[wi].x);
+                // displacement coefficients over the canonical edges (shared ones merged)
+                double a1 = p.t[1], a2 = p.t[2], b1 = p.s[1], b2 = p.s[2];
+                if (topo == kSharedEdge || topo == kCoincident) {
+                    a1 -= b1;
+                    b1 = 0;
+                }
+                if (topo == kCoincident) {
+                    a2 -= b2;
+                    b2 = 0;
+                }
+                float *q = &out[12 * row];
+                const double v[11] = {p.t[0], p.t[1], p.t[2], p.s[0], p.s[1], p.s[2], a1, a2, b1, b2,
+                                      p.w * gauss[ui].w * gauss[vi].w * gauss[wi].w};
+                for (int c = 0; c < 11; ++c)
+                    q[c] = float(v[c]);
+            }
+    for (unsigned ri = 0; ri < order; ++ri) {
+        const double r = gauss[ri].x;
+        out[12 * 13 * per + 4 * ri] = float(r);
+        out[12 * 13 * per + 4 * ri + 1] = float(r * r * r * gauss[ri].w);
+    }
+    return out;
+}
 
 void uploadRuleTables(cudaStream_t stream) {
     static bool done = false;
@@ -1064,6 +1377,8 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
     const uint64_t pairs = uint64_t(g.T) * (g.T - 1) / 2;
     if (g.N > 65535 || B > 65535 || E > 65535)
         throw std::runtime_error("Dense assembly grid limits exceeded (more than 65535 vertices, frequencies or excitations).");
+    double *recD = static_cast<double *>(ws.records);
+    float *recF = static_cast<float *>(ws.records);
     cudaCheck(cudaMemsetAsync(ws.binCounts, 0, sizeof(uint32_t) * kBins * B, stream), "bin reset");
     if (pairs) {
         TimedScope scope(timer, "classify_pairs", stream);
@@ -1078,9 +1393,13 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
     launchRegular<16>(g, ks, B, ws, 2, error, stream, timer, mixed);
     launchRegular<64>(g, ks, B, ws, 3, error, stream, timer, mixed);
     if (g.touchingCount) {
-        TimedScope scope(timer, "singular", stream);
-        singularKernel<<<dim3(g.touchingCount, B), 128, 0, stream>>>(g.panels, g.T, g.touching, ks, gaussSingular,
-                                                                     g.singularOrder, ws.records, error);
+        TimedScope scope(timer, mixed ? "singular_mixed" : "singular", stream);
+        if (mixed)
+            singularMixedKernel<<<dim3((g.touchingCount + 3) / 4, B), 128, 0, stream>>>(
+                g.panels, g.T, g.touching, g.touchingCount, ks, g.singularTable, g.singularOrder, recF, error);
+        else
+            singularKernel<<<dim3(g.touchingCount, B), 128, 0, stream>>>(g.panels, g.T, g.touching, ks,
+                                                                         gaussSingular, g.singularOrder, recD, error);
         cudaCheck(cudaGetLastError(), "singular assembly launch");
     }
     if (g.nearPairCount - g.projectedPairCount) {
@@ -1089,10 +1408,10 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         const dim3 grid((tensorPairs + 1) / 2, B);
         if (mixed)
             nearWarpKernel<true><<<grid, 64, 0, stream>>>(g.panels, g.T, g.nearPairs, tensorPairs, g.patches, ks,
-                                                          ws.records, error);
+                                                          recF, error);
         else
             nearWarpKernel<false><<<grid, 64, 0, stream>>>(g.panels, g.T, g.nearPairs, tensorPairs, g.patches, ks,
-                                                           ws.records, error);
+                                                           recD, error);
         cudaCheck(cudaGetLastError(), "near assembly launch");
     }
     if (g.projectedPairCount) {
@@ -1100,16 +1419,19 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         const NearPairJob *projected = g.nearPairs + (g.nearPairCount - g.projectedPairCount);
         if (mixed)
             nearKernel<true><<<dim3(g.projectedPairCount, B), 128, 0, stream>>>(g.panels, g.T, projected, g.patches,
-                                                                                ks, ws.records, error);
+                                                                                ks, recF, error);
         else
             nearKernel<false><<<dim3(g.projectedPairCount, B), 128, 0, stream>>>(g.panels, g.T, projected, g.patches,
-                                                                                 ks, ws.records, error);
+                                                                                 ks, recD, error);
         cudaCheck(cudaGetLastError(), "projected near assembly launch");
     }
     {
         TimedScope scope(timer, "gather_trial", stream);
-        gatherTrialKernel<<<dim3((g.T + 127) / 128, g.N, B), 128, 0, stream>>>(ws.records, g.incOffsets, g.incPanel,
-                                                                               g.incLocal, g.T, g.N, ws.columns);
+        const dim3 grid((g.T + 127) / 128, g.N, B);
+        if (mixed)
+            gatherTrialKernel<<<grid, 128, 0, stream>>>(recF, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N, ws.columns);
+        else
+            gatherTrialKernel<<<grid, 128, 0, stream>>>(recD, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N, ws.columns);
         cudaCheck(cudaGetLastError(), "trial gather launch");
     }
     {
@@ -1120,7 +1442,11 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
     }
     {
         TimedScope scope(timer, "rhs_panel", stream);
-        rhsPanelKernel<<<dim3((g.T + 127) / 128, E, B), 128, 0, stream>>>(ws.records, flux, g.T, E, ws.panelRhs);
+        const dim3 grid((g.T + 127) / 128, E, B);
+        if (mixed)
+            rhsPanelKernel<<<grid, 128, 0, stream>>>(recF, flux, g.T, E, ws.panelRhs);
+        else
+            rhsPanelKernel<<<grid, 128, 0, stream>>>(recD, flux, g.T, E, ws.panelRhs);
     }
     {
         TimedScope scope(timer, "rhs_vertex", stream);

@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 namespace hsb {
@@ -21,9 +22,20 @@ struct DPanel {
 
 // Pair-block record of one ordered (test, trial) panel pair: the 3x3 P1xP1
 // Burton-Miller block (curl term included) and the 3 P1xDP0 right-hand-side
-// moments, complex FP64 (24 doubles = 192 B). Records live at
-// slot = trial * T + test so that consecutive test panels are adjacent.
+// moments, 12 complex values (24 reals: FP64 in the plain form, FP32 in the
+// mixed form). Slot = trial * T + test. A frequency's records form four
+// planes of T*T slots with 3 complex values each: plane j < 3 holds column j
+// of the block (rows i = 0..2), plane 3 the right-hand-side moments, so the
+// trial-vertex gather reads one contiguous column per (trial, test) slot and
+// consecutive test panels are adjacent.
 constexpr int kRecordDoubles = 24;
+
+// Offset (in reals) of record element e of a slot: e < 9 is block entry
+// (row e / 3, column e % 3), e >= 9 right-hand-side row e - 9.
+HS_HD size_t recordOffset(uint32_t T, size_t slot, int e) {
+    const int plane = e < 9 ? e % 3 : 3, row = e < 9 ? e / 3 : e - 9;
+    return ((size_t(plane) * T * T + slot) * 3 + row) * 2;
+}
 
 // Device error word codes (cuda_solver.cu:705-715).
 enum DeviceError : int {
@@ -66,17 +78,24 @@ struct AssemblyGeometry {
     uint32_t projectedPairCount;    // the last near pairs, those with projected patches
     double nearTolerance;
     uint32_t minimumDegree, singularOrder;
+    const float4 *singularTable;    // mixed-form touching tuples (buildSingularTable)
 };
 
 // Quadrature tables copied to __constant__ memory at first use.
 void uploadRuleTables(cudaStream_t stream);
+
+// Touching-pair tuples of the mixed form for one singular order: per
+// (topology block vertex|edge|coincident, sector, u, v, w) twelve floats
+// (canonical test and trial barycentrics at radius 1, displacement
+// coefficients a1 a2 b1 b2, weight, pad), then per radial node (r, r^3 w, 0, 0).
+std::vector<float> buildSingularTable(unsigned order);
 
 // Per-batch assembly of B frequencies. ks[B]; flux q[B][E][T] complex;
 // outputs A[B][N*N] (column-major) and rhs[B][E][N] complex. Workspace:
 // records [B][T*T][24], gathered columns C[B][N][3T] complex, per-panel rhs
 // partials R[B][E][3T] complex, pair bins [B][4][pairs] and counters.
 struct AssemblyWorkspace {
-    double *records;
+    void *records;                  // double (plain form) or float (mixed form) records
     double *columns;
     double *panelRhs;
     uint2 *bins;

@@ -270,6 +270,7 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
     upload(dNearPairs_, nearPairs, s);
     upload(dPatches_, plan_.patches, s);
     upload(dGauss_, g, s);
+    upload(dSingularTable_, buildSingularTable(o.singular_order), s);
     cuda(cudaStreamSynchronize(s), "CUDA synchronization");
     singularSamples_ = 0;
     for (const auto &j : plan_.touching)
@@ -328,7 +329,7 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O) {
     dWork32_.ensure(B * E * N * 8);
     size_t bytes = 0;
     for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_, &dMass_,
-                                  &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dRecords_, &dColumns_,
+                                  &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_, &dRecords_, &dColumns_,
                                   &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
                                   &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_,
                                   &dWork32_})
@@ -447,7 +448,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
                          dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
                          o.near_relative_tolerance,
-                         o.quadrature_order, o.singular_order};
+                         o.quadrature_order, o.singular_order, dSingularTable_.as<float4>()};
     double maxEdge = 0;
     for (const auto &p : space_.panels)
         maxEdge = std::max(maxEdge, p.maxEdge);
@@ -754,7 +755,7 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
                          dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
                          o.near_relative_tolerance,
-                         o.quadrature_order, o.singular_order};
+                         o.quadrature_order, o.singular_order, dSingularTable_.as<float4>()};
     AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
                          dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
     assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), 1, 1, ws, dA_.as<double>(),

@@ -90,7 +90,7 @@ class Session {
     double planK_ = -1;
     Plan plan_;
     double planMs_ = 0;
-    DeviceBuffer dPairCode_, dTouching_, dNearPairs_, dPatches_, dGauss_;
+    DeviceBuffer dPairCode_, dTouching_, dNearPairs_, dPatches_, dGauss_, dSingularTable_;
     uint32_t touchingCount_ = 0, nearPairCount_ = 0, projectedPairCount_ = 0;
     uint64_t singularSamples_ = 0, nearSamples_ = 0;
     // workspaces (grow only)
