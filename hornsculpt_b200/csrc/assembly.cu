@@ -251,23 +251,25 @@ __device__ __forceinline__ void mixedValues(double dx, double dy, double dz, flo
 }
 
 // Regular pairs in the mixed form: one unordered pair per thread, NP x NP
-// samples, trial bases contracted per test point, no shared memory and no
-// FP64 arithmetic per sample.
+// samples, trial bases contracted per test point, no FP64 per sample.
 //
 // Phase. Rounding r or k*r to FP32 leaves an O(eps_fp32 * k*r) phase error
 // that no quadrature refinement removes (panel_integrals.cuh:91-142 keeps
 // FP64 for k*r > 1 for that reason). Here the pair's centre distance r0 and
-// its phase k*r0 are FP64 (reduced modulo pi/2 once per pair) and each sample
-// adds k*(r - r0) = k*Delta/(r + r0) with Delta = r^2 - r0^2 = d.(2c + d),
-// c the centre displacement and d the small point offset; Delta comes from
-// products with d only, so its FP32 error is O(eps * |d| * r0) and the phase
-// error O(eps * k * |d|), independent of k*r0. sin/cos are Taylor
-// polynomials on [-pi/4, pi/4] (truncation below 2e-9) with the quadrant
-// carried as an integer.
-// Amplitude. The displacement c + d is FP32 (relative error ~eps_fp32, as
-// for the reference's mixed sample); the normal projections use that the
-// trial edges are orthogonal to the trial normal.
-__constant__ float cRuleF[kRulePoints * 4];
+// its phase k*r0 are FP64 (reduced modulo 2 pi once per pair) and each sample
+// adds k*(r - r0) = k*Delta/(r + r0) with Delta = r^2 - r0^2. With c the
+// centre displacement, p the test point's offset and e(y) = E1 b1 + E2 b2 the
+// trial point's offset (trial edges E1, E2), Delta = (2c + p).p
+// - 2 (c + p).e(y) + |e(y)|^2, a quadratic in the trial barycentrics whose
+// coefficients are formed once per pair and test point; its terms are
+// O(r0 * h), so the FP32 phase error is O(eps * k * h), independent of k*r0.
+// r^2 = r0^2 + Delta. sin/cos of the phase reduced to [-pi, pi] use the
+// hardware approximation (absolute error about 4e-7).
+// Amplitude. FP32 throughout (relative error ~eps_fp32, as for the
+// reference's mixed sample); the double-layer projection (x - y).n_trial is
+// constant over the trial panel and the adjoint one affine in b1, b2.
+// Rule table per point: b0, b1, b2, w, b1^2, 2 b1 b2, b2^2, 0.
+__constant__ float cRuleF[kRulePoints * 8];
 
 // (sin, cos) of x + q*pi/2 for |x| <= pi/4 (plus a small margin).
 __device__ __forceinline__ void sinCosQuadrant(float x, int q, float &sn, float &cs) {
@@ -284,7 +286,13 @@ __device__ __forceinline__ void sinCosQuadrant(float x, int q, float &sn, float 
     cs = __int_as_float(__float_as_int(b) ^ (((q + 1) & 2) << 30));
 }
 
-constexpr double kHalfPiHi = 1.5707963267948966, kHalfPiLo = 6.123233995736766e-17, kTwoOverPi = 0.6366197723675814;
+
+template <int NP>
+__global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__restrict__ panels, const Bounds *__restrict__ bounds,
+                                                             uint32_t T, const double *__restrict__ ks,
+                                                             const uint2 *__restrict__ bins,
+                                                             const uint32_t *__restrict__ binCounts, size_t binCapacity,
+                                                             int bin, float *__restrict__ records, int *error);
 
 // Record element o of an unordered pair (0..11 forward block, 12..23
 // reverse block; see pairRecordValue) from its staged FP32 row: moments
@@ -330,8 +338,9 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__res
     __shared__ uint2 sPair[4][32];
     constexpr int RO = ruleOffset<NP>();
     constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52: adding and subtracting rounds to an integer
-    constexpr float kRoundF = 12582912.f;          // 1.5 * 2^23, the same for FP32
-    constexpr float kHalfPiHiF = 1.57079637f, kHalfPiLoF = -4.37113883e-8f, kTwoOverPiF = 0.636619772f;
+    constexpr double kTwoPi = 6.283185307179586, kTwoPiLo = 2.4492935982947064e-16, kInvTwoPi = 0.15915494309189535;
+    constexpr float kRoundF = 12582912.f;  // 1.5 * 2^23, the same for FP32
+    constexpr float kTwoPiHiF = 6.28318548f, kTwoPiLoF = -1.74845553e-7f, kInvTwoPiF = 0.159154943f;
     const int f = blockIdx.y;
     const double k = ks[f], invk = 1.0 / k;
     const float kf = float(k), invkf = float(invk);
@@ -346,16 +355,15 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__res
         const DPanel &A = panels[pr.x];
         const DPanel &S = panels[pr.y];
         const V3 ca = bounds[pr.x].center, cb = bounds[pr.y].center;
-        // centre displacement, distance and phase in FP64; phase = theta0 + q0 pi/2
+        // centre displacement, distance and phase (reduced to [-pi, pi]) in FP64
         const double cx = ca.x - cb.x, cy = ca.y - cb.y, cz = ca.z - cb.z;
-        const double r0 = sqrt(cx * cx + cy * cy + cz * cz);
+        const double r0sqd = cx * cx + cy * cy + cz * cz, r0 = sqrt(r0sqd);
         const double ph0 = k * r0;
-        const double q0d = (ph0 * kTwoOverPi + kRound) - kRound;
-        const float theta0 = float(fma(-q0d, kHalfPiLo, fma(-q0d, kHalfPiHi, ph0)));
-        const int q0 = int(q0d - 4.0 * floor(q0d * 0.25));  // q0 mod 4, exact for |q0d| < 2^50
+        const double turns = (ph0 * kInvTwoPi + kRound) - kRound;
+        const float theta0 = float(fma(-turns, kTwoPiLo, fma(-turns, kTwoPi, ph0)));
         const float c[3] = {float(cx), float(cy), float(cz)};
-        const float r0f = float(r0);
-        // offset of the test panel's first vertex from the trial panel's, both about the centres
+        const float r0f = float(r0), r0sq = float(r0sqd);
+        // test point offsets about the test centre, trial offsets about the trial centre
         const float o0[3] = {float((A.v0[0] - ca.x) - (S.v0[0] - cb.x)), float((A.v0[1] - ca.y) - (S.v0[1] - cb.y)),
                              float((A.v0[2] - ca.z) - (S.v0[2] - cb.z))};
         const float ae1[3] = {float(A.e1[0]), float(A.e1[1]), float(A.e1[2])};
@@ -364,7 +372,10 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__res
         const float se2[3] = {float(S.e2[0]), float(S.e2[1]), float(S.e2[2])};
         const float ns[3] = {float(S.n[0]), float(S.n[1]), float(S.n[2])};
         const float nt[3] = {float(A.n[0]), float(A.n[1]), float(A.n[2])};
-        // trial edges against the test normal (the trial normal sees none of them)
+        // |e(y)|^2 coefficients and trial edges against the test normal
+        const float E11 = float(S.e1[0] * S.e1[0] + S.e1[1] * S.e1[1] + S.e1[2] * S.e1[2]);
+        const float E12 = float(S.e1[0] * S.e2[0] + S.e1[1] * S.e2[1] + S.e1[2] * S.e2[2]);
+        const float E22 = float(S.e2[0] * S.e2[0] + S.e2[1] * S.e2[1] + S.e2[2] * S.e2[2]);
         const float t1 = float(S.e1[0] * A.n[0] + S.e1[1] * A.n[1] + S.e1[2] * A.n[2]);
         const float t2 = float(S.e2[0] * A.n[0] + S.e2[1] * A.n[1] + S.e2[2] * A.n[2]);
         const float w4 = float(4.0 * A.area * S.area * kInvFourPi);
@@ -372,73 +383,77 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__res
 #pragma unroll
         for (int i = 0; i < 54; ++i)
             M[i] = 0.f;
-        bool bad = false;
+        float r2min = 3.4e38f;
 #pragma unroll 1
         for (int x = 0; x < NP; ++x) {
-            const float bx1 = cRuleF[4 * (RO + x) + 1], bx2 = cRuleF[4 * (RO + x) + 2];
-            // offset of test point x from the trial panel's first vertex, about the centres
-            float P[3];
+            const float bx1 = cRuleF[8 * (RO + x) + 1], bx2 = cRuleF[8 * (RO + x) + 2];
+            // P: test point minus the trial panel's first vertex, about the centres; CP = c + P
+            float P[3], CP[3], C2P[3];
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
+            for (int i = 0; i < 3; ++i) {
                 P[i] = fmaf(ae1[i], bx1, fmaf(ae2[i], bx2, o0[i]));
-            const float CP[3] = {c[0] + P[0], c[1] + P[1], c[2] + P[2]};
+                CP[i] = c[i] + P[i];
+                C2P[i] = c[i] + CP[i];
+            }
             const float psx = CP[0] * ns[0] + CP[1] * ns[1] + CP[2] * ns[2];
             const float qtx = -(CP[0] * nt[0] + CP[1] * nt[1] + CP[2] * nt[2]);
-            const float wx = cRuleF[4 * (RO + x) + 3] * w4;
-            float Sv[18];
+            // Delta = Ax + a1 b1 + a2 b2 + E11 b1^2 + 2 E12 b1 b2 + E22 b2^2
+            const float Ax = C2P[0] * P[0] + C2P[1] * P[1] + C2P[2] * P[2];
+            const float a1 = -2.f * (CP[0] * se1[0] + CP[1] * se1[1] + CP[2] * se1[2]);
+            const float a2 = -2.f * (CP[0] * se2[0] + CP[1] * se2[1] + CP[2] * se2[2]);
+            const float wx = cRuleF[8 * (RO + x) + 3] * w4;
+            float G[6], U[6], Q[6];
 #pragma unroll
-            for (int i = 0; i < 18; ++i)
-                Sv[i] = 0.f;
+            for (int i = 0; i < 6; ++i)
+                G[i] = U[i] = Q[i] = 0.f;
 #pragma unroll(NP <= 16 ? NP : 4)
             for (int y = 0; y < NP; ++y) {
-                const float b0 = cRuleF[4 * (RO + y)], b1 = cRuleF[4 * (RO + y) + 1], b2 = cRuleF[4 * (RO + y) + 2];
-                float d[3], fx[3];
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    d[i] = fmaf(-se1[i], b1, fmaf(-se2[i], b2, P[i]));
-                    fx[i] = c[i] + d[i];
-                }
-                const float r2 = fmaf(fx[0], fx[0], fmaf(fx[1], fx[1], fx[2] * fx[2]));
-                bad |= !(r2 > 0.f) || !isfinite(r2);
+                const float *ry = cRuleF + 8 * (RO + y);
+                const float b0 = ry[0], b1 = ry[1], b2 = ry[2];
+                const float delta = fmaf(E22, ry[6], fmaf(E12, ry[5], fmaf(E11, ry[4], fmaf(a2, b2, fmaf(a1, b1, Ax)))));
+                const float r2 = r0sq + delta;
+                r2min = fminf(r2min, r2);
                 const float rinv = rsqrtf(r2);
                 const float r = r2 * rinv;
-                const float delta = fmaf(d[0], fx[0] + c[0], fmaf(d[1], fx[1] + c[1], d[2] * (fx[2] + c[2])));
                 const float theta = fmaf(kf, __fdividef(delta, r + r0f), theta0);
-                const float qf = fmaf(theta, kTwoOverPiF, kRoundF);
-                const int q = q0 + __float_as_int(qf);
-                const float qn = qf - kRoundF;
-                const float th = fmaf(-qn, kHalfPiLoF, fmaf(-qn, kHalfPiHiF, theta));
+                const float qn = fmaf(theta, kInvTwoPiF, kRoundF) - kRoundF;
                 float sn, cs;
-                sinCosQuadrant(th, q, sn, cs);
+                __sincosf(fmaf(-qn, kTwoPiLoF, fmaf(-qn, kTwoPiHiF, theta)), &sn, &cs);
                 const float kr = kf * r;
-                const float sc = wx * cRuleF[4 * (RO + y) + 3] * rinv;
+                const float sc = (wx * ry[3]) * rinv;
                 const float gr = cs * sc, gi = -sn * sc;
                 const float rr = fmaf(-gi, kr, gr), ri = fmaf(gr, kr, gi);
                 const float rinv2 = rinv * rinv;
-                const float ps = psx * rinv2;
-                const float qt = fmaf(t1, b1, fmaf(t2, b2, qtx)) * rinv2;
-                const float val[6] = {gr, gi, rr * ps, ri * ps, rr * qt, ri * qt};
+                const float ur = rr * rinv2, ui = ri * rinv2;
+                const float qt = fmaf(t1, b1, fmaf(t2, b2, qtx));
+                const float qr = ur * qt, qi = ui * qt;
                 const float bs[3] = {b0, b1, b2};
 #pragma unroll
-                for (int kind = 0; kind < 3; ++kind)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        Sv[kind * 6 + 2 * j] = fmaf(val[2 * kind], bs[j], Sv[kind * 6 + 2 * j]);
-                        Sv[kind * 6 + 2 * j + 1] = fmaf(val[2 * kind + 1], bs[j], Sv[kind * 6 + 2 * j + 1]);
-                    }
+                for (int j = 0; j < 3; ++j) {
+                    G[2 * j] = fmaf(gr, bs[j], G[2 * j]);
+                    G[2 * j + 1] = fmaf(gi, bs[j], G[2 * j + 1]);
+                    U[2 * j] = fmaf(ur, bs[j], U[2 * j]);
+                    U[2 * j + 1] = fmaf(ui, bs[j], U[2 * j + 1]);
+                    Q[2 * j] = fmaf(qr, bs[j], Q[2 * j]);
+                    Q[2 * j + 1] = fmaf(qi, bs[j], Q[2 * j + 1]);
+                }
             }
-            const float bt[3] = {cRuleF[4 * (RO + x)], bx1, bx2};
+            const float bt[3] = {cRuleF[8 * (RO + x)], bx1, bx2};
 #pragma unroll
-            for (int kind = 0; kind < 3; ++kind)
+            for (int i = 0; i < 3; ++i) {
+                const float bp = bt[i] * psx;
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
-#pragma unroll
-                    for (int j = 0; j < 3; ++j) {
-                        M[kind * 18 + 2 * (3 * i + j)] = fmaf(bt[i], Sv[kind * 6 + 2 * j], M[kind * 18 + 2 * (3 * i + j)]);
-                        M[kind * 18 + 2 * (3 * i + j) + 1] =
-                            fmaf(bt[i], Sv[kind * 6 + 2 * j + 1], M[kind * 18 + 2 * (3 * i + j) + 1]);
-                    }
+                for (int j = 0; j < 6; ++j) {
+                    M[6 * i + j] = fmaf(bt[i], G[j], M[6 * i + j]);
+                    M[18 + 6 * i + j] = fmaf(bp, U[j], M[18 + 6 * i + j]);
+                    M[36 + 6 * i + j] = fmaf(bt[i], Q[j], M[36 + 6 * i + j]);
+                }
+            }
         }
+        bool bad = !(r2min > 0.f);
+#pragma unroll
+        for (int i = 0; i < 54; ++i)
+            bad |= !isfinite(M[i]);
         if (bad)
             flagError(error, kErrDistance);
         // stage this pair's moments and per-pair factors for the warp's record writes
@@ -1349,9 +1364,13 @@ void uploadRuleTables(cudaStream_t stream) {
         }
     }
     cudaCheck(cudaMemcpyToSymbolAsync(cRule, table, sizeof(table), 0, cudaMemcpyHostToDevice, stream), "rule upload");
-    static float tableF[kRulePoints * 4];
-    for (int i = 0; i < kRulePoints * 4; ++i)
-        tableF[i] = float(table[i]);
+    static float tableF[kRulePoints * 8];
+    for (int i = 0; i < kRulePoints; ++i) {
+        const double b1 = table[4 * i + 1], b2 = table[4 * i + 2];
+        const double v[8] = {table[4 * i], b1, b2, table[4 * i + 3], b1 * b1, 2 * b1 * b2, b2 * b2, 0.0};
+        for (int c = 0; c < 8; ++c)
+            tableF[8 * i + c] = float(v[c]);
+    }
     cudaCheck(cudaMemcpyToSymbolAsync(cRuleF, tableF, sizeof(tableF), 0, cudaMemcpyHostToDevice, stream),
               "rule upload");
     double g20[40];

@@ -11,6 +11,7 @@
 #include "device_types.cuh"
 #include "kernel_timer.hpp"
 
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 
@@ -131,6 +132,157 @@ __global__ void __launch_bounds__(512) panelKernel(R *LU, uint32_t N, uint32_t k
     }
 }
 
+// Panel factorisation with the panel resident in shared memory (rows
+// [k0, N) x jb columns). Rows stay in place: step j selects the pivot among
+// the rows not yet selected (largest |re|+|im|, lowest row on ties), every
+// thread eliminates column j from its own rows and takes its candidate for
+// column j+1 in the same pass, so a column costs one barrier. The selection
+// order is turned into the LAPACK interchange sequence at the end and the
+// panel is written back in interchanged order.
+template <class R>
+__global__ void __launch_bounds__(1024) panelSmemKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb, int *pivots,
+                                                        int *info) {
+    extern __shared__ __align__(16) unsigned char rawSmem[];
+    const uint32_t rows = N - k0;
+    C2<R> *P = reinterpret_cast<C2<R> *>(rawSmem);                 // [jb][rows]
+    int *arrangement = reinterpret_cast<int *>(P + size_t(jb) * rows);  // position -> local row
+    int *where = arrangement + rows;                                 // local row -> position
+    uint32_t taken = 0;  // bit r: this thread's r-th row (threadIdx.x + r * blockDim.x) is a pivot row
+    __shared__ R sBest[2][32];
+    __shared__ int sRow[2][32];
+    __shared__ int sSel[kPanel];
+    R *M = LU + size_t(blockIdx.x) * N * N * 2;
+    int *piv = pivots + size_t(blockIdx.x) * N;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+    // stage the panel: a batch of independent column loads in flight per thread
+    constexpr int kLoad = sizeof(R) == 8 ? 4 : 8;
+    for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) {
+        for (uint32_t q0 = 0; q0 < jb; q0 += kLoad) {
+            C2<R> v[kLoad];
+#pragma unroll
+            for (int t = 0; t < kLoad; ++t)
+                if (q0 + t < jb)
+                    v[t] = ld2(M + 2 * (size_t(k0 + q0 + t) * N + k0 + i));
+#pragma unroll
+            for (int t = 0; t < kLoad; ++t)
+                if (q0 + t < jb)
+                    P[size_t(q0 + t) * rows + i] = v[t];
+        }
+        arrangement[i] = int(i);
+        where[i] = int(i);
+    }
+    __syncthreads();
+    // candidates for column 0
+    R best = -1;
+    int bestRow = int(rows);
+    for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x) {
+        const C2<R> v = P[i];
+        R a = fabs(v.x) + fabs(v.y);
+        if (!(a >= R(0)))
+            a = 0;  // a NaN row competes as zero, so a pivot row always exists
+        if (a > best) {
+            best = a;
+            bestRow = int(i);
+        }
+    }
+    for (uint32_t j = 0; j < jb; ++j) {
+        const int buf = j & 1;
+        for (int off = 16; off > 0; off >>= 1) {
+            const R ob = __shfl_down_sync(0xffffffffu, best, off);
+            const int oi = __shfl_down_sync(0xffffffffu, bestRow, off);
+            if (ob > best || (ob == best && oi < bestRow)) {
+                best = ob;
+                bestRow = oi;
+            }
+        }
+        if (lane == 0) {
+            sBest[buf][warp] = best;
+            sRow[buf][warp] = bestRow;
+        }
+        __syncthreads();
+        // every warp reduces the warp candidates by shuffles (same result in every warp)
+        R pb = lane < warps ? sBest[buf][lane] : R(-1);
+        int p = lane < warps ? sRow[buf][lane] : int(rows);
+        for (int off = 16; off > 0; off >>= 1) {
+            const R ob = __shfl_xor_sync(0xffffffffu, pb, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, p, off);
+            if (ob > pb || (ob == pb && oi < p)) {
+                pb = ob;
+                p = oi;
+            }
+        }
+        if (threadIdx.x == 0) {
+            sSel[j] = p;
+            if (!(pb > 0) && *info == 0)
+                atomicCAS(info, 0, int(k0 + j) + 1);
+        }
+        const C2<R> d = P[size_t(j) * rows + p];
+        const R den = d.x * d.x + d.y * d.y;
+        const R rden = den > 0 ? R(1) / den : R(0);
+        const C2<R> inv = mk<R>(d.x * rden, -d.y * rden);
+        best = -1;
+        bestRow = int(rows);
+        uint32_t r = 0;
+        for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x, ++r) {
+            if (int(i) == p)
+                taken |= 1u << r;
+            if (taken >> r & 1u)
+                continue;
+            const C2<R> l = cmul<R>(P[size_t(j) * rows + i], inv);
+            P[size_t(j) * rows + i] = l;
+            // eliminate in chunks of columns: loads first, then updates and stores
+            constexpr int kChunk = sizeof(R) == 8 ? 4 : 8;
+            C2<R> next = mk<R>(0, 0);
+            for (uint32_t q0 = j + 1; q0 < jb; q0 += kChunk) {
+                C2<R> v[kChunk], pv[kChunk];
+#pragma unroll
+                for (int t = 0; t < kChunk; ++t)
+                    if (q0 + t < jb) {
+                        v[t] = P[size_t(q0 + t) * rows + i];
+                        pv[t] = P[size_t(q0 + t) * rows + p];
+                    }
+#pragma unroll
+                for (int t = 0; t < kChunk; ++t)
+                    if (q0 + t < jb) {
+                        csub<R>(v[t], l, pv[t]);
+                        P[size_t(q0 + t) * rows + i] = v[t];
+                    }
+                if (q0 == j + 1)
+                    next = v[0];
+            }
+            if (j + 1 < jb) {
+                R a = fabs(next.x) + fabs(next.y);
+                if (!(a >= R(0)))
+                    a = 0;
+                if (a > best) {
+                    best = a;
+                    bestRow = int(i);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // selection order -> interchange sequence (row k0+j swapped with row piv[k0+j])
+    if (threadIdx.x == 0)
+        for (uint32_t j = 0; j < jb; ++j) {
+            const int r = sSel[j], pj = where[r], rj = arrangement[j];
+            piv[k0 + j] = int(k0) + pj;
+            arrangement[j] = r;
+            arrangement[pj] = rj;
+            where[r] = int(j);
+            where[rj] = pj;
+        }
+    __syncthreads();
+    for (uint32_t q = 0; q < jb; ++q)
+        for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x)
+            st2(M + 2 * (size_t(k0 + q) * N + k0 + i), P[size_t(q) * rows + arrangement[i]]);
+}
+
+template <class R> size_t panelSmemBytes(uint32_t rows, uint32_t jb) {
+    return size_t(rows) * jb * sizeof(C2<R>) + size_t(rows) * 8;
+}
+constexpr size_t kPanelSmemLimit = 220 * 1024;
+
 // Row interchanges of the panel applied to columns outside it.
 template <class R> __global__ void swapKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb, const int *pivots) {
     const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -148,26 +300,45 @@ template <class R> __global__ void swapKernel(R *LU, uint32_t N, uint32_t k0, ui
     }
 }
 
-// U12 = L11^{-1} A12 (unit lower L11 of the panel), one thread per column.
-template <class R> __global__ void trsmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb) {
-    __shared__ C2<R> L[kPanel][kPanel];
+// U12 = L11^{-1} A12 (unit lower L11 of the panel) for 32 columns per CTA:
+// L11 and the 32x32 tile of A12 are staged in shared memory with coalesced
+// column reads; a warp solves one column at a time (lane = row, L11 row in
+// registers, the solved unknown broadcast by shuffle).
+template <class R> __global__ void __launch_bounds__(256) trsmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb) {
+    __shared__ C2<R> L[kPanel][kPanel + 1];
+    __shared__ C2<R> X[kPanel][kPanel + 1];  // [column][row]
     R *M = LU + size_t(blockIdx.y) * N * N * 2;
+    const uint32_t c0 = k0 + jb + blockIdx.x * kPanel;
+    const uint32_t cols = min(uint32_t(kPanel), N - c0);
     for (uint32_t e = threadIdx.x; e < jb * jb; e += blockDim.x) {
         const uint32_t r = e % jb, c = e / jb;
         L[r][c] = ld2(M + 2 * (size_t(k0 + c) * N + k0 + r));
     }
+    for (uint32_t e = threadIdx.x; e < cols * jb; e += blockDim.x) {
+        const uint32_t r = e % jb, c = e / jb;
+        X[c][r] = ld2(M + 2 * (size_t(c0 + c) * N + k0 + r));
+    }
     __syncthreads();
-    const uint32_t col = k0 + jb + blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= N)
-        return;
-    R *C = M + 2 * size_t(col) * N;
-    C2<R> x[kPanel];
-    for (uint32_t i = 0; i < jb; ++i) {
-        C2<R> v = ld2(C + 2 * (k0 + i));
-        for (uint32_t m = 0; m < i; ++m)
-            csub<R>(v, L[i][m], x[m]);
-        x[i] = v;
-        st2(C + 2 * (k0 + i), v);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    C2<R> row[kPanel];
+#pragma unroll
+    for (int m = 0; m < kPanel; ++m)
+        row[m] = (lane < int(jb) && m < int(jb)) ? L[lane][m] : mk<R>(0, 0);
+    for (uint32_t c = warp; c < cols; c += blockDim.x >> 5) {
+        C2<R> v = lane < int(jb) ? X[c][lane] : mk<R>(0, 0);
+#pragma unroll
+        for (int m = 0; m < kPanel; ++m) {
+            const C2<R> xm = mk<R>(__shfl_sync(0xffffffffu, v.x, m), __shfl_sync(0xffffffffu, v.y, m));
+            if (lane > m)
+                csub<R>(v, row[m], xm);
+        }
+        if (lane < int(jb))
+            X[c][lane] = v;
+    }
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < cols * jb; e += blockDim.x) {
+        const uint32_t r = e % jb, c = e / jb;
+        st2(M + 2 * (size_t(c0 + c) * N + k0 + r), X[c][r]);
     }
 }
 
@@ -227,9 +398,12 @@ template <class R> __global__ void __launch_bounds__(256) gemmKernel(R *LU, uint
 }
 
 // Forward / back substitution of one right-hand side per CTA, with the
-// vector staged in shared memory.
+// vector staged in shared memory. Blocks of 32 unknowns: warp 0 loads the
+// 32x32 diagonal block into registers (independent coalesced loads, lane =
+// row) and solves it with shuffles; then every thread updates its rows with
+// the block's 32 columns.
 template <class R>
-__global__ void __launch_bounds__(256) solveKernel(const R *LU, const int *pivots, uint32_t N, uint32_t E, R *X) {
+__global__ void __launch_bounds__(sizeof(R) == 8 ? 256 : 512) solveKernel(const R *LU, const int *pivots, uint32_t N, uint32_t E, R *X) {
     extern __shared__ __align__(16) unsigned char rawSmem[];
     C2<R> *x = reinterpret_cast<C2<R> *>(rawSmem);
     const uint32_t e = blockIdx.x, f = blockIdx.y;
@@ -250,41 +424,59 @@ __global__ void __launch_bounds__(256) solveKernel(const R *LU, const int *pivot
         }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const C2<R> zero = mk<R>(0, 0);
+    // forward: unit lower triangle
     for (uint32_t k = 0; k < N; k += 32) {
         const uint32_t kb = min(32u, N - k);
         if (warp == 0) {
-            C2<R> mine = lane < int(kb) ? x[k + lane] : mk<R>(0, 0);
-            for (uint32_t m = 0; m < kb; ++m) {
+            C2<R> L[32];
+#pragma unroll
+            for (int m = 0; m < 32; ++m)
+                L[m] = (m < int(kb) && lane < int(kb)) ? ld2(M + 2 * (size_t(k + m) * N + k + lane)) : zero;
+            C2<R> mine = lane < int(kb) ? x[k + lane] : zero;
+#pragma unroll
+            for (int m = 0; m < 32; ++m) {
                 const C2<R> xm = mk<R>(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
-                if (lane > int(m) && lane < int(kb))
-                    csub<R>(mine, ld2(M + 2 * (size_t(k + m) * N + k + lane)), xm);
+                if (lane > m)
+                    csub<R>(mine, L[m], xm);
             }
             if (lane < int(kb))
                 x[k + lane] = mine;
         }
         __syncthreads();
-        for (uint32_t i = k + kb + threadIdx.x; i < N; i += blockDim.x) {
-            C2<R> v = x[i];
-            for (uint32_t m = 0; m < kb; ++m)
-                csub<R>(v, ld2(M + 2 * (size_t(k + m) * N + i)), x[k + m]);
-            x[i] = v;
+        if (kb == 32) {
+            for (uint32_t i = k + 32 + threadIdx.x; i < N; i += blockDim.x) {
+                C2<R> v = x[i];
+#pragma unroll
+                for (int m = 0; m < 32; ++m)
+                    csub<R>(v, ld2(M + 2 * (size_t(k + m) * N + i)), x[k + m]);
+                x[i] = v;
+            }
         }
         __syncthreads();
     }
+    // backward: upper triangle with its diagonal
     const uint32_t blocks = (N + 31) / 32;
     for (uint32_t bi = blocks; bi-- > 0;) {
         const uint32_t k = bi * 32, kb = min(32u, N - k);
         if (warp == 0) {
-            C2<R> mine = lane < int(kb) ? x[k + lane] : mk<R>(0, 0);
-            for (int m = int(kb) - 1; m >= 0; --m) {
-                if (lane == m) {
-                    const C2<R> d = ld2(M + 2 * (size_t(k + m) * N + k + m));
-                    const R den = d.x * d.x + d.y * d.y;
-                    mine = mk<R>((mine.x * d.x + mine.y * d.y) / den, (mine.y * d.x - mine.x * d.y) / den);
+            C2<R> U[32];
+#pragma unroll
+            for (int m = 0; m < 32; ++m)
+                U[m] = (m < int(kb) && lane < int(kb)) ? ld2(M + 2 * (size_t(k + m) * N + k + lane)) : zero;
+            C2<R> mine = lane < int(kb) ? x[k + lane] : zero;
+#pragma unroll
+            for (int m = 31; m >= 0; --m) {
+                if (m < int(kb)) {
+                    if (lane == m) {
+                        const C2<R> d = U[m];
+                        const R den = d.x * d.x + d.y * d.y;
+                        mine = mk<R>((mine.x * d.x + mine.y * d.y) / den, (mine.y * d.x - mine.x * d.y) / den);
+                    }
+                    const C2<R> xm = mk<R>(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
+                    if (lane < m)
+                        csub<R>(mine, U[m], xm);
                 }
-                const C2<R> xm = mk<R>(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
-                if (lane < m)
-                    csub<R>(mine, ld2(M + 2 * (size_t(k + m) * N + k + lane)), xm);
             }
             if (lane < int(kb))
                 x[k + lane] = mine;
@@ -292,8 +484,14 @@ __global__ void __launch_bounds__(256) solveKernel(const R *LU, const int *pivot
         __syncthreads();
         for (uint32_t i = threadIdx.x; i < k; i += blockDim.x) {
             C2<R> v = x[i];
-            for (uint32_t m = 0; m < kb; ++m)
-                csub<R>(v, ld2(M + 2 * (size_t(k + m) * N + i)), x[k + m]);
+            if (kb == 32) {
+#pragma unroll
+                for (int m = 0; m < 32; ++m)
+                    csub<R>(v, ld2(M + 2 * (size_t(k + m) * N + i)), x[k + m]);
+            } else {
+                for (uint32_t m = 0; m < kb; ++m)
+                    csub<R>(v, ld2(M + 2 * (size_t(k + m) * N + i)), x[k + m]);
+            }
             x[i] = v;
         }
         __syncthreads();
@@ -377,13 +575,21 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
     if (!attr) {
         check(cudaFuncSetAttribute(gemmKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gemmSmem)),
               "gemm smem attribute");
+        check(cudaFuncSetAttribute(panelSmemKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   int(kPanelSmemLimit)),
+              "panel smem attribute");
         attr = true;
     }
     for (uint32_t k0 = 0; k0 < N; k0 += kPanel) {
         const uint32_t jb = min(uint32_t(kPanel), N - k0);
         {
             TimedScope s(timer, "lu_panel", stream);
-            panelKernel<R><<<B, 512, 0, stream>>>(LU, N, k0, jb, pivots, info);
+            const size_t bytes = panelSmemBytes<R>(N - k0, jb);
+            if (bytes <= kPanelSmemLimit)
+                panelSmemKernel<R><<<B, std::min(1024u, (N - k0 + 31) / 32 * 32), bytes, stream>>>(LU, N, k0, jb,
+                                                                                                   pivots, info);
+            else
+                panelKernel<R><<<B, 512, 0, stream>>>(LU, N, k0, jb, pivots, info);
         }
         {
             TimedScope s(timer, "lu_swap", stream);
@@ -393,7 +599,7 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
         if (rest) {
             {
                 TimedScope s(timer, "lu_trsm", stream);
-                trsmKernel<R><<<dim3((rest + 127) / 128, B), 128, 0, stream>>>(LU, N, k0, jb);
+                trsmKernel<R><<<dim3((rest + kPanel - 1) / kPanel, B), 256, 0, stream>>>(LU, N, k0, jb);
             }
             TimedScope s(timer, "lu_gemm", stream);
             gemmKernel<R><<<dim3((rest + 63) / 64, (rest + 63) / 64, B), 256, gemmSmem, stream>>>(LU, N, k0, jb);
@@ -414,7 +620,7 @@ template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32
         attr = smem;
     }
     TimedScope s(timer, "lu_solve", stream);
-    solveKernel<R><<<dim3(E, B), 256, smem, stream>>>(LU, pivots, N, E, x);
+    solveKernel<R><<<dim3(E, B), sizeof(R) == 8 ? 256 : 512, smem, stream>>>(LU, pivots, N, E, x);
     check(cudaGetLastError(), "triangular solve launch");
 }
 
