@@ -287,73 +287,88 @@ __device__ __forceinline__ void sinCosQuadrant(float x, int q, float &sn, float 
 }
 
 
-template <int NP>
-__global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__restrict__ panels, const Bounds *__restrict__ bounds,
-                                                             uint32_t T, const double *__restrict__ ks,
-                                                             const uint2 *__restrict__ bins,
-                                                             const uint32_t *__restrict__ binCounts, size_t binCapacity,
-                                                             int bin, float *__restrict__ records, int *error);
-
-// Record element o of an unordered pair (0..11 forward block, 12..23
-// reverse block; see pairRecordValue) from its staged FP32 row: moments
-// MG, MP, MQ (54), sum of MG (2), k n_t.n_s (1), curl_ti.curl_sj (9).
-constexpr int kStageMG = 0, kStageMP = 18, kStageMQ = 36, kStageGsum = 54, kStageKnn = 56, kStageCurl = 57,
-              kStageStride = 67;  // 66 values, odd stride: conflict-free rows
-
-__device__ __forceinline__ void stagedRecordValue(int o, const float *m, float invk, float &re, float &im) {
-    const bool reverse = o >= 12;
-    const int e = reverse ? o - 12 : o;
-    const float *MG = m + kStageMG;
-    const float *X = m + (reverse ? kStageMQ : kStageMP);
-    const float *Y = m + (reverse ? kStageMP : kStageMQ);
-    if (e < 9) {
-        const int row = e / 3, col = e % 3;
-        const int i = reverse ? col : row, j = reverse ? row : col, c = 2 * (3 * i + j);
-        const float knn = m[kStageKnn], curl = m[kStageCurl + 3 * i + j] * invk;
-        re = fmaf(m[kStageGsum + 1], curl, fmaf(-knn, MG[c + 1], -X[c]));
-        im = fmaf(-m[kStageGsum], curl, fmaf(knn, MG[c], -X[c + 1]));
-    } else {
-        const int a = e - 9;
-        float sgr = 0.f, sgi = 0.f, syr = 0.f, syi = 0.f;
+// Both records of an unordered regular pair (forward: test A, trial S;
+// reverse: test S, trial A) from its FP32 moments (the layout and formulas of
+// pairRecordValue), stored straight into the record planes. ps = plane stride.
+__device__ __forceinline__ void storePairRecords(const float (&M)[54], const MixedPanel *__restrict__ pa,
+                                                 const MixedPanel *__restrict__ pb, float k, float invk, float *fwd,
+                                                 float *rev, size_t ps, bool &nonFinite) {
+    const float *MG = M, *MP = M + 18, *MQ = M + 36;
+    const float4 na = pa->n, nb = pb->n;
+    const float knn = k * (na.x * nb.x + na.y * nb.y + na.z * nb.z);
+    float gre = 0.f, gim = 0.f;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        gre += MG[2 * c];
+        gim += MG[2 * c + 1];
+    }
+    gre *= invk;
+    gim *= invk;
+    const float4 ca[3] = {pa->curl[0], pa->curl[1], pa->curl[2]}, cs[3] = {pb->curl[0], pb->curl[1], pb->curl[2]};
+    float check = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)      // A's local vertex
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {  // S's local vertex
+            const float curl = ca[i].x * cs[j].x + ca[i].y * cs[j].y + ca[i].z * cs[j].z;
+            const int m = 2 * (3 * i + j);
+            // forward element (row i, col j); reverse element (row j, col i)
+            const float fr = fmaf(gim, curl, fmaf(-knn, MG[m + 1], -MP[m]));
+            const float fi = fmaf(-gre, curl, fmaf(knn, MG[m], -MP[m + 1]));
+            const float rr = fmaf(gim, curl, fmaf(-knn, MG[m + 1], -MQ[m]));
+            const float ri = fmaf(-gre, curl, fmaf(knn, MG[m], -MQ[m + 1]));
+            *reinterpret_cast<float2 *>(fwd + j * ps + 2 * i) = make_float2(fr, fi);
+            *reinterpret_cast<float2 *>(rev + i * ps + 2 * j) = make_float2(rr, ri);
+            check += fabsf(fr) + fabsf(fi) + fabsf(rr) + fabsf(ri);
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        // forward rhs row a (A's vertex): sum over S's vertices; reverse rhs row a (S's vertex): over A's
+        float fgr = 0.f, fgi = 0.f, fyr = 0.f, fyi = 0.f, rgr = 0.f, rgi = 0.f, ryr = 0.f, ryi = 0.f;
 #pragma unroll
         for (int b = 0; b < 3; ++b) {
-            const int c = reverse ? 2 * (3 * b + a) : 2 * (3 * a + b);
-            sgr += MG[c];
-            sgi += MG[c + 1];
-            syr += Y[c];
-            syi += Y[c + 1];
+            const int mf = 2 * (3 * a + b), mr = 2 * (3 * b + a);
+            fgr += MG[mf];
+            fgi += MG[mf + 1];
+            fyr += MQ[mf];
+            fyi += MQ[mf + 1];
+            rgr += MG[mr];
+            rgi += MG[mr + 1];
+            ryr += MP[mr];
+            ryi += MP[mr + 1];
         }
-        re = fmaf(-syi, invk, -sgr);
-        im = fmaf(syr, invk, -sgi);
+        const float2 fv = make_float2(fmaf(-fyi, invk, -fgr), fmaf(fyr, invk, -fgi));
+        const float2 rv = make_float2(fmaf(-ryi, invk, -rgr), fmaf(ryr, invk, -rgi));
+        *reinterpret_cast<float2 *>(fwd + 3 * ps + 2 * a) = fv;
+        *reinterpret_cast<float2 *>(rev + 3 * ps + 2 * a) = rv;
+        check += fabsf(fv.x) + fabsf(fv.y) + fabsf(rv.x) + fabsf(rv.y);
     }
+    nonFinite |= !isfinite(check);
 }
 
 template <int NP>
-__global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__restrict__ panels, const Bounds *__restrict__ bounds,
-                                                             uint32_t T, const double *__restrict__ ks,
+__global__ void __launch_bounds__(128, 4) regularMixedKernel(const MixedPanel *__restrict__ mpanels,
+                                                             const Bounds *__restrict__ bounds, uint32_t T,
+                                                             const double *__restrict__ ks,
                                                              const uint2 *__restrict__ bins,
                                                              const uint32_t *__restrict__ binCounts, size_t binCapacity,
                                                              int bin, float *__restrict__ records, int *error) {
-    __shared__ float sStage[4][32][kStageStride];
-    __shared__ uint2 sPair[4][32];
     constexpr int RO = ruleOffset<NP>();
     constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52: adding and subtracting rounds to an integer
     constexpr double kTwoPi = 6.283185307179586, kTwoPiLo = 2.4492935982947064e-16, kInvTwoPi = 0.15915494309189535;
     constexpr float kRoundF = 12582912.f;  // 1.5 * 2^23, the same for FP32
     constexpr float kTwoPiHiF = 6.28318548f, kTwoPiLoF = -1.74845553e-7f, kInvTwoPiF = 0.159154943f;
     const int f = blockIdx.y;
-    const double k = ks[f], invk = 1.0 / k;
-    const float kf = float(k), invkf = float(invk);
+    const double k = ks[f];
+    const float kf = float(k), invkf = float(1.0 / k);
     const uint32_t count = binCounts[f * kBins + bin];
     const uint2 *list = bins + (size_t(f) * kBins + bin) * binCapacity;
     float *rec = records + size_t(f) * T * T * kRecordDoubles;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (uint32_t base = blockIdx.x * blockDim.x + warp * 32; base < count; base += gridDim.x * blockDim.x) {
-      const uint32_t p = base + lane;
-      if (p < count) {
+    const size_t planeStride = size_t(T) * T * 6;
+    bool bad = false, nonFinite = false;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
         const uint2 pr = list[p];
-        const DPanel &A = panels[pr.x];
-        const DPanel &S = panels[pr.y];
+        const MixedPanel &A = mpanels[pr.x], &S = mpanels[pr.y];
         const V3 ca = bounds[pr.x].center, cb = bounds[pr.y].center;
         // centre displacement, distance and phase (reduced to [-pi, pi]) in FP64
         const double cx = ca.x - cb.x, cy = ca.y - cb.y, cz = ca.z - cb.z;
@@ -363,22 +378,18 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__res
         const float theta0 = float(fma(-turns, kTwoPiLo, fma(-turns, kTwoPi, ph0)));
         const float c[3] = {float(cx), float(cy), float(cz)};
         const float r0f = float(r0), r0sq = float(r0sqd);
-        // test point offsets about the test centre, trial offsets about the trial centre
-        const float o0[3] = {float((A.v0[0] - ca.x) - (S.v0[0] - cb.x)), float((A.v0[1] - ca.y) - (S.v0[1] - cb.y)),
-                             float((A.v0[2] - ca.z) - (S.v0[2] - cb.z))};
-        const float ae1[3] = {float(A.e1[0]), float(A.e1[1]), float(A.e1[2])};
-        const float ae2[3] = {float(A.e2[0]), float(A.e2[1]), float(A.e2[2])};
-        const float se1[3] = {float(S.e1[0]), float(S.e1[1]), float(S.e1[2])};
-        const float se2[3] = {float(S.e2[0]), float(S.e2[1]), float(S.e2[2])};
-        const float ns[3] = {float(S.n[0]), float(S.n[1]), float(S.n[2])};
-        const float nt[3] = {float(A.n[0]), float(A.n[1]), float(A.n[2])};
+        // test first vertex minus trial first vertex, about the centres
+        const float4 aOff = A.offset, sOff = S.offset, aE1 = A.e1, aE2 = A.e2, sE1 = S.e1, sE2 = S.e2, aN = A.n,
+                     sN = S.n;
+        const float o0[3] = {aOff.x - sOff.x, aOff.y - sOff.y, aOff.z - sOff.z};
+        const float ae1[3] = {aE1.x, aE1.y, aE1.z}, ae2[3] = {aE2.x, aE2.y, aE2.z};
+        const float se1[3] = {sE1.x, sE1.y, sE1.z}, se2[3] = {sE2.x, sE2.y, sE2.z};
+        const float ns[3] = {sN.x, sN.y, sN.z}, nt[3] = {aN.x, aN.y, aN.z};
         // |e(y)|^2 coefficients and trial edges against the test normal
-        const float E11 = float(S.e1[0] * S.e1[0] + S.e1[1] * S.e1[1] + S.e1[2] * S.e1[2]);
-        const float E12 = float(S.e1[0] * S.e2[0] + S.e1[1] * S.e2[1] + S.e1[2] * S.e2[2]);
-        const float E22 = float(S.e2[0] * S.e2[0] + S.e2[1] * S.e2[1] + S.e2[2] * S.e2[2]);
-        const float t1 = float(S.e1[0] * A.n[0] + S.e1[1] * A.n[1] + S.e1[2] * A.n[2]);
-        const float t2 = float(S.e2[0] * A.n[0] + S.e2[1] * A.n[1] + S.e2[2] * A.n[2]);
-        const float w4 = float(4.0 * A.area * S.area * kInvFourPi);
+        const float E11 = sE1.w, E12 = sN.w, E22 = sE2.w;
+        const float t1 = se1[0] * nt[0] + se1[1] * nt[1] + se1[2] * nt[2];
+        const float t2 = se2[0] * nt[0] + se2[1] * nt[1] + se2[2] * nt[2];
+        const float w4 = 4.f * aOff.w * sOff.w * float(kInvFourPi);
         float M[54];
 #pragma unroll
         for (int i = 0; i < 54; ++i)
@@ -450,52 +461,14 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const DPanel *__res
                 }
             }
         }
-        bool bad = !(r2min > 0.f);
-#pragma unroll
-        for (int i = 0; i < 54; ++i)
-            bad |= !isfinite(M[i]);
-        if (bad)
-            flagError(error, kErrDistance);
-        // stage this pair's moments and per-pair factors for the warp's record writes
-        float *row = sStage[warp][lane];
-        float gre = 0.f, gim = 0.f;
-#pragma unroll
-        for (int c = 0; c < 54; ++c)
-            row[c] = M[c];
-#pragma unroll
-        for (int c = 0; c < 9; ++c) {
-            gre += M[2 * c];
-            gim += M[2 * c + 1];
-        }
-        row[kStageGsum] = gre;
-        row[kStageGsum + 1] = gim;
-        row[kStageKnn] = float(k * (A.n[0] * S.n[0] + A.n[1] * S.n[1] + A.n[2] * S.n[2]));
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j)
-                row[kStageCurl + 3 * i + j] = float(A.curl[3 * i] * S.curl[3 * j] + A.curl[3 * i + 1] * S.curl[3 * j + 1] +
-                                                    A.curl[3 * i + 2] * S.curl[3 * j + 2]);
-        sPair[warp][lane] = pr;
-      }
-      __syncwarp();
-      // 24 record elements per pair, written by consecutive lanes (contiguous columns)
-      const uint32_t valid = min(32u, count - base);
-      bool nonFinite = false;
-      for (uint32_t idx = lane; idx < valid * 24; idx += 32) {
-          const uint32_t j = idx / 24;
-          const int o = int(idx % 24);
-          const uint2 pr = sPair[warp][j];
-          float re, im;
-          stagedRecordValue(o, sStage[warp][j], invkf, re, im);
-          nonFinite |= !isfinite(re) || !isfinite(im);
-          const size_t slot = o < 12 ? size_t(pr.y) * T + pr.x : size_t(pr.x) * T + pr.y;
-          *reinterpret_cast<float2 *>(rec + recordOffset(T, slot, o < 12 ? o : o - 12)) = make_float2(re, im);
-      }
-      if (nonFinite)
-          flagError(error, kErrNonFinite);
-      __syncwarp();
+        bad |= !(r2min > 0.f);
+        storePairRecords(M, &A, &S, kf, invkf, rec + (size_t(pr.y) * T + pr.x) * 6,
+                         rec + (size_t(pr.x) * T + pr.y) * 6, planeStride, nonFinite);
     }
+    if (bad)
+        flagError(error, kErrDistance);
+    if (nonFinite)
+        flagError(error, kErrNonFinite);
 }
 
 // Sorts unordered regular pairs of each frequency into rule bins.
@@ -1298,7 +1271,7 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
     TimedScope scope(timer, mixed ? mixedNames[bin] : names[bin], stream);
     if (mixed) {
         const dim3 grid(unsigned(smCount() * 16), B);
-        regularMixedKernel<NP><<<grid, 128, 0, stream>>>(g.panels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
+        regularMixedKernel<NP><<<grid, 128, 0, stream>>>(g.mixedPanels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
                                                          ws.binCapacity, bin, static_cast<float *>(ws.records),
                                                          error);
     } else {

@@ -62,6 +62,29 @@ struct TouchingJob {
     uint8_t permTest[3], permTrial[3], pad[2];
 };
 
+// FP32 view of a panel for the mixed form (112 B): first vertex minus the
+// bounding-ball centre and the area, the edges e1 = v1 - v0, e2 = v2 - v0
+// with |e1|^2 and |e2|^2, the normal with e1.e2, and the P1 basis curls.
+struct MixedPanel {
+    float4 offset, e1, e2, n;
+    float4 curl[3];
+};
+
+inline MixedPanel makeMixedPanel(const DPanel &p, const Bounds &b) {
+    MixedPanel m{};
+    const double o[3] = {p.v0[0] - b.center.x, p.v0[1] - b.center.y, p.v0[2] - b.center.z};
+    const double e11 = p.e1[0] * p.e1[0] + p.e1[1] * p.e1[1] + p.e1[2] * p.e1[2];
+    const double e22 = p.e2[0] * p.e2[0] + p.e2[1] * p.e2[1] + p.e2[2] * p.e2[2];
+    const double e12 = p.e1[0] * p.e2[0] + p.e1[1] * p.e2[1] + p.e1[2] * p.e2[2];
+    m.offset = make_float4(float(o[0]), float(o[1]), float(o[2]), float(p.area));
+    m.e1 = make_float4(float(p.e1[0]), float(p.e1[1]), float(p.e1[2]), float(e11));
+    m.e2 = make_float4(float(p.e2[0]), float(p.e2[1]), float(p.e2[2]), float(e22));
+    m.n = make_float4(float(p.n[0]), float(p.n[1]), float(p.n[2]), float(e12));
+    for (int i = 0; i < 3; ++i)
+        m.curl[i] = make_float4(float(p.curl[3 * i]), float(p.curl[3 * i + 1]), float(p.curl[3 * i + 2]), 0.f);
+    return m;
+}
+
 struct AssemblyGeometry {
     const DPanel *panels;
     const Bounds *bounds;
@@ -79,7 +102,9 @@ struct AssemblyGeometry {
     double nearTolerance;
     uint32_t minimumDegree, singularOrder;
     const float4 *singularTable;    // mixed-form touching tuples (buildSingularTable)
+    const MixedPanel *mixedPanels;  // FP32 panel view of the mixed form
 };
+
 
 // Quadrature tables copied to __constant__ memory at first use.
 void uploadRuleTables(cudaStream_t stream);

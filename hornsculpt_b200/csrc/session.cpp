@@ -192,8 +192,12 @@ void Session::uploadGeometry() {
     for (size_t v = 0; v < N; ++v)
         scale[v] = 1.0 / space_.lumpedMass[v];
     const cudaStream_t s = stream();
+    std::vector<MixedPanel> mixedPanels(T);
+    for (size_t t = 0; t < T; ++t)
+        mixedPanels[t] = makeMixedPanel(panels[t], bounds[t]);
     upload(dPanels_, panels, s);
     upload(dBounds_, bounds, s);
+    upload(dMixedPanels_, mixedPanels, s);
     upload(dIncOffsets_, space_.incOffsets, s);
     upload(dIncPanel_, space_.incPanel, s);
     upload(dIncLocal_, space_.incLocal, s);
@@ -328,7 +332,7 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O) {
     dDegrees_.ensure(B * 4);
     dWork32_.ensure(B * E * N * 8);
     size_t bytes = 0;
-    for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_, &dMass_,
+    for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dMixedPanels_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_, &dMass_,
                                   &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_, &dRecords_, &dColumns_,
                                   &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
                                   &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_,
@@ -448,7 +452,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
                          dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
                          o.near_relative_tolerance,
-                         o.quadrature_order, o.singular_order, dSingularTable_.as<float4>()};
+                         o.quadrature_order, o.singular_order, dSingularTable_.as<float4>(),
+                         dMixedPanels_.as<MixedPanel>()};
     double maxEdge = 0;
     for (const auto &p : space_.panels)
         maxEdge = std::max(maxEdge, p.maxEdge);
@@ -755,7 +760,8 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
                          dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
                          o.near_relative_tolerance,
-                         o.quadrature_order, o.singular_order, dSingularTable_.as<float4>()};
+                         o.quadrature_order, o.singular_order, dSingularTable_.as<float4>(),
+                         dMixedPanels_.as<MixedPanel>()};
     AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
                          dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
     assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), 1, 1, ws, dA_.as<double>(),

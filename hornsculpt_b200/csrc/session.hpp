@@ -83,7 +83,7 @@ class Session {
     KernelTimer timer_;
 
     // geometry (frequency independent)
-    DeviceBuffer dPanels_, dBounds_, dIncOffsets_, dIncPanel_, dIncLocal_, dRowScale_, dMass_, dError_;
+    DeviceBuffer dPanels_, dBounds_, dMixedPanels_, dIncOffsets_, dIncPanel_, dIncLocal_, dRowScale_, dMass_, dError_;
     // plan cache
     bool planValid_ = false;
     hs_numerics planNumerics_{};
