@@ -234,7 +234,7 @@ __device__ __forceinline__ void mixedValues(double dx, double dy, double dz, flo
     const double turns = (ph * kInvTwoPi + 6755399441055744.0) - 6755399441055744.0;  // round to nearest
     const double th = fma(-turns, kTwoPiLo, fma(-turns, kTwoPiHi, ph));
     float sn, cs;
-    sincosf(float(th), &sn, &cs);
+    __sincosf(float(th), &sn, &cs);  // th in [-pi, pi]: hardware sin/cos, absolute error about 4e-7
     const float kr = float(ph);
     const float sc = w * rinv;
     const float gr = cs * sc, gi = -sn * sc;
@@ -270,22 +270,6 @@ __device__ __forceinline__ void mixedValues(double dx, double dy, double dz, flo
 // constant over the trial panel and the adjoint one affine in b1, b2.
 // Rule table per point: b0, b1, b2, w, b1^2, 2 b1 b2, b2^2, 0.
 __constant__ float cRuleF[kRulePoints * 8];
-
-// (sin, cos) of x + q*pi/2 for |x| <= pi/4 (plus a small margin).
-__device__ __forceinline__ void sinCosQuadrant(float x, int q, float &sn, float &cs) {
-    const float x2 = x * x;
-    // Taylor series of sin and cos truncated after x^9 and x^10
-    const float ps = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, 2.75573192e-6f, -1.98412698e-4f), 8.33333333e-3f),
-                                   -1.66666667e-1f), 1.f);
-    const float pc = fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, fmaf(x2, -2.75573192e-7f, 2.48015873e-5f),
-                                                     -1.38888889e-3f), 4.16666667e-2f), -0.5f), 1.f);
-    const float s = x * ps;
-    const bool odd = q & 1;
-    const float a = odd ? pc : s, b = odd ? s : pc;
-    sn = __int_as_float(__float_as_int(a) ^ ((q & 2) << 30));
-    cs = __int_as_float(__float_as_int(b) ^ (((q + 1) & 2) << 30));
-}
-
 
 // Both records of an unordered regular pair (forward: test A, trial S;
 // reverse: test S, trial A) from its FP32 moments (the layout and formulas of
@@ -685,15 +669,16 @@ __global__ void __launch_bounds__(128) singularKernel(const DPanel *__restrict__
 // panels the shared edges are merged and their coefficients are differences
 // formed in FP64, so l keeps FP32 relative accuracy where the two points
 // nearly meet. Touching pairs have k*r <= 2 k h, so the FP32 phase needs no
-// FP64 help. Moments accumulate in canonical order and are permuted back to
-// local order once per job.
+// FP64 help; it is reduced to [-pi, pi] for the hardware sin/cos (absolute
+// error about 4e-7). Moments accumulate in canonical order and are permuted
+// back to local order once per job.
 __global__ void __launch_bounds__(128) singularMixedKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                            const TouchingJob *__restrict__ jobs, uint32_t jobCount,
                                                            const double *__restrict__ ks,
                                                            const float4 *__restrict__ table, uint32_t order,
                                                            float *__restrict__ records, int *error) {
-    constexpr float kRoundF = 12582912.f, kHalfPiHiF = 1.57079637f, kHalfPiLoF = -4.37113883e-8f,
-                    kTwoOverPiF = 0.636619772f;
+    constexpr float kRoundF = 12582912.f, kTwoPiHiF = 6.28318548f, kTwoPiLoF = -1.74845553e-7f,
+                    kInvTwoPiF = 0.159154943f;
     const uint32_t jobIndex = blockIdx.x * 4 + (threadIdx.x >> 5);
     const unsigned lane = threadIdx.x & 31;
     if (jobIndex >= jobCount)
@@ -749,15 +734,16 @@ __global__ void __launch_bounds__(128) singularMixedKernel(const DPanel *__restr
         bad |= !(lr2 > 0.f) || !isfinite(lr2);
         const float linv = rsqrtf(lr2), llen = lr2 * linv;
         const float pw = q2.z * w4;
+#pragma unroll 4
         for (uint32_t ri = 0; ri < order; ++ri) {
-            const float4 rad = radial[ri];  // (r, r^3 w_r)
+            const float4 rad = radial[ri];  // (r, r^3 w_r, 1/r, 1 - r)
             const float r = rad.x;
             // sample at radial fraction r: displacement r*l, distance r*|l|
-            const float rinv = linv * __frcp_rn(r), kr = kf * (llen * r);
-            const float qf = fmaf(kr, kTwoOverPiF, kRoundF);
-            const float qn = qf - kRoundF;
+            const float rinv = linv * rad.z, kr = kf * (llen * r);
+            // phase reduced to [-pi, pi], hardware sin/cos (absolute error about 4e-7)
+            const float qn = fmaf(kr, kInvTwoPiF, kRoundF) - kRoundF;
             float sn, cs;
-            sinCosQuadrant(fmaf(-qn, kHalfPiLoF, fmaf(-qn, kHalfPiHiF, kr)), __float_as_int(qf), sn, cs);
+            __sincosf(fmaf(-qn, kTwoPiLoF, fmaf(-qn, kTwoPiHiF, kr)), &sn, &cs);
             const float sc = pw * rad.y * rinv;
             const float gr = cs * sc, gi = -sn * sc;
             g[0] += gr;
@@ -768,8 +754,8 @@ __global__ void __launch_bounds__(128) singularMixedKernel(const DPanel *__restr
             const float ps = ps1 * inv, qt = qt1 * inv;
             const float ar = fmaf(-rr, ps, -knn * gi), ai = fmaf(-ri2, ps, knn * gr);
             const float br = fmaf(-ri2 * qt, invkf, -gr), bi = fmaf(rr * qt, invkf, -gi);
-            const float bt[3] = {fmaf(r, pt[0], 1.f - r), r * pt[1], r * pt[2]};
-            const float bs[3] = {fmaf(r, pq[0], 1.f - r), r * pq[1], r * pq[2]};
+            const float bt[3] = {fmaf(r, pt[0], rad.w), r * pt[1], r * pt[2]};
+            const float bs[3] = {fmaf(r, pq[0], rad.w), r * pq[1], r * pq[2]};
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 b[2 * i] = fmaf(br, bt[i], b[2 * i]);
@@ -1315,6 +1301,8 @@ std::vector<float> buildSingularTable(unsigned order) {
         const double r = gauss[ri].x;
         out[12 * 13 * per + 4 * ri] = float(r);
         out[12 * 13 * per + 4 * ri + 1] = float(r * r * r * gauss[ri].w);
+        out[12 * 13 * per + 4 * ri + 2] = float(1.0 / r);
+        out[12 * 13 * per + 4 * ri + 3] = float(1.0 - r);
     }
     return out;
 }

@@ -112,7 +112,7 @@ void uploadRuleTables(cudaStream_t stream);
 // Touching-pair tuples of the mixed form for one singular order: per
 // (topology block vertex|edge|coincident, sector, u, v, w) twelve floats
 // (canonical test and trial barycentrics at radius 1, displacement
-// coefficients a1 a2 b1 b2, weight, pad), then per radial node (r, r^3 w, 0, 0).
+// coefficients a1 a2 b1 b2, weight, pad), then per radial node (r, r^3 w, 1/r, 1 - r).
 std::vector<float> buildSingularTable(unsigned order);
 
 // Per-batch assembly of B frequencies. ks[B]; flux q[B][E][T] complex;
