@@ -42,13 +42,19 @@ METRIC = "freq-point solves/s (dense mixed-precision form at <=1e-5 surface-pres
 # sincos 1, weight 2, g 2, g(1+ikr) 4, 1/r^2 1, two normal projections 12,
 # P and Q 4, three basis contractions 36.
 FLOPS_PER_REGULAR_SAMPLE = 85
-# Mixed-form regular sample, counted from its kernel source: FP64 trial point
-# 9 + displacement 3 + |d|^2 5 + Newton root 5 + r and k*r 2 + turns 2 +
-# reduction 4; FP32 |d|^2 5, 1/r 1, sincos 1, weights 3, g 2, g(1+ikr) 4,
-# 1/r^2 1, normal projections 12, P and Q 4, trial contractions 36, test
-# contraction amortised over the rule (108/NP, taken at NP = 12) 9.
-MIXED_FP64_FLOPS_PER_SAMPLE = 30
-MIXED_FP32_FLOPS_PER_SAMPLE = 78
+# Mixed-form regular sample (all FP32), counted from its kernel source:
+# r^2 - r0^2 polynomial 10, r^2 1, 1/r 1, r 1, r + r0 1, quotient 2, phase 2,
+# turns 3, reduction 4, sin and cos 2, k*r 1, weight 2, g 2, g(1+ikr) 4,
+# 1/r^2 1, P 2, adjoint projection 4, Q 2, trial contractions 36.
+MIXED_FP32_FLOPS_PER_SAMPLE = 81
+# Per test point of a pair: the test-side contraction of the three kinds
+# (54 FMA) and the double-layer projection factor (6).
+MIXED_FP32_FLOPS_PER_TEST_POINT = 114
+# DRAM bytes per unordered q12 pair of regularMixedKernel<12> (reads of panel
+# data and bins, the two FP32 records' writes), from the ncu capture of
+# regularMixedKernel<12> (ncu summary in profiles/); scaled by the pairs of a
+# launch for the roofline's traffic figure.
+REGULAR_Q12_DRAM_BYTES_PER_PAIR = 325
 CONFIG = {"workload": "C1 icosphere s3 (642 v / 1280 t), 32 log freqs 100 Hz-5 kHz, 3 observers, dense; "
                       "mixed form timed, plain FP64 form timed beside it",
           "mesh": "icosphere-3 r=0.1 m", "frequencies": 32, "observers": 3, "excitations": 1,
@@ -91,7 +97,7 @@ class ClockSampler:
 
     REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, device_index: int, enabled: bool = True, period_s: float = 0.25):
+    def __init__(self, device_index: int, enabled: bool = True, period_s: float = 0.02):
         self.device = device_index
         self.enabled = enabled
         self.period = period_s
@@ -238,7 +244,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-clock-sampler", action="store_true", help="skip nvidia-smi sampling (diagnostics)")
     ap.add_argument("--sweep-frequencies", type=int, default=32,
-                    help="solve only the first n sweep frequencies (small profiling cases)")
+                    help="solve only n sweep frequencies (small profiling cases)")
+    ap.add_argument("--first-frequency", type=int, default=0,
+                    help="index of the first sweep frequency solved (small profiling cases)")
     args = ap.parse_args()
     rank, world, local = env_rank()
     if args.impl == "reference":
@@ -256,7 +264,7 @@ def main():
     stream = torch.cuda.Stream()
     mesh = hs.icosphere(3)
     req = request(hs)
-    req.frequencies = FREQUENCIES[: args.sweep_frequencies]
+    req.frequencies = FREQUENCIES[args.first_frequency: args.first_frequency + args.sweep_frequencies]
     req.interaction_plan_frequencies = FREQUENCIES
     solver = hs.CudaBemSolver(mesh)
     solver.set_stream(stream.cuda_stream)
@@ -322,10 +330,13 @@ def main():
 
         p_ms, p_total = regular_stats(plain, "regular_q")
         m_ms, m_total = regular_stats(mixed, "regular_mixed_q")
-        p_samples, m_samples = plain["work"]["regular_samples"], mixed["work"]["regular_samples"]
+        p_samples = plain["work"]["regular_samples"]
         p_achieved = p_samples * FLOPS_PER_REGULAR_SAMPLE / (p_ms / 1e3) / 1e12
-        m64 = m_samples * MIXED_FP64_FLOPS_PER_SAMPLE / (m_ms / 1e3) / 1e12
-        m32 = m_samples * MIXED_FP32_FLOPS_PER_SAMPLE / (m_ms / 1e3) / 1e12
+        # the mixed form's single largest launch: regularMixedKernel<12>, one launch per step
+        q12_ms = mixed["profile"].get("regular_mixed_q12", (0.0, 0))[0] / args.steps
+        q12_pairs = mixed["work"]["pairs_q12"] / args.steps
+        q12_flop = q12_pairs * (144 * MIXED_FP32_FLOPS_PER_SAMPLE + 12 * MIXED_FP32_FLOPS_PER_TEST_POINT)
+        m32 = q12_flop / (q12_ms / 1e3) / 1e12 if q12_ms > 0 else 0.0
         # area-weighted relative L2 of DP0 surface pressure, mixed vs plain, worst frequency
         v = mesh.vertices[mesh.triangles]
         area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
@@ -363,15 +374,17 @@ def main():
                           "(first upload to last result download, host control included); e2e: wall clock of "
                           "the Python API call with host request and result buffers",
             },
-            "roofline": {"kernel": "regularMixedKernel (4 rule sizes), the mixed form's dominant kernel",
-                         "bound": "fp64+fp32 pipes", "unit": "TFLOP/s",
-                         "achieved": {"fp64": m64, "fp32": m32}, "peak": {"fp64": fp64, "fp32": fp32},
-                         "frac": max(m64 / fp64, m32 / fp32),
-                         "peak_source": "cuBLAS DGEMM and SGEMM (TF32 off) 4096^3 measured in this run; "
-                                        "MEASURED_PEAKS.json has no FP32/FP64 figures",
-                         "traffic": None, "share_of_device_time": m_ms / m_total,
-                         "algorithmic": f"{m_samples} samples x ({MIXED_FP64_FLOPS_PER_SAMPLE} FP64 + "
-                                        f"{MIXED_FP32_FLOPS_PER_SAMPLE} FP32 FLOP)"},
+            "roofline": {"kernel": "regularMixedKernel<12> (mixed form, largest launch)", "bound": "fp32",
+                         "achieved": m32, "peak": fp32, "unit": "TFLOP/s", "frac": m32 / fp32,
+                         "peak_source": "cuBLAS SGEMM (TF32 off) 4096^3 measured in this run; MEASURED_PEAKS.json "
+                                        "has no FP32 figure",
+                         "traffic": (REGULAR_Q12_DRAM_BYTES_PER_PAIR * q12_pairs
+                                     if REGULAR_Q12_DRAM_BYTES_PER_PAIR else None),
+                         "traffic_note": "DRAM bytes per launch: ncu bytes per q12 pair x pairs of the launch",
+                         "launch_ms": q12_ms, "pairs_per_launch": q12_pairs,
+                         "share_of_device_time": q12_ms * args.steps / m_total,
+                         "algorithmic": f"per q12 pair 144 samples x {MIXED_FP32_FLOPS_PER_SAMPLE} + 12 test points "
+                                        f"x {MIXED_FP32_FLOPS_PER_TEST_POINT} FP32 FLOP"},
             "roofline_fp64_plain": {"kernel": "regularPairsKernel (4 rule sizes)", "bound": "fp64",
                                     "achieved": p_achieved, "peak": fp64, "unit": "TFLOP/s", "frac": p_achieved / fp64,
                                     "share_of_device_time": p_ms / p_total,

@@ -25,6 +25,7 @@ namespace hsb {
 namespace {
 
 constexpr double kInvFourPi = 0.07957747154594766788;
+constexpr size_t kGatherColumnSmem = 200 * 1024;  // fused column gather: 3T complex FP64 entries
 
 // Rule points (b0, b1, b2, w) of the four regular bins, in bin order
 // (offsets 0, 6, 18, 34).
@@ -1135,6 +1136,85 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
 // Deterministic gathers: records -> per-(test panel, trial vertex) columns ->
 // matrix entries, and records x flux -> right-hand side.
 // ---------------------------------------------------------------------------
+// Both gathers in one CTA per matrix column (trial vertex b, frequency f),
+// for meshes whose 3T column entries fit in shared memory: first the
+// per-(test panel, local row) sums over the trial panels at b (coalesced
+// plane reads), then each row's sum over its incident panels plus the half
+// mass, written as a contiguous column. Same summation order as
+// gatherTrialKernel followed by gatherTestKernel.
+template <class Rec>
+__global__ void __launch_bounds__(512, 2) gatherColumnKernel(const Rec *__restrict__ records,
+                                                          const uint32_t *__restrict__ incOffsets,
+                                                          const uint32_t *__restrict__ incPanel,
+                                                          const uint8_t *__restrict__ incLocal,
+                                                          const DPanel *__restrict__ panels,
+                                                          const double *__restrict__ rowScale, uint32_t T, uint32_t N,
+                                                          double *__restrict__ A) {
+    extern __shared__ double2 column[];  // [3T]: entry (test panel t, local row la) of column b
+    const uint32_t b = blockIdx.x;
+    const int f = blockIdx.y;
+    const Rec *rec = records + size_t(f) * T * T * kRecordDoubles;
+    const uint32_t o0 = incOffsets[b], o1 = incOffsets[b + 1];
+    for (uint32_t t = threadIdx.x; t < T; t += blockDim.x) {
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        // trial panels at b in chunks of 4: the record loads of a chunk are in flight together
+        for (uint32_t o = o0; o < o1; o += 4) {
+            Rec v[4][6];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (o + u < o1) {
+                    const Rec *r = rec + recordOffset(T, size_t(incPanel[o + u]) * T + t, incLocal[o + u]);
+#pragma unroll
+                    for (int c = 0; c < 6; ++c)
+                        v[u][c] = r[c];
+                }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (o + u < o1)
+#pragma unroll
+                    for (int c = 0; c < 6; ++c)
+                        acc[c] += double(v[u][c]);
+        }
+#pragma unroll
+        for (int la = 0; la < 3; ++la)
+            column[3 * t + la] = make_double2(acc[2 * la], acc[2 * la + 1]);
+    }
+    __syncthreads();
+    for (uint32_t a = threadIdx.x; a < N; a += blockDim.x) {
+        double re = 0, im = 0;
+        const uint32_t a0 = incOffsets[a], a1 = incOffsets[a + 1];
+        for (uint32_t o = a0; o < a1; o += 4) {
+            uint32_t t[4], n[4][3];
+            int la[4];
+            double area[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (o + u < a1) {
+                    t[u] = incPanel[o + u];
+                    la[u] = incLocal[o + u];
+                    const DPanel &p = panels[t[u]];
+                    n[u][0] = p.nodes[0];
+                    n[u][1] = p.nodes[1];
+                    n[u][2] = p.nodes[2];
+                    area[u] = p.area;
+                }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (o + u < a1) {
+                    const double2 v = column[3 * t[u] + la[u]];
+                    re += v.x;
+                    im += v.y;
+                    if (n[u][0] == b || n[u][1] == b || n[u][2] == b)
+                        re += area[u] * (a == b ? 2.0 : 1.0) / 24.0;
+                }
+        }
+        const double sc = rowScale[a];
+        double *dst = A + (size_t(f) * N * N + size_t(b) * N + a) * 2;
+        dst[0] = re * sc;
+        dst[1] = im * sc;
+    }
+}
+
 template <class Rec>
 __global__ void gatherTrialKernel(const Rec *__restrict__ records, const uint32_t *__restrict__ incOffsets,
                                   const uint32_t *__restrict__ incPanel, const uint8_t *__restrict__ incLocal,
@@ -1187,33 +1267,49 @@ __global__ void gatherTestKernel(const double *__restrict__ columns, const DPane
     dst[1] = im * sc;
 }
 
+// Per-panel right-hand-side partials: sum over trial panels s of the
+// (s, t) moments times the flux of s. A CTA takes 32 test panels; its 8
+// warps take every 8th trial panel, and the partial sums are added in a
+// fixed order (deterministic).
 template <class Rec>
-__global__ void rhsPanelKernel(const Rec *__restrict__ records, const double *__restrict__ flux, uint32_t T,
-                               uint32_t E, double *__restrict__ panelRhs) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) rhsPanelKernel(const Rec *__restrict__ records, const double *__restrict__ flux,
+                                                      uint32_t T, uint32_t E, double *__restrict__ panelRhs) {
+    __shared__ double part[8][32][6];
+    const uint32_t lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const uint32_t t = blockIdx.x * 32 + lane;
     const uint32_t e = blockIdx.y;
     const int f = blockIdx.z;
-    if (t >= T)
-        return;
     const Rec *rec = records + size_t(f) * T * T * kRecordDoubles;
     const double *q = flux + (size_t(f) * E + e) * 2 * T;
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (uint32_t s = 0; s < T; ++s) {
-        const double qr = q[2 * s], qi = q[2 * s + 1];
-        if (qr == 0 && qi == 0)
-            continue;
-        const Rec *r = rec + recordOffset(T, size_t(s) * T + t, 9);
+    if (t < T)
+        for (uint32_t s = g; s < T; s += 8) {
+            const double qr = q[2 * s], qi = q[2 * s + 1];
+            if (qr == 0 && qi == 0)
+                continue;
+            const Rec *r = rec + recordOffset(T, size_t(s) * T + t, 9);
 #pragma unroll
-        for (int la = 0; la < 3; ++la) {
-            const double rr = r[2 * la], ri = r[2 * la + 1];
-            acc[2 * la] += rr * qr - ri * qi;
-            acc[2 * la + 1] += rr * qi + ri * qr;
+            for (int la = 0; la < 3; ++la) {
+                const double rr = r[2 * la], ri = r[2 * la + 1];
+                acc[2 * la] += rr * qr - ri * qi;
+                acc[2 * la + 1] += rr * qi + ri * qr;
+            }
         }
-    }
-    double *dst = panelRhs + (size_t(f) * E + e) * 6 * T + 6 * size_t(t);
 #pragma unroll
     for (int c = 0; c < 6; ++c)
-        dst[c] = acc[c];
+        part[g][lane][c] = acc[c];
+    __syncthreads();
+    if (g != 0 || t >= T)
+        return;
+    double *dst = panelRhs + (size_t(f) * E + e) * 6 * T + 6 * size_t(t);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        double v = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w)
+            v += part[w][lane][c];
+        dst[c] = v;
+    }
 }
 
 __global__ void rhsVertexKernel(const double *__restrict__ panelRhs, const uint32_t *__restrict__ incOffsets,
@@ -1405,28 +1501,53 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
                                                                                  ks, recD, error);
         cudaCheck(cudaGetLastError(), "projected near assembly launch");
     }
-    {
-        TimedScope scope(timer, "gather_trial", stream);
-        const dim3 grid((g.T + 127) / 128, g.N, B);
+    const size_t columnBytes = size_t(3) * g.T * sizeof(double2);
+    if (columnBytes <= kGatherColumnSmem) {
+        TimedScope scope(timer, "gather_column", stream);
+        static bool attr = false;
+        if (!attr) {
+            cudaCheck(cudaFuncSetAttribute(gatherColumnKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(kGatherColumnSmem)),
+                      "gather smem attribute");
+            cudaCheck(cudaFuncSetAttribute(gatherColumnKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           int(kGatherColumnSmem)),
+                      "gather smem attribute");
+            attr = true;
+        }
+        const dim3 grid(g.N, B);
         if (mixed)
-            gatherTrialKernel<<<grid, 128, 0, stream>>>(recF, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N, ws.columns);
+            gatherColumnKernel<<<grid, 512, columnBytes, stream>>>(recF, g.incOffsets, g.incPanel, g.incLocal,
+                                                                   g.panels, g.rowScale, g.T, g.N, A);
         else
-            gatherTrialKernel<<<grid, 128, 0, stream>>>(recD, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N, ws.columns);
-        cudaCheck(cudaGetLastError(), "trial gather launch");
-    }
-    {
-        TimedScope scope(timer, "gather_test", stream);
-        gatherTestKernel<<<dim3((g.N + 127) / 128, g.N, B), 128, 0, stream>>>(
-            ws.columns, g.panels, g.incOffsets, g.incPanel, g.incLocal, g.rowScale, g.T, g.N, A);
-        cudaCheck(cudaGetLastError(), "test gather launch");
+            gatherColumnKernel<<<grid, 512, columnBytes, stream>>>(recD, g.incOffsets, g.incPanel, g.incLocal,
+                                                                   g.panels, g.rowScale, g.T, g.N, A);
+        cudaCheck(cudaGetLastError(), "column gather launch");
+    } else {
+        {
+            TimedScope scope(timer, "gather_trial", stream);
+            const dim3 grid((g.T + 127) / 128, g.N, B);
+            if (mixed)
+                gatherTrialKernel<<<grid, 128, 0, stream>>>(recF, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N,
+                                                            ws.columns);
+            else
+                gatherTrialKernel<<<grid, 128, 0, stream>>>(recD, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N,
+                                                            ws.columns);
+            cudaCheck(cudaGetLastError(), "trial gather launch");
+        }
+        {
+            TimedScope scope(timer, "gather_test", stream);
+            gatherTestKernel<<<dim3((g.N + 127) / 128, g.N, B), 128, 0, stream>>>(
+                ws.columns, g.panels, g.incOffsets, g.incPanel, g.incLocal, g.rowScale, g.T, g.N, A);
+            cudaCheck(cudaGetLastError(), "test gather launch");
+        }
     }
     {
         TimedScope scope(timer, "rhs_panel", stream);
-        const dim3 grid((g.T + 127) / 128, E, B);
+        const dim3 grid((g.T + 31) / 32, E, B);
         if (mixed)
-            rhsPanelKernel<<<grid, 128, 0, stream>>>(recF, flux, g.T, E, ws.panelRhs);
+            rhsPanelKernel<<<grid, 256, 0, stream>>>(recF, flux, g.T, E, ws.panelRhs);
         else
-            rhsPanelKernel<<<grid, 128, 0, stream>>>(recD, flux, g.T, E, ws.panelRhs);
+            rhsPanelKernel<<<grid, 256, 0, stream>>>(recD, flux, g.T, E, ws.panelRhs);
     }
     {
         TimedScope scope(timer, "rhs_vertex", stream);

@@ -500,21 +500,36 @@ __global__ void __launch_bounds__(sizeof(R) == 8 ? 256 : 512) solveKernel(const 
         st2(out + 2 * i, x[i]);
 }
 
-// r = b - A x per row (FP64 accumulation), plus mass-scaled squares for the norms.
-__global__ void residualKernel(const double *A, const double *b, const double *x, const double *mass, uint32_t N,
-                               uint32_t E, double *correction, double *squares) {
-    const uint32_t a = blockIdx.x * blockDim.x + threadIdx.x;
+// r = b - A x per row (FP64 accumulation), plus mass-scaled squares for the
+// norms. A CTA takes 32 rows; its 8 warps take every 8th column, and the 8
+// partial sums are added in a fixed order (deterministic).
+__global__ void __launch_bounds__(256) residualKernel(const double *A, const double *b, const double *x,
+                                                      const double *mass, uint32_t N, uint32_t E, double *correction,
+                                                      double *squares) {
+    __shared__ double2 part[8][32];
+    const uint32_t lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const uint32_t a = blockIdx.x * 32 + lane;
     const uint32_t e = blockIdx.y, f = blockIdx.z;
-    if (a >= N)
-        return;
     const double *M = A + size_t(f) * N * N * 2;
     const double *xv = x + (size_t(f) * E + e) * N * 2;
     double re = 0, im = 0;
-    for (uint32_t c = 0; c < N; ++c) {
-        const double2 m = ld2(M + 2 * (size_t(c) * N + a));
-        const double2 v = ld2(xv + 2 * c);
-        re += m.x * v.x - m.y * v.y;
-        im += m.x * v.y + m.y * v.x;
+    if (a < N)
+        for (uint32_t c = g; c < N; c += 8) {
+            const double2 m = ld2(M + 2 * (size_t(c) * N + a));
+            const double2 v = ld2(xv + 2 * c);
+            re += m.x * v.x - m.y * v.y;
+            im += m.x * v.y + m.y * v.x;
+        }
+    part[g][lane] = mk<double>(re, im);
+    __syncthreads();
+    if (g != 0 || a >= N)
+        return;
+    re = 0;
+    im = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        re += part[w][lane].x;
+        im += part[w][lane].y;
     }
     const size_t idx = (size_t(f) * E + e) * N + a;
     const double2 bb = ld2(b + 2 * idx);
@@ -648,7 +663,7 @@ void residualBatch(const double *A, const double *b, const double *x, const doub
     double *squares = norms + 2 * size_t(B) * E;  // scratch after the norms
     {
         TimedScope s(timer, "residual", stream);
-        residualKernel<<<dim3((N + 127) / 128, E, B), 128, 0, stream>>>(A, b, x, mass, N, E, correction, squares);
+        residualKernel<<<dim3((N + 31) / 32, E, B), 256, 0, stream>>>(A, b, x, mass, N, E, correction, squares);
     }
     {
         TimedScope s(timer, "residual_norm", stream);
