@@ -310,7 +310,8 @@ class CudaBemSolver:
                                             complex(*x.volume_impedance)) for x in imp[: info.impedance_count]]
                 excs.append(BemExcitationResult(
                     name=request.excitations[e].name, observer_pressure=_cplx(ob[: 2 * O]), impedances=impedances,
-                    refinement_steps=info.refinement_steps, boundary_residual=info.boundary_residual,
+                    refinement_steps=info.refinement_steps, iterations=info.iterations,
+                    boundary_residual=info.boundary_residual,
                     field_quadrature_comparison_degree=info.field_comparison_degree,
                     field_quadrature_verification_degree=info.field_verification_degree,
                     field_quadrature_discrepancy=info.field_discrepancy,

@@ -1441,10 +1441,15 @@ void uploadRuleTables(cudaStream_t stream) {
     done = true;
 }
 
-size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B) {
+bool gatherUsesColumns(uint32_t T) { return size_t(3) * T * sizeof(double2) > kGatherColumnSmem; }
+
+size_t recordBytes(uint32_t T, bool mixed) { return size_t(T) * T * kRecordDoubles * (mixed ? 4 : 8); }
+
+size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B, bool mixed) {
     const size_t pairs = size_t(T) * (T - 1) / 2;
-    return size_t(B) * (size_t(T) * T * kRecordDoubles * 8 + size_t(N) * 6 * T * 8 + size_t(E) * 6 * T * 8 +
-                        kBins * pairs * sizeof(uint2) + kBins * sizeof(uint32_t));
+    const size_t columns = gatherUsesColumns(T) ? size_t(N) * 6 * T * 8 : 0;
+    return size_t(B) * (recordBytes(T, mixed) + columns + size_t(E) * 6 * T * 8 + kBins * pairs * sizeof(uint2) +
+                        kBins * sizeof(uint32_t));
 }
 
 void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *gaussSingular, const double *flux,
@@ -1502,7 +1507,7 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         cudaCheck(cudaGetLastError(), "projected near assembly launch");
     }
     const size_t columnBytes = size_t(3) * g.T * sizeof(double2);
-    if (columnBytes <= kGatherColumnSmem) {
+    if (!gatherUsesColumns(g.T)) {
         TimedScope scope(timer, "gather_column", stream);
         static bool attr = false;
         if (!attr) {

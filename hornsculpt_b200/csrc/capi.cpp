@@ -167,7 +167,7 @@ hs_status hs_result_excitation_info(const hs_result *r, size_t f, size_t e, hs_e
         return fail(HS_E_INVALID, "Result index out of range.");
     out->boundary_residual = x->residual;
     out->refinement_steps = x->refinements;
-    out->iterations = 0;
+    out->iterations = x->iterations;
     out->field_comparison_degree = x->fieldDegree;
     out->field_verification_degree = x->fieldNext;
     out->field_discrepancy = x->fieldDiscrepancy;

@@ -127,9 +127,13 @@ struct AssemblyWorkspace {
     uint32_t *binCounts;
     size_t binCapacity;
 };
-size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B);
-// mixed: regular and near pairs with FP32 kernel arithmetic (displacement and
-// phase k*r in FP64), touching pairs in FP64 either way.
+size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B, bool mixed);
+// Record bytes of one frequency; whether the gather needs the columns buffer
+// (meshes whose 3T column entries exceed the fused gather's shared memory).
+size_t recordBytes(uint32_t T, bool mixed);
+bool gatherUsesColumns(uint32_t T);
+// mixed: FP32 samples and records (phases kept exact: centre phase in FP64 for
+// regular pairs, FP64 displacement and phase for near pairs), FP64 matrix.
 void assembleBatch(const AssemblyGeometry &geo, const double *ks, const double *gaussSingular, const double *flux,
                    uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
                    cudaStream_t stream, class KernelTimer *timer, bool mixed = false);
@@ -151,6 +155,17 @@ void residualBatch(const double *A, const double *b, const double *x, const doub
 void addCorrectionBatch(double *x, const double *correction, size_t count, cudaStream_t stream);
 void addCorrectionBatch(double *x, const float *correction, size_t count, cudaStream_t stream);
 void roundToFloat(const double *in, float *out, size_t count, cudaStream_t stream);
+
+// One left-preconditioned GMRES cycle (at most m Arnoldi steps) per system of
+// a batch: solves A_f d = r_s with M = the FP32 LU of A_f and adds d to x_s
+// (systems s = f * E + e; a zero r_s is left alone). Stops a system once its
+// preconditioned residual estimate is at most tol relative to its start.
+// Returns the Arnoldi steps taken by the batch; stepsOut[s] holds each
+// system's. The workspace holds gmresWorkspaceBytes(N, B * E, m) bytes.
+size_t gmresWorkspaceBytes(uint32_t N, uint32_t S, uint32_t m);
+uint32_t gmresCycleBatch(const double *A, const float *LU32, const int *pivots, uint32_t N, uint32_t B, uint32_t E,
+                         const double *r, double *x, uint32_t m, double tol, void *workspace, cudaStream_t stream,
+                         KernelTimer *timer, std::vector<uint32_t> &stepsOut);
 
 // Observer fields of one rule degree for every (batch, excitation, observer).
 struct FieldRequest {

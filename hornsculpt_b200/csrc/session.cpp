@@ -96,6 +96,9 @@ void validateRequest(const hs_request &r) {
                  o.fmm_restart_length > 300 ||
                  (w != 32 && w != 64 && w != 128 && w != 256 && w != 512 && w != 1024 && w != 2048))))
         throw InvalidArgument("Invalid Fast Multipole or GMRES settings.");
+    if (o.precision == HS_PRECISION_MIXED && (o.fmm_maximum_iterations < 1 || o.fmm_maximum_iterations > 10000 ||
+                                               o.fmm_restart_length < 2 || o.fmm_restart_length > 300))
+        throw InvalidArgument("Invalid Fast Multipole or GMRES settings.");
     if (!std::isfinite(r.density) || r.density <= 0 || !std::isfinite(r.sound_speed) || r.sound_speed <= 0 ||
         !r.frequency_count || !r.excitation_count || (o.quadrature_order != 2 && o.quadrature_order != 4) ||
         o.singular_order < 2 || o.singular_order > 20 || !std::isfinite(o.near_distance_ratio) ||
@@ -295,10 +298,11 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
     planMs_ = msSince(start);
 }
 
-uint32_t Session::chooseBatch(uint32_t F, uint32_t E, uint32_t O) const {
+uint32_t Session::chooseBatch(uint32_t F, uint32_t E, uint32_t O, bool mixed, uint32_t restart) const {
     const uint64_t T = space_.panels.size(), N = space_.vertices.size();
-    const uint64_t perFrequency = assemblyWorkspaceBytes(uint32_t(T), uint32_t(N), E, 1) + 2 * N * N * 16 +
-                                  4 * E * N * 16 + E * T * 16 + fieldPartialsBytes(uint32_t(T), E, O, 1) + 64;
+    const uint64_t perFrequency = assemblyWorkspaceBytes(uint32_t(T), uint32_t(N), E, 1, mixed) + 2 * N * N * 16 +
+                                  4 * E * N * 16 + E * T * 16 + fieldPartialsBytes(uint32_t(T), E, O, 1) +
+                                  (mixed ? gmresWorkspaceBytes(uint32_t(N), E, restart) : 0) + 64;
     size_t free = 0, total = 0;
     cuda(cudaMemGetInfo(&free, &total), "CUDA memory query");
     const uint64_t budget = uint64_t(double(free) * .6);
@@ -308,11 +312,14 @@ uint32_t Session::chooseBatch(uint32_t F, uint32_t E, uint32_t O) const {
     return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>({uint64_t(F), budget / perFrequency, 32})));
 }
 
-void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O) {
+void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, uint32_t restart) {
     const size_t T = space_.panels.size(), N = space_.vertices.size();
     const size_t pairs = T * (T - 1) / 2;
-    dRecords_.ensure(std::max<size_t>(B * T * T * kRecordDoubles * 8, 16));
-    dColumns_.ensure(B * N * 6 * T * 8);
+    dRecords_.ensure(std::max<size_t>(B * recordBytes(uint32_t(T), mixed), 16));
+    if (gatherUsesColumns(uint32_t(T)))
+        dColumns_.ensure(B * N * 6 * T * 8);
+    if (mixed)
+        dGmres_.ensure(gmresWorkspaceBytes(uint32_t(N), B * E, restart));
     dPanelRhs_.ensure(B * E * 6 * T * 8);
     dBins_.ensure(std::max<size_t>(B * kBins * pairs * sizeof(uint2), 16));
     dBinCounts_.ensure(B * kBins * sizeof(uint32_t));
@@ -336,7 +343,7 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O) {
                                   &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_, &dRecords_, &dColumns_,
                                   &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
                                   &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_,
-                                  &dWork32_})
+                                  &dWork32_, &dGmres_})
         bytes += b->bytes();
     peakBytes_ = std::max(peakBytes_, bytes);
 }
@@ -436,8 +443,10 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     const double planMs = planMs_;
     checkCancel();
     const cudaStream_t s = stream();
-    const uint32_t Bmax = chooseBatch(F, E, O);
-    ensureWorkspace(Bmax, E, O);
+    const bool mixedForm = o.precision == HS_PRECISION_MIXED;
+    const uint32_t restart = o.fmm_restart_length;
+    const uint32_t Bmax = chooseBatch(F, E, O, mixedForm, restart);
+    ensureWorkspace(Bmax, E, O, mixedForm, restart);
     if (O)
         cuda(cudaMemcpyAsync(dObservers_.as<void>(), observers.data(), observers.size() * 8, cudaMemcpyHostToDevice, s),
              "observer upload");
@@ -540,7 +549,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         const double target = mixed ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
         const uint32_t maxSteps = mixed ? std::max<uint32_t>(o.maximum_refinement_steps, 10) : o.maximum_refinement_steps;
         const auto residualStart = Clock::now();
-        std::vector<uint32_t> steps(B, 0);
+        std::vector<uint32_t> steps(B, 0), krylov(size_t(B) * E, 0), cycle;
         std::vector<double> relative(size_t(B) * E, 0);
         std::vector<double> norms(2 * size_t(B) * E);
         for (;;) {
@@ -580,13 +589,15 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 break;
             const auto t0 = Clock::now();
             if (mixed) {
-                {
-                    TimedScope scope(&timer_, "round_fp32", s);
-                    roundToFloat(dCorr_.as<double>(), work32, vectorReals, s);
-                }
-                luSolveBatch(LU32, dPivots_.as<int>(), N, B, E, work32, s, &timer_);
-                TimedScope scope(&timer_, "add_correction", s);
-                addCorrectionBatch(dX_.as<double>(), work32, vectorReals, s);
+                // GMRES-IR: one FP64 GMRES cycle on A d = r, preconditioned by the
+                // FP32 LU, reducing the preconditioned residual far enough that
+                // the worst system lands a hundredfold below the target.
+                const double worst = *std::max_element(relative.begin(), relative.end());
+                const double tol = std::clamp(.01 * target / worst, 1e-13, .5);
+                gmresCycleBatch(dA_.as<double>(), LU32, dPivots_.as<int>(), N, B, E, dCorr_.as<double>(),
+                                dX_.as<double>(), restart, tol, dGmres_.as<void>(), s, &timer_, cycle);
+                for (size_t q = 0; q < cycle.size(); ++q)
+                    krylov[q] += cycle[q];
             } else {
                 luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dCorr_.as<double>(), s, &timer_);
                 TimedScope scope(&timer_, "add_correction", s);
@@ -702,6 +713,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 er.trace.assign(x.begin() + (size_t(b) * E + e) * N, x.begin() + (size_t(b) * E + e + 1) * N);
                 er.residual = relative[size_t(b) * E + e];
                 er.refinements = steps[b];
+                er.iterations = krylov[size_t(b) * E + e];
                 er.fieldDegree = fieldDeg[size_t(b) * E + e];
                 er.fieldNext = fieldNext[size_t(b) * E + e];
                 er.fieldDiscrepancy = fieldDisc[size_t(b) * E + e];
@@ -751,7 +763,7 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
                             double *rhs) {
     preparePlan(o, planK, nullptr);
     const uint32_t T = uint32_t(space_.panels.size()), N = uint32_t(space_.vertices.size());
-    ensureWorkspace(1, 1, 0);
+    ensureWorkspace(1, 1, 0, o.precision == HS_PRECISION_MIXED, o.fmm_restart_length);
     const cudaStream_t s = stream();
     cuda(cudaMemcpyAsync(dKs_.as<void>(), &k, 8, cudaMemcpyHostToDevice, s), "k upload");
     cuda(cudaMemcpyAsync(dFlux_.as<void>(), flux, size_t(T) * 16, cudaMemcpyHostToDevice, s), "flux upload");

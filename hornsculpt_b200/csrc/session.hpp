@@ -37,7 +37,7 @@ using cplx = std::complex<double>;
 struct ExcitationResult {
     std::vector<cplx> trace, surface, normalDerivative, observer;
     double residual{};
-    uint32_t refinements{}, fieldDegree{}, fieldNext{};
+    uint32_t refinements{}, iterations{}, fieldDegree{}, fieldNext{};
     double fieldDiscrepancy{};
     std::vector<hs_face_impedance> impedances;
 };
@@ -70,8 +70,8 @@ class Session {
     struct Batch;
     void uploadGeometry();
     void preparePlan(const hs_numerics &numerics, double maxK, const volatile int32_t *cancel);
-    void ensureWorkspace(uint32_t B, uint32_t E, uint32_t O);
-    uint32_t chooseBatch(uint32_t F, uint32_t E, uint32_t O) const;
+    void ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, uint32_t restart);
+    uint32_t chooseBatch(uint32_t F, uint32_t E, uint32_t O, bool mixed, uint32_t restart) const;
     void checkDeviceError(const char *where);
     cudaStream_t stream() const { return external_ ? external_ : own_; }
 
@@ -95,7 +95,7 @@ class Session {
     uint64_t singularSamples_ = 0, nearSamples_ = 0;
     // workspaces (grow only)
     DeviceBuffer dRecords_, dColumns_, dPanelRhs_, dBins_, dBinCounts_, dA_, dLU_, dRhs_, dX_, dCorr_, dNorms_,
-        dPivots_, dInfo_, dKs_, dFlux_, dObservers_, dPartials_, dField_, dDegrees_, dWork32_;
+        dPivots_, dInfo_, dKs_, dFlux_, dObservers_, dPartials_, dField_, dDegrees_, dWork32_, dGmres_;
     size_t peakBytes_ = 0;
 };
 

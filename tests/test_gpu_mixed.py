@@ -52,3 +52,36 @@ def test_mixed_solve_matches_plain_form(make, freqs):
         assert err <= MIXED_TOL
         assert m.boundary_residual <= 1e-10
         assert rel_l2(m.observer_pressure, p.observer_pressure) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("restart", [40, 2], ids=["restart40", "restart2"])
+def test_mixed_gmres_ir(restart):
+    """GMRES-IR: FP64 GMRES cycles preconditioned by the FP32 LU drive every
+    system to <= 1e-10 relative residual; Krylov steps are reported and a short
+    restart only adds outer steps. The result equals the plain form within the
+    mixed-form tolerance, and repeats bit for bit."""
+    mesh = meshes.octahedral_sphere(3)
+    freqs = [150.0, 900.0, 1715.0]
+    exc = [hs.BemExcitation("unit", [hs.FaceVelocity(1, 1.0)]),
+           hs.BemExcitation("half", [hs.FaceVelocity(1, 0.5 - 0.25j)])]
+    numerics = hs.BemNumerics(precision="mixed", fast_multipole=hs.FastMultipoleSettings(restart_length=restart))
+    with hs.CudaBemSolver(mesh) as solver:
+        plain = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc))
+        first = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc, numerics=numerics))
+        again = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc, numerics=numerics))
+    for fp, fm, fa in zip(plain.frequencies, first.frequencies, again.frequencies):
+        for p, m, a in zip(fp.excitations, fm.excitations, fa.excitations):
+            assert m.boundary_residual <= 1e-10
+            assert m.refinement_steps >= 1 and m.iterations >= m.refinement_steps
+            assert m.iterations <= m.refinement_steps * restart
+            assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
+            assert np.array_equal(m.boundary.pressure_trace, a.boundary.pressure_trace)
+
+
+def test_mixed_rejects_bad_gmres_settings():
+    mesh = meshes.octahedral_sphere(2)
+    numerics = hs.BemNumerics(precision="mixed", fast_multipole=hs.FastMultipoleSettings(restart_length=1))
+    with hs.CudaBemSolver(mesh) as solver:
+        with pytest.raises(ValueError, match="GMRES settings"):
+            solver.solve(hs.BemRequest(frequencies=[500.0], excitations=[hs.BemExcitation("u", [hs.FaceVelocity(1, 1.0)])],
+                                       numerics=numerics))
