@@ -19,8 +19,9 @@ struct EdgeUse {
 };
 
 // Separating-axis test of two triangles with no common vertex: the 2 face
-// normals and the 9 edge-edge cross products. Touching within `eps` counts
-// as intersecting.
+// normals, the 9 edge-edge cross products and the 6 in-plane edge normals
+// (the last separate coplanar triangles, for which every other axis is the
+// common normal). Touching within `eps` counts as intersecting.
 bool trianglesIntersect(const V3 *a, const V3 *b, double eps) {
     auto separated = [&](V3 axis) {
         const double l = len(axis);
@@ -39,12 +40,16 @@ bool trianglesIntersect(const V3 *a, const V3 *b, double eps) {
     };
     const V3 ea[3] = {a[1] - a[0], a[2] - a[1], a[0] - a[2]};
     const V3 eb[3] = {b[1] - b[0], b[2] - b[1], b[0] - b[2]};
-    if (separated(cross(ea[0], ea[1])) || separated(cross(eb[0], eb[1])))
+    const V3 na = cross(ea[0], ea[1]), nb = cross(eb[0], eb[1]);
+    if (separated(na) || separated(nb))
         return false;
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j)
             if (separated(cross(ea[i], eb[j])))
                 return false;
+    for (int i = 0; i < 3; ++i)
+        if (separated(cross(na, ea[i])) || separated(cross(nb, eb[i])))
+            return false;
     return true;
 }
 

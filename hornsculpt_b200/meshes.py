@@ -116,3 +116,132 @@ def scalene_tetrahedron() -> SurfaceMesh:
 def signed_volume(mesh: SurfaceMesh) -> float:
     v = mesh.vertices[mesh.triangles] - mesh.vertices.min(0)
     return float(np.einsum("ij,ij->i", v[:, 0], np.cross(v[:, 1], v[:, 2])).sum() / 6)
+
+
+# Face ids of the horn: the driven throat disc and the rigid rest of the shell.
+HORN_THROAT = 1
+HORN_SHELL = 2
+
+
+def _meridian_piece(curve, length: float, h: float, interior_jitter, rng, jitter: float):
+    """Points of one meridian piece at equal arc-length steps of at most h.
+
+    curve(t) -> (z, r) for t in [0, 1]; the end points are kept exactly (sharp
+    corners between pieces); interior points move along the meridian by up to
+    jitter * h when interior_jitter is set."""
+    n = max(1, int(math.ceil(length / h - 1e-9)))
+    t_fine = np.linspace(0.0, 1.0, 4097)
+    p_fine = np.array([curve(t) for t in t_fine])
+    s_fine = np.concatenate([[0.0], np.cumsum(np.hypot(*np.diff(p_fine, axis=0).T))])
+    targets = np.linspace(0.0, s_fine[-1], n + 1)
+    if interior_jitter and n > 1:
+        targets[1:-1] += rng.uniform(-jitter, jitter, n - 1) * h
+    t = np.interp(targets, s_fine, t_fine)
+    return [curve(x) for x in t]
+
+
+def exponential_horn(throat_radius: float = 0.025, mouth_radius: float = 0.15, length: float = 0.3,
+                     wall: float = 0.003, rear: float = 0.003, h: float | None = None, frequency: float = 8000.0,
+                     sound_speed: float = 343.0, seed: int = 0, jitter: float = 0.05,
+                     flare: float = 1.0) -> SurfaceMesh:
+    """Closed exponential-horn shell, meshed isotropically at edge length h.
+
+    Inner skin r(z) = r_t exp(m z^flare / L^(flare-1)) from the throat (z = 0)
+    to the mouth (z = L, r = mouth radius); outer skin at r(z) + wall; an
+    annular mouth rim; a rigid rear cap body of thickness `rear` behind the
+    throat; the throat disc (face HORN_THROAT, Driven) closes the inner skin.
+    flare = 1 is the plain exponential; larger values bend the flare towards
+    the mouth. Default h is lambda/6 at `frequency`. Nodes move tangentially by
+    up to jitter * h (uniform, numpy Generator seeded with `seed`), except on
+    the axis and on the corner rings of the meridian. The surface is a solid of
+    revolution about z: genus 0, watertight, outward-oriented."""
+    if h is None:
+        h = sound_speed / frequency / 6.0
+    if not (0 < throat_radius < mouth_radius and length > 0 and wall > 0 and rear > 0 and h > 0):
+        raise ValueError("invalid horn dimensions")
+    rng = np.random.default_rng(seed)
+    m = math.log(mouth_radius / throat_radius)
+
+    def inner(z):
+        return throat_radius * math.exp(m * (z / length) ** flare)
+
+    ro0 = throat_radius + wall
+    rim_outer, rim_inner = inner(length) + wall, inner(length)
+    # meridian pieces (z, r), traversed so that the solid lies to the right
+    pieces = [
+        (lambda t: (-rear, t * ro0), ro0, False),                                   # rear cap disc
+        (lambda t: (-rear + t * rear, ro0), rear, False),                            # rear cap side
+        (lambda t: (t * length, inner(t * length) + wall), None, True),              # outer skin
+        (lambda t: (length, rim_outer - t * wall), wall, False),                     # mouth rim
+        (lambda t: ((1 - t) * length, inner((1 - t) * length)), None, True),         # inner skin
+        (lambda t: (0.0, throat_radius * (1 - t)), throat_radius, False),            # throat disc
+    ]
+    meridian, corner, piece_of = [], [], []
+    for index, (curve, plen, interior) in enumerate(pieces):
+        if plen is None:
+            zs = np.linspace(0.0, 1.0, 2001)
+            p = np.array([curve(x) for x in zs])
+            plen = float(np.hypot(*np.diff(p, axis=0).T).sum())
+        pts = _meridian_piece(curve, plen, h, interior, rng, jitter)
+        start = 0 if index == 0 else 1  # the first point of a piece is the last of the previous
+        for k in range(start, len(pts)):
+            meridian.append(pts[k])
+            corner.append(k == 0 or k == len(pts) - 1)
+            piece_of.append(index)
+    # rings: the axis points are single vertices
+    vertices, rings = [], []
+    for i, (z, r) in enumerate(meridian):
+        if r <= 1e-12:
+            rings.append([len(vertices)])
+            vertices.append((0.0, 0.0, z))
+            continue
+        n = max(3, int(round(2 * math.pi * r / h)))
+        offset = 0.5 * (i % 2)
+        angles = 2 * math.pi * (np.arange(n) + offset) / n
+        if not corner[i]:
+            angles = angles + rng.uniform(-jitter, jitter, n) * h / r
+        ring = []
+        for a in angles:
+            ring.append(len(vertices))
+            vertices.append((r * math.cos(a), r * math.sin(a), z))
+        rings.append(ring)
+
+    def ring_angles(ring):
+        v = np.asarray([vertices[q] for q in ring])
+        return np.mod(np.arctan2(v[:, 1], v[:, 0]), 2 * math.pi)
+
+    triangles, faces = [], []
+    for i in range(len(rings) - 1):
+        A, B = rings[i], rings[i + 1]
+        face = HORN_THROAT if piece_of[i + 1] == 5 else HORN_SHELL  # the strip belongs to its outer node's piece
+        if len(A) == 1 or len(B) == 1:
+            if len(A) == 1:
+                for j in range(len(B)):
+                    triangles.append((A[0], B[(j + 1) % len(B)], B[j]))
+            else:
+                for j in range(len(A)):
+                    triangles.append((A[j], A[(j + 1) % len(A)], B[0]))
+            faces += [face] * (len(B) if len(A) == 1 else len(A))
+            continue
+        # zip the two rings by angle, starting at each ring's smallest angle
+        aa, ab = ring_angles(A), ring_angles(B)
+        oa, ob = np.argsort(aa), np.argsort(ab)
+        A = [A[q] for q in oa]
+        B = [B[q] for q in ob]
+        ta = np.concatenate([aa[oa], aa[oa][:1] + 2 * math.pi])
+        tb = np.concatenate([ab[ob], ab[ob][:1] + 2 * math.pi])
+        ia = ib = 0
+        while ia < len(A) or ib < len(B):
+            if ib == len(B) or (ia < len(A) and ta[ia + 1] <= tb[ib + 1]):
+                triangles.append((A[ia % len(A)], A[(ia + 1) % len(A)], B[ib % len(B)]))
+                ia += 1
+            else:
+                triangles.append((A[ia % len(A)], B[(ib + 1) % len(B)], B[ib % len(B)]))
+                ib += 1
+            faces.append(face)
+    verts = np.asarray(vertices)
+    tris = np.asarray(triangles, dtype=np.int64)
+    mesh = SurfaceMesh(verts, tris, np.asarray(faces), np.where(np.asarray(faces) == HORN_THROAT, DRIVEN, WALL))
+    if signed_volume(mesh) < 0:
+        mesh = SurfaceMesh(verts, tris[:, ::-1], mesh.face_ids, mesh.boundary)
+    return mesh

@@ -113,3 +113,85 @@ def test_non_finite_mesh_rejected():
     v[3, 1] = np.nan
     with pytest.raises(ValueError, match="not finite"):
         _session(meshes.SurfaceMesh(v, m.triangles, m.face_ids, m.boundary))
+
+
+def _passes_host_validation(mesh):
+    """Session creation validates the mesh on the host before it looks for a
+    device: with a GPU the session opens; without one the only error is the
+    missing device."""
+    try:
+        hs.CudaBemSolver(mesh).close()
+    except ValueError:
+        return False
+    except hs.BemError as e:
+        assert "CUDA device" in str(e)
+    return True
+
+
+@pytest.mark.parametrize("h,triangles", [(None, 12756), (0.004, 39776)])
+def test_exponential_horn(h, triangles):
+    """The horn shell of the precision-form workload: watertight, every
+    directed edge paired with its reverse, outward (positive volume), all
+    triangle angles >= 20 degrees (qualified for the regular rules), the throat
+    disc its own Driven face, seeded and reproducible, accepted by the
+    library's exterior-surface validation."""
+    m = meshes.exponential_horn(h=h, seed=7)
+    assert abs(m.triangle_count - triangles) <= 0.01 * triangles  # ring counts follow the jittered meridian
+    edges = {}
+    for t in m.triangles:
+        for a, b in ((t[0], t[1]), (t[1], t[2]), (t[2], t[0])):
+            edges[(a, b)] = edges.get((a, b), 0) + 1
+    assert all(c == 1 and edges.get((b, a)) == 1 for (a, b), c in edges.items())
+    assert meshes.signed_volume(m) > 0
+    v = m.vertices[m.triangles]
+    for i in range(3):
+        u, w = v[:, (i + 1) % 3] - v[:, i], v[:, (i + 2) % 3] - v[:, i]
+        cos = (u * w).sum(-1) / np.linalg.norm(u, axis=-1) / np.linalg.norm(w, axis=-1)
+        assert np.degrees(np.arccos(np.clip(cos, -1, 1))).min() >= 20
+    throat = m.face_ids == meshes.HORN_THROAT
+    assert throat.any() and (m.boundary[throat] == meshes.DRIVEN).all() and (m.boundary[~throat] == meshes.WALL).all()
+    # the throat disc lies in z = 0 inside the throat radius
+    tv = m.vertices[m.triangles[throat]]
+    assert np.allclose(tv[..., 2], 0) and np.hypot(tv[..., 0], tv[..., 1]).max() <= 0.025 + 1e-12
+    again = meshes.exponential_horn(h=h, seed=7)
+    assert np.array_equal(again.vertices, m.vertices) and np.array_equal(again.triangles, m.triangles)
+    assert not np.array_equal(meshes.exponential_horn(h=h, seed=8).vertices, m.vertices)
+    if h is None:
+        assert _passes_host_validation(m)
+
+
+def _box(n: int, size: float = 0.1) -> meshes.SurfaceMesh:
+    """Closed outward box with an n x n grid of quads per side (flat faces)."""
+    verts, index, tris = [], {}, []
+
+    def vid(p):
+        key = tuple(np.round(p, 12))
+        if key not in index:
+            index[key] = len(verts)
+            verts.append(p)
+        return index[key]
+
+    g = np.linspace(-size / 2, size / 2, n + 1)
+    for axis in range(3):
+        for sign in (-1, 1):
+            u, w = [(axis + 1) % 3, (axis + 2) % 3][:: sign]
+            for i in range(n):
+                for j in range(n):
+                    corners = []
+                    for di, dj in ((0, 0), (1, 0), (1, 1), (0, 1)):
+                        p = np.zeros(3)
+                        p[axis] = sign * size / 2
+                        p[u], p[w] = g[i + di], g[j + dj]
+                        corners.append(vid(p))
+                    a, b, c, d = corners
+                    tris += [(a, b, c), (a, c, d)]
+    m = meshes.SurfaceMesh(np.asarray(verts), np.asarray(tris), np.ones(len(tris)), np.ones(len(tris)))
+    if meshes.signed_volume(m) < 0:
+        m = meshes.SurfaceMesh(m.vertices, m.triangles[:, ::-1], m.face_ids, m.boundary)
+    return m
+
+
+def test_flat_faces_accepted():
+    """Coplanar triangles without a common vertex are separated by in-plane
+    axes: a box with flat gridded sides is a valid exterior surface."""
+    assert _passes_host_validation(_box(4))
