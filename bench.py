@@ -235,6 +235,80 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+C3_FREQUENCIES = [250.0, 1000.0, 2500.0]
+
+
+def c3_cases(hs):
+    """Mixed dense sizes (N = 2k, 4k, 8k complex DOFs) of the sphere and horn
+    families: icosphere / octahedral sphere refinements and the seeded horn
+    shell at the edge length that gives the size."""
+    m = hs.meshes
+    return [("sphere", "icosphere-4 r=0.1 m", lambda: m.icosphere(4)),
+            ("sphere", "octahedral-5 r=0.1 m", lambda: m.octahedral_sphere(5)),
+            ("sphere", "ring-meshed sphere h=4 mm r=0.1 m seed 0", lambda: m.revolved_sphere(h=0.004)),
+            ("horn", "exponential horn h=12.8 mm seed 0", lambda: m.exponential_horn(h=0.0128)),
+            ("horn", "exponential horn h=9.0 mm seed 0", lambda: m.exponential_horn(h=0.0090)),
+            ("horn", "exponential horn h=6.4 mm seed 0", lambda: m.exponential_horn(h=0.0064))]
+
+
+def run_c3(args):
+    """Per mesh: the plain FP64 form and the mixed form (FP32 samples and LU,
+    FP64 GMRES-IR to 1e-10) on the same frequencies; one JSON line each with
+    the per-frequency device time of both forms and the mixed form's
+    surface-pressure error against the plain form."""
+    import numpy as np
+    import torch
+
+    import hornsculpt_b200 as hs
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    for family, name, make in c3_cases(hs):
+        mesh = make()
+        if family == "horn":
+            exc = [hs.BemExcitation("throat", [hs.FaceVelocity(hs.meshes.HORN_THROAT, 1.0)])]
+            obs = [(0.0, 0.0, 1.0), (0.5, 0.0, 0.8), (0.0, 0.0, -1.0)]
+        else:
+            exc = [hs.BemExcitation("uniform", [hs.FaceVelocity(1, 1.0)])]
+            obs = OBSERVERS
+        v = mesh.vertices[mesh.triangles]
+        area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+        line = {"workload": "C3 mixed dense size", "family": family, "mesh": name, "N": mesh.vertex_count,
+                "T": mesh.triangle_count, "frequencies": C3_FREQUENCIES}
+        results = {}
+        with hs.CudaBemSolver(mesh) as solver:
+            solver.set_stream(stream.cuda_stream)
+            for form in ("fp64", "mixed"):
+                req = hs.BemRequest(frequencies=C3_FREQUENCIES, observers=obs, excitations=exc,
+                                    medium=hs.AcousticMedium(DENSITY, SOUND_SPEED),
+                                    numerics=hs.BemNumerics(precision=form))
+                solver.solve(req)  # plan, workspace and warm-up
+                solver.set_profiling(True)
+                t0 = time.perf_counter()
+                res = solver.solve(req)
+                wall = time.perf_counter() - t0
+                prof = solver.profile()
+                solver.set_profiling(False)
+                span = prof.pop("solve_span", (0.0, 0))[0]
+                results[form] = res
+                line[form] = {"ms_per_frequency": span / len(C3_FREQUENCIES),
+                              "wall_ms_per_frequency": 1e3 * wall / len(C3_FREQUENCIES),
+                              "solves_per_s": 1e3 * len(C3_FREQUENCIES) / span if span else None,
+                              "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])[:8]},
+                              "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations)}
+                if form == "mixed":
+                    line[form]["gmres_iterations"] = [e.iterations for f in res.frequencies for e in f.excitations]
+        err = 0.0
+        for fp, fm in zip(results["fp64"].frequencies, results["mixed"].frequencies):
+            a, b = fp.excitations[0].boundary.surface_pressure, fm.excitations[0].boundary.surface_pressure
+            err = max(err, float(np.sqrt((area * np.abs(b - a) ** 2).sum() / (area * np.abs(a) ** 2).sum())))
+        line["max_rel_err_surface_mixed_vs_fp64"] = err
+        line["mixed_over_fp64"] = line["fp64"]["ms_per_frequency"] / line["mixed"]["ms_per_frequency"]
+        print(json.dumps(line), flush=True)
+        del results
+        torch.cuda.empty_cache()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -247,10 +321,14 @@ def main():
                     help="solve only n sweep frequencies (small profiling cases)")
     ap.add_argument("--first-frequency", type=int, default=0,
                     help="index of the first sweep frequency solved (small profiling cases)")
+    ap.add_argument("--workload", default="c1", choices=["c1", "c3"],
+                    help="c1: the headline sweep; c3: mixed dense sizes N = 2k-8k (one line per mesh)")
     args = ap.parse_args()
     rank, world, local = env_rank()
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "c3":
+        return run_c3(args)
 
     import numpy as np
     import torch

@@ -140,42 +140,15 @@ def _meridian_piece(curve, length: float, h: float, interior_jitter, rng, jitter
     return [curve(x) for x in t]
 
 
-def exponential_horn(throat_radius: float = 0.025, mouth_radius: float = 0.15, length: float = 0.3,
-                     wall: float = 0.003, rear: float = 0.003, h: float | None = None, frequency: float = 8000.0,
-                     sound_speed: float = 343.0, seed: int = 0, jitter: float = 0.05,
-                     flare: float = 1.0) -> SurfaceMesh:
-    """Closed exponential-horn shell, meshed isotropically at edge length h.
+def _surface_of_revolution(pieces, h: float, rng, jitter: float, face_of_piece) -> SurfaceMesh:
+    """Mesh of the surface swept by a closed meridian about the z axis.
 
-    Inner skin r(z) = r_t exp(m z^flare / L^(flare-1)) from the throat (z = 0)
-    to the mouth (z = L, r = mouth radius); outer skin at r(z) + wall; an
-    annular mouth rim; a rigid rear cap body of thickness `rear` behind the
-    throat; the throat disc (face HORN_THROAT, Driven) closes the inner skin.
-    flare = 1 is the plain exponential; larger values bend the flare towards
-    the mouth. Default h is lambda/6 at `frequency`. Nodes move tangentially by
-    up to jitter * h (uniform, numpy Generator seeded with `seed`), except on
-    the axis and on the corner rings of the meridian. The surface is a solid of
-    revolution about z: genus 0, watertight, outward-oriented."""
-    if h is None:
-        h = sound_speed / frequency / 6.0
-    if not (0 < throat_radius < mouth_radius and length > 0 and wall > 0 and rear > 0 and h > 0):
-        raise ValueError("invalid horn dimensions")
-    rng = np.random.default_rng(seed)
-    m = math.log(mouth_radius / throat_radius)
-
-    def inner(z):
-        return throat_radius * math.exp(m * (z / length) ** flare)
-
-    ro0 = throat_radius + wall
-    rim_outer, rim_inner = inner(length) + wall, inner(length)
-    # meridian pieces (z, r), traversed so that the solid lies to the right
-    pieces = [
-        (lambda t: (-rear, t * ro0), ro0, False),                                   # rear cap disc
-        (lambda t: (-rear + t * rear, ro0), rear, False),                            # rear cap side
-        (lambda t: (t * length, inner(t * length) + wall), None, True),              # outer skin
-        (lambda t: (length, rim_outer - t * wall), wall, False),                     # mouth rim
-        (lambda t: ((1 - t) * length, inner((1 - t) * length)), None, True),         # inner skin
-        (lambda t: (0.0, throat_radius * (1 - t)), throat_radius, False),            # throat disc
-    ]
+    pieces: (curve(t) -> (z, r), arc length or None, jitter interior points)
+    traversed so that the solid lies to the right in the (z, r) half-plane and
+    starting and ending on the axis. Each meridian node becomes a ring of
+    max(3, round(2 pi r / h)) nodes (a single vertex on the axis); adjacent
+    rings are zipped by angle. Ring nodes move by up to jitter * h along the
+    ring except on corner rings (piece ends)."""
     meridian, corner, piece_of = [], [], []
     for index, (curve, plen, interior) in enumerate(pieces):
         if plen is None:
@@ -188,7 +161,6 @@ def exponential_horn(throat_radius: float = 0.025, mouth_radius: float = 0.15, l
             meridian.append(pts[k])
             corner.append(k == 0 or k == len(pts) - 1)
             piece_of.append(index)
-    # rings: the axis points are single vertices
     vertices, rings = [], []
     for i, (z, r) in enumerate(meridian):
         if r <= 1e-12:
@@ -213,7 +185,7 @@ def exponential_horn(throat_radius: float = 0.025, mouth_radius: float = 0.15, l
     triangles, faces = [], []
     for i in range(len(rings) - 1):
         A, B = rings[i], rings[i + 1]
-        face = HORN_THROAT if piece_of[i + 1] == 5 else HORN_SHELL  # the strip belongs to its outer node's piece
+        face = face_of_piece(piece_of[i + 1])  # the strip belongs to its outer node's piece
         if len(A) == 1 or len(B) == 1:
             if len(A) == 1:
                 for j in range(len(B)):
@@ -241,7 +213,58 @@ def exponential_horn(throat_radius: float = 0.025, mouth_radius: float = 0.15, l
             faces.append(face)
     verts = np.asarray(vertices)
     tris = np.asarray(triangles, dtype=np.int64)
-    mesh = SurfaceMesh(verts, tris, np.asarray(faces), np.where(np.asarray(faces) == HORN_THROAT, DRIVEN, WALL))
+    faces = np.asarray(faces)
+    mesh = SurfaceMesh(verts, tris, faces, np.where(faces == HORN_THROAT, DRIVEN, WALL))
     if signed_volume(mesh) < 0:
         mesh = SurfaceMesh(verts, tris[:, ::-1], mesh.face_ids, mesh.boundary)
     return mesh
+
+
+def exponential_horn(throat_radius: float = 0.025, mouth_radius: float = 0.15, length: float = 0.3,
+                     wall: float = 0.003, rear: float = 0.003, h: float | None = None, frequency: float = 8000.0,
+                     sound_speed: float = 343.0, seed: int = 0, jitter: float = 0.05,
+                     flare: float = 1.0) -> SurfaceMesh:
+    """Closed exponential-horn shell, meshed isotropically at edge length h.
+
+    Inner skin r(z) = r_t exp(m (z/L)^flare) with m = ln(r_mouth / r_t), from
+    the throat (z = 0) to the mouth (z = L); outer skin at r(z) + wall; an
+    annular mouth rim; a rigid rear cap body of thickness `rear` behind the
+    throat; the throat disc (face HORN_THROAT, Driven) closes the inner skin,
+    everything else is face HORN_SHELL (wall). flare = 1 is the plain
+    exponential; larger values bend the flare towards the mouth. Default h is
+    lambda/6 at `frequency`. Nodes move tangentially by up to jitter * h
+    (uniform, numpy Generator seeded with `seed`), except on the axis and the
+    corner rings. A solid of revolution about z: genus 0, watertight,
+    outward-oriented."""
+    if h is None:
+        h = sound_speed / frequency / 6.0
+    if not (0 < throat_radius < mouth_radius and length > 0 and wall > 0 and rear > 0 and h > 0):
+        raise ValueError("invalid horn dimensions")
+    rng = np.random.default_rng(seed)
+    m = math.log(mouth_radius / throat_radius)
+
+    def inner(z):
+        return throat_radius * math.exp(m * (z / length) ** flare)
+
+    ro0 = throat_radius + wall
+    rim_outer = inner(length) + wall
+    pieces = [
+        (lambda t: (-rear, t * ro0), ro0, False),                                   # rear cap disc
+        (lambda t: (-rear + t * rear, ro0), rear, False),                            # rear cap side
+        (lambda t: (t * length, inner(t * length) + wall), None, True),              # outer skin
+        (lambda t: (length, rim_outer - t * wall), wall, False),                     # mouth rim
+        (lambda t: ((1 - t) * length, inner((1 - t) * length)), None, True),         # inner skin
+        (lambda t: (0.0, throat_radius * (1 - t)), throat_radius, False),            # throat disc
+    ]
+    return _surface_of_revolution(pieces, h, rng, jitter, lambda p: HORN_THROAT if p == 5 else HORN_SHELL)
+
+
+def revolved_sphere(radius: float = 0.1, h: float = 0.01, seed: int = 0, jitter: float = 0.05,
+                    face_id: int = 1) -> SurfaceMesh:
+    """Sphere meshed by rings at edge length h (any size between the
+    icosahedral levels), all one Driven face; seeded tangential jitter."""
+    rng = np.random.default_rng(seed)
+    pieces = [(lambda t: (-radius * math.cos(math.pi * t), radius * math.sin(math.pi * t)), math.pi * radius, True)]
+    mesh = _surface_of_revolution(pieces, h, rng, jitter, lambda p: HORN_THROAT)
+    return SurfaceMesh(mesh.vertices, mesh.triangles, np.full(mesh.triangle_count, face_id),
+                       np.full(mesh.triangle_count, DRIVEN))

@@ -195,3 +195,11 @@ def test_flat_faces_accepted():
     """Coplanar triangles without a common vertex are separated by in-plane
     axes: a box with flat gridded sides is a valid exterior surface."""
     assert _passes_host_validation(_box(4))
+
+
+def test_revolved_sphere():
+    s = meshes.revolved_sphere(radius=0.1, h=0.004, seed=3)
+    assert 7500 < s.vertex_count < 8300
+    assert abs(meshes.signed_volume(s) - 4 / 3 * np.pi * 0.1 ** 3) < 2e-3 * 4 / 3 * np.pi * 0.1 ** 3
+    assert np.allclose(np.linalg.norm(s.vertices, axis=1), 0.1)
+    assert _passes_host_validation(meshes.revolved_sphere(radius=0.1, h=0.02))
