@@ -57,6 +57,16 @@ class hs_frequency_info(C.Structure):
                 ("interaction_plan_reused", C.c_int32)]
 
 
+class hs_serve_options(C.Structure):
+    _fields_ = [("workers", C.c_uint32), ("memory_fraction", C.c_double), ("resident_meshes", C.c_uint32),
+                ("planning_frequency", C.c_double), ("max_batch_frequencies", C.c_uint32)]
+
+
+class hs_serve_timing(C.Structure):
+    _fields_ = [("queue_ms", C.c_double), ("run_ms", C.c_double), ("latency_ms", C.c_double),
+                ("footprint_bytes", C.c_size_t), ("batched_requests", C.c_uint32)]
+
+
 PROGRESS_FN = C.CFUNCTYPE(None, C.POINTER(hs_progress), C.c_void_p)
 _P = C.c_void_p
 _lib = None
@@ -109,6 +119,12 @@ def load():
                                                     C.c_uint32, C.c_int32, _P, C.c_double, C.c_double, C.c_uint32,
                                                     _P, _P]),
         "hs_bem_debug_assemble": (C.c_int, [_P, C.POINTER(hs_numerics), C.c_double, C.c_double, _P, _P, _P]),
+        "hs_serve_options_default": (None, [C.POINTER(hs_serve_options)]),
+        "hs_serve_create": (C.c_int, [C.POINTER(hs_serve_options), C.POINTER(_P)]),
+        "hs_serve_submit": (C.c_int, [_P, _P, C.c_size_t, _P, _P, _P, C.c_size_t, C.POINTER(hs_request),
+                                      C.POINTER(C.c_uint64)]),
+        "hs_serve_wait": (C.c_int, [_P, C.c_uint64, C.POINTER(_P), C.POINTER(hs_serve_timing)]),
+        "hs_serve_destroy": (None, [_P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import functools
 from typing import Callable, Optional, Sequence
 
 import numpy as np
@@ -200,6 +201,7 @@ class CudaBemSolver:
         self.close()
 
     @staticmethod
+    @functools.lru_cache(maxsize=None)
     def device_description() -> str:
         buf = C.create_string_buffer(256)
         _lib.check(_lib.load().hs_device_description(buf, 256))
@@ -333,6 +335,89 @@ class CudaBemSolver:
         _lib.check(self._lib.hs_bem_debug_assemble(self._handle, C.byref(n), plan_k, k, q.ctypes.data, A.ctypes.data,
                                                    b.ctypes.data))
         return _cplx(A).reshape(N, N).T, _cplx(b)  # column-major -> [row, col]
+
+
+@dataclasses.dataclass
+class ServeOptions:
+    """hs_serve_options: the serving form's request loop."""
+    workers: int = 4
+    memory_fraction: float = 0.6
+    resident_meshes: int = 8
+    planning_frequency: float = 0.0   # Hz; > 0: every request plans at this frequency
+    max_batch_frequencies: int = 32
+
+
+@dataclasses.dataclass
+class ServeTiming:
+    queue_ms: float
+    run_ms: float
+    latency_ms: float
+    footprint_bytes: int
+    batched_requests: int
+
+
+class BemServer:
+    """Serving form: a persistent request loop on the current CUDA device.
+
+    submit() copies a mesh and request and returns a ticket at once; the
+    library admits requests in arrival order as device memory allows, runs up
+    to `workers` at once on separate streams (requests on different meshes
+    overlap on the GPU), keeps meshes resident for reuse and batches queued
+    requests on the same mesh. wait(ticket) returns (BemResult, ServeTiming)."""
+
+    _c_request = CudaBemSolver._c_request
+    _read = CudaBemSolver._read
+    device_description = staticmethod(CudaBemSolver.device_description)
+
+    def __init__(self, options: ServeOptions = ServeOptions()):
+        lib = _lib.load()
+        o = _lib.hs_serve_options()
+        lib.hs_serve_options_default(C.byref(o))
+        for f in dataclasses.fields(options):
+            setattr(o, f.name, getattr(options, f.name))
+        handle = C.c_void_p()
+        _lib.check(lib.hs_serve_create(C.byref(o), C.byref(handle)))
+        self._handle, self._lib = handle, lib
+        self._requests = {}
+
+    def submit(self, mesh: SurfaceMesh, request: BemRequest) -> int:
+        req, keep = self._c_request(request)
+        ticket = C.c_uint64()
+        _lib.check(self._lib.hs_serve_submit(self._handle, mesh.vertices.ctypes.data, mesh.vertex_count,
+                                             mesh.triangles.ctypes.data, mesh.face_ids.ctypes.data,
+                                             mesh.boundary.ctypes.data, mesh.triangle_count, C.byref(req),
+                                             C.byref(ticket)))
+        del keep
+        self._requests[ticket.value] = request
+        return ticket.value
+
+    def wait(self, ticket: int):
+        request = self._requests.pop(ticket, None)
+        if request is None:
+            raise ValueError("Unknown or already collected serving ticket.")
+        out = C.c_void_p()
+        t = _lib.hs_serve_timing()
+        status = self._lib.hs_serve_wait(self._handle, ticket, C.byref(out), C.byref(t))
+        _lib.check(status)
+        try:
+            result = self._read(out, request)
+        finally:
+            self._lib.hs_result_free(out)
+        return result, ServeTiming(t.queue_ms, t.run_ms, t.latency_ms, t.footprint_bytes, t.batched_requests)
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.hs_serve_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def host_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float) -> dict:

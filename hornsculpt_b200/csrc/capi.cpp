@@ -1,6 +1,7 @@
 // extern "C" entry points of include/hs_bem.h: exceptions of the session
 // layer become hs_status codes plus a thread-local message.
 #include "hs_bem.h"
+#include "serve.hpp"
 #include "session.hpp"
 
 #include <cstring>
@@ -13,6 +14,9 @@ struct hs_bem_session {
 };
 struct hs_result {
     std::unique_ptr<Result> impl;
+};
+struct hs_server {
+    std::unique_ptr<Server> impl;
 };
 
 namespace {
@@ -354,5 +358,79 @@ hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_co
                              tolerance, maximum_depth, static_cast<cudaStream_t>(cuda_stream), observer_pressure);
     });
 }
+
+void hs_serve_options_default(hs_serve_options *o) {
+    if (!o)
+        return;
+    *o = hs_serve_options{};
+    o->workers = 4;
+    o->memory_fraction = 0.6;
+    o->resident_meshes = 8;
+    o->planning_frequency = 0;
+    o->max_batch_frequencies = 32;
+}
+
+hs_status hs_serve_create(const hs_serve_options *options, hs_server **out) {
+    if (!options || !out)
+        return fail(HS_E_INVALID, "Serving options and output pointer must be non-null.");
+    *out = nullptr;
+    return guarded([&]() {
+        auto s = std::make_unique<hs_server>();
+        s->impl = std::make_unique<Server>(*options);
+        *out = s.release();
+    });
+}
+
+hs_status hs_serve_submit(hs_server *server, const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                          const uint32_t *face_ids, const uint8_t *boundary, size_t triangle_count,
+                          const hs_request *request, uint64_t *ticket) {
+    if (!server || !request || !ticket)
+        return fail(HS_E_INVALID, "Server, request and ticket pointers must be non-null.");
+    if ((!vertices && vertex_count) || (!triangle_count || !triangles || !face_ids || !boundary))
+        return fail(HS_E_INVALID, "BEM mesh has no vertices.");
+    if (!request->frequency_count || !request->frequencies || (request->observer_count && !request->observers) ||
+        !request->excitation_count || !request->excitation_face_offsets)
+        return fail(HS_E_INVALID, "Invalid BEM medium, frequencies, excitation or Galerkin settings.");
+    const size_t faces = request->excitation_face_offsets[request->excitation_count];
+    if (faces && (!request->excitation_face_ids || !request->excitation_velocities))
+        return fail(HS_E_INVALID, "Excitation must assign each known Driven face at most once.");
+    return guarded([&]() {
+        MeshInput mesh;
+        mesh.vertices.resize(vertex_count);
+        for (size_t i = 0; i < vertex_count; ++i)
+            mesh.vertices[i] = V3{vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]};
+        mesh.triangles.assign(triangles, triangles + 3 * triangle_count);
+        mesh.faces.assign(face_ids, face_ids + triangle_count);
+        mesh.driven.resize(triangle_count);
+        for (size_t t = 0; t < triangle_count; ++t) {
+            if (boundary[t] > HS_DRIVEN)
+                throw InvalidArgument("Triangle boundary must be wall (0) or driven (1).");
+            mesh.driven[t] = boundary[t];
+        }
+        *ticket = server->impl->submit(std::move(mesh), *request);
+    });
+}
+
+hs_status hs_serve_wait(hs_server *server, uint64_t ticket, hs_result **out, hs_serve_timing *timing) {
+    if (!server || !out)
+        return fail(HS_E_INVALID, "Server and result pointers must be non-null.");
+    *out = nullptr;
+    return guarded([&]() {
+        hs_serve_timing t{};
+        auto r = std::make_unique<hs_result>();
+        try {
+            r->impl = server->impl->wait(ticket, t);
+        } catch (...) {
+            if (timing)
+                *timing = t;
+            throw;
+        }
+        if (timing)
+            *timing = t;
+        *out = r.release();
+    });
+}
+
+void hs_serve_destroy(hs_server *server) { delete server; }
 
 }  // extern "C"

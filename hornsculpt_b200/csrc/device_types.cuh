@@ -158,14 +158,15 @@ void roundToFloat(const double *in, float *out, size_t count, cudaStream_t strea
 
 // One left-preconditioned GMRES cycle (at most m Arnoldi steps) per system of
 // a batch: solves A_f d = r_s with M = the FP32 LU of A_f and adds d to x_s
-// (systems s = f * E + e; a zero r_s is left alone). Stops a system once its
-// preconditioned residual estimate is at most tol relative to its start.
+// (systems s = f * E + e; a zero r_s is left alone). Stops system s once its
+// preconditioned residual estimate is at most tolerances[s] relative to its
+// start, so each system's result does not depend on the others in the batch.
 // Returns the Arnoldi steps taken by the batch; stepsOut[s] holds each
 // system's. The workspace holds gmresWorkspaceBytes(N, B * E, m) bytes.
 size_t gmresWorkspaceBytes(uint32_t N, uint32_t S, uint32_t m);
 uint32_t gmresCycleBatch(const double *A, const float *LU32, const int *pivots, uint32_t N, uint32_t B, uint32_t E,
-                         const double *r, double *x, uint32_t m, double tol, void *workspace, cudaStream_t stream,
-                         KernelTimer *timer, std::vector<uint32_t> &stepsOut);
+                         const double *r, double *x, uint32_t m, const std::vector<double> &tolerances,
+                         void *workspace, cudaStream_t stream, KernelTimer *timer, std::vector<uint32_t> &stepsOut);
 
 // Observer fields of one rule degree for every (batch, excitation, observer).
 struct FieldRequest {

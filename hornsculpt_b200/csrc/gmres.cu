@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256) normalizeKernel(const double *z, uint32_t
 // the rotated right-hand side g and the residual estimate |g_{j+1}| / beta.
 // Rotation k is (c_k real, s_k complex): [x; y] -> [c x + s y; -conj(s) x + c y].
 __global__ void givensKernel(uint32_t S, uint32_t m, uint32_t j, double *hess, double *rot, double *g,
-                             const double *beta, double tol, double *estimate, int *active, uint32_t *steps) {
+                             const double *beta, const double *tol, double *estimate, int *active, uint32_t *steps) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= S || !active[s])
         return;
@@ -229,7 +229,7 @@ __global__ void givensKernel(uint32_t S, uint32_t m, uint32_t j, double *hess, d
     const double est = hypot(gs[j + 1].x, gs[j + 1].y) / beta[s];
     estimate[s] = est;
     steps[s] = j + 1;
-    if (!(est > tol) || j + 1 == m)
+    if (!(est > tol[s]) || j + 1 == m)
         active[s] = 0;
 }
 
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256) updateKernel(const double *basis, const d
 
 // Workspace pieces, each 256-byte aligned, in carve order.
 struct GmresLayout {
-    size_t basis, hess, g, dots, rot, beta, estimate, active, steps, z, z32, total;
+    size_t basis, hess, g, dots, rot, beta, estimate, tol, active, steps, z, z32, total;
 };
 
 GmresLayout gmresLayout(uint32_t N, uint32_t S, uint32_t m) {
@@ -293,6 +293,7 @@ GmresLayout gmresLayout(uint32_t N, uint32_t S, uint32_t m) {
     l.rot = take(size_t(S) * m * 24);
     l.beta = take(size_t(S) * 8);
     l.estimate = take(size_t(S) * 8);
+    l.tol = take(size_t(S) * 8);
     l.active = take(size_t(S) * 4);
     l.steps = take(size_t(S) * 4);
     l.z = take(size_t(S) * N * 16);
@@ -304,8 +305,8 @@ GmresLayout gmresLayout(uint32_t N, uint32_t S, uint32_t m) {
 size_t gmresWorkspaceBytes(uint32_t N, uint32_t S, uint32_t m) { return gmresLayout(N, S, m).total; }
 
 uint32_t gmresCycleBatch(const double *A, const float *LU32, const int *pivots, uint32_t N, uint32_t B, uint32_t E,
-                         const double *r, double *x, uint32_t m, double tol, void *workspace, cudaStream_t stream,
-                         KernelTimer *timer, std::vector<uint32_t> &stepsOut) {
+                         const double *r, double *x, uint32_t m, const std::vector<double> &tolerances,
+                         void *workspace, cudaStream_t stream, KernelTimer *timer, std::vector<uint32_t> &stepsOut) {
     const uint32_t S = B * E;
     const GmresLayout l = gmresLayout(N, S, m);
     char *w = static_cast<char *>(workspace);
@@ -316,6 +317,11 @@ uint32_t gmresCycleBatch(const double *A, const float *LU32, const int *pivots, 
     double *rot = reinterpret_cast<double *>(w + l.rot);
     double *beta = reinterpret_cast<double *>(w + l.beta);
     double *estimate = reinterpret_cast<double *>(w + l.estimate);
+    double *tol = reinterpret_cast<double *>(w + l.tol);
+    if (tolerances.size() != S)
+        throw std::runtime_error("GMRES needs one tolerance per system.");
+    check(cudaMemcpyAsync(tol, tolerances.data(), S * sizeof(double), cudaMemcpyHostToDevice, stream),
+          "GMRES tolerances");
     int *active = reinterpret_cast<int *>(w + l.active);
     uint32_t *steps = reinterpret_cast<uint32_t *>(w + l.steps);
     double *z = reinterpret_cast<double *>(w + l.z);

@@ -298,14 +298,41 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
     planMs_ = msSince(start);
 }
 
+namespace {
+uint64_t perFrequencyBytes(uint64_t T, uint64_t N, uint32_t E, uint32_t O, bool mixed, uint32_t restart) {
+    return assemblyWorkspaceBytes(uint32_t(T), uint32_t(N), E, 1, mixed) + 2 * N * N * 16 + 4 * E * N * 16 +
+           E * T * 16 + fieldPartialsBytes(uint32_t(T), E, O, 1) +
+           (mixed ? gmresWorkspaceBytes(uint32_t(N), E, restart) : 0) + 64;
+}
+}  // namespace
+
+size_t solveFootprint(size_t T, size_t N, uint32_t E, uint32_t O, uint32_t B, bool mixed, uint32_t restart) {
+    // geometry (panels, bounds, FP32 panels, incidence, scales) and plan
+    // (pair codes, touching jobs, near pairs and patches at about a dozen
+    // neighbours per panel)
+    const size_t geometry = T * (200 + 48 + 112 + 16) + N * 24, plan = T * (T - 1) / 2 + T * 16 * 40 + T * 16 * 220;
+    return geometry + plan + B * perFrequencyBytes(T, N, E, O, mixed, restart);
+}
+
+size_t Session::residentBytes() const {
+    size_t bytes = 0;
+    for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dMixedPanels_, &dIncOffsets_, &dIncPanel_, &dIncLocal_,
+                                  &dRowScale_, &dMass_, &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_,
+                                  &dSingularTable_, &dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dA_,
+                                  &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_, &dPivots_, &dKs_, &dFlux_, &dObservers_,
+                                  &dPartials_, &dField_, &dDegrees_, &dWork32_, &dGmres_})
+        bytes += b->bytes();
+    return bytes;
+}
+
 uint32_t Session::chooseBatch(uint32_t F, uint32_t E, uint32_t O, bool mixed, uint32_t restart) const {
     const uint64_t T = space_.panels.size(), N = space_.vertices.size();
-    const uint64_t perFrequency = assemblyWorkspaceBytes(uint32_t(T), uint32_t(N), E, 1, mixed) + 2 * N * N * 16 +
-                                  4 * E * N * 16 + E * T * 16 + fieldPartialsBytes(uint32_t(T), E, O, 1) +
-                                  (mixed ? gmresWorkspaceBytes(uint32_t(N), E, restart) : 0) + 64;
+    const uint64_t perFrequency = perFrequencyBytes(T, N, E, O, mixed, restart);
     size_t free = 0, total = 0;
     cuda(cudaMemGetInfo(&free, &total), "CUDA memory query");
-    const uint64_t budget = uint64_t(double(free) * .6);
+    uint64_t budget = uint64_t(double(free) * .6);
+    if (memoryBudget_)
+        budget = std::min<uint64_t>(budget, memoryBudget_);
     if (perFrequency > budget)
         throw OutOfMemory("BEM dense workspace of " + std::to_string(perFrequency >> 20) + " MiB per frequency exceeds the " +
                           std::to_string(budget >> 20) + " MiB device budget.");
@@ -589,13 +616,14 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 break;
             const auto t0 = Clock::now();
             if (mixed) {
-                // GMRES-IR: one FP64 GMRES cycle on A d = r, preconditioned by the
-                // FP32 LU, reducing the preconditioned residual far enough that
-                // the worst system lands a hundredfold below the target.
-                const double worst = *std::max_element(relative.begin(), relative.end());
-                const double tol = std::clamp(.01 * target / worst, 1e-13, .5);
+                // GMRES-IR: one FP64 GMRES cycle on A d = r per system, preconditioned
+                // by the FP32 LU, reducing each system's preconditioned residual far
+                // enough that it lands a hundredfold below the target.
+                std::vector<double> tolerances(relative.size());
+                for (size_t q = 0; q < relative.size(); ++q)
+                    tolerances[q] = relative[q] > 0 ? std::clamp(.01 * target / relative[q], 1e-13, .5) : .5;
                 gmresCycleBatch(dA_.as<double>(), LU32, dPivots_.as<int>(), N, B, E, dCorr_.as<double>(),
-                                dX_.as<double>(), restart, tol, dGmres_.as<void>(), s, &timer_, cycle);
+                                dX_.as<double>(), restart, tolerances, dGmres_.as<void>(), s, &timer_, cycle);
                 for (size_t q = 0; q < cycle.size(); ++q)
                     krylov[q] += cycle[q];
             } else {

@@ -62,6 +62,11 @@ class Session {
     void debugAssemble(const hs_numerics &numerics, double planK, double k, const double *flux, double *matrix,
                        double *rhs);
     KernelTimer &timer() { return timer_; }
+    // Device bytes a solve may hold beyond the resident geometry and plan
+    // (0: 60 % of free memory); bounds the frequency batch.
+    void setMemoryBudget(size_t bytes) { memoryBudget_ = bytes; }
+    // Device bytes held now (geometry, plan and grown workspaces).
+    size_t residentBytes() const;
     // regular pairs per bin (4), regular samples, touching samples, near samples, frequencies
     std::vector<uint64_t> work = std::vector<uint64_t>(8, 0);
     std::mutex mutex;
@@ -97,6 +102,12 @@ class Session {
     DeviceBuffer dRecords_, dColumns_, dPanelRhs_, dBins_, dBinCounts_, dA_, dLU_, dRhs_, dX_, dCorr_, dNorms_,
         dPivots_, dInfo_, dKs_, dFlux_, dObservers_, dPartials_, dField_, dDegrees_, dWork32_, dGmres_;
     size_t peakBytes_ = 0;
+    size_t memoryBudget_ = 0;
 };
+
+// Device bytes of one solve of F frequencies on a mesh with T panels and N
+// vertices, batched B at a time: workspace of the batch plus the session's
+// geometry and plan (for admission before a session exists).
+size_t solveFootprint(size_t T, size_t N, uint32_t E, uint32_t O, uint32_t B, bool mixed, uint32_t restart);
 
 }  // namespace hsb

@@ -240,6 +240,10 @@ def exponential_horn(throat_radius: float = 0.025, mouth_radius: float = 0.15, l
         h = sound_speed / frequency / 6.0
     if not (0 < throat_radius < mouth_radius and length > 0 and wall > 0 and rear > 0 and h > 0):
         raise ValueError("invalid horn dimensions")
+    # ring facets bulge by about h^2 / (8 r) towards the axis: keep that below half
+    # the wall at the throat, or the inner and outer skins cross
+    if h * h / (8 * throat_radius) > 0.5 * wall:
+        raise ValueError(f"edge length {h} m is too coarse for a {wall} m wall at a {throat_radius} m throat")
     rng = np.random.default_rng(seed)
     m = math.log(mouth_radius / throat_radius)
 

@@ -246,6 +246,50 @@ hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_co
                                         double far_reference_distance, double tolerance, uint32_t maximum_depth,
                                         void *cuda_stream, double *observer_pressure);
 
+/* ---------------------------------------------------------------------------
+ * Serving form (no reference counterpart; the reference solves one request per
+ * CudaBemSolver::solve call): a persistent request loop on the current device.
+ * Requests (mesh + request) are submitted at any time and admitted in arrival
+ * order as device memory allows (by the estimated footprint of the solve);
+ * `workers` requests run at once, each on its own CUDA stream, so requests on
+ * different meshes overlap on the GPU. Sessions stay resident per mesh
+ * (geometry, plan, workspaces; least recently used evicted), and queued
+ * requests on the same mesh with the same settings are solved in one call with
+ * their frequencies batched. With planning_frequency > 0 every request plans
+ * its interactions at that frequency, so a result is the same whatever it was
+ * batched with (frequencies above it are rejected).
+ * ------------------------------------------------------------------------- */
+typedef struct hs_server hs_server;
+
+typedef struct hs_serve_options {
+    uint32_t workers;                     /* requests on the device at once (default 4) */
+    double memory_fraction;               /* share of the device memory free at creation that
+                                             admitted requests may hold (default 0.6) */
+    uint32_t resident_meshes;             /* sessions kept for reuse (default 8) */
+    double planning_frequency;            /* Hz; 0 plans per request (default 0) */
+    uint32_t max_batch_frequencies;       /* frequencies factored together (1..32, default 32) */
+} hs_serve_options;
+
+typedef struct hs_serve_timing {
+    double queue_ms;                      /* arrival to start on a worker */
+    double run_ms;                        /* start to finish */
+    double latency_ms;                    /* arrival to finish */
+    size_t footprint_bytes;               /* device bytes reserved at admission */
+    uint32_t batched_requests;            /* requests solved in the same session call */
+} hs_serve_timing;
+
+void hs_serve_options_default(hs_serve_options *options);
+hs_status hs_serve_create(const hs_serve_options *options, hs_server **out);
+/* Copies the mesh and request; validates the mesh and frequencies at once. */
+hs_status hs_serve_submit(hs_server *server, const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                          const uint32_t *face_ids, const uint8_t *boundary, size_t triangle_count,
+                          const hs_request *request, uint64_t *ticket);
+/* Blocks until the request is done; returns its result (free with
+ * hs_result_free) or its error status. Each ticket is collected once. */
+hs_status hs_serve_wait(hs_server *server, uint64_t ticket, hs_result **out, hs_serve_timing *timing);
+/* Cancels queued requests, finishes running ones, releases the device state. */
+void hs_serve_destroy(hs_server *server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -203,3 +203,8 @@ def test_revolved_sphere():
     assert abs(meshes.signed_volume(s) - 4 / 3 * np.pi * 0.1 ** 3) < 2e-3 * 4 / 3 * np.pi * 0.1 ** 3
     assert np.allclose(np.linalg.norm(s.vertices, axis=1), 0.1)
     assert _passes_host_validation(meshes.revolved_sphere(radius=0.1, h=0.02))
+
+
+def test_horn_too_coarse_for_its_wall():
+    with pytest.raises(ValueError, match="too coarse"):
+        meshes.exponential_horn(h=0.03)
