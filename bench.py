@@ -309,6 +309,133 @@ def run_c3(args):
         torch.cuda.empty_cache()
 
 
+def serve_stream(hs, count: int, seed: int, rate: float, distinct: int = 0):
+    """Seeded Poisson stream of horn requests: throat U[15, 50] mm, mouth
+    U[80, 300] mm, length U[100, 600] mm, flare exponent U[1, 4], triangle
+    count log-uniform in [2k, 4k] (the dense form's range at interactive
+    planning cost; larger meshes need the FMM form), wall max(3 mm, 1.2 h) so
+    the mouth rim meshes with angles >= 20 degrees, 1-16 frequencies
+    log-uniform in 200 Hz-20 kHz kept where k * (longest edge) <= 1.9 (below
+    the plan's all-pairs switch at 2). Returns [(arrival_s, mesh, frequencies)]
+    and the number of rejected frequencies."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    stream, t, rejected = [], 0.0, 0
+    if distinct:
+        # a design-iteration stream: `distinct` horns, each request a random subset of
+        # its mesh's 16-point raster (passed as the planning raster, so plans are reused)
+        designs, _ = serve_stream(hs, distinct, seed + 1, rate)
+        rasters = []
+        for _, mesh, _, _ in designs:
+            fmax = min(20000.0, 1.9 / mesh.max_edge() * SOUND_SPEED / (2 * math.pi))
+            rasters.append([float(f) for f in np.round(np.geomspace(200.0, fmax, 16), 3)])
+        while len(stream) < count:
+            d = int(rng.integers(distinct))
+            n = int(rng.integers(1, 17))
+            freqs = sorted(rng.choice(rasters[d], size=n, replace=False).tolist())
+            t += rng.exponential(1.0 / rate)
+            stream.append((t, designs[d][1], freqs, rasters[d]))
+        return stream, 0
+    while len(stream) < count:
+        throat, mouth = rng.uniform(0.015, 0.050), rng.uniform(0.080, 0.300)
+        length, flare = rng.uniform(0.100, 0.600), rng.uniform(1.0, 4.0)
+        target = math.exp(rng.uniform(math.log(2000), math.log(4000)))
+        z = np.linspace(0, length, 400)
+        r = throat * np.exp(math.log(mouth / throat) * (z / length) ** flare)
+        lateral = float(np.sum(np.pi * (r[1:] + r[:-1]) * np.hypot(np.diff(z), np.diff(r))))
+        h = math.sqrt(2.1 * lateral / (0.433 * target))
+        wall = max(0.003, 1.2 * h)
+        mesh = hs.meshes.exponential_horn(throat, mouth, length, wall=wall, rear=wall, h=h,
+                                          seed=int(rng.integers(1 << 31)), flare=flare)
+        kmax = 1.9 / mesh.max_edge()
+        freqs = sorted(set(np.round(np.exp(rng.uniform(math.log(200), math.log(20000), int(rng.integers(1, 17)))), 3)))
+        kept = [float(f) for f in freqs if 2 * math.pi * f / SOUND_SPEED <= kmax]
+        rejected += len(freqs) - len(kept)
+        t += rng.exponential(1.0 / rate)
+        if kept:
+            stream.append((t, mesh, kept, None))
+    return stream, rejected
+
+
+def run_serve(args):
+    """Serving form on the stream above, mixed form and plain FP64 form back to
+    back on the same B200: freq-point solves/s over the makespan and p50/p99
+    request latency (arrival to result, measured inside the library)."""
+    import threading
+
+    import numpy as np
+
+    import hornsculpt_b200 as hs
+
+    stream, rejected = serve_stream(hs, args.serve_requests, args.serve_seed, args.serve_rate, args.serve_distinct)
+    line = {"workload": "C5 serving loop (seeded Poisson horn stream" +
+                        (f", {args.serve_distinct} designs revisited" if args.serve_distinct else ", every mesh new") + ")",
+            "requests": len(stream),
+            "rate_per_s": args.serve_rate, "seed": args.serve_seed, "rejected_frequencies": rejected,
+            "frequency_points": sum(len(f) for _, _, f, _ in stream),
+            "triangles": [min(m.triangle_count for _, m, _, _ in stream), max(m.triangle_count for _, m, _, _ in stream)]}
+    for form in ("mixed", "fp64"):
+        latencies, errors = [None] * len(stream), []
+        with hs.BemServer(hs.ServeOptions(workers=args.serve_workers)) as server:
+            # warm the library (CUDA context, rule tables) outside the timed stream
+            warm = stream[0]
+            server.wait(server.submit(meshes_warm := hs.meshes.icosphere(2), hs.BemRequest(
+                frequencies=[500.0], excitations=[hs.BemExcitation("u", [hs.FaceVelocity(1, 1.0)])],
+                numerics=hs.BemNumerics(precision=form))))
+            del warm, meshes_warm
+            tickets = [None] * len(stream)
+            done = threading.Event()
+            abandon = threading.Event()
+
+            def collect():
+                for i in range(len(stream)):
+                    while tickets[i] is None:
+                        if abandon.is_set():
+                            return
+                        time.sleep(0.0005)
+                    if tickets[i] < 0:
+                        continue
+                    try:
+                        _, timing = server.wait(tickets[i])
+                        latencies[i] = timing.latency_ms
+                    except Exception as e:  # recorded, not fatal
+                        errors.append(f"{type(e).__name__}: {e}")
+                done.set()
+
+            waiter = threading.Thread(target=collect, daemon=True)
+            waiter.start()
+            t0 = time.perf_counter()
+            try:
+                for i, (arrival, mesh, freqs, raster) in enumerate(stream):
+                    delay = arrival - (time.perf_counter() - t0)
+                    if delay > 0:
+                        time.sleep(delay)
+                    req = hs.BemRequest(frequencies=freqs, observers=[(0.0, 0.0, 1.0)],
+                                        excitations=[hs.BemExcitation("throat",
+                                                                      [hs.FaceVelocity(hs.meshes.HORN_THROAT, 1.0)])],
+                                        numerics=hs.BemNumerics(precision=form),
+                                        interaction_plan_frequencies=raster or [])
+                    try:
+                        tickets[i] = server.submit(mesh, req)
+                    except Exception as e:  # recorded, not fatal
+                        errors.append(f"submit {type(e).__name__}: {e}")
+                        tickets[i] = -1
+            finally:
+                if not done.wait(timeout=args.serve_timeout):
+                    abandon.set()
+                    errors.append("stream did not finish within the serving timeout")
+            makespan = time.perf_counter() - t0
+        ok = [x for x in latencies if x is not None]
+        points = sum(len(f) for (_, _, f, _), x in zip(stream, latencies) if x is not None)
+        line[form] = {"solves_per_s": points / makespan, "makespan_s": makespan,
+                      "p50_ms": float(np.percentile(ok, 50)) if ok else None,
+                      "p99_ms": float(np.percentile(ok, 99)) if ok else None,
+                      "completed": len(ok), "errors": errors[:5]}
+    line["mixed_over_fp64_solves_per_s"] = line["mixed"]["solves_per_s"] / line["fp64"]["solves_per_s"]
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -321,14 +448,24 @@ def main():
                     help="solve only n sweep frequencies (small profiling cases)")
     ap.add_argument("--first-frequency", type=int, default=0,
                     help="index of the first sweep frequency solved (small profiling cases)")
-    ap.add_argument("--workload", default="c1", choices=["c1", "c3"],
-                    help="c1: the headline sweep; c3: mixed dense sizes N = 2k-8k (one line per mesh)")
+    ap.add_argument("--workload", default="c1", choices=["c1", "c3", "serve"],
+                    help="c1: the headline sweep; c3: mixed dense sizes N = 2k-8k (one line per mesh); "
+                         "serve: the serving loop on a seeded Poisson horn stream")
+    ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--serve-rate", type=float, default=1.0, help="mean arrivals per second")
+    ap.add_argument("--serve-timeout", type=float, default=400.0, help="seconds to wait for a stream to drain")
+    ap.add_argument("--serve-seed", type=int, default=2026)
+    ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--serve-distinct", type=int, default=0,
+                    help="> 0: requests revisit this many horn designs (planning rasters reused)")
     args = ap.parse_args()
     rank, world, local = env_rank()
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload == "c3":
         return run_c3(args)
+    if args.workload == "serve":
+        return run_serve(args)
 
     import numpy as np
     import torch

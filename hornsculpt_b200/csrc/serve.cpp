@@ -42,6 +42,8 @@ double msBetween(std::chrono::steady_clock::time_point a, std::chrono::steady_cl
 
 RequestCopy::RequestCopy(const hs_request &r) : base(r) {
     frequencies.assign(r.frequencies, r.frequencies + r.frequency_count);
+    if (r.plan_frequency_count)
+        raster.assign(r.plan_frequencies, r.plan_frequencies + r.plan_frequency_count);
     observers.assign(r.observers, r.observers + 3 * r.observer_count);
     offsets.assign(r.excitation_face_offsets, r.excitation_face_offsets + r.excitation_count + 1);
     const size_t faces = offsets.back();
@@ -52,12 +54,12 @@ RequestCopy::RequestCopy(const hs_request &r) : base(r) {
     base.plan_frequency_count = 0;
 }
 
-hs_request RequestCopy::view(const std::vector<double> &freqs, const std::vector<double> &raster) const {
+hs_request RequestCopy::view(const std::vector<double> &freqs, const std::vector<double> &planRaster) const {
     hs_request r = base;
     r.frequencies = freqs.data();
     r.frequency_count = freqs.size();
-    r.plan_frequencies = raster.empty() ? nullptr : raster.data();
-    r.plan_frequency_count = raster.size();
+    r.plan_frequencies = planRaster.empty() ? nullptr : planRaster.data();
+    r.plan_frequency_count = planRaster.size();
     r.observers = observers.empty() ? nullptr : observers.data();
     r.excitation_face_offsets = offsets.data();
     r.excitation_face_ids = faceIds.empty() ? nullptr : faceIds.data();
@@ -71,7 +73,7 @@ bool RequestCopy::compatible(const RequestCopy &o) const {
            base.far_field == o.base.far_field && std::memcmp(base.far_origin, o.base.far_origin, sizeof base.far_origin) == 0 &&
            base.far_reference_distance == o.base.far_reference_distance &&
            std::memcmp(&base.numerics, &o.base.numerics, sizeof base.numerics) == 0 && observers == o.observers &&
-           offsets == o.offsets && faceIds == o.faceIds && velocities == o.velocities;
+           offsets == o.offsets && faceIds == o.faceIds && velocities == o.velocities && raster == o.raster;
 }
 
 Server::Server(const hs_serve_options &options) : options_(options) {
@@ -111,9 +113,13 @@ uint64_t Server::submit(MeshInput mesh, const hs_request &request) {
     auto job = std::make_shared<Job>(Job{0, meshKey(mesh), std::make_shared<const MeshInput>(std::move(mesh)),
                                          RequestCopy(request)});
     const double limit = options_.planning_frequency;
-    for (double f : job->request.frequencies)
+    const auto &raster = job->request.raster;
+    for (double f : job->request.frequencies) {
         if (!std::isfinite(f) || f <= 0 || (limit > 0 && f > limit))
             throw InvalidArgument("Served frequencies must be finite, positive and at most the planning frequency.");
+        if (!raster.empty() && std::find(raster.begin(), raster.end(), f) == raster.end())
+            throw InvalidArgument("Solved frequency is invalid or absent from its interaction planning raster.");
+    }
     std::lock_guard<std::mutex> lock(mutex_);
     if (stop_)
         throw Cancelled();
@@ -154,7 +160,7 @@ std::vector<std::shared_ptr<Server::Job>> Server::takeGroup(size_t &footprint) {
             continue;  // another worker is on this mesh; later requests on other meshes may go
         std::vector<std::shared_ptr<Job>> group{head};
         std::set<double> freqs(head->request.frequencies.begin(), head->request.frequencies.end());
-        if (options_.planning_frequency > 0)
+        if (options_.planning_frequency > 0 || !head->request.raster.empty())
             for (auto jt = std::next(it); jt != queue_.end(); ++jt)
                 if ((*jt)->meshKey == head->meshKey && (*jt)->request.compatible(head->request)) {
                     std::set<double> merged = freqs;
@@ -296,12 +302,15 @@ void Server::worker(int index) {
             for (auto &job : group)
                 unique.insert(job->request.frequencies.begin(), job->request.frequencies.end());
             freqs.assign(unique.begin(), unique.end());
+            // planning raster: the request's own (a client sweeping one mesh keeps its
+            // plan), else the server's planning frequency, else the solved frequencies
             std::vector<double> raster;
-            if (options_.planning_frequency > 0) {
-                raster = freqs;
-                if (!unique.count(options_.planning_frequency))
-                    raster.push_back(options_.planning_frequency);
-                std::sort(raster.begin(), raster.end());
+            if (!head.request.raster.empty() || options_.planning_frequency > 0) {
+                std::set<double> r(unique);
+                r.insert(head.request.raster.begin(), head.request.raster.end());
+                if (options_.planning_frequency > 0)
+                    r.insert(options_.planning_frequency);
+                raster.assign(r.begin(), r.end());
             }
             const size_t T = head.mesh->faces.size(), N = head.mesh->vertices.size();
             const size_t resident = solveFootprint(T, N, 0, 0, 0, false, 0);

@@ -30,12 +30,12 @@ namespace hsb {
 // Owned copy of an hs_request (the caller's arrays may go away after submit).
 struct RequestCopy {
     hs_request base{};
-    std::vector<double> frequencies, observers, velocities;
+    std::vector<double> frequencies, raster, observers, velocities;
     std::vector<size_t> offsets;
     std::vector<uint32_t> faceIds;
     explicit RequestCopy(const hs_request &r);
-    hs_request view(const std::vector<double> &freqs, const std::vector<double> &raster) const;
-    bool compatible(const RequestCopy &o) const;  // everything but the frequencies equal
+    hs_request view(const std::vector<double> &freqs, const std::vector<double> &planRaster) const;
+    bool compatible(const RequestCopy &o) const;  // everything but the frequencies equal (planning raster too)
 };
 
 class Server {
