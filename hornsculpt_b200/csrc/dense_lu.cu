@@ -11,6 +11,8 @@
 #include "device_types.cuh"
 #include "kernel_timer.hpp"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <stdexcept>
 #include <string>
@@ -276,6 +278,211 @@ __global__ void __launch_bounds__(1024) panelSmemKernel(R *LU, uint32_t N, uint3
     for (uint32_t q = 0; q < jb; ++q)
         for (uint32_t i = threadIdx.x; i < rows; i += blockDim.x)
             st2(M + 2 * (size_t(k0 + q) * N + k0 + i), P[size_t(q) * rows + arrangement[i]]);
+}
+
+// Panel factorisation for tall panels, spread over a thread-block cluster:
+// CTA r of the cluster holds panel rows [r * rowsPerBlock, ...) in shared
+// memory. Pivot choice, tie rule and interchange sequence are those of
+// panelSmemKernel. Per column: each warp's best candidate goes to its CTA's
+// shared memory (double-buffered by column parity); one cluster barrier;
+// every warp reduces the candidates of all CTAs through distributed shared
+// memory; one warp per CTA copies the pivot row from the CTA that holds it;
+// each CTA eliminates its own rows. Rows that are pivots never change again,
+// so reading them remotely needs no further barrier; a final cluster barrier
+// keeps every CTA's shared memory alive until all remote reads are done.
+template <class R> constexpr uint32_t kClusterRows = sizeof(R) == 8 ? 384 : 768;
+constexpr uint32_t kMaxCluster = 16;
+
+template <class R> struct ClusterPanelShared {
+    R best[2][32];
+    int idx[2][32];
+    C2<R> pivot[kPanel];
+    int sel[kPanel];
+    int mapRow[2 * kPanel], mapPos[2 * kPanel];
+    int mapCount;
+};
+
+template <class R>
+__global__ void __launch_bounds__(1024) panelClusterKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb,
+                                                           uint32_t rowsPerBlock, int *pivots, int *info) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) unsigned char rawSmem[];
+    __shared__ ClusterPanelShared<R> sh;
+    C2<R> *P = reinterpret_cast<C2<R> *>(rawSmem);  // [jb][rowsPerBlock]
+    const uint32_t rank = cluster.block_rank(), C = cluster.num_blocks();
+    const uint32_t rows = N - k0, rowBegin = rank * rowsPerBlock;
+    const uint32_t myRows = rowBegin < rows ? min(rowsPerBlock, rows - rowBegin) : 0u;
+    R *M = LU + size_t(blockIdx.y) * N * N * 2;
+    int *piv = pivots + size_t(blockIdx.y) * N;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = int(blockDim.x >> 5);
+    const uint32_t i = threadIdx.x;  // one row per thread: blockDim.x >= rowsPerBlock
+    const bool own = i < myRows;
+    const uint32_t g = rowBegin + i;  // panel row of this thread
+    constexpr int kLoad = sizeof(R) == 8 ? 4 : 8;
+    if (own)
+        for (uint32_t q0 = 0; q0 < jb; q0 += kLoad) {
+            C2<R> v[kLoad];
+#pragma unroll
+            for (int t = 0; t < kLoad; ++t)
+                if (q0 + t < jb)
+                    v[t] = ld2(M + 2 * (size_t(k0 + q0 + t) * N + k0 + g));
+#pragma unroll
+            for (int t = 0; t < kLoad; ++t)
+                if (q0 + t < jb)
+                    P[size_t(q0 + t) * rowsPerBlock + i] = v[t];
+        }
+    bool taken = !own;
+    const auto magnitude = [](C2<R> z) {
+        const R a = fabs(z.x) + fabs(z.y);
+        return a >= R(0) ? a : R(0);  // a NaN row competes as zero, so a pivot row always exists
+    };
+    R best = own ? magnitude(P[i]) : R(-1);
+    int bestRow = own ? int(g) : int(rows);
+    for (uint32_t j = 0; j < jb; ++j) {
+        const int buf = j & 1;
+        for (int off = 16; off > 0; off >>= 1) {
+            const R ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bestRow, off);
+            if (ob > best || (ob == best && oi < bestRow)) {
+                best = ob;
+                bestRow = oi;
+            }
+        }
+        if (lane == 0) {
+            sh.best[buf][warp] = best;
+            sh.idx[buf][warp] = bestRow;
+        }
+        cluster.sync();
+        // all candidates of the cluster, read through distributed shared memory
+        R pb = R(-1);
+        int p = int(rows);
+        for (uint32_t e = lane; e < C * uint32_t(W); e += 32) {
+            const ClusterPanelShared<R> *other = cluster.map_shared_rank(&sh, int(e / W));
+            const R b = other->best[buf][e % W];
+            const int r = other->idx[buf][e % W];
+            if (b > pb || (b == pb && r < p)) {
+                pb = b;
+                p = r;
+            }
+        }
+        for (int off = 16; off > 0; off >>= 1) {
+            const R ob = __shfl_xor_sync(0xffffffffu, pb, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, p, off);
+            if (ob > pb || (ob == pb && oi < p)) {
+                pb = ob;
+                p = oi;
+            }
+        }
+        if (warp == 0) {
+            // copy the pivot row (columns j.. of panel row p) from its CTA
+            const C2<R> *src = cluster.map_shared_rank(P, int(uint32_t(p) / rowsPerBlock));
+            const uint32_t local = uint32_t(p) % rowsPerBlock;
+            if (uint32_t(lane) >= j && uint32_t(lane) < jb)
+                sh.pivot[lane] = src[size_t(lane) * rowsPerBlock + local];
+            if (rank == 0 && lane == 0) {
+                sh.sel[j] = p;
+                if (!(pb > 0) && *info == 0)
+                    atomicCAS(info, 0, int(k0 + j) + 1);
+            }
+        }
+        __syncthreads();
+        const C2<R> d = sh.pivot[j];
+        const R den = d.x * d.x + d.y * d.y;
+        const R rden = den > 0 ? R(1) / den : R(0);
+        const C2<R> inv = mk<R>(d.x * rden, -d.y * rden);
+        if (own && int(g) == p)
+            taken = true;
+        best = -1;
+        bestRow = int(rows);
+        if (!taken) {
+            const C2<R> l = cmul<R>(P[size_t(j) * rowsPerBlock + i], inv);
+            P[size_t(j) * rowsPerBlock + i] = l;
+            C2<R> next = mk<R>(0, 0);
+            for (uint32_t q0 = j + 1; q0 < jb; q0 += kLoad) {
+                C2<R> v[kLoad];
+#pragma unroll
+                for (int t = 0; t < kLoad; ++t)
+                    if (q0 + t < jb)
+                        v[t] = P[size_t(q0 + t) * rowsPerBlock + i];
+#pragma unroll
+                for (int t = 0; t < kLoad; ++t)
+                    if (q0 + t < jb) {
+                        csub<R>(v[t], l, sh.pivot[q0 + t]);
+                        P[size_t(q0 + t) * rowsPerBlock + i] = v[t];
+                    }
+                if (q0 == j + 1)
+                    next = v[0];
+            }
+            if (j + 1 < jb) {
+                best = magnitude(next);
+                bestRow = int(g);
+            }
+        }
+    }
+    cluster.sync();
+    // interchange sequence (rank 0) and the final position of every row that moved
+    if (rank == 0 && threadIdx.x == 0) {
+        int arrRow[2 * kPanel], arrPos[2 * kPanel], whereRow[2 * kPanel], wherePos[2 * kPanel];
+        int na = 0, nw = 0;
+        const auto arrangementAt = [&](int pos) {
+            for (int q = 0; q < na; ++q)
+                if (arrPos[q] == pos)
+                    return arrRow[q];
+            return pos;
+        };
+        const auto whereOf = [&](int row) {
+            for (int q = 0; q < nw; ++q)
+                if (whereRow[q] == row)
+                    return wherePos[q];
+            return row;
+        };
+        const auto setArrangement = [&](int pos, int row) {
+            for (int q = 0; q < na; ++q)
+                if (arrPos[q] == pos) {
+                    arrRow[q] = row;
+                    return;
+                }
+            arrPos[na] = pos;
+            arrRow[na++] = row;
+        };
+        const auto setWhere = [&](int row, int pos) {
+            for (int q = 0; q < nw; ++q)
+                if (whereRow[q] == row) {
+                    wherePos[q] = pos;
+                    return;
+                }
+            whereRow[nw] = row;
+            wherePos[nw++] = pos;
+        };
+        for (uint32_t j = 0; j < jb; ++j) {
+            const int r = sh.sel[j], pj = whereOf(r), rj = arrangementAt(int(j));
+            piv[k0 + j] = int(k0) + pj;
+            setArrangement(int(j), r);
+            setArrangement(pj, rj);
+            setWhere(r, int(j));
+            setWhere(rj, pj);
+        }
+        int n = 0;
+        for (int q = 0; q < nw; ++q)
+            if (whereRow[q] != wherePos[q]) {
+                sh.mapRow[n] = whereRow[q];
+                sh.mapPos[n++] = wherePos[q];
+            }
+        sh.mapCount = n;
+    }
+    cluster.sync();
+    const ClusterPanelShared<R> *root = cluster.map_shared_rank(&sh, 0);
+    if (own) {
+        uint32_t pos = g;
+        const int n = root->mapCount;
+        for (int q = 0; q < n; ++q)
+            if (root->mapRow[q] == int(g))
+                pos = uint32_t(root->mapPos[q]);
+        for (uint32_t q = 0; q < jb; ++q)
+            st2(M + 2 * (size_t(k0 + q) * N + k0 + pos), P[size_t(q) * rowsPerBlock + i]);
+    }
+    cluster.sync();  // keep rank 0's map alive until every CTA has read it
 }
 
 template <class R> size_t panelSmemBytes(uint32_t rows, uint32_t jb) {
@@ -582,6 +789,47 @@ __global__ void toFloatKernel(const double *in, float *out, size_t count) {
         out[i] = float(in[i]);
 }
 
+// Largest cluster the panel kernel may use on this device: 16 CTAs (opt-in)
+// when the device can schedule such a cluster with full panel shared memory,
+// else the portable 8, else none.
+template <class R> uint32_t clusterLimit() {
+    static int limit = -1;
+    if (limit >= 0)
+        return uint32_t(limit);
+    const size_t smem = size_t(kPanel) * kClusterRows<R> * sizeof(C2<R>);
+    limit = 0;
+    if (cudaFuncSetAttribute(panelClusterKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    for (uint32_t c : {kMaxCluster, 8u}) {
+        if (c > 8 &&
+            cudaFuncSetAttribute(panelClusterKernel<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(c, 1);
+        cfg.blockDim = dim3(kClusterRows<R>);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = c;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&clusters, panelClusterKernel<R>, &cfg) == cudaSuccess && clusters > 0) {
+            limit = int(c);
+            break;
+        }
+        cudaGetLastError();
+    }
+    return uint32_t(limit);
+}
+
 template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                                KernelTimer *timer) {
     check(cudaMemsetAsync(info, 0, sizeof(int), stream), "LU info reset");
@@ -600,7 +848,25 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
         {
             TimedScope s(timer, "lu_panel", stream);
             const size_t bytes = panelSmemBytes<R>(N - k0, jb);
-            if (bytes <= kPanelSmemLimit)
+            const uint32_t rows = N - k0;
+            if (bytes > kPanelSmemLimit && rows <= kClusterRows<R> * clusterLimit<R>()) {
+                const uint32_t C = (rows + kClusterRows<R> - 1) / kClusterRows<R>;
+                const uint32_t perBlock = (rows + C - 1) / C;
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3(C, B);
+                cfg.blockDim = dim3((perBlock + 31) / 32 * 32);
+                cfg.dynamicSmemBytes = size_t(jb) * perBlock * sizeof(C2<R>);
+                cfg.stream = stream;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = C;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                check(cudaLaunchKernelEx(&cfg, panelClusterKernel<R>, LU, N, k0, jb, perBlock, pivots, info),
+                      "cluster panel launch");
+            } else if (bytes <= kPanelSmemLimit)
                 panelSmemKernel<R><<<B, std::min(1024u, (N - k0 + 31) / 32 * 32), bytes, stream>>>(LU, N, k0, jb,
                                                                                                    pivots, info);
             else

@@ -85,3 +85,20 @@ def test_mixed_rejects_bad_gmres_settings():
         with pytest.raises(ValueError, match="GMRES settings"):
             solver.solve(hs.BemRequest(frequencies=[500.0], excitations=[hs.BemExcitation("u", [hs.FaceVelocity(1, 1.0)])],
                                        numerics=numerics))
+
+
+def test_tall_panels_on_a_cluster():
+    """N = 1026 puts the first LU panels above one CTA's shared memory in both
+    forms (FP64 beyond 430 rows, FP32 beyond 860): they are factored by a
+    thread-block cluster. Both forms converge (the plain form within its
+    reference refinement budget) and agree within the mixed tolerance."""
+    mesh = meshes.octahedral_sphere(4)
+    freqs = [400.0, 1300.0]
+    exc = [hs.BemExcitation("unit", [hs.FaceVelocity(1, 1.0)])]
+    with hs.CudaBemSolver(mesh) as solver:
+        plain = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc))
+        mixed = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc, numerics=MIXED))
+    for fp, fm in zip(plain.frequencies, mixed.frequencies):
+        p, m = fp.excitations[0], fm.excitations[0]
+        assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
+        assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
