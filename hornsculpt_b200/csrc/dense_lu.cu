@@ -604,6 +604,163 @@ template <class R> __global__ void __launch_bounds__(256) gemmKernel(R *LU, uint
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 trailing update on the tensor cores (tcgen05): A22 -= L21 * U12 as one
+// real GEMM of the split complex operands,
+//   [C_re; C_im] = [[L_re, -L_im]; [L_im, L_re]] * [U_re; U_im],
+// M' = 128 (64 complex rows, real parts over imaginary parts), K' = 64 (the 32
+// complex panel columns), N = 128 complex columns per CTA. Operands are split
+// into TF32 hi + lo parts and multiplied as hi*hi + hi*lo + lo*hi (3xTF32) with
+// FP32 accumulation in tensor memory, which keeps FP32 accuracy. Shared-memory
+// tiles use the K-major, unswizzled canonical layout: 8-row x 16-byte core
+// matrices, row groups 128 B apart (SBO), 16-byte K chunks (M'/8)*128 B apart
+// (LBO). One thread issues the MMAs and commits them to an mbarrier; the wait is
+// bounded (a timeout leaves kTensorTimeout in the LU status word and skips the
+// update). The product is read from tensor memory (32x32b per warp), staged in
+// shared memory and subtracted from A22 with coalesced accesses.
+// ---------------------------------------------------------------------------
+constexpr int kTileRows = 64, kTileCols = 64, kTileK = 2 * kPanel;  // complex rows, complex cols, real K
+constexpr int kTensorThreads = 256;
+constexpr int kTensorTimeout = -1;
+
+__device__ __forceinline__ uint32_t smemAddr(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ float tf32Round(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// offset (floats) of element (row r, k) in a K-major core-matrix tile of `rows` rows
+__device__ __forceinline__ int coreOffset(int r, int k, int rows) {
+    return ((k >> 2) * (rows >> 3) + (r >> 3)) * 32 + (r & 7) * 4 + (k & 3);
+}
+
+// UMMA shared-memory matrix descriptor: start, LBO, SBO (16-byte units), version 1, no swizzle
+__device__ __forceinline__ uint64_t matrixDescriptor(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr >> 4) & 0x3FFF) | (uint64_t((lbo >> 4) & 0x3FFF) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
+}
+
+__global__ void __launch_bounds__(kTensorThreads) gemmTensorKernel(float *LU, uint32_t N, uint32_t k0, uint32_t jb,
+                                                                   int *info) {
+    constexpr int MA = 2 * kTileRows, NB = kTileCols;  // A' rows (real over imaginary), B' rows (columns)
+    extern __shared__ __align__(1024) float tile[];     // aHi, aLo [MA x 64], bHi, bLo [NB x 64]
+    float *aHi = tile, *aLo = tile + MA * kTileK, *bHi = tile + 2 * MA * kTileK, *bLo = bHi + NB * kTileK;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmemBase;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    float *M = LU + size_t(blockIdx.z) * N * N * 2;
+    const uint32_t r0 = k0 + jb + blockIdx.x * kTileRows, c0 = k0 + jb + blockIdx.y * kTileCols;
+    // A' from L21. A warp fills whole core matrices: lane = (row & 7) * 4 + (k & 3), so the
+    // 32 stores of a warp cover 128 contiguous bytes; the loads read 8 consecutive rows
+    // of 4 panel columns.
+    for (int cm = warp; cm < (kTileRows / 8) * (kPanel / 4); cm += kTensorThreads / 32) {
+        const int i = (cm % (kTileRows / 8)) * 8 + (lane >> 2), k = (cm / (kTileRows / 8)) * 4 + (lane & 3);
+        float2 v = make_float2(0.f, 0.f);
+        if (r0 + i < N && uint32_t(k) < jb)
+            v = *reinterpret_cast<const float2 *>(M + 2 * (size_t(k0 + k) * N + r0 + i));
+        const float parts[4] = {v.x, -v.y, v.y, v.x};  // (i, k), (i, k+32), (i+64, k), (i+64, k+32)
+        const int rows[4] = {i, i, i + kTileRows, i + kTileRows}, ks[4] = {k, k + kPanel, k, k + kPanel};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float h = tf32Round(parts[q]);
+            aHi[coreOffset(rows[q], ks[q], MA)] = h;
+            aLo[coreOffset(rows[q], ks[q], MA)] = tf32Round(parts[q] - h);
+        }
+    }
+    // B' from U12, the same way (row = tile column j, k = panel row)
+    for (int cm = warp; cm < (kTileCols / 8) * (kPanel / 4); cm += kTensorThreads / 32) {
+        const int j = (cm % (kTileCols / 8)) * 8 + (lane >> 2), k = (cm / (kTileCols / 8)) * 4 + (lane & 3);
+        float2 v = make_float2(0.f, 0.f);
+        if (c0 + j < N && uint32_t(k) < jb)
+            v = *reinterpret_cast<const float2 *>(M + 2 * (size_t(c0 + j) * N + k0 + k));
+        const float hr = tf32Round(v.x), hi = tf32Round(v.y);
+        bHi[coreOffset(j, k, NB)] = hr;
+        bLo[coreOffset(j, k, NB)] = tf32Round(v.x - hr);
+        bHi[coreOffset(j, k + kPanel, NB)] = hi;
+        bLo[coreOffset(j, k + kPanel, NB)] = tf32Round(v.y - hi);
+    }
+    if (tid == 0)
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&mbar)));
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(&tmemBase)),
+                     "r"(NB));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        asm volatile("tcgen05.fence::before_thread_sync;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;");  // tiles written by threads, read by the tensor cores
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmemBase;
+    if (tid == 0) {
+        // D: F32; A, B: TF32, K-major; N = NB (>> 3), M = MA (>> 4)
+        const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(NB >> 3) << 17) | (uint32_t(MA >> 4) << 24);
+        const float *As[3] = {aHi, aHi, aLo}, *Bs[3] = {bHi, bLo, bHi};
+        constexpr uint32_t lboA = (MA / 8) * 128, lboB = (NB / 8) * 128, sbo = 128;
+        for (int pass = 0; pass < 3; ++pass)
+            for (int s = 0; s < kTileK / 8; ++s) {
+                const uint64_t da = matrixDescriptor(smemAddr(As[pass]) + uint32_t(2 * s) * lboA, lboA, sbo);
+                const uint64_t db = matrixDescriptor(smemAddr(Bs[pass]) + uint32_t(2 * s) * lboB, lboB, sbo);
+                const uint32_t accumulate = (pass | s) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+            }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+            smemAddr(&mbar)));
+    }
+    uint32_t done = 0;
+    for (long it = 0; it < 20000000 && !done; ++it)
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smemAddr(&mbar)), "r"(0));
+    if (!done && tid == 0)
+        atomicCAS(info, 0, kTensorTimeout);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    constexpr int kStride = NB + 1;
+    float *staged = tile;  // [MA][NB + 1]: product rows (real parts then imaginary parts) x columns
+    if (done) {
+        // warp w reads lanes 32 (w % 4) .. + 31 and columns 32 (w / 4) .. + 31
+        const int quarter = warp & 3, c = (warp >> 2) * 32;
+        uint32_t v[32];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+            : "r"(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(c)));
+        asm volatile("tcgen05.wait::ld.sync.aligned;");
+        const int row = quarter * 32 + lane;
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            staged[row * kStride + c + j] = __uint_as_float(v[j]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NB));
+    if (!done)
+        return;
+    for (int e = tid; e < kTileRows * kTileCols; e += kTensorThreads) {
+        const int i = e % kTileRows, j = e / kTileRows;
+        if (r0 + i >= N || c0 + j >= N)
+            continue;
+        float2 *dst = reinterpret_cast<float2 *>(M + 2 * (size_t(c0 + j) * N + r0 + i));
+        float2 v = *dst;
+        v.x -= staged[i * kStride + j];
+        v.y -= staged[(i + kTileRows) * kStride + j];
+        *dst = v;
+    }
+}
+
+constexpr size_t kTensorTileBytes = size_t(2) * (2 * kTileRows + kTileCols) * kTileK * sizeof(float);  // 96 KB
+
 // Forward / back substitution of one right-hand side per CTA, with the
 // vector staged in shared memory. Blocks of 32 unknowns: warp 0 loads the
 // 32x32 diagonal block into registers (independent coalesced loads, lane =
@@ -841,6 +998,10 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
         check(cudaFuncSetAttribute(panelSmemKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(kPanelSmemLimit)),
               "panel smem attribute");
+        if constexpr (sizeof(R) == 4)
+            check(cudaFuncSetAttribute(gemmTensorKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(kTensorTileBytes)),
+                  "tensor gemm smem attribute");
         attr = true;
     }
     for (uint32_t k0 = 0; k0 < N; k0 += kPanel) {

@@ -551,6 +551,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         int info = 0;
         cuda(cudaMemcpyAsync(&info, dInfo_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, s), "LU info");
         cuda(cudaStreamSynchronize(s), "CUDA pivoted LU");
+        if (info < 0)
+            throw NumericError("CUDA Burton-Miller factorization: a tensor-core trailing update did not complete.");
         if (info)
             throw NumericError("CUDA Burton-Miller factorization failed at pivot " + std::to_string(info));
         const double factorMs = msSince(factorStart);
