@@ -507,16 +507,18 @@ template <class R> __global__ void swapKernel(R *LU, uint32_t N, uint32_t k0, ui
     }
 }
 
-// U12 = L11^{-1} A12 (unit lower L11 of the panel) for 32 columns per CTA:
-// L11 and the 32x32 tile of A12 are staged in shared memory with coalesced
-// column reads; a warp solves one column at a time (lane = row, L11 row in
-// registers, the solved unknown broadcast by shuffle).
-template <class R> __global__ void __launch_bounds__(256) trsmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb) {
+// U12 = L11^{-1} A12 (unit lower L11 of the panel) for columns
+// [k0 + jb, cEnd), 32 per CTA: L11 and the 32x32 tile of A12 are staged in
+// shared memory with coalesced column reads; a warp solves one column at a
+// time (lane = row, L11 row in registers, the solved unknown broadcast by
+// shuffle).
+template <class R>
+__global__ void __launch_bounds__(256) trsmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb, uint32_t cEnd) {
     __shared__ C2<R> L[kPanel][kPanel + 1];
     __shared__ C2<R> X[kPanel][kPanel + 1];  // [column][row]
     R *M = LU + size_t(blockIdx.y) * N * N * 2;
     const uint32_t c0 = k0 + jb + blockIdx.x * kPanel;
-    const uint32_t cols = min(uint32_t(kPanel), N - c0);
+    const uint32_t cols = min(uint32_t(kPanel), cEnd - c0);
     for (uint32_t e = threadIdx.x; e < jb * jb; e += blockDim.x) {
         const uint32_t r = e % jb, c = e / jb;
         L[r][c] = ld2(M + 2 * (size_t(k0 + c) * N + k0 + r));
@@ -549,8 +551,10 @@ template <class R> __global__ void __launch_bounds__(256) trsmKernel(R *LU, uint
     }
 }
 
-// A22 -= L21 * U12 with 64x64 output tiles, K = jb <= 32.
-template <class R> __global__ void __launch_bounds__(256) gemmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb) {
+// A22 -= L21 * U12 with 64x64 output tiles, K = jb <= 32, over rows
+// [k0 + jb, N) and columns [k0 + jb, cEnd).
+template <class R>
+__global__ void __launch_bounds__(256) gemmKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb, uint32_t cEnd) {
     extern __shared__ __align__(16) unsigned char rawSmem[];
     C2<R> *sA = reinterpret_cast<C2<R> *>(rawSmem);  // [kPanel][64]  L21 tile, k-major
     C2<R> *sB = sA + kPanel * 64;                      // [kPanel][64]  U12 tile, k-major
@@ -560,7 +564,7 @@ template <class R> __global__ void __launch_bounds__(256) gemmKernel(R *LU, uint
         const uint32_t kk = e / 64, x = e % 64;
         const uint32_t r = r0 + x, c = c0 + x;
         sA[kk * 64 + x] = r < N ? ld2(M + 2 * (size_t(k0 + kk) * N + r)) : mk<R>(0, 0);
-        sB[kk * 64 + x] = c < N ? ld2(M + 2 * (size_t(c) * N + k0 + kk)) : mk<R>(0, 0);
+        sB[kk * 64 + x] = c < cEnd ? ld2(M + 2 * (size_t(c) * N + k0 + kk)) : mk<R>(0, 0);
     }
     __syncthreads();
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -585,43 +589,75 @@ template <class R> __global__ void __launch_bounds__(256) gemmKernel(R *LU, uint
                 acc[i][j].y += a[i].x * b[j].y + a[i].y * b[j].x;
             }
     }
+    // the 16 outputs are read first (independent loads in flight), then written
+    C2<R> old[4][4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const uint32_t c = c0 + ty + 16 * j;
-        if (c >= N)
-            continue;
+    for (int j = 0; j < 4; ++j)
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-            const uint32_t r = r0 + tx + 16 * i;
-            if (r >= N)
-                continue;
-            R *e = M + 2 * (size_t(c) * N + r);
-            C2<R> v = ld2(e);
-            v.x -= acc[i][j].x;
-            v.y -= acc[i][j].y;
-            st2(e, v);
+            const uint32_t r = r0 + tx + 16 * i, c = c0 + ty + 16 * j;
+            old[i][j] = (r < N && c < cEnd) ? ld2(M + 2 * (size_t(c) * N + r)) : mk<R>(0, 0);
         }
-    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const uint32_t r = r0 + tx + 16 * i, c = c0 + ty + 16 * j;
+            if (r < N && c < cEnd)
+                st2(M + 2 * (size_t(c) * N + r), mk<R>(old[i][j].x - acc[i][j].x, old[i][j].y - acc[i][j].y));
+        }
 }
 
 // ---------------------------------------------------------------------------
-// FP32 trailing update on the tensor cores (tcgen05): A22 -= L21 * U12 as one
-// real GEMM of the split complex operands,
-//   [C_re; C_im] = [[L_re, -L_im]; [L_im, L_re]] * [U_re; U_im],
-// M' = 128 (64 complex rows, real parts over imaginary parts), K' = 64 (the 32
-// complex panel columns), N = 128 complex columns per CTA. Operands are split
-// into TF32 hi + lo parts and multiplied as hi*hi + hi*lo + lo*hi (3xTF32) with
-// FP32 accumulation in tensor memory, which keeps FP32 accuracy. Shared-memory
-// tiles use the K-major, unswizzled canonical layout: 8-row x 16-byte core
-// matrices, row groups 128 B apart (SBO), 16-byte K chunks (M'/8)*128 B apart
-// (LBO). One thread issues the MMAs and commits them to an mbarrier; the wait is
-// bounded (a timeout leaves kTensorTimeout in the LU status word and skips the
-// update). The product is read from tensor memory (32x32b per warp), staged in
-// shared memory and subtracted from A22 with coalesced accesses.
+// FP32 trailing update of the two-level factorisation on the tensor cores
+// (tcgen05): A22 -= L21 * U12 with K = kOuter = 128 complex columns, as a real
+// GEMM of the split complex operands, output real parts and imaginary parts
+// side by side:
+//   [C_re, C_im] = [L_re, L_im] * [[U_re, U_im]; [-U_im, U_re]].
+// Operands are multiplied as hi*hi + hi*lo + lo*hi (3xTF32: TF32 hi part plus
+// TF32 remainder) with FP32 accumulation, which keeps FP32 accuracy.
+//
+// packKernel converts L21 and U12 once per outer block into operand tiles
+// that are already in the tensor cores' shared-memory layout (K-major,
+// unswizzled canonical layout: 8-row x 16-byte core matrices, row groups 128 B
+// apart (SBO), 16-byte K chunks (rows/8)*128 B apart (LBO)), hi then lo, one
+// tile per 128 rows (A) or 64 complex columns (B, 128 operand rows) and per
+// stage of 16 complex K columns. trailingTensorKernel then owns 128 complex
+// rows x 64 complex columns of A22 (an M = 128, N = 128 real accumulator in
+// tensor memory) and runs three roles:
+//   * warp 0 copies the stage tiles into a ring of kTcStages shared-memory
+//     buffers with bulk asynchronous copies that complete on the buffer's
+//     `full` mbarrier;
+//   * warp 1 issues the stage's MMAs from one thread and commits them to the
+//     buffer's `empty` mbarrier, which lets warp 0 refill it; after the last
+//     stage it commits to `done`;
+//   * every thread loads its 32 outputs of A22 at the start (the loads overlap
+//     the main loop), waits for `done`, reads its accumulator row (32 lanes x
+//     32 columns, real and imaginary parts) from tensor memory and writes the
+//     updated outputs (a warp writes 32 consecutive rows of a column).
+// Every wait is bounded by a clock budget; a timeout leaves kTensorTimeout in
+// the LU status word and skips the update.
 // ---------------------------------------------------------------------------
-constexpr int kTileRows = 64, kTileCols = 64, kTileK = 2 * kPanel;  // complex rows, complex cols, real K
-constexpr int kTensorThreads = 256;
+constexpr int kOuter = 128;                            // outer block width of the two-level factorisation
+constexpr int kTcRows = 128, kTcCols = 64, kTcK = 16;  // complex rows, complex columns, complex K per stage
+constexpr int kTcStages = 3, kTcThreads = 256;
+constexpr int kTcSteps = kOuter / kTcK;                // stages per update
+constexpr int kTcTile = 2 * kTcRows * (2 * kTcK);      // floats of one operand tile, hi + lo (A and B alike)
+constexpr size_t kTcSmem = size_t(kTcStages) * 2 * kTcTile * sizeof(float);  // 192 KB: one CTA per SM
 constexpr int kTensorTimeout = -1;
+constexpr long long kWaitCycles = 4000000000ll;  // about two seconds
+
+static_assert(2 * kTcCols == kTcRows, "A and B operand tiles have the same shape");
+static_assert(kOuter % kTcK == 0 && kOuter % kPanel == 0, "outer block must hold whole stages and panels");
+static_assert(kTcSmem > 114 * 1024 && kTcSmem <= 227 * 1024, "one CTA per SM keeps tensor-memory allocation uncontended");
+
+// floats of the packed operand tiles of one matrix (the first outer block has the most)
+size_t packFloats(uint32_t N) {
+    if (N <= uint32_t(kOuter))
+        return 0;
+    const size_t rest = N - kOuter;
+    return ((rest + kTcRows - 1) / kTcRows + (rest + kTcCols - 1) / kTcCols) * kTcSteps * size_t(kTcTile);
+}
 
 __device__ __forceinline__ uint32_t smemAddr(const void *p) { return uint32_t(__cvta_generic_to_shared(p)); }
 
@@ -642,124 +678,262 @@ __device__ __forceinline__ uint64_t matrixDescriptor(uint32_t addr, uint32_t lbo
            (uint64_t((sbo >> 4) & 0x3FFF) << 32) | (uint64_t(1) << 46);
 }
 
-__global__ void __launch_bounds__(kTensorThreads) gemmTensorKernel(float *LU, uint32_t N, uint32_t k0, uint32_t jb,
-                                                                   int *info) {
-    constexpr int MA = 2 * kTileRows, NB = kTileCols;  // A' rows (real over imaginary), B' rows (columns)
-    extern __shared__ __align__(1024) float tile[];     // aHi, aLo [MA x 64], bHi, bLo [NB x 64]
-    float *aHi = tile, *aLo = tile + MA * kTileK, *bHi = tile + 2 * MA * kTileK, *bLo = bHi + NB * kTileK;
-    __shared__ __align__(8) uint64_t mbar;
-    __shared__ uint32_t tmemBase;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    float *M = LU + size_t(blockIdx.z) * N * N * 2;
-    const uint32_t r0 = k0 + jb + blockIdx.x * kTileRows, c0 = k0 + jb + blockIdx.y * kTileCols;
-    // A' from L21. A warp fills whole core matrices: lane = (row & 7) * 4 + (k & 3), so the
-    // 32 stores of a warp cover 128 contiguous bytes; the loads read 8 consecutive rows
-    // of 4 panel columns.
-    for (int cm = warp; cm < (kTileRows / 8) * (kPanel / 4); cm += kTensorThreads / 32) {
-        const int i = (cm % (kTileRows / 8)) * 8 + (lane >> 2), k = (cm / (kTileRows / 8)) * 4 + (lane & 3);
-        float2 v = make_float2(0.f, 0.f);
-        if (r0 + i < N && uint32_t(k) < jb)
-            v = *reinterpret_cast<const float2 *>(M + 2 * (size_t(k0 + k) * N + r0 + i));
-        const float parts[4] = {v.x, -v.y, v.y, v.x};  // (i, k), (i, k+32), (i+64, k), (i+64, k+32)
-        const int rows[4] = {i, i, i + kTileRows, i + kTileRows}, ks[4] = {k, k + kPanel, k, k + kPanel};
+// Bounded wait for the phase of `parity` on an mbarrier; false on timeout.
+__device__ __forceinline__ bool waitPhase(uint32_t bar, uint32_t parity) {
+    const long long start = clock64();
+    uint32_t done = 0;
+    while (!done) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity));
+        if (!done && clock64() - start > kWaitCycles)
+            return false;
+    }
+    return true;
+}
+
+// Operand tiles of one outer block: per matrix the A tiles of L21 [row tile][stage], then the B tiles
+// of U12 [column tile][stage]. Grid: (row tiles + column tiles, stages, matrices).
+__global__ void __launch_bounds__(256) packKernel(const float *LU, uint32_t N, uint32_t K0, float *pack,
+                                                  size_t packStride) {
+    const uint32_t begin = K0 + kOuter, rest = N - begin;
+    const uint32_t rowTiles = (rest + kTcRows - 1) / kTcRows, t = blockIdx.x, c = blockIdx.y;
+    const float *M = LU + size_t(blockIdx.z) * N * N * 2;
+    float *hi = pack + blockIdx.z * packStride + (size_t(t) * kTcSteps + c) * kTcTile, *lo = hi + kTcTile / 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t kc = K0 + c * kTcK;
+    // a warp fills whole core matrices: lane = (row & 7) * 4 + (k & 3), 32 stores to 128 contiguous bytes
+    if (t < rowTiles) {  // A: row i takes (L_re, L_im) at k and k + 16
+        const uint32_t r0 = begin + t * kTcRows;
+        float2 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int cm = warp + 8 * q, i = (cm % 16) * 8 + (lane >> 2), k = (cm / 16) * 4 + (lane & 3);
+            v[q] = r0 + i < N ? *reinterpret_cast<const float2 *>(M + 2 * (size_t(kc + k) * N + r0 + i))
+                              : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int cm = warp + 8 * q, i = (cm % 16) * 8 + (lane >> 2), k = (cm / 16) * 4 + (lane & 3);
+            const float hr = tf32Round(v[q].x), hm = tf32Round(v[q].y);
+            hi[coreOffset(i, k, kTcRows)] = hr;
+            lo[coreOffset(i, k, kTcRows)] = tf32Round(v[q].x - hr);
+            hi[coreOffset(i, k + kTcK, kTcRows)] = hm;
+            lo[coreOffset(i, k + kTcK, kTcRows)] = tf32Round(v[q].y - hm);
+        }
+    } else {  // B: operand row j takes (U_re, -U_im), row j + 64 takes (U_im, U_re)
+        const uint32_t c0 = begin + (t - rowTiles) * kTcCols;
+        float2 v[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const float h = tf32Round(parts[q]);
-            aHi[coreOffset(rows[q], ks[q], MA)] = h;
-            aLo[coreOffset(rows[q], ks[q], MA)] = tf32Round(parts[q] - h);
+            const int cm = warp + 8 * q, j = (cm % 8) * 8 + (lane >> 2), k = (cm / 8) * 4 + (lane & 3);
+            v[q] = c0 + j < N ? *reinterpret_cast<const float2 *>(M + 2 * (size_t(c0 + j) * N + kc + k))
+                              : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int cm = warp + 8 * q, j = (cm % 8) * 8 + (lane >> 2), k = (cm / 8) * 4 + (lane & 3);
+            const float parts[4] = {v[q].x, -v[q].y, v[q].y, v[q].x};  // (j, k), (j, k+16), (j+64, k), (j+64, k+16)
+            const int rows[4] = {j, j, j + kTcCols, j + kTcCols}, ks[4] = {k, k + kTcK, k, k + kTcK};
+#pragma unroll
+            for (int p = 0; p < 4; ++p) {
+                const float h = tf32Round(parts[p]);
+                hi[coreOffset(rows[p], ks[p], kTcRows)] = h;
+                lo[coreOffset(rows[p], ks[p], kTcRows)] = tf32Round(parts[p] - h);
+            }
         }
     }
-    // B' from U12, the same way (row = tile column j, k = panel row)
-    for (int cm = warp; cm < (kTileCols / 8) * (kPanel / 4); cm += kTensorThreads / 32) {
-        const int j = (cm % (kTileCols / 8)) * 8 + (lane >> 2), k = (cm / (kTileCols / 8)) * 4 + (lane & 3);
-        float2 v = make_float2(0.f, 0.f);
-        if (c0 + j < N && uint32_t(k) < jb)
-            v = *reinterpret_cast<const float2 *>(M + 2 * (size_t(c0 + j) * N + k0 + k));
-        const float hr = tf32Round(v.x), hi = tf32Round(v.y);
-        bHi[coreOffset(j, k, NB)] = hr;
-        bLo[coreOffset(j, k, NB)] = tf32Round(v.x - hr);
-        bHi[coreOffset(j, k + kPanel, NB)] = hi;
-        bLo[coreOffset(j, k + kPanel, NB)] = tf32Round(v.y - hi);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) trailingTensorKernel(float *LU, uint32_t N, uint32_t K0,
+                                                                      const float *pack, size_t packStride,
+                                                                      int *info) {
+    extern __shared__ __align__(1024) float ring[];  // kTcStages x {A hi, A lo, B hi, B lo}
+    __shared__ __align__(8) uint64_t full[kTcStages], empty[kTcStages], done;
+    __shared__ uint32_t tmemBase;
+    constexpr int NB = 2 * kTcCols;  // real accumulator columns
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint32_t begin = K0 + kOuter, rest = N - begin;
+    const uint32_t rowTiles = (rest + kTcRows - 1) / kTcRows;
+    const uint32_t r0 = begin + blockIdx.x * kTcRows, c0 = begin + blockIdx.y * kTcCols;
+    float *M = LU + size_t(blockIdx.z) * N * N * 2;
+    const float *tilesA = pack + blockIdx.z * packStride + size_t(blockIdx.x) * kTcSteps * kTcTile;
+    const float *tilesB = pack + blockIdx.z * packStride + (size_t(rowTiles) + blockIdx.y) * kTcSteps * kTcTile;
+    // this thread's outputs: row 32 (warp % 4) + lane, columns 32 (warp / 4) .. + 31
+    const int quarter = warp & 3, half = warp >> 2;
+    const uint32_t row = r0 + quarter * 32 + lane, col0 = c0 + half * 32;
+    float2 old[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+        old[j] = (row < N && col0 + j < N) ? *reinterpret_cast<const float2 *>(M + 2 * (size_t(col0 + j) * N + row))
+                                           : make_float2(0.f, 0.f);
+    if (tid == 0) {
+        for (int s = 0; s < kTcStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&empty[s])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&done)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
     }
-    if (tid == 0)
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smemAddr(&mbar)));
-    if (warp == 0) {
+    if (warp == 2) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smemAddr(&tmemBase)),
                      "r"(NB));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
         asm volatile("tcgen05.fence::before_thread_sync;");
     }
-    asm volatile("fence.proxy.async.shared::cta;");  // tiles written by threads, read by the tensor cores
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmemBase;
-    if (tid == 0) {
-        // D: F32; A, B: TF32, K-major; N = NB (>> 3), M = MA (>> 4)
-        const uint32_t idesc = (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(NB >> 3) << 17) | (uint32_t(MA >> 4) << 24);
-        const float *As[3] = {aHi, aHi, aLo}, *Bs[3] = {bHi, bLo, bHi};
-        constexpr uint32_t lboA = (MA / 8) * 128, lboB = (NB / 8) * 128, sbo = 128;
-        for (int pass = 0; pass < 3; ++pass)
-            for (int s = 0; s < kTileK / 8; ++s) {
-                const uint64_t da = matrixDescriptor(smemAddr(As[pass]) + uint32_t(2 * s) * lboA, lboA, sbo);
-                const uint64_t db = matrixDescriptor(smemAddr(Bs[pass]) + uint32_t(2 * s) * lboB, lboB, sbo);
-                const uint32_t accumulate = (pass | s) ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                    "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+    bool ok = true;
+    int issued = 0;
+    if (warp == 0) {  // producer
+        for (int c = 0; c < kTcSteps; ++c) {
+            const int s = c % kTcStages;
+            if (c >= kTcStages) {  // the MMAs of stage c - kTcStages have read this buffer
+                ok = __all_sync(0xffffffffu, waitPhase(smemAddr(&empty[s]), uint32_t((c - kTcStages) / kTcStages) & 1u));
+                if (!ok)
+                    break;
             }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            smemAddr(&mbar)));
+            if (lane == 0) {
+                const uint32_t dst = smemAddr(ring + size_t(s) * 2 * kTcTile), bar = smemAddr(&full[s]);
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                             "r"(uint32_t(2 * kTcTile * sizeof(float))));
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                    "l"(tilesA + size_t(c) * kTcTile), "r"(uint32_t(kTcTile * sizeof(float))), "r"(bar)
+                    : "memory");
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        dst + uint32_t(kTcTile * sizeof(float))),
+                    "l"(tilesB + size_t(c) * kTcTile), "r"(uint32_t(kTcTile * sizeof(float))), "r"(bar)
+                    : "memory");
+            }
+            issued = c + 1;
+        }
+    } else if (warp == 1) {  // MMA issue
+        // D: F32; A, B: TF32, K-major; N = NB (>> 3), M = 128 (>> 4)
+        constexpr uint32_t idesc =
+            (1u << 4) | (2u << 7) | (2u << 10) | (uint32_t(NB >> 3) << 17) | (uint32_t(kTcRows >> 4) << 24);
+        constexpr uint32_t lbo = (kTcRows / 8) * 128, sbo = 128;
+        for (int c = 0; c < kTcSteps; ++c) {
+            const int s = c % kTcStages;
+            ok = __all_sync(0xffffffffu, waitPhase(smemAddr(&full[s]), uint32_t(c / kTcStages) & 1u));
+            if (!ok)
+                break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            if (lane == 0) {
+                const uint32_t aHi = smemAddr(ring + size_t(s) * 2 * kTcTile), aLo = aHi + kTcTile * 2;
+                const uint32_t bHi = aHi + kTcTile * 4, bLo = bHi + kTcTile * 2;
+                const uint32_t As[3] = {aHi, aHi, aLo}, Bs[3] = {bHi, bLo, bHi};
+#pragma unroll
+                for (int pass = 0; pass < 3; ++pass)
+#pragma unroll
+                    for (int step = 0; step < 2 * kTcK / 8; ++step) {
+                        const uint64_t da = matrixDescriptor(As[pass] + uint32_t(2 * step) * lbo, lbo, sbo);
+                        const uint64_t db = matrixDescriptor(Bs[pass] + uint32_t(2 * step) * lbo, lbo, sbo);
+                        const uint32_t accumulate = (c | pass | step) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                            "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
+                    }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smemAddr(&empty[s])));
+                if (c == kTcSteps - 1)  // completes when every MMA of the CTA has
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                        smemAddr(&done)));
+            }
+            __syncwarp();
+        }
     }
-    uint32_t done = 0;
-    for (long it = 0; it < 20000000 && !done; ++it)
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(smemAddr(&mbar)), "r"(0));
-    if (!done && tid == 0)
-        atomicCAS(info, 0, kTensorTimeout);
+    const bool accumulated = __syncthreads_and(ok && waitPhase(smemAddr(&done), 0));
+    if (!accumulated) {
+        if (tid == 0)
+            atomicCAS(info, 0, kTensorTimeout);
+        if (warp == 0)  // let the last copies into each buffer land before the CTA exits
+            for (int c = issued > kTcStages ? issued - kTcStages : 0; c < issued; ++c)
+                waitPhase(smemAddr(&full[c % kTcStages]), uint32_t(c / kTcStages) & 1u);
+    }
     asm volatile("tcgen05.fence::after_thread_sync;");
-    constexpr int kStride = NB + 1;
-    float *staged = tile;  // [MA][NB + 1]: product rows (real parts then imaginary parts) x columns
-    if (done) {
-        // warp w reads lanes 32 (w % 4) .. + 31 and columns 32 (w / 4) .. + 31
-        const int quarter = warp & 3, c = (warp >> 2) * 32;
-        uint32_t v[32];
+    if (accumulated) {
+        uint32_t re[32], im[32];
+        const uint32_t lanes = uint32_t(quarter * 32) << 16;
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
             "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-              "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
-              "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
-              "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-            : "r"(tmem + (uint32_t(quarter * 32) << 16) + uint32_t(c)));
+            : "=r"(re[0]), "=r"(re[1]), "=r"(re[2]), "=r"(re[3]), "=r"(re[4]), "=r"(re[5]), "=r"(re[6]), "=r"(re[7]),
+              "=r"(re[8]), "=r"(re[9]), "=r"(re[10]), "=r"(re[11]), "=r"(re[12]), "=r"(re[13]), "=r"(re[14]),
+              "=r"(re[15]), "=r"(re[16]), "=r"(re[17]), "=r"(re[18]), "=r"(re[19]), "=r"(re[20]), "=r"(re[21]),
+              "=r"(re[22]), "=r"(re[23]), "=r"(re[24]), "=r"(re[25]), "=r"(re[26]), "=r"(re[27]), "=r"(re[28]),
+              "=r"(re[29]), "=r"(re[30]), "=r"(re[31])
+            : "r"(tmem + lanes + uint32_t(half * 32)));
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(im[0]), "=r"(im[1]), "=r"(im[2]), "=r"(im[3]), "=r"(im[4]), "=r"(im[5]), "=r"(im[6]), "=r"(im[7]),
+              "=r"(im[8]), "=r"(im[9]), "=r"(im[10]), "=r"(im[11]), "=r"(im[12]), "=r"(im[13]), "=r"(im[14]),
+              "=r"(im[15]), "=r"(im[16]), "=r"(im[17]), "=r"(im[18]), "=r"(im[19]), "=r"(im[20]), "=r"(im[21]),
+              "=r"(im[22]), "=r"(im[23]), "=r"(im[24]), "=r"(im[25]), "=r"(im[26]), "=r"(im[27]), "=r"(im[28]),
+              "=r"(im[29]), "=r"(im[30]), "=r"(im[31])
+            : "r"(tmem + lanes + uint32_t(kTcCols + half * 32)));
         asm volatile("tcgen05.wait::ld.sync.aligned;");
-        const int row = quarter * 32 + lane;
 #pragma unroll
         for (int j = 0; j < 32; ++j)
-            staged[row * kStride + c + j] = __uint_as_float(v[j]);
+            if (row < N && col0 + j < N)
+                *reinterpret_cast<float2 *>(M + 2 * (size_t(col0 + j) * N + row)) =
+                    make_float2(old[j].x - __uint_as_float(re[j]), old[j].y - __uint_as_float(im[j]));
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0)
+    if (warp == 2)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NB));
-    if (!done)
-        return;
-    for (int e = tid; e < kTileRows * kTileCols; e += kTensorThreads) {
-        const int i = e % kTileRows, j = e / kTileRows;
-        if (r0 + i >= N || c0 + j >= N)
-            continue;
-        float2 *dst = reinterpret_cast<float2 *>(M + 2 * (size_t(c0 + j) * N + r0 + i));
-        float2 v = *dst;
-        v.x -= staged[i * kStride + j];
-        v.y -= staged[(i + kTileRows) * kStride + j];
-        *dst = v;
-    }
 }
 
-constexpr size_t kTensorTileBytes = size_t(2) * (2 * kTileRows + kTileCols) * kTileK * sizeof(float);  // 96 KB
+// U12 = L11^{-1} A12 for the outer block (L11: the kOuter x kOuter unit lower
+// triangle at (K0, K0)), over the trailing columns [K0 + kOuter, N). L11 is
+// staged in shared memory column by column (coalesced); a warp solves one
+// column at a time with lane l holding rows l, l + 32, l + 64, l + 96 in
+// registers and the solved unknown broadcast by shuffle.
+constexpr int kTrsmColumns = 64, kTrsmThreads = 512;
+constexpr size_t kTrsmSmem = size_t(kOuter) * kOuter * sizeof(float2);  // 128 KB
+
+__global__ void __launch_bounds__(kTrsmThreads, 1) trsmBlockKernel(float *LU, uint32_t N, uint32_t K0) {
+    extern __shared__ __align__(16) float2 Lc[];  // [column m][row]
+    float *M = LU + size_t(blockIdx.y) * N * N * 2;
+    for (uint32_t e = threadIdx.x; e < uint32_t(kOuter * kOuter); e += blockDim.x) {
+        const uint32_t r = e % kOuter, m = e / kOuter;
+        Lc[e] = *reinterpret_cast<const float2 *>(M + 2 * (size_t(K0 + m) * N + K0 + r));
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t c0 = K0 + kOuter + blockIdx.x * kTrsmColumns;
+    for (uint32_t c = c0 + warp; c < min(N, c0 + kTrsmColumns); c += kTrsmThreads / 32) {
+        float2 *col = reinterpret_cast<float2 *>(M + 2 * (size_t(c) * N + K0));
+        float2 v[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            v[s] = col[lane + 32 * s];
+#pragma unroll
+        for (int sb = 0; sb < 4; ++sb)
+#pragma unroll 8
+            for (int mm = 0; mm < 32; ++mm) {
+                const int m = 32 * sb + mm;
+                const float2 x =
+                    make_float2(__shfl_sync(0xffffffffu, v[sb].x, mm), __shfl_sync(0xffffffffu, v[sb].y, mm));
+#pragma unroll
+                for (int s = sb; s < 4; ++s)
+                    if (lane + 32 * s > m) {
+                        const float2 a = Lc[m * kOuter + lane + 32 * s];
+                        v[s].x -= a.x * x.x - a.y * x.y;
+                        v[s].y -= a.x * x.y + a.y * x.x;
+                    }
+            }
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            col[lane + 32 * s] = v[s];
+    }
+}
 
 // Forward / back substitution of one right-hand side per CTA, with the
 // vector staged in shared memory. Blocks of 32 unknowns: warp 0 loads the
@@ -987,8 +1161,15 @@ template <class R> uint32_t clusterLimit() {
     return uint32_t(limit);
 }
 
+// Right-looking LU with partial pivoting, 32-wide panels. FP64 runs one
+// level: every panel updates the whole trailing matrix (K = 32). FP32 runs two
+// levels: panels update only the rest of their kOuter-wide outer block, then
+// the outer block's U12 is solved (trsmBlockKernel) and the trailing matrix is
+// updated once with K = kOuter on the tensor cores (trailingTensorKernel).
+// Pivot choices follow the same rule in both; only the order of the update
+// sums differs.
 template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
-                               KernelTimer *timer) {
+                               KernelTimer *timer, float *pack) {
     check(cudaMemsetAsync(info, 0, sizeof(int), stream), "LU info reset");
     const size_t gemmSmem = 2 * kPanel * 64 * sizeof(C2<R>);
     static bool attr = false;
@@ -998,55 +1179,83 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
         check(cudaFuncSetAttribute(panelSmemKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    int(kPanelSmemLimit)),
               "panel smem attribute");
-        if constexpr (sizeof(R) == 4)
-            check(cudaFuncSetAttribute(gemmTensorKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(kTensorTileBytes)),
-                  "tensor gemm smem attribute");
+        if constexpr (sizeof(R) == 4) {
+            check(cudaFuncSetAttribute(trailingTensorKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem)),
+                  "tensor update smem attribute");
+            check(cudaFuncSetAttribute(trsmBlockKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrsmSmem)),
+                  "block trsm smem attribute");
+        }
         attr = true;
     }
-    for (uint32_t k0 = 0; k0 < N; k0 += kPanel) {
-        const uint32_t jb = min(uint32_t(kPanel), N - k0);
-        {
-            TimedScope s(timer, "lu_panel", stream);
-            const size_t bytes = panelSmemBytes<R>(N - k0, jb);
-            const uint32_t rows = N - k0;
-            if (bytes > kPanelSmemLimit && rows <= kClusterRows<R> * clusterLimit<R>()) {
-                const uint32_t C = (rows + kClusterRows<R> - 1) / kClusterRows<R>;
-                const uint32_t perBlock = (rows + C - 1) / C;
-                cudaLaunchConfig_t cfg{};
-                cfg.gridDim = dim3(C, B);
-                cfg.blockDim = dim3((perBlock + 31) / 32 * 32);
-                cfg.dynamicSmemBytes = size_t(jb) * perBlock * sizeof(C2<R>);
-                cfg.stream = stream;
-                cudaLaunchAttribute attr[1];
-                attr[0].id = cudaLaunchAttributeClusterDimension;
-                attr[0].val.clusterDim.x = C;
-                attr[0].val.clusterDim.y = 1;
-                attr[0].val.clusterDim.z = 1;
-                cfg.attrs = attr;
-                cfg.numAttrs = 1;
-                check(cudaLaunchKernelEx(&cfg, panelClusterKernel<R>, LU, N, k0, jb, perBlock, pivots, info),
-                      "cluster panel launch");
-            } else if (bytes <= kPanelSmemLimit)
-                panelSmemKernel<R><<<B, std::min(1024u, (N - k0 + 31) / 32 * 32), bytes, stream>>>(LU, N, k0, jb,
-                                                                                                   pivots, info);
-            else
-                panelKernel<R><<<B, 512, 0, stream>>>(LU, N, k0, jb, pivots, info);
-        }
-        {
-            TimedScope s(timer, "lu_swap", stream);
-            swapKernel<R><<<dim3((N + 127) / 128, B), 128, 0, stream>>>(LU, N, k0, jb, pivots);
-        }
-        const uint32_t rest = N - k0 - jb;
-        if (rest) {
+    const uint32_t outer = sizeof(R) == 4 ? uint32_t(kOuter) : N;
+    for (uint32_t K0 = 0; K0 < N; K0 += outer) {
+        const uint32_t end = std::min(N, K0 + outer);
+        for (uint32_t k0 = K0; k0 < end; k0 += kPanel) {
+            const uint32_t jb = std::min(uint32_t(kPanel), end - k0);
             {
-                TimedScope s(timer, "lu_trsm", stream);
-                trsmKernel<R><<<dim3((rest + kPanel - 1) / kPanel, B), 256, 0, stream>>>(LU, N, k0, jb);
+                TimedScope s(timer, "lu_panel", stream);
+                const size_t bytes = panelSmemBytes<R>(N - k0, jb);
+                const uint32_t rows = N - k0;
+                if (bytes > kPanelSmemLimit && rows <= kClusterRows<R> * clusterLimit<R>()) {
+                    const uint32_t C = (rows + kClusterRows<R> - 1) / kClusterRows<R>;
+                    const uint32_t perBlock = (rows + C - 1) / C;
+                    cudaLaunchConfig_t cfg{};
+                    cfg.gridDim = dim3(C, B);
+                    cfg.blockDim = dim3((perBlock + 31) / 32 * 32);
+                    cfg.dynamicSmemBytes = size_t(jb) * perBlock * sizeof(C2<R>);
+                    cfg.stream = stream;
+                    cudaLaunchAttribute attr[1];
+                    attr[0].id = cudaLaunchAttributeClusterDimension;
+                    attr[0].val.clusterDim.x = C;
+                    attr[0].val.clusterDim.y = 1;
+                    attr[0].val.clusterDim.z = 1;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = 1;
+                    check(cudaLaunchKernelEx(&cfg, panelClusterKernel<R>, LU, N, k0, jb, perBlock, pivots, info),
+                          "cluster panel launch");
+                } else if (bytes <= kPanelSmemLimit)
+                    panelSmemKernel<R><<<B, std::min(1024u, (N - k0 + 31) / 32 * 32), bytes, stream>>>(
+                        LU, N, k0, jb, pivots, info);
+                else
+                    panelKernel<R><<<B, 512, 0, stream>>>(LU, N, k0, jb, pivots, info);
             }
-            TimedScope s(timer, "lu_gemm", stream);
-            gemmKernel<R><<<dim3((rest + 63) / 64, (rest + 63) / 64, B), 256, gemmSmem, stream>>>(LU, N, k0, jb);
+            {
+                TimedScope s(timer, "lu_swap", stream);
+                swapKernel<R><<<dim3((N + 127) / 128, B), 128, 0, stream>>>(LU, N, k0, jb, pivots);
+            }
+            const uint32_t cols = end - k0 - jb;  // columns of the outer block right of the panel
+            if (cols) {
+                {
+                    TimedScope s(timer, "lu_trsm", stream);
+                    trsmKernel<R><<<dim3((cols + kPanel - 1) / kPanel, B), 256, 0, stream>>>(LU, N, k0, jb, end);
+                }
+                TimedScope s(timer, "lu_gemm", stream);
+                const uint32_t rows = N - k0 - jb;
+                gemmKernel<R><<<dim3((rows + 63) / 64, (cols + 63) / 64, B), 256, gemmSmem, stream>>>(LU, N, k0, jb,
+                                                                                                      end);
+            }
+            check(cudaGetLastError(), "LU launch");
         }
-        check(cudaGetLastError(), "LU launch");
+        if constexpr (sizeof(R) == 4) {
+            if (end < N) {
+                const uint32_t rest = N - end;
+                {
+                    TimedScope s(timer, "lu_trsm_outer", stream);
+                    trsmBlockKernel<<<dim3((rest + kTrsmColumns - 1) / kTrsmColumns, B), kTrsmThreads, kTrsmSmem,
+                                      stream>>>(LU, N, K0);
+                }
+                const uint32_t rowTiles = (rest + kTcRows - 1) / kTcRows, colTiles = (rest + kTcCols - 1) / kTcCols;
+                const size_t packStride = packFloats(N);
+                {
+                    TimedScope s(timer, "lu_pack", stream);
+                    packKernel<<<dim3(rowTiles + colTiles, kTcSteps, B), 256, 0, stream>>>(LU, N, K0, pack, packStride);
+                }
+                TimedScope s(timer, "lu_gemm_tensor", stream);
+                trailingTensorKernel<<<dim3(rowTiles, colTiles, B), kTcThreads, kTcSmem, stream>>>(LU, N, K0, pack,
+                                                                                                    packStride, info);
+                check(cudaGetLastError(), "LU outer update launch");
+            }
+        }
     }
 }
 
@@ -1070,11 +1279,11 @@ template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32
 
 void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                    KernelTimer *timer) {
-    factor<double>(LU, N, B, pivots, info, stream, timer);
+    factor<double>(LU, N, B, pivots, info, stream, timer, nullptr);
 }
 void luFactorBatch(float *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
-                   KernelTimer *timer) {
-    factor<float>(LU, N, B, pivots, info, stream, timer);
+                   KernelTimer *timer, float *pack) {
+    factor<float>(LU, N, B, pivots, info, stream, timer, pack);
 }
 void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
                   cudaStream_t stream, KernelTimer *timer) {
@@ -1113,5 +1322,6 @@ void roundToFloat(const double *in, float *out, size_t count, cudaStream_t strea
 }
 
 size_t luWorkspaceBytes(uint32_t N, uint32_t B) { return size_t(B) * N * sizeof(int); }
+size_t luPackBytes(uint32_t N, uint32_t B) { return size_t(B) * packFloats(N) * sizeof(float); }
 
 }  // namespace hsb

@@ -142,8 +142,11 @@ void assembleBatch(const AssemblyGeometry &geo, const double *ks, const double *
 size_t luWorkspaceBytes(uint32_t N, uint32_t B);
 void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                    class KernelTimer *timer);
+// FP32 factorisation: `pack` holds luPackBytes(N, B) of operand tiles for the
+// tensor-core trailing updates.
+size_t luPackBytes(uint32_t N, uint32_t B);
 void luFactorBatch(float *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
-                   class KernelTimer *timer);
+                   class KernelTimer *timer, float *pack);
 void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
                   cudaStream_t stream, class KernelTimer *timer);
 void luSolveBatch(const float *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, float *x,

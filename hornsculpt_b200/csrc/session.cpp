@@ -302,7 +302,7 @@ namespace {
 uint64_t perFrequencyBytes(uint64_t T, uint64_t N, uint32_t E, uint32_t O, bool mixed, uint32_t restart) {
     return assemblyWorkspaceBytes(uint32_t(T), uint32_t(N), E, 1, mixed) + 2 * N * N * 16 + 4 * E * N * 16 +
            E * T * 16 + fieldPartialsBytes(uint32_t(T), E, O, 1) +
-           (mixed ? gmresWorkspaceBytes(uint32_t(N), E, restart) : 0) + 64;
+           (mixed ? gmresWorkspaceBytes(uint32_t(N), E, restart) + luPackBytes(uint32_t(N), 1) : 0) + 64;
 }
 }  // namespace
 
@@ -320,7 +320,7 @@ size_t Session::residentBytes() const {
                                   &dRowScale_, &dMass_, &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_,
                                   &dSingularTable_, &dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dA_,
                                   &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_, &dPivots_, &dKs_, &dFlux_, &dObservers_,
-                                  &dPartials_, &dField_, &dDegrees_, &dWork32_, &dGmres_})
+                                  &dPartials_, &dField_, &dDegrees_, &dWork32_, &dGmres_, &dLuPack_})
         bytes += b->bytes();
     return bytes;
 }
@@ -345,8 +345,10 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, ui
     dRecords_.ensure(std::max<size_t>(B * recordBytes(uint32_t(T), mixed), 16));
     if (gatherUsesColumns(uint32_t(T)))
         dColumns_.ensure(B * N * 6 * T * 8);
-    if (mixed)
+    if (mixed) {
         dGmres_.ensure(gmresWorkspaceBytes(uint32_t(N), B * E, restart));
+        dLuPack_.ensure(std::max<size_t>(luPackBytes(uint32_t(N), B), 16));
+    }
     dPanelRhs_.ensure(B * E * 6 * T * 8);
     dBins_.ensure(std::max<size_t>(B * kBins * pairs * sizeof(uint2), 16));
     dBinCounts_.ensure(B * kBins * sizeof(uint32_t));
@@ -370,7 +372,7 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, ui
                                   &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_, &dRecords_, &dColumns_,
                                   &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
                                   &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_,
-                                  &dWork32_, &dGmres_})
+                                  &dWork32_, &dGmres_, &dLuPack_})
         bytes += b->bytes();
     peakBytes_ = std::max(peakBytes_, bytes);
 }
@@ -542,7 +544,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 TimedScope scope(&timer_, "round_fp32", s);
                 roundToFloat(dA_.as<double>(), LU32, matrixReals, s);
             }
-            luFactorBatch(LU32, N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_);
+            luFactorBatch(LU32, N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_, dLuPack_.as<float>());
         } else {
             cuda(cudaMemcpyAsync(dLU_.as<void>(), dA_.as<void>(), matrixReals * 8, cudaMemcpyDeviceToDevice, s),
                  "factorization copy");
