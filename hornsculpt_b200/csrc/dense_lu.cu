@@ -281,64 +281,89 @@ __global__ void __launch_bounds__(1024) panelSmemKernel(R *LU, uint32_t N, uint3
 }
 
 // Panel factorisation for tall panels, spread over a thread-block cluster:
-// CTA r of the cluster holds panel rows [r * rowsPerBlock, ...) in shared
-// memory. Pivot choice, tie rule and interchange sequence are those of
-// panelSmemKernel. Per column: each warp's best candidate goes to its CTA's
-// shared memory (double-buffered by column parity); one cluster barrier;
+// CTA r of the cluster owns panel rows [r * rowsPerBlock, ...). The first
+// `cap` of them live in shared memory, one per thread; the rest (at most
+// kGlobalSlots per thread) stay in place in global memory and are eliminated
+// there by their thread. Pivot choice, tie rule and interchange sequence are
+// those of panelSmemKernel. Per column: each warp's best candidate goes to its
+// CTA's shared memory (double-buffered by column parity); one cluster barrier;
 // every warp reduces the candidates of all CTAs through distributed shared
-// memory; one warp per CTA copies the pivot row from the CTA that holds it;
-// each CTA eliminates its own rows. Rows that are pivots never change again,
-// so reading them remotely needs no further barrier; a final cluster barrier
-// keeps every CTA's shared memory alive until all remote reads are done.
+// memory; one warp per CTA copies the pivot row from the CTA that holds it
+// (distributed shared memory, or global memory for a row kept there); each
+// CTA eliminates its own rows. Rows that are pivots never change again, so
+// reading them remotely needs no further barrier. Write-back: a row kept in
+// global memory moves only when it is a pivot, to one of the first jb
+// positions, whose own rows are in CTA 0's shared memory; such rows are copied
+// first, and after a cluster barrier the shared-memory rows are written to
+// their final positions. A final cluster barrier keeps every CTA's shared
+// memory alive until all remote reads are done.
 template <class R> constexpr uint32_t kClusterRows = sizeof(R) == 8 ? 384 : 768;
 constexpr uint32_t kMaxCluster = 16;
+constexpr int kGlobalSlots = 4;
 
 template <class R> struct ClusterPanelShared {
-    R best[2][32];
-    int idx[2][32];
+    R best[32];
+    int idx[32];
+    R ctaBest[2];  // this CTA's candidate per column parity
+    int ctaIdx[2];
     C2<R> pivot[kPanel];
     int sel[kPanel];
     int mapRow[2 * kPanel], mapPos[2 * kPanel];
     int mapCount;
 };
 
-template <class R>
+template <class R, int Slots>
 __global__ void __launch_bounds__(1024) panelClusterKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb,
-                                                           uint32_t rowsPerBlock, int *pivots, int *info) {
+                                                           uint32_t rowsPerBlock, uint32_t cap, int *pivots,
+                                                           int *info) {
     namespace cg = cooperative_groups;
     cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char rawSmem[];
     __shared__ ClusterPanelShared<R> sh;
-    C2<R> *P = reinterpret_cast<C2<R> *>(rawSmem);  // [jb][rowsPerBlock]
+    C2<R> *P = reinterpret_cast<C2<R> *>(rawSmem);  // [jb][cap]
     const uint32_t rank = cluster.block_rank(), C = cluster.num_blocks();
     const uint32_t rows = N - k0, rowBegin = rank * rowsPerBlock;
     const uint32_t myRows = rowBegin < rows ? min(rowsPerBlock, rows - rowBegin) : 0u;
     R *M = LU + size_t(blockIdx.y) * N * N * 2;
     int *piv = pivots + size_t(blockIdx.y) * N;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = int(blockDim.x >> 5);
-    const uint32_t i = threadIdx.x;  // one row per thread: blockDim.x >= rowsPerBlock
-    const bool own = i < myRows;
-    const uint32_t g = rowBegin + i;  // panel row of this thread
+    const uint32_t i = threadIdx.x;
+    // slot 0: shared-memory row i; slot s >= 1: global row cap + (s - 1) * blockDim + i
+    const auto local = [&](int s) { return s == 0 ? i : cap + uint32_t(s - 1) * blockDim.x + i; };
+    const auto owns = [&](int s) { return s == 0 ? (i < cap && i < myRows) : local(s) < myRows; };
+    const auto column = [&](uint32_t q) { return M + 2 * (size_t(k0 + q) * N + k0); };  // panel column q
     constexpr int kLoad = sizeof(R) == 8 ? 4 : 8;
-    if (own)
+    if (owns(0))
         for (uint32_t q0 = 0; q0 < jb; q0 += kLoad) {
             C2<R> v[kLoad];
 #pragma unroll
             for (int t = 0; t < kLoad; ++t)
                 if (q0 + t < jb)
-                    v[t] = ld2(M + 2 * (size_t(k0 + q0 + t) * N + k0 + g));
+                    v[t] = ld2(column(q0 + t) + 2 * (rowBegin + i));
 #pragma unroll
             for (int t = 0; t < kLoad; ++t)
                 if (q0 + t < jb)
-                    P[size_t(q0 + t) * rowsPerBlock + i] = v[t];
+                    P[size_t(q0 + t) * cap + i] = v[t];
         }
-    bool taken = !own;
     const auto magnitude = [](C2<R> z) {
         const R a = fabs(z.x) + fabs(z.y);
         return a >= R(0) ? a : R(0);  // a NaN row competes as zero, so a pivot row always exists
     };
-    R best = own ? magnitude(P[i]) : R(-1);
-    int bestRow = own ? int(g) : int(rows);
+    bool taken[1 + Slots];
+    R best = R(-1);
+    int bestRow = int(rows);
+#pragma unroll
+    for (int s = 0; s <= Slots; ++s) {
+        taken[s] = !owns(s);
+        if (!taken[s]) {
+            const uint32_t g = rowBegin + local(s);
+            const R m = magnitude(s == 0 ? P[i] : ld2(column(0) + 2 * g));
+            if (m > best || (m == best && int(g) < bestRow)) {
+                best = m;
+                bestRow = int(g);
+            }
+        }
+    }
     for (uint32_t j = 0; j < jb; ++j) {
         const int buf = j & 1;
         for (int off = 16; off > 0; off >>= 1) {
@@ -350,21 +375,34 @@ __global__ void __launch_bounds__(1024) panelClusterKernel(R *LU, uint32_t N, ui
             }
         }
         if (lane == 0) {
-            sh.best[buf][warp] = best;
-            sh.idx[buf][warp] = bestRow;
+            sh.best[warp] = best;
+            sh.idx[warp] = bestRow;
+        }
+        __syncthreads();
+        if (warp == 0) {  // this CTA's candidate
+            R b = lane < W ? sh.best[lane] : R(-1);
+            int r = lane < W ? sh.idx[lane] : int(rows);
+            for (int off = 16; off > 0; off >>= 1) {
+                const R ob = __shfl_xor_sync(0xffffffffu, b, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, r, off);
+                if (ob > b || (ob == b && oi < r)) {
+                    b = ob;
+                    r = oi;
+                }
+            }
+            if (lane == 0) {
+                sh.ctaBest[buf] = b;
+                sh.ctaIdx[buf] = r;
+            }
         }
         cluster.sync();
-        // all candidates of the cluster, read through distributed shared memory
+        // the candidates of all CTAs, one per lane, read through distributed shared memory
         R pb = R(-1);
         int p = int(rows);
-        for (uint32_t e = lane; e < C * uint32_t(W); e += 32) {
-            const ClusterPanelShared<R> *other = cluster.map_shared_rank(&sh, int(e / W));
-            const R b = other->best[buf][e % W];
-            const int r = other->idx[buf][e % W];
-            if (b > pb || (b == pb && r < p)) {
-                pb = b;
-                p = r;
-            }
+        if (uint32_t(lane) < C) {
+            const ClusterPanelShared<R> *other = cluster.map_shared_rank(&sh, lane);
+            pb = other->ctaBest[buf];
+            p = other->ctaIdx[buf];
         }
         for (int off = 16; off > 0; off >>= 1) {
             const R ob = __shfl_xor_sync(0xffffffffu, pb, off);
@@ -375,11 +413,14 @@ __global__ void __launch_bounds__(1024) panelClusterKernel(R *LU, uint32_t N, ui
             }
         }
         if (warp == 0) {
-            // copy the pivot row (columns j.. of panel row p) from its CTA
-            const C2<R> *src = cluster.map_shared_rank(P, int(uint32_t(p) / rowsPerBlock));
-            const uint32_t local = uint32_t(p) % rowsPerBlock;
-            if (uint32_t(lane) >= j && uint32_t(lane) < jb)
-                sh.pivot[lane] = src[size_t(lane) * rowsPerBlock + local];
+            // copy the pivot row (columns j.. of panel row p) from the CTA that holds it
+            const uint32_t owner = uint32_t(p) / rowsPerBlock, at = uint32_t(p) % rowsPerBlock;
+            if (uint32_t(lane) >= j && uint32_t(lane) < jb) {
+                if (at < cap)
+                    sh.pivot[lane] = cluster.map_shared_rank(P, int(owner))[size_t(lane) * cap + at];
+                else
+                    sh.pivot[lane] = ld2(column(lane) + 2 * uint32_t(p));
+            }
             if (rank == 0 && lane == 0) {
                 sh.sel[j] = p;
                 if (!(pb > 0) && *info == 0)
@@ -391,32 +432,61 @@ __global__ void __launch_bounds__(1024) panelClusterKernel(R *LU, uint32_t N, ui
         const R den = d.x * d.x + d.y * d.y;
         const R rden = den > 0 ? R(1) / den : R(0);
         const C2<R> inv = mk<R>(d.x * rden, -d.y * rden);
-        if (own && int(g) == p)
-            taken = true;
         best = -1;
         bestRow = int(rows);
-        if (!taken) {
-            const C2<R> l = cmul<R>(P[size_t(j) * rowsPerBlock + i], inv);
-            P[size_t(j) * rowsPerBlock + i] = l;
+#pragma unroll
+        for (int s = 0; s <= Slots; ++s) {
+            if (taken[s])
+                continue;
+            const uint32_t g = rowBegin + local(s);
+            if (int(g) == p) {
+                taken[s] = true;
+                continue;
+            }
             C2<R> next = mk<R>(0, 0);
-            for (uint32_t q0 = j + 1; q0 < jb; q0 += kLoad) {
-                C2<R> v[kLoad];
+            if (s == 0) {
+                const C2<R> l = cmul<R>(P[size_t(j) * cap + i], inv);
+                P[size_t(j) * cap + i] = l;
+                for (uint32_t q0 = j + 1; q0 < jb; q0 += kLoad) {
+                    C2<R> v[kLoad];
 #pragma unroll
-                for (int t = 0; t < kLoad; ++t)
-                    if (q0 + t < jb)
-                        v[t] = P[size_t(q0 + t) * rowsPerBlock + i];
+                    for (int t = 0; t < kLoad; ++t)
+                        if (q0 + t < jb)
+                            v[t] = P[size_t(q0 + t) * cap + i];
 #pragma unroll
-                for (int t = 0; t < kLoad; ++t)
-                    if (q0 + t < jb) {
-                        csub<R>(v[t], l, sh.pivot[q0 + t]);
-                        P[size_t(q0 + t) * rowsPerBlock + i] = v[t];
-                    }
-                if (q0 == j + 1)
-                    next = v[0];
+                    for (int t = 0; t < kLoad; ++t)
+                        if (q0 + t < jb) {
+                            csub<R>(v[t], l, sh.pivot[q0 + t]);
+                            P[size_t(q0 + t) * cap + i] = v[t];
+                        }
+                    if (q0 == j + 1)
+                        next = v[0];
+                }
+            } else {
+                const C2<R> l = cmul<R>(ld2(column(j) + 2 * g), inv);
+                st2(column(j) + 2 * g, l);
+                for (uint32_t q0 = j + 1; q0 < jb; q0 += kLoad) {
+                    C2<R> v[kLoad];
+#pragma unroll
+                    for (int t = 0; t < kLoad; ++t)
+                        if (q0 + t < jb)
+                            v[t] = ld2(column(q0 + t) + 2 * g);
+#pragma unroll
+                    for (int t = 0; t < kLoad; ++t)
+                        if (q0 + t < jb) {
+                            csub<R>(v[t], l, sh.pivot[q0 + t]);
+                            st2(column(q0 + t) + 2 * g, v[t]);
+                        }
+                    if (q0 == j + 1)
+                        next = v[0];
+                }
             }
             if (j + 1 < jb) {
-                best = magnitude(next);
-                bestRow = int(g);
+                const R m = magnitude(next);
+                if (m > best || (m == best && int(g) < bestRow)) {
+                    best = m;
+                    bestRow = int(g);
+                }
             }
         }
     }
@@ -473,14 +543,28 @@ __global__ void __launch_bounds__(1024) panelClusterKernel(R *LU, uint32_t N, ui
     }
     cluster.sync();
     const ClusterPanelShared<R> *root = cluster.map_shared_rank(&sh, 0);
-    if (own) {
+    const int moved = root->mapCount;
+    const auto finalPosition = [&](uint32_t g) {
         uint32_t pos = g;
-        const int n = root->mapCount;
-        for (int q = 0; q < n; ++q)
+        for (int q = 0; q < moved; ++q)
             if (root->mapRow[q] == int(g))
                 pos = uint32_t(root->mapPos[q]);
+        return pos;
+    };
+    // pivots kept in global memory move to their positions (< jb; those rows are in CTA 0's shared memory)
+#pragma unroll
+    for (int s = 1; s <= Slots; ++s)
+        if (owns(s)) {
+            const uint32_t g = rowBegin + local(s), pos = finalPosition(g);
+            if (pos != g)
+                for (uint32_t q = 0; q < jb; ++q)
+                    st2(column(q) + 2 * pos, ld2(column(q) + 2 * g));
+        }
+    cluster.sync();
+    if (owns(0)) {
+        const uint32_t g = rowBegin + i, pos = finalPosition(g);
         for (uint32_t q = 0; q < jb; ++q)
-            st2(M + 2 * (size_t(k0 + q) * N + k0 + pos), P[size_t(q) * rowsPerBlock + i]);
+            st2(column(q) + 2 * pos, P[size_t(q) * cap + i]);
     }
     cluster.sync();  // keep rank 0's map alive until every CTA has read it
 }
@@ -1038,6 +1122,189 @@ __global__ void __launch_bounds__(sizeof(R) == 8 ? 256 : 512) solveKernel(const 
         st2(out + 2 * i, x[i]);
 }
 
+// Blocked triangular solves for many CTAs. The row interchanges of a
+// factorisation are composed once into a permutation (permutationKernel,
+// stored after the interchanges), so a solve starts with a parallel gather of
+// the right-hand side into a work vector. Forward and backward substitution
+// then run in blocks of kTriBlock unknowns, one launch per block: CTA 0 brings
+// the next block's rows up to date with the block solved last and solves the
+// next diagonal block (32 x 32 sub-blocks in warp 0's registers, as in
+// solveKernel); the other CTAs apply the block solved last to every remaining
+// row (64 rows x 4 column groups of 32 per CTA, coalesced column reads, the four
+// partial sums added in a fixed order). The backward sweep writes each solved
+// block to the output vector.
+constexpr uint32_t kTriBlock = 128, kTriRows = 64;
+constexpr uint32_t kSmallSolve = 1024;  // up to this N the one-CTA-per-system kernel is faster
+
+__global__ void permutationKernel(const int *pivots, uint32_t N, int *perm) {
+    extern __shared__ int p[];
+    const int *piv = pivots + size_t(blockIdx.x) * N;
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
+        p[i] = int(i);
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (uint32_t c = 0; c < N; ++c) {
+            const int q = piv[c];
+            if (q != int(c)) {
+                const int t = p[c];
+                p[c] = p[q];
+                p[q] = t;
+            }
+        }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
+        perm[size_t(blockIdx.x) * N + i] = p[i];
+}
+
+// work[f][e][i] = x[f][e][perm[f][i]]
+template <class R> __global__ void gatherRhsKernel(const R *x, const int *perm, uint32_t N, uint32_t E, R *work) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, e = blockIdx.y, f = blockIdx.z;
+    if (i >= N)
+        return;
+    const size_t v = (size_t(f) * E + e) * N;
+    st2(work + 2 * (v + i), ld2(x + 2 * (v + perm[size_t(f) * N + i])));
+}
+
+// One step of a sweep. Known block: unknowns [c0, c0 + cw) (cw = 0 on the first step); next block
+// [n0, n0 + nw). Forward (Lower): unit lower triangle, updated rows [n0 + nw, N). Backward: upper
+// triangle with its diagonal, updated rows [0, n0).
+template <class R, bool Lower>
+__global__ void __launch_bounds__(256) triStepKernel(const R *LU, uint32_t N, uint32_t E, R *work, R *out, uint32_t c0,
+                                                     uint32_t cw, uint32_t n0, uint32_t nw) {
+    __shared__ C2<R> y[kTriBlock];
+    __shared__ C2<R> part[4][kTriBlock];
+    __shared__ C2<R> v[kTriBlock];
+    const uint32_t e = blockIdx.y, f = blockIdx.z, tid = threadIdx.x;
+    const R *M = LU + size_t(f) * N * N * 2;
+    R *w = work + (size_t(f) * E + e) * N * 2;
+    const C2<R> zero = mk<R>(0, 0);
+    for (uint32_t i = tid; i < cw; i += blockDim.x)
+        y[i] = ld2(w + 2 * (c0 + i));
+    __syncthreads();
+    if (blockIdx.x > 0) {  // rows outside the next block
+        const uint32_t i = tid % kTriRows, g = tid / kTriRows;
+        const uint32_t r = (Lower ? n0 + nw : 0) + (blockIdx.x - 1) * kTriRows + i;
+        const uint32_t rEnd = Lower ? N : n0;
+        C2<R> acc = zero;
+        if (r < rEnd) {
+            if (cw == kTriBlock) {  // full block: the 32 column loads in flight together
+                C2<R> a[32];
+#pragma unroll
+                for (int c = 0; c < 32; ++c)
+                    a[c] = ld2(M + 2 * (size_t(c0 + 32 * g + c) * N + r));
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    const C2<R> b = y[32 * g + c];
+                    acc.x += a[c].x * b.x - a[c].y * b.y;
+                    acc.y += a[c].x * b.y + a[c].y * b.x;
+                }
+            } else {
+                const uint32_t cEnd = min(cw, 32 * g + 32);
+                for (uint32_t c = 32 * g; c < cEnd; ++c) {
+                    const C2<R> a = ld2(M + 2 * (size_t(c0 + c) * N + r)), b = y[c];
+                    acc.x += a.x * b.x - a.y * b.y;
+                    acc.y += a.x * b.y + a.y * b.x;
+                }
+            }
+        }
+        part[g][i] = acc;
+        __syncthreads();
+        if (g == 0 && r < rEnd) {
+            C2<R> t = ld2(w + 2 * r);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                t.x -= part[q][i].x;
+                t.y -= part[q][i].y;
+            }
+            st2(w + 2 * r, t);
+        }
+        return;
+    }
+    // CTA 0: the next block's rows, then its diagonal block
+    {
+        const uint32_t i = tid % kTriBlock, g = tid / kTriBlock;  // 2 groups of 64 columns
+        C2<R> acc = zero;
+        if (i < nw) {
+            const uint32_t cEnd = min(cw, 64 * g + 64);
+            for (uint32_t c = 64 * g; c < cEnd; c += 16) {  // 16 column loads in flight together
+                C2<R> a[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q)
+                    a[q] = c + q < cEnd ? ld2(M + 2 * (size_t(c0 + c + q) * N + n0 + i)) : zero;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const C2<R> b = c + q < cEnd ? y[c + q] : zero;
+                    acc.x += a[q].x * b.x - a[q].y * b.y;
+                    acc.y += a[q].x * b.y + a[q].y * b.x;
+                }
+            }
+        }
+        part[g][i] = acc;
+        __syncthreads();
+        if (tid < nw) {
+            C2<R> t = ld2(w + 2 * (n0 + tid));
+            t.x -= part[0][tid].x + part[1][tid].x;
+            t.y -= part[0][tid].y + part[1][tid].y;
+            v[tid] = t;
+        }
+        __syncthreads();
+    }
+    const int lane = tid & 31, warp = tid >> 5;
+    const uint32_t subs = (nw + 31) / 32;
+    for (uint32_t q = 0; q < subs; ++q) {
+        const uint32_t sb = Lower ? q : subs - 1 - q;  // sub-block order
+        const uint32_t k = 32 * sb, kb = min(32u, nw - k);
+        if (warp == 0) {
+            C2<R> L[32];
+#pragma unroll
+            for (int m = 0; m < 32; ++m)
+                L[m] = (m < int(kb) && lane < int(kb)) ? ld2(M + 2 * (size_t(n0 + k + m) * N + n0 + k + lane)) : zero;
+            C2<R> mine = lane < int(kb) ? v[k + lane] : zero;
+            if (Lower) {
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const C2<R> xm = mk<R>(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
+                    if (lane > m)
+                        csub<R>(mine, L[m], xm);
+                }
+            } else {
+#pragma unroll
+                for (int m = 31; m >= 0; --m) {
+                    if (m < int(kb)) {
+                        if (lane == m) {
+                            const C2<R> d = L[m];
+                            const R den = d.x * d.x + d.y * d.y;
+                            mine = mk<R>((mine.x * d.x + mine.y * d.y) / den, (mine.y * d.x - mine.x * d.y) / den);
+                        }
+                        const C2<R> xm =
+                            mk<R>(__shfl_sync(0xffffffffu, mine.x, m), __shfl_sync(0xffffffffu, mine.y, m));
+                        if (lane < m)
+                            csub<R>(mine, L[m], xm);
+                    }
+                }
+            }
+            if (lane < int(kb))
+                v[k + lane] = mine;
+        }
+        __syncthreads();
+        // the rest of the block: rows after (forward) or before (backward) the sub-block
+        const uint32_t rBegin = Lower ? k + kb : 0, rEnd = Lower ? nw : k;
+        for (uint32_t r = rBegin + tid; r < rEnd; r += blockDim.x) {
+            C2<R> t = v[r];
+#pragma unroll 8
+            for (uint32_t m = 0; m < kb; ++m)
+                csub<R>(t, ld2(M + 2 * (size_t(n0 + k + m) * N + n0 + r)), v[k + m]);
+            v[r] = t;
+        }
+        __syncthreads();
+    }
+    if (tid < nw) {
+        st2(w + 2 * (n0 + tid), v[tid]);
+        if (!Lower)
+            st2(out + 2 * ((size_t(f) * E + e) * N + n0 + tid), v[tid]);
+    }
+}
+
 // r = b - A x per row (FP64 accumulation), plus mass-scaled squares for the
 // norms. A CTA takes 32 rows; its 8 warps take every 8th column, and the 8
 // partial sums are added in a fixed order (deterministic).
@@ -1129,20 +1396,23 @@ template <class R> uint32_t clusterLimit() {
         return uint32_t(limit);
     const size_t smem = size_t(kPanel) * kClusterRows<R> * sizeof(C2<R>);
     limit = 0;
-    if (cudaFuncSetAttribute(panelClusterKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) !=
-        cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
+    for (const void *kernel : {reinterpret_cast<const void *>(panelClusterKernel<R, 0>),
+                               reinterpret_cast<const void *>(panelClusterKernel<R, kGlobalSlots>)})
+        if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
+            cudaGetLastError();
+            return 0;
+        }
     for (uint32_t c : {kMaxCluster, 8u}) {
-        if (c > 8 &&
-            cudaFuncSetAttribute(panelClusterKernel<R>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+        if (c > 8 && (cudaFuncSetAttribute(panelClusterKernel<R, 0>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                          cudaSuccess ||
+                      cudaFuncSetAttribute(panelClusterKernel<R, kGlobalSlots>,
+                                           cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
             cudaGetLastError();
             continue;
         }
         cudaLaunchConfig_t cfg{};
         cfg.gridDim = dim3(c, 1);
-        cfg.blockDim = dim3(kClusterRows<R>);
+        cfg.blockDim = dim3(1024);  // the largest launch: rows kept in global memory as well
         cfg.dynamicSmemBytes = smem;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1152,7 +1422,8 @@ template <class R> uint32_t clusterLimit() {
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        if (cudaOccupancyMaxActiveClusters(&clusters, panelClusterKernel<R>, &cfg) == cudaSuccess && clusters > 0) {
+        if (cudaOccupancyMaxActiveClusters(&clusters, panelClusterKernel<R, kGlobalSlots>, &cfg) == cudaSuccess &&
+            clusters > 0) {
             limit = int(c);
             break;
         }
@@ -1196,13 +1467,17 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
                 TimedScope s(timer, "lu_panel", stream);
                 const size_t bytes = panelSmemBytes<R>(N - k0, jb);
                 const uint32_t rows = N - k0;
-                if (bytes > kPanelSmemLimit && rows <= kClusterRows<R> * clusterLimit<R>()) {
-                    const uint32_t C = (rows + kClusterRows<R> - 1) / kClusterRows<R>;
+                const uint32_t limit = clusterLimit<R>();
+                if (bytes > kPanelSmemLimit && rows <= limit * (kClusterRows<R> + kGlobalSlots * 1024u)) {
+                    // as few CTAs as hold the panel in shared memory, else the whole cluster with the
+                    // rows beyond kClusterRows per CTA kept in global memory
+                    const uint32_t C = std::min(limit, (rows + kClusterRows<R> - 1) / kClusterRows<R>);
                     const uint32_t perBlock = (rows + C - 1) / C;
+                    const uint32_t cap = std::min(perBlock, kClusterRows<R>);
                     cudaLaunchConfig_t cfg{};
                     cfg.gridDim = dim3(C, B);
-                    cfg.blockDim = dim3((perBlock + 31) / 32 * 32);
-                    cfg.dynamicSmemBytes = size_t(jb) * perBlock * sizeof(C2<R>);
+                    cfg.blockDim = dim3(perBlock <= cap ? (perBlock + 31) / 32 * 32 : 1024u);
+                    cfg.dynamicSmemBytes = size_t(jb) * cap * sizeof(C2<R>);
                     cfg.stream = stream;
                     cudaLaunchAttribute attr[1];
                     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1211,8 +1486,14 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
                     attr[0].val.clusterDim.z = 1;
                     cfg.attrs = attr;
                     cfg.numAttrs = 1;
-                    check(cudaLaunchKernelEx(&cfg, panelClusterKernel<R>, LU, N, k0, jb, perBlock, pivots, info),
-                          "cluster panel launch");
+                    if (perBlock <= cap)
+                        check(cudaLaunchKernelEx(&cfg, panelClusterKernel<R, 0>, LU, N, k0, jb, perBlock, cap, pivots,
+                                                 info),
+                              "cluster panel launch");
+                    else
+                        check(cudaLaunchKernelEx(&cfg, panelClusterKernel<R, kGlobalSlots>, LU, N, k0, jb, perBlock, cap,
+                                                 pivots, info),
+                              "cluster panel launch");
                 } else if (bytes <= kPanelSmemLimit)
                     panelSmemKernel<R><<<B, std::min(1024u, (N - k0 + 31) / 32 * 32), bytes, stream>>>(
                         LU, N, k0, jb, pivots, info);
@@ -1260,19 +1541,53 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
 }
 
 template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, R *x,
-                              cudaStream_t stream, KernelTimer *timer) {
+                              void *scratch, cudaStream_t stream, KernelTimer *timer) {
+    TimedScope s(timer, "lu_solve", stream);
     const size_t smem = size_t(N) * sizeof(C2<R>);
-    if (smem > 227 * 1024)
-        throw std::runtime_error("Dense solve vector exceeds shared memory (N too large for the dense form).");
+    if (N <= kSmallSolve) {  // one CTA per system: the vector in shared memory, no launch per block
+        static size_t attr = 0;
+        if (smem > 48 * 1024 && smem > attr) {
+            check(cudaFuncSetAttribute(solveKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+                  "solve smem attribute");
+            attr = smem;
+        }
+        solveKernel<R><<<dim3(E, B), sizeof(R) == 8 ? 256 : 512, smem, stream>>>(LU, pivots, N, E, x);
+        check(cudaGetLastError(), "triangular solve launch");
+        return;
+    }
+    const int *perm = pivots + size_t(B) * N;
+    R *work = static_cast<R *>(scratch);
+    gatherRhsKernel<R><<<dim3((N + 255) / 256, E, B), 256, 0, stream>>>(x, perm, N, E, work);
+    const uint32_t blocks = (N + kTriBlock - 1) / kTriBlock;
+    // forward: block b is solved in step b with the rows updated by block b - 1
+    for (uint32_t b = 0; b < blocks; ++b) {
+        const uint32_t n0 = b * kTriBlock, nw = std::min(kTriBlock, N - n0);
+        const uint32_t c0 = b ? n0 - kTriBlock : 0, cw = b ? kTriBlock : 0;
+        const uint32_t rows = N - n0 - nw;
+        triStepKernel<R, true><<<dim3(1 + (rows + kTriRows - 1) / kTriRows, E, B), 256, 0, stream>>>(
+            LU, N, E, work, x, c0, cw, n0, nw);
+    }
+    // backward: from the last block up
+    for (uint32_t q = 0; q < blocks; ++q) {
+        const uint32_t b = blocks - 1 - q;
+        const uint32_t n0 = b * kTriBlock, nw = std::min(kTriBlock, N - n0);
+        const uint32_t c0 = q ? n0 + kTriBlock : 0, cw = q ? std::min(kTriBlock, N - c0) : 0;
+        triStepKernel<R, false><<<dim3(1 + (n0 + kTriRows - 1) / kTriRows, E, B), 256, 0, stream>>>(
+            LU, N, E, work, x, c0, cw, n0, nw);
+    }
+    check(cudaGetLastError(), "triangular solve launch");
+}
+
+template <class R> void permutation(const int *pivots, uint32_t N, uint32_t B, cudaStream_t stream) {
+    const size_t smem = size_t(N) * sizeof(int);
     static size_t attr = 0;
     if (smem > 48 * 1024 && smem > attr) {
-        check(cudaFuncSetAttribute(solveKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
-              "solve smem attribute");
+        check(cudaFuncSetAttribute(permutationKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+              "permutation smem attribute");
         attr = smem;
     }
-    TimedScope s(timer, "lu_solve", stream);
-    solveKernel<R><<<dim3(E, B), sizeof(R) == 8 ? 256 : 512, smem, stream>>>(LU, pivots, N, E, x);
-    check(cudaGetLastError(), "triangular solve launch");
+    permutationKernel<<<B, 256, smem, stream>>>(pivots, N, const_cast<int *>(pivots) + size_t(B) * N);
+    check(cudaGetLastError(), "permutation launch");
 }
 
 }  // namespace
@@ -1280,18 +1595,20 @@ template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32
 void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                    KernelTimer *timer) {
     factor<double>(LU, N, B, pivots, info, stream, timer, nullptr);
+    permutation<double>(pivots, N, B, stream);
 }
 void luFactorBatch(float *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                    KernelTimer *timer, float *pack) {
     factor<float>(LU, N, B, pivots, info, stream, timer, pack);
+    permutation<float>(pivots, N, B, stream);
 }
 void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
-                  cudaStream_t stream, KernelTimer *timer) {
-    solve<double>(LU, pivots, N, B, E, x, stream, timer);
+                  void *scratch, cudaStream_t stream, KernelTimer *timer) {
+    solve<double>(LU, pivots, N, B, E, x, scratch, stream, timer);
 }
 void luSolveBatch(const float *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, float *x,
-                  cudaStream_t stream, KernelTimer *timer) {
-    solve<float>(LU, pivots, N, B, E, x, stream, timer);
+                  void *scratch, cudaStream_t stream, KernelTimer *timer) {
+    solve<float>(LU, pivots, N, B, E, x, scratch, stream, timer);
 }
 
 void residualBatch(const double *A, const double *b, const double *x, const double *mass, uint32_t N, uint32_t B,
@@ -1321,7 +1638,7 @@ void roundToFloat(const double *in, float *out, size_t count, cudaStream_t strea
     check(cudaGetLastError(), "FP32 rounding launch");
 }
 
-size_t luWorkspaceBytes(uint32_t N, uint32_t B) { return size_t(B) * N * sizeof(int); }
+size_t luWorkspaceBytes(uint32_t N, uint32_t B) { return 2 * size_t(B) * N * sizeof(int); }
 size_t luPackBytes(uint32_t N, uint32_t B) { return size_t(B) * packFloats(N) * sizeof(float); }
 
 }  // namespace hsb

@@ -138,7 +138,10 @@ void assembleBatch(const AssemblyGeometry &geo, const double *ks, const double *
                    uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
                    cudaStream_t stream, class KernelTimer *timer, bool mixed = false);
 
-// Batched dense LU (partial pivoting) and solves, complex FP64 column-major.
+// Batched dense LU (partial pivoting) and solves, complex column-major. The
+// pivot buffer holds luWorkspaceBytes(N, B): the LAPACK-style interchanges
+// of each matrix, then their composition as a permutation. A solve needs
+// B * E * N complex elements of scratch.
 size_t luWorkspaceBytes(uint32_t N, uint32_t B);
 void luFactorBatch(double *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                    class KernelTimer *timer);
@@ -148,9 +151,9 @@ size_t luPackBytes(uint32_t N, uint32_t B);
 void luFactorBatch(float *LU, uint32_t N, uint32_t B, int *pivots, int *info, cudaStream_t stream,
                    class KernelTimer *timer, float *pack);
 void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
-                  cudaStream_t stream, class KernelTimer *timer);
+                  void *scratch, cudaStream_t stream, class KernelTimer *timer);
 void luSolveBatch(const float *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, float *x,
-                  cudaStream_t stream, class KernelTimer *timer);
+                  void *scratch, cudaStream_t stream, class KernelTimer *timer);
 // r = b - A x (FP64); writes the correction rhs into `correction` and the
 // mass-scaled residual norm and rhs norm per (batch, excitation) into norms[2].
 void residualBatch(const double *A, const double *b, const double *x, const double *mass, uint32_t N, uint32_t B,

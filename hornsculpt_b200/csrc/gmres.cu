@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256) updateKernel(const double *basis, const d
 
 // Workspace pieces, each 256-byte aligned, in carve order.
 struct GmresLayout {
-    size_t basis, hess, g, dots, rot, beta, estimate, tol, active, steps, z, z32, total;
+    size_t basis, hess, g, dots, rot, beta, estimate, tol, active, steps, z, z32, solve, total;
 };
 
 GmresLayout gmresLayout(uint32_t N, uint32_t S, uint32_t m) {
@@ -298,6 +298,7 @@ GmresLayout gmresLayout(uint32_t N, uint32_t S, uint32_t m) {
     l.steps = take(size_t(S) * 4);
     l.z = take(size_t(S) * N * 16);
     l.z32 = take(size_t(S) * N * 8);
+    l.solve = take(size_t(S) * N * 8);  // triangular-solve scratch
     l.total = at;
     return l;
 }
@@ -330,7 +331,7 @@ uint32_t gmresCycleBatch(const double *A, const float *LU32, const int *pivots, 
     const auto precondition = [&](const double *in) {  // z = M^{-1} in
         TimedScope scope(timer, "gmres_precondition", stream);
         roundToFloat(in, z32, reals, stream);
-        luSolveBatch(LU32, pivots, N, B, E, z32, stream, nullptr);
+        luSolveBatch(LU32, pivots, N, B, E, z32, w + l.solve, stream, nullptr);
         toDoubleKernel<<<unsigned((reals + 255) / 256), 256, 0, stream>>>(z32, z, reals);
     };
     precondition(r);

@@ -301,7 +301,7 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
 namespace {
 uint64_t perFrequencyBytes(uint64_t T, uint64_t N, uint32_t E, uint32_t O, bool mixed, uint32_t restart) {
     return assemblyWorkspaceBytes(uint32_t(T), uint32_t(N), E, 1, mixed) + 2 * N * N * 16 + 4 * E * N * 16 +
-           E * T * 16 + fieldPartialsBytes(uint32_t(T), E, O, 1) +
+           E * T * 16 + E * N * 16 + 8 * N + fieldPartialsBytes(uint32_t(T), E, O, 1) +
            (mixed ? gmresWorkspaceBytes(uint32_t(N), E, restart) + luPackBytes(uint32_t(N), 1) : 0) + 64;
 }
 }  // namespace
@@ -320,7 +320,7 @@ size_t Session::residentBytes() const {
                                   &dRowScale_, &dMass_, &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_,
                                   &dSingularTable_, &dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dA_,
                                   &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_, &dPivots_, &dKs_, &dFlux_, &dObservers_,
-                                  &dPartials_, &dField_, &dDegrees_, &dWork32_, &dGmres_, &dLuPack_})
+                                  &dPartials_, &dField_, &dDegrees_, &dWork32_, &dGmres_, &dLuPack_, &dSolveScratch_})
         bytes += b->bytes();
     return bytes;
 }
@@ -358,7 +358,8 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, ui
     dX_.ensure(B * E * N * 16);
     dCorr_.ensure(B * E * N * 16);
     dNorms_.ensure(2 * B * E * 8 + 2 * B * E * N * 8);
-    dPivots_.ensure(B * N * sizeof(int));
+    dPivots_.ensure(luWorkspaceBytes(uint32_t(N), B));
+    dSolveScratch_.ensure(B * E * N * 16);
     dInfo_.ensure(16);
     dKs_.ensure(B * 8);
     dFlux_.ensure(B * E * T * 16);
@@ -372,7 +373,7 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, ui
                                   &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_, &dRecords_, &dColumns_,
                                   &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
                                   &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_,
-                                  &dWork32_, &dGmres_, &dLuPack_})
+                                  &dWork32_, &dGmres_, &dLuPack_, &dSolveScratch_})
         bytes += b->bytes();
     peakBytes_ = std::max(peakBytes_, bytes);
 }
@@ -564,14 +565,15 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 TimedScope scope(&timer_, "round_fp32", s);
                 roundToFloat(dRhs_.as<double>(), work32, vectorReals, s);
             }
-            luSolveBatch(LU32, dPivots_.as<int>(), N, B, E, work32, s, &timer_);
+            luSolveBatch(LU32, dPivots_.as<int>(), N, B, E, work32, dSolveScratch_.as<void>(), s, &timer_);
             cuda(cudaMemsetAsync(dX_.as<void>(), 0, vectorReals * 8, s), "solution reset");
             TimedScope scope(&timer_, "add_correction", s);
             addCorrectionBatch(dX_.as<double>(), work32, vectorReals, s);
         } else {
             cuda(cudaMemcpyAsync(dX_.as<void>(), dRhs_.as<void>(), vectorReals * 8, cudaMemcpyDeviceToDevice, s),
                  "rhs copy");
-            luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), s, &timer_);
+            luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), dSolveScratch_.as<void>(), s,
+                         &timer_);
         }
         cuda(cudaStreamSynchronize(s), "CUDA multi-RHS solve");
         double triMs = msSince(triStart);
@@ -631,7 +633,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 for (size_t q = 0; q < cycle.size(); ++q)
                     krylov[q] += cycle[q];
             } else {
-                luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dCorr_.as<double>(), s, &timer_);
+                luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dCorr_.as<double>(),
+                             dSolveScratch_.as<void>(), s, &timer_);
                 TimedScope scope(&timer_, "add_correction", s);
                 addCorrectionBatch(dX_.as<double>(), dCorr_.as<double>(), vectorReals, s);
             }

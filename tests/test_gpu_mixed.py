@@ -102,3 +102,22 @@ def test_tall_panels_on_a_cluster():
         p, m = fp.excitations[0], fm.excitations[0]
         assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
         assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
+
+
+@pytest.mark.parametrize("make", [lambda: meshes.octahedral_sphere(5), lambda: meshes.revolved_sphere(h=0.004)],
+                         ids=["N4098", "N7899"])
+def test_panels_beyond_cluster_shared_memory(make):
+    """Panels taller than a full cluster's shared memory (FP64 above 8 x 384
+    rows at N = 4098, FP32 above 8 x 768 rows at N = 7899) keep their extra
+    rows in global memory. Both forms converge and agree within the mixed
+    tolerance, so both LU paths (FP64 one-level, FP32 two-level with the
+    tensor-core update) and the blocked triangular solves are exercised at
+    these sizes."""
+    mesh = make()
+    exc = [hs.BemExcitation("unit", [hs.FaceVelocity(1, 1.0)])]
+    with hs.CudaBemSolver(mesh) as solver:
+        plain = solver.solve(hs.BemRequest(frequencies=[700.0], excitations=exc))
+        mixed = solver.solve(hs.BemRequest(frequencies=[700.0], excitations=exc, numerics=MIXED))
+    p, m = plain.frequencies[0].excitations[0], mixed.frequencies[0].excitations[0]
+    assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
+    assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
