@@ -313,6 +313,71 @@ def run_c3(args):
         torch.cuda.empty_cache()
 
 
+C4_FREQUENCIES = [float(f) for f in __import__("numpy").geomspace(100.0, 12000.0, 64)]
+
+
+def run_c4(args):
+    """Batched sweeps on larger meshes: icospheres s4 / s5 (2562 / 10242 vertices),
+    64 log frequencies 100 Hz-12 kHz, one interaction plan per mesh (the raster's
+    planning frequency). The mixed form solves all 64 frequencies; the plain FP64
+    form solves every 8th of them (8 points, the comparison set). One JSON line per
+    mesh. The C2 horn (about 40k triangles) is not run: its pair records exceed the
+    dense form's device memory."""
+    import numpy as np
+    import torch
+
+    import hornsculpt_b200 as hs
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    exc = [hs.BemExcitation("uniform", [hs.FaceVelocity(1, 1.0)])]
+    plain_freqs = C4_FREQUENCIES[::8]
+    for name, make in (("icosphere-4 r=0.1 m", lambda: hs.meshes.icosphere(4)),
+                       ("icosphere-5 r=0.1 m", lambda: hs.meshes.icosphere(5))):
+        mesh = make()
+        v = mesh.vertices[mesh.triangles]
+        area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+        line = {"workload": "C4 batched sweep", "mesh": name, "N": mesh.vertex_count, "T": mesh.triangle_count,
+                "frequencies": {"mixed": len(C4_FREQUENCIES), "fp64": len(plain_freqs), "range_hz": [100.0, 12000.0]}}
+        results = {}
+        for form, freqs in (("fp64", plain_freqs), ("mixed", C4_FREQUENCIES)):
+            # one session per form: at s5 each form's workspace alone takes over half the device
+            torch.cuda.synchronize()
+            line.setdefault("device_free_gib_before", {})[form] = round(torch.cuda.mem_get_info()[0] / 2**30, 1)
+            with hs.CudaBemSolver(mesh) as solver:
+                solver.set_stream(stream.cuda_stream)
+
+                def request(fs):
+                    return hs.BemRequest(frequencies=fs, observers=OBSERVERS, excitations=exc,
+                                         medium=hs.AcousticMedium(DENSITY, SOUND_SPEED),
+                                         numerics=hs.BemNumerics(precision=form),
+                                         interaction_plan_frequencies=C4_FREQUENCIES)
+                solver.solve(request(freqs[-1:]))  # plan, workspace and warm-up
+                solver.set_profiling(True)
+                t0 = time.perf_counter()
+                res = solver.solve(request(freqs))
+                wall = time.perf_counter() - t0
+                prof = solver.profile()
+                solver.set_profiling(False)
+                span = prof.pop("solve_span", (0.0, 0))[0]
+                results[form] = res
+                line[form] = {"ms_per_frequency": span / len(freqs), "wall_ms_per_frequency": 1e3 * wall / len(freqs),
+                              "solves_per_s": 1e3 * len(freqs) / span if span else None,
+                              "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])[:8]},
+                              "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations)}
+        err = 0.0
+        mixed_at = {f.frequency: f for f in results["mixed"].frequencies}
+        for fp in results["fp64"].frequencies:
+            a = fp.excitations[0].boundary.surface_pressure
+            b = mixed_at[fp.frequency].excitations[0].boundary.surface_pressure
+            err = max(err, float(np.sqrt((area * np.abs(b - a) ** 2).sum() / (area * np.abs(a) ** 2).sum())))
+        line["max_rel_err_surface_mixed_vs_fp64"] = err
+        line["mixed_over_fp64"] = line["fp64"]["ms_per_frequency"] / line["mixed"]["ms_per_frequency"]
+        print(json.dumps(line), flush=True)
+        del results
+        torch.cuda.empty_cache()
+
+
 def serve_stream(hs, count: int, seed: int, rate: float, distinct: int = 0):
     """Seeded Poisson stream of horn requests: throat U[15, 50] mm, mouth
     U[80, 300] mm, length U[100, 600] mm, flare exponent U[1, 4], triangle
@@ -452,8 +517,9 @@ def main():
                     help="solve only n sweep frequencies (small profiling cases)")
     ap.add_argument("--first-frequency", type=int, default=0,
                     help="index of the first sweep frequency solved (small profiling cases)")
-    ap.add_argument("--workload", default="c1", choices=["c1", "c3", "serve"],
+    ap.add_argument("--workload", default="c1", choices=["c1", "c3", "c4", "serve"],
                     help="c1: the headline sweep; c3: mixed dense sizes N = 2k-8k (one line per mesh); "
+                         "c4: 64-frequency sweeps on icospheres s4/s5; "
                          "serve: the serving loop on a seeded Poisson horn stream")
     ap.add_argument("--c3-cases", default="", help="c3: comma-separated case indices (default: all)")
     ap.add_argument("--c3-forms", default="fp64,mixed", help="c3: forms to run (the error needs both)")
@@ -470,6 +536,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "c3":
         return run_c3(args)
+    if args.workload == "c4":
+        return run_c4(args)
     if args.workload == "serve":
         return run_serve(args)
 

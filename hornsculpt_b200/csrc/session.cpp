@@ -330,7 +330,13 @@ uint32_t Session::chooseBatch(uint32_t F, uint32_t E, uint32_t O, bool mixed, ui
     const uint64_t perFrequency = perFrequencyBytes(T, N, E, O, mixed, restart);
     size_t free = 0, total = 0;
     cuda(cudaMemGetInfo(&free, &total), "CUDA memory query");
-    uint64_t budget = uint64_t(double(free) * .6);
+    // the batch workspace this session already holds is reused (or freed before it grows)
+    size_t held = 0;
+    for (const DeviceBuffer *b : {&dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_,
+                                  &dX_, &dCorr_, &dNorms_, &dPivots_, &dKs_, &dFlux_, &dPartials_, &dField_, &dDegrees_,
+                                  &dWork32_, &dGmres_, &dLuPack_, &dSolveScratch_})
+        held += b->bytes();
+    uint64_t budget = uint64_t(double(free + held) * .6);
     if (memoryBudget_)
         budget = std::min<uint64_t>(budget, memoryBudget_);
     if (perFrequency > budget)
