@@ -491,64 +491,86 @@ __global__ void __launch_bounds__(1024) panelClusterKernel(R *LU, uint32_t N, ui
         }
     }
     cluster.sync();
-    // interchange sequence (rank 0) and the final position of every row that moved
-    if (rank == 0 && threadIdx.x == 0) {
-        int arrRow[2 * kPanel], arrPos[2 * kPanel], whereRow[2 * kPanel], wherePos[2 * kPanel];
-        int na = 0, nw = 0;
-        const auto arrangementAt = [&](int pos) {
-            for (int q = 0; q < na; ++q)
-                if (arrPos[q] == pos)
-                    return arrRow[q];
-            return pos;
-        };
-        const auto whereOf = [&](int row) {
-            for (int q = 0; q < nw; ++q)
-                if (whereRow[q] == row)
-                    return wherePos[q];
+    // Interchange sequence and the final position of every row that moved, by warp 0 of
+    // rank 0: the (row, position) pairs of the moved rows live in lane registers, two per
+    // lane (at most 2 * jb), and each lookup is one ballot.
+    if (rank == 0 && warp == 0) {
+        int rowA = -1, posA = 0, rowB = -1, posB = 0;  // slots lane and lane + 32
+        int n = 0;
+        const auto whereOf = [&](int row) {  // current position of a row
+            const unsigned a = __ballot_sync(0xffffffffu, rowA == row), b = __ballot_sync(0xffffffffu, rowB == row);
+            if (a)
+                return __shfl_sync(0xffffffffu, posA, __ffs(a) - 1);
+            if (b)
+                return __shfl_sync(0xffffffffu, posB, __ffs(b) - 1);
             return row;
         };
-        const auto setArrangement = [&](int pos, int row) {
-            for (int q = 0; q < na; ++q)
-                if (arrPos[q] == pos) {
-                    arrRow[q] = row;
-                    return;
-                }
-            arrPos[na] = pos;
-            arrRow[na++] = row;
+        const auto rowAt = [&](int pos) {  // row currently at a position
+            const unsigned a = __ballot_sync(0xffffffffu, rowA >= 0 && posA == pos);
+            const unsigned b = __ballot_sync(0xffffffffu, rowB >= 0 && posB == pos);
+            if (a)
+                return __shfl_sync(0xffffffffu, rowA, __ffs(a) - 1);
+            if (b)
+                return __shfl_sync(0xffffffffu, rowB, __ffs(b) - 1);
+            return pos;
         };
         const auto setWhere = [&](int row, int pos) {
-            for (int q = 0; q < nw; ++q)
-                if (whereRow[q] == row) {
-                    wherePos[q] = pos;
-                    return;
+            const unsigned a = __ballot_sync(0xffffffffu, rowA == row), b = __ballot_sync(0xffffffffu, rowB == row);
+            if (a) {
+                if (lane == __ffs(a) - 1)
+                    posA = pos;
+            } else if (b) {
+                if (lane == __ffs(b) - 1)
+                    posB = pos;
+            } else {
+                if (n < 32 && lane == n) {
+                    rowA = row;
+                    posA = pos;
+                } else if (n >= 32 && lane == n - 32) {
+                    rowB = row;
+                    posB = pos;
                 }
-            whereRow[nw] = row;
-            wherePos[nw++] = pos;
+                ++n;
+            }
         };
         for (uint32_t j = 0; j < jb; ++j) {
-            const int r = sh.sel[j], pj = whereOf(r), rj = arrangementAt(int(j));
-            piv[k0 + j] = int(k0) + pj;
-            setArrangement(int(j), r);
-            setArrangement(pj, rj);
+            const int r = sh.sel[j], pj = whereOf(r), rj = rowAt(int(j));
+            if (lane == 0)
+                piv[k0 + j] = int(k0) + pj;
             setWhere(r, int(j));
             setWhere(rj, pj);
         }
-        int n = 0;
-        for (int q = 0; q < nw; ++q)
-            if (whereRow[q] != wherePos[q]) {
-                sh.mapRow[n] = whereRow[q];
-                sh.mapPos[n++] = wherePos[q];
-            }
-        sh.mapCount = n;
+        const unsigned a = __ballot_sync(0xffffffffu, rowA >= 0 && rowA != posA);
+        const unsigned b = __ballot_sync(0xffffffffu, rowB >= 0 && rowB != posB);
+        const unsigned below = (1u << lane) - 1u;
+        if (a >> lane & 1u) {
+            sh.mapRow[__popc(a & below)] = rowA;
+            sh.mapPos[__popc(a & below)] = posA;
+        }
+        if (b >> lane & 1u) {
+            sh.mapRow[__popc(a) + __popc(b & below)] = rowB;
+            sh.mapPos[__popc(a) + __popc(b & below)] = posB;
+        }
+        if (lane == 0)
+            sh.mapCount = __popc(a) + __popc(b);
     }
     cluster.sync();
-    const ClusterPanelShared<R> *root = cluster.map_shared_rank(&sh, 0);
-    const int moved = root->mapCount;
+    if (rank != 0) {  // a local copy of rank 0's map
+        const ClusterPanelShared<R> *root = cluster.map_shared_rank(&sh, 0);
+        for (uint32_t q = threadIdx.x; q < 2 * kPanel; q += blockDim.x) {
+            sh.mapRow[q] = root->mapRow[q];
+            sh.mapPos[q] = root->mapPos[q];
+        }
+        if (threadIdx.x == 0)
+            sh.mapCount = root->mapCount;
+    }
+    __syncthreads();
+    const int moved = sh.mapCount;
     const auto finalPosition = [&](uint32_t g) {
         uint32_t pos = g;
         for (int q = 0; q < moved; ++q)
-            if (root->mapRow[q] == int(g))
-                pos = uint32_t(root->mapPos[q]);
+            if (sh.mapRow[q] == int(g))
+                pos = uint32_t(sh.mapPos[q]);
         return pos;
     };
     // pivots kept in global memory move to their positions (< jb; those rows are in CTA 0's shared memory)
