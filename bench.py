@@ -313,6 +313,67 @@ def run_c3(args):
         torch.cuda.empty_cache()
 
 
+C2_FREQUENCIES = [float(f) for f in __import__("numpy").geomspace(200.0, 8000.0, 16)]
+
+
+def run_c2(args):
+    """The C2 horn: exponential horn r(x) = r_t exp(m x), r_t = 25 mm, r_m = 150 mm,
+    L = 300 mm, 3 mm wall, rear cap, throat disc driven at 1 m/s, isotropic
+    h = lambda(8 kHz)/6 = 7.15 mm with +-5 % tangential jitter (seed 0); 16 log
+    frequencies 200 Hz-8 kHz. The reference solves this configuration with its
+    FMM; here both dense forms run (one session each, one interaction plan for
+    the raster). One JSON line; the actual triangle count is in it."""
+    import numpy as np
+    import torch
+
+    import hornsculpt_b200 as hs
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    mesh = hs.meshes.exponential_horn()
+    v = mesh.vertices[mesh.triangles]
+    area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+    exc = [hs.BemExcitation("throat", [hs.FaceVelocity(hs.meshes.HORN_THROAT, 1.0)])]
+    obs = [(0.0, 0.0, 1.0), (0.5, 0.0, 0.8), (0.0, 0.0, -1.0)]
+    line = {"workload": "C2 horn sweep (dense forms)", "mesh": "exponential horn r_t 25 mm, r_m 150 mm, L 300 mm, "
+            "wall 3 mm, h 7.15 mm, seed 0", "N": mesh.vertex_count, "T": mesh.triangle_count,
+            "frequencies": len(C2_FREQUENCIES), "range_hz": [200.0, 8000.0]}
+    results = {}
+    for form in ("fp64", "mixed"):
+        with hs.CudaBemSolver(mesh) as solver:
+            solver.set_stream(stream.cuda_stream)
+
+            def request(fs):
+                return hs.BemRequest(frequencies=fs, observers=obs, excitations=exc,
+                                     medium=hs.AcousticMedium(DENSITY, SOUND_SPEED),
+                                     numerics=hs.BemNumerics(precision=form),
+                                     interaction_plan_frequencies=C2_FREQUENCIES)
+            t0 = time.perf_counter()
+            solver.solve(request(C2_FREQUENCIES[-1:]))  # plan, workspace and warm-up
+            first = time.perf_counter() - t0
+            solver.set_profiling(True)
+            t0 = time.perf_counter()
+            res = solver.solve(request(C2_FREQUENCIES))
+            wall = time.perf_counter() - t0
+            prof = solver.profile()
+            solver.set_profiling(False)
+            span = prof.pop("solve_span", (0.0, 0))[0]
+            results[form] = res
+            line[form] = {"ms_per_frequency": span / len(C2_FREQUENCIES),
+                          "wall_ms_per_frequency": 1e3 * wall / len(C2_FREQUENCIES),
+                          "solves_per_s": 1e3 * len(C2_FREQUENCIES) / span if span else None,
+                          "first_call_s_with_planning": round(first, 2),
+                          "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])[:8]},
+                          "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations)}
+    err = 0.0
+    for fp, fm in zip(results["fp64"].frequencies, results["mixed"].frequencies):
+        a, b = fp.excitations[0].boundary.surface_pressure, fm.excitations[0].boundary.surface_pressure
+        err = max(err, float(np.sqrt((area * np.abs(b - a) ** 2).sum() / (area * np.abs(a) ** 2).sum())))
+    line["max_rel_err_surface_mixed_vs_fp64"] = err
+    line["mixed_over_fp64"] = line["fp64"]["ms_per_frequency"] / line["mixed"]["ms_per_frequency"]
+    print(json.dumps(line), flush=True)
+
+
 C4_FREQUENCIES = [float(f) for f in __import__("numpy").geomspace(100.0, 12000.0, 64)]
 
 
@@ -321,8 +382,7 @@ def run_c4(args):
     64 log frequencies 100 Hz-12 kHz, one interaction plan per mesh (the raster's
     planning frequency). The mixed form solves all 64 frequencies; the plain FP64
     form solves every 8th of them (8 points, the comparison set). One JSON line per
-    mesh. The C2 horn (about 40k triangles) is not run: its pair records exceed the
-    dense form's device memory."""
+    mesh; the third mesh is the C2 horn (12.8k triangles), driven at its throat."""
     import numpy as np
     import torch
 
@@ -330,10 +390,16 @@ def run_c4(args):
 
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
-    exc = [hs.BemExcitation("uniform", [hs.FaceVelocity(1, 1.0)])]
+    sphere = [hs.BemExcitation("uniform", [hs.FaceVelocity(1, 1.0)])]
+    throat = [hs.BemExcitation("throat", [hs.FaceVelocity(hs.meshes.HORN_THROAT, 1.0)])]
     plain_freqs = C4_FREQUENCIES[::8]
-    for name, make in (("icosphere-4 r=0.1 m", lambda: hs.meshes.icosphere(4)),
-                       ("icosphere-5 r=0.1 m", lambda: hs.meshes.icosphere(5))):
+    only = [int(c) for c in args.c3_cases.split(",")] if args.c3_cases else None
+    cases = (("icosphere-4 r=0.1 m", lambda: hs.meshes.icosphere(4), sphere),
+             ("icosphere-5 r=0.1 m", lambda: hs.meshes.icosphere(5), sphere),
+             ("C2 horn h=7.15 mm seed 0", lambda: hs.meshes.exponential_horn(), throat))
+    for c, (name, make, exc) in enumerate(cases):
+        if only is not None and c not in only:
+            continue
         mesh = make()
         v = mesh.vertices[mesh.triangles]
         area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
@@ -517,11 +583,12 @@ def main():
                     help="solve only n sweep frequencies (small profiling cases)")
     ap.add_argument("--first-frequency", type=int, default=0,
                     help="index of the first sweep frequency solved (small profiling cases)")
-    ap.add_argument("--workload", default="c1", choices=["c1", "c3", "c4", "serve"],
-                    help="c1: the headline sweep; c3: mixed dense sizes N = 2k-8k (one line per mesh); "
+    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4", "serve"],
+                    help="c1: the headline sweep; c2: the 12.8k-triangle horn sweep (dense forms); "
+                         "c3: mixed dense sizes N = 2k-8k (one line per mesh); "
                          "c4: 64-frequency sweeps on icospheres s4/s5; "
                          "serve: the serving loop on a seeded Poisson horn stream")
-    ap.add_argument("--c3-cases", default="", help="c3: comma-separated case indices (default: all)")
+    ap.add_argument("--c3-cases", default="", help="c3/c4: comma-separated case indices (default: all)")
     ap.add_argument("--c3-forms", default="fp64,mixed", help="c3: forms to run (the error needs both)")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=1.0, help="mean arrivals per second")
@@ -538,6 +605,8 @@ def main():
         return run_c3(args)
     if args.workload == "c4":
         return run_c4(args)
+    if args.workload == "c2":
+        return run_c2(args)
     if args.workload == "serve":
         return run_serve(args)
 
