@@ -239,16 +239,19 @@ C3_FREQUENCIES = [250.0, 1000.0, 2500.0]
 
 
 def c3_cases(hs):
-    """Mixed dense sizes (N = 2k, 4k, 8k complex DOFs) of the sphere and horn
+    """Mixed dense sizes (N = 2k, 4k, 8k, 16k complex DOFs) of the sphere and horn
     families: icosphere / octahedral sphere refinements and the seeded horn
-    shell at the edge length that gives the size."""
+    shell at the edge length that gives the size. A fourth element limits the
+    forms run for that case."""
     m = hs.meshes
     return [("sphere", "icosphere-4 r=0.1 m", lambda: m.icosphere(4)),
             ("sphere", "octahedral-5 r=0.1 m", lambda: m.octahedral_sphere(5)),
             ("sphere", "ring-meshed sphere h=4 mm r=0.1 m seed 0", lambda: m.revolved_sphere(h=0.004)),
             ("horn", "exponential horn h=12.8 mm seed 0", lambda: m.exponential_horn(h=0.0128)),
             ("horn", "exponential horn h=9.0 mm seed 0", lambda: m.exponential_horn(h=0.0090)),
-            ("horn", "exponential horn h=6.4 mm seed 0", lambda: m.exponential_horn(h=0.0064))]
+            ("horn", "exponential horn h=6.4 mm seed 0", lambda: m.exponential_horn(h=0.0064)),
+            # N = 16k: mixed form only (the plain form's FP64 pair records alone would be 206 GB)
+            ("sphere", "octahedral-6 r=0.1 m", lambda: m.octahedral_sphere(6), ("mixed",))]
 
 
 def run_c3(args):
@@ -266,7 +269,9 @@ def run_c3(args):
     cases = c3_cases(hs)
     chosen = [int(c) for c in args.c3_cases.split(",")] if args.c3_cases else range(len(cases))
     forms = tuple(args.c3_forms.split(","))
-    for family, name, make in (cases[c] for c in chosen):
+    for case in (cases[c] for c in chosen):
+        family, name, make = case[:3]
+        case_forms = tuple(f for f in forms if len(case) < 4 or f in case[3])
         mesh = make()
         if family == "horn":
             exc = [hs.BemExcitation("throat", [hs.FaceVelocity(hs.meshes.HORN_THROAT, 1.0)])]
@@ -281,7 +286,7 @@ def run_c3(args):
         results = {}
         with hs.CudaBemSolver(mesh) as solver:
             solver.set_stream(stream.cuda_stream)
-            for form in forms:
+            for form in case_forms:
                 req = hs.BemRequest(frequencies=C3_FREQUENCIES, observers=obs, excitations=exc,
                                     medium=hs.AcousticMedium(DENSITY, SOUND_SPEED),
                                     numerics=hs.BemNumerics(precision=form))
@@ -585,7 +590,7 @@ def main():
                     help="index of the first sweep frequency solved (small profiling cases)")
     ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4", "serve"],
                     help="c1: the headline sweep; c2: the 12.8k-triangle horn sweep (dense forms); "
-                         "c3: mixed dense sizes N = 2k-8k (one line per mesh); "
+                         "c3: mixed dense sizes N = 2k-16k (one line per mesh); "
                          "c4: 64-frequency sweeps on icospheres s4/s5; "
                          "serve: the serving loop on a seeded Poisson horn stream")
     ap.add_argument("--c3-cases", default="", help="c3/c4: comma-separated case indices (default: all)")

@@ -44,6 +44,11 @@ void cudaCheck(cudaError_t e, const char *what) {
 
 __device__ __forceinline__ void flagError(int *error, int code) { atomicExch(error, code); }
 
+// First entry of bin `bin` of frequency f (exactly packed bins when offsets are given).
+__device__ __forceinline__ size_t binStart(const uint64_t *offsets, size_t capacity, int f, int bin) {
+    return offsets ? size_t(offsets[f * kBins + bin]) : (size_t(f) * kBins + bin) * capacity;
+}
+
 // Moment accumulators of one ordered pair: MG = sum g bt bs, MP = sum P bt bs,
 // MQ = sum Q bt bs (3x3 complex each) where, for delta = x_test - y_trial,
 // g = w exp(-ikr)/(4 pi r), P = g (1+ikr) (delta.n_trial)/r^2 (double layer),
@@ -105,7 +110,8 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
                                                           const double *__restrict__ ks,
                                                           const uint2 *__restrict__ bins,
                                                           const uint32_t *__restrict__ binCounts, size_t binCapacity,
-                                                          int bin, double *__restrict__ records, int *error) {
+                                                          const uint64_t *__restrict__ binOffsets, int bin,
+                                                          double *__restrict__ records, int *error) {
     constexpr int PPC = 192 / NP;
     constexpr int RO = ruleOffset<NP>();
     __shared__ double sS[192][18];
@@ -114,7 +120,7 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
     const int f = blockIdx.y;
     const double k = ks[f], invk = 1.0 / k;
     const uint32_t count = binCounts[f * kBins + bin];
-    const uint2 *list = bins + (size_t(f) * kBins + bin) * binCapacity;
+    const uint2 *list = bins + binStart(binOffsets, binCapacity, f, bin);
     double *rec = records + size_t(f) * T * T * kRecordDoubles;
     const int l = threadIdx.x / NP, x = threadIdx.x % NP;
     for (uint32_t base = blockIdx.x * PPC; base < count; base += gridDim.x * PPC) {
@@ -337,7 +343,8 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const MixedPanel *_
                                                              const double *__restrict__ ks,
                                                              const uint2 *__restrict__ bins,
                                                              const uint32_t *__restrict__ binCounts, size_t binCapacity,
-                                                             int bin, float *__restrict__ records, int *error) {
+                                                             const uint64_t *__restrict__ binOffsets, int bin,
+                                                             float *__restrict__ records, int *error) {
     constexpr int RO = ruleOffset<NP>();
     constexpr double kRound = 6755399441055744.0;  // 1.5 * 2^52: adding and subtracting rounds to an integer
     constexpr double kTwoPi = 6.283185307179586, kTwoPiLo = 2.4492935982947064e-16, kInvTwoPi = 0.15915494309189535;
@@ -347,7 +354,7 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const MixedPanel *_
     const double k = ks[f];
     const float kf = float(k), invkf = float(1.0 / k);
     const uint32_t count = binCounts[f * kBins + bin];
-    const uint2 *list = bins + (size_t(f) * kBins + bin) * binCapacity;
+    const uint2 *list = bins + binStart(binOffsets, binCapacity, f, bin);
     float *rec = records + size_t(f) * T * T * kRecordDoubles;
     const size_t planeStride = size_t(T) * T * 6;
     bool bad = false, nonFinite = false;
@@ -459,7 +466,8 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const MixedPanel *_
 // Sorts unordered regular pairs of each frequency into rule bins.
 __global__ void classifyPairsKernel(const uint8_t *__restrict__ pairCode, const Bounds *__restrict__ bounds,
                                     uint64_t pairs, const double *__restrict__ ks, double tol, uint32_t minDegree,
-                                    uint2 *bins, uint32_t *binCounts, size_t binCapacity, int *error) {
+                                    uint2 *bins, uint32_t *binCounts, size_t binCapacity,
+                                    const uint64_t *binOffsets, bool countOnly, int *error) {
     const int f = blockIdx.y;
     const double k = ks[f];
     const unsigned lane = threadIdx.x & 31;
@@ -501,9 +509,21 @@ __global__ void classifyPairsKernel(const uint8_t *__restrict__ pairCode, const 
             if (lane == unsigned(__ffs(mask) - 1))
                 start = atomicAdd(&binCounts[f * kBins + b], uint32_t(__popc(mask)));
             start = __shfl_sync(0xffffffffu, start, __ffs(mask) - 1);
-            if (bin == b)
-                bins[(size_t(f) * kBins + b) * binCapacity + start + __popc(mask & ((1u << lane) - 1))] = make_uint2(i, j);
+            if (bin == b && !countOnly)
+                bins[binStart(binOffsets, binCapacity, f, b) + start + __popc(mask & ((1u << lane) - 1))] =
+                    make_uint2(i, j);
         }
+    }
+}
+
+// Exclusive scan of the bin counts of all frequencies into bin offsets (a few
+// dozen entries, one thread); the counts start again from zero for the fill pass.
+__global__ void binOffsetsKernel(uint32_t *binCounts, uint64_t *binOffsets, uint32_t n) {
+    uint64_t sum = 0;
+    for (uint32_t q = 0; q < n; ++q) {
+        binOffsets[q] = sum;
+        sum += binCounts[q];
+        binCounts[q] = 0;
     }
 }
 
@@ -1218,7 +1238,7 @@ __global__ void __launch_bounds__(512, 2) gatherColumnKernel(const Rec *__restri
 template <class Rec>
 __global__ void gatherTrialKernel(const Rec *__restrict__ records, const uint32_t *__restrict__ incOffsets,
                                   const uint32_t *__restrict__ incPanel, const uint8_t *__restrict__ incLocal,
-                                  uint32_t T, uint32_t N, double *__restrict__ columns) {
+                                  uint32_t T, uint32_t N, Rec *__restrict__ columns) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t b = blockIdx.y;
     const int f = blockIdx.z;
@@ -1235,13 +1255,14 @@ __global__ void gatherTrialKernel(const Rec *__restrict__ records, const uint32_
         for (int c = 0; c < 6; ++c)
             acc[c] += double(r[c]);
     }
-    double *dst = columns + (size_t(f) * N + b) * 6 * T + 6 * size_t(t);
+    Rec *dst = columns + (size_t(f) * N + b) * 6 * T + 6 * size_t(t);
 #pragma unroll
     for (int c = 0; c < 6; ++c)
-        dst[c] = acc[c];
+        dst[c] = Rec(acc[c]);
 }
 
-__global__ void gatherTestKernel(const double *__restrict__ columns, const DPanel *__restrict__ panels,
+template <class Rec>
+__global__ void gatherTestKernel(const Rec *__restrict__ columns, const DPanel *__restrict__ panels,
                                  const uint32_t *__restrict__ incOffsets, const uint32_t *__restrict__ incPanel,
                                  const uint8_t *__restrict__ incLocal, const double *__restrict__ rowScale, uint32_t T,
                                  uint32_t N, double *__restrict__ A) {
@@ -1250,13 +1271,13 @@ __global__ void gatherTestKernel(const double *__restrict__ columns, const DPane
     const int f = blockIdx.z;
     if (a >= N)
         return;
-    const double *col = columns + (size_t(f) * N + b) * 6 * T;
+    const Rec *col = columns + (size_t(f) * N + b) * 6 * T;
     double re = 0, im = 0;
     for (uint32_t o = incOffsets[a]; o < incOffsets[a + 1]; ++o) {
         const uint32_t t = incPanel[o];
         const int la = incLocal[o];
-        re += col[6 * size_t(t) + 2 * la];
-        im += col[6 * size_t(t) + 2 * la + 1];
+        re += double(col[6 * size_t(t) + 2 * la]);
+        im += double(col[6 * size_t(t) + 2 * la + 1]);
         const DPanel &p = panels[t];
         if (p.nodes[0] == b || p.nodes[1] == b || p.nodes[2] == b)
             re += p.area * (a == b ? 2.0 : 1.0) / 24.0;
@@ -1354,12 +1375,12 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
     if (mixed) {
         const dim3 grid(unsigned(smCount() * 16), B);
         regularMixedKernel<NP><<<grid, 128, 0, stream>>>(g.mixedPanels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
-                                                         ws.binCapacity, bin, static_cast<float *>(ws.records),
-                                                         error);
+                                                         ws.binCapacity, ws.binOffsets, bin,
+                                                         static_cast<float *>(ws.records), error);
     } else {
         const dim3 grid(unsigned(smCount() * 6), B);
         regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
-                                                         bin, static_cast<double *>(ws.records), error);
+                                                         ws.binOffsets, bin, static_cast<double *>(ws.records), error);
     }
     cudaCheck(cudaGetLastError(), "regular pair assembly launch");
 }
@@ -1447,9 +1468,9 @@ size_t recordBytes(uint32_t T, bool mixed) { return size_t(T) * T * kRecordDoubl
 
 size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B, bool mixed) {
     const size_t pairs = size_t(T) * (T - 1) / 2;
-    const size_t columns = gatherUsesColumns(T) ? size_t(N) * 6 * T * 8 : 0;
-    return size_t(B) * (recordBytes(T, mixed) + columns + size_t(E) * 6 * T * 8 + kBins * pairs * sizeof(uint2) +
-                        kBins * sizeof(uint32_t));
+    const size_t columns = gatherUsesColumns(T) ? size_t(N) * 6 * T * (mixed ? 4 : 8) : 0;
+    const size_t bins = (T > kExactBinsT ? 1 : kBins) * pairs * sizeof(uint2);
+    return size_t(B) * (recordBytes(T, mixed) + columns + size_t(E) * 6 * T * 8 + bins + kBins * (4 + 8));
 }
 
 void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *gaussSingular, const double *flux,
@@ -1464,9 +1485,15 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
     if (pairs) {
         TimedScope scope(timer, "classify_pairs", stream);
         const unsigned blocks = unsigned(std::min<uint64_t>((pairs + 255) / 256, uint64_t(smCount()) * 16));
+        if (ws.binOffsets) {  // count, scan, fill
+            classifyPairsKernel<<<dim3(blocks, B), 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, g.nearTolerance,
+                                                                     g.minimumDegree, ws.bins, ws.binCounts,
+                                                                     ws.binCapacity, ws.binOffsets, true, error);
+            binOffsetsKernel<<<1, 1, 0, stream>>>(ws.binCounts, ws.binOffsets, B * kBins);
+        }
         classifyPairsKernel<<<dim3(blocks, B), 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, g.nearTolerance,
                                                                  g.minimumDegree, ws.bins, ws.binCounts,
-                                                                 ws.binCapacity, error);
+                                                                 ws.binCapacity, ws.binOffsets, false, error);
         cudaCheck(cudaGetLastError(), "pair classification launch");
     }
     launchRegular<6>(g, ks, B, ws, 0, error, stream, timer, mixed);
@@ -1533,16 +1560,23 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
             const dim3 grid((g.T + 127) / 128, g.N, B);
             if (mixed)
                 gatherTrialKernel<<<grid, 128, 0, stream>>>(recF, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N,
-                                                            ws.columns);
+                                                            static_cast<float *>(ws.columns));
             else
                 gatherTrialKernel<<<grid, 128, 0, stream>>>(recD, g.incOffsets, g.incPanel, g.incLocal, g.T, g.N,
-                                                            ws.columns);
+                                                            static_cast<double *>(ws.columns));
             cudaCheck(cudaGetLastError(), "trial gather launch");
         }
         {
             TimedScope scope(timer, "gather_test", stream);
-            gatherTestKernel<<<dim3((g.N + 127) / 128, g.N, B), 128, 0, stream>>>(
-                ws.columns, g.panels, g.incOffsets, g.incPanel, g.incLocal, g.rowScale, g.T, g.N, A);
+            const dim3 grid((g.N + 127) / 128, g.N, B);
+            if (mixed)
+                gatherTestKernel<<<grid, 128, 0, stream>>>(static_cast<const float *>(ws.columns), g.panels,
+                                                           g.incOffsets, g.incPanel, g.incLocal, g.rowScale, g.T, g.N,
+                                                           A);
+            else
+                gatherTestKernel<<<grid, 128, 0, stream>>>(static_cast<const double *>(ws.columns), g.panels,
+                                                           g.incOffsets, g.incPanel, g.incLocal, g.rowScale, g.T, g.N,
+                                                           A);
             cudaCheck(cudaGetLastError(), "test gather launch");
         }
     }

@@ -121,12 +121,18 @@ std::vector<float> buildSingularTable(unsigned order);
 // partials R[B][E][3T] complex, pair bins [B][4][pairs] and counters.
 struct AssemblyWorkspace {
     void *records;                  // double (plain form) or float (mixed form) records
-    double *columns;
+    void *columns;                  // trial-gathered columns, the record type
     double *panelRhs;
     uint2 *bins;
     uint32_t *binCounts;
     size_t binCapacity;
+    // Set for meshes above kExactBinsT triangles: the bins of each frequency are packed
+    // into `pairs` entries, bin b of frequency f starting at binOffsets[f * kBins + b]
+    // (B * kBins entries, filled by the assembly: count pass, scan, fill pass). Null:
+    // every bin has binCapacity entries.
+    uint64_t *binOffsets = nullptr;
 };
+constexpr uint32_t kExactBinsT = 10000;
 size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B, bool mixed);
 // Record bytes of one frequency; whether the gather needs the columns buffer
 // (meshes whose 3T column entries exceed the fused gather's shared memory).

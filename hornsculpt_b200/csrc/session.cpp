@@ -318,7 +318,7 @@ size_t Session::residentBytes() const {
     size_t bytes = 0;
     for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dMixedPanels_, &dIncOffsets_, &dIncPanel_, &dIncLocal_,
                                   &dRowScale_, &dMass_, &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_,
-                                  &dSingularTable_, &dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dA_,
+                                  &dSingularTable_, &dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dBinOffsets_, &dA_,
                                   &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_, &dPivots_, &dKs_, &dFlux_, &dObservers_,
                                   &dPartials_, &dField_, &dDegrees_, &dWork32_, &dGmres_, &dLuPack_, &dSolveScratch_})
         bytes += b->bytes();
@@ -332,11 +332,13 @@ uint32_t Session::chooseBatch(uint32_t F, uint32_t E, uint32_t O, bool mixed, ui
     cuda(cudaMemGetInfo(&free, &total), "CUDA memory query");
     // the batch workspace this session already holds is reused (or freed before it grows)
     size_t held = 0;
-    for (const DeviceBuffer *b : {&dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_,
+    for (const DeviceBuffer *b : {&dRecords_, &dColumns_, &dPanelRhs_, &dBins_, &dBinCounts_, &dBinOffsets_, &dA_, &dLU_, &dRhs_,
                                   &dX_, &dCorr_, &dNorms_, &dPivots_, &dKs_, &dFlux_, &dPartials_, &dField_, &dDegrees_,
                                   &dWork32_, &dGmres_, &dLuPack_, &dSolveScratch_})
         held += b->bytes();
     uint64_t budget = uint64_t(double(free + held) * .6);
+    if (perFrequency > budget)  // one frequency at a time may take up to 90 %
+        budget = uint64_t(double(free + held) * .9);
     if (memoryBudget_)
         budget = std::min<uint64_t>(budget, memoryBudget_);
     if (perFrequency > budget)
@@ -350,14 +352,16 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, ui
     const size_t pairs = T * (T - 1) / 2;
     dRecords_.ensure(std::max<size_t>(B * recordBytes(uint32_t(T), mixed), 16));
     if (gatherUsesColumns(uint32_t(T)))
-        dColumns_.ensure(B * N * 6 * T * 8);
+        dColumns_.ensure(B * N * 6 * T * (mixed ? 4 : 8));
     if (mixed) {
         dGmres_.ensure(gmresWorkspaceBytes(uint32_t(N), B * E, restart));
         dLuPack_.ensure(std::max<size_t>(luPackBytes(uint32_t(N), B), 16));
     }
     dPanelRhs_.ensure(B * E * 6 * T * 8);
-    dBins_.ensure(std::max<size_t>(B * kBins * pairs * sizeof(uint2), 16));
+    dBins_.ensure(std::max<size_t>(B * (T > kExactBinsT ? 1 : kBins) * pairs * sizeof(uint2), 16));
     dBinCounts_.ensure(B * kBins * sizeof(uint32_t));
+    if (T > kExactBinsT)
+        dBinOffsets_.ensure(B * kBins * sizeof(uint64_t));
     dA_.ensure(B * N * N * 16);
     dLU_.ensure(B * N * N * 16);
     dRhs_.ensure(B * E * N * 16);
@@ -377,7 +381,7 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, ui
     size_t bytes = 0;
     for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dMixedPanels_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_, &dMass_,
                                   &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_, &dRecords_, &dColumns_,
-                                  &dPanelRhs_, &dBins_, &dBinCounts_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
+                                  &dPanelRhs_, &dBins_, &dBinCounts_, &dBinOffsets_, &dA_, &dLU_, &dRhs_, &dX_, &dCorr_, &dNorms_,
                                   &dPivots_, &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_,
                                   &dWork32_, &dGmres_, &dLuPack_, &dSolveScratch_})
         bytes += b->bytes();
@@ -519,8 +523,9 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         }
         cuda(cudaMemcpyAsync(dKs_.as<void>(), ks.data(), B * 8, cudaMemcpyHostToDevice, s), "k upload");
         cuda(cudaMemcpyAsync(dFlux_.as<void>(), flux.data(), flux.size() * 16, cudaMemcpyHostToDevice, s), "flux upload");
-        AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
-                             dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
+        AssemblyWorkspace ws{dRecords_.as<void>(), dColumns_.as<void>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
+                             dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2,
+                             T > kExactBinsT ? dBinOffsets_.as<uint64_t>() : nullptr};
         const bool mixed = o.precision == HS_PRECISION_MIXED;
         assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws, dA_.as<double>(),
                       dRhs_.as<double>(), dError_.as<int>(), s, &timer_, mixed);
@@ -815,8 +820,9 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
                          o.near_relative_tolerance,
                          o.quadrature_order, o.singular_order, dSingularTable_.as<float4>(),
                          dMixedPanels_.as<MixedPanel>()};
-    AssemblyWorkspace ws{dRecords_.as<double>(), dColumns_.as<double>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
-                         dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2};
+    AssemblyWorkspace ws{dRecords_.as<void>(), dColumns_.as<void>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
+                         dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2,
+                         T > kExactBinsT ? dBinOffsets_.as<uint64_t>() : nullptr};
     assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), 1, 1, ws, dA_.as<double>(),
                   dRhs_.as<double>(), dError_.as<int>(), s, &timer_, o.precision == HS_PRECISION_MIXED);
     checkDeviceError("CUDA Galerkin assembly");

@@ -99,7 +99,7 @@ class Session {
     uint32_t touchingCount_ = 0, nearPairCount_ = 0, projectedPairCount_ = 0;
     uint64_t singularSamples_ = 0, nearSamples_ = 0;
     // workspaces (grow only)
-    DeviceBuffer dRecords_, dColumns_, dPanelRhs_, dBins_, dBinCounts_, dA_, dLU_, dRhs_, dX_, dCorr_, dNorms_,
+    DeviceBuffer dRecords_, dColumns_, dPanelRhs_, dBins_, dBinCounts_, dBinOffsets_, dA_, dLU_, dRhs_, dX_, dCorr_, dNorms_,
         dPivots_, dInfo_, dKs_, dFlux_, dObservers_, dPartials_, dField_, dDegrees_, dWork32_, dGmres_, dLuPack_, dSolveScratch_;
     size_t peakBytes_ = 0;
     size_t memoryBudget_ = 0;
