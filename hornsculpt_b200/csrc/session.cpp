@@ -159,6 +159,20 @@ Session::~Session() {
         cudaStreamSynchronize(own_);
         cudaStreamDestroy(own_);
     }
+    if (phaseReady_)
+        for (cudaEvent_t e : {phase_.batch, phase_.assembled, phase_.factored, phase_.solved, phase_.refine0,
+                              phase_.refine1})
+            cudaEventDestroy(e);
+}
+
+Session::PhaseEvents &Session::phaseEvents() {
+    if (!phaseReady_) {
+        for (cudaEvent_t *e : {&phase_.batch, &phase_.assembled, &phase_.factored, &phase_.solved, &phase_.refine0,
+                               &phase_.refine1})
+            cuda(cudaEventCreate(e), "phase event");
+        phaseReady_ = true;
+    }
+    return phase_;
 }
 
 void Session::setStream(cudaStream_t s) {
@@ -512,7 +526,10 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     for (uint32_t f0 = 0; f0 < F; f0 += Bmax) {
         checkCancel();
         const uint32_t B = std::min(Bmax, F - f0);
-        const auto batchStart = Clock::now();
+        // Phase times come from events on the session stream; the host waits for the
+        // device only where it needs data (residual norms, GMRES estimates, fields).
+        PhaseEvents &ev = phaseEvents();
+        cuda(cudaEventRecord(ev.batch, s), "phase event");
         std::vector<double> ks(B);
         std::vector<cplx> flux(size_t(B) * E * T);
         for (uint32_t b = 0; b < B; ++b) {
@@ -529,8 +546,9 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         const bool mixed = o.precision == HS_PRECISION_MIXED;
         assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws, dA_.as<double>(),
                       dRhs_.as<double>(), dError_.as<int>(), s, &timer_, mixed);
-        checkDeviceError("CUDA Galerkin assembly");
-        if (timer_.enabled()) {
+        cuda(cudaEventRecord(ev.assembled, s), "phase event");
+        // the assembly error word is checked with the first residual norms
+        const auto countWork = [&]() {
             std::vector<uint32_t> counts(size_t(B) * kBins);
             cuda(cudaMemcpy(counts.data(), dBinCounts_.as<void>(), counts.size() * 4, cudaMemcpyDeviceToHost),
                  "bin counts");
@@ -543,12 +561,10 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             work[5] += uint64_t(B) * singularSamples_;
             work[6] += uint64_t(B) * nearSamples_;
             work[7] += B;
-        }
-        const double assemblyMs = msSince(batchStart);
+        };
         checkCancel();
         // LU of every matrix of the batch (FP64, or an FP32 copy in the mixed
         // form), then the initial solves.
-        const auto factorStart = Clock::now();
         const size_t matrixReals = size_t(B) * N * N * 2, vectorReals = size_t(B) * E * N * 2;
         float *LU32 = dLU_.as<float>(), *work32 = dWork32_.as<float>();
         if (mixed) {
@@ -562,15 +578,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                  "factorization copy");
             luFactorBatch(dLU_.as<double>(), N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_);
         }
-        int info = 0;
-        cuda(cudaMemcpyAsync(&info, dInfo_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, s), "LU info");
-        cuda(cudaStreamSynchronize(s), "CUDA pivoted LU");
-        if (info < 0)
-            throw NumericError("CUDA Burton-Miller factorization: a tensor-core trailing update did not complete.");
-        if (info)
-            throw NumericError("CUDA Burton-Miller factorization failed at pivot " + std::to_string(info));
-        const double factorMs = msSince(factorStart);
-        const auto triStart = Clock::now();
+        cuda(cudaEventRecord(ev.factored, s), "phase event");
+        // the LU status is checked with the first residual norms
         if (mixed) {
             {
                 TimedScope scope(&timer_, "round_fp32", s);
@@ -586,8 +595,9 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), dSolveScratch_.as<void>(), s,
                          &timer_);
         }
-        cuda(cudaStreamSynchronize(s), "CUDA multi-RHS solve");
-        double triMs = msSince(triStart);
+        cuda(cudaEventRecord(ev.solved, s), "phase event");
+        double assemblyMs = 0, factorMs = 0, triMs = 0;
+        bool refining = false;  // a refinement solve between ev.refine0 and ev.refine1 awaits its time
         // FP64 refinement (cuda_solver.cu:1519-1581), per frequency. The mixed
         // form refines against the FP64 residual to min(tolerance, 1e-10).
         const double target = mixed ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
@@ -603,6 +613,29 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             cuda(cudaMemcpyAsync(norms.data(), dNorms_.as<void>(), norms.size() * 8, cudaMemcpyDeviceToHost, s),
                  "residual norms");
             cuda(cudaStreamSynchronize(s), "CUDA FP64 physical residual");
+            if (refining) {
+                float ms = 0;
+                cuda(cudaEventElapsedTime(&ms, ev.refine0, ev.refine1), "phase time");
+                triMs += ms;
+                refining = false;
+            } else {  // first pass: assembly and factorisation status, phase times
+                checkDeviceError("CUDA Galerkin assembly");
+                int info = 0;
+                cuda(cudaMemcpy(&info, dInfo_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost), "LU info");
+                if (info < 0)
+                    throw NumericError("CUDA Burton-Miller factorization: a tensor-core trailing update did not complete.");
+                if (info)
+                    throw NumericError("CUDA Burton-Miller factorization failed at pivot " + std::to_string(info));
+                float a = 0, b = 0, c = 0;
+                cuda(cudaEventElapsedTime(&a, ev.batch, ev.assembled), "phase time");
+                cuda(cudaEventElapsedTime(&b, ev.assembled, ev.factored), "phase time");
+                cuda(cudaEventElapsedTime(&c, ev.factored, ev.solved), "phase time");
+                assemblyMs = a;
+                factorMs = b;
+                triMs = c;
+                if (timer_.enabled())
+                    countWork();
+            }
             bool any = false;
             for (uint32_t b = 0; b < B; ++b) {
                 double largest = 0;
@@ -631,7 +664,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             }
             if (!any)
                 break;
-            const auto t0 = Clock::now();
+            cuda(cudaEventRecord(ev.refine0, s), "phase event");
             if (mixed) {
                 // GMRES-IR: one FP64 GMRES cycle on A d = r per system, preconditioned
                 // by the FP32 LU, reducing each system's preconditioned residual far
@@ -649,8 +682,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 TimedScope scope(&timer_, "add_correction", s);
                 addCorrectionBatch(dX_.as<double>(), dCorr_.as<double>(), vectorReals, s);
             }
-            cuda(cudaStreamSynchronize(s), "CUDA refinement solve");
-            triMs += msSince(t0);
+            cuda(cudaEventRecord(ev.refine1, s), "phase event");
+            refining = true;
         }
         const double residualMs = msSince(residualStart);
         // Observer fields with the degree-comparison loop (cuda_solver.cu:1717-1799).

@@ -78,6 +78,13 @@ class Session {
     void ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, uint32_t restart);
     uint32_t chooseBatch(uint32_t F, uint32_t E, uint32_t O, bool mixed, uint32_t restart) const;
     void checkDeviceError(const char *where);
+    // Events at the phase boundaries of a frequency batch (created on first use).
+    struct PhaseEvents {
+        cudaEvent_t batch{}, assembled{}, factored{}, solved{}, refine0{}, refine1{};
+    };
+    PhaseEvents &phaseEvents();
+    PhaseEvents phase_{};
+    bool phaseReady_ = false;
     cudaStream_t stream() const { return external_ ? external_ : own_; }
 
     MeshInput mesh_;
