@@ -693,7 +693,7 @@ __global__ void __launch_bounds__(128) singularKernel(const DPanel *__restrict__
 // FP64 help; it is reduced to [-pi, pi] for the hardware sin/cos (absolute
 // error about 4e-7). Moments accumulate in canonical order and are permuted
 // back to local order once per job.
-__global__ void __launch_bounds__(128) singularMixedKernel(const DPanel *__restrict__ panels, uint32_t T,
+__global__ void __launch_bounds__(128, 6) singularMixedKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                            const TouchingJob *__restrict__ jobs, uint32_t jobCount,
                                                            const double *__restrict__ ks,
                                                            const float4 *__restrict__ table, uint32_t order,
@@ -932,7 +932,7 @@ __device__ __forceinline__ void plainValues(double dx, double dy, double dz, dou
 // shared memory by the 27 lanes that own a (kind, i, j) moment. Pairs with
 // projected patches go to nearKernel.
 template <bool Mixed>
-__global__ void __launch_bounds__(64) nearWarpKernel(const DPanel *__restrict__ panels, uint32_t T,
+__global__ void __launch_bounds__(64, Mixed ? 10 : 1) nearWarpKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                       const NearPairJob *__restrict__ jobs, uint32_t jobCount,
                                                       const Patch *__restrict__ patches, const double *__restrict__ ks,
                                                       std::conditional_t<Mixed, float, double> *__restrict__ records,
