@@ -121,3 +121,20 @@ def test_panels_beyond_cluster_shared_memory(make):
     p, m = plain.frequencies[0].excitations[0], mixed.frequencies[0].excitations[0]
     assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
     assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
+
+
+def test_exactly_packed_bins_above_ten_thousand_triangles():
+    """Above 10k triangles the regular pairs are binned exactly (count pass,
+    on-device scan, fill pass) and the mixed form's trial-gathered columns are
+    FP32. At T = 10090 both forms run that path and agree within the mixed
+    tolerance; the plain form's residual meets its reference budget."""
+    mesh = meshes.revolved_sphere(h=0.005)
+    assert mesh.triangle_count > 10000
+    exc = [hs.BemExcitation("unit", [hs.FaceVelocity(1, 1.0)])]
+    with hs.CudaBemSolver(mesh) as solver:
+        plain = solver.solve(hs.BemRequest(frequencies=[900.0], excitations=exc))
+    with hs.CudaBemSolver(mesh) as solver:
+        mixed = solver.solve(hs.BemRequest(frequencies=[900.0], excitations=exc, numerics=MIXED))
+    p, m = plain.frequencies[0].excitations[0], mixed.frequencies[0].excitations[0]
+    assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
+    assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
