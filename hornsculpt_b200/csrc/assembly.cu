@@ -1162,6 +1162,27 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
 // plane reads), then each row's sum over its incident panels plus the half
 // mass, written as a contiguous column. Same summation order as
 // gatherTrialKernel followed by gatherTestKernel.
+// Three complex values of a record plane entry as three vector loads (entries
+// are 6 values: 24 B in FP32, 48 B in FP64, so 8- and 16-byte aligned).
+__device__ __forceinline__ void load6(const float *r, float (&v)[6]) {
+    const float2 *q = reinterpret_cast<const float2 *>(r);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float2 x = q[c];
+        v[2 * c] = x.x;
+        v[2 * c + 1] = x.y;
+    }
+}
+__device__ __forceinline__ void load6(const double *r, double (&v)[6]) {
+    const double2 *q = reinterpret_cast<const double2 *>(r);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const double2 x = q[c];
+        v[2 * c] = x.x;
+        v[2 * c + 1] = x.y;
+    }
+}
+
 template <class Rec>
 __global__ void __launch_bounds__(512, 2) gatherColumnKernel(const Rec *__restrict__ records,
                                                           const uint32_t *__restrict__ incOffsets,
@@ -1182,12 +1203,8 @@ __global__ void __launch_bounds__(512, 2) gatherColumnKernel(const Rec *__restri
             Rec v[4][6];
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (o + u < o1) {
-                    const Rec *r = rec + recordOffset(T, size_t(incPanel[o + u]) * T + t, incLocal[o + u]);
-#pragma unroll
-                    for (int c = 0; c < 6; ++c)
-                        v[u][c] = r[c];
-                }
+                if (o + u < o1)
+                    load6(rec + recordOffset(T, size_t(incPanel[o + u]) * T + t, incLocal[o + u]), v[u]);
 #pragma unroll
             for (int u = 0; u < 4; ++u)
                 if (o + u < o1)
