@@ -1267,10 +1267,11 @@ __global__ void gatherTrialKernel(const Rec *__restrict__ records, const uint32_
         const uint32_t s = incPanel[o];
         const int lb = incLocal[o];
         // column lb of the (trial s, test t) block: 3 contiguous complex values
-        const Rec *r = rec + recordOffset(T, size_t(s) * T + t, lb);
+        Rec v[6];
+        load6(rec + recordOffset(T, size_t(s) * T + t, lb), v);
 #pragma unroll
         for (int c = 0; c < 6; ++c)
-            acc[c] += double(r[c]);
+            acc[c] += double(v[c]);
     }
     Rec *dst = columns + (size_t(f) * N + b) * 6 * T + 6 * size_t(t);
 #pragma unroll
@@ -1325,7 +1326,8 @@ __global__ void __launch_bounds__(256) rhsPanelKernel(const Rec *__restrict__ re
             const double qr = q[2 * s], qi = q[2 * s + 1];
             if (qr == 0 && qi == 0)
                 continue;
-            const Rec *r = rec + recordOffset(T, size_t(s) * T + t, 9);
+            Rec r[6];
+            load6(rec + recordOffset(T, size_t(s) * T + t, 9), r);
 #pragma unroll
             for (int la = 0; la < 3; ++la) {
                 const double rr = r[2 * la], ri = r[2 * la + 1];
