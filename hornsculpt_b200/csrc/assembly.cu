@@ -463,18 +463,19 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const MixedPanel *_
         flagError(error, kErrNonFinite);
 }
 
-// Sorts unordered regular pairs of each frequency into rule bins.
+// Sorts unordered regular pairs of each frequency into rule bins. A thread
+// decodes its pair, reads the pair code and both panels' bounds once, then
+// classifies it at every frequency of the batch; appends are warp-aggregated.
 __global__ void classifyPairsKernel(const uint8_t *__restrict__ pairCode, const Bounds *__restrict__ bounds,
-                                    uint64_t pairs, const double *__restrict__ ks, double tol, uint32_t minDegree,
-                                    uint2 *bins, uint32_t *binCounts, size_t binCapacity,
+                                    uint64_t pairs, const double *__restrict__ ks, uint32_t B, double tol,
+                                    uint32_t minDegree, uint2 *bins, uint32_t *binCounts, size_t binCapacity,
                                     const uint64_t *binOffsets, bool countOnly, int *error) {
-    const int f = blockIdx.y;
-    const double k = ks[f];
     const unsigned lane = threadIdx.x & 31;
     for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < pairs; base += uint64_t(gridDim.x) * blockDim.x) {
         const uint64_t u = base + threadIdx.x;
-        int bin = -1;
         uint32_t i = 0, j = 0;
+        uint8_t code = kPairTouching;  // no bin
+        Bounds bi{}, bj{};
         if (u < pairs) {
             uint64_t hi = uint64_t((1.0 + sqrt(1.0 + 8.0 * double(u))) * 0.5);
             while (hi * (hi - 1) / 2 > u)
@@ -483,13 +484,20 @@ __global__ void classifyPairsKernel(const uint8_t *__restrict__ pairCode, const 
                 ++hi;
             i = uint32_t(u - hi * (hi - 1) / 2);
             j = uint32_t(hi);
-            const uint8_t code = pairCode[u];
+            code = pairCode[u];
+            if (code == kPairRegular) {
+                bi = bounds[i];
+                bj = bounds[j];
+            }
+        }
+        for (uint32_t f = 0; f < B; ++f) {
+            int bin = -1;
             if (code == kPairWhole8)
                 bin = 2;
             else if (code == kPairWhole14)
                 bin = 3;
             else if (code == kPairRegular) {
-                const unsigned d = qualifiedDegree(bounds[i], bounds[j], k, tol, minDegree);
+                const unsigned d = qualifiedDegree(bi, bj, ks[f], tol, minDegree);
                 if (d == 4)
                     bin = 0;
                 else if (d == 6)
@@ -499,19 +507,19 @@ __global__ void classifyPairsKernel(const uint8_t *__restrict__ pairCode, const 
                 else
                     flagError(error, kErrEscapedPlan);
             }
-        }
 #pragma unroll
-        for (int b = 0; b < kBins; ++b) {
-            const unsigned mask = __ballot_sync(0xffffffffu, bin == b);
-            if (!mask)
-                continue;
-            uint32_t start = 0;
-            if (lane == unsigned(__ffs(mask) - 1))
-                start = atomicAdd(&binCounts[f * kBins + b], uint32_t(__popc(mask)));
-            start = __shfl_sync(0xffffffffu, start, __ffs(mask) - 1);
-            if (bin == b && !countOnly)
-                bins[binStart(binOffsets, binCapacity, f, b) + start + __popc(mask & ((1u << lane) - 1))] =
-                    make_uint2(i, j);
+            for (int b = 0; b < kBins; ++b) {
+                const unsigned mask = __ballot_sync(0xffffffffu, bin == b);
+                if (!mask)
+                    continue;
+                uint32_t start = 0;
+                if (lane == unsigned(__ffs(mask) - 1))
+                    start = atomicAdd(&binCounts[f * kBins + b], uint32_t(__popc(mask)));
+                start = __shfl_sync(0xffffffffu, start, __ffs(mask) - 1);
+                if (bin == b && !countOnly)
+                    bins[binStart(binOffsets, binCapacity, int(f), b) + start + __popc(mask & ((1u << lane) - 1))] =
+                        make_uint2(i, j);
+            }
         }
     }
 }
@@ -1505,14 +1513,14 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         TimedScope scope(timer, "classify_pairs", stream);
         const unsigned blocks = unsigned(std::min<uint64_t>((pairs + 255) / 256, uint64_t(smCount()) * 16));
         if (ws.binOffsets) {  // count, scan, fill
-            classifyPairsKernel<<<dim3(blocks, B), 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, g.nearTolerance,
-                                                                     g.minimumDegree, ws.bins, ws.binCounts,
-                                                                     ws.binCapacity, ws.binOffsets, true, error);
+            classifyPairsKernel<<<blocks, 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, B, g.nearTolerance,
+                                                            g.minimumDegree, ws.bins, ws.binCounts, ws.binCapacity,
+                                                            ws.binOffsets, true, error);
             binOffsetsKernel<<<1, 1, 0, stream>>>(ws.binCounts, ws.binOffsets, B * kBins);
         }
-        classifyPairsKernel<<<dim3(blocks, B), 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, g.nearTolerance,
-                                                                 g.minimumDegree, ws.bins, ws.binCounts,
-                                                                 ws.binCapacity, ws.binOffsets, false, error);
+        classifyPairsKernel<<<blocks, 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, B, g.nearTolerance,
+                                                        g.minimumDegree, ws.bins, ws.binCounts, ws.binCapacity,
+                                                        ws.binOffsets, false, error);
         cudaCheck(cudaGetLastError(), "pair classification launch");
     }
     launchRegular<6>(g, ks, B, ws, 0, error, stream, timer, mixed);
