@@ -463,28 +463,44 @@ __global__ void __launch_bounds__(128, 4) regularMixedKernel(const MixedPanel *_
         flagError(error, kErrNonFinite);
 }
 
-// Sorts unordered regular pairs of each frequency into rule bins. A thread
-// decodes its pair, reads the pair code and both panels' bounds once, then
-// classifies it at every frequency of the batch; appends are warp-aggregated.
+// Number of 8 x 4 pair tiles before block q of trial panels j = 4q .. 4q + 3
+// (block q holds q / 2 + 1 tiles of 8 test panels i = 8p .. 8p + 7, i < j).
+__host__ __device__ inline uint64_t tilesBefore(uint64_t q) {
+    const uint64_t m = q / 2;
+    return q % 2 ? (m + 1) * (m + 1) : m * (m + 1);
+}
+
+// Sorts unordered regular pairs of each frequency into rule bins. Pairs are
+// enumerated in tiles of 8 test x 4 trial panels, one tile per warp, so a
+// warp's pairs (kept in lane order by the warp-aggregated appends) write both
+// orientations of their records in runs of whole sectors: 8 consecutive slots
+// per trial panel forward, 4 per test panel in reverse. A thread decodes its
+// pair, reads the pair code and both panels' bounds once, then classifies it
+// at every frequency of the batch.
 __global__ void classifyPairsKernel(const uint8_t *__restrict__ pairCode, const Bounds *__restrict__ bounds,
-                                    uint64_t pairs, const double *__restrict__ ks, uint32_t B, double tol,
+                                    uint32_t T, const double *__restrict__ ks, uint32_t B, double tol,
                                     uint32_t minDegree, uint2 *bins, uint32_t *binCounts, size_t binCapacity,
                                     const uint64_t *binOffsets, bool countOnly, int *error) {
     const unsigned lane = threadIdx.x & 31;
-    for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < pairs; base += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t u = base + threadIdx.x;
+    const uint64_t threads = 32 * tilesBefore((uint64_t(T) + 3) / 4);
+    for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < threads; base += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t tile = (base + threadIdx.x) / 32;  // the same for the whole warp
         uint32_t i = 0, j = 0;
         uint8_t code = kPairTouching;  // no bin
         Bounds bi{}, bj{};
-        if (u < pairs) {
-            uint64_t hi = uint64_t((1.0 + sqrt(1.0 + 8.0 * double(u))) * 0.5);
-            while (hi * (hi - 1) / 2 > u)
-                --hi;
-            while ((hi + 1) * hi / 2 <= u)
-                ++hi;
-            i = uint32_t(u - hi * (hi - 1) / 2);
-            j = uint32_t(hi);
-            code = pairCode[u];
+        if (tile < threads / 32) {
+            uint64_t m = uint64_t((sqrt(4.0 * double(tile) + 1.0) - 1.0) * 0.5);
+            while (m * (m + 1) > tile)
+                --m;
+            while ((m + 1) * (m + 2) <= tile)
+                ++m;
+            const uint64_t q = tile >= (m + 1) * (m + 1) ? 2 * m + 1 : 2 * m;
+            const uint64_t p = tile - tilesBefore(q);
+            i = uint32_t(8 * p + (lane & 7));
+            j = uint32_t(4 * q + (lane >> 3));
+        }
+        if (j < T && i < j) {
+            code = pairCode[uint64_t(j) * (j - 1) / 2 + i];
             if (code == kPairRegular) {
                 bi = bounds[i];
                 bj = bounds[j];
@@ -1513,12 +1529,12 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         TimedScope scope(timer, "classify_pairs", stream);
         const unsigned blocks = unsigned(std::min<uint64_t>((pairs + 255) / 256, uint64_t(smCount()) * 16));
         if (ws.binOffsets) {  // count, scan, fill
-            classifyPairsKernel<<<blocks, 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, B, g.nearTolerance,
+            classifyPairsKernel<<<blocks, 256, 0, stream>>>(g.pairCode, g.bounds, g.T, ks, B, g.nearTolerance,
                                                             g.minimumDegree, ws.bins, ws.binCounts, ws.binCapacity,
                                                             ws.binOffsets, true, error);
             binOffsetsKernel<<<1, 1, 0, stream>>>(ws.binCounts, ws.binOffsets, B * kBins);
         }
-        classifyPairsKernel<<<blocks, 256, 0, stream>>>(g.pairCode, g.bounds, pairs, ks, B, g.nearTolerance,
+        classifyPairsKernel<<<blocks, 256, 0, stream>>>(g.pairCode, g.bounds, g.T, ks, B, g.nearTolerance,
                                                         g.minimumDegree, ws.bins, ws.binCounts, ws.binCapacity,
                                                         ws.binOffsets, false, error);
         cudaCheck(cudaGetLastError(), "pair classification launch");
