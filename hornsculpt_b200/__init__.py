@@ -6,7 +6,8 @@ kernels); this package is its Python host mirror plus synthetic meshes.
 from .bem import (AcousticMedium, BemBoundaryData, BemCancelled, BemError, BemExcitation, BemExcitationResult,
                   BemFrequencyResult, BemNumerics, BemRequest, BemResult, BemServer, BemUnsupported, CudaBemSolver,
                   CudaStorageOptions, FaceImpedance, FaceVelocity, FarFieldObservation, FastMultipoleSettings,
-                  ServeOptions, ServeTiming, StopToken, host_plan)
+                  FieldPointStatus, PressureFieldSample, PressureFieldSettings, ServeOptions, ServeTiming, StopToken,
+                  host_plan)
 from .meshes import (DRIVEN, WALL, SurfaceMesh, exponential_horn, icosphere, octahedral_sphere, revolved_sphere,
                      scalene_tetrahedron)
 
@@ -14,6 +15,7 @@ __all__ = [
     "AcousticMedium", "BemBoundaryData", "BemCancelled", "BemError", "BemExcitation", "BemExcitationResult",
     "BemFrequencyResult", "BemNumerics", "BemRequest", "BemResult", "BemServer", "BemUnsupported", "CudaBemSolver",
     "CudaStorageOptions", "FaceImpedance", "FaceVelocity", "FarFieldObservation", "FastMultipoleSettings",
+    "FieldPointStatus", "PressureFieldSample", "PressureFieldSettings",
     "ServeOptions", "ServeTiming", "StopToken", "host_plan", "DRIVEN", "WALL", "SurfaceMesh", "exponential_horn",
     "icosphere", "octahedral_sphere", "revolved_sphere", "scalene_tetrahedron",
 ]

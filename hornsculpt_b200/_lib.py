@@ -67,6 +67,11 @@ class hs_serve_timing(C.Structure):
                 ("footprint_bytes", C.c_size_t), ("batched_requests", C.c_uint32)]
 
 
+class hs_field_settings(C.Structure):
+    _fields_ = [("minimum_boundary_distance", C.c_double), ("relative_quadrature_tolerance", C.c_double),
+                ("maximum_quadrature_depth", C.c_uint32)]
+
+
 PROGRESS_FN = C.CFUNCTYPE(None, C.POINTER(hs_progress), C.c_void_p)
 _P = C.c_void_p
 _lib = None
@@ -119,6 +124,9 @@ def load():
                                                     C.c_uint32, C.c_int32, _P, C.c_double, C.c_double, C.c_uint32,
                                                     _P, _P]),
         "hs_bem_debug_assemble": (C.c_int, [_P, C.POINTER(hs_numerics), C.c_double, C.c_double, _P, _P, _P]),
+        "hs_field_settings_default": (C.c_int, [C.POINTER(hs_field_settings)]),
+        "hs_bem_pressure_field": (C.c_int, [_P, C.c_double, C.c_double, _P, _P, _P, C.c_size_t,
+                                            C.POINTER(hs_field_settings), _P, _P]),
         "hs_serve_options_default": (None, [C.POINTER(hs_serve_options)]),
         "hs_serve_create": (C.c_int, [C.POINTER(hs_serve_options), C.POINTER(_P)]),
         "hs_serve_submit": (C.c_int, [_P, _P, C.c_size_t, _P, _P, _P, C.c_size_t, C.POINTER(hs_request),

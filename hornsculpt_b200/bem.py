@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import enum
 import functools
 from typing import Callable, Optional, Sequence
 
@@ -149,6 +150,29 @@ class BemResult:
     acceleration: str = "dense"
 
 
+class FieldPointStatus(enum.IntEnum):
+    """Status of a pressure field sample (field_evaluation.hpp:8)."""
+    AIR = 0
+    BOUNDARY = 1
+    EXCLUDED = 2
+    QUADRATURE_NOT_CONVERGED = 3
+
+
+@dataclasses.dataclass
+class PressureFieldSettings:
+    """Sampling settings of evaluatePressureField (field_evaluation.hpp:14-20)."""
+    minimum_boundary_distance: float = 1e-4  # m; a sampling exclusion distance
+    relative_quadrature_tolerance: float = 1e-4
+    maximum_quadrature_depth: int = 8
+
+
+@dataclasses.dataclass
+class PressureFieldSample:
+    position: tuple
+    pressure: complex
+    status: FieldPointStatus
+
+
 class StopToken:
     """Cooperative cancellation flag polled by the solver between device batches."""
 
@@ -247,6 +271,30 @@ class CudaBemSolver:
         finally:
             self._lib.hs_result_free(out)
             del keep
+
+    def pressure_field(self, frequency: float, solution: BemExcitationResult, points,
+                       settings: PressureFieldSettings = PressureFieldSettings(),
+                       medium: AcousticMedium = AcousticMedium()) -> list:
+        """Pressure samples at world points from a solution's boundary traces:
+        HornSculpt's evaluatePressureField (field_evaluation.hpp:29-33) for the
+        exterior closed-surface form, on the GPU with this session's mesh. Points
+        within minimum_boundary_distance of the surface are BOUNDARY, points
+        inside the closed surface EXCLUDED, points whose adaptive quadrature does
+        not converge within the depth QUADRATURE_NOT_CONVERGED (pressure 0)."""
+        b = solution.boundary
+        trace = np.ascontiguousarray(np.asarray(b.pressure_trace, np.complex128)).view(np.float64)
+        deriv = np.ascontiguousarray(np.asarray(b.normal_derivative, np.complex128)).view(np.float64)
+        pts = np.ascontiguousarray(np.asarray(points, np.float64).reshape(-1, 3))
+        n = len(pts)
+        out = np.zeros(2 * max(n, 1))
+        status = np.zeros(max(n, 1), np.int32)
+        st = _lib.hs_field_settings(settings.minimum_boundary_distance, settings.relative_quadrature_tolerance,
+                                    settings.maximum_quadrature_depth)
+        _lib.check(self._lib.hs_bem_pressure_field(self._handle, frequency, medium.sound_speed, trace.ctypes.data,
+                                                   deriv.ctypes.data, pts.ctypes.data, n, C.byref(st),
+                                                   out.ctypes.data, status.ctypes.data))
+        return [PressureFieldSample(tuple(pts[i]), complex(out[2 * i], out[2 * i + 1]), FieldPointStatus(status[i]))
+                for i in range(n)]
 
     # -- marshalling --------------------------------------------------------
     def _c_request(self, r: BemRequest):

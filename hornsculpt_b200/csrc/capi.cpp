@@ -126,6 +126,25 @@ hs_status hs_bem_session_set_stream(hs_bem_session *s, void *stream) {
     });
 }
 
+hs_status hs_field_settings_default(hs_field_settings *out) {
+    if (!out)
+        return fail(HS_E_INVALID, "Settings pointer is null.");
+    *out = hs_field_settings{1e-4, 1e-4, 8};  // PressureFieldSettings defaults (field_evaluation.hpp:14-20)
+    return HS_OK;
+}
+
+hs_status hs_bem_pressure_field(hs_bem_session *s, double frequency, double sound_speed, const double *pressure_trace,
+                                const double *normal_derivative, const double *points, size_t point_count,
+                                const hs_field_settings *settings, double *pressure, int32_t *status) {
+    if (!s || !pressure_trace || !normal_derivative || !settings || (point_count && (!points || !pressure || !status)))
+        return fail(HS_E_INVALID, "Session, traces, settings, points and outputs must be non-null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->pressureField(frequency, sound_speed, pressure_trace, normal_derivative, points, point_count,
+                               *settings, pressure, status);
+    });
+}
+
 hs_status hs_bem_solve(hs_bem_session *s, const hs_request *request, const volatile int32_t *cancel,
                        hs_progress_fn progress, void *user, hs_result **out) {
     if (!s || !request || !out)

@@ -191,6 +191,12 @@ struct FieldRequest {
     double tolerance;
     uint32_t maximumDepth;
 };
+// Post-solve pressure samples at points (local coordinates, count x 3): for
+// each point a status (0 air, 1 boundary, 2 excluded, 3 quadrature not
+// converged) and, for air, the pressure from the P1 trace and DP0 flux.
+void samplePressureField(const DPanel *panels, uint32_t T, const double *trace, const double *flux,
+                         const double *points, uint32_t count, double k, double minDistance, double tolerance,
+                         uint32_t maxDepth, double *pressure, int32_t *status, cudaStream_t stream);
 void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double *pressure, const double *flux,
                         const uint32_t *batchDegree, double *partials, double *out, int *error,
                         cudaStream_t stream, class KernelTimer *timer);

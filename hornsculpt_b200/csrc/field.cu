@@ -237,17 +237,218 @@ void check(cudaError_t e, const char *what) {
         throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-}  // namespace
+constexpr int32_t kFieldAir = 0, kFieldBoundary = 1, kFieldExcluded = 2, kFieldNotConverged = 3;
 
-size_t fieldPartialsBytes(uint32_t T, uint32_t E, uint32_t O, uint32_t B) {
-    return size_t(B) * E * O * ((T + kTile - 1) / kTile) * 2 * sizeof(double);
+// ---------------------------------------------------------------------------
+// Post-solve pressure samples at arbitrary points (the exterior form of
+// evaluatePressureField, field_evaluation.cpp:330-463): a point within
+// minDistance of a panel is "boundary"; otherwise the summed solid angle of
+// the panels (field_evaluation.cpp:70-75) decides inside ("excluded") or air;
+// air points get p(x) = sum over panels of (D p - S q), each panel integrated
+// adaptively (field_evaluation.cpp:85-142): a patch is accepted when its phase
+// span k h sqrt(fraction) <= pi and the degree-4 and degree-8 rules agree to
+// tolerance times the fine magnitude, else it is quartered, up to maxDepth
+// (beyond it the point is "not converged"). One CTA per point, threads over
+// panels with an explicit depth-first patch stack in the reference's child
+// order; the per-thread sums are added in a fixed order.
+// ---------------------------------------------------------------------------
+constexpr int kFieldThreads = 256;
+constexpr int kFieldStack = 3 * 12 + 1;  // depth-first stack for maxDepth <= 12
+
+// closest-point distance from p to a panel (Ericson, Real-Time Collision
+// Detection, 5.1.5, as field_evaluation.cpp:44-69)
+__device__ double pointPanelDistance(V3 p, const DPanel &t) {
+    const V3 a = v3(t.v0[0], t.v0[1], t.v0[2]), ab = v3(t.e1[0], t.e1[1], t.e1[2]), ac = v3(t.e2[0], t.e2[1], t.e2[2]);
+    const V3 b = a + ab, c = a + ac;
+    const V3 ap = p - a;
+    const double d1 = dot(ab, ap), d2 = dot(ac, ap);
+    if (d1 <= 0 && d2 <= 0)
+        return sqrt(norm2(ap));
+    const V3 bp = p - b;
+    const double d3 = dot(ab, bp), d4 = dot(ac, bp);
+    if (d3 >= 0 && d4 <= d3)
+        return sqrt(norm2(bp));
+    const double vc = d1 * d4 - d3 * d2;
+    if (vc <= 0 && d1 >= 0 && d3 <= 0)
+        return sqrt(norm2(ap - ab * (d1 / (d1 - d3))));
+    const V3 cp = p - c;
+    const double d5 = dot(ab, cp), d6 = dot(ac, cp);
+    if (d6 >= 0 && d5 <= d6)
+        return sqrt(norm2(cp));
+    const double vb = d5 * d2 - d1 * d6;
+    if (vb <= 0 && d2 >= 0 && d6 <= 0)
+        return sqrt(norm2(ap - ac * (d2 / (d2 - d6))));
+    const double va = d3 * d6 - d5 * d4;
+    if (va <= 0 && d4 >= d3 && d5 >= d6) {
+        const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+        return sqrt(norm2(bp - (c - b) * w));
+    }
+    return fabs(dot(ap, v3(t.n[0], t.n[1], t.n[2])));
 }
 
-void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double *pressure, const double *flux,
-                        const uint32_t *batchDegree, double *partials, double *out, int *error, cudaStream_t stream,
-                        KernelTimer *timer) {
-    static bool uploaded = false;
-    if (!uploaded) {
+// solid angle of a panel seen from p (Van Oosterom and Strackee)
+__device__ double panelSolidAngle(V3 p, const DPanel &t) {
+    const V3 a = v3(t.v0[0], t.v0[1], t.v0[2]) - p;
+    const V3 b = a + v3(t.e1[0], t.e1[1], t.e1[2]), c = a + v3(t.e2[0], t.e2[1], t.e2[2]);
+    const double la = sqrt(norm2(a)), lb = sqrt(norm2(b)), lc = sqrt(norm2(c));
+    return 2 * atan2(dot(a, cross(b, c)), la * lb * lc + dot(a, b) * lc + dot(b, c) * la + dot(c, a) * lb);
+}
+
+struct SamplePatch {
+    double b[9];  // barycentrics of the patch corners in the panel
+    double fraction;
+    uint32_t depth;
+};
+
+// D p - S q over one patch with one rule, and the magnitude sum |D p| + |S q|
+__device__ void patchIntegral(const DPanel &t, const SamplePatch &patch, V3 x, double k, const double (&p)[6],
+                              double qr, double qi, int offset, int count, double &re, double &im, double &mag) {
+    re = im = mag = 0;
+    const V3 n = v3(t.n[0], t.n[1], t.n[2]);
+    for (int r = 0; r < count; ++r) {
+        const double *rule = cField + 4 * (offset + r);
+        double b[3];
+        for (int i = 0; i < 3; ++i)
+            b[i] = patch.b[i] * rule[0] + patch.b[3 + i] * rule[1] + patch.b[6 + i] * rule[2];
+        // y = v0 b0 + v1 b1 + v2 b2 with v1 = v0 + e1, v2 = v0 + e2
+        V3 y;
+        y.x = t.v0[0] * b[0] + (t.v0[0] + t.e1[0]) * b[1] + (t.v0[0] + t.e2[0]) * b[2];
+        y.y = t.v0[1] * b[0] + (t.v0[1] + t.e1[1]) * b[1] + (t.v0[1] + t.e2[1]) * b[2];
+        y.z = t.v0[2] * b[0] + (t.v0[2] + t.e1[2]) * b[1] + (t.v0[2] + t.e2[2]) * b[2];
+        const V3 d = x - y;
+        const double rr = sqrt(norm2(d));
+        double sn, cs;
+        sincos(k * rr, &sn, &cs);
+        const double gm = kInvFourPi / rr, gr = gm * cs, gi = -gm * sn;  // exp(-ikr) / (4 pi r)
+        const double bq = b[0] + b[1] + b[2];
+        const double sr = gr * qr * bq - gi * qi * bq, si = gr * qi * bq + gi * qr * bq;  // g (b . q)
+        const double pr = b[0] * p[0] + b[1] * p[2] + b[2] * p[4], pi = b[0] * p[1] + b[1] * p[3] + b[2] * p[5];
+        const double proj = dot(d, n) / rr;
+        // g (1/r + i k) proj (b . p)
+        const double hr = (gr / rr - gi * k) * proj, hi = (gi / rr + gr * k) * proj;
+        const double dr = hr * pr - hi * pi, di = hr * pi + hi * pr;
+        const double w = 2 * t.area * patch.fraction * rule[3];
+        re += w * (dr - sr);
+        im += w * (di - si);
+        mag += w * (sqrt(dr * dr + di * di) + sqrt(sr * sr + si * si));
+    }
+}
+
+__global__ void __launch_bounds__(kFieldThreads) pressureFieldKernel(const DPanel *__restrict__ panels, uint32_t T,
+                                                                     const double *__restrict__ trace,
+                                                                     const double *__restrict__ flux,
+                                                                     const double *__restrict__ points, double k,
+                                                                     double minDistance, double tolerance,
+                                                                     uint32_t maxDepth, double *__restrict__ out,
+                                                                     int32_t *__restrict__ status) {
+    __shared__ double sA[kFieldThreads], sB[kFieldThreads];
+    __shared__ int sFlag[kFieldThreads];
+    const uint32_t pt = blockIdx.x, tid = threadIdx.x;
+    const V3 x = v3(points[3 * pt], points[3 * pt + 1], points[3 * pt + 2]);
+    // classification: boundary distance and solid angle
+    int near = 0;
+    double angle = 0;
+    for (uint32_t t = tid; t < T; t += kFieldThreads) {
+        near |= pointPanelDistance(x, panels[t]) <= minDistance;
+        angle += panelSolidAngle(x, panels[t]);
+    }
+    sA[tid] = angle;
+    sFlag[tid] = near;
+    __syncthreads();
+    for (int s = kFieldThreads / 2; s > 0; s >>= 1) {
+        if (tid < unsigned(s)) {
+            sA[tid] += sA[tid + s];
+            sFlag[tid] |= sFlag[tid + s];
+        }
+        __syncthreads();
+    }
+    const bool boundary = sFlag[0] != 0;
+    const bool inside = fabs(sA[0]) > 2 * 3.14159265358979323846;
+    __syncthreads();
+    if (boundary || inside) {
+        if (tid == 0) {
+            status[pt] = boundary ? kFieldBoundary : kFieldExcluded;
+            out[2 * pt] = out[2 * pt + 1] = 0;
+        }
+        return;
+    }
+    // air: adaptive D p - S q per panel
+    double re = 0, im = 0;
+    int failed = 0;
+    SamplePatch stack[kFieldStack];
+    for (uint32_t t = tid; t < T && !failed; t += kFieldThreads) {
+        const DPanel &panel = panels[t];
+        double p[6];
+        for (int i = 0; i < 3; ++i) {
+            p[2 * i] = trace[2 * panel.nodes[i]];
+            p[2 * i + 1] = trace[2 * panel.nodes[i] + 1];
+        }
+        const double qr = flux[2 * t], qi = flux[2 * t + 1];
+        if (qr == 0 && qi == 0 && p[0] == 0 && p[1] == 0 && p[2] == 0 && p[3] == 0 && p[4] == 0 && p[5] == 0)
+            continue;
+        int top = 0;
+        stack[top++] = SamplePatch{{1, 0, 0, 0, 1, 0, 0, 0, 1}, 1.0, 0};
+        while (top > 0) {
+            const SamplePatch patch = stack[--top];
+            double cr, ci, cm, fr, fi, fm;
+            patchIntegral(panel, patch, x, k, p, qr, qi, 0, 6, cr, ci, cm);    // degree 4
+            patchIntegral(panel, patch, x, k, p, qr, qi, 18, 16, fr, fi, fm);  // degree 8
+            const double span = k * panel.maxEdge * sqrt(patch.fraction);
+            const double diff = sqrt((fr - cr) * (fr - cr) + (fi - ci) * (fi - ci));
+            if (span <= 3.14159265358979323846 && diff <= tolerance * fmax(fm, 1e-300)) {
+                re += fr;
+                im += fi;
+                continue;
+            }
+            if (patch.depth >= maxDepth) {
+                failed = 1;
+                break;
+            }
+            // children pushed in reverse so that the first is integrated first
+            double ab[3], bc[3], ca[3];
+            for (int i = 0; i < 3; ++i) {
+                ab[i] = (patch.b[i] + patch.b[3 + i]) * .5;
+                bc[i] = (patch.b[3 + i] + patch.b[6 + i]) * .5;
+                ca[i] = (patch.b[6 + i] + patch.b[i]) * .5;
+            }
+            const double *corners[4][3] = {{patch.b, ab, ca}, {ab, patch.b + 3, bc}, {ca, bc, patch.b + 6}, {ab, bc, ca}};
+            for (int c = 3; c >= 0; --c) {
+                SamplePatch child;
+                for (int v = 0; v < 3; ++v)
+                    for (int i = 0; i < 3; ++i)
+                        child.b[3 * v + i] = corners[c][v][i];
+                child.fraction = patch.fraction * .25;
+                child.depth = patch.depth + 1;
+                stack[top++] = child;
+            }
+        }
+    }
+    sA[tid] = re;
+    sB[tid] = im;
+    sFlag[tid] = failed;
+    __syncthreads();
+    for (int s = kFieldThreads / 2; s > 0; s >>= 1) {
+        if (tid < unsigned(s)) {
+            sA[tid] += sA[tid + s];
+            sB[tid] += sB[tid + s];
+            sFlag[tid] |= sFlag[tid + s];
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        const bool ok = !sFlag[0] && isfinite(sA[0]) && isfinite(sB[0]);
+        status[pt] = ok ? kFieldAir : kFieldNotConverged;
+        out[2 * pt] = ok ? sA[0] : 0;
+        out[2 * pt + 1] = ok ? sB[0] : 0;
+    }
+}
+
+}  // namespace
+
+// The field rules (degrees 4, 6, 8, 12, 14) in constant memory, once per process.
+void uploadFieldRules(cudaStream_t stream) {
+    static std::once_flag once;
+    std::call_once(once, [&]() {
         double table[kFieldPoints * 4];
         int o = 0;
         for (unsigned d : {4u, 6u, 8u, 12u, 14u})
@@ -261,8 +462,30 @@ void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double 
         check(cudaMemcpyToSymbolAsync(cField, table, sizeof(table), 0, cudaMemcpyHostToDevice, stream),
               "field rule upload");
         check(cudaStreamSynchronize(stream), "field rule upload");
-        uploaded = true;
-    }
+    });
+}
+
+void samplePressureField(const DPanel *panels, uint32_t T, const double *trace, const double *flux,
+                         const double *points, uint32_t count, double k, double minDistance, double tolerance,
+                         uint32_t maxDepth, double *pressure, int32_t *status, cudaStream_t stream) {
+    if (maxDepth > 12)
+        throw std::invalid_argument("Invalid pressure field settings.");
+    uploadFieldRules(stream);
+    if (!count)
+        return;
+    pressureFieldKernel<<<count, kFieldThreads, 0, stream>>>(panels, T, trace, flux, points, k, minDistance, tolerance,
+                                                           maxDepth, pressure, status);
+    check(cudaGetLastError(), "pressure field launch");
+}
+
+size_t fieldPartialsBytes(uint32_t T, uint32_t E, uint32_t O, uint32_t B) {
+    return size_t(B) * E * O * ((T + kTile - 1) / kTile) * 2 * sizeof(double);
+}
+
+void evaluateFieldBatch(const FieldRequest &req, const double *ks, const double *pressure, const double *flux,
+                        const uint32_t *batchDegree, double *partials, double *out, int *error, cudaStream_t stream,
+                        KernelTimer *timer) {
+    uploadFieldRules(stream);
     const uint32_t tiles = (req.T + kTile - 1) / kTile;
     const size_t outputs = size_t(req.B) * req.E * req.O;
     if (!outputs)

@@ -402,6 +402,55 @@ void Session::ensureWorkspace(uint32_t B, uint32_t E, uint32_t O, bool mixed, ui
     peakBytes_ = std::max(peakBytes_, bytes);
 }
 
+void Session::pressureField(double frequency, double soundSpeed, const double *trace, const double *normalDerivative,
+                            const double *points, size_t count, const hs_field_settings &st, double *pressure,
+                            int32_t *status) {
+    // checks and messages of evaluatePressureField (field_evaluation.cpp:334-356)
+    if (!std::isfinite(frequency) || frequency <= 0 || !std::isfinite(soundSpeed) || soundSpeed <= 0 ||
+        !std::isfinite(st.minimum_boundary_distance) || st.minimum_boundary_distance <= 0 ||
+        !std::isfinite(st.relative_quadrature_tolerance) || st.relative_quadrature_tolerance <= 0 ||
+        st.relative_quadrature_tolerance > .01 || st.maximum_quadrature_depth > 12)
+        throw InvalidArgument("Invalid pressure field settings.");
+    const size_t T = space_.panels.size(), N = space_.vertices.size();
+    for (size_t i = 0; i < 2 * N; ++i)
+        if (!std::isfinite(trace[i]))
+            throw InvalidArgument("Non-finite pressure trace.");
+    for (size_t i = 0; i < 2 * T; ++i)
+        if (!std::isfinite(normalDerivative[i]))
+            throw InvalidArgument("Non-finite derivative trace.");
+    if (count > 0x7fffffffu)
+        throw InvalidArgument("Too many pressure field points.");
+    std::vector<double> local(3 * count);
+    for (size_t i = 0; i < count; ++i) {
+        if (!std::isfinite(points[3 * i]) || !std::isfinite(points[3 * i + 1]) || !std::isfinite(points[3 * i + 2]))
+            throw InvalidArgument("Invalid pressure field point.");
+        local[3 * i] = points[3 * i] - origin_.x;  // session coordinates are centred on vertex 0
+        local[3 * i + 1] = points[3 * i + 1] - origin_.y;
+        local[3 * i + 2] = points[3 * i + 2] - origin_.z;
+    }
+    if (!count)
+        return;
+    const cudaStream_t s = stream();
+    dSamplePoints_.ensure(local.size() * 8);
+    dSampleTrace_.ensure(N * 16);
+    dSampleFlux_.ensure(T * 16);
+    dSampleOut_.ensure(count * 16);
+    dSampleStatus_.ensure(count * 4);
+    cuda(cudaMemcpyAsync(dSamplePoints_.as<void>(), local.data(), local.size() * 8, cudaMemcpyHostToDevice, s),
+         "field points upload");
+    cuda(cudaMemcpyAsync(dSampleTrace_.as<void>(), trace, N * 16, cudaMemcpyHostToDevice, s), "trace upload");
+    cuda(cudaMemcpyAsync(dSampleFlux_.as<void>(), normalDerivative, T * 16, cudaMemcpyHostToDevice, s),
+         "derivative upload");
+    const double k = 2 * M_PI * frequency / soundSpeed;
+    samplePressureField(dPanels_.as<DPanel>(), uint32_t(T), dSampleTrace_.as<double>(), dSampleFlux_.as<double>(),
+                        dSamplePoints_.as<double>(), uint32_t(count), k, st.minimum_boundary_distance,
+                        st.relative_quadrature_tolerance, st.maximum_quadrature_depth, dSampleOut_.as<double>(),
+                        dSampleStatus_.as<int32_t>(), s);
+    cuda(cudaMemcpyAsync(pressure, dSampleOut_.as<void>(), count * 16, cudaMemcpyDeviceToHost, s), "field download");
+    cuda(cudaMemcpyAsync(status, dSampleStatus_.as<void>(), count * 4, cudaMemcpyDeviceToHost, s), "field download");
+    cuda(cudaStreamSynchronize(s), "CUDA pressure field");
+}
+
 void Session::checkDeviceError(const char *where) {
     int code = 0;
     cuda(cudaMemcpyAsync(&code, dError_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, stream()), where);

@@ -65,6 +65,10 @@ class Session {
     // Device bytes a solve may hold beyond the resident geometry and plan
     // (0: 60 % of free memory); bounds the frequency batch.
     void setMemoryBudget(size_t bytes) { memoryBudget_ = bytes; }
+    // Pressure samples at world points from a solution's traces (hs_bem_pressure_field).
+    void pressureField(double frequency, double soundSpeed, const double *trace, const double *normalDerivative,
+                       const double *points, size_t count, const hs_field_settings &settings, double *pressure,
+                       int32_t *status);
     // Device bytes held now (geometry, plan and grown workspaces).
     size_t residentBytes() const;
     // regular pairs per bin (4), regular samples, touching samples, near samples, frequencies
@@ -95,6 +99,7 @@ class Session {
     KernelTimer timer_;
 
     // geometry (frequency independent)
+    DeviceBuffer dSamplePoints_, dSampleTrace_, dSampleFlux_, dSampleOut_, dSampleStatus_;
     DeviceBuffer dPanels_, dBounds_, dMixedPanels_, dIncOffsets_, dIncPanel_, dIncLocal_, dRowScale_, dMass_, dError_;
     // plan cache
     bool planValid_ = false;

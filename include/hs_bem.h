@@ -246,6 +246,31 @@ hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_co
                                         double far_reference_distance, double tolerance, uint32_t maximum_depth,
                                         void *cuda_stream, double *observer_pressure);
 
+/* Post-solve pressure samples at arbitrary points. Replaces
+ * hornsculpt::evaluatePressureField (field_evaluation.hpp:29-33,
+ * field_evaluation.cpp:330-463) for the exterior closed-surface form (no
+ * baffle, sub-domains, symmetry or axisymmetric contract): from a solution's
+ * P1 pressure trace (vertex_count complex, interleaved re/im) and DP0 outward
+ * normal derivative (triangle_count complex), at `point_count` world points
+ * (x, y, z), with the session's mesh. Per point a status (enum below) and, for
+ * air points, the pressure D p - S q with the reference's adaptive quadrature
+ * (degree 4 against degree 8 per patch, quartering to maximum_quadrature_depth).
+ * Host buffers; runs on the session's stream and returns when done. Invalid
+ * settings (minimum_boundary_distance <= 0, tolerance outside (0, 0.01],
+ * depth > 12, frequency or sound speed not positive), non-finite traces or
+ * points return HS_E_INVALID with the reference's messages. */
+enum { HS_FIELD_AIR = 0, HS_FIELD_BOUNDARY = 1, HS_FIELD_EXCLUDED = 2, HS_FIELD_NOT_CONVERGED = 3 };
+typedef struct hs_field_settings {
+    double minimum_boundary_distance;     /* m; default 1e-4 */
+    double relative_quadrature_tolerance; /* default 1e-4 */
+    uint32_t maximum_quadrature_depth;    /* default 8 */
+} hs_field_settings;
+hs_status hs_field_settings_default(hs_field_settings *out);
+hs_status hs_bem_pressure_field(hs_bem_session *session, double frequency, double sound_speed,
+                                const double *pressure_trace, const double *normal_derivative, const double *points,
+                                size_t point_count, const hs_field_settings *settings, double *pressure,
+                                int32_t *status);
+
 /* ---------------------------------------------------------------------------
  * Serving form (no reference counterpart; the reference solves one request per
  * CudaBemSolver::solve call): a persistent request loop on the current device.

@@ -83,6 +83,9 @@ def _load_ref():
         lib.ref_estimate_patch.argtypes = [_f64p, _f64p, _u32p, _u32p, _f64p, C.c_double, _f64p, _f64p]
         lib.ref_triangle_rule.argtypes = [C.c_uint, _P, C.POINTER(C.c_size_t)]
         lib.ref_gauss.argtypes = [C.c_uint, _f64p]
+        lib.ref_pressure_field.argtypes = [_f64p, C.c_size_t, _u32p, C.c_size_t, _f64p, _f64p, C.c_double,
+                                           C.c_double, _f64p, C.c_size_t, C.c_double, C.c_double, C.c_uint, _f64p,
+                                           np.ctypeslib.ndpointer(np.int32, flags="C")]
         _ref = lib
     return _ref
 
@@ -152,6 +155,24 @@ def reference_gauss(order: int) -> np.ndarray:
     out = np.zeros((order, 2))
     _check(lib, "ref", lib.ref_gauss(order, out.ravel()))
     return out
+
+
+def reference_pressure_field(mesh, frequency: float, sound_speed: float, pressure_trace, normal_derivative, points,
+                             minimum_boundary_distance: float = 1e-4, tolerance: float = 1e-4, depth: int = 8):
+    """HornSculpt's own evaluatePressureField (field_evaluation.cpp:330-463) on
+    the exterior mesh: (pressures complex [P], statuses int [P])."""
+    lib = _load_ref()
+    verts = np.ascontiguousarray(mesh.vertices, np.float64).ravel()
+    tris = np.ascontiguousarray(mesh.triangles, np.uint32).ravel()
+    trace = np.ascontiguousarray(np.asarray(pressure_trace, np.complex128)).view(np.float64)
+    deriv = np.ascontiguousarray(np.asarray(normal_derivative, np.complex128)).view(np.float64)
+    pts = np.ascontiguousarray(np.asarray(points, np.float64).reshape(-1, 3))
+    out = np.zeros(2 * len(pts))
+    status = np.zeros(len(pts), np.int32)
+    _check(lib, "ref", lib.ref_pressure_field(verts, mesh.vertex_count, tris, mesh.triangle_count, trace, deriv,
+                                              frequency, sound_speed, pts.ravel(), len(pts),
+                                              minimum_boundary_distance, tolerance, depth, out, status))
+    return out.view(np.complex128), status
 
 
 def estimate_patch(which: str, tri_a, tri_b, nodes_a, nodes_b, patch22, k):

@@ -1,9 +1,12 @@
 // Test infrastructure only: a C entry layer over HornSculpt's own CPU
-// galerkin code (space.cpp, pair_quadrature.cpp, interaction_plan.cpp),
-// compiled from the reference tree by oracle/Makefile into oracle/_ref/.
-// It exposes the reference's interaction plan and patch estimator with the
-// same flat layout as the restated oracle so tests can compare them exactly.
+// galerkin code (space.cpp, pair_quadrature.cpp, interaction_plan.cpp) and its
+// post-solve field evaluation (field_evaluation.cpp), compiled from the
+// reference tree by oracle/Makefile into oracle/_ref/. It exposes the
+// reference's interaction plan and patch estimator with the same flat layout
+// as the restated oracle so tests can compare them exactly, and
+// evaluatePressureField for the GPU point-sampling parity tests.
 #include "galerkin/interaction_plan.hpp"
+#include <hornsculpt/field_evaluation.hpp>
 #include "galerkin/pair_quadrature.hpp"
 #include "galerkin/space.hpp"
 
@@ -176,6 +179,50 @@ int ref_estimate_patch(const double *tri9a, const double *tri9b, const uint32_t 
         errors3[1] = e.innerError;
         errors3[2] = e.outerError;
         return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return 2;
+    }
+}
+
+// evaluatePressureField (field_evaluation.cpp:330-463) on an exterior closed
+// mesh (world coordinates, as given): P1 trace nv and DP0 derivative nt
+// complex (interleaved); per point the pressure and the FieldPointStatus.
+int ref_pressure_field(const double *verts, size_t nv, const uint32_t *tris, size_t nt, const double *trace,
+                       const double *derivative, double frequency, double soundSpeed, const double *points, size_t np,
+                       double minDistance, double tolerance, unsigned depth, double *out, int *status) {
+    try {
+        SurfaceMesh m;
+        for (size_t i = 0; i < nv; ++i)
+            m.vertices.push_back({verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]});
+        for (size_t i = 0; i < nt; ++i)
+            m.triangles.push_back({{tris[3 * i], tris[3 * i + 1], tris[3 * i + 2]}, 0, BoundaryCondition::wall});
+        BemRequest request;
+        request.medium.soundSpeed = soundSpeed;
+        BemBoundaryData boundary;
+        for (size_t i = 0; i < nv; ++i)
+            boundary.pressureTrace.emplace_back(trace[2 * i], trace[2 * i + 1]);
+        for (size_t i = 0; i < nt; ++i)
+            boundary.normalDerivative.emplace_back(derivative[2 * i], derivative[2 * i + 1]);
+        BemExcitationResult solution;
+        solution.setBoundary(std::move(boundary));
+        std::vector<Vec3> pts;
+        for (size_t i = 0; i < np; ++i)
+            pts.push_back({points[3 * i], points[3 * i + 1], points[3 * i + 2]});
+        PressureFieldSettings settings;
+        settings.minimumBoundaryDistance = minDistance;
+        settings.relativeQuadratureTolerance = tolerance;
+        settings.maximumQuadratureDepth = depth;
+        const auto samples = evaluatePressureField(m, request, frequency, solution, pts, settings);
+        for (size_t i = 0; i < np; ++i) {
+            out[2 * i] = samples[i].pressure.real();
+            out[2 * i + 1] = samples[i].pressure.imag();
+            status[i] = int(samples[i].status);
+        }
+        return 0;
+    } catch (const std::invalid_argument &e) {
+        lastError = e.what();
+        return 1;
     } catch (const std::exception &e) {
         lastError = e.what();
         return 2;

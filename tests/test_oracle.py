@@ -105,3 +105,30 @@ def test_patch_estimates_match_reference():
         mr, er = O.estimate_patch("ref", a, b, [0, 1, 2], [3, 4, 5], patch, 30.0)
         assert np.max(np.abs(mo - mr)) <= 1e-13 * np.max(np.abs(mr))
         assert np.allclose(eo, er, rtol=1e-9, atol=1e-18)
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="oracle/_ref not built (reference tree absent)")
+def test_reference_pressure_field_pulsating_sphere():
+    """HornSculpt's own evaluatePressureField (compiled into oracle/_ref), fed
+    the analytic pulsating-sphere traces on icosphere s3: points inside are
+    excluded, a point 0.1 um off the surface is boundary, air points (one
+    0.5 mm off the surface, which needs adaptive subdivision) agree with the
+    analytic field to the mesh's discretisation error."""
+    mesh = meshes.icosphere(3)
+    a, c, rho, f, v = 0.1, 343.0, 1.21, 500.0, 1.0
+    k = 2 * np.pi * f / c
+
+    def exact(r):
+        return rho * c * v * (1j * k * a / (1 + 1j * k * a)) * (a / r) * np.exp(-1j * k * (r - a))
+
+    trace = exact(np.linalg.norm(mesh.vertices, axis=1))
+    q = np.full(mesh.triangle_count, -1j * rho * 2 * np.pi * f * v)
+    pts = np.array([(0, 0, .3), (.2, .1, 0), (0, 0, 0), (.1000001, 0, 0), (0, 0, .1005)])
+    p, status = O.reference_pressure_field(mesh, f, c, trace, q, pts)
+    assert list(status) == [0, 0, 2, 1, 0]
+    for i in (0, 1, 4):
+        r = np.linalg.norm(pts[i])
+        assert abs(p[i] - exact(r)) <= 1e-2 * abs(exact(r))
+    assert p[2] == 0 and p[3] == 0
+    with pytest.raises(ValueError, match="Invalid pressure field settings"):
+        O.reference_pressure_field(mesh, f, c, trace, q, pts, tolerance=0.5)
