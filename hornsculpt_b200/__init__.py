@@ -8,6 +8,7 @@ from .bem import (AcousticMedium, BemBoundaryData, BemCancelled, BemError, BemEx
                   CudaStorageOptions, FaceImpedance, FaceVelocity, FarFieldObservation, FastMultipoleSettings,
                   FieldPointStatus, PressureFieldSample, PressureFieldSettings, ServeOptions, ServeTiming, StopToken,
                   host_plan)
+from .fixtures import read_fixture, write_fixture
 from .meshes import (DRIVEN, WALL, SurfaceMesh, exponential_horn, icosphere, octahedral_sphere, revolved_sphere,
                      scalene_tetrahedron)
 
@@ -17,5 +18,5 @@ __all__ = [
     "CudaStorageOptions", "FaceImpedance", "FaceVelocity", "FarFieldObservation", "FastMultipoleSettings",
     "FieldPointStatus", "PressureFieldSample", "PressureFieldSettings",
     "ServeOptions", "ServeTiming", "StopToken", "host_plan", "DRIVEN", "WALL", "SurfaceMesh", "exponential_horn",
-    "icosphere", "octahedral_sphere", "revolved_sphere", "scalene_tetrahedron",
+    "icosphere", "octahedral_sphere", "revolved_sphere", "scalene_tetrahedron", "read_fixture", "write_fixture",
 ]

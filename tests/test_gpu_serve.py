@@ -95,3 +95,17 @@ def test_bad_requests_fail_at_submit():
             server.wait(12345)
     with pytest.raises(ValueError, match="serving options"):
         hs.BemServer(hs.ServeOptions(workers=0))
+
+
+def test_reference_fixture_request_is_served():
+    """A request in the reference's fixture JSON (hornsculpt-solver-input-1) read back
+    and served gives the result of the request it was written from, bit for bit."""
+    import json
+    sphere = meshes.octahedral_sphere(3)
+    request = _request([500.0, 1200.0])
+    mesh2, request2, _ = hs.read_fixture(json.dumps(hs.write_fixture(sphere, request, "sphere")).encode())
+    request2.numerics = hs.BemNumerics(precision="mixed")
+    with hs.BemServer(hs.ServeOptions(workers=2, planning_frequency=PLAN_HZ)) as server:
+        direct = server.wait(server.submit(sphere, request))[0]
+        replayed = server.wait(server.submit(mesh2, request2))[0]
+    _same(direct, replayed)
