@@ -124,6 +124,12 @@ def load():
                                                     C.c_uint32, C.c_int32, _P, C.c_double, C.c_double, C.c_uint32,
                                                     _P, _P]),
         "hs_bem_debug_assemble": (C.c_int, [_P, C.POINTER(hs_numerics), C.c_double, C.c_double, _P, _P, _P]),
+        "hs_bem_debug_fmm_far": (C.c_int, [_P, C.POINTER(hs_numerics), C.c_double, C.c_double, _P, _P, _P, _P,
+                                           C.c_size_t, C.POINTER(C.c_size_t), _P, C.c_size_t,
+                                           C.POINTER(C.c_size_t)]),
+        "hs_bem_debug_fmm_selftest": (C.c_int, [C.POINTER(C.c_double)]),
+        "hs_bem_debug_fmm_tree": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, C.c_uint32, C.c_double, C.c_double, _P,
+                                            _P, C.c_size_t]),
         "hs_field_settings_default": (C.c_int, [C.POINTER(hs_field_settings)]),
         "hs_bem_pressure_field": (C.c_int, [_P, C.c_double, C.c_double, _P, _P, _P, C.c_size_t,
                                             C.POINTER(hs_field_settings), _P, _P]),

@@ -365,6 +365,77 @@ hs_status hs_bem_debug_assemble(hs_bem_session *s, const hs_numerics *numerics, 
     });
 }
 
+hs_status hs_bem_debug_fmm_far(hs_bem_session *s, const hs_numerics *numerics, double k, double tolerance,
+                               const double *pressure, double *far, uint32_t *near_row_start, uint32_t *near_cols,
+                               size_t near_capacity, size_t *near_count, uint32_t *level_info, size_t level_capacity,
+                               size_t *level_count) {
+    if (!s || !numerics || !pressure || !far)
+        return fail(HS_E_INVALID, "Debug fast-multipole pointers must be non-null.");
+    if (!std::isfinite(k) || k <= 0 || !std::isfinite(tolerance) || tolerance <= 0 || tolerance >= 1)
+        return fail(HS_E_INVALID, "Debug fast multipole needs k > 0 and 0 < tolerance < 1.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        std::vector<uint32_t> row, col;
+        std::vector<hsb::FmmLevelInfo> levels;
+        s->impl->debugFmmFar(*numerics, k, tolerance, pressure, far, row, col, levels);
+        if (near_count)
+            *near_count = col.size();
+        if (near_row_start)
+            std::copy(row.begin(), row.end(), near_row_start);
+        if (near_cols)
+            std::copy(col.begin(), col.begin() + std::min(col.size(), near_capacity), near_cols);
+        if (level_count)
+            *level_count = levels.size();
+        if (level_info)
+            for (size_t i = 0; i < std::min(levels.size(), level_capacity); ++i) {
+                level_info[4 * i] = levels[i].level;
+                level_info[4 * i + 1] = levels[i].order;
+                level_info[4 * i + 2] = levels[i].nodes;
+                level_info[4 * i + 3] = levels[i].m2lLinks;
+            }
+    });
+}
+
+hs_status hs_bem_debug_fmm_selftest(double *error) {
+    if (!error)
+        return fail(HS_E_INVALID, "Self-test error pointer must be non-null.");
+    return guarded([&]() { *error = hsb::fmmSelfTest(); });
+}
+
+hs_status hs_bem_debug_fmm_tree(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                size_t triangle_count, uint32_t leaf_capacity, double separation_ratio,
+                                double near_distance_ratio, size_t *sizes, uint32_t *links, size_t capacity) {
+    if (!vertices || !triangles || !sizes || !vertex_count || !triangle_count)
+        return fail(HS_E_INVALID, "Debug tree needs a mesh and a sizes array.");
+    return guarded([&]() {
+        std::vector<double> v(vertices, vertices + 3 * vertex_count);
+        for (size_t i = 0; i < vertex_count; ++i)
+            for (int d = 0; d < 3; ++d)
+                v[3 * i + d] = vertices[3 * i + d] - vertices[d];
+        hsb::FmmTreeSettings st;
+        st.leafCapacity = leaf_capacity;
+        st.separationRatio = separation_ratio;
+        st.nearDistanceRatio = near_distance_ratio;
+        const hsb::FmmTree tree = hsb::buildSupportTree(v.data(), uint32_t(vertex_count), triangles,
+                                                        uint32_t(triangle_count), st);
+        sizes[0] = tree.nodes.size();
+        sizes[1] = tree.levels.size();
+        sizes[2] = tree.ppNear.size();
+        sizes[3] = tree.ppFar.size();
+        sizes[4] = tree.pfNear.size();
+        sizes[5] = tree.pfFar.size();
+        size_t at = 0;
+        for (const auto *list : {&tree.ppNear, &tree.ppFar, &tree.pfNear, &tree.pfFar})
+            for (const auto &lk : *list) {
+                if (links && at < capacity) {
+                    links[2 * at] = lk.target;
+                    links[2 * at + 1] = lk.source;
+                }
+                ++at;
+            }
+    });
+}
+
 hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_count, const uint32_t *triangles,
                                         size_t triangle_count, const double *pressure_trace, const double *flux,
                                         const double *observers, size_t observer_count, double wavenumber,

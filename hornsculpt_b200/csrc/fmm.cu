@@ -1,0 +1,1223 @@
+// Far-field operator of the fast-multipole form: leaf emission (P2M),
+// rotation-coaxial-rotation translations (M2M, M2L, L2L) and leaf testing
+// (L2P) of the six expansion channels V (3) and W (3), FP64.
+//
+// Reference stages (support_fmm_operator.cu:1220-1296): P2M
+// emitSpherical (wideband_leaf.cu:64-150), LF transfers rotate -> axial ->
+// rotate (wideband_rotation.cu:19-99, wideband_axial.cu:10-90), L2P
+// testSpherical. Work layout here: one CTA per output node for every
+// translation (its links in a fixed order, so sums are deterministic), one
+// warp per quadrature point for expansion tables, the local expansion's
+// divergence formed once per leaf in coefficient space.
+#include "fmm.hpp"
+#include "fmm_math.cuh"
+#include "kernel_timer.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+
+namespace hsb {
+namespace {
+
+void fmmCheck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess)
+        throw CudaError(std::string("CUDA fast multipole ") + what + ": " + cudaGetErrorString(e));
+}
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    DevBuf(DevBuf &&o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    ~DevBuf() {
+        if (p)
+            cudaFree(p);
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+    void upload(const void *src, size_t n, cudaStream_t s) {
+        ensure(n);
+        if (n)
+            fmmCheck(cudaMemcpyAsync(p, src, n, cudaMemcpyHostToDevice, s), "upload");
+    }
+    void ensure(size_t n) {
+        if (n <= bytes)
+            return;
+        if (p)
+            fmmCheck(cudaFree(p), "free");
+        p = nullptr;
+        bytes = 0;
+        if (cudaMalloc(&p, n) != cudaSuccess) {
+            p = nullptr;
+            throw OutOfMemory("CUDA fast multipole workspace allocation failed.");
+        }
+        bytes = n;
+    }
+};
+template <class T> void uploadVec(DevBuf &b, const std::vector<T> &v, cudaStream_t s) {
+    b.upload(v.data(), v.size() * sizeof(T), s);
+}
+
+struct FmmPanel {
+    double v0[3], e1[3], e2[3], n[3], curl[9], area;
+    uint32_t nodes[3], pad;
+};
+// A panel touching a leaf's pressure supports: bit a of mask set when vertex
+// a belongs to the leaf; inc[a] the vertex-incidence index of (vertex, panel).
+struct FmmItem {
+    uint32_t panel, mask, inc[3];
+};
+// One translation input: source node, Wigner class, coaxial class, azimuth.
+struct TransLink {
+    uint32_t source, wclass, cclass, pad;
+    double phi;
+};
+
+constexpr int kRulePts = 6;
+__constant__ double cFmmRule[kRulePts * 4];  // b0, b1, b2, physical weight fraction (sum 1)
+constexpr int kWarps = 8;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmulConj(double2 a, double2 b) {  // conj(a) * b
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// Warp table of the regular solid harmonics at d: j_n(k|d|) (n <= P),
+// Theta_n^m(cos t) (triIndex) and exp(i m phi) (m <= P).
+struct PointTable {
+    double *j, *th;
+    double2 *eph;
+};
+// Doubles of one table, even so that every table starts 16-byte aligned.
+HS_HD size_t tableDoubles(int P) {
+    const size_t d = size_t(P + 1) + size_t(P + 1) * (P + 2) / 2 + 2 * size_t(P + 1);
+    return (d + 1) & ~size_t(1);
+}
+__device__ PointTable tableAt(double *base, int P) {
+    PointTable t;
+    t.eph = reinterpret_cast<double2 *>(base);
+    t.j = base + 2 * (P + 1);
+    t.th = t.j + (P + 1);
+    return t;
+}
+__device__ void fillTable(const PointTable &t, int P, double dx, double dy, double dz, double k, int lane) {
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    const double ct = r > 0 ? dz / r : 1.0;
+    const double st = sqrt(fmax(0.0, 1.0 - ct * ct));
+    const double ph = atan2(dy, dx);
+    if (lane == 0)
+        besselJ(P, k * r, t.j);
+    for (int m = lane; m <= P; m += 32) {
+        thetaColumn(m, P, ct, st, t.th);
+        double s, c;
+        sincos(m * ph, &s, &c);
+        t.eph[m] = make_double2(c, s);
+    }
+    __syncwarp();
+}
+// R_n^m = j_n Y_n^m from a table.
+__device__ __forceinline__ double2 solidR(const PointTable &t, int n, int m) {
+    const int am = m < 0 ? -m : m;
+    const double a = t.j[n] * t.th[triIndex(n, am)];
+    const double2 e = t.eph[am];
+    if (m >= 0)
+        return make_double2(a * e.x, a * e.y);
+    const double sg = (am & 1) ? -1.0 : 1.0;  // Theta_n^-m = (-1)^m Theta_n^m, exp(-i m phi)
+    return make_double2(sg * a * e.x, -sg * a * e.y);
+}
+__device__ __forceinline__ void decode(int k, int &n, int &m) {
+    n = int(sqrt(double(k)));
+    while (n * n > k)
+        --n;
+    while ((n + 1) * (n + 1) <= k)
+        ++n;
+    m = k - n * n - n;
+}
+
+// Quadrature point q of an item's panel: position and the six channel strengths.
+__device__ void pointStrengths(const FmmPanel &P, uint32_t mask, int q, const double2 *p, double *x, double2 (&s)[6]) {
+    const double b0 = cFmmRule[4 * q], b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
+    const double w = cFmmRule[4 * q + 3] * P.area;
+    for (int d = 0; d < 3; ++d)
+        x[d] = P.v0[d] + b1 * P.e1[d] + b2 * P.e2[d];
+    const double b[3] = {b0, b1, b2};
+    double2 phiP = make_double2(0, 0);  // sum_a phi_a p_a
+    double2 curl[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+    for (int a = 0; a < 3; ++a) {
+        if (!((mask >> a) & 1))
+            continue;
+        const double2 pa = p[P.nodes[a]];
+        phiP = cadd(phiP, make_double2(b[a] * pa.x, b[a] * pa.y));
+        for (int d = 0; d < 3; ++d)
+            curl[d] = cadd(curl[d], make_double2(P.curl[3 * a + d] * pa.x, P.curl[3 * a + d] * pa.y));
+    }
+    for (int d = 0; d < 3; ++d) {
+        s[d] = make_double2(w * P.n[d] * phiP.x, w * P.n[d] * phiP.y);
+        s[3 + d] = make_double2(w * curl[d].x, w * curl[d].y);
+    }
+}
+
+// P2M of the leaves of one level: M[c][n,m] = sum over points s_c conj(R_n^m(y - centre)).
+__global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ panels,
+                                                 const uint32_t *__restrict__ leaves, const uint32_t *__restrict__ itemStart,
+                                                 const FmmItem *__restrict__ items, const double *__restrict__ centers,
+                                                 const uint64_t *__restrict__ coefOffset, int p, double k,
+                                                 const double2 *__restrict__ pvec, double2 *M) {
+    extern __shared__ double smem[];
+    const int P = p;
+    const size_t td = tableDoubles(P);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *tables = smem;
+    double2 *str = reinterpret_cast<double2 *>(smem + kWarps * td);  // [warp][6]
+    const uint32_t leaf = leaves[blockIdx.x];
+    const double *c = centers + 3 * size_t(leaf);
+    const uint32_t i0 = itemStart[blockIdx.x], i1 = itemStart[blockIdx.x + 1];
+    const uint32_t points = (i1 - i0) * kRulePts;
+    const int nc = (P + 1) * (P + 1);
+    double2 *out = M + coefOffset[leaf];
+    const PointTable mine = tableAt(tables + warp * td, P);
+    for (int chunk = 0; chunk * 256 < nc; ++chunk) {
+        const int kk = chunk * 256 + threadIdx.x;
+        int n = 0, m = 0;
+        if (kk < nc)
+            decode(kk, n, m);
+        double2 acc[6];
+        for (int ch = 0; ch < 6; ++ch)
+            acc[ch] = make_double2(0, 0);
+        for (uint32_t base = 0; base < points; base += kWarps) {
+            const uint32_t idx = base + warp;
+            if (idx < points) {
+                const FmmItem it = items[i0 + idx / kRulePts];
+                double x[3];
+                double2 s[6];
+                pointStrengths(panels[it.panel], it.mask, idx % kRulePts, pvec, x, s);
+                fillTable(mine, P, x[0] - c[0], x[1] - c[1], x[2] - c[2], k, lane);
+                if (lane < 6)
+                    str[warp * 6 + lane] = s[lane];
+            }
+            __syncthreads();
+            if (kk < nc)
+                for (int w = 0; w < kWarps && base + w < points; ++w) {
+                    const PointTable t = tableAt(tables + w * td, P);
+                    const double2 R = solidR(t, n, m);
+                    for (int ch = 0; ch < 6; ++ch)
+                        acc[ch] = cadd(acc[ch], cmulConj(R, str[w * 6 + ch]));
+                }
+            __syncthreads();
+        }
+        if (kk < nc)
+            for (int ch = 0; ch < 6; ++ch)
+                out[size_t(ch) * nc + kk] = acc[ch];
+    }
+}
+
+// One translation per link into the CTA's output node, channels in chunks:
+// rotate the input to the link axis, coaxial translation, rotate back.
+__global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restrict__ outNodes,
+                                                       const uint32_t *__restrict__ linkStart,
+                                                       const TransLink *__restrict__ links, int pin, int pout, int chunkCh,
+                                                       const double2 *__restrict__ inCoef, double2 *outCoef,
+                                                       const uint64_t *__restrict__ coefOffset,
+                                                       const double *__restrict__ wigner,
+                                                       const uint64_t *__restrict__ wignerStart,
+                                                       const double2 *__restrict__ coax,
+                                                       const uint64_t *__restrict__ coaxStart, int zeroFirst) {
+    extern __shared__ double smem[];
+    const int nin = (pin + 1) * (pin + 1), nout = (pout + 1) * (pout + 1);
+    const int pmax = pin > pout ? pin : pout;
+    const int nmax = nin > nout ? nin : nout;
+    double2 *eph = reinterpret_cast<double2 *>(smem);
+    double2 *a = eph + (pmax + 1);
+    double2 *b = a + size_t(chunkCh) * nmax;
+    double2 *cbuf = b + size_t(chunkCh) * nmax;
+    const uint32_t node = outNodes[blockIdx.x];
+    double2 *out = outCoef + coefOffset[node];
+    if (zeroFirst)
+        for (int i = threadIdx.x; i < 6 * nout; i += blockDim.x)
+            out[i] = make_double2(0, 0);
+    __syncthreads();
+    for (uint32_t li = linkStart[blockIdx.x]; li < linkStart[blockIdx.x + 1]; ++li) {
+        const TransLink L = links[li];
+        const double2 *in = inCoef + coefOffset[L.source];
+        const double *dtab = wigner + wignerStart[L.wclass];
+        const double2 *ctab = coax + coaxStart[L.cclass];
+        for (int m = threadIdx.x; m <= pmax; m += blockDim.x) {
+            double s, c;
+            sincos(m * L.phi, &s, &c);
+            eph[m] = make_double2(c, s);
+        }
+        for (int c0 = 0; c0 < 6; c0 += chunkCh) {
+            const int cc = min(chunkCh, 6 - c0);
+            for (int i = threadIdx.x; i < cc * nin; i += blockDim.x)
+                a[i] = in[size_t(c0) * nin + i];
+            __syncthreads();
+            // forward rotation: b[n, m'] = sum_m a[n, m] exp(i m phi) d^n[m, m']
+            for (int i = threadIdx.x; i < cc * nin; i += blockDim.x) {
+                const int ch = i / nin, kk = i - ch * nin;
+                int n, mp;
+                decode(kk, n, mp);
+                const double *d = dtab + wignerOffset(n) + (mp + n);
+                const int w = 2 * n + 1;
+                double2 acc = make_double2(0, 0);
+                for (int m = -n; m <= n; ++m) {
+                    const double2 e = m >= 0 ? eph[m] : make_double2(eph[-m].x, -eph[-m].y);
+                    const double2 v = cmul(a[ch * nin + coefIndex(n, m)], e);
+                    const double dv = d[size_t(m + n) * w];
+                    acc.x += v.x * dv;
+                    acc.y += v.y * dv;
+                }
+                b[ch * nin + kk] = acc;
+            }
+            __syncthreads();
+            // coaxial translation per |m|: c[n', m] = sum_n C_|m|[n][n'] b[n, m]
+            for (int i = threadIdx.x; i < cc * nout; i += blockDim.x) {
+                const int ch = i / nout, kk = i - ch * nout;
+                int np, m;
+                decode(kk, np, m);
+                const int am = m < 0 ? -m : m;
+                double2 acc = make_double2(0, 0);
+                if (am <= pin) {
+                    size_t off = 0;
+                    for (int j = 0; j < am; ++j)
+                        off += size_t(pin + 1 - j) * (pout + 1 - j);
+                    const double2 *C = ctab + off;
+                    const int wo = pout + 1 - am;
+                    for (int n = am; n <= pin; ++n) {
+                        const double2 cv = C[size_t(n - am) * wo + (np - am)];
+                        const double2 v = b[ch * nin + coefIndex(n, m)];
+                        acc = cadd(acc, cmul(cv, v));
+                    }
+                }
+                cbuf[ch * nout + kk] = acc;
+            }
+            __syncthreads();
+            // back rotation: out[n, m1] += exp(-i m1 phi) sum_m d^n[m1, m] c[n, m]
+            for (int i = threadIdx.x; i < cc * nout; i += blockDim.x) {
+                const int ch = i / nout, kk = i - ch * nout;
+                int n, m1;
+                decode(kk, n, m1);
+                const int w = 2 * n + 1;
+                const double *d = dtab + wignerOffset(n) + size_t(m1 + n) * w;
+                double2 acc = make_double2(0, 0);
+                for (int m = -n; m <= n; ++m) {
+                    const double2 v = cbuf[ch * nout + coefIndex(n, m)];
+                    const double dv = d[m + n];
+                    acc.x += v.x * dv;
+                    acc.y += v.y * dv;
+                }
+                const double2 e = m1 >= 0 ? make_double2(eph[m1].x, -eph[m1].y) : eph[-m1];
+                const size_t o = size_t(c0 + ch) * nout + kk;
+                out[o] = cadd(out[o], cmul(acc, e));
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Coefficient-space derivatives of a regular expansion (k = 1 scaling):
+// dz R_n^m = A(n,m) R_{n-1}^m - A(n+1,m) R_{n+1}^m, d+ = dx + i dy and d- = dx - i dy
+// raise / lower m with the coefficients below.
+__device__ __forceinline__ double coefA(int n, int m) {
+    return n <= 0 ? 0.0 : sqrt(fmax(0.0, double(n * n - m * m) / ((2.0 * n - 1) * (2.0 * n + 1))));
+}
+__device__ __forceinline__ double coefBm(int n, int m) {
+    return n <= 0 ? 0.0 : sqrt(fmax(0.0, double((n - m - 1) * (n - m)) / ((2.0 * n - 1) * (2.0 * n + 1))));
+}
+__device__ __forceinline__ double coefBp(int n, int m) {
+    return n < 0 ? 0.0 : sqrt(fmax(0.0, double((n + m + 1) * (n + m + 2)) / ((2.0 * n + 1) * (2.0 * n + 3))));
+}
+__device__ __forceinline__ double coefCm(int n, int m) {
+    return n <= 0 ? 0.0 : sqrt(fmax(0.0, double((n + m - 1) * (n + m)) / ((2.0 * n - 1) * (2.0 * n + 1))));
+}
+__device__ __forceinline__ double coefCp(int n, int m) {
+    return n < 0 ? 0.0 : sqrt(fmax(0.0, double((n - m + 1) * (n - m + 2)) / ((2.0 * n + 1) * (2.0 * n + 3))));
+}
+__device__ __forceinline__ double2 coefAt(const double2 *L, int p, int n, int m) {
+    if (n < 0 || n > p || m < -n || m > n)
+        return make_double2(0, 0);
+    return L[coefIndex(n, m)];
+}
+
+// L2P of the leaves of one level: forms D = div V (degree p + 1) in shared
+// memory, then one warp per item evaluates V, W, D at its quadrature points
+// and writes the item's incidence contributions
+//   far[inc_a] = sum_q w phi_a (D + i k n.V) - (i / k) w curl_a . W.
+__global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ panels,
+                                                 const uint32_t *__restrict__ leaves, const uint32_t *__restrict__ itemStart,
+                                                 const FmmItem *__restrict__ items, const double *__restrict__ centers,
+                                                 const uint64_t *__restrict__ coefOffset, int p, double k,
+                                                 const double2 *__restrict__ Lcoef, double2 *far) {
+    extern __shared__ double smem[];
+    const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
+    const size_t td = tableDoubles(P);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2 *Ls = reinterpret_cast<double2 *>(smem);  // [6][nc]
+    double2 *Ld = Ls + 6 * nc;                        // [nd]
+    double *tables = reinterpret_cast<double *>(Ld + nd);
+    const uint32_t leaf = leaves[blockIdx.x];
+    const double2 *L = Lcoef + coefOffset[leaf];
+    for (int i = threadIdx.x; i < 6 * nc; i += blockDim.x)
+        Ls[i] = L[i];
+    __syncthreads();
+    // D = dx Vx + dy Vy + dz Vz = (d+ U- + d- U+) / 2 + dz Vz, U-+ = Vx -+ i Vy (times k)
+    for (int kk = threadIdx.x; kk < nd; kk += blockDim.x) {
+        int n, m;
+        decode(kk, n, m);
+        const double2 *Vx = Ls, *Vy = Ls + nc, *Vz = Ls + 2 * nc;
+        const auto U = [&](int nn, int mm, double sign) {  // Vx + sign i Vy
+            const double2 x = coefAt(Vx, p, nn, mm), y = coefAt(Vy, p, nn, mm);
+            return make_double2(x.x - sign * y.y, x.y + sign * y.x);
+        };
+        // dz: L_{n+1,m} A(n+1,m) - L_{n-1,m} A(n,m)
+        const double2 z1 = coefAt(Vz, p, n + 1, m), z0 = coefAt(Vz, p, n - 1, m);
+        const double a1 = coefA(n + 1, m), a0 = coefA(n, m);
+        double2 d = make_double2(z1.x * a1 - z0.x * a0, z1.y * a1 - z0.y * a0);
+        // d+ U-: U-_{n+1,m-1} Bm(n+1,m-1) + U-_{n-1,m-1} Bp(n-1,m-1)
+        const double2 u1 = U(n + 1, m - 1, -1), u0 = U(n - 1, m - 1, -1);
+        const double bm = coefBm(n + 1, m - 1), bp = coefBp(n - 1, m - 1);
+        d.x += 0.5 * (u1.x * bm + u0.x * bp);
+        d.y += 0.5 * (u1.y * bm + u0.y * bp);
+        // d- U+: -(U+_{n+1,m+1} Cm(n+1,m+1) + U+_{n-1,m+1} Cp(n-1,m+1))
+        const double2 v1 = U(n + 1, m + 1, 1), v0 = U(n - 1, m + 1, 1);
+        const double cm = coefCm(n + 1, m + 1), cp = coefCp(n - 1, m + 1);
+        d.x -= 0.5 * (v1.x * cm + v0.x * cp);
+        d.y -= 0.5 * (v1.y * cm + v0.y * cp);
+        Ld[kk] = make_double2(k * d.x, k * d.y);
+    }
+    __syncthreads();
+    const uint32_t i0 = itemStart[blockIdx.x], i1 = itemStart[blockIdx.x + 1];
+    const double *c = centers + 3 * size_t(leaf);
+    const PointTable t = tableAt(tables + warp * td, P);
+    for (uint32_t it = i0 + warp; it < i1; it += kWarps) {
+        const FmmItem item = items[it];
+        const FmmPanel &Pn = panels[item.panel];
+        double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+        for (int q = 0; q < kRulePts; ++q) {
+            const double b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
+            double x[3];
+            for (int d = 0; d < 3; ++d)
+                x[d] = Pn.v0[d] + b1 * Pn.e1[d] + b2 * Pn.e2[d];
+            fillTable(t, P, x[0] - c[0], x[1] - c[1], x[2] - c[2], k, lane);
+            double2 f[7];
+            for (int ch = 0; ch < 7; ++ch)
+                f[ch] = make_double2(0, 0);
+            for (int kk = lane; kk < nd; kk += 32) {
+                int n, m;
+                decode(kk, n, m);
+                const double2 R = solidR(t, n, m);
+                if (kk < nc)
+                    for (int ch = 0; ch < 6; ++ch)
+                        f[ch] = cadd(f[ch], cmul(Ls[ch * nc + kk], R));
+                f[6] = cadd(f[6], cmul(Ld[kk], R));
+            }
+            for (int ch = 0; ch < 7; ++ch)
+                for (int o = 16; o > 0; o >>= 1) {
+                    f[ch].x += __shfl_xor_sync(0xffffffffu, f[ch].x, o);
+                    f[ch].y += __shfl_xor_sync(0xffffffffu, f[ch].y, o);
+                }
+            __syncwarp();
+            // fields = -i k * sums
+            double2 F[7];
+            for (int ch = 0; ch < 7; ++ch)
+                F[ch] = make_double2(k * f[ch].y, -k * f[ch].x);
+            const double w = cFmmRule[4 * q + 3] * Pn.area;
+            const double bq[3] = {cFmmRule[4 * q], b1, b2};
+            // D + i k n.V
+            double2 nv = make_double2(0, 0);
+            for (int d = 0; d < 3; ++d) {
+                nv.x += Pn.n[d] * F[d].x;
+                nv.y += Pn.n[d] * F[d].y;
+            }
+            const double2 s0 = make_double2(F[6].x - k * nv.y, F[6].y + k * nv.x);
+            for (int a = 0; a < 3; ++a) {
+                if (!((item.mask >> a) & 1))
+                    continue;
+                double2 cw = make_double2(0, 0);
+                for (int d = 0; d < 3; ++d) {
+                    cw.x += Pn.curl[3 * a + d] * F[3 + d].x;
+                    cw.y += Pn.curl[3 * a + d] * F[3 + d].y;
+                }
+                // - (i / k) w curl . W
+                acc[a].x += w * bq[a] * s0.x + w * cw.y / k;
+                acc[a].y += w * bq[a] * s0.y - w * cw.x / k;
+            }
+        }
+        if (lane == 0)
+            for (int a = 0; a < 3; ++a)
+                if ((item.mask >> a) & 1)
+                    far[item.inc[a]] = acc[a];
+    }
+}
+
+// y_i = sum of the incidence contributions of vertex i (fixed order).
+__global__ void starSumKernel(const double2 *__restrict__ far, const uint32_t *__restrict__ incOffsets, uint32_t N,
+                              double2 *y) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N)
+        return;
+    double2 s = make_double2(0, 0);
+    for (uint32_t j = incOffsets[i]; j < incOffsets[i + 1]; ++j)
+        s = cadd(s, far[j]);
+    y[i] = s;
+}
+
+// Coaxial translation tables: one thread per (class, |m|, n, n'). fl holds
+// per class 4 pi i^? f_l(k t) Y_l^0(z) premultiplied: fl[class][l].
+__global__ void coaxKernel(uint32_t classes, const int *__restrict__ pin, const int *__restrict__ pout,
+                           const uint64_t *__restrict__ start, const double2 *__restrict__ fl, int lmax,
+                           const double *__restrict__ gaunt, const uint32_t *__restrict__ gauntOff, int gP,
+                           double2 *coax) {
+    const uint32_t cls = blockIdx.y;
+    if (cls >= classes)
+        return;
+    const int a = pin[cls], b = pout[cls];
+    size_t total = 0;
+    for (int j = 0; j <= min(a, b); ++j)
+        total += size_t(a + 1 - j) * (b + 1 - j);
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < total; e += size_t(gridDim.x) * blockDim.x) {
+        size_t off = 0;
+        int mm = 0;
+        while (off + size_t(a + 1 - mm) * (b + 1 - mm) <= e) {
+            off += size_t(a + 1 - mm) * (b + 1 - mm);
+            ++mm;
+        }
+        const size_t r = e - off;
+        const int wo = b + 1 - mm;
+        const int n = mm + int(r / wo), np = mm + int(r % wo);
+        const double *g = gaunt + gauntOff[(size_t(mm) * (gP + 1) + n) * (gP + 1) + np];
+        const double2 *f = fl + size_t(cls) * (lmax + 1);
+        double2 acc = make_double2(0, 0);
+        int idx = 0;
+        for (int l = abs(n - np); l <= n + np; l += 2, ++idx) {
+            const int e4 = ((n - np - l) / 2) & 1;  // i^(n - n' - l) = (-1)^((n - n' - l) / 2)
+            const double sg = e4 ? -1.0 : 1.0;
+            acc.x += sg * g[idx] * f[l].x;
+            acc.y += sg * g[idx] * f[l].y;
+        }
+        coax[start[cls] + e] = acc;
+    }
+}
+
+// ---------------------------------------------------------------- host math
+
+// Gauss-Legendre nodes and weights on [-1, 1] by Newton iteration.
+void gaussLegendre(int n, std::vector<double> &x, std::vector<double> &w) {
+    x.resize(n);
+    w.resize(n);
+    for (int i = 0; i < n; ++i) {
+        double z = std::cos(kFmmPi * (i + 0.75) / (n + 0.5)), dp = 0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1, p1 = z;
+            for (int j = 2; j <= n; ++j) {
+                const double p2 = ((2.0 * j - 1) * z * p1 - (j - 1.0) * p0) / j;
+                p0 = p1;
+                p1 = p2;
+            }
+            if (n == 1) {
+                p1 = z;
+                p0 = 1;
+            }
+            dp = n * (z * p1 - p0) / (z * z - 1);
+            const double dz = p1 / dp;
+            z -= dz;
+            if (std::abs(dz) < 1e-16)
+                break;
+        }
+        x[i] = z;
+        w[i] = 2 / ((1 - z * z) * dp * dp);
+    }
+}
+
+// Gaunt coefficients 2 pi int Theta_n^m Theta_l^0 Theta_n'^m, per (m, n, n') the
+// values for l = |n - n'|, |n - n'| + 2, ..., n + n' (others vanish).
+struct GauntTable {
+    int P = -1;
+    std::vector<double> values;
+    std::vector<uint32_t> offsets;  // (m * (P + 1) + n) * (P + 1) + n'
+};
+const GauntTable &gauntTable(int P) {
+    static std::mutex mu;
+    static std::map<int, GauntTable> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto found = cache.find(P);
+    if (found != cache.end())
+        return found->second;
+    GauntTable g;
+    g.P = P;
+    const int L = 2 * P;
+    std::vector<double> xq, wq;
+    gaussLegendre((3 * P) / 2 + 2, xq, wq);
+    const size_t tri = size_t(L + 1) * (L + 2) / 2;
+    std::vector<double> th(xq.size() * tri);
+    for (size_t q = 0; q < xq.size(); ++q)
+        for (int m = 0; m <= L; ++m)
+            thetaColumn(m, L, xq[q], std::sqrt(std::max(0.0, 1 - xq[q] * xq[q])), th.data() + q * tri);
+    g.offsets.assign(size_t(P + 1) * (P + 1) * (P + 1), 0);
+    for (int m = 0; m <= P; ++m)
+        for (int n = m; n <= P; ++n)
+            for (int np = m; np <= P; ++np) {
+                g.offsets[(size_t(m) * (P + 1) + n) * (P + 1) + np] = uint32_t(g.values.size());
+                for (int l = std::abs(n - np); l <= n + np; l += 2) {
+                    double s = 0;
+                    for (size_t q = 0; q < xq.size(); ++q) {
+                        const double *t = th.data() + q * tri;
+                        s += wq[q] * t[triIndex(n, m)] * t[triIndex(l, 0)] * t[triIndex(np, m)];
+                    }
+                    g.values.push_back(2 * kFmmPi * s);
+                }
+            }
+    return cache.emplace(P, std::move(g)).first->second;
+}
+
+// Wigner small-d blocks d^n[m, m'] (n <= P) for one polar angle.
+void wignerBlocks(int P, double cosb, std::vector<double> &out) {
+    const double sh = std::sqrt(std::max(0.0, (1 - cosb) / 2)), chh = std::sqrt(std::max(0.0, (1 + cosb) / 2));
+    const size_t base = out.size();
+    out.resize(base + wignerOffset(P + 1));
+    for (int n = 0; n <= P; ++n) {
+        const int w = 2 * n + 1;
+        double *d = out.data() + base + wignerOffset(n);
+        for (int m = -n; m <= n; ++m)
+            for (int mp = -n; mp <= n; ++mp)
+                d[size_t(m + n) * w + (mp + n)] = wignerSmallD(n, m, mp, cosb, sh, chh);
+    }
+}
+
+// Per-class radial factors 4 pi f_l(k t) Y_l^0(z), l <= lmax (f = h or j).
+void radialFactors(double kt, bool hankel, int lmax, std::complex<double> *f) {
+    std::vector<double> j(lmax + 1), y(lmax + 1);
+    besselJ(lmax, kt, j.data());
+    if (hankel)
+        besselY(lmax, kt, y.data());
+    for (int l = 0; l <= lmax; ++l) {
+        const double ylm0 = std::sqrt((2.0 * l + 1) / (4 * kFmmPi));
+        f[l] = 4 * kFmmPi * ylm0 * std::complex<double>(j[l], hankel ? -y[l] : 0.0);
+    }
+}
+
+int64_t gcd64(int64_t a, int64_t b) {
+    a = std::llabs(a);
+    b = std::llabs(b);
+    while (b) {
+        const int64_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+}  // namespace
+
+// -------------------------------------------------------------- the operator
+
+struct FmmOperator::Impl {
+    uint32_t N = 0, T = 0;
+    std::vector<uint32_t> incOffsets;
+    // per level (index = tree level): order, nodes with pressure supports
+    int lmin = 0, lmax = -1;
+    std::vector<int> order;
+    std::vector<std::vector<uint32_t>> levelNodes;
+    std::vector<std::vector<uint32_t>> leafNodes;  // leaves with pressure supports, per level
+    std::vector<std::vector<uint32_t>> leafItemStart;
+    std::vector<FmmItem> items;
+    std::vector<uint32_t> itemBase;  // per level: first item of the level's leaf list
+    // translations (host plans, per level)
+    struct Plan {
+        std::vector<uint32_t> outNodes, linkStart;
+        std::vector<TransLink> links;
+        std::vector<std::tuple<int, double, bool>> coaxUse;  // (level, distance, hankel) per coax class of the plan
+    };
+    std::vector<Plan> m2m, m2l, l2l;  // m2m[l]: parents at l; m2l[l]; l2l[l]: children at l
+    std::vector<double> wclassCos;    // polar class -> cos(theta)
+    std::vector<int> wclassP;         // polar class -> order needed (set in prepare)
+    // device
+    DevBuf panels, centers, coefOffset, incOff, far, y;
+    DevBuf Mc, Lc;
+    DevBuf wigner, wignerStart, coax, coaxStart, coaxPin, coaxPout, fl, gaunt, gauntOff;
+    DevBuf dItems;
+    std::vector<uint64_t> hostCoefOffset;
+    size_t coefTotal = 0;
+    int wignerP = -1;
+    int gauntP = -1;
+    // plan buffers per (kind, level)
+    struct DevPlan {
+        DevBuf out, start, links;
+        uint32_t count = 0;
+    };
+    std::vector<DevPlan> dm2m, dm2l, dl2l;
+    std::vector<DevBuf> dLeaves, dLeafStart;
+    std::vector<std::vector<uint32_t>> coaxClassOf;  // per kind*levels: local coax class index -> global
+};
+
+namespace {
+uint64_t polarKey(int64_t x, int64_t y, int64_t z) {
+    const int64_t n2 = x * x + y * y + z * z;
+    if (z == 0)
+        return 0;
+    const int64_t z2 = z * z, g = gcd64(z2, n2);
+    return (uint64_t(z > 0 ? 2 : 1) << 60) | (uint64_t(z2 / g) << 30) | uint64_t(n2 / g);
+}
+}  // namespace
+
+FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : impl_(std::make_unique<Impl>()) {
+    Impl &I = *impl_;
+    I.N = uint32_t(space.vertices.size());
+    I.T = uint32_t(space.panels.size());
+    std::vector<double> V(3 * size_t(I.N));
+    for (uint32_t v = 0; v < I.N; ++v) {
+        V[3 * v] = space.vertices[v].x;
+        V[3 * v + 1] = space.vertices[v].y;
+        V[3 * v + 2] = space.vertices[v].z;
+    }
+    std::vector<uint32_t> tri(3 * size_t(I.T));
+    for (uint32_t t = 0; t < I.T; ++t)
+        for (int a = 0; a < 3; ++a)
+            tri[3 * t + a] = space.panels[t].nodes[a];
+    tree_ = buildSupportTree(V.data(), I.N, tri.data(), I.T, settings);
+    I.incOffsets = space.incOffsets;
+    const auto &nodes = tree_.nodes;
+    const int levels = int(tree_.levels.size());
+    // near CSR (rows i, columns of the near leaves' supports)
+    {
+        std::vector<std::vector<uint32_t>> nearSources(nodes.size());
+        for (const auto &lk : tree_.ppNear)
+            nearSources[lk.target].push_back(lk.source);
+        nearRow_.assign(I.N + 1, 0);
+        std::vector<std::vector<uint32_t>> rows(I.N);
+        for (uint32_t ln = 0; ln < nodes.size(); ++ln) {
+            if (nearSources[ln].empty())
+                continue;
+            std::vector<uint32_t> cols;
+            for (uint32_t s : nearSources[ln])
+                for (uint32_t q = nodes[s].firstP; q < nodes[s].firstP + nodes[s].countP; ++q)
+                    cols.push_back(tree_.pressureOrder[q]);
+            std::sort(cols.begin(), cols.end());
+            for (uint32_t q = nodes[ln].firstP; q < nodes[ln].firstP + nodes[ln].countP; ++q)
+                rows[tree_.pressureOrder[q]] = cols;
+        }
+        for (uint32_t i = 0; i < I.N; ++i)
+            nearRow_[i + 1] = nearRow_[i] + uint32_t(rows[i].size());
+        nearCol_.reserve(nearRow_[I.N]);
+        for (uint32_t i = 0; i < I.N; ++i)
+            nearCol_.insert(nearCol_.end(), rows[i].begin(), rows[i].end());
+    }
+    // levels taking part in the far field
+    I.lmin = levels;
+    I.lmax = -1;
+    for (const auto &lk : tree_.ppFar) {
+        I.lmin = std::min<int>(I.lmin, nodes[lk.target].level);
+        I.lmax = std::max<int>(I.lmax, nodes[lk.target].level);
+    }
+    if (tree_.ppFar.empty())
+        return;
+    I.lmax = levels - 1;  // expansions reach every leaf below the coarsest far level
+    I.levelNodes.assign(levels, {});
+    I.leafNodes.assign(levels, {});
+    I.leafItemStart.assign(levels, {});
+    std::vector<uint64_t> coefSlot(nodes.size(), UINT64_MAX);
+    for (int l = I.lmin; l < levels; ++l)
+        for (uint32_t id : tree_.levels[l])
+            if (nodes[id].countP)
+                I.levelNodes[l].push_back(id);
+    // items of the leaves (panels of the leaf's vertex stars, by panel id)
+    I.dLeaves.resize(levels);
+    I.dLeafStart.resize(levels);
+    I.itemBase.assign(levels + 1, 0);
+    for (int l = I.lmin; l < levels; ++l) {
+        I.itemBase[l] = uint32_t(I.items.size());
+        for (uint32_t id : I.levelNodes[l]) {
+            if (!nodes[id].leaf())
+                continue;
+            I.leafNodes[l].push_back(id);
+            I.leafItemStart[l].push_back(uint32_t(I.items.size()) - I.itemBase[l]);
+            std::map<uint32_t, FmmItem> touched;
+            for (uint32_t q = nodes[id].firstP; q < nodes[id].firstP + nodes[id].countP; ++q) {
+                const uint32_t v = tree_.pressureOrder[q];
+                for (uint32_t j = space.incOffsets[v]; j < space.incOffsets[v + 1]; ++j) {
+                    const uint32_t t = space.incPanel[j];
+                    const int a = space.incLocal[j];
+                    auto &it = touched[t];
+                    it.panel = t;
+                    it.mask |= 1u << a;
+                    it.inc[a] = j;
+                }
+            }
+            for (auto &kv : touched)
+                I.items.push_back(kv.second);
+        }
+        I.leafItemStart[l].push_back(uint32_t(I.items.size()) - I.itemBase[l]);
+    }
+    // translation plans with their polar and coaxial classes
+    std::map<uint64_t, int> polar;
+    const auto polarClass = [&](int64_t x, int64_t y, int64_t z) {
+        const uint64_t key = polarKey(x, y, z);
+        auto f = polar.find(key);
+        if (f != polar.end())
+            return f->second;
+        const double c = z == 0 ? 0.0 : double(z) / std::sqrt(double(x * x + y * y + z * z));
+        I.wclassCos.push_back(c);
+        I.wclassP.push_back(0);
+        return polar[key] = int(I.wclassCos.size()) - 1;
+    };
+    I.m2m.assign(levels, {});
+    I.m2l.assign(levels, {});
+    I.l2l.assign(levels, {});
+    const auto widthOf = [&](int l) { return 2 * nodes[tree_.levels[l][0]].half; };
+    // M2L: targets at level l with their far sources (sorted), coax class per distance
+    {
+        std::vector<std::vector<uint32_t>> farSources(nodes.size());
+        for (const auto &lk : tree_.ppFar)
+            farSources[lk.target].push_back(lk.source);
+        for (int l = I.lmin; l < levels; ++l) {
+            Impl::Plan &pl = I.m2l[l];
+            std::map<int64_t, int> dist;
+            const double w = widthOf(l);
+            for (uint32_t id : I.levelNodes[l]) {
+                auto &src = farSources[id];
+                if (src.empty())
+                    continue;
+                std::sort(src.begin(), src.end());
+                pl.outNodes.push_back(id);
+                pl.linkStart.push_back(uint32_t(pl.links.size()));
+                for (uint32_t s : src) {
+                    const double d[3] = {nodes[id].center[0] - nodes[s].center[0],
+                                         nodes[id].center[1] - nodes[s].center[1],
+                                         nodes[id].center[2] - nodes[s].center[2]};
+                    const int64_t ix = std::llround(d[0] / w), iy = std::llround(d[1] / w), iz = std::llround(d[2] / w);
+                    const int64_t n2 = ix * ix + iy * iy + iz * iz;
+                    auto f = dist.find(n2);
+                    int cc;
+                    if (f == dist.end()) {
+                        cc = int(pl.coaxUse.size());
+                        pl.coaxUse.emplace_back(l, std::sqrt(double(n2)) * w, true);
+                        dist[n2] = cc;
+                    } else
+                        cc = f->second;
+                    TransLink lk{s, uint32_t(polarClass(ix, iy, iz)), uint32_t(cc), 0, std::atan2(d[1], d[0])};
+                    pl.links.push_back(lk);
+                }
+            }
+            pl.linkStart.push_back(uint32_t(pl.links.size()));
+        }
+    }
+    // M2M (parents at level l from children at l + 1) and L2L (children at l + 1 from parents at l)
+    for (int l = I.lmin; l + 1 < levels; ++l) {
+        Impl::Plan &up = I.m2m[l], &down = I.l2l[l + 1];
+        const double h = 0.5 * widthOf(l + 1);  // child half width
+        up.coaxUse.emplace_back(l, std::sqrt(3.0) * h, false);
+        down.coaxUse.emplace_back(l + 1, std::sqrt(3.0) * h, false);
+        for (uint32_t id : I.levelNodes[l]) {
+            if (nodes[id].leaf())
+                continue;
+            up.outNodes.push_back(id);
+            up.linkStart.push_back(uint32_t(up.links.size()));
+            for (uint32_t c : nodes[id].child) {
+                if (c == kNoNode || !nodes[c].countP)
+                    continue;
+                const double d[3] = {nodes[id].center[0] - nodes[c].center[0], nodes[id].center[1] - nodes[c].center[1],
+                                     nodes[id].center[2] - nodes[c].center[2]};
+                const int64_t ix = d[0] > 0 ? 1 : -1, iy = d[1] > 0 ? 1 : -1, iz = d[2] > 0 ? 1 : -1;
+                up.links.push_back({c, uint32_t(polarClass(ix, iy, iz)), 0, 0, std::atan2(d[1], d[0])});
+                down.outNodes.push_back(c);
+                down.linkStart.push_back(uint32_t(down.links.size()));
+                down.links.push_back({id, uint32_t(polarClass(-ix, -iy, -iz)), 0, 0, std::atan2(-d[1], -d[0])});
+            }
+        }
+        up.linkStart.push_back(uint32_t(up.links.size()));
+        down.linkStart.push_back(uint32_t(down.links.size()));
+    }
+    // geometry upload
+    std::vector<FmmPanel> fp(I.T);
+    for (uint32_t t = 0; t < I.T; ++t) {
+        const HostPanel &hp = space.panels[t];
+        FmmPanel &q = fp[t];
+        const double v0[3] = {hp.v[0].x, hp.v[0].y, hp.v[0].z};
+        const double v1[3] = {hp.v[1].x, hp.v[1].y, hp.v[1].z};
+        const double v2[3] = {hp.v[2].x, hp.v[2].y, hp.v[2].z};
+        for (int d = 0; d < 3; ++d) {
+            q.v0[d] = v0[d];
+            q.e1[d] = v1[d] - v0[d];
+            q.e2[d] = v2[d] - v0[d];
+        }
+        q.n[0] = hp.n.x;
+        q.n[1] = hp.n.y;
+        q.n[2] = hp.n.z;
+        for (int a = 0; a < 3; ++a) {
+            q.curl[3 * a] = hp.curl[a].x;
+            q.curl[3 * a + 1] = hp.curl[a].y;
+            q.curl[3 * a + 2] = hp.curl[a].z;
+            q.nodes[a] = hp.nodes[a];
+        }
+        q.area = hp.area;
+    }
+    cudaStream_t s = nullptr;
+    uploadVec(I.panels, fp, s);
+    std::vector<double> cen(3 * nodes.size());
+    for (size_t i = 0; i < nodes.size(); ++i)
+        for (int d = 0; d < 3; ++d)
+            cen[3 * i + d] = nodes[i].center[d];
+    uploadVec(I.centers, cen, s);
+    uploadVec(I.incOff, I.incOffsets, s);
+    uploadVec(I.dItems, I.items, s);
+    I.dm2m.resize(levels);
+    I.dm2l.resize(levels);
+    I.dl2l.resize(levels);
+    for (int l = I.lmin; l < levels; ++l) {
+        uploadVec(I.dLeaves[l], I.leafNodes[l], s);
+        uploadVec(I.dLeafStart[l], I.leafItemStart[l], s);
+        const auto put = [&](Impl::DevPlan &d, const Impl::Plan &p) {
+            d.count = uint32_t(p.outNodes.size());
+            uploadVec(d.out, p.outNodes, s);
+            uploadVec(d.start, p.linkStart, s);
+            uploadVec(d.links, p.links, s);
+        };
+        put(I.dm2m[l], I.m2m[l]);
+        put(I.dm2l[l], I.m2l[l]);
+        put(I.dl2l[l], I.l2l[l]);
+    }
+    std::vector<TriPoint> rule = triangleRule(4);
+    if (rule.size() != kRulePts)
+        throw std::logic_error("fast multipole: unexpected degree-4 rule size");
+    double ws = 0;
+    for (const auto &r : rule)
+        ws += r.w;
+    double hr[kRulePts * 4];
+    for (int q = 0; q < kRulePts; ++q) {
+        hr[4 * q] = rule[q].b[0];
+        hr[4 * q + 1] = rule[q].b[1];
+        hr[4 * q + 2] = rule[q].b[2];
+        hr[4 * q + 3] = rule[q].w / ws;
+    }
+    fmmCheck(cudaMemcpyToSymbol(cFmmRule, hr, sizeof(hr)), "rule upload");
+    fmmCheck(cudaDeviceSynchronize(), "setup");
+    I.far.ensure(3 * size_t(I.T) * 16);
+}
+
+FmmOperator::~FmmOperator() = default;
+
+void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
+    Impl &I = *impl_;
+    k_ = k;
+    levelInfo_.clear();
+    if (tree_.ppFar.empty())
+        return;
+    const auto &nodes = tree_.nodes;
+    const int levels = int(tree_.levels.size());
+    const double d0 = -std::log10(std::clamp(tolerance, 1e-15, 1e-2));
+    I.order.assign(levels, 0);
+    for (int l = I.lmin; l < levels; ++l) {
+        double r = 0;
+        for (uint32_t id : I.levelNodes[l])
+            r = std::max(r, nodes[id].radiusP);
+        const double kd = 2 * k * r;
+        const int hf = int(std::ceil(kd + 1.8 * std::pow(d0, 2.0 / 3.0) * std::cbrt(kd)));
+        const int lf = int(std::ceil(1.3 * d0)) + 1;
+        I.order[l] = std::min(kFmmMaxOrder, std::max(hf, lf));
+        levelInfo_.push_back({uint32_t(l), uint32_t(I.order[l]), uint32_t(I.levelNodes[l].size()),
+                              uint32_t(I.m2l[l].links.size()), r});
+    }
+    // coefficient storage: 6 channels per node of every taking part level
+    I.hostCoefOffset.assign(nodes.size(), 0);
+    size_t at = 0;
+    for (int l = I.lmin; l < levels; ++l) {
+        const size_t nc = size_t(I.order[l] + 1) * (I.order[l] + 1);
+        for (uint32_t id : I.levelNodes[l]) {
+            I.hostCoefOffset[id] = at;
+            at += 6 * nc;
+        }
+    }
+    I.coefTotal = at;
+    I.Mc.ensure(at * 16);
+    I.Lc.ensure(at * 16);
+    uploadVec(I.coefOffset, I.hostCoefOffset, stream);
+    // Wigner tables (per polar class, to the largest order it meets)
+    std::vector<int> need(I.wclassCos.size(), 0);
+    for (int l = I.lmin; l < levels; ++l) {
+        for (const auto &lk : I.m2l[l].links)
+            need[lk.wclass] = std::max(need[lk.wclass], I.order[l]);
+        for (const auto &lk : I.m2m[l].links)
+            need[lk.wclass] = std::max({need[lk.wclass], I.order[l], I.order[l + 1]});
+        for (const auto &lk : I.l2l[l].links)
+            need[lk.wclass] = std::max({need[lk.wclass], I.order[l], I.order[l - 1]});
+    }
+    bool grow = false;
+    for (size_t c = 0; c < need.size(); ++c)
+        grow |= need[c] > I.wclassP[c];
+    if (grow) {
+        std::vector<double> tab;
+        std::vector<uint64_t> start;
+        for (size_t c = 0; c < need.size(); ++c) {
+            I.wclassP[c] = std::max(I.wclassP[c], need[c]);
+            start.push_back(tab.size());
+            wignerBlocks(I.wclassP[c], I.wclassCos[c], tab);
+        }
+        uploadVec(I.wigner, tab, stream);
+        uploadVec(I.wignerStart, start, stream);
+    }
+    // coaxial classes of this wavenumber
+    int P = 0;
+    for (int l = I.lmin; l < levels; ++l)
+        P = std::max(P, I.order[l]);
+    const GauntTable &g = gauntTable(P);
+    if (I.gauntP != P) {
+        uploadVec(I.gaunt, g.values, stream);
+        uploadVec(I.gauntOff, g.offsets, stream);
+        I.gauntP = P;
+    }
+    std::vector<int> pin, pout;
+    std::vector<uint64_t> start;
+    std::vector<std::complex<double>> fl;
+    const int lmaxF = 2 * P;
+    uint64_t total = 0;
+    const auto addClass = [&](int a, int b, double t, bool hankel) {
+        pin.push_back(a);
+        pout.push_back(b);
+        start.push_back(total);
+        for (int j = 0; j <= std::min(a, b); ++j)
+            total += uint64_t(a + 1 - j) * (b + 1 - j);
+        const size_t at0 = fl.size();
+        fl.resize(at0 + lmaxF + 1);
+        radialFactors(k * t, hankel, lmaxF, fl.data() + at0);
+        return uint32_t(pin.size() - 1);
+    };
+    I.coaxClassOf.assign(3 * levels, {});
+    for (int l = I.lmin; l < levels; ++l) {
+        for (const auto &u : I.m2l[l].coaxUse)
+            I.coaxClassOf[l].push_back(addClass(I.order[l], I.order[l], std::get<1>(u), true));
+        for (const auto &u : I.m2m[l].coaxUse)
+            I.coaxClassOf[levels + l].push_back(addClass(I.order[l + 1], I.order[l], std::get<1>(u), false));
+        for (const auto &u : I.l2l[l].coaxUse)
+            I.coaxClassOf[2 * levels + l].push_back(addClass(I.order[l - 1], I.order[l], std::get<1>(u), false));
+    }
+    uploadVec(I.coaxPin, pin, stream);
+    uploadVec(I.coaxPout, pout, stream);
+    uploadVec(I.coaxStart, start, stream);
+    uploadVec(I.fl, fl, stream);
+    I.coax.ensure(total * 16);
+    coaxKernel<<<dim3(64, uint32_t(pin.size())), 256, 0, stream>>>(
+        uint32_t(pin.size()), I.coaxPin.as<int>(), I.coaxPout.as<int>(), I.coaxStart.as<uint64_t>(),
+        I.fl.as<double2>(), lmaxF, I.gaunt.as<double>(), I.gauntOff.as<uint32_t>(), P, I.coax.as<double2>());
+    fmmCheck(cudaGetLastError(), "coaxial table launch");
+    // local coax class ids -> global ids in the link lists
+    for (int l = I.lmin; l < levels; ++l) {
+        const auto remap = [&](const Impl::Plan &pl, Impl::DevPlan &d, const std::vector<uint32_t> &cls) {
+            if (pl.links.empty())
+                return;
+            std::vector<TransLink> links = pl.links;
+            for (auto &lk : links)
+                lk.cclass = cls[lk.cclass];
+            uploadVec(d.links, links, stream);
+        };
+        remap(I.m2l[l], I.dm2l[l], I.coaxClassOf[l]);
+        remap(I.m2m[l], I.dm2m[l], I.coaxClassOf[levels + l]);
+        remap(I.l2l[l], I.dl2l[l], I.coaxClassOf[2 * levels + l]);
+    }
+    fmmCheck(cudaStreamSynchronize(stream), "prepare");
+}
+
+void FmmOperator::applyFar(const double *p, size_t stride, uint32_t S, double *y, cudaStream_t stream,
+                           KernelTimer *timer) {
+    Impl &I = *impl_;
+    const uint32_t N = I.N;
+    for (uint32_t sys = 0; sys < S; ++sys) {
+        const double2 *pv = reinterpret_cast<const double2 *>(p + sys * stride);
+        double2 *yv = reinterpret_cast<double2 *>(y + size_t(sys) * N * 2);
+        if (tree_.ppFar.empty()) {
+            fmmCheck(cudaMemsetAsync(yv, 0, size_t(N) * 16, stream), "zero far");
+            continue;
+        }
+        const int levels = int(tree_.levels.size());
+        fmmCheck(cudaMemsetAsync(I.far.p, 0, 3 * size_t(I.T) * 16, stream), "zero contributions");
+        fmmCheck(cudaMemsetAsync(I.Lc.p, 0, I.coefTotal * 16, stream), "zero locals");
+        const auto smemTranslate = [&](int pin, int pout, int &chunk) {
+            const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1));
+            chunk = 6;
+            while (chunk > 1 && (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16 > 200 * 1024)
+                --chunk;
+            return (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16;
+        };
+        const auto translate = [&](Impl::DevPlan &d, int pin, int pout, const double2 *in, double2 *out, bool zero) {
+            if (!d.count)
+                return;
+            int chunk;
+            const size_t sm = smemTranslate(pin, pout, chunk);
+            fmmCheck(cudaFuncSetAttribute(translateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                     "translate smem");
+            translateKernel<<<d.count, 256, sm, stream>>>(d.out.as<uint32_t>(), d.start.as<uint32_t>(),
+                                                          d.links.as<TransLink>(), pin, pout, chunk, in, out,
+                                                          I.coefOffset.as<uint64_t>(), I.wigner.as<double>(),
+                                                          I.wignerStart.as<uint64_t>(), I.coax.as<double2>(),
+                                                          I.coaxStart.as<uint64_t>(), zero ? 1 : 0);
+            fmmCheck(cudaGetLastError(), "translate launch");
+        };
+        {
+            TimedScope scope(timer, "fmm_p2m", stream);
+            for (int l = I.lmin; l < levels; ++l) {
+                const uint32_t leaves = uint32_t(I.leafNodes[l].size());
+                if (!leaves)
+                    continue;
+                const int P = I.order[l];
+                const size_t td = tableDoubles(P);
+                const size_t sm = (kWarps * td) * 8 + kWarps * 6 * 16;
+                fmmCheck(cudaFuncSetAttribute(p2mKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                         "p2m smem");
+                p2mKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
+                                                       I.dLeafStart[l].as<uint32_t>(), I.dItems.as<FmmItem>() + I.itemBase[l],
+                                                       I.centers.as<double>(), I.coefOffset.as<uint64_t>(), P, k_, pv,
+                                                       I.Mc.as<double2>());
+                fmmCheck(cudaGetLastError(), "p2m launch");
+            }
+        }
+        {
+            TimedScope scope(timer, "fmm_m2m", stream);
+            for (int l = levels - 2; l >= I.lmin; --l)
+                translate(I.dm2m[l], I.order[l + 1], I.order[l], I.Mc.as<double2>(), I.Mc.as<double2>(), true);
+        }
+        {
+            TimedScope scope(timer, "fmm_m2l", stream);
+            for (int l = I.lmin; l < levels; ++l)
+                translate(I.dm2l[l], I.order[l], I.order[l], I.Mc.as<double2>(), I.Lc.as<double2>(), false);
+        }
+        {
+            TimedScope scope(timer, "fmm_l2l", stream);
+            for (int l = I.lmin + 1; l < levels; ++l)
+                translate(I.dl2l[l], I.order[l - 1], I.order[l], I.Lc.as<double2>(), I.Lc.as<double2>(), false);
+        }
+        {
+            TimedScope scope(timer, "fmm_l2p", stream);
+            for (int l = I.lmin; l < levels; ++l) {
+                const uint32_t leaves = uint32_t(I.leafNodes[l].size());
+                if (!leaves)
+                    continue;
+                const int p = I.order[l], P = p + 1;
+                const size_t td = tableDoubles(P);
+                const size_t sm = (6 * size_t(p + 1) * (p + 1) + size_t(P + 1) * (P + 1)) * 16 + kWarps * td * 8;
+                fmmCheck(cudaFuncSetAttribute(l2pKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                         "l2p smem");
+                l2pKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
+                                                       I.dLeafStart[l].as<uint32_t>(), I.dItems.as<FmmItem>() + I.itemBase[l],
+                                                       I.centers.as<double>(), I.coefOffset.as<uint64_t>(), p, k_,
+                                                       I.Lc.as<double2>(), I.far.as<double2>());
+                fmmCheck(cudaGetLastError(), "l2p launch");
+            }
+            starSumKernel<<<(N + 255) / 256, 256, 0, stream>>>(I.far.as<double2>(), I.incOff.as<uint32_t>(), N, yv);
+            fmmCheck(cudaGetLastError(), "star sum launch");
+        }
+    }
+}
+
+// ------------------------------------------------------------- self-test
+
+double fmmSelfTest() {
+    using cd = std::complex<double>;
+    std::mt19937_64 rng(7);
+    std::uniform_real_distribution<double> U(-0.5, 0.5);
+    const double k = 3.0;
+    const int p = 16;
+    const int nc = (p + 1) * (p + 1);
+    // direct field of random sources near the origin at targets near t
+    const int ns = 12, nt = 6;
+    std::vector<std::array<double, 3>> ys(ns), xs(nt);
+    std::vector<cd> s(ns);
+    for (auto &y : ys)
+        y = {U(rng), U(rng), U(rng)};
+    for (auto &v : s)
+        v = cd(U(rng), U(rng));
+    const double t[3] = {2.1, -1.3, 1.7};
+    for (auto &x : xs)
+        x = {t[0] + U(rng), t[1] + U(rng), t[2] + U(rng)};
+    const auto R = [&](int P, const double *d, std::vector<cd> &out) {
+        const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        const double ct = r > 0 ? d[2] / r : 1, st = std::sqrt(std::max(0.0, 1 - ct * ct)), ph = std::atan2(d[1], d[0]);
+        std::vector<double> j(P + 1), th(size_t(P + 1) * (P + 2) / 2);
+        besselJ(P, k * r, j.data());
+        for (int m = 0; m <= P; ++m)
+            thetaColumn(m, P, ct, st, th.data());
+        out.assign(size_t(P + 1) * (P + 1), 0);
+        for (int n = 0; n <= P; ++n)
+            for (int m = -n; m <= n; ++m) {
+                const int am = std::abs(m);
+                const double sg = (m < 0 && (am & 1)) ? -1 : 1;
+                out[coefIndex(n, m)] = j[n] * sg * th[triIndex(n, am)] * std::polar(1.0, m * ph);
+            }
+    };
+    std::vector<cd> M(nc, 0), Rv;
+    for (int i = 0; i < ns; ++i) {
+        R(p, ys[i].data(), Rv);
+        for (int q = 0; q < nc; ++q)
+            M[q] += s[i] * std::conj(Rv[q]);
+    }
+    // rotate -> coaxial (S|R) -> rotate back
+    const double tl = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    const double cb = t[2] / tl, ph = std::atan2(t[1], t[0]);
+    std::vector<double> dtab;
+    wignerBlocks(p, cb, dtab);
+    std::vector<cd> a(nc), b(nc, 0), c(nc, 0), L(nc, 0);
+    for (int n = 0; n <= p; ++n)
+        for (int mp = -n; mp <= n; ++mp) {
+            cd acc = 0;
+            for (int m = -n; m <= n; ++m)
+                acc += M[coefIndex(n, m)] * std::polar(1.0, m * ph) *
+                       dtab[wignerOffset(n) + size_t(m + n) * (2 * n + 1) + (mp + n)];
+            b[coefIndex(n, mp)] = acc;
+        }
+    const GauntTable &g = gauntTable(p);
+    std::vector<cd> fl(2 * p + 1);
+    radialFactors(k * tl, true, 2 * p, fl.data());
+    for (int np = 0; np <= p; ++np)
+        for (int m = -np; m <= np; ++m) {
+            const int am = std::abs(m);
+            cd acc = 0;
+            for (int n = am; n <= p; ++n) {
+                const double *gv = g.values.data() + g.offsets[(size_t(am) * (p + 1) + n) * (p + 1) + np];
+                cd cv = 0;
+                int idx = 0;
+                for (int l = std::abs(n - np); l <= n + np; l += 2, ++idx)
+                    cv += (((n - np - l) / 2) & 1 ? -1.0 : 1.0) * gv[idx] * fl[l];
+                acc += cv * b[coefIndex(n, m)];
+            }
+            c[coefIndex(np, m)] = acc;
+        }
+    for (int n = 0; n <= p; ++n)
+        for (int m1 = -n; m1 <= n; ++m1) {
+            cd acc = 0;
+            for (int m = -n; m <= n; ++m)
+                acc += dtab[wignerOffset(n) + size_t(m1 + n) * (2 * n + 1) + (m + n)] * c[coefIndex(n, m)];
+            L[coefIndex(n, m1)] = acc * std::polar(1.0, -m1 * ph);
+        }
+    double err = 0, ref = 0;
+    for (int i = 0; i < nt; ++i) {
+        cd direct = 0;
+        for (int q = 0; q < ns; ++q) {
+            const double dx = xs[i][0] - ys[q][0], dy = xs[i][1] - ys[q][1], dz = xs[i][2] - ys[q][2];
+            const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+            direct += s[q] * std::polar(1.0 / (4 * kFmmPi * r), -k * r);
+        }
+        const double d[3] = {xs[i][0] - t[0], xs[i][1] - t[1], xs[i][2] - t[2]};
+        R(p, d, Rv);
+        cd f = 0;
+        for (int q = 0; q < nc; ++q)
+            f += L[q] * Rv[q];
+        f *= cd(0, -k);
+        err = std::max(err, std::abs(f - direct));
+        ref = std::max(ref, std::abs(direct));
+    }
+    return err / ref;
+}
+
+}  // namespace hsb

@@ -1,0 +1,67 @@
+// Far-field operator of the fast-multipole form (fmm.cu) on the support tree
+// of fmm_tree.cpp.
+//
+// The operator splits the Burton-Miller matrix by support pairs: entries of
+// near support pairs (leaf pairs of the partition) are exact Galerkin entries,
+// the rest are applied through spherical-wave expansions of the fields
+//   V(x) = sum_j p_j int G(x, y) n(y) phi_j(y) dy,   W(x) = sum_j p_j int G(x, y) curl phi_j(y) dy,
+// tested as  y_i = int phi_i (div V + i k n.V) - (i / k) int curl phi_i . W,
+// the far part of the record formula of the dense form (double layer
+// d/dn_y G = -n.grad_x G, so its field is -div V; Maue curl term with
+// alpha = -i / k). Panel integrals use the degree-4 Dunavant rule.
+#pragma once
+
+#include "fmm_tree.hpp"
+#include "host_mesh.hpp"
+
+#include <cuda_runtime.h>
+#include <memory>
+#include <vector>
+
+namespace hsb {
+
+class KernelTimer;
+
+struct FmmLevelInfo {
+    uint32_t level, order, nodes, m2lLinks;
+    double radius;
+};
+
+class FmmOperator {
+  public:
+    FmmOperator(const Space &space, const FmmTreeSettings &settings);
+    ~FmmOperator();
+    FmmOperator(const FmmOperator &) = delete;
+    FmmOperator &operator=(const FmmOperator &) = delete;
+
+    // Expansion orders and translation tables for one wavenumber; the orders
+    // follow the wideband excess-bandwidth rule p = kD + 1.8 d^(2/3) (kD)^(1/3)
+    // (wideband_transfer.cpp:285-303) with d = -log10(tolerance), floored by a
+    // low-frequency order.
+    void prepare(double k, double tolerance, cudaStream_t stream);
+    // y[s] = far part of the raw (not row-equilibrated) operator applied to
+    // p[s] for S systems (complex, interleaved; system stride `stride` reals).
+    void applyFar(const double *p, size_t stride, uint32_t S, double *y, cudaStream_t stream, KernelTimer *timer);
+
+    const FmmTree &tree() const { return tree_; }
+    const std::vector<FmmLevelInfo> &levels() const { return levelInfo_; }
+    // Near support pairs (pressure x pressure) as CSR over rows i, columns sorted.
+    const std::vector<uint32_t> &nearRowStart() const { return nearRow_; }
+    const std::vector<uint32_t> &nearCols() const { return nearCol_; }
+    double wavenumber() const { return k_; }
+
+  private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+    FmmTree tree_;
+    std::vector<FmmLevelInfo> levelInfo_;
+    std::vector<uint32_t> nearRow_, nearCol_;
+    double k_ = 0;
+};
+
+// Host self-test of the expansion primitives (special functions, Wigner
+// rotations, Gaunt-built coaxial translations, coefficient derivatives)
+// against direct kernel sums. Returns the largest relative error.
+double fmmSelfTest();
+
+}  // namespace hsb

@@ -913,4 +913,38 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
     cuda(cudaStreamSynchronize(s), "CUDA synchronization");
 }
 
+FmmOperator &Session::fmmOperator(const hs_numerics &o) {
+    FmmTreeSettings st;
+    st.leafCapacity = o.fmm_leaf_support_capacity ? o.fmm_leaf_support_capacity : 32;
+    st.separationRatio = std::isfinite(o.fmm_separation_ratio) && o.fmm_separation_ratio > 1 ? o.fmm_separation_ratio : 1.5;
+    if (!fmm_ || st.leafCapacity != fmmSettings_.leafCapacity || st.separationRatio != fmmSettings_.separationRatio) {
+        fmm_.reset();
+        fmm_ = std::make_unique<FmmOperator>(space_, st);
+        fmmSettings_ = st;
+    }
+    return *fmm_;
+}
+
+void Session::debugFmmFar(const hs_numerics &o, double k, double tolerance, const double *pressure, double *far,
+                          std::vector<uint32_t> &nearRow, std::vector<uint32_t> &nearCol,
+                          std::vector<FmmLevelInfo> &levels) {
+    FmmOperator &op = fmmOperator(o);
+    const cudaStream_t s = stream();
+    const size_t N = space_.vertices.size();
+    op.prepare(k, tolerance, s);
+    dFmmIn_.ensure(N * 16);
+    dFmmOut_.ensure(N * 16);
+    cuda(cudaMemcpyAsync(dFmmIn_.as<void>(), pressure, N * 16, cudaMemcpyHostToDevice, s), "pressure upload");
+    op.applyFar(dFmmIn_.as<double>(), 2 * N, 1, dFmmOut_.as<double>(), s, &timer_);
+    cuda(cudaMemcpyAsync(far, dFmmOut_.as<void>(), N * 16, cudaMemcpyDeviceToHost, s), "far download");
+    cuda(cudaStreamSynchronize(s), "CUDA fast multipole");
+    for (size_t i = 0; i < N; ++i) {  // row equilibration 1 / lumped mass
+        far[2 * i] /= space_.lumpedMass[i];
+        far[2 * i + 1] /= space_.lumpedMass[i];
+    }
+    nearRow = op.nearRowStart();
+    nearCol = op.nearCols();
+    levels = op.levels();
+}
+
 }  // namespace hsb

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "device_types.cuh"
+#include "fmm.hpp"
 #include "hs_bem.h"
 #include "kernel_timer.hpp"
 #include "planner.hpp"
@@ -61,6 +62,11 @@ class Session {
     const Plan &plan(const hs_numerics &numerics, double maxK, const volatile int32_t *cancel);
     void debugAssemble(const hs_numerics &numerics, double planK, double k, const double *flux, double *matrix,
                        double *rhs);
+    // Far part of the fast-multipole operator (row-equilibrated like the dense
+    // matrix) applied to a P1 vector, with the near support-pair pattern.
+    void debugFmmFar(const hs_numerics &numerics, double k, double tolerance, const double *pressure, double *far,
+                     std::vector<uint32_t> &nearRow, std::vector<uint32_t> &nearCol,
+                     std::vector<FmmLevelInfo> &levels);
     KernelTimer &timer() { return timer_; }
     // Device bytes a solve may hold beyond the resident geometry and plan
     // (0: 60 % of free memory); bounds the frequency batch.
@@ -115,6 +121,12 @@ class Session {
         dPivots_, dInfo_, dKs_, dFlux_, dObservers_, dPartials_, dField_, dDegrees_, dWork32_, dGmres_, dLuPack_, dSolveScratch_;
     size_t peakBytes_ = 0;
     size_t memoryBudget_ = 0;
+    // fast-multipole form: operator on the support tree (built on first use
+    // for a tree setting) and its workspaces
+    FmmOperator &fmmOperator(const hs_numerics &numerics);
+    std::unique_ptr<FmmOperator> fmm_;
+    FmmTreeSettings fmmSettings_{};
+    DeviceBuffer dFmmIn_, dFmmOut_;
 };
 
 // Device bytes of one solve of F frequencies on a mesh with T panels and N

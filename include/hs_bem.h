@@ -218,6 +218,31 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
                             uint32_t *near_offsets, uint32_t *near_trials);
 hs_status hs_bem_debug_assemble(hs_bem_session *session, const hs_numerics *numerics, double plan_k, double k,
                                 const double *flux, double *matrix, double *rhs);
+/* Fast-multipole test hooks. hs_bem_debug_fmm_far applies the far part of the
+ * fast-multipole operator (support pairs outside the near leaf pairs of the
+ * support tree, row-equilibrated like hs_bem_debug_assemble's matrix) to a P1
+ * vector `pressure` (vertex_count complex) at wavenumber k with expansion
+ * tolerance `tolerance`, writing `far` (vertex_count complex); near_row_start
+ * (vertex_count + 1) and near_cols (capacity near_capacity, sorted per row)
+ * receive the near pattern, near_count its size; level_info receives per
+ * far-field level {level, order, nodes, M2L links} (capacity level_capacity
+ * rows of 4 u32), level_count their number. Pointers after `far` may be NULL.
+ * hs_bem_debug_fmm_selftest checks the expansion primitives (Bessel and
+ * Legendre recurrences, Wigner rotations, Gaunt-built coaxial translations)
+ * against a direct kernel sum on the host and writes the relative error. */
+hs_status hs_bem_debug_fmm_far(hs_bem_session *session, const hs_numerics *numerics, double k, double tolerance,
+                               const double *pressure, double *far, uint32_t *near_row_start, uint32_t *near_cols,
+                               size_t near_capacity, size_t *near_count, uint32_t *level_info, size_t level_capacity,
+                               size_t *level_count);
+hs_status hs_bem_debug_fmm_selftest(double *error);
+/* The support tree of the fast-multipole form (host only): the mesh centred on
+ * vertex 0 like a session; sizes = {nodes, levels, pressure-pressure near,
+ * pressure-pressure far, pressure-flux near, pressure-flux far} and links the
+ * (target, source) node pairs of the four lists in that order (capacity pairs
+ * at most; NULL to query sizes). */
+hs_status hs_bem_debug_fmm_tree(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                size_t triangle_count, uint32_t leaf_capacity, double separation_ratio,
+                                double near_distance_ratio, size_t *sizes, uint32_t *links, size_t capacity);
 
 /* Allocation-free observer field. No counterpart in the reference: it is an
  * addition for callers that cannot allocate device memory when they need a

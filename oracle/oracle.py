@@ -175,6 +175,27 @@ def reference_pressure_field(mesh, frequency: float, sound_speed: float, pressur
     return out.view(np.complex128), status
 
 
+def reference_support_tree(mesh, leaf_capacity=32, separation_ratio=1.5, near_distance_ratio=2.0):
+    """The reference's makeSupportTree (fmm/support_tree.cpp:407) on the mesh centred
+    on vertex 0: (sizes[6], links (M, 2)) with sizes = nodes, levels, pp near, pp far,
+    pf near, pf far and links the four lists' (target, source) pairs in that order."""
+    lib = _load_ref()
+    sizes = np.zeros(6, np.uintp)
+    verts = np.ascontiguousarray(mesh.vertices, np.float64)
+    tris = np.ascontiguousarray(mesh.triangles, np.uint32)
+    lib.ref_support_tree.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_uint, C.c_double, C.c_double,
+                                     C.c_void_p, C.c_void_p, C.c_size_t]
+    _check(lib, "ref", lib.ref_support_tree(verts.ctypes.data, mesh.vertex_count, tris.ctypes.data,
+                                            mesh.triangle_count, leaf_capacity, separation_ratio, near_distance_ratio,
+                                            sizes.ctypes.data, None, 0))
+    total = int(sizes[2:].sum())
+    links = np.zeros((max(total, 1), 2), np.uint32)
+    _check(lib, "ref", lib.ref_support_tree(verts.ctypes.data, mesh.vertex_count, tris.ctypes.data,
+                                            mesh.triangle_count, leaf_capacity, separation_ratio, near_distance_ratio,
+                                            sizes.ctypes.data, links.ctypes.data, total))
+    return sizes.astype(np.int64), links[:total]
+
+
 def estimate_patch(which: str, tri_a, tri_b, nodes_a, nodes_b, patch22, k):
     lib = _load_oracle() if which == "oracle" else _load_ref()
     prefix = "oracle" if which == "oracle" else "ref"

@@ -4,11 +4,13 @@
 // reference tree by oracle/Makefile into oracle/_ref/. It exposes the
 // reference's interaction plan and patch estimator with the same flat layout
 // as the restated oracle so tests can compare them exactly, and
-// evaluatePressureField for the GPU point-sampling parity tests.
+// evaluatePressureField for the GPU point-sampling parity tests, and the
+// fast-multipole support tree (fmm/support_tree.cpp) for the tree parity test.
 #include "galerkin/interaction_plan.hpp"
 #include <hornsculpt/field_evaluation.hpp>
 #include "galerkin/pair_quadrature.hpp"
 #include "galerkin/space.hpp"
+#include "fmm/support_tree.hpp"
 
 #include <cstring>
 #include <string>
@@ -226,6 +228,42 @@ int ref_pressure_field(const double *verts, size_t nv, const uint32_t *tris, siz
     } catch (const std::exception &e) {
         lastError = e.what();
         return 2;
+    }
+}
+
+// makeSupportTree on the centred mesh: sizes = {nodes, levels, pp near, pp far,
+// pf near, pf far}; links = (target, source) pairs of the four lists in that
+// order (capacity pairs at most).
+int ref_support_tree(const double *verts, size_t nv, const uint32_t *tris, size_t nt, unsigned leafCapacity,
+                     double separationRatio, double nearDistanceRatio, size_t *sizes, uint32_t *links,
+                     size_t capacity) {
+    try {
+        const Space space = buildSpace(makeMesh(verts, nv, tris, nt));
+        wideband::SupportTreeSettings st;
+        st.leafCapacity = leafCapacity;
+        st.separationRatio = separationRatio;
+        st.nearDistanceRatio = nearDistanceRatio;
+        const auto tree = wideband::makeSupportTree(space, st);
+        sizes[0] = tree.nodes.size();
+        sizes[1] = tree.levels.size();
+        sizes[2] = tree.pressurePressure.nearInteractions.size();
+        sizes[3] = tree.pressurePressure.farInteractions.size();
+        sizes[4] = tree.pressureFlux.nearInteractions.size();
+        sizes[5] = tree.pressureFlux.farInteractions.size();
+        size_t at = 0;
+        for (const auto *list : {&tree.pressurePressure.nearInteractions, &tree.pressurePressure.farInteractions,
+                                 &tree.pressureFlux.nearInteractions, &tree.pressureFlux.farInteractions})
+            for (const auto &lk : *list) {
+                if (at < capacity) {
+                    links[2 * at] = lk.target;
+                    links[2 * at + 1] = lk.source;
+                }
+                ++at;
+            }
+        return 0;
+    } catch (const std::exception &e) {
+        lastError = e.what();
+        return 1;
     }
 }
 }
