@@ -384,6 +384,26 @@ class CudaBemSolver:
                                                    b.ctypes.data))
         return _cplx(A).reshape(N, N).T, _cplx(b)  # column-major -> [row, col]
 
+    def debug_fmm_far(self, numerics: BemNumerics, k: float, tolerance: float, pressure: np.ndarray):
+        """Far part of the fast-multipole operator applied to a P1 vector (row-equilibrated
+        like debug_assemble), the near support-pair pattern as CSR (row_start, cols) and
+        the far-field levels as rows (level, order, nodes, M2L links)."""
+        N = self._mesh.vertex_count
+        p = np.zeros(2 * N)
+        p[0::2], p[1::2] = np.real(pressure), np.imag(pressure)
+        far = np.zeros(2 * N)
+        row = np.zeros(N + 1, np.uint32)
+        count, levels = C.c_size_t(), C.c_size_t()
+        n = numerics.to_c()
+        _lib.check(self._lib.hs_bem_debug_fmm_far(self._handle, C.byref(n), k, tolerance, p.ctypes.data, far.ctypes.data,
+                                                  row.ctypes.data, None, 0, C.byref(count), None, 0, C.byref(levels)))
+        cols = np.zeros(max(count.value, 1), np.uint32)
+        info = np.zeros((max(levels.value, 1), 4), np.uint32)
+        _lib.check(self._lib.hs_bem_debug_fmm_far(self._handle, C.byref(n), k, tolerance, p.ctypes.data, far.ctypes.data,
+                                                  row.ctypes.data, cols.ctypes.data, count.value, C.byref(count),
+                                                  info.ctypes.data, levels.value, C.byref(levels)))
+        return _cplx(far), row, cols[: count.value], info[: levels.value]
+
 
 @dataclasses.dataclass
 class ServeOptions:

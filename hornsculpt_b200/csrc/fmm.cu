@@ -88,6 +88,7 @@ struct TransLink {
 constexpr int kRulePts = 6;
 __constant__ double cFmmRule[kRulePts * 4];  // b0, b1, b2, physical weight fraction (sum 1)
 constexpr int kWarps = 8;
+constexpr size_t kMaxShared = 227 * 1024;  // dynamic shared memory per CTA (opt-in)
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -1074,6 +1075,8 @@ void FmmOperator::applyFar(const double *p, size_t stride, uint32_t S, double *y
                 const int P = I.order[l];
                 const size_t td = tableDoubles(P);
                 const size_t sm = (kWarps * td) * 8 + kWarps * 6 * 16;
+                if (sm > kMaxShared)
+                    throw Unsupported("Fast-multipole leaf order exceeds the shared-memory tables; refine the tree.");
                 fmmCheck(cudaFuncSetAttribute(p2mKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                          "p2m smem");
                 p2mKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
@@ -1107,6 +1110,8 @@ void FmmOperator::applyFar(const double *p, size_t stride, uint32_t S, double *y
                 const int p = I.order[l], P = p + 1;
                 const size_t td = tableDoubles(P);
                 const size_t sm = (6 * size_t(p + 1) * (p + 1) + size_t(P + 1) * (P + 1)) * 16 + kWarps * td * 8;
+                if (sm > kMaxShared)
+                    throw Unsupported("Fast-multipole leaf order exceeds the shared-memory tables; refine the tree.");
                 fmmCheck(cudaFuncSetAttribute(l2pKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                          "l2p smem");
                 l2pKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
