@@ -6,6 +6,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <functional>
 #include <vector>
 #include <cuda_runtime.h>
 
@@ -179,6 +180,12 @@ size_t gmresWorkspaceBytes(uint32_t N, uint32_t S, uint32_t m);
 uint32_t gmresCycleBatch(const double *A, const float *LU32, const int *pivots, uint32_t N, uint32_t B, uint32_t E,
                          const double *r, double *x, uint32_t m, const std::vector<double> &tolerances,
                          void *workspace, cudaStream_t stream, KernelTimer *timer, std::vector<uint32_t> &stepsOut);
+// The same cycle with a caller-supplied operator and preconditioner (gmres.cu).
+uint32_t gmresCycleOperator(uint32_t N, uint32_t S, const double *r, double *x, uint32_t m,
+                            const std::vector<double> &tolerances, void *workspace, cudaStream_t stream,
+                            KernelTimer *timer, std::vector<uint32_t> &stepsOut,
+                            const std::function<void(const double *, size_t, double *)> &apply,
+                            const std::function<void(const double *, double *)> &precondition);
 
 // Observer fields of one rule degree for every (batch, excitation, observer).
 struct FieldRequest {

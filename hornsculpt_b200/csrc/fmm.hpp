@@ -59,6 +59,34 @@ class FmmOperator {
     double k_ = 0;
 };
 
+// The fast-multipole linear system of one frequency: A = N + R F, with N the
+// exact near support-pair entries (CSR of the operator's pattern), F the far
+// expansion operator and R = 1 / lumped mass the row equilibration. Solved by
+// restarted GMRES (CGS2, Givens) left-preconditioned by block Jacobi on the
+// leaves' diagonal blocks of N (SupportBlockJacobi,
+// cuda/support_preconditioner.cu:33-191: spatially ordered diagonal blocks of
+// the near matrix, inverted once per frequency).
+class FmmSystem {
+  public:
+    FmmSystem(FmmOperator &op, const double *rowScale, const double *mass);
+    ~FmmSystem();
+    // Near values from the row-equilibrated dense matrix (column-major N x N).
+    void nearFromDense(const double *A, cudaStream_t stream, KernelTimer *timer);
+    void factorBlocks(cudaStream_t stream, KernelTimer *timer);
+    void apply(const double *x, size_t stride, uint32_t S, double *y, cudaStream_t stream, KernelTimer *timer);
+    void precondition(const double *in, double *out, uint32_t S, cudaStream_t stream);
+    // x_s = A^{-1} b_s to mass-weighted relative residual `target` (x starts at 0).
+    // relative[s]: final relative residual of the operator; iterations[s]: Arnoldi steps.
+    void solve(const double *b, double *x, uint32_t S, double target, uint32_t restart, uint32_t maxIterations,
+               cudaStream_t stream, KernelTimer *timer, std::vector<double> &relative,
+               std::vector<uint32_t> &iterations);
+
+  private:
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+    FmmOperator &op_;
+};
+
 // Host self-test of the expansion primitives (special functions, Wigner
 // rotations, Gaunt-built coaxial translations, coefficient derivatives)
 // against direct kernel sums. Returns the largest relative error.

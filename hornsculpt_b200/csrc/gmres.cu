@@ -13,6 +13,7 @@
 #include "kernel_timer.hpp"
 
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <stdexcept>
 #include <string>
@@ -346,6 +347,78 @@ uint32_t gmresCycleBatch(const double *A, const float *LU32, const int *pivots, 
                 A, N, E, basis + size_t(j) * N * 2, size_t(m + 1) * N * 2, z, active);
         }
         precondition(z);  // z = M^{-1} A V_j
+        {
+            TimedScope scope(timer, "gmres_orthogonalize", stream);
+            for (int pass = 0; pass < 2; ++pass) {
+                dotKernel<<<dim3(j + 1, S), 256, 0, stream>>>(basis, z, N, m, j, hess, dots, pass == 1, active);
+                subtractKernel<<<dim3((N + 255) / 256, S), 256, 0, stream>>>(basis, dots, N, m, j, z, active);
+            }
+            normalizeKernel<<<S, 256, 0, stream>>>(z, N, m, j, basis, hess, active);
+            givensKernel<<<(S + 127) / 128, 128, 0, stream>>>(S, m, j, hess, rot, g, beta, tol, estimate, active,
+                                                              steps);
+        }
+        check(cudaGetLastError(), "GMRES step launch");
+        check(cudaMemcpyAsync(hostActive.data(), active, S * sizeof(int), cudaMemcpyDeviceToHost, stream),
+              "GMRES state");
+        check(cudaStreamSynchronize(stream), "GMRES step");
+        if (std::none_of(hostActive.begin(), hostActive.end(), [](int a) { return a != 0; })) {
+            ++j;
+            break;
+        }
+    }
+    {
+        TimedScope scope(timer, "gmres_update", stream);
+        updateKernel<<<S, 256, m * sizeof(double2), stream>>>(basis, hess, g, steps, N, m, x);
+        check(cudaGetLastError(), "GMRES update launch");
+    }
+    stepsOut.resize(S);
+    check(cudaMemcpyAsync(stepsOut.data(), steps, S * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream),
+          "GMRES steps");
+    check(cudaStreamSynchronize(stream), "GMRES update");
+    return j;
+}
+
+// The same cycle with the operator and the preconditioner supplied by the
+// caller: apply(v, stride, z) writes z_s = A v_s for every system (v_s at
+// v + s * stride reals), precondition(in, out) writes out_s = M^{-1} in_s
+// (out may equal in). Used by the fast-multipole form, whose A is the near
+// matrix plus the far-field expansion operator.
+uint32_t gmresCycleOperator(uint32_t N, uint32_t S, const double *r, double *x, uint32_t m,
+                            const std::vector<double> &tolerances, void *workspace, cudaStream_t stream,
+                            KernelTimer *timer, std::vector<uint32_t> &stepsOut,
+                            const std::function<void(const double *, size_t, double *)> &apply,
+                            const std::function<void(const double *, double *)> &precondition) {
+    const GmresLayout l = gmresLayout(N, S, m);
+    char *w = static_cast<char *>(workspace);
+    double *basis = reinterpret_cast<double *>(w + l.basis);
+    double *hess = reinterpret_cast<double *>(w + l.hess);
+    double *g = reinterpret_cast<double *>(w + l.g);
+    double *dots = reinterpret_cast<double *>(w + l.dots);
+    double *rot = reinterpret_cast<double *>(w + l.rot);
+    double *beta = reinterpret_cast<double *>(w + l.beta);
+    double *estimate = reinterpret_cast<double *>(w + l.estimate);
+    double *tol = reinterpret_cast<double *>(w + l.tol);
+    if (tolerances.size() != S)
+        throw std::runtime_error("GMRES needs one tolerance per system.");
+    check(cudaMemcpyAsync(tol, tolerances.data(), S * sizeof(double), cudaMemcpyHostToDevice, stream),
+          "GMRES tolerances");
+    int *active = reinterpret_cast<int *>(w + l.active);
+    uint32_t *steps = reinterpret_cast<uint32_t *>(w + l.steps);
+    double *z = reinterpret_cast<double *>(w + l.z);
+    {
+        TimedScope scope(timer, "gmres_precondition", stream);
+        precondition(r, z);
+    }
+    startKernel<<<S, 256, 0, stream>>>(z, N, m, basis, g, beta, estimate, active, steps);
+    check(cudaGetLastError(), "GMRES start launch");
+    std::vector<int> hostActive(S);
+    uint32_t j = 0;
+    for (; j < m; ++j) {
+        apply(basis + size_t(j) * N * 2, size_t(m + 1) * N * 2, z);
+        {
+            TimedScope scope(timer, "gmres_precondition", stream);
+            precondition(z, z);
+        }
         {
             TimedScope scope(timer, "gmres_orthogonalize", stream);
             for (int pass = 0; pass < 2; ++pass) {

@@ -107,8 +107,9 @@ void validateRequest(const hs_request &r) {
         !std::isfinite(o.relative_residual_tolerance) || o.relative_residual_tolerance < 1e-7 ||
         o.relative_residual_tolerance > .01 || o.maximum_refinement_steps > 10)
         throw InvalidArgument("Invalid BEM medium, frequencies, excitation or Galerkin settings.");
-    if (fmm)
-        throw Unsupported("The fast-multipole acceleration is not part of this build; use the dense form.");
+    if (fmm && o.precision == HS_PRECISION_MIXED)
+        throw Unsupported("The mixed-precision fast-multipole form is not part of this build; use the FP64 fast "
+                          "multipole or the dense mixed form.");
     if (o.precision != HS_PRECISION_FP64 && o.precision != HS_PRECISION_MIXED)
         throw InvalidArgument("Invalid BEM precision form.");
     if (r.excitation_count > 1024 || r.observer_count > 100000)
@@ -593,6 +594,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                              dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2,
                              T > kExactBinsT ? dBinOffsets_.as<uint64_t>() : nullptr};
         const bool mixed = o.precision == HS_PRECISION_MIXED;
+        const bool fmmForm = o.acceleration == HS_FAST_MULTIPOLE;
         assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws, dA_.as<double>(),
                       dRhs_.as<double>(), dError_.as<int>(), s, &timer_, mixed);
         cuda(cudaEventRecord(ev.assembled, s), "phase event");
@@ -612,6 +614,59 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             work[7] += B;
         };
         checkCancel();
+        double assemblyMs = 0, factorMs = 0, triMs = 0, residualMs = 0;
+        std::vector<uint32_t> steps(B, 0), krylov(size_t(B) * E, 0), cycle;
+        std::vector<double> relative(size_t(B) * E, 0);
+        const double target = mixed ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
+        if (fmmForm) {
+            // Fast-multipole form: per frequency the near support pairs of the
+            // assembled matrix, block-Jacobi on the leaf blocks and GMRES on
+            // near + expansion far field (support_fmm_solve.cu:401-525).
+            FmmOperator &op = fmmOperator(o);
+            if (!fmmSystem_ || fmmSystemOp_ != &op) {
+                fmmSystem_.reset();
+                fmmSystem_ = std::make_unique<FmmSystem>(op, dRowScale_.as<double>(), dMass_.as<double>());
+                fmmSystemOp_ = &op;
+            }
+            cuda(cudaEventRecord(ev.factored, s), "phase event");
+            const double expansionTolerance = std::clamp(.01 * target, 1e-10, 1e-6);
+            const auto solveStart = Clock::now();
+            std::vector<double> rel;
+            std::vector<uint32_t> its;
+            for (uint32_t b = 0; b < B; ++b) {
+                checkCancel();
+                op.prepare(ks[b], expansionTolerance, s);
+                fmmSystem_->nearFromDense(dA_.as<double>() + size_t(b) * N * N * 2, s, &timer_);
+                fmmSystem_->factorBlocks(s, &timer_);
+                fmmSystem_->solve(dRhs_.as<double>() + size_t(b) * E * N * 2, dX_.as<double>() + size_t(b) * E * N * 2,
+                                  E, target, o.fmm_restart_length, o.fmm_maximum_iterations, s, &timer_, rel, its);
+                for (uint32_t e = 0; e < E; ++e)
+                    krylov[size_t(b) * E + e] = its[e];
+            }
+            cuda(cudaEventRecord(ev.solved, s), "phase event");
+            // the residual of the assembled operator, as the dense form reports it
+            std::vector<double> norms(2 * size_t(B) * E);
+            residualBatch(dA_.as<double>(), dRhs_.as<double>(), dX_.as<double>(), dMass_.as<double>(), N, B, E,
+                          dCorr_.as<double>(), dNorms_.as<double>(), s, &timer_);
+            cuda(cudaMemcpyAsync(norms.data(), dNorms_.as<void>(), norms.size() * 8, cudaMemcpyDeviceToHost, s),
+                 "residual norms");
+            cuda(cudaStreamSynchronize(s), "CUDA fast-multipole residual");
+            checkDeviceError("CUDA Galerkin assembly");
+            for (size_t q = 0; q < relative.size(); ++q) {
+                const double res = norms[2 * q], rhs = norms[2 * q + 1];
+                relative[q] = rhs > 0 ? res / rhs : (res == 0 ? 0 : std::numeric_limits<double>::infinity());
+                if (!std::isfinite(relative[q]) || relative[q] > 10 * target)
+                    throw NoConvergence("Fast-multipole solution misses the Burton-Miller residual tolerance.");
+            }
+            float a = 0, c = 0;
+            cuda(cudaEventElapsedTime(&a, ev.batch, ev.assembled), "phase time");
+            cuda(cudaEventElapsedTime(&c, ev.factored, ev.solved), "phase time");
+            assemblyMs = a;
+            triMs = c;
+            residualMs = msSince(solveStart);
+            if (timer_.enabled())
+                countWork();
+        } else {
         // LU of every matrix of the batch (FP64, or an FP32 copy in the mixed
         // form), then the initial solves.
         const size_t matrixReals = size_t(B) * N * N * 2, vectorReals = size_t(B) * E * N * 2;
@@ -645,15 +700,11 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                          &timer_);
         }
         cuda(cudaEventRecord(ev.solved, s), "phase event");
-        double assemblyMs = 0, factorMs = 0, triMs = 0;
         bool refining = false;  // a refinement solve between ev.refine0 and ev.refine1 awaits its time
         // FP64 refinement (cuda_solver.cu:1519-1581), per frequency. The mixed
         // form refines against the FP64 residual to min(tolerance, 1e-10).
-        const double target = mixed ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
         const uint32_t maxSteps = mixed ? std::max<uint32_t>(o.maximum_refinement_steps, 10) : o.maximum_refinement_steps;
         const auto residualStart = Clock::now();
-        std::vector<uint32_t> steps(B, 0), krylov(size_t(B) * E, 0), cycle;
-        std::vector<double> relative(size_t(B) * E, 0);
         std::vector<double> norms(2 * size_t(B) * E);
         for (;;) {
             checkCancel();
@@ -734,7 +785,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             cuda(cudaEventRecord(ev.refine1, s), "phase event");
             refining = true;
         }
-        const double residualMs = msSince(residualStart);
+        residualMs = msSince(residualStart);
+        }
         // Observer fields with the degree-comparison loop (cuda_solver.cu:1717-1799).
         const auto fieldStart = Clock::now();
         std::vector<cplx> field(size_t(B) * E * O, 0);
@@ -918,6 +970,8 @@ FmmOperator &Session::fmmOperator(const hs_numerics &o) {
     st.leafCapacity = o.fmm_leaf_support_capacity ? o.fmm_leaf_support_capacity : 32;
     st.separationRatio = std::isfinite(o.fmm_separation_ratio) && o.fmm_separation_ratio > 1 ? o.fmm_separation_ratio : 1.5;
     if (!fmm_ || st.leafCapacity != fmmSettings_.leafCapacity || st.separationRatio != fmmSettings_.separationRatio) {
+        fmmSystem_.reset();
+        fmmSystemOp_ = nullptr;
         fmm_.reset();
         fmm_ = std::make_unique<FmmOperator>(space_, st);
         fmmSettings_ = st;

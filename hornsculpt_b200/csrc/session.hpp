@@ -125,6 +125,8 @@ class Session {
     // for a tree setting) and its workspaces
     FmmOperator &fmmOperator(const hs_numerics &numerics);
     std::unique_ptr<FmmOperator> fmm_;
+    std::unique_ptr<FmmSystem> fmmSystem_;
+    const FmmOperator *fmmSystemOp_ = nullptr;
     FmmTreeSettings fmmSettings_{};
     DeviceBuffer dFmmIn_, dFmmOut_;
 };

@@ -47,9 +47,9 @@ def test_invalid_requests(solver, kw, match):
         solver.solve(req(**kw))
 
 
-def test_fast_multipole_is_reported_unsupported(solver):
+def test_mixed_fast_multipole_is_reported_unsupported(solver):
     with pytest.raises(hs.BemUnsupported):
-        solver.solve(req(numerics=hs.BemNumerics(acceleration="fast_multipole")))
+        solver.solve(req(numerics=hs.BemNumerics(acceleration="fast_multipole", precision="mixed")))
 
 
 def test_electrically_coarse_mesh_rejected():
