@@ -344,14 +344,16 @@ def run_c2(args):
             "wall 3 mm, h 7.15 mm, seed 0", "N": mesh.vertex_count, "T": mesh.triangle_count,
             "frequencies": len(C2_FREQUENCIES), "range_hz": [200.0, 8000.0]}
     results = {}
-    for form in ("fp64", "mixed"):
+    forms = [f for f in args.c2_forms.split(",") if f]
+    for form in forms:
         with hs.CudaBemSolver(mesh) as solver:
             solver.set_stream(stream.cuda_stream)
 
             def request(fs):
+                numerics = (hs.BemNumerics(precision="fp64", acceleration="fast_multipole") if form == "fmm64"
+                            else hs.BemNumerics(precision=form))
                 return hs.BemRequest(frequencies=fs, observers=obs, excitations=exc,
-                                     medium=hs.AcousticMedium(DENSITY, SOUND_SPEED),
-                                     numerics=hs.BemNumerics(precision=form),
+                                     medium=hs.AcousticMedium(DENSITY, SOUND_SPEED), numerics=numerics,
                                      interaction_plan_frequencies=C2_FREQUENCIES)
             t0 = time.perf_counter()
             solver.solve(request(C2_FREQUENCIES[-1:]))  # plan, workspace and warm-up
@@ -368,14 +370,18 @@ def run_c2(args):
                           "wall_ms_per_frequency": 1e3 * wall / len(C2_FREQUENCIES),
                           "solves_per_s": 1e3 * len(C2_FREQUENCIES) / span if span else None,
                           "first_call_s_with_planning": round(first, 2),
-                          "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])[:8]},
-                          "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations)}
-    err = 0.0
-    for fp, fm in zip(results["fp64"].frequencies, results["mixed"].frequencies):
-        a, b = fp.excitations[0].boundary.surface_pressure, fm.excitations[0].boundary.surface_pressure
-        err = max(err, float(np.sqrt((area * np.abs(b - a) ** 2).sum() / (area * np.abs(a) ** 2).sum())))
-    line["max_rel_err_surface_mixed_vs_fp64"] = err
-    line["mixed_over_fp64"] = line["fp64"]["ms_per_frequency"] / line["mixed"]["ms_per_frequency"]
+                          "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])[:12]},
+                          "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations),
+                          "gmres_iterations": [f.excitations[0].iterations for f in res.frequencies]}
+    for other in [f for f in forms if f != "fp64"]:
+        if "fp64" not in results:
+            break
+        err = 0.0
+        for fp, fm in zip(results["fp64"].frequencies, results[other].frequencies):
+            a, b = fp.excitations[0].boundary.surface_pressure, fm.excitations[0].boundary.surface_pressure
+            err = max(err, float(np.sqrt((area * np.abs(b - a) ** 2).sum() / (area * np.abs(a) ** 2).sum())))
+        line[f"max_rel_err_surface_{other}_vs_fp64"] = err
+        line[f"{other}_over_fp64"] = line["fp64"]["ms_per_frequency"] / line[other]["ms_per_frequency"]
     print(json.dumps(line), flush=True)
 
 
@@ -594,6 +600,8 @@ def main():
                          "c4: 64-frequency sweeps on icospheres s4/s5; "
                          "serve: the serving loop on a seeded Poisson horn stream")
     ap.add_argument("--c3-cases", default="", help="c3/c4: comma-separated case indices (default: all)")
+    ap.add_argument("--c2-forms", default="fp64,mixed,fmm64",
+                    help="C2 forms: fp64 and mixed dense, fmm64 the FP64 fast-multipole form")
     ap.add_argument("--c3-forms", default="fp64,mixed", help="c3: forms to run (the error needs both)")
     ap.add_argument("--serve-requests", type=int, default=60)
     ap.add_argument("--serve-rate", type=float, default=1.0, help="mean arrivals per second")

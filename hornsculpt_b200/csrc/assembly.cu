@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
                                                           const uint2 *__restrict__ bins,
                                                           const uint32_t *__restrict__ binCounts, size_t binCapacity,
                                                           const uint64_t *__restrict__ binOffsets, int bin,
-                                                          double *__restrict__ records, int *error) {
+                                                          double *__restrict__ records, SlotMap map, int *error) {
     constexpr int PPC = 192 / NP;
     constexpr int RO = ruleOffset<NP>();
     __shared__ double sS[192][18];
@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
     const double k = ks[f], invk = 1.0 / k;
     const uint32_t count = binCounts[f * kBins + bin];
     const uint2 *list = bins + binStart(binOffsets, binCapacity, f, bin);
-    double *rec = records + size_t(f) * T * T * kRecordDoubles;
+    double *rec = records + size_t(f) * map.planeSlots * kRecordDoubles;
     const int l = threadIdx.x / NP, x = threadIdx.x % NP;
     for (uint32_t base = blockIdx.x * PPC; base < count; base += gridDim.x * PPC) {
         const uint32_t p = base + l;
@@ -205,11 +205,15 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
             const uint2 pr = list[base + pl];
             double re, im;
             pairRecordValue(o, &sM[pl][0], &sM[pl][18], &sM[pl][36], panels[pr.x], panels[pr.y], k, invk, re, im);
-            const size_t slot = o < 12 ? size_t(pr.y) * T + pr.x : size_t(pr.x) * T + pr.y;
+            const size_t slot = o < 12 ? mapSlot(map, T, pr.x, pr.y) : mapSlot(map, T, pr.y, pr.x);
             const int e = o < 12 ? o : o - 12;
-            double *dst = rec + recordOffset(T, slot, e);
             if (!isfinite(re) || !isfinite(im))
                 flagError(error, kErrNonFinite);
+            if (slot == kNoSlot) {
+                flagError(error, kErrEscapedPlan);
+                continue;
+            }
+            double *dst = rec + mapOffset(map.planeSlots, slot, e);
             dst[0] = re;
             dst[1] = im;
         }
@@ -551,6 +555,55 @@ __global__ void binOffsetsKernel(uint32_t *binCounts, uint64_t *binOffsets, uint
     }
 }
 
+// The classification of classifyPairsKernel for a list of unordered pairs
+// (i < j): the fast-multipole near field, whose records are only those of the
+// near support pairs. Appends warp-aggregated like the full enumeration.
+__global__ void classifyListKernel(const uint2 *__restrict__ list, uint64_t count, const uint8_t *__restrict__ pairCode,
+                                   const Bounds *__restrict__ bounds, const double *__restrict__ ks, uint32_t B,
+                                   double tol, uint32_t minDegree, uint2 *bins, uint32_t *binCounts,
+                                   size_t binCapacity, int *error) {
+    const unsigned lane = threadIdx.x & 31;
+    const uint64_t padded = (count + 31) / 32 * 32;
+    for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < padded; q += uint64_t(gridDim.x) * blockDim.x) {
+        uint8_t code = kPairTouching;
+        uint2 pr = make_uint2(0, 0);
+        Bounds bi{}, bj{};
+        if (q < count) {
+            pr = list[q];
+            code = pairCode[uint64_t(pr.y) * (pr.y - 1) / 2 + pr.x];
+            if (code == kPairRegular) {
+                bi = bounds[pr.x];
+                bj = bounds[pr.y];
+            }
+        }
+        for (uint32_t f = 0; f < B; ++f) {
+            int bin = -1;
+            if (code == kPairWhole8)
+                bin = 2;
+            else if (code == kPairWhole14)
+                bin = 3;
+            else if (code == kPairRegular) {
+                const unsigned d = qualifiedDegree(bi, bj, ks[f], tol, minDegree);
+                bin = d == 4 ? 0 : d == 6 ? 1 : d == 8 ? 2 : -1;
+                if (bin < 0)
+                    flagError(error, kErrEscapedPlan);
+            }
+#pragma unroll
+            for (int b = 0; b < kBins; ++b) {
+                const unsigned mask = __ballot_sync(0xffffffffu, bin == b);
+                if (!mask)
+                    continue;
+                uint32_t start = 0;
+                if (lane == unsigned(__ffs(mask) - 1))
+                    start = atomicAdd(&binCounts[f * kBins + b], uint32_t(__popc(mask)));
+                start = __shfl_sync(0xffffffffu, start, __ffs(mask) - 1);
+                if (bin == b)
+                    bins[(size_t(f) * kBins + b) * binCapacity + start + __popc(mask & ((1u << lane) - 1))] = pr;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Touching pairs (cuda_solver.cu:382-429): one CTA per ordered job, threads
 // over (sector, u, v, w), the radial Gauss variable factored out because
@@ -619,7 +672,7 @@ __global__ void __launch_bounds__(128) singularKernel(const DPanel *__restrict__
                                                       const TouchingJob *__restrict__ jobs,
                                                       const double *__restrict__ ks,
                                                       const double *__restrict__ gauss, uint32_t order,
-                                                      double *__restrict__ records, int *error) {
+                                                      double *__restrict__ records, SlotMap map, int *error) {
     __shared__ double red[4][26];
     const TouchingJob job = jobs[blockIdx.x];
     const int f = blockIdx.y;
@@ -698,9 +751,14 @@ __global__ void __launch_bounds__(128) singularKernel(const DPanel *__restrict__
         }
         if (!isfinite(re) || !isfinite(im))
             flagError(error, kErrNonFinite);
-        double *dst = records + size_t(f) * T * T * kRecordDoubles + recordOffset(T, size_t(job.trial) * T + job.test, o);
-        dst[0] = re;
-        dst[1] = im;
+        const size_t slot = mapSlot(map, T, job.test, job.trial);
+        if (slot == kNoSlot)
+            flagError(error, kErrEscapedPlan);
+        else {
+            double *dst = records + size_t(f) * map.planeSlots * kRecordDoubles + mapOffset(map.planeSlots, slot, o);
+            dst[0] = re;
+            dst[1] = im;
+        }
     }
 }
 
@@ -960,7 +1018,7 @@ __global__ void __launch_bounds__(64, Mixed ? 10 : 1) nearWarpKernel(const DPane
                                                       const NearPairJob *__restrict__ jobs, uint32_t jobCount,
                                                       const Patch *__restrict__ patches, const double *__restrict__ ks,
                                                       std::conditional_t<Mixed, float, double> *__restrict__ records,
-                                                      int *error) {
+                                                      SlotMap map, int *error) {
     using Acc = std::conditional_t<Mixed, float, double>;
     __shared__ Acc sS[2][64][18];     // per warp: trial-contracted values S(x)
     __shared__ double sB[2][64][3];   // per warp: mapped test barycentrics
@@ -1072,11 +1130,14 @@ __global__ void __launch_bounds__(64, Mixed ? 10 : 1) nearWarpKernel(const DPane
         pairRecordValue(o, &sM[warp][0], &sM[warp][18], &sM[warp][36], t, s, k, invk, re, im);
         if (!isfinite(re) || !isfinite(im))
             flagError(error, kErrNonFinite);
-        const size_t slot = o < 12 ? size_t(job.second) * T + job.first : size_t(job.first) * T + job.second;
+        const size_t slot = o < 12 ? mapSlot(map, T, job.first, job.second) : mapSlot(map, T, job.second, job.first);
         const int e = o < 12 ? o : o - 12;
-        Acc *dst = records + size_t(f) * T * T * kRecordDoubles + recordOffset(T, slot, e);
-        dst[0] = Acc(re);
-        dst[1] = Acc(im);
+        if (slot != kNoSlot) {
+            Acc *dst = records + size_t(f) * map.planeSlots * kRecordDoubles + mapOffset(map.planeSlots, slot, e);
+            dst[0] = Acc(re);
+            dst[1] = Acc(im);
+        } else
+            flagError(error, kErrEscapedPlan);
     }
 }
 
@@ -1085,7 +1146,7 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
                                                   const NearPairJob *__restrict__ jobs,
                                                   const Patch *__restrict__ patches, const double *__restrict__ ks,
                                                   std::conditional_t<Mixed, float, double> *__restrict__ records,
-                                                  int *error) {
+                                                  SlotMap map, int *error) {
     using Acc = std::conditional_t<Mixed, float, double>;
     __shared__ double red[4][54];
     __shared__ double pts[2][64][3];
@@ -1168,11 +1229,14 @@ __global__ void __launch_bounds__(128) nearKernel(const DPanel *__restrict__ pan
         pairRecordValue(o, &red[0][0], &red[0][18], &red[0][36], t, s, k, invk, re, im);
         if (!isfinite(re) || !isfinite(im))
             flagError(error, kErrNonFinite);
-        const size_t slot = o < 12 ? size_t(job.second) * T + job.first : size_t(job.first) * T + job.second;
+        const size_t slot = o < 12 ? mapSlot(map, T, job.first, job.second) : mapSlot(map, T, job.second, job.first);
         const int e = o < 12 ? o : o - 12;
-        Acc *dst = records + size_t(f) * T * T * kRecordDoubles + recordOffset(T, slot, e);
-        dst[0] = Acc(re);
-        dst[1] = Acc(im);
+        if (slot != kNoSlot) {
+            Acc *dst = records + size_t(f) * map.planeSlots * kRecordDoubles + mapOffset(map.planeSlots, slot, e);
+            dst[0] = Acc(re);
+            dst[1] = Acc(im);
+        } else
+            flagError(error, kErrEscapedPlan);
     }
 }
 
@@ -1410,7 +1474,7 @@ int smCount() {
 
 template <int NP>
 void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, const AssemblyWorkspace &ws, int bin,
-                   int *error, cudaStream_t stream, KernelTimer *timer, bool mixed) {
+                   int *error, cudaStream_t stream, KernelTimer *timer, bool mixed, const SlotMap &map) {
     const char *names[kBins] = {"regular_q6", "regular_q12", "regular_q16", "regular_q64"};
     const char *mixedNames[kBins] = {"regular_mixed_q6", "regular_mixed_q12", "regular_mixed_q16",
                                      "regular_mixed_q64"};
@@ -1423,7 +1487,8 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
     } else {
         const dim3 grid(unsigned(smCount() * 6), B);
         regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
-                                                         ws.binOffsets, bin, static_cast<double *>(ws.records), error);
+                                                         ws.binOffsets, bin, static_cast<double *>(ws.records), map,
+                                                         error);
     }
     cudaCheck(cudaGetLastError(), "regular pair assembly launch");
 }
@@ -1516,16 +1581,27 @@ size_t assemblyWorkspaceBytes(uint32_t T, uint32_t N, uint32_t E, uint32_t B, bo
     return size_t(B) * (recordBytes(T, mixed) + columns + size_t(E) * 6 * T * 8 + bins + kBins * (4 + 8));
 }
 
-void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *gaussSingular, const double *flux,
-                   uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
-                   cudaStream_t stream, KernelTimer *timer, bool mixed) {
+namespace {
+// Pair records of B frequencies: classification into rule bins (all
+// unordered pairs, or the listed ones), then the regular, touching and near
+// kernels, every record stored at its slot of `map`.
+void computeRecords(const AssemblyGeometry &g, const double *ks, const double *gaussSingular, uint32_t B,
+                    const AssemblyWorkspace &ws, const SlotMap &map, const uint2 *pairList, uint64_t listCount,
+                    int *error, cudaStream_t stream, KernelTimer *timer, bool mixed) {
     const uint64_t pairs = uint64_t(g.T) * (g.T - 1) / 2;
-    if (g.N > 65535 || B > 65535 || E > 65535)
-        throw std::runtime_error("Dense assembly grid limits exceeded (more than 65535 vertices, frequencies or excitations).");
     double *recD = static_cast<double *>(ws.records);
     float *recF = static_cast<float *>(ws.records);
     cudaCheck(cudaMemsetAsync(ws.binCounts, 0, sizeof(uint32_t) * kBins * B, stream), "bin reset");
-    if (pairs) {
+    if (pairList) {
+        TimedScope scope(timer, "classify_pairs", stream);
+        if (listCount) {
+            const unsigned blocks = unsigned(std::min<uint64_t>((listCount + 255) / 256, uint64_t(smCount()) * 16));
+            classifyListKernel<<<blocks, 256, 0, stream>>>(pairList, listCount, g.pairCode, g.bounds, ks, B,
+                                                           g.nearTolerance, g.minimumDegree, ws.bins, ws.binCounts,
+                                                           ws.binCapacity, error);
+            cudaCheck(cudaGetLastError(), "pair list classification launch");
+        }
+    } else if (pairs) {
         TimedScope scope(timer, "classify_pairs", stream);
         const unsigned blocks = unsigned(std::min<uint64_t>((pairs + 255) / 256, uint64_t(smCount()) * 16));
         if (ws.binOffsets) {  // count, scan, fill
@@ -1539,10 +1615,10 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
                                                         ws.binOffsets, false, error);
         cudaCheck(cudaGetLastError(), "pair classification launch");
     }
-    launchRegular<6>(g, ks, B, ws, 0, error, stream, timer, mixed);
-    launchRegular<12>(g, ks, B, ws, 1, error, stream, timer, mixed);
-    launchRegular<16>(g, ks, B, ws, 2, error, stream, timer, mixed);
-    launchRegular<64>(g, ks, B, ws, 3, error, stream, timer, mixed);
+    launchRegular<6>(g, ks, B, ws, 0, error, stream, timer, mixed, map);
+    launchRegular<12>(g, ks, B, ws, 1, error, stream, timer, mixed, map);
+    launchRegular<16>(g, ks, B, ws, 2, error, stream, timer, mixed, map);
+    launchRegular<64>(g, ks, B, ws, 3, error, stream, timer, mixed, map);
     if (g.touchingCount) {
         TimedScope scope(timer, mixed ? "singular_mixed" : "singular", stream);
         if (mixed)
@@ -1550,7 +1626,8 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
                 g.panels, g.T, g.touching, g.touchingCount, ks, g.singularTable, g.singularOrder, recF, error);
         else
             singularKernel<<<dim3(g.touchingCount, B), 128, 0, stream>>>(g.panels, g.T, g.touching, ks,
-                                                                         gaussSingular, g.singularOrder, recD, error);
+                                                                         gaussSingular, g.singularOrder, recD, map,
+                                                                         error);
         cudaCheck(cudaGetLastError(), "singular assembly launch");
     }
     if (g.nearPairCount - g.projectedPairCount) {
@@ -1559,10 +1636,10 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         const dim3 grid((tensorPairs + 1) / 2, B);
         if (mixed)
             nearWarpKernel<true><<<grid, 64, 0, stream>>>(g.panels, g.T, g.nearPairs, tensorPairs, g.patches, ks,
-                                                          recF, error);
+                                                          recF, map, error);
         else
             nearWarpKernel<false><<<grid, 64, 0, stream>>>(g.panels, g.T, g.nearPairs, tensorPairs, g.patches, ks,
-                                                           recD, error);
+                                                           recD, map, error);
         cudaCheck(cudaGetLastError(), "near assembly launch");
     }
     if (g.projectedPairCount) {
@@ -1570,12 +1647,25 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
         const NearPairJob *projected = g.nearPairs + (g.nearPairCount - g.projectedPairCount);
         if (mixed)
             nearKernel<true><<<dim3(g.projectedPairCount, B), 128, 0, stream>>>(g.panels, g.T, projected, g.patches,
-                                                                                ks, recF, error);
+                                                                                ks, recF, map, error);
         else
             nearKernel<false><<<dim3(g.projectedPairCount, B), 128, 0, stream>>>(g.panels, g.T, projected, g.patches,
-                                                                                 ks, recD, error);
+                                                                                 ks, recD, map, error);
         cudaCheck(cudaGetLastError(), "projected near assembly launch");
     }
+}
+}  // namespace
+
+void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *gaussSingular, const double *flux,
+                   uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
+                   cudaStream_t stream, KernelTimer *timer, bool mixed) {
+    if (g.N > 65535 || B > 65535 || E > 65535)
+        throw std::runtime_error("Dense assembly grid limits exceeded (more than 65535 vertices, frequencies or excitations).");
+    SlotMap dense;
+    dense.planeSlots = size_t(g.T) * g.T;
+    computeRecords(g, ks, gaussSingular, B, ws, dense, nullptr, 0, error, stream, timer, mixed);
+    double *recD = static_cast<double *>(ws.records);
+    float *recF = static_cast<float *>(ws.records);
     const size_t columnBytes = size_t(3) * g.T * sizeof(double2);
     if (!gatherUsesColumns(g.T)) {
         TimedScope scope(timer, "gather_column", stream);
@@ -1637,6 +1727,132 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
                                                                            g.incLocal, g.rowScale, g.T, g.N, E, rhs);
     }
     cudaCheck(cudaGetLastError(), "rhs gather launch");
+}
+
+// ---------------------------------------------------------------------------
+// Fast-multipole near field: records of the near panel pairs only (SlotMap
+// over a panel-pair CSR), reduced into the near support-pair CSR values and
+// the near part of the right-hand side.
+// ---------------------------------------------------------------------------
+namespace {
+
+// vals[e] for entry e = (i, j) of the near CSR: rowScale_i (sum over the
+// panels a of star i and s of star j of block entry (la, lb) of record (a, s)
+// plus the P1 mass term of the panels holding both i and j). One warp per row.
+__global__ void nearValuesKernel(const double *__restrict__ records, SlotMap map, const uint32_t *__restrict__ nearRow,
+                                 const uint32_t *__restrict__ nearCol, const uint32_t *__restrict__ incOffsets,
+                                 const uint32_t *__restrict__ incPanel, const uint8_t *__restrict__ incLocal,
+                                 const DPanel *__restrict__ panels, const double *__restrict__ rowScale, uint32_t T,
+                                 uint32_t N, double2 *vals, int *error) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (i >= N)
+        return;
+    const double sc = rowScale[i];
+    for (uint32_t e = nearRow[i] + lane; e < nearRow[i + 1]; e += 32) {
+        const uint32_t j = nearCol[e];
+        double re = 0, im = 0;
+        for (uint32_t oa = incOffsets[i]; oa < incOffsets[i + 1]; ++oa) {
+            const uint32_t a = incPanel[oa];
+            const int la = incLocal[oa];
+            for (uint32_t os = incOffsets[j]; os < incOffsets[j + 1]; ++os) {
+                const size_t slot = mapSlot(map, T, a, incPanel[os]);
+                if (slot == kNoSlot) {
+                    flagError(error, kErrEscapedPlan);
+                    continue;
+                }
+                const double *r = records + mapOffset(map.planeSlots, slot, 3 * la + incLocal[os]);
+                re += r[0];
+                im += r[1];
+            }
+            const DPanel &p = panels[a];
+            if (p.nodes[0] == j || p.nodes[1] == j || p.nodes[2] == j)
+                re += p.area * (i == j ? 2.0 : 1.0) / 24.0;
+        }
+        vals[e] = make_double2(re * sc, im * sc);
+    }
+}
+
+// Near right-hand side: rhs_i = rowScale_i sum over near j, panels s of star j
+// (weight 1/3: a panel's flux is emitted through its three vertex supports)
+// and panels a of star i of rhs moment la of record (a, s) times q_s.
+__global__ void nearRhsKernel(const double *__restrict__ records, SlotMap map, const uint32_t *__restrict__ nearRow,
+                              const uint32_t *__restrict__ nearCol, const uint32_t *__restrict__ incOffsets,
+                              const uint32_t *__restrict__ incPanel, const uint8_t *__restrict__ incLocal,
+                              const double2 *__restrict__ flux, const double *__restrict__ rowScale, uint32_t T,
+                              uint32_t N, uint32_t E, double2 *rhs, int *error) {
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const uint32_t ex = blockIdx.y;
+    if (i >= N)
+        return;
+    const double2 *q = flux + size_t(ex) * T;
+    double re = 0, im = 0;
+    for (uint32_t e = nearRow[i] + lane; e < nearRow[i + 1]; e += 32) {
+        const uint32_t j = nearCol[e];
+        for (uint32_t os = incOffsets[j]; os < incOffsets[j + 1]; ++os) {
+            const uint32_t sp = incPanel[os];
+            const double2 qs = q[sp];
+            if (qs.x == 0 && qs.y == 0)
+                continue;
+            double mr = 0, mi = 0;
+            for (uint32_t oa = incOffsets[i]; oa < incOffsets[i + 1]; ++oa) {
+                const size_t slot = mapSlot(map, T, incPanel[oa], sp);
+                if (slot == kNoSlot) {
+                    flagError(error, kErrEscapedPlan);
+                    continue;
+                }
+                const double *r = records + mapOffset(map.planeSlots, slot, 9 + incLocal[oa]);
+                mr += r[0];
+                mi += r[1];
+            }
+            re += (mr * qs.x - mi * qs.y) / 3.0;
+            im += (mr * qs.y + mi * qs.x) / 3.0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0)
+        rhs[size_t(ex) * N + i] = make_double2(re * rowScale[i], im * rowScale[i]);
+}
+
+}  // namespace
+
+size_t nearFieldWorkspaceBytes(size_t pairSlots, uint64_t pairCount) {
+    return pairSlots * kRecordDoubles * 8 + kBins * pairCount * sizeof(uint2) + kBins * 16;
+}
+
+void assembleNearField(const AssemblyGeometry &g, const double *k, const double *gaussSingular, const double *flux,
+                       uint32_t E, const NearFieldLayout &nf, void *workspace, double *vals, double *rhsNear,
+                       int *error, cudaStream_t stream, KernelTimer *timer) {
+    char *w = static_cast<char *>(workspace);
+    AssemblyWorkspace ws{};
+    ws.records = w;
+    ws.bins = reinterpret_cast<uint2 *>(w + nf.pairSlots * kRecordDoubles * 8);
+    ws.binCounts = reinterpret_cast<uint32_t *>(w + nf.pairSlots * kRecordDoubles * 8 + kBins * nf.pairCount * sizeof(uint2));
+    ws.binCapacity = nf.pairCount;
+    ws.binOffsets = nullptr;
+    SlotMap map;
+    map.row = nf.pairRow;
+    map.col = nf.pairCol;
+    map.planeSlots = nf.pairSlots;
+    cudaCheck(cudaMemsetAsync(ws.records, 0, nf.pairSlots * kRecordDoubles * 8, stream), "near record reset");
+    computeRecords(g, k, gaussSingular, 1, ws, map, nf.pairList, nf.pairCount, error, stream, timer, false);
+    {
+        TimedScope scope(timer, "fmm_near_values", stream);
+        nearValuesKernel<<<(g.N * 32 + 255) / 256, 256, 0, stream>>>(
+            static_cast<const double *>(ws.records), map, nf.nearRow, nf.nearCol, g.incOffsets, g.incPanel,
+            g.incLocal, g.panels, g.rowScale, g.T, g.N, reinterpret_cast<double2 *>(vals), error);
+        cudaCheck(cudaGetLastError(), "near values launch");
+    }
+    {
+        TimedScope scope(timer, "fmm_near_rhs", stream);
+        nearRhsKernel<<<dim3((g.N * 32 + 255) / 256, E), 256, 0, stream>>>(
+            static_cast<const double *>(ws.records), map, nf.nearRow, nf.nearCol, g.incOffsets, g.incPanel,
+            g.incLocal, reinterpret_cast<const double2 *>(flux), g.rowScale, g.T, g.N, E,
+            reinterpret_cast<double2 *>(rhsNear), error);
+        cudaCheck(cudaGetLastError(), "near rhs launch");
+    }
 }
 
 }  // namespace hsb

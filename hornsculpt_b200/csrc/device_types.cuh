@@ -38,6 +38,35 @@ HS_HD size_t recordOffset(uint32_t T, size_t slot, int e) {
     return ((size_t(plane) * T * T + slot) * 3 + row) * 2;
 }
 
+// Stored (test, trial) slots of the record planes: all T*T ordered pairs
+// (row == nullptr, slot = trial * T + test) or, for the fast-multipole near
+// field, the pairs of a CSR over test panels (columns sorted), slot = the
+// CSR position. planeSlots: slots per plane (T*T or the CSR size).
+struct SlotMap {
+    const uint32_t *row = nullptr, *col = nullptr;
+    size_t planeSlots = 0;
+};
+constexpr size_t kNoSlot = ~size_t(0);
+HS_HD size_t mapSlot(const SlotMap &m, uint32_t T, uint32_t test, uint32_t trial) {
+    if (!m.row)
+        return size_t(trial) * T + test;
+    uint32_t lo = m.row[test], hi = m.row[test + 1];
+    const uint32_t end = hi;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (m.col[mid] < trial)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo < end && m.col[lo] == trial ? size_t(lo) : kNoSlot;
+}
+// Offset (in reals) of record element e of a slot in a plane set of planeSlots slots.
+HS_HD size_t mapOffset(size_t planeSlots, size_t slot, int e) {
+    const int plane = e < 9 ? e % 3 : 3, row = e < 9 ? e / 3 : e - 9;
+    return ((size_t(plane) * planeSlots + slot) * 3 + row) * 2;
+}
+
 // Device error word codes (cuda_solver.cu:705-715).
 enum DeviceError : int {
     kErrDistance = 1,      // zero or invalid source distance
@@ -144,6 +173,24 @@ bool gatherUsesColumns(uint32_t T);
 void assembleBatch(const AssemblyGeometry &geo, const double *ks, const double *gaussSingular, const double *flux,
                    uint32_t E, uint32_t B, const AssemblyWorkspace &ws, double *A, double *rhs, int *error,
                    cudaStream_t stream, class KernelTimer *timer, bool mixed = false);
+
+// Fast-multipole near field of one frequency (assembly.cu): the records of
+// the near panel pairs (pairRow/pairCol: CSR over test panels, pairList: the
+// unordered pairs i < j to classify), reduced into the near support-pair
+// values (nearRow/nearCol, row-equilibrated) and the near right-hand side
+// rhsNear[E][N] (row-equilibrated). The workspace holds
+// nearFieldWorkspaceBytes(pairSlots, pairCount) bytes.
+struct NearFieldLayout {
+    const uint32_t *pairRow, *pairCol;
+    size_t pairSlots;
+    const uint2 *pairList;
+    uint64_t pairCount;
+    const uint32_t *nearRow, *nearCol;
+};
+size_t nearFieldWorkspaceBytes(size_t pairSlots, uint64_t pairCount);
+void assembleNearField(const AssemblyGeometry &g, const double *k, const double *gaussSingular, const double *flux,
+                       uint32_t E, const NearFieldLayout &nf, void *workspace, double *vals, double *rhsNear,
+                       int *error, cudaStream_t stream, class KernelTimer *timer);
 
 // Batched dense LU (partial pivoting) and solves, complex column-major. The
 // pivot buffer holds luWorkspaceBytes(N, B): the LAPACK-style interchanges

@@ -173,14 +173,29 @@ __device__ void pointStrengths(const FmmPanel &P, uint32_t mask, int q, const do
     }
 }
 
+// Right-hand-side source: panel s's flux q_s emitted through the leaf's
+// vertex supports of s, 1/3 per support (channel 0).
+__device__ void fluxStrength(const FmmPanel &P, uint32_t panel, uint32_t mask, int q, const double2 *flux, double *x,
+                             double2 (&s)[6]) {
+    const double b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
+    const double w = cFmmRule[4 * q + 3] * P.area * double(__popc(mask)) / 3.0;
+    for (int d = 0; d < 3; ++d)
+        x[d] = P.v0[d] + b1 * P.e1[d] + b2 * P.e2[d];
+    const double2 qs = flux[panel];
+    s[0] = make_double2(w * qs.x, w * qs.y);
+    for (int c = 1; c < 6; ++c)
+        s[c] = make_double2(0, 0);
+}
+
 // P2M of the leaves of one level: M[c][n,m] = sum over points s_c conj(R_n^m(y - centre)).
 __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ panels,
                                                  const uint32_t *__restrict__ leaves, const uint32_t *__restrict__ itemStart,
                                                  const FmmItem *__restrict__ items, const double *__restrict__ centers,
                                                  const uint64_t *__restrict__ coefOffset, int p, double k,
-                                                 const double2 *__restrict__ pvec, double2 *M) {
+                                                 const double2 *__restrict__ pvec, double2 *M, int rhsMode) {
     extern __shared__ double smem[];
     const int P = p;
+    const int nch = rhsMode ? 1 : 6;
     const size_t td = tableDoubles(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *tables = smem;
@@ -206,7 +221,10 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
                 const FmmItem it = items[i0 + idx / kRulePts];
                 double x[3];
                 double2 s[6];
-                pointStrengths(panels[it.panel], it.mask, idx % kRulePts, pvec, x, s);
+                if (rhsMode)
+                    fluxStrength(panels[it.panel], it.panel, it.mask, idx % kRulePts, pvec, x, s);
+                else
+                    pointStrengths(panels[it.panel], it.mask, idx % kRulePts, pvec, x, s);
                 fillTable(mine, P, x[0] - c[0], x[1] - c[1], x[2] - c[2], k, lane);
                 if (lane < 6)
                     str[warp * 6 + lane] = s[lane];
@@ -216,13 +234,13 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
                 for (int w = 0; w < kWarps && base + w < points; ++w) {
                     const PointTable t = tableAt(tables + w * td, P);
                     const double2 R = solidR(t, n, m);
-                    for (int ch = 0; ch < 6; ++ch)
+                    for (int ch = 0; ch < nch; ++ch)
                         acc[ch] = cadd(acc[ch], cmulConj(R, str[w * 6 + ch]));
                 }
             __syncthreads();
         }
         if (kk < nc)
-            for (int ch = 0; ch < 6; ++ch)
+            for (int ch = 0; ch < nch; ++ch)
                 out[size_t(ch) * nc + kk] = acc[ch];
     }
 }
@@ -237,7 +255,8 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                                                        const double *__restrict__ wigner,
                                                        const uint64_t *__restrict__ wignerStart,
                                                        const double2 *__restrict__ coax,
-                                                       const uint64_t *__restrict__ coaxStart, int zeroFirst) {
+                                                       const uint64_t *__restrict__ coaxStart, int zeroFirst,
+                                                       int nch) {
     extern __shared__ double smem[];
     const int nin = (pin + 1) * (pin + 1), nout = (pout + 1) * (pout + 1);
     const int pmax = pin > pout ? pin : pout;
@@ -249,7 +268,7 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
     const uint32_t node = outNodes[blockIdx.x];
     double2 *out = outCoef + coefOffset[node];
     if (zeroFirst)
-        for (int i = threadIdx.x; i < 6 * nout; i += blockDim.x)
+        for (int i = threadIdx.x; i < nch * nout; i += blockDim.x)
             out[i] = make_double2(0, 0);
     __syncthreads();
     for (uint32_t li = linkStart[blockIdx.x]; li < linkStart[blockIdx.x + 1]; ++li) {
@@ -262,8 +281,8 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
             sincos(m * L.phi, &s, &c);
             eph[m] = make_double2(c, s);
         }
-        for (int c0 = 0; c0 < 6; c0 += chunkCh) {
-            const int cc = min(chunkCh, 6 - c0);
+        for (int c0 = 0; c0 < nch; c0 += chunkCh) {
+            const int cc = min(chunkCh, nch - c0);
             for (int i = threadIdx.x; i < cc * nin; i += blockDim.x)
                 a[i] = in[size_t(c0) * nin + i];
             __syncthreads();
@@ -457,6 +476,102 @@ __global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ pa
                 acc[a].x += w * bq[a] * s0.x + w * cw.y / k;
                 acc[a].y += w * bq[a] * s0.y - w * cw.x / k;
             }
+        }
+        if (lane == 0)
+            for (int a = 0; a < 3; ++a)
+                if ((item.mask >> a) & 1)
+                    far[item.inc[a]] = acc[a];
+    }
+}
+
+// L2P of the right-hand-side field S (channel 0): forms grad S (degree p + 1)
+// in shared memory, then one warp per item writes
+//   far[inc_a] = sum_q w phi_a (-S + (i / k) n . grad S)
+// (the far part of -S q - alpha K' q with alpha = -i / k).
+__global__ void __launch_bounds__(256) l2pRhsKernel(const FmmPanel *__restrict__ panels,
+                                                    const uint32_t *__restrict__ leaves,
+                                                    const uint32_t *__restrict__ itemStart,
+                                                    const FmmItem *__restrict__ items, const double *__restrict__ centers,
+                                                    const uint64_t *__restrict__ coefOffset, int p, double k,
+                                                    const double2 *__restrict__ Lcoef, double2 *far) {
+    extern __shared__ double smem[];
+    const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
+    const size_t td = tableDoubles(P);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2 *Ls = reinterpret_cast<double2 *>(smem);  // [nc]
+    double2 *Lg = Ls + nc;                            // [3][nd]: d/dx, d/dy, d/dz
+    double *tables = reinterpret_cast<double *>(Lg + 3 * nd);
+    const uint32_t leaf = leaves[blockIdx.x];
+    const double2 *L = Lcoef + coefOffset[leaf];
+    for (int i = threadIdx.x; i < nc; i += blockDim.x)
+        Ls[i] = L[i];
+    __syncthreads();
+    for (int kk = threadIdx.x; kk < nd; kk += blockDim.x) {
+        int n, m;
+        decode(kk, n, m);
+        const double2 z1 = coefAt(Ls, p, n + 1, m), z0 = coefAt(Ls, p, n - 1, m);
+        const double a1 = coefA(n + 1, m), a0 = coefA(n, m);
+        const double2 dz = make_double2(z1.x * a1 - z0.x * a0, z1.y * a1 - z0.y * a0);
+        const double2 u1 = coefAt(Ls, p, n + 1, m - 1), u0 = coefAt(Ls, p, n - 1, m - 1);
+        const double bm = coefBm(n + 1, m - 1), bp = coefBp(n - 1, m - 1);
+        const double2 dp = make_double2(u1.x * bm + u0.x * bp, u1.y * bm + u0.y * bp);
+        const double2 v1 = coefAt(Ls, p, n + 1, m + 1), v0 = coefAt(Ls, p, n - 1, m + 1);
+        const double cm = coefCm(n + 1, m + 1), cp = coefCp(n - 1, m + 1);
+        const double2 dm = make_double2(-(v1.x * cm + v0.x * cp), -(v1.y * cm + v0.y * cp));
+        // dx = (d+ + d-) / 2, dy = -i (d+ - d-) / 2
+        Lg[kk] = make_double2(0.5 * k * (dp.x + dm.x), 0.5 * k * (dp.y + dm.y));
+        Lg[nd + kk] = make_double2(0.5 * k * (dp.y - dm.y), -0.5 * k * (dp.x - dm.x));
+        Lg[2 * nd + kk] = make_double2(k * dz.x, k * dz.y);
+    }
+    __syncthreads();
+    const uint32_t i0 = itemStart[blockIdx.x], i1 = itemStart[blockIdx.x + 1];
+    const double *c = centers + 3 * size_t(leaf);
+    const PointTable t = tableAt(tables + warp * td, P);
+    for (uint32_t it = i0 + warp; it < i1; it += kWarps) {
+        const FmmItem item = items[it];
+        const FmmPanel &Pn = panels[item.panel];
+        double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+        for (int q = 0; q < kRulePts; ++q) {
+            const double b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
+            double x[3];
+            for (int d = 0; d < 3; ++d)
+                x[d] = Pn.v0[d] + b1 * Pn.e1[d] + b2 * Pn.e2[d];
+            fillTable(t, P, x[0] - c[0], x[1] - c[1], x[2] - c[2], k, lane);
+            double2 f[4];
+            for (int ch = 0; ch < 4; ++ch)
+                f[ch] = make_double2(0, 0);
+            for (int kk = lane; kk < nd; kk += 32) {
+                int n, m;
+                decode(kk, n, m);
+                const double2 R = solidR(t, n, m);
+                if (kk < nc)
+                    f[0] = cadd(f[0], cmul(Ls[kk], R));
+                for (int d = 0; d < 3; ++d)
+                    f[1 + d] = cadd(f[1 + d], cmul(Lg[d * nd + kk], R));
+            }
+            for (int ch = 0; ch < 4; ++ch)
+                for (int o = 16; o > 0; o >>= 1) {
+                    f[ch].x += __shfl_xor_sync(0xffffffffu, f[ch].x, o);
+                    f[ch].y += __shfl_xor_sync(0xffffffffu, f[ch].y, o);
+                }
+            __syncwarp();
+            double2 F[4];
+            for (int ch = 0; ch < 4; ++ch)
+                F[ch] = make_double2(k * f[ch].y, -k * f[ch].x);  // -i k * sums
+            double2 dn = make_double2(0, 0);
+            for (int d = 0; d < 3; ++d) {
+                dn.x += Pn.n[d] * F[1 + d].x;
+                dn.y += Pn.n[d] * F[1 + d].y;
+            }
+            // -S + (i / k) n.grad S
+            const double2 v = make_double2(-F[0].x - dn.y / k, -F[0].y + dn.x / k);
+            const double w = cFmmRule[4 * q + 3] * Pn.area;
+            const double bq[3] = {cFmmRule[4 * q], b1, b2};
+            for (int a = 0; a < 3; ++a)
+                if ((item.mask >> a) & 1) {
+                    acc[a].x += w * bq[a] * v.x;
+                    acc[a].y += w * bq[a] * v.y;
+                }
         }
         if (lane == 0)
             for (int a = 0; a < 3; ++a)
@@ -716,6 +831,45 @@ FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : 
         nearCol_.reserve(nearRow_[I.N]);
         for (uint32_t i = 0; i < I.N; ++i)
             nearCol_.insert(nearCol_.end(), rows[i].begin(), rows[i].end());
+    }
+    // near panel pairs: the panels of the stars of every near leaf pair, both orientations
+    {
+        std::vector<std::vector<uint32_t>> leafPanels(nodes.size());
+        for (uint32_t ln = 0; ln < nodes.size(); ++ln) {
+            if (!nodes[ln].leaf() || !nodes[ln].countP)
+                continue;
+            auto &ps = leafPanels[ln];
+            for (uint32_t q = nodes[ln].firstP; q < nodes[ln].firstP + nodes[ln].countP; ++q) {
+                const uint32_t v = tree_.pressureOrder[q];
+                for (uint32_t j = space.incOffsets[v]; j < space.incOffsets[v + 1]; ++j)
+                    ps.push_back(space.incPanel[j]);
+            }
+            std::sort(ps.begin(), ps.end());
+            ps.erase(std::unique(ps.begin(), ps.end()), ps.end());
+        }
+        std::vector<std::vector<uint32_t>> rows(I.T);
+        for (const auto &lk : tree_.ppNear)
+            for (uint32_t a : leafPanels[lk.target]) {
+                auto &r = rows[a];
+                r.insert(r.end(), leafPanels[lk.source].begin(), leafPanels[lk.source].end());
+                for (uint32_t b : leafPanels[lk.source])
+                    rows[b].push_back(a);
+            }
+        panelRow_.assign(I.T + 1, 0);
+        for (uint32_t a = 0; a < I.T; ++a) {
+            auto &r = rows[a];
+            std::sort(r.begin(), r.end());
+            r.erase(std::unique(r.begin(), r.end()), r.end());
+            panelRow_[a + 1] = panelRow_[a] + uint32_t(r.size());
+        }
+        panelCol_.reserve(panelRow_[I.T]);
+        for (uint32_t a = 0; a < I.T; ++a) {
+            for (uint32_t b : rows[a])
+                if (a < b)
+                    panelPairs_.emplace_back(a, b);
+            panelCol_.insert(panelCol_.end(), rows[a].begin(), rows[a].end());
+            std::vector<uint32_t>().swap(rows[a]);
+        }
     }
     // levels taking part in the far field
     I.lmin = levels;
@@ -1033,96 +1187,116 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
 
 void FmmOperator::applyFar(const double *p, size_t stride, uint32_t S, double *y, cudaStream_t stream,
                            KernelTimer *timer) {
+    for (uint32_t sys = 0; sys < S; ++sys)
+        run(p + sys * stride, false, y + size_t(sys) * impl_->N * 2, stream, timer);
+}
+
+void FmmOperator::applyFarRhs(const double *q, uint32_t S, double *y, cudaStream_t stream, KernelTimer *timer) {
+    for (uint32_t sys = 0; sys < S; ++sys)
+        run(q + size_t(sys) * impl_->T * 2, true, y + size_t(sys) * impl_->N * 2, stream, timer);
+}
+
+void FmmOperator::run(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer) {
     Impl &I = *impl_;
     const uint32_t N = I.N;
-    for (uint32_t sys = 0; sys < S; ++sys) {
-        const double2 *pv = reinterpret_cast<const double2 *>(p + sys * stride);
-        double2 *yv = reinterpret_cast<double2 *>(y + size_t(sys) * N * 2);
-        if (tree_.ppFar.empty()) {
-            fmmCheck(cudaMemsetAsync(yv, 0, size_t(N) * 16, stream), "zero far");
-            continue;
+    const double2 *pv = reinterpret_cast<const double2 *>(src);
+    double2 *yv = reinterpret_cast<double2 *>(y);
+    if (tree_.ppFar.empty()) {
+        fmmCheck(cudaMemsetAsync(yv, 0, size_t(N) * 16, stream), "zero far");
+        return;
+    }
+    const int nch = rhs ? 1 : 6;
+    const int levels = int(tree_.levels.size());
+    fmmCheck(cudaMemsetAsync(I.far.p, 0, 3 * size_t(I.T) * 16, stream), "zero contributions");
+    fmmCheck(cudaMemsetAsync(I.Lc.p, 0, I.coefTotal * 16, stream), "zero locals");
+    const auto smemTranslate = [&](int pin, int pout, int &chunk) {
+        const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1));
+        chunk = nch;
+        while (chunk > 1 && (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16 > 200 * 1024)
+            --chunk;
+        return (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16;
+    };
+    const auto translate = [&](Impl::DevPlan &d, int pin, int pout, const double2 *in, double2 *out, bool zero) {
+        if (!d.count)
+            return;
+        int chunk;
+        const size_t sm = smemTranslate(pin, pout, chunk);
+        fmmCheck(cudaFuncSetAttribute(translateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                 "translate smem");
+        translateKernel<<<d.count, 256, sm, stream>>>(d.out.as<uint32_t>(), d.start.as<uint32_t>(),
+                                                      d.links.as<TransLink>(), pin, pout, chunk, in, out,
+                                                      I.coefOffset.as<uint64_t>(), I.wigner.as<double>(),
+                                                      I.wignerStart.as<uint64_t>(), I.coax.as<double2>(),
+                                                      I.coaxStart.as<uint64_t>(), zero ? 1 : 0, nch);
+        fmmCheck(cudaGetLastError(), "translate launch");
+    };
+    {
+        TimedScope scope(timer, "fmm_p2m", stream);
+        for (int l = I.lmin; l < levels; ++l) {
+            const uint32_t leaves = uint32_t(I.leafNodes[l].size());
+            if (!leaves)
+                continue;
+            const int P = I.order[l];
+            const size_t td = tableDoubles(P);
+            const size_t sm = (kWarps * td) * 8 + kWarps * 6 * 16;
+            if (sm > kMaxShared)
+                throw Unsupported("Fast-multipole leaf order exceeds the shared-memory tables; refine the tree.");
+            fmmCheck(cudaFuncSetAttribute(p2mKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                     "p2m smem");
+            p2mKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
+                                                   I.dLeafStart[l].as<uint32_t>(), I.dItems.as<FmmItem>() + I.itemBase[l],
+                                                   I.centers.as<double>(), I.coefOffset.as<uint64_t>(), P, k_, pv,
+                                                   I.Mc.as<double2>(), rhs ? 1 : 0);
+            fmmCheck(cudaGetLastError(), "p2m launch");
         }
-        const int levels = int(tree_.levels.size());
-        fmmCheck(cudaMemsetAsync(I.far.p, 0, 3 * size_t(I.T) * 16, stream), "zero contributions");
-        fmmCheck(cudaMemsetAsync(I.Lc.p, 0, I.coefTotal * 16, stream), "zero locals");
-        const auto smemTranslate = [&](int pin, int pout, int &chunk) {
-            const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1));
-            chunk = 6;
-            while (chunk > 1 && (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16 > 200 * 1024)
-                --chunk;
-            return (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16;
-        };
-        const auto translate = [&](Impl::DevPlan &d, int pin, int pout, const double2 *in, double2 *out, bool zero) {
-            if (!d.count)
-                return;
-            int chunk;
-            const size_t sm = smemTranslate(pin, pout, chunk);
-            fmmCheck(cudaFuncSetAttribute(translateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
-                     "translate smem");
-            translateKernel<<<d.count, 256, sm, stream>>>(d.out.as<uint32_t>(), d.start.as<uint32_t>(),
-                                                          d.links.as<TransLink>(), pin, pout, chunk, in, out,
-                                                          I.coefOffset.as<uint64_t>(), I.wigner.as<double>(),
-                                                          I.wignerStart.as<uint64_t>(), I.coax.as<double2>(),
-                                                          I.coaxStart.as<uint64_t>(), zero ? 1 : 0);
-            fmmCheck(cudaGetLastError(), "translate launch");
-        };
-        {
-            TimedScope scope(timer, "fmm_p2m", stream);
-            for (int l = I.lmin; l < levels; ++l) {
-                const uint32_t leaves = uint32_t(I.leafNodes[l].size());
-                if (!leaves)
-                    continue;
-                const int P = I.order[l];
-                const size_t td = tableDoubles(P);
-                const size_t sm = (kWarps * td) * 8 + kWarps * 6 * 16;
-                if (sm > kMaxShared)
-                    throw Unsupported("Fast-multipole leaf order exceeds the shared-memory tables; refine the tree.");
-                fmmCheck(cudaFuncSetAttribute(p2mKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
-                         "p2m smem");
-                p2mKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
-                                                       I.dLeafStart[l].as<uint32_t>(), I.dItems.as<FmmItem>() + I.itemBase[l],
-                                                       I.centers.as<double>(), I.coefOffset.as<uint64_t>(), P, k_, pv,
-                                                       I.Mc.as<double2>());
-                fmmCheck(cudaGetLastError(), "p2m launch");
-            }
-        }
-        {
-            TimedScope scope(timer, "fmm_m2m", stream);
-            for (int l = levels - 2; l >= I.lmin; --l)
-                translate(I.dm2m[l], I.order[l + 1], I.order[l], I.Mc.as<double2>(), I.Mc.as<double2>(), true);
-        }
-        {
-            TimedScope scope(timer, "fmm_m2l", stream);
-            for (int l = I.lmin; l < levels; ++l)
-                translate(I.dm2l[l], I.order[l], I.order[l], I.Mc.as<double2>(), I.Lc.as<double2>(), false);
-        }
-        {
-            TimedScope scope(timer, "fmm_l2l", stream);
-            for (int l = I.lmin + 1; l < levels; ++l)
-                translate(I.dl2l[l], I.order[l - 1], I.order[l], I.Lc.as<double2>(), I.Lc.as<double2>(), false);
-        }
-        {
-            TimedScope scope(timer, "fmm_l2p", stream);
-            for (int l = I.lmin; l < levels; ++l) {
-                const uint32_t leaves = uint32_t(I.leafNodes[l].size());
-                if (!leaves)
-                    continue;
-                const int p = I.order[l], P = p + 1;
-                const size_t td = tableDoubles(P);
-                const size_t sm = (6 * size_t(p + 1) * (p + 1) + size_t(P + 1) * (P + 1)) * 16 + kWarps * td * 8;
-                if (sm > kMaxShared)
-                    throw Unsupported("Fast-multipole leaf order exceeds the shared-memory tables; refine the tree.");
+    }
+    {
+        TimedScope scope(timer, "fmm_m2m", stream);
+        for (int l = levels - 2; l >= I.lmin; --l)
+            translate(I.dm2m[l], I.order[l + 1], I.order[l], I.Mc.as<double2>(), I.Mc.as<double2>(), true);
+    }
+    {
+        TimedScope scope(timer, "fmm_m2l", stream);
+        for (int l = I.lmin; l < levels; ++l)
+            translate(I.dm2l[l], I.order[l], I.order[l], I.Mc.as<double2>(), I.Lc.as<double2>(), false);
+    }
+    {
+        TimedScope scope(timer, "fmm_l2l", stream);
+        for (int l = I.lmin + 1; l < levels; ++l)
+            translate(I.dl2l[l], I.order[l - 1], I.order[l], I.Lc.as<double2>(), I.Lc.as<double2>(), false);
+    }
+    {
+        TimedScope scope(timer, "fmm_l2p", stream);
+        for (int l = I.lmin; l < levels; ++l) {
+            const uint32_t leaves = uint32_t(I.leafNodes[l].size());
+            if (!leaves)
+                continue;
+            const int p = I.order[l], P = p + 1;
+            const size_t td = tableDoubles(P);
+            const size_t nc = size_t(p + 1) * (p + 1), nd = size_t(P + 1) * (P + 1);
+            const size_t sm = (rhs ? nc + 3 * nd : 6 * nc + nd) * 16 + kWarps * td * 8;
+            if (sm > kMaxShared)
+                throw Unsupported("Fast-multipole leaf order exceeds the shared-memory tables; refine the tree.");
+            if (rhs) {
+                fmmCheck(cudaFuncSetAttribute(l2pRhsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                         "l2p smem");
+                l2pRhsKernel<<<leaves, 256, sm, stream>>>(
+                    I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(), I.dLeafStart[l].as<uint32_t>(),
+                    I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(), I.coefOffset.as<uint64_t>(), p, k_,
+                    I.Lc.as<double2>(), I.far.as<double2>());
+            } else {
                 fmmCheck(cudaFuncSetAttribute(l2pKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                          "l2p smem");
                 l2pKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
-                                                       I.dLeafStart[l].as<uint32_t>(), I.dItems.as<FmmItem>() + I.itemBase[l],
-                                                       I.centers.as<double>(), I.coefOffset.as<uint64_t>(), p, k_,
-                                                       I.Lc.as<double2>(), I.far.as<double2>());
-                fmmCheck(cudaGetLastError(), "l2p launch");
+                                                       I.dLeafStart[l].as<uint32_t>(),
+                                                       I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(),
+                                                       I.coefOffset.as<uint64_t>(), p, k_, I.Lc.as<double2>(),
+                                                       I.far.as<double2>());
             }
-            starSumKernel<<<(N + 255) / 256, 256, 0, stream>>>(I.far.as<double2>(), I.incOff.as<uint32_t>(), N, yv);
-            fmmCheck(cudaGetLastError(), "star sum launch");
+            fmmCheck(cudaGetLastError(), "l2p launch");
         }
+        starSumKernel<<<(N + 255) / 256, 256, 0, stream>>>(I.far.as<double2>(), I.incOff.as<uint32_t>(), N, yv);
+        fmmCheck(cudaGetLastError(), "star sum launch");
     }
 }
 

@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 #include <memory>
+#include <utility>
 #include <vector>
 
 namespace hsb {
@@ -42,6 +43,15 @@ class FmmOperator {
     // y[s] = far part of the raw (not row-equilibrated) operator applied to
     // p[s] for S systems (complex, interleaved; system stride `stride` reals).
     void applyFar(const double *p, size_t stride, uint32_t S, double *y, cudaStream_t stream, KernelTimer *timer);
+    // y[s] = far part of the raw right-hand side -S q - alpha K' q for per-panel
+    // flux q[s] (T complex each): each panel's flux is emitted through its three
+    // vertex supports (1/3 each), so the near part pairs with it exactly.
+    void applyFarRhs(const double *q, uint32_t S, double *y, cudaStream_t stream, KernelTimer *timer);
+    // Near panel pairs: CSR over test panels (sorted trials) of every (a, s) with a
+    // vertex pair in a near support pair, and its unordered pairs a < s.
+    const std::vector<uint32_t> &nearPanelRow() const { return panelRow_; }
+    const std::vector<uint32_t> &nearPanelCol() const { return panelCol_; }
+    const std::vector<std::pair<uint32_t, uint32_t>> &nearPanelPairs() const { return panelPairs_; }
 
     const FmmTree &tree() const { return tree_; }
     const std::vector<FmmLevelInfo> &levels() const { return levelInfo_; }
@@ -56,7 +66,10 @@ class FmmOperator {
     FmmTree tree_;
     std::vector<FmmLevelInfo> levelInfo_;
     std::vector<uint32_t> nearRow_, nearCol_;
+    std::vector<uint32_t> panelRow_, panelCol_;
+    std::vector<std::pair<uint32_t, uint32_t>> panelPairs_;
     double k_ = 0;
+    void run(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer);
 };
 
 // The fast-multipole linear system of one frequency: A = N + R F, with N the
@@ -72,6 +85,13 @@ class FmmSystem {
     ~FmmSystem();
     // Near values from the row-equilibrated dense matrix (column-major N x N).
     void nearFromDense(const double *A, cudaStream_t stream, KernelTimer *timer);
+    // Device storage of the near values (CSR order of the operator's pattern),
+    // filled directly by the near-field assembly; device near CSR arrays.
+    double *nearValues();
+    const uint32_t *nearRowDevice() const;
+    const uint32_t *nearColDevice() const;
+    // b_s += rowScale * far_s for S systems (N complex each).
+    void addScaled(double *b, const double *far, uint32_t S, cudaStream_t stream);
     void factorBlocks(cudaStream_t stream, KernelTimer *timer);
     void apply(const double *x, size_t stride, uint32_t S, double *y, cudaStream_t stream, KernelTimer *timer);
     void precondition(const double *in, double *out, uint32_t S, cudaStream_t stream);

@@ -293,6 +293,26 @@ void FmmSystem::nearFromDense(const double *A, cudaStream_t stream, KernelTimer 
     sysCheck(cudaGetLastError(), "near gather launch");
 }
 
+static __global__ void addScaledKernel(double2 *b, const double2 *far, const double *rowScale, uint32_t N, size_t count) {
+    const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= count)
+        return;
+    const double s = rowScale[i % N];
+    b[i] = make_double2(b[i].x + s * far[i].x, b[i].y + s * far[i].y);
+}
+
+double *FmmSystem::nearValues() { return impl_->vals.as<double>(); }
+const uint32_t *FmmSystem::nearRowDevice() const { return impl_->rowStart.as<uint32_t>(); }
+const uint32_t *FmmSystem::nearColDevice() const { return impl_->cols.as<uint32_t>(); }
+
+void FmmSystem::addScaled(double *b, const double *far, uint32_t S, cudaStream_t stream) {
+    const size_t count = size_t(S) * impl_->N;
+    addScaledKernel<<<unsigned((count + 255) / 256), 256, 0, stream>>>(reinterpret_cast<double2 *>(b),
+                                                                       reinterpret_cast<const double2 *>(far),
+                                                                       impl_->rowScale, impl_->N, count);
+    sysCheck(cudaGetLastError(), "rhs far launch");
+}
+
 void FmmSystem::factorBlocks(cudaStream_t stream, KernelTimer *timer) {
     Impl &I = *impl_;
     TimedScope scope(timer, "fmm_block_jacobi", stream);

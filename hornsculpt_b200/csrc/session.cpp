@@ -549,8 +549,14 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     const cudaStream_t s = stream();
     const bool mixedForm = o.precision == HS_PRECISION_MIXED;
     const uint32_t restart = o.fmm_restart_length;
-    const uint32_t Bmax = chooseBatch(F, E, O, mixedForm, restart);
-    ensureWorkspace(Bmax, E, O, mixedForm, restart);
+    const bool fmmRequest = o.acceleration == HS_FAST_MULTIPOLE;
+    // The fast-multipole form runs one frequency at a time on its own sparse
+    // near-field workspace (no dense records or matrices).
+    const uint32_t Bmax = fmmRequest ? 1 : chooseBatch(F, E, O, mixedForm, restart);
+    if (fmmRequest)
+        ensureFmmWorkspace(o, E, O);
+    else
+        ensureWorkspace(Bmax, E, O, mixedForm, restart);
     if (O)
         cuda(cudaMemcpyAsync(dObservers_.as<void>(), observers.data(), observers.size() * 8, cudaMemcpyHostToDevice, s),
              "observer upload");
@@ -595,8 +601,9 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                              T > kExactBinsT ? dBinOffsets_.as<uint64_t>() : nullptr};
         const bool mixed = o.precision == HS_PRECISION_MIXED;
         const bool fmmForm = o.acceleration == HS_FAST_MULTIPOLE;
-        assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws, dA_.as<double>(),
-                      dRhs_.as<double>(), dError_.as<int>(), s, &timer_, mixed);
+        if (!fmmForm)
+            assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws,
+                          dA_.as<double>(), dRhs_.as<double>(), dError_.as<int>(), s, &timer_, mixed);
         cuda(cudaEventRecord(ev.assembled, s), "phase event");
         // the assembly error word is checked with the first residual norms
         const auto countWork = [&]() {
@@ -619,16 +626,15 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         std::vector<double> relative(size_t(B) * E, 0);
         const double target = mixed ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
         if (fmmForm) {
-            // Fast-multipole form: per frequency the near support pairs of the
-            // assembled matrix, block-Jacobi on the leaf blocks and GMRES on
-            // near + expansion far field (support_fmm_solve.cu:401-525).
+            // Fast-multipole form: per frequency the exact near support pairs
+            // (records of the near panel pairs only), the right-hand side as
+            // near part plus expansion far field, block-Jacobi on the leaf
+            // blocks and GMRES on near + expansion far field
+            // (support_fmm_solve.cu:401-525).
             FmmOperator &op = fmmOperator(o);
-            if (!fmmSystem_ || fmmSystemOp_ != &op) {
-                fmmSystem_.reset();
-                fmmSystem_ = std::make_unique<FmmSystem>(op, dRowScale_.as<double>(), dMass_.as<double>());
-                fmmSystemOp_ = &op;
-            }
-            cuda(cudaEventRecord(ev.factored, s), "phase event");
+            const NearFieldLayout layout{dPanelRow_.as<uint32_t>(), dPanelCol_.as<uint32_t>(), op.nearPanelCol().size(),
+                                         dPanelPairs_.as<uint2>(), op.nearPanelPairs().size(),
+                                         fmmSystem_->nearRowDevice(), fmmSystem_->nearColDevice()};
             const double expansionTolerance = std::clamp(.01 * target, 1e-10, 1e-6);
             const auto solveStart = Clock::now();
             std::vector<double> rel;
@@ -636,28 +642,29 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             for (uint32_t b = 0; b < B; ++b) {
                 checkCancel();
                 op.prepare(ks[b], expansionTolerance, s);
-                fmmSystem_->nearFromDense(dA_.as<double>() + size_t(b) * N * N * 2, s, &timer_);
+                // near support pairs and the near right-hand side from the near panel-pair records
+                double *rhsB = dRhs_.as<double>() + size_t(b) * E * N * 2;
+                const double *fluxB = dFlux_.as<double>() + size_t(b) * E * T * 2;
+                assembleNearField(geo, dKs_.as<double>() + b, dGauss_.as<double>(), fluxB, E, layout,
+                                  dNearWork_.as<void>(), fmmSystem_->nearValues(), rhsB, dError_.as<int>(), s, &timer_);
+                cuda(cudaEventRecord(ev.assembled, s), "phase event");
+                {
+                    TimedScope scope(&timer_, "fmm_rhs_far", s);
+                    op.applyFarRhs(fluxB, E, dCorr_.as<double>(), s, &timer_);
+                    fmmSystem_->addScaled(rhsB, dCorr_.as<double>(), E, s);
+                }
+                cuda(cudaEventRecord(ev.factored, s), "phase event");
                 fmmSystem_->factorBlocks(s, &timer_);
                 fmmSystem_->solve(dRhs_.as<double>() + size_t(b) * E * N * 2, dX_.as<double>() + size_t(b) * E * N * 2,
                                   E, target, o.fmm_restart_length, o.fmm_maximum_iterations, s, &timer_, rel, its);
-                for (uint32_t e = 0; e < E; ++e)
+                for (uint32_t e = 0; e < E; ++e) {
                     krylov[size_t(b) * E + e] = its[e];
+                    relative[size_t(b) * E + e] = rel[e];
+                }
             }
             cuda(cudaEventRecord(ev.solved, s), "phase event");
-            // the residual of the assembled operator, as the dense form reports it
-            std::vector<double> norms(2 * size_t(B) * E);
-            residualBatch(dA_.as<double>(), dRhs_.as<double>(), dX_.as<double>(), dMass_.as<double>(), N, B, E,
-                          dCorr_.as<double>(), dNorms_.as<double>(), s, &timer_);
-            cuda(cudaMemcpyAsync(norms.data(), dNorms_.as<void>(), norms.size() * 8, cudaMemcpyDeviceToHost, s),
-                 "residual norms");
-            cuda(cudaStreamSynchronize(s), "CUDA fast-multipole residual");
-            checkDeviceError("CUDA Galerkin assembly");
-            for (size_t q = 0; q < relative.size(); ++q) {
-                const double res = norms[2 * q], rhs = norms[2 * q + 1];
-                relative[q] = rhs > 0 ? res / rhs : (res == 0 ? 0 : std::numeric_limits<double>::infinity());
-                if (!std::isfinite(relative[q]) || relative[q] > 10 * target)
-                    throw NoConvergence("Fast-multipole solution misses the Burton-Miller residual tolerance.");
-            }
+            cuda(cudaStreamSynchronize(s), "CUDA fast-multipole solve");
+            checkDeviceError("CUDA Galerkin near-field assembly");
             float a = 0, c = 0;
             cuda(cudaEventElapsedTime(&a, ev.batch, ev.assembled), "phase time");
             cuda(cudaEventElapsedTime(&c, ev.factored, ev.solved), "phase time");
@@ -963,6 +970,45 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
     cuda(cudaMemcpyAsync(matrix, dA_.as<void>(), size_t(N) * N * 16, cudaMemcpyDeviceToHost, s), "matrix download");
     cuda(cudaMemcpyAsync(rhs, dRhs_.as<void>(), size_t(N) * 16, cudaMemcpyDeviceToHost, s), "rhs download");
     cuda(cudaStreamSynchronize(s), "CUDA synchronization");
+}
+
+void Session::ensureFmmWorkspace(const hs_numerics &o, uint32_t E, uint32_t O) {
+    const size_t T = space_.panels.size(), N = space_.vertices.size();
+    FmmOperator &op = fmmOperator(o);
+    if (!fmmSystem_ || fmmSystemOp_ != &op) {
+        fmmSystem_.reset();
+        fmmSystem_ = std::make_unique<FmmSystem>(op, dRowScale_.as<double>(), dMass_.as<double>());
+        fmmSystemOp_ = &op;
+        const cudaStream_t s = stream();
+        const auto put = [&](DeviceBuffer &b, const void *src, size_t bytes) {
+            b.ensure(std::max<size_t>(bytes, 16));
+            if (bytes)
+                cuda(cudaMemcpyAsync(b.as<void>(), src, bytes, cudaMemcpyHostToDevice, s), "near panel upload");
+        };
+        put(dPanelRow_, op.nearPanelRow().data(), op.nearPanelRow().size() * 4);
+        put(dPanelCol_, op.nearPanelCol().data(), op.nearPanelCol().size() * 4);
+        put(dPanelPairs_, op.nearPanelPairs().data(), op.nearPanelPairs().size() * 8);
+        cuda(cudaStreamSynchronize(s), "near panel upload");
+    }
+    dNearWork_.ensure(nearFieldWorkspaceBytes(op.nearPanelCol().size(), op.nearPanelPairs().size()));
+    dRhs_.ensure(E * N * 16);
+    dX_.ensure(E * N * 16);
+    dCorr_.ensure(E * N * 16);
+    dNorms_.ensure(2 * E * 8 + 2 * E * N * 8);
+    dBinCounts_.ensure(kBins * sizeof(uint32_t));
+    dKs_.ensure(8);
+    dFlux_.ensure(E * T * 16);
+    dObservers_.ensure(std::max<size_t>(O * 3 * 8, 16));
+    dPartials_.ensure(std::max<size_t>(fieldPartialsBytes(uint32_t(T), E, O, 1), 16));
+    dField_.ensure(std::max<size_t>(E * O * 16, 16));
+    dDegrees_.ensure(4);
+    size_t bytes = 0;
+    for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dMixedPanels_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_,
+                                  &dMass_, &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_,
+                                  &dNearWork_, &dPanelRow_, &dPanelCol_, &dPanelPairs_, &dRhs_, &dX_, &dCorr_, &dNorms_,
+                                  &dKs_, &dFlux_, &dObservers_, &dPartials_, &dField_, &dDegrees_})
+        bytes += b->bytes();
+    peakBytes_ = std::max(peakBytes_, bytes);
 }
 
 FmmOperator &Session::fmmOperator(const hs_numerics &o) {

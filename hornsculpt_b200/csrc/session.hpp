@@ -128,7 +128,8 @@ class Session {
     std::unique_ptr<FmmSystem> fmmSystem_;
     const FmmOperator *fmmSystemOp_ = nullptr;
     FmmTreeSettings fmmSettings_{};
-    DeviceBuffer dFmmIn_, dFmmOut_;
+    DeviceBuffer dFmmIn_, dFmmOut_, dNearWork_, dPanelRow_, dPanelCol_, dPanelPairs_;
+    void ensureFmmWorkspace(const hs_numerics &numerics, uint32_t E, uint32_t O);
 };
 
 // Device bytes of one solve of F frequencies on a mesh with T panels and N
