@@ -335,13 +335,13 @@ def run_c2(args):
 
     torch.cuda.set_device(0)
     stream = torch.cuda.Stream()
-    mesh = hs.meshes.exponential_horn()
+    mesh = hs.meshes.exponential_horn(h=args.c2_h) if args.c2_h else hs.meshes.exponential_horn()
     v = mesh.vertices[mesh.triangles]
     area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
     exc = [hs.BemExcitation("throat", [hs.FaceVelocity(hs.meshes.HORN_THROAT, 1.0)])]
     obs = [(0.0, 0.0, 1.0), (0.5, 0.0, 0.8), (0.0, 0.0, -1.0)]
-    line = {"workload": "C2 horn sweep (dense forms)", "mesh": "exponential horn r_t 25 mm, r_m 150 mm, L 300 mm, "
-            "wall 3 mm, h 7.15 mm, seed 0", "N": mesh.vertex_count, "T": mesh.triangle_count,
+    line = {"workload": "C2 horn sweep", "mesh": "exponential horn r_t 25 mm, r_m 150 mm, L 300 mm, "
+            f"wall 3 mm, h {1e3 * (args.c2_h or 0.00715):.2f} mm, seed 0", "N": mesh.vertex_count, "T": mesh.triangle_count,
             "frequencies": len(C2_FREQUENCIES), "range_hz": [200.0, 8000.0]}
     results = {}
     forms = [f for f in args.c2_forms.split(",") if f]
@@ -600,6 +600,8 @@ def main():
                          "c4: 64-frequency sweeps on icospheres s4/s5; "
                          "serve: the serving loop on a seeded Poisson horn stream")
     ap.add_argument("--c3-cases", default="", help="c3/c4: comma-separated case indices (default: all)")
+    ap.add_argument("--c2-h", type=float, default=0.0,
+                    help="C2 edge length in metres (0: 7.15 mm, the spec's lambda(8 kHz)/6)")
     ap.add_argument("--c2-forms", default="fp64,mixed,fmm64",
                     help="C2 forms: fp64 and mixed dense, fmm64 the FP64 fast-multipole form")
     ap.add_argument("--c3-forms", default="fp64,mixed", help="c3: forms to run (the error needs both)")

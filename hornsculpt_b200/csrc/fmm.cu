@@ -246,7 +246,10 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
 }
 
 // One translation per link into the CTA's output node, channels in chunks:
-// rotate the input to the link axis, coaxial translation, rotate back.
+// rotate the input to the link axis, coaxial translation, rotate back. A
+// thread owns one coefficient for every channel of the chunk, so each Wigner
+// and coaxial entry is read once per chunk; the azimuth phases are applied
+// when the input is staged and when the output is accumulated.
 __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restrict__ outNodes,
                                                        const uint32_t *__restrict__ linkStart,
                                                        const TransLink *__restrict__ links, int pin, int pout, int chunkCh,
@@ -277,72 +280,105 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
         const double *dtab = wigner + wignerStart[L.wclass];
         const double2 *ctab = coax + coaxStart[L.cclass];
         for (int m = threadIdx.x; m <= pmax; m += blockDim.x) {
-            double s, c;
-            sincos(m * L.phi, &s, &c);
-            eph[m] = make_double2(c, s);
+            double sn, cs;
+            sincos(m * L.phi, &sn, &cs);
+            eph[m] = make_double2(cs, sn);
         }
+        __syncthreads();
         for (int c0 = 0; c0 < nch; c0 += chunkCh) {
             const int cc = min(chunkCh, nch - c0);
-            for (int i = threadIdx.x; i < cc * nin; i += blockDim.x)
-                a[i] = in[size_t(c0) * nin + i];
-            __syncthreads();
-            // forward rotation: b[n, m'] = sum_m a[n, m] exp(i m phi) d^n[m, m']
+            // staged input with the azimuth phase: a[n, m] = in[n, m] exp(i m phi)
             for (int i = threadIdx.x; i < cc * nin; i += blockDim.x) {
                 const int ch = i / nin, kk = i - ch * nin;
+                int n, m;
+                decode(kk, n, m);
+                const double2 e = m >= 0 ? eph[m] : make_double2(eph[-m].x, -eph[-m].y);
+                a[ch * nin + kk] = cmul(in[size_t(c0 + ch) * nin + kk], e);
+            }
+            __syncthreads();
+            // forward rotation: b[n, m'] = sum_m a[n, m] d^n[m, m']
+            for (int kk = threadIdx.x; kk < nin; kk += blockDim.x) {
                 int n, mp;
                 decode(kk, n, mp);
+                const int w = 2 * n + 1, base = n * n;
                 const double *d = dtab + wignerOffset(n) + (mp + n);
-                const int w = 2 * n + 1;
-                double2 acc = make_double2(0, 0);
-                for (int m = -n; m <= n; ++m) {
-                    const double2 e = m >= 0 ? eph[m] : make_double2(eph[-m].x, -eph[-m].y);
-                    const double2 v = cmul(a[ch * nin + coefIndex(n, m)], e);
-                    const double dv = d[size_t(m + n) * w];
-                    acc.x += v.x * dv;
-                    acc.y += v.y * dv;
+                double2 acc[6];
+#pragma unroll
+                for (int ch = 0; ch < 6; ++ch)
+                    acc[ch] = make_double2(0, 0);
+                for (int j = 0; j < w; ++j) {
+                    const double dv = d[size_t(j) * w];
+#pragma unroll
+                    for (int ch = 0; ch < 6; ++ch)
+                        if (ch < cc) {
+                            const double2 v = a[ch * nin + base + j];
+                            acc[ch].x += v.x * dv;
+                            acc[ch].y += v.y * dv;
+                        }
                 }
-                b[ch * nin + kk] = acc;
+#pragma unroll
+                for (int ch = 0; ch < 6; ++ch)
+                    if (ch < cc)
+                        b[ch * nin + kk] = acc[ch];
             }
             __syncthreads();
             // coaxial translation per |m|: c[n', m] = sum_n C_|m|[n][n'] b[n, m]
-            for (int i = threadIdx.x; i < cc * nout; i += blockDim.x) {
-                const int ch = i / nout, kk = i - ch * nout;
+            for (int kk = threadIdx.x; kk < nout; kk += blockDim.x) {
                 int np, m;
                 decode(kk, np, m);
                 const int am = m < 0 ? -m : m;
-                double2 acc = make_double2(0, 0);
+                double2 acc[6];
+#pragma unroll
+                for (int ch = 0; ch < 6; ++ch)
+                    acc[ch] = make_double2(0, 0);
                 if (am <= pin) {
                     size_t off = 0;
                     for (int j = 0; j < am; ++j)
                         off += size_t(pin + 1 - j) * (pout + 1 - j);
-                    const double2 *C = ctab + off;
                     const int wo = pout + 1 - am;
+                    const double2 *C = ctab + off + (np - am);
                     for (int n = am; n <= pin; ++n) {
-                        const double2 cv = C[size_t(n - am) * wo + (np - am)];
-                        const double2 v = b[ch * nin + coefIndex(n, m)];
-                        acc = cadd(acc, cmul(cv, v));
+                        const double2 cv = C[size_t(n - am) * wo];
+                        const int src = n * n + n + m;
+#pragma unroll
+                        for (int ch = 0; ch < 6; ++ch)
+                            if (ch < cc)
+                                acc[ch] = cadd(acc[ch], cmul(cv, b[ch * nin + src]));
                     }
                 }
-                cbuf[ch * nout + kk] = acc;
+#pragma unroll
+                for (int ch = 0; ch < 6; ++ch)
+                    if (ch < cc)
+                        cbuf[ch * nout + kk] = acc[ch];
             }
             __syncthreads();
             // back rotation: out[n, m1] += exp(-i m1 phi) sum_m d^n[m1, m] c[n, m]
-            for (int i = threadIdx.x; i < cc * nout; i += blockDim.x) {
-                const int ch = i / nout, kk = i - ch * nout;
+            for (int kk = threadIdx.x; kk < nout; kk += blockDim.x) {
                 int n, m1;
                 decode(kk, n, m1);
-                const int w = 2 * n + 1;
+                const int w = 2 * n + 1, base = n * n;
                 const double *d = dtab + wignerOffset(n) + size_t(m1 + n) * w;
-                double2 acc = make_double2(0, 0);
-                for (int m = -n; m <= n; ++m) {
-                    const double2 v = cbuf[ch * nout + coefIndex(n, m)];
-                    const double dv = d[m + n];
-                    acc.x += v.x * dv;
-                    acc.y += v.y * dv;
+                double2 acc[6];
+#pragma unroll
+                for (int ch = 0; ch < 6; ++ch)
+                    acc[ch] = make_double2(0, 0);
+                for (int j = 0; j < w; ++j) {
+                    const double dv = d[j];
+#pragma unroll
+                    for (int ch = 0; ch < 6; ++ch)
+                        if (ch < cc) {
+                            const double2 v = cbuf[ch * nout + base + j];
+                            acc[ch].x += v.x * dv;
+                            acc[ch].y += v.y * dv;
+                        }
                 }
                 const double2 e = m1 >= 0 ? make_double2(eph[m1].x, -eph[m1].y) : eph[-m1];
-                const size_t o = size_t(c0 + ch) * nout + kk;
-                out[o] = cadd(out[o], cmul(acc, e));
+#pragma unroll
+                for (int ch = 0; ch < 6; ++ch)
+                    if (ch < cc) {
+                        const size_t o = size_t(c0 + ch) * nout + kk;
+                        out[o] = cadd(out[o], cmul(acc[ch], e));
+                    }
             }
             __syncthreads();
         }
