@@ -39,10 +39,11 @@ typedef enum hs_status {
     HS_E_NOCONVERGE = 4,  /* refinement or field-degree loop exhausted (cuda_solver.cu:1559-1565, 1792-1796) */
     HS_E_NOMEM = 5,       /* memory preflight (cuda_solver.cu:1161-1163, 1261-1264) */
     HS_E_CANCELLED = 6,   /* "BEM calculation cancelled." (cuda_solver.cu:49-52) */
-    HS_E_UNSUPPORTED = 7  /* sub-domain, baffle, axisymmetric or fast-multipole requests */
+    HS_E_UNSUPPORTED = 7  /* sub-domain, baffle, axisymmetric or mixed-precision fast-multipole requests */
 } hs_status;
 
 typedef enum hs_boundary { HS_WALL = 0, HS_DRIVEN = 1 } hs_boundary;   /* mesh.hpp:17 */
+/* HS_FAST_MULTIPOLE: FP64 support-tree FMM + GMRES (precision must be HS_PRECISION_FP64). */
 typedef enum hs_acceleration { HS_DENSE = 0, HS_FAST_MULTIPOLE = 1 } hs_acceleration; /* bem.hpp:38 */
 typedef enum hs_precision {
     HS_PRECISION_FP64 = 0,  /* plain form: the reference method evaluated entirely in FP64 */
