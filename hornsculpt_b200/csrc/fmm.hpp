@@ -92,6 +92,12 @@ class FmmSystem {
     const uint32_t *nearColDevice() const;
     // b_s += rowScale * far_s for S systems (N complex each).
     void addScaled(double *b, const double *far, uint32_t S, cudaStream_t stream);
+    // r_s = b_s - A x_s with the operator as currently prepared; relative[s] its
+    // mass-weighted norm over that of b_s.
+    void residual(const double *b, const double *x, uint32_t S, double *r, std::vector<double> &relative,
+                  cudaStream_t stream, KernelTimer *timer);
+    // x += d (reals values).
+    void add(double *x, const double *d, size_t reals, cudaStream_t stream);
     void factorBlocks(cudaStream_t stream, KernelTimer *timer);
     void apply(const double *x, size_t stride, uint32_t S, double *y, cudaStream_t stream, KernelTimer *timer);
     void precondition(const double *in, double *out, uint32_t S, cudaStream_t stream);

@@ -313,6 +313,28 @@ void FmmSystem::addScaled(double *b, const double *far, uint32_t S, cudaStream_t
     sysCheck(cudaGetLastError(), "rhs far launch");
 }
 
+void FmmSystem::residual(const double *b, const double *x, uint32_t S, double *r, std::vector<double> &relative,
+                         cudaStream_t stream, KernelTimer *timer) {
+    Impl &I = *impl_;
+    I.tmp.ensure(size_t(S) * I.N * 16);
+    I.norms.ensure(size_t(S) * 16);
+    apply(x, size_t(I.N) * 2, S, I.tmp.as<double>(), stream, timer);
+    residualNormKernel<<<S, 256, 0, stream>>>(reinterpret_cast<const double2 *>(b), I.tmp.as<double2>(), I.mass, I.N,
+                                              reinterpret_cast<double2 *>(r), I.norms.as<double>());
+    sysCheck(cudaGetLastError(), "residual launch");
+    std::vector<double> norms(2 * S);
+    sysCheck(cudaMemcpyAsync(norms.data(), I.norms.p, norms.size() * 8, cudaMemcpyDeviceToHost, stream), "norms");
+    sysCheck(cudaStreamSynchronize(stream), "residual");
+    relative.resize(S);
+    for (uint32_t s = 0; s < S; ++s)
+        relative[s] = norms[2 * s + 1] > 0 ? norms[2 * s] / norms[2 * s + 1] : 0.0;
+}
+
+void FmmSystem::add(double *x, const double *d, size_t reals, cudaStream_t stream) {
+    addKernel<<<unsigned((reals + 255) / 256), 256, 0, stream>>>(x, d, reals);
+    sysCheck(cudaGetLastError(), "add launch");
+}
+
 void FmmSystem::factorBlocks(cudaStream_t stream, KernelTimer *timer) {
     Impl &I = *impl_;
     TimedScope scope(timer, "fmm_block_jacobi", stream);
