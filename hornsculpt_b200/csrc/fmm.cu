@@ -250,9 +250,13 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
 // thread owns one coefficient for every channel of the chunk, so each Wigner
 // and coaxial entry is read once per chunk; the azimuth phases are applied
 // when the input is staged and when the output is accumulated.
+// The channels [blockIdx.y * CPC, +CPC) of the output node go to one CTA:
+// channels are independent outputs, so spreading them over CTAs multiplies
+// the grid (few output nodes on the coarse levels) with no reduction.
+template <int CPC>
 __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restrict__ outNodes,
                                                        const uint32_t *__restrict__ linkStart,
-                                                       const TransLink *__restrict__ links, int pin, int pout, int chunkCh,
+                                                       const TransLink *__restrict__ links, int pin, int pout,
                                                        const double2 *__restrict__ inCoef, double2 *outCoef,
                                                        const uint64_t *__restrict__ coefOffset,
                                                        const double *__restrict__ wigner,
@@ -260,6 +264,7 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                                                        const double2 *__restrict__ coax,
                                                        const uint64_t *__restrict__ coaxStart, int zeroFirst,
                                                        int nch) {
+    constexpr int chunkCh = CPC;
     extern __shared__ double smem[];
     const int nin = (pin + 1) * (pin + 1), nout = (pout + 1) * (pout + 1);
     const int pmax = pin > pout ? pin : pout;
@@ -269,9 +274,12 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
     double2 *b = a + size_t(chunkCh) * nmax;
     double2 *cbuf = b + size_t(chunkCh) * nmax;
     const uint32_t node = outNodes[blockIdx.x];
+    const int cFirst = blockIdx.y * CPC, cEnd = min(nch, cFirst + CPC);
+    if (cFirst >= nch)
+        return;
     double2 *out = outCoef + coefOffset[node];
     if (zeroFirst)
-        for (int i = threadIdx.x; i < nch * nout; i += blockDim.x)
+        for (int i = cFirst * nout + threadIdx.x; i < cEnd * nout; i += blockDim.x)
             out[i] = make_double2(0, 0);
     __syncthreads();
     for (uint32_t li = linkStart[blockIdx.x]; li < linkStart[blockIdx.x + 1]; ++li) {
@@ -285,8 +293,8 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
             eph[m] = make_double2(cs, sn);
         }
         __syncthreads();
-        for (int c0 = 0; c0 < nch; c0 += chunkCh) {
-            const int cc = min(chunkCh, nch - c0);
+        for (int c0 = cFirst; c0 < cEnd; c0 += chunkCh) {
+            const int cc = min(chunkCh, cEnd - c0);
             // staged input with the azimuth phase: a[n, m] = in[n, m] exp(i m phi)
             for (int i = threadIdx.x; i < cc * nin; i += blockDim.x) {
                 const int ch = i / nin, kk = i - ch * nin;
@@ -302,14 +310,14 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 decode(kk, n, mp);
                 const int w = 2 * n + 1, base = n * n;
                 const double *d = dtab + wignerOffset(n) + (mp + n);
-                double2 acc[6];
+                double2 acc[CPC];
 #pragma unroll
-                for (int ch = 0; ch < 6; ++ch)
+                for (int ch = 0; ch < CPC; ++ch)
                     acc[ch] = make_double2(0, 0);
                 for (int j = 0; j < w; ++j) {
                     const double dv = d[size_t(j) * w];
 #pragma unroll
-                    for (int ch = 0; ch < 6; ++ch)
+                    for (int ch = 0; ch < CPC; ++ch)
                         if (ch < cc) {
                             const double2 v = a[ch * nin + base + j];
                             acc[ch].x += v.x * dv;
@@ -317,7 +325,7 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                         }
                 }
 #pragma unroll
-                for (int ch = 0; ch < 6; ++ch)
+                for (int ch = 0; ch < CPC; ++ch)
                     if (ch < cc)
                         b[ch * nin + kk] = acc[ch];
             }
@@ -327,9 +335,9 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 int np, m;
                 decode(kk, np, m);
                 const int am = m < 0 ? -m : m;
-                double2 acc[6];
+                double2 acc[CPC];
 #pragma unroll
-                for (int ch = 0; ch < 6; ++ch)
+                for (int ch = 0; ch < CPC; ++ch)
                     acc[ch] = make_double2(0, 0);
                 if (am <= pin) {
                     size_t off = 0;
@@ -341,13 +349,13 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                         const double2 cv = C[size_t(n - am) * wo];
                         const int src = n * n + n + m;
 #pragma unroll
-                        for (int ch = 0; ch < 6; ++ch)
+                        for (int ch = 0; ch < CPC; ++ch)
                             if (ch < cc)
                                 acc[ch] = cadd(acc[ch], cmul(cv, b[ch * nin + src]));
                     }
                 }
 #pragma unroll
-                for (int ch = 0; ch < 6; ++ch)
+                for (int ch = 0; ch < CPC; ++ch)
                     if (ch < cc)
                         cbuf[ch * nout + kk] = acc[ch];
             }
@@ -358,14 +366,14 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 decode(kk, n, m1);
                 const int w = 2 * n + 1, base = n * n;
                 const double *d = dtab + wignerOffset(n) + size_t(m1 + n) * w;
-                double2 acc[6];
+                double2 acc[CPC];
 #pragma unroll
-                for (int ch = 0; ch < 6; ++ch)
+                for (int ch = 0; ch < CPC; ++ch)
                     acc[ch] = make_double2(0, 0);
                 for (int j = 0; j < w; ++j) {
                     const double dv = d[j];
 #pragma unroll
-                    for (int ch = 0; ch < 6; ++ch)
+                    for (int ch = 0; ch < CPC; ++ch)
                         if (ch < cc) {
                             const double2 v = cbuf[ch * nout + base + j];
                             acc[ch].x += v.x * dv;
@@ -374,7 +382,7 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 }
                 const double2 e = m1 >= 0 ? make_double2(eph[m1].x, -eph[m1].y) : eph[-m1];
 #pragma unroll
-                for (int ch = 0; ch < 6; ++ch)
+                for (int ch = 0; ch < CPC; ++ch)
                     if (ch < cc) {
                         const size_t o = size_t(c0 + ch) * nout + kk;
                         out[o] = cadd(out[o], cmul(acc[ch], e));
@@ -1245,25 +1253,31 @@ void FmmOperator::run(const double *src, bool rhs, double *y, cudaStream_t strea
     const int levels = int(tree_.levels.size());
     fmmCheck(cudaMemsetAsync(I.far.p, 0, 3 * size_t(I.T) * 16, stream), "zero contributions");
     fmmCheck(cudaMemsetAsync(I.Lc.p, 0, I.coefTotal * 16, stream), "zero locals");
-    const auto smemTranslate = [&](int pin, int pout, int &chunk) {
-        const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1));
-        chunk = nch;
-        while (chunk > 1 && (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16 > 200 * 1024)
-            --chunk;
-        return (size_t(3) * chunk * nmax + std::max(pin, pout) + 1) * 16;
-    };
+    // channels per CTA: enough CTAs for about four waves of 148 SMs, fewer
+    // (more reuse of each Wigner and coaxial entry) when the level has many nodes
     const auto translate = [&](Impl::DevPlan &d, int pin, int pout, const double2 *in, double2 *out, bool zero) {
         if (!d.count)
             return;
-        int chunk;
-        const size_t sm = smemTranslate(pin, pout, chunk);
-        fmmCheck(cudaFuncSetAttribute(translateKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
-                 "translate smem");
-        translateKernel<<<d.count, 256, sm, stream>>>(d.out.as<uint32_t>(), d.start.as<uint32_t>(),
-                                                      d.links.as<TransLink>(), pin, pout, chunk, in, out,
-                                                      I.coefOffset.as<uint64_t>(), I.wigner.as<double>(),
-                                                      I.wignerStart.as<uint64_t>(), I.coax.as<double2>(),
-                                                      I.coaxStart.as<uint64_t>(), zero ? 1 : 0, nch);
+        const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1));
+        int cpc = nch == 1 ? 1 : d.count >= 2400 ? 3 : d.count >= 1200 ? 2 : 1;
+        while (cpc > 1 && (size_t(3) * cpc * nmax + std::max(pin, pout) + 1) * 16 > 200 * 1024)
+            cpc = cpc == 3 ? 2 : 1;
+        const size_t sm = (size_t(3) * cpc * nmax + std::max(pin, pout) + 1) * 16;
+        const dim3 grid(d.count, unsigned((nch + cpc - 1) / cpc));
+        const auto launch = [&](auto kernel) {
+            fmmCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                     "translate smem");
+            kernel<<<grid, 256, sm, stream>>>(d.out.as<uint32_t>(), d.start.as<uint32_t>(), d.links.as<TransLink>(),
+                                              pin, pout, in, out, I.coefOffset.as<uint64_t>(), I.wigner.as<double>(),
+                                              I.wignerStart.as<uint64_t>(), I.coax.as<double2>(),
+                                              I.coaxStart.as<uint64_t>(), zero ? 1 : 0, nch);
+        };
+        if (cpc == 3)
+            launch(translateKernel<3>);
+        else if (cpc == 2)
+            launch(translateKernel<2>);
+        else
+            launch(translateKernel<1>);
         fmmCheck(cudaGetLastError(), "translate launch");
     };
     {
