@@ -75,13 +75,15 @@ class FmmOperator {
 // The fast-multipole linear system of one frequency: A = N + R F, with N the
 // exact near support-pair entries (CSR of the operator's pattern), F the far
 // expansion operator and R = 1 / lumped mass the row equilibration. Solved by
-// restarted GMRES (CGS2, Givens) left-preconditioned by block Jacobi on the
-// leaves' diagonal blocks of N (SupportBlockJacobi,
+// restarted GMRES (CGS2, Givens) left-preconditioned by block Jacobi on
+// spatially ordered diagonal blocks of N (SupportBlockJacobi,
 // cuda/support_preconditioner.cu:33-191: spatially ordered diagonal blocks of
 // the near matrix, inverted once per frequency).
 class FmmSystem {
   public:
-    FmmSystem(FmmOperator &op, const double *rowScale, const double *mass);
+    // blockWidth: supports per preconditioner block (at most 64); consecutive
+    // leaves in tree order are merged up to it.
+    FmmSystem(FmmOperator &op, const double *rowScale, const double *mass, uint32_t blockWidth);
     ~FmmSystem();
     // Near values from the row-equilibrated dense matrix (column-major N x N).
     void nearFromDense(const double *A, cudaStream_t stream, KernelTimer *timer);

@@ -244,7 +244,7 @@ struct FmmSystem::Impl {
     uint32_t gmresS = 0, gmresM = 0;
 };
 
-FmmSystem::FmmSystem(FmmOperator &op, const double *rowScale, const double *mass)
+FmmSystem::FmmSystem(FmmOperator &op, const double *rowScale, const double *mass, uint32_t blockWidth)
     : impl_(std::make_unique<Impl>()), op_(op) {
     Impl &I = *impl_;
     const auto &row = op.nearRowStart();
@@ -255,22 +255,34 @@ FmmSystem::FmmSystem(FmmOperator &op, const double *rowScale, const double *mass
     I.rowStart.upload(row, s);
     I.cols.upload(op.nearCols(), s);
     I.vals.ensure(std::max<size_t>(op.nearCols().size(), 1) * 16);
-    // diagonal blocks: each leaf's pressure supports (split above kMaxBlock)
+    // diagonal blocks: consecutive leaves in tree order (spatially adjacent)
+    // merged up to the block width, a leaf above it split
     const FmmTree &t = op.tree();
+    const uint32_t width = std::clamp<uint32_t>(blockWidth, 1, kMaxBlock);
     std::vector<uint32_t> bs{0}, bv;
     std::vector<uint64_t> is{0};
+    std::vector<uint32_t> cur;
+    const auto flush = [&]() {
+        if (cur.empty())
+            return;
+        std::sort(cur.begin(), cur.end());
+        bv.insert(bv.end(), cur.begin(), cur.end());
+        bs.push_back(uint32_t(bv.size()));
+        is.push_back(is.back() + uint64_t(cur.size()) * cur.size());
+        cur.clear();
+    };
     for (const auto &n : t.nodes) {
         if (!n.leaf() || !n.countP)
             continue;
-        for (uint32_t q0 = 0; q0 < n.countP; q0 += kMaxBlock) {
-            const uint32_t q1 = std::min(n.countP, q0 + kMaxBlock);
-            std::vector<uint32_t> vs(t.pressureOrder.begin() + n.firstP + q0, t.pressureOrder.begin() + n.firstP + q1);
-            std::sort(vs.begin(), vs.end());
-            bv.insert(bv.end(), vs.begin(), vs.end());
-            bs.push_back(uint32_t(bv.size()));
-            is.push_back(is.back() + uint64_t(vs.size()) * vs.size());
+        if (cur.size() + n.countP > width)
+            flush();
+        for (uint32_t q = 0; q < n.countP; ++q) {
+            cur.push_back(t.pressureOrder[n.firstP + q]);
+            if (cur.size() == width)
+                flush();
         }
     }
+    flush();
     if (bv.size() != I.N)
         throw std::logic_error("fast multipole: leaf blocks do not cover the vertices");
     I.blocks = uint32_t(bs.size() - 1);

@@ -635,6 +635,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             const NearFieldLayout layout{dPanelRow_.as<uint32_t>(), dPanelCol_.as<uint32_t>(), op.nearPanelCol().size(),
                                          dPanelPairs_.as<uint2>(), op.nearPanelPairs().size(),
                                          fmmSystem_->nearRowDevice(), fmmSystem_->nearColDevice()};
+            // working expansions at 1 % of the target (the audit checks them against
+            // expansions ten times finer)
             const double expansionTolerance = std::clamp(.01 * target, 1e-10, 1e-6);
             const auto solveStart = Clock::now();
             std::vector<double> rel;
@@ -1021,9 +1023,11 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
 void Session::ensureFmmWorkspace(const hs_numerics &o, uint32_t E, uint32_t O) {
     const size_t T = space_.panels.size(), N = space_.vertices.size();
     FmmOperator &op = fmmOperator(o);
-    if (!fmmSystem_ || fmmSystemOp_ != &op) {
+    if (!fmmSystem_ || fmmSystemOp_ != &op || fmmBlockWidth_ != o.fmm_preconditioner_block_width) {
         fmmSystem_.reset();
-        fmmSystem_ = std::make_unique<FmmSystem>(op, dRowScale_.as<double>(), dMass_.as<double>());
+        fmmBlockWidth_ = o.fmm_preconditioner_block_width;
+        fmmSystem_ = std::make_unique<FmmSystem>(op, dRowScale_.as<double>(), dMass_.as<double>(),
+                                                 o.fmm_preconditioner_block_width);
         fmmSystemOp_ = &op;
         const cudaStream_t s = stream();
         const auto put = [&](DeviceBuffer &b, const void *src, size_t bytes) {

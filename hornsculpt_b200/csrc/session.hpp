@@ -127,6 +127,7 @@ class Session {
     std::unique_ptr<FmmOperator> fmm_;
     std::unique_ptr<FmmSystem> fmmSystem_;
     const FmmOperator *fmmSystemOp_ = nullptr;
+    uint32_t fmmBlockWidth_ = 0;
     FmmTreeSettings fmmSettings_{};
     DeviceBuffer dFmmIn_, dFmmOut_, dNearWork_, dPanelRow_, dPanelCol_, dPanelPairs_, dAuditWork_, dAuditFine_;
     void ensureFmmWorkspace(const hs_numerics &numerics, uint32_t E, uint32_t O);
