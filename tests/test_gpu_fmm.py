@@ -67,3 +67,49 @@ def test_fast_multipole_solve_matches_dense(case, freqs):
         assert ef.iterations > 0
         assert ef.boundary_residual <= 1e-6
         assert trace < 1e-5 and field < 1e-5
+
+
+def _fmm(tol=1e-7, **kw):
+    return hs.BemNumerics(precision="fp64", acceleration="fast_multipole", relative_residual_tolerance=tol, **kw)
+
+
+def test_all_near_partition_equals_dense():
+    """A mesh whose support tree has no far pairs: the fast-multipole form is the
+    exact near matrix plus GMRES, so it meets the dense solve to the GMRES target."""
+    mesh = meshes.icosphere(1)
+    req = lambda n: hs.BemRequest(frequencies=[800.0], observers=[(0, 0, 0.5)],
+                                  excitations=[hs.BemExcitation("u", [hs.FaceVelocity(1, 1.0)])], numerics=n)
+    with hs.CudaBemSolver(mesh) as solver:
+        far, row, cols, levels = solver.debug_fmm_far(FP64, 2 * np.pi * 800 / 343, 1e-8, np.ones(mesh.vertex_count))
+        dense = solver.solve(req(hs.BemNumerics(precision="fp64", relative_residual_tolerance=1e-7)))
+        fmm = solver.solve(req(_fmm()))
+    assert len(levels) == 0 and np.all(far == 0) and len(cols) == mesh.vertex_count ** 2
+    a, b = dense.frequencies[0].excitations[0], fmm.frequencies[0].excitations[0]
+    assert np.linalg.norm(b.boundary.pressure_trace - a.boundary.pressure_trace) < 1e-6 * np.linalg.norm(
+        a.boundary.pressure_trace)
+
+
+def test_two_excitations_and_repeatability():
+    """Two excitations solved together equal each solved alone, and a repeated solve
+    agrees far inside the solver tolerance (the form is not bitwise repeatable: a
+    repeat differs at about 1e-9 relative)."""
+    mesh = meshes.exponential_horn(h=0.0128, seed=5)
+    throat = hs.BemExcitation("throat", [hs.FaceVelocity(meshes.HORN_THROAT, 1.0)])
+    rng = np.random.default_rng(3)
+    faces = sorted(set(int(f) for f in mesh.face_ids))
+    other = hs.BemExcitation("mix", [hs.FaceVelocity(f, complex(rng.normal(), rng.normal())) for f in faces
+                                     if f == meshes.HORN_THROAT])
+    req = lambda ex: hs.BemRequest(frequencies=[700.0, 2100.0], observers=[(0, 0, 0.5)], excitations=ex,
+                                   numerics=_fmm(1e-6))
+    with hs.CudaBemSolver(mesh) as solver:
+        both = solver.solve(req([throat, other]))
+        again = solver.solve(req([throat, other]))
+        alone = solver.solve(req([other]))
+    for f in range(2):
+        for e in range(2):
+            a = both.frequencies[f].excitations[e].boundary.pressure_trace
+            b = again.frequencies[f].excitations[e].boundary.pressure_trace
+            assert np.linalg.norm(a - b) <= 1e-7 * np.linalg.norm(a)
+        t2, t1 = both.frequencies[f].excitations[1].boundary.pressure_trace, \
+            alone.frequencies[f].excitations[0].boundary.pressure_trace
+        assert np.linalg.norm(t2 - t1) < 5e-6 * np.linalg.norm(t1)
