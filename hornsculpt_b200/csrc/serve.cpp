@@ -176,8 +176,10 @@ std::vector<std::shared_ptr<Server::Job>> Server::takeGroup(size_t &footprint) {
         const bool mixed = o.precision == HS_PRECISION_MIXED;
         const uint32_t E = uint32_t(head->request.base.excitation_count), O = uint32_t(head->request.base.observer_count);
         uint32_t B = uint32_t(std::min<size_t>(freqs.size(), options_.max_batch_frequencies));
-        size_t need = solveFootprint(T, N, E, O, B, mixed, o.fmm_restart_length);
-        while (B > 1 && need > budget_) {
+        const bool fmm = o.acceleration == HS_FAST_MULTIPOLE;
+        size_t need = fmm ? fmmSolveFootprint(T, N, E, O, o.fmm_restart_length)
+                          : solveFootprint(T, N, E, O, B, mixed, o.fmm_restart_length);
+        while (!fmm && B > 1 && need > budget_) {
             B = (B + 1) / 2;
             need = solveFootprint(T, N, E, O, B, mixed, o.fmm_restart_length);
         }

@@ -329,6 +329,17 @@ size_t solveFootprint(size_t T, size_t N, uint32_t E, uint32_t O, uint32_t B, bo
     return geometry + plan + B * perFrequencyBytes(T, N, E, O, mixed, restart);
 }
 
+size_t fmmSolveFootprint(size_t T, size_t N, uint32_t E, uint32_t O, uint32_t restart) {
+    // geometry and plan as for the dense form; near records and their pair
+    // lists at about 700 near panel pairs per panel, near CSR values, GMRES
+    // basis and the expansion tables (a fixed allowance)
+    const size_t geometry = T * (200 + 48 + 112 + 16) + N * 24, plan = T * (T - 1) / 2 + T * 16 * 40 + T * 16 * 220;
+    const size_t nearField = T * 700 * (kRecordDoubles * 8 + 4 + 8 + 8) + N * 500 * 20;
+    const size_t solve = size_t(E) * N * 16 * (restart + 12) + N * 6 * 1024 * 16 * 2;
+    const size_t fields = fieldPartialsBytes(uint32_t(T), E, O, 1) + size_t(E) * T * 16;
+    return geometry + plan + nearField + solve + fields + (size_t(256) << 20);
+}
+
 size_t Session::residentBytes() const {
     size_t bytes = 0;
     for (const DeviceBuffer *b : {&dPanels_, &dBounds_, &dMixedPanels_, &dIncOffsets_, &dIncPanel_, &dIncLocal_,

@@ -137,5 +137,7 @@ class Session {
 // vertices, batched B at a time: workspace of the batch plus the session's
 // geometry and plan (for admission before a session exists).
 size_t solveFootprint(size_t T, size_t N, uint32_t E, uint32_t O, uint32_t B, bool mixed, uint32_t restart);
+// The same for the fast-multipole form (one frequency at a time, sparse near field).
+size_t fmmSolveFootprint(size_t T, size_t N, uint32_t E, uint32_t O, uint32_t restart);
 
 }  // namespace hsb

@@ -109,3 +109,22 @@ def test_reference_fixture_request_is_served():
         direct = server.wait(server.submit(sphere, request))[0]
         replayed = server.wait(server.submit(mesh2, request2))[0]
     _same(direct, replayed)
+
+
+def test_fast_multipole_request_is_served():
+    """A fast-multipole (FP64) request through the serving loop: admitted by its sparse
+    footprint and equal to the direct session solve within the solver tolerance."""
+    horn = meshes.exponential_horn(h=0.0128, seed=5)
+    request = hs.BemRequest(frequencies=[900.0], observers=[(0, 0, 0.6)],
+                            excitations=[hs.BemExcitation("drive", [hs.FaceVelocity(meshes.HORN_THROAT, 1.0)])],
+                            numerics=hs.BemNumerics(precision="fp64", acceleration="fast_multipole",
+                                                    relative_residual_tolerance=1e-6))
+    with hs.BemServer(hs.ServeOptions(workers=1, planning_frequency=PLAN_HZ)) as server:
+        served, timing = server.wait(server.submit(horn, request))
+    request.interaction_plan_frequencies = sorted(set(request.frequencies) | {PLAN_HZ})
+    with hs.CudaBemSolver(horn) as solver:
+        direct = solver.solve(request)
+    a = served.frequencies[0].excitations[0].boundary.pressure_trace
+    b = direct.frequencies[0].excitations[0].boundary.pressure_trace
+    assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(b)
+    assert served.frequencies[0].excitations[0].iterations > 0 and timing.footprint_bytes > 0
