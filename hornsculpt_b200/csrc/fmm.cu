@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                                                        const uint64_t *__restrict__ wignerStart,
                                                        const double2 *__restrict__ coax,
                                                        const uint64_t *__restrict__ coaxStart, int zeroFirst,
-                                                       int nch) {
+                                                       int nch, int K, double2 *partial) {
     constexpr int chunkCh = CPC;
     extern __shared__ double smem[];
     const int nin = (pin + 1) * (pin + 1), nout = (pout + 1) * (pout + 1);
@@ -273,16 +273,21 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
     double2 *a = eph + (pmax + 1);
     double2 *b = a + size_t(chunkCh) * nmax;
     double2 *cbuf = b + size_t(chunkCh) * nmax;
-    const uint32_t node = outNodes[blockIdx.x];
+    // K CTAs share an output node's links (contiguous parts); with K > 1 each
+    // writes its own partial sum, added in a fixed order by reduceKernel
+    const uint32_t oi = blockIdx.x / K, part = blockIdx.x % K;
+    const uint32_t node = outNodes[oi];
     const int cFirst = blockIdx.y * CPC, cEnd = min(nch, cFirst + CPC);
     if (cFirst >= nch)
         return;
-    double2 *out = outCoef + coefOffset[node];
-    if (zeroFirst)
+    double2 *out = K > 1 ? partial + size_t(blockIdx.x) * 6 * nout : outCoef + coefOffset[node];
+    if (zeroFirst || K > 1)
         for (int i = cFirst * nout + threadIdx.x; i < cEnd * nout; i += blockDim.x)
             out[i] = make_double2(0, 0);
     __syncthreads();
-    for (uint32_t li = linkStart[blockIdx.x]; li < linkStart[blockIdx.x + 1]; ++li) {
+    const uint32_t l0 = linkStart[oi], len = linkStart[oi + 1] - l0;
+    const uint32_t lBegin = l0 + uint32_t(uint64_t(len) * part / K), lEnd = l0 + uint32_t(uint64_t(len) * (part + 1) / K);
+    for (uint32_t li = lBegin; li < lEnd; ++li) {
         const TransLink L = links[li];
         const double2 *in = inCoef + coefOffset[L.source];
         const double *dtab = wigner + wignerStart[L.wclass];
@@ -390,6 +395,20 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
             }
             __syncthreads();
         }
+    }
+}
+
+// out[node] (+)= sum over k of the K partial sums of the node, in order of k.
+__global__ void reduceKernel(const uint32_t *__restrict__ outNodes, const uint64_t *__restrict__ coefOffset,
+                             const double2 *__restrict__ partial, int K, int nout, int nch, int assign,
+                             double2 *outCoef) {
+    const uint32_t oi = blockIdx.x;
+    double2 *out = outCoef + coefOffset[outNodes[oi]];
+    for (int e = threadIdx.x; e < nch * nout; e += blockDim.x) {
+        double2 acc = assign ? make_double2(0, 0) : out[e];
+        for (int k = 0; k < K; ++k)
+            acc = cadd(acc, partial[(size_t(oi) * K + k) * 6 * nout + e]);
+        out[e] = acc;
     }
 }
 
@@ -807,7 +826,7 @@ struct FmmOperator::Impl {
     std::vector<int> wclassP;         // polar class -> order needed (set in prepare)
     // device
     DevBuf panels, centers, coefOffset, incOff, far, y;
-    DevBuf Mc, Lc;
+    DevBuf Mc, Lc, partial;
     DevBuf wigner, wignerStart, coax, coaxStart, coaxPin, coaxPout, fl, gaunt, gauntOff;
     DevBuf dItems;
     std::vector<uint64_t> hostCoefOffset;
@@ -1258,27 +1277,43 @@ void FmmOperator::run(const double *src, bool rhs, double *y, cudaStream_t strea
     const auto translate = [&](Impl::DevPlan &d, int pin, int pout, const double2 *in, double2 *out, bool zero) {
         if (!d.count)
             return;
-        const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1));
-        int cpc = nch == 1 ? 1 : d.count >= 2400 ? 3 : d.count >= 1200 ? 2 : 1;
-        while (cpc > 1 && (size_t(3) * cpc * nmax + std::max(pin, pout) + 1) * 16 > 200 * 1024)
-            cpc = cpc == 3 ? 2 : 1;
-        const size_t sm = (size_t(3) * cpc * nmax + std::max(pin, pout) + 1) * 16;
-        const dim3 grid(d.count, unsigned((nch + cpc - 1) / cpc));
+        const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1)), nout = (pout + 1) * (pout + 1);
+        // all channels in one CTA where shared memory allows two CTAs per SM (each
+        // Wigner and coaxial entry then serves every channel), links split over K
+        // CTAs per output node for about eight CTAs per SM
+        const auto bytes = [&](int c) { return (size_t(3) * c * nmax + std::max(pin, pout) + 1) * 16; };
+        int cpc = nch == 1 ? 1 : 6;
+        while (cpc > 1 && bytes(cpc) > 110 * 1024)
+            cpc = cpc == 6 ? 3 : cpc == 3 ? 2 : 1;
+        const size_t sm = bytes(cpc);
+        const unsigned groups = unsigned((nch + cpc - 1) / cpc);
+        const int K = int(std::clamp<size_t>((size_t(148) * 8 + d.count * groups - 1) / (d.count * groups), 1, 8));
+        if (K > 1)
+            I.partial.ensure(size_t(d.count) * K * 6 * nout * 16);
+        const dim3 grid(d.count * K, groups);
         const auto launch = [&](auto kernel) {
             fmmCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                      "translate smem");
             kernel<<<grid, 256, sm, stream>>>(d.out.as<uint32_t>(), d.start.as<uint32_t>(), d.links.as<TransLink>(),
                                               pin, pout, in, out, I.coefOffset.as<uint64_t>(), I.wigner.as<double>(),
                                               I.wignerStart.as<uint64_t>(), I.coax.as<double2>(),
-                                              I.coaxStart.as<uint64_t>(), zero ? 1 : 0, nch);
+                                              I.coaxStart.as<uint64_t>(), zero ? 1 : 0, nch, K,
+                                              I.partial.as<double2>());
         };
-        if (cpc == 3)
+        if (cpc == 6)
+            launch(translateKernel<6>);
+        else if (cpc == 3)
             launch(translateKernel<3>);
         else if (cpc == 2)
             launch(translateKernel<2>);
         else
             launch(translateKernel<1>);
         fmmCheck(cudaGetLastError(), "translate launch");
+        if (K > 1) {
+            reduceKernel<<<d.count, 256, 0, stream>>>(d.out.as<uint32_t>(), I.coefOffset.as<uint64_t>(),
+                                                      I.partial.as<double2>(), K, nout, nch, zero ? 1 : 0, out);
+            fmmCheck(cudaGetLastError(), "translate reduce launch");
+        }
     };
     {
         TimedScope scope(timer, "fmm_p2m", stream);
