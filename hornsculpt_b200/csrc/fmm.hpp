@@ -85,8 +85,6 @@ class FmmSystem {
     // leaves in tree order are merged up to it.
     FmmSystem(FmmOperator &op, const double *rowScale, const double *mass, uint32_t blockWidth);
     ~FmmSystem();
-    // Near values from the row-equilibrated dense matrix (column-major N x N).
-    void nearFromDense(const double *A, cudaStream_t stream, KernelTimer *timer);
     // Device storage of the near values (CSR order of the operator's pattern),
     // filled directly by the near-field assembly; device near CSR arrays.
     double *nearValues();

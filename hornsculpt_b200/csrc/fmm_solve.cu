@@ -51,15 +51,6 @@ struct Buf {
 
 constexpr uint32_t kMaxBlock = 64;
 
-__global__ void nearGatherKernel(const double2 *__restrict__ A, uint32_t N, const uint32_t *__restrict__ rowStart,
-                                 const uint32_t *__restrict__ cols, double2 *vals) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N)
-        return;
-    for (uint32_t e = rowStart[i]; e < rowStart[i + 1]; ++e)
-        vals[e] = A[size_t(cols[e]) * N + i];
-}
-
 // y_i = sum_e vals[e] x[col e] + rowScale_i far_i, one warp per row (fixed order).
 __global__ void spmvKernel(const uint32_t *__restrict__ rowStart, const uint32_t *__restrict__ cols,
                            const double2 *__restrict__ vals, const double2 *__restrict__ x, const double2 *__restrict__ far,
@@ -295,15 +286,6 @@ FmmSystem::FmmSystem(FmmOperator &op, const double *rowScale, const double *mass
 }
 
 FmmSystem::~FmmSystem() = default;
-
-void FmmSystem::nearFromDense(const double *A, cudaStream_t stream, KernelTimer *timer) {
-    Impl &I = *impl_;
-    TimedScope scope(timer, "fmm_near_values", stream);
-    nearGatherKernel<<<(I.N + 127) / 128, 128, 0, stream>>>(reinterpret_cast<const double2 *>(A), I.N,
-                                                            I.rowStart.as<uint32_t>(), I.cols.as<uint32_t>(),
-                                                            I.vals.as<double2>());
-    sysCheck(cudaGetLastError(), "near gather launch");
-}
 
 static __global__ void addScaledKernel(double2 *b, const double2 *far, const double *rowScale, uint32_t N, size_t count) {
     const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
