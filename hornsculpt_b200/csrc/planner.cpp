@@ -108,8 +108,13 @@ std::array<cplx, 4> pointKernels(V3 d, double k, double scale) {
     const double r = std::sqrt(norm2(d));
     if (!(r > 0))
         throw InvalidArgument("Disjoint quadrature panels intersect or contain duplicate geometric nodes.");
-    const cplx g = std::exp(cplx(0, -k * r)) / r;
-    const cplx der = -g * cplx(1, k * r) * (scale / (r * r));
+    double sn, cs;  // exp(-i k r) = cos + i sin of the same argument
+    ::sincos(-k * r, &sn, &cs);
+    const cplx g = cplx(cs, sn) / r;
+    // -g (1 + i k r), written out: the same products and sums as the complex
+    // product, without the library's NaN-recovery call per point
+    const double kr = k * r;
+    const cplx der = cplx(-g.real() + g.imag() * kr, -g.real() * kr - g.imag()) * (scale / (r * r));
     return {g, der * d.x, der * d.y, der * d.z};
 }
 
@@ -127,19 +132,31 @@ Moments tensorMoments(const HostPanel &t, const HostPanel &s, const Sub &a, cons
                       const std::vector<TriPoint> &rule, double k, double scale) {
     Moments m{};
     const V3 origin = t.v[0] - s.v[0];
+    // trial barycentrics and points, the same for every test point
+    constexpr size_t kMaxRule = 64;
+    if (rule.size() > kMaxRule)
+        throw std::logic_error("pair rule larger than the planner's point table");
+    double bsAll[kMaxRule][3];
+    V3 lsAll[kMaxRule];
+    for (size_t q = 0; q < rule.size(); ++q) {
+        double *bs = bsAll[q];
+        bs[0] = bs[1] = bs[2] = 0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                bs[i] += rule[q].b[j] * b.v[j][i];
+        lsAll[q] = localPoint(s, bs);
+    }
     for (const auto &x : rule) {
         double bt[3] = {0, 0, 0};
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j)
                 bt[i] += x.b[j] * a.v[j][i];
         const V3 lt = localPoint(t, bt);
-        for (const auto &y : rule) {
-            double bs[3] = {0, 0, 0};
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j)
-                    bs[i] += y.b[j] * b.v[j][i];
+        for (size_t q = 0; q < rule.size(); ++q) {
+            const auto &y = rule[q];
+            const double *bs = bsAll[q];
             const double w = x.w * y.w * a.fraction * b.fraction;
-            const auto ker = pointKernels(origin + (lt - localPoint(s, bs)), k, scale);
+            const auto ker = pointKernels(origin + (lt - lsAll[q]), k, scale);
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) {
                     const double ww = w * bt[i] * bs[j];
