@@ -9,6 +9,7 @@ from .bem import (AcousticMedium, BemBoundaryData, BemCancelled, BemError, BemEx
                   FieldPointStatus, PressureFieldSample, PressureFieldSettings, ServeOptions, ServeTiming, StopToken,
                   host_plan)
 from .fixtures import read_fixture, write_fixture
+from .study import StudyRequest, complex_result_document, describe_study_capabilities, parse_study_request
 from .meshes import (DRIVEN, WALL, SurfaceMesh, exponential_horn, icosphere, octahedral_sphere, revolved_sphere,
                      scalene_tetrahedron)
 
@@ -18,5 +19,6 @@ __all__ = [
     "CudaStorageOptions", "FaceImpedance", "FaceVelocity", "FarFieldObservation", "FastMultipoleSettings",
     "FieldPointStatus", "PressureFieldSample", "PressureFieldSettings",
     "ServeOptions", "ServeTiming", "StopToken", "host_plan", "DRIVEN", "WALL", "SurfaceMesh", "exponential_horn",
-    "icosphere", "octahedral_sphere", "revolved_sphere", "scalene_tetrahedron", "read_fixture", "write_fixture",
+    "icosphere", "octahedral_sphere", "revolved_sphere", "scalene_tetrahedron", "read_fixture", "write_fixture", "StudyRequest", "parse_study_request",
+    "describe_study_capabilities", "complex_result_document",
 ]
