@@ -86,3 +86,29 @@ def test_progress_and_plan_reuse(solver):
     assert r2.frequencies[0].interaction_plan_reused
     a, b = r1.frequencies[0].excitations[0], r2.frequencies[0].excitations[0]
     assert np.array_equal(a.boundary.pressure_trace, b.boundary.pressure_trace)
+
+
+def test_lem_coupled_solve_equals_direct_solve_of_coupled_velocities():
+    """BEM side of LEM coupling: the superposed unit-port solves equal one direct solve
+    with the coupled face velocities, and the port pressures close with the network's."""
+    m = meshes.icosphere(2)
+    c = m.vertices[m.triangles].mean(axis=1)
+    faces = np.where(c[:, 2] > 0.06, 17, np.where(c[:, 0] < -0.06, 29, 90)).astype(np.uint32)
+    kind = np.where(faces == 90, meshes.WALL, meshes.DRIVEN).astype(np.uint8)
+    mesh = hs.SurfaceMesh(m.vertices, m.triangles, faces, kind)
+    flows = np.array([2e-4 + 1e-5j, -5e-5j])
+
+    def network(f, Z):
+        return [hs.PortSolution(q, p) for q, p in zip(flows, Z @ flows)]
+    request = hs.BemRequest(frequencies=[600.0], excitations=[], observers=[(0, 0, 0.5)],
+                            numerics=hs.BemNumerics(relative_residual_tolerance=1e-7))
+    ports = [hs.BemPort("front", [17]), hs.BemPort("side", [29])]
+    with hs.CudaBemSolver(mesh) as solver:
+        coupled = hs.coupled_solve(solver, mesh, ports, request, network)[0]
+        direct = solver.solve(hs.BemRequest(frequencies=[600.0], observers=[(0, 0, 0.5)],
+                                            excitations=[hs.BemExcitation("lem", coupled.face_velocities)],
+                                            numerics=request.numerics))
+    d = direct.frequencies[0].excitations[0]
+    assert np.linalg.norm(coupled.pressure_trace - d.boundary.pressure_trace) <= 1e-6 * np.linalg.norm(
+        d.boundary.pressure_trace)
+    assert abs(coupled.observer_pressure[0] - d.observer_pressure[0]) <= 1e-6 * abs(d.observer_pressure[0])
