@@ -53,3 +53,18 @@ def test_invalid_tree_settings_are_rejected():
     with pytest.raises(Exception, match="settings are invalid"):
         _lib.check(lib.hs_bem_debug_fmm_tree(v.ctypes.data, mesh.vertex_count, t.ctypes.data, mesh.triangle_count, 0,
                                              1.5, 2.0, sizes.ctypes.data, None, 0))
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference tree absent")
+@pytest.mark.parametrize("case, leaf, sep, ratio", [
+    ("revolved", 8, 1.5, 2.0), ("revolved", 64, 3.0, 1.0), ("ico4", 16, 1.5, 0.0),
+    ("horn_coarse", 4, 1.8, 2.0), ("tetra", 4, 1.5, 2.0)])
+def test_support_tree_matches_reference_more(case, leaf, sep, ratio):
+    mesh = {"revolved": lambda: meshes.revolved_sphere(h=0.012, seed=2),
+            "ico4": lambda: meshes.icosphere(4),
+            "horn_coarse": lambda: meshes.exponential_horn(h=0.016, seed=1),
+            "tetra": lambda: meshes.scalene_tetrahedron()}[case]()
+    mine, links = _tree(mesh, leaf, sep, ratio)
+    ref, ref_links = O.reference_support_tree(mesh, leaf, sep, ratio)
+    assert list(mine) == list(ref)
+    assert np.array_equal(links, ref_links)
