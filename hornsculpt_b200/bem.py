@@ -504,3 +504,29 @@ def host_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float) -> dict:
                                      out["patches"].ctypes.data, out["whole"].ctypes.data, out["offsets"].ctypes.data,
                                      out["trials"].ctypes.data))
     return out
+
+
+def debug_lu_factor(matrices: np.ndarray, fp32: bool = False):
+    """The solver's batched LU of complex matrices (batch x n x n, [row, col]).
+
+    Returns (factors, pivots, info): factors batch x n x n complex holding unit
+    L below the diagonal and U on and above it (LAPACK zgetrf layout), pivots
+    batch x n 0-based row interchanges, info the batch's breakdown word.
+    fp32 selects the mixed form's FP32 factorisation (input rounded to FP32,
+    tensor-core trailing updates)."""
+    lib = _lib.load()
+    a = np.asarray(matrices, np.complex128)
+    if a.ndim == 2:
+        a = a[None]
+    batch, n, m = a.shape
+    if n != m:
+        raise ValueError("debug_lu_factor needs square matrices")
+    cm = np.ascontiguousarray(np.transpose(a, (0, 2, 1)))  # column-major per matrix
+    src = np.ascontiguousarray(np.stack([cm.real, cm.imag], -1))
+    out = np.zeros_like(src)
+    piv = np.zeros((batch, n), np.int32)
+    info = C.c_int32()
+    _lib.check(lib.hs_bem_debug_lu(1 if fp32 else 0, n, batch, src.ctypes.data, out.ctypes.data, piv.ctypes.data,
+                                   C.byref(info)))
+    factors = np.transpose(out[..., 0] + 1j * out[..., 1], (0, 2, 1))
+    return factors, piv, info.value

@@ -12,6 +12,7 @@
 // adjoint kernel at the same points. Pair blocks are written to per-pair
 // records (no atomics) and reduced to the matrix by two deterministic
 // gathers (trial vertex, then test vertex), so results are bit-reproducible.
+#include "device_once.hpp"
 #include "device_types.cuh"
 #include "host_mesh.hpp"
 #include "kernel_timer.hpp"
@@ -1461,15 +1462,13 @@ __global__ void rhsVertexKernel(const double *__restrict__ panelRhs, const uint3
 }
 
 int smCount() {
-    static int count = 0;
-    if (!count) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
-        if (count <= 0)
-            count = 148;
-    }
-    return count;
+    static PerDeviceValue<int> count;
+    return count.get([]() {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, currentDevice()) != cudaSuccess || n <= 0)
+            n = 148;
+        return n;
+    });
 }
 
 template <int NP>
@@ -1532,10 +1531,8 @@ std::vector<float> buildSingularTable(unsigned order) {
     return out;
 }
 
-void uploadRuleTables(cudaStream_t stream) {
-    static bool done = false;
-    if (done)
-        return;
+namespace {
+void uploadRuleTablesNow(cudaStream_t stream) {
     double table[kRulePoints * 4];
     const unsigned degrees[kBins] = {4, 6, 8, 14};
     int o = 0;
@@ -1567,7 +1564,14 @@ void uploadRuleTables(cudaStream_t stream) {
     }
     cudaCheck(cudaMemcpyToSymbolAsync(cGauss20, g20, sizeof(g20), 0, cudaMemcpyHostToDevice, stream), "gauss upload");
     cudaCheck(cudaStreamSynchronize(stream), "rule upload sync");
-    done = true;
+}
+}  // namespace
+
+// The rule tables in constant memory, once per device (each device has its own
+// copy of the __constant__ arrays).
+void uploadRuleTables(cudaStream_t stream) {
+    static PerDeviceOnce once;
+    once.run([&]() { uploadRuleTablesNow(stream); });
 }
 
 bool gatherUsesColumns(uint32_t T) { return size_t(3) * T * sizeof(double2) > kGatherColumnSmem; }
@@ -1669,16 +1673,15 @@ void assembleBatch(const AssemblyGeometry &g, const double *ks, const double *ga
     const size_t columnBytes = size_t(3) * g.T * sizeof(double2);
     if (!gatherUsesColumns(g.T)) {
         TimedScope scope(timer, "gather_column", stream);
-        static bool attr = false;
-        if (!attr) {
+        static PerDeviceOnce attributes;
+        attributes.run([]() {
             cudaCheck(cudaFuncSetAttribute(gatherColumnKernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            int(kGatherColumnSmem)),
                       "gather smem attribute");
             cudaCheck(cudaFuncSetAttribute(gatherColumnKernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            int(kGatherColumnSmem)),
                       "gather smem attribute");
-            attr = true;
-        }
+        });
         const dim3 grid(g.N, B);
         if (mixed)
             gatherColumnKernel<<<grid, 512, columnBytes, stream>>>(recF, g.incOffsets, g.incPanel, g.incLocal,

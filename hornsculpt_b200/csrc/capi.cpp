@@ -365,6 +365,19 @@ hs_status hs_bem_debug_assemble(hs_bem_session *s, const hs_numerics *numerics, 
     });
 }
 
+hs_status hs_bem_debug_lu(uint32_t precision, size_t n, size_t batch, const double *matrices, double *factors,
+                          int32_t *pivots, int32_t *info) {
+    if (!matrices || !factors || !pivots || !info)
+        return fail(HS_E_INVALID, "Debug LU pointers must be non-null.");
+    if (precision != HS_PRECISION_FP64 && precision != HS_PRECISION_MIXED)
+        return fail(HS_E_INVALID, "Debug LU precision must be HS_PRECISION_FP64 or HS_PRECISION_MIXED.");
+    if (n == 0 || batch == 0 || n > 65536 || batch > 64)
+        return fail(HS_E_INVALID, "Debug LU needs 1 <= n <= 65536 and 1 <= batch <= 64.");
+    return guarded([&]() {
+        debugLuFactor(precision == HS_PRECISION_MIXED, uint32_t(n), uint32_t(batch), matrices, factors, pivots, info);
+    });
+}
+
 hs_status hs_bem_debug_fmm_far(hs_bem_session *s, const hs_numerics *numerics, double k, double tolerance,
                                const double *pressure, double *far, uint32_t *near_row_start, uint32_t *near_cols,
                                size_t near_capacity, size_t *near_count, uint32_t *level_info, size_t level_capacity,

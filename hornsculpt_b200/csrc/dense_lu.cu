@@ -8,6 +8,7 @@
 // with panel width 32: a single-CTA panel factorisation per matrix, row
 // interchanges outside the panel, a unit-lower triangular solve for the U
 // block row and a shared-memory tiled complex GEMM for the trailing update.
+#include "device_once.hpp"
 #include "device_types.cuh"
 #include "kernel_timer.hpp"
 
@@ -16,6 +17,7 @@
 #include <algorithm>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 namespace hsb {
 namespace {
@@ -1412,12 +1414,9 @@ __global__ void toFloatKernel(const double *in, float *out, size_t count) {
 // Largest cluster the panel kernel may use on this device: 16 CTAs (opt-in)
 // when the device can schedule such a cluster with full panel shared memory,
 // else the portable 8, else none.
-template <class R> uint32_t clusterLimit() {
-    static int limit = -1;
-    if (limit >= 0)
-        return uint32_t(limit);
+template <class R> uint32_t clusterLimitNow() {
     const size_t smem = size_t(kPanel) * kClusterRows<R> * sizeof(C2<R>);
-    limit = 0;
+    int limit = 0;
     for (const void *kernel : {reinterpret_cast<const void *>(panelClusterKernel<R, 0>),
                                reinterpret_cast<const void *>(panelClusterKernel<R, kGlobalSlots>)})
         if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess) {
@@ -1453,6 +1452,10 @@ template <class R> uint32_t clusterLimit() {
     }
     return uint32_t(limit);
 }
+template <class R> uint32_t clusterLimit() {
+    static PerDeviceValue<uint32_t> limit;
+    return limit.get([]() { return clusterLimitNow<R>(); });
+}
 
 // Right-looking LU with partial pivoting, 32-wide panels. FP64 runs one
 // level: every panel updates the whole trailing matrix (K = 32). FP32 runs two
@@ -1465,8 +1468,8 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
                                KernelTimer *timer, float *pack) {
     check(cudaMemsetAsync(info, 0, sizeof(int), stream), "LU info reset");
     const size_t gemmSmem = 2 * kPanel * 64 * sizeof(C2<R>);
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attributes;
+    attributes.run([&]() {
         check(cudaFuncSetAttribute(gemmKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(gemmSmem)),
               "gemm smem attribute");
         check(cudaFuncSetAttribute(panelSmemKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1478,8 +1481,7 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
             check(cudaFuncSetAttribute(trsmBlockKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrsmSmem)),
                   "block trsm smem attribute");
         }
-        attr = true;
-    }
+    });
     const uint32_t outer = sizeof(R) == 4 ? uint32_t(kOuter) : N;
     for (uint32_t K0 = 0; K0 < N; K0 += outer) {
         const uint32_t end = std::min(N, K0 + outer);
@@ -1567,12 +1569,10 @@ template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32
     TimedScope s(timer, "lu_solve", stream);
     const size_t smem = size_t(N) * sizeof(C2<R>);
     if (N <= kSmallSolve) {  // one CTA per system: the vector in shared memory, no launch per block
-        static size_t attr = 0;
-        if (smem > 48 * 1024 && smem > attr) {
+        static PerDeviceHighWater attr;
+        if (smem > 48 * 1024 && attr.raise(smem))
             check(cudaFuncSetAttribute(solveKernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
                   "solve smem attribute");
-            attr = smem;
-        }
         solveKernel<R><<<dim3(E, B), sizeof(R) == 8 ? 256 : 512, smem, stream>>>(LU, pivots, N, E, x);
         check(cudaGetLastError(), "triangular solve launch");
         return;
@@ -1602,12 +1602,10 @@ template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32
 
 template <class R> void permutation(const int *pivots, uint32_t N, uint32_t B, cudaStream_t stream) {
     const size_t smem = size_t(N) * sizeof(int);
-    static size_t attr = 0;
-    if (smem > 48 * 1024 && smem > attr) {
+    static PerDeviceHighWater attr;
+    if (smem > 48 * 1024 && attr.raise(smem))
         check(cudaFuncSetAttribute(permutationKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
               "permutation smem attribute");
-        attr = smem;
-    }
     permutationKernel<<<B, 256, smem, stream>>>(pivots, N, const_cast<int *>(pivots) + size_t(B) * N);
     check(cudaGetLastError(), "permutation launch");
 }
@@ -1658,6 +1656,49 @@ void addCorrectionBatch(double *x, const float *correction, size_t count, cudaSt
 void roundToFloat(const double *in, float *out, size_t count, cudaStream_t stream) {
     toFloatKernel<<<unsigned((count + 255) / 256), 256, 0, stream>>>(in, out, count);
     check(cudaGetLastError(), "FP32 rounding launch");
+}
+
+namespace {
+// Device memory of the LU test hook, freed on every exit path.
+struct HookBuffer {
+    void *p = nullptr;
+    explicit HookBuffer(size_t bytes) { check(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "LU hook allocation"); }
+    ~HookBuffer() { cudaFree(p); }
+    HookBuffer(const HookBuffer &) = delete;
+    HookBuffer &operator=(const HookBuffer &) = delete;
+};
+}  // namespace
+
+void debugLuFactor(bool fp32, uint32_t N, uint32_t B, const double *matrices, double *factors, int *pivots,
+                   int *info) {
+    const size_t reals = size_t(B) * N * N * 2;
+    cudaStream_t stream = nullptr;
+    check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "LU hook stream");
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } guard{stream};
+    HookBuffer lu(reals * (fp32 ? sizeof(float) : sizeof(double))), piv(luWorkspaceBytes(N, B)), status(sizeof(int));
+    if (fp32) {
+        HookBuffer pack(luPackBytes(N, B));
+        std::vector<float> host(matrices, matrices + reals);
+        check(cudaMemcpyAsync(lu.p, host.data(), reals * sizeof(float), cudaMemcpyHostToDevice, stream), "LU hook upload");
+        luFactorBatch(static_cast<float *>(lu.p), N, B, static_cast<int *>(piv.p), static_cast<int *>(status.p), stream,
+                      nullptr, static_cast<float *>(pack.p));
+        check(cudaMemcpyAsync(host.data(), lu.p, reals * sizeof(float), cudaMemcpyDeviceToHost, stream), "LU hook download");
+        check(cudaMemcpyAsync(pivots, piv.p, size_t(B) * N * sizeof(int), cudaMemcpyDeviceToHost, stream), "LU hook pivots");
+        check(cudaMemcpyAsync(info, status.p, sizeof(int), cudaMemcpyDeviceToHost, stream), "LU hook status");
+        check(cudaStreamSynchronize(stream), "LU hook");
+        std::copy(host.begin(), host.end(), factors);
+        return;
+    }
+    check(cudaMemcpyAsync(lu.p, matrices, reals * sizeof(double), cudaMemcpyHostToDevice, stream), "LU hook upload");
+    luFactorBatch(static_cast<double *>(lu.p), N, B, static_cast<int *>(piv.p), static_cast<int *>(status.p), stream,
+                  nullptr);
+    check(cudaMemcpyAsync(factors, lu.p, reals * sizeof(double), cudaMemcpyDeviceToHost, stream), "LU hook download");
+    check(cudaMemcpyAsync(pivots, piv.p, size_t(B) * N * sizeof(int), cudaMemcpyDeviceToHost, stream), "LU hook pivots");
+    check(cudaMemcpyAsync(info, status.p, sizeof(int), cudaMemcpyDeviceToHost, stream), "LU hook status");
+    check(cudaStreamSynchronize(stream), "LU hook");
 }
 
 size_t luWorkspaceBytes(uint32_t N, uint32_t B) { return 2 * size_t(B) * N * sizeof(int); }

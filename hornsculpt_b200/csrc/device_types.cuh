@@ -206,6 +206,13 @@ void luFactorBatch(float *LU, uint32_t N, uint32_t B, int *pivots, int *info, cu
                    class KernelTimer *timer, float *pack);
 void luSolveBatch(const double *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, double *x,
                   void *scratch, cudaStream_t stream, class KernelTimer *timer);
+// Test hook: factors B host matrices (complex column-major, interleaved) with
+// the batched kernels above, FP64 or FP32 (FP32 in, rounded from the FP64
+// input), and returns the factors (as doubles), the 0-based interchange
+// sequence and the breakdown word (first zero pivot + 1, -1 for a tensor-core
+// timeout, 0 when every pivot is nonzero).
+void debugLuFactor(bool fp32, uint32_t N, uint32_t B, const double *matrices, double *factors, int *pivots,
+                   int *info);
 void luSolveBatch(const float *LU, const int *pivots, uint32_t N, uint32_t B, uint32_t E, float *x,
                   void *scratch, cudaStream_t stream, class KernelTimer *timer);
 // r = b - A x (FP64); writes the correction rhs into `correction` and the

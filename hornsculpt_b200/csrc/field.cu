@@ -4,6 +4,7 @@
 // or the asymptotic far field F(d) exp(-ikR)/R. FP64 throughout; one CTA
 // per (frequency, excitation, observer, 256-panel tile), reduced over tiles
 // in a fixed order.
+#include "device_once.hpp"
 #include "device_types.cuh"
 #include "host_mesh.hpp"
 #include "kernel_timer.hpp"
@@ -445,10 +446,11 @@ __global__ void __launch_bounds__(kFieldThreads) pressureFieldKernel(const DPane
 
 }  // namespace
 
-// The field rules (degrees 4, 6, 8, 12, 14) in constant memory, once per process.
+// The field rules (degrees 4, 6, 8, 12, 14) in constant memory, once per
+// device (each device has its own copy of the __constant__ table).
 void uploadFieldRules(cudaStream_t stream) {
-    static std::once_flag once;
-    std::call_once(once, [&]() {
+    static PerDeviceOnce once;
+    once.run([&]() {
         double table[kFieldPoints * 4];
         int o = 0;
         for (unsigned d : {4u, 6u, 8u, 12u, 14u})
@@ -608,7 +610,9 @@ void *gNoAllocAddress[256] = {};
 // Set-up once per device, with that device current: the host name of the
 // array is only a stand-in, so its device address is looked up here and
 // passed to the kernels. The first call on a device does this look-up and
-// should therefore come before any stream capture on that device.
+// should therefore come before any stream capture on that device. The address
+// is kept for the life of the process, which assumes the device's primary
+// context lives that long too (no cudaDeviceReset between calls).
 static double *noAllocScratch(int device) {
     std::lock_guard<std::mutex> lock(gNoAllocMutex);
     if (device < 0 || device >= 256)
@@ -684,8 +688,8 @@ void observerFieldNoAlloc(const double *vertices, size_t vertexCount, const uint
     check(cudaStreamSynchronize(stream), "no-allocation field preparation");
     if (prepared == kErrIndex)
         throw std::invalid_argument("No-allocation field: a triangle has an invalid vertex index.");
-    if (prepared == kErrDegenerate)
-        throw NumericError("Galerkin triangle is degenerate or numerically unresolved.");
+    if (prepared == kErrDegenerate)  // the same input class and message as a session's mesh check
+        throw std::invalid_argument("Galerkin triangle is degenerate or numerically unresolved.");
     if (prepared == kErrDistance)
         throw std::invalid_argument("A far-field direction must differ from its origin.");
     FieldRequest req{panels, T, N, 1, O, 1, localObservers, farField,

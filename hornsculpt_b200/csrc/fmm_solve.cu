@@ -86,6 +86,7 @@ __global__ void __launch_bounds__(256) blockInverseKernel(const uint32_t *__rest
                                                           const uint64_t *__restrict__ invStart, double2 *inv,
                                                           int *flag) {
     extern __shared__ double2 aug[];  // nb x 2nb, row-major
+    __shared__ double2 factor[kMaxBlock];
     __shared__ int pivotRow;
     __shared__ int singular;
     const uint32_t b0 = blockStart[blockIdx.x], nb = blockStart[blockIdx.x + 1] - b0;
@@ -147,12 +148,17 @@ __global__ void __launch_bounds__(256) blockInverseKernel(const uint32_t *__rest
             const double2 v = aug[c * w + k];
             aug[c * w + k] = make_double2(v.x * ip.x - v.y * ip.y, v.x * ip.y + v.y * ip.x);
         }
+        // column c of every row is read before any row is updated: the thread that
+        // updates (r, c) would otherwise overwrite the factor other threads of row r
+        // still have to read
+        for (uint32_t r = threadIdx.x; r < nb; r += blockDim.x)
+            factor[r] = aug[r * w + c];
         __syncthreads();
         for (uint32_t e = threadIdx.x; e < nb * w; e += blockDim.x) {
             const uint32_t r = e / w, k = e % w;
             if (r == c)
                 continue;
-            const double2 f = aug[r * w + c], v = aug[c * w + k];
+            const double2 f = factor[r], v = aug[c * w + k];
             aug[e] = make_double2(aug[e].x - (f.x * v.x - f.y * v.y), aug[e].y - (f.x * v.y + f.y * v.x));
         }
         __syncthreads();

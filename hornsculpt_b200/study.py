@@ -72,9 +72,15 @@ def _array(value, maximum: int, minimum: int = 0) -> list:
 
 
 def _number(value) -> float:
-    if isinstance(value, bool) or not isinstance(value, (int, float)) or not math.isfinite(value):
+    if isinstance(value, bool) or not isinstance(value, (int, float)):
         _project("Endliche Zahl erwartet.")
-    return float(value)
+    try:  # an integer literal beyond double range reads as infinity in the reference's parser
+        result = float(value)
+    except OverflowError:
+        result = math.inf
+    if not math.isfinite(result):
+        _project("Endliche Zahl erwartet.")
+    return result
 
 
 def _positive(value) -> float:

@@ -219,6 +219,18 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
                             uint32_t *near_offsets, uint32_t *near_trials);
 hs_status hs_bem_debug_assemble(hs_bem_session *session, const hs_numerics *numerics, double plan_k, double k,
                                 const double *flux, double *matrix, double *rhs);
+/* LU test hook: factors `batch` complex n x n matrices (host, column-major,
+ * interleaved re/im) with the solver's batched LU kernels — FP64
+ * (HS_PRECISION_FP64: the plain form's factorisation) or FP32
+ * (HS_PRECISION_MIXED: the input rounded to FP32, the two-level factorisation
+ * with tensor-core trailing updates). `factors` (same layout, doubles)
+ * receives L (unit diagonal, strictly below it) and U in place, like LAPACK
+ * zgetrf / the reference's cusolverDnCgetrf (cuda_solver.cu:1485-1513);
+ * `pivots` (batch x n) the row interchange sequence, 0-based (ipiv - 1 in
+ * LAPACK terms); `info` one status word for the batch: 0, or the first zero
+ * pivot's column + 1 (-1: a tensor-core update did not complete). */
+hs_status hs_bem_debug_lu(uint32_t precision, size_t n, size_t batch, const double *matrices, double *factors,
+                          int32_t *pivots, int32_t *info);
 /* Fast-multipole test hooks. hs_bem_debug_fmm_far applies the far part of the
  * fast-multipole operator (support pairs outside the near leaf pairs of the
  * support tree, row-equilibrated like hs_bem_debug_assemble's matrix) to a P1
@@ -262,9 +274,12 @@ hs_status hs_bem_debug_fmm_tree(const double *vertices, size_t vertex_count, con
  * triangle_count * 200 + observer_count * 24 +
  * observer_count * ceil(triangle_count / 256) * 16 + 256 bytes to 4 MiB (larger
  * requests return HS_E_INVALID). The first call on a device looks up that
- * array's device address, so make it before any stream capture on that device.
- * All calls share the array: calls that overlap on the GPU race and must be
- * serialised. The call returns after the work on `cuda_stream` has finished. */
+ * array's device address, so make it before any stream capture on that device;
+ * the address is kept until the process exits, so do not reset the device
+ * between calls. All calls share the array: calls that overlap on the GPU race
+ * and must be serialised. The call reads status words back and waits for
+ * `cuda_stream`; it returns after the work on that stream has finished. A
+ * degenerate triangle returns HS_E_INVALID, as at session creation. */
 hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_count, const uint32_t *triangles,
                                         size_t triangle_count, const double *pressure_trace, const double *flux,
                                         const double *observers, size_t observer_count, double wavenumber,

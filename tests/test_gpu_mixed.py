@@ -14,6 +14,9 @@ pytestmark = pytest.mark.gpu
 
 MIXED_TOL = 1e-5
 MIXED = hs.BemNumerics(precision="mixed")
+# The plain form solves with an FP64 LU: its relative residual sits near FP64
+# round-off (about 1e-13), far below the reference's refinement target.
+PLAIN_RESIDUAL = 1e-12
 
 
 def test_mixed_assembly_against_oracle():
@@ -100,7 +103,7 @@ def test_tall_panels_on_a_cluster():
         mixed = solver.solve(hs.BemRequest(frequencies=freqs, excitations=exc, numerics=MIXED))
     for fp, fm in zip(plain.frequencies, mixed.frequencies):
         p, m = fp.excitations[0], fm.excitations[0]
-        assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
+        assert p.boundary_residual <= PLAIN_RESIDUAL and m.boundary_residual <= 1e-10
         assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
 
 
@@ -119,7 +122,7 @@ def test_panels_beyond_cluster_shared_memory(make):
         plain = solver.solve(hs.BemRequest(frequencies=[700.0], excitations=exc))
         mixed = solver.solve(hs.BemRequest(frequencies=[700.0], excitations=exc, numerics=MIXED))
     p, m = plain.frequencies[0].excitations[0], mixed.frequencies[0].excitations[0]
-    assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
+    assert p.boundary_residual <= PLAIN_RESIDUAL and m.boundary_residual <= 1e-10
     assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL
 
 
@@ -136,5 +139,5 @@ def test_exactly_packed_bins_above_ten_thousand_triangles():
     with hs.CudaBemSolver(mesh) as solver:
         mixed = solver.solve(hs.BemRequest(frequencies=[900.0], excitations=exc, numerics=MIXED))
     p, m = plain.frequencies[0].excitations[0], mixed.frequencies[0].excitations[0]
-    assert p.boundary_residual <= 5e-5 and m.boundary_residual <= 1e-10
+    assert p.boundary_residual <= PLAIN_RESIDUAL and m.boundary_residual <= 1e-10
     assert rel_l2(m.boundary.pressure_trace, p.boundary.pressure_trace) <= MIXED_TOL

@@ -98,6 +98,9 @@ def _edit(path, value=None, delete=False):
     (_edit(["numerics", "nearMaximumDepth"], 11), "Ungültige Ganzzahl oder ID."),
     (_edit(["numerics", "quadratureOrder"], 4), "Unbekanntes Feld: quadratureOrder"),
     (_edit(["medium", "densityKgM3"], -1), "Positive Zahl erwartet."),
+    # an integer literal beyond double range (JSON digits, not a float) is rejected as not finite
+    (_edit(["medium", "densityKgM3"], 10 ** 400), "Endliche Zahl erwartet."),
+    (_edit(["frequenciesHz"], [200, 10 ** 400]), "Endliche Zahl erwartet."),
 ])
 def test_study_errors(study, message):
     if message is None:  # a valid variant
