@@ -118,6 +118,11 @@ def load():
         "hs_bem_session_set_profiling": (C.c_int, [_P, C.c_int32]),
         "hs_bem_session_profile": (C.c_int, [_P, C.c_char_p, C.c_size_t, _P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
         "hs_bem_session_work": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "hs_bem_session_set_graphs": (C.c_int, [_P, C.c_int32]),
+        "hs_autotune_set_enabled": (C.c_int, [C.c_int32]),
+        "hs_autotune_clear": (C.c_int, []),
+        "hs_autotune_report": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),
+        "hs_bem_session_graph_launches": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
         "hs_bem_debug_plan": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, C.POINTER(hs_numerics), C.c_double, _P, _P,
                                         _P, _P, _P, _P, _P]),
         "hs_bem_observer_field_noalloc": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, _P, _P, _P, C.c_size_t, C.c_double,

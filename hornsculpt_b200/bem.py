@@ -251,6 +251,16 @@ class CudaBemSolver:
     WORK_KEYS = ("pairs_q6", "pairs_q12", "pairs_q16", "pairs_q64", "regular_samples", "singular_samples",
                  "near_samples", "frequencies")
 
+    def set_graphs(self, enabled: bool) -> None:
+        """Replay of the dense batch chain and the fast-multipole far-field apply as captured CUDA graphs."""
+        _lib.check(self._lib.hs_bem_session_set_graphs(self._handle, int(enabled)))
+
+    def graph_launches(self) -> int:
+        """Dense-chain graph replays of this session so far."""
+        n = C.c_uint64()
+        _lib.check(self._lib.hs_bem_session_graph_launches(self._handle, C.byref(n)))
+        return n.value
+
     def work(self) -> dict:
         """Work counters (pairs per regular rule, samples per pair class) since profiling was enabled."""
         buf = (C.c_uint64 * 8)()
@@ -530,3 +540,27 @@ def debug_lu_factor(matrices: np.ndarray, fp32: bool = False):
                                    C.byref(info)))
     factors = np.transpose(out[..., 0] + 1j * out[..., 1], (0, 2, 1))
     return factors, piv, info.value
+
+
+def autotune_report() -> dict:
+    """{size class: (chosen candidate, [ms per candidate])} of the launch-shape autotuner."""
+    lib = _lib.load()
+    need = C.c_size_t()
+    _lib.check(lib.hs_autotune_report(None, 0, C.byref(need)))
+    buf = C.create_string_buffer(need.value)
+    _lib.check(lib.hs_autotune_report(buf, need.value, C.byref(need)))
+    out = {}
+    for item in buf.value.decode().split(";"):
+        if item:
+            key, rest = item.split("=")
+            choice, ms = rest.split(":")
+            out[key] = (int(choice), [float(x) for x in ms.split("/") if x])
+    return out
+
+
+def autotune_enable(enabled: bool = True) -> None:
+    _lib.check(_lib.load().hs_autotune_set_enabled(int(enabled)))
+
+
+def autotune_clear() -> None:
+    _lib.check(_lib.load().hs_autotune_clear())

@@ -40,10 +40,8 @@ def _compile(src: pathlib.Path, verbose_ptxas: bool) -> pathlib.Path:
         return obj
     cmd = [_nvcc(), "-std=c++20", "-O3", "-lineinfo", *ARCH, "-Xcompiler", "-fPIC", "-I", str(INCLUDE), "-I",
            str(CSRC), "-c", str(src), "-o", str(obj)]
-    if src.suffix == ".cu":
-        cmd += ["--use_fast_math"] if False else []
-        if verbose_ptxas:
-            cmd += ["-Xptxas", "-v"]
+    if src.suffix == ".cu" and verbose_ptxas:
+        cmd += ["-Xptxas", "-v"]
     subprocess.run(cmd, check=True)
     return obj
 

@@ -12,6 +12,7 @@
 // adjoint kernel at the same points. Pair blocks are written to per-pair
 // records (no atomics) and reduced to the matrix by two deterministic
 // gathers (trial vertex, then test vertex), so results are bit-reproducible.
+#include "autotune.hpp"
 #include "device_once.hpp"
 #include "device_types.cuh"
 #include "host_mesh.hpp"
@@ -1478,18 +1479,38 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
     const char *mixedNames[kBins] = {"regular_mixed_q6", "regular_mixed_q12", "regular_mixed_q16",
                                      "regular_mixed_q64"};
     TimedScope scope(timer, mixed ? mixedNames[bin] : names[bin], stream);
-    if (mixed) {
-        const dim3 grid(unsigned(smCount() * 16), B);
-        regularMixedKernel<NP><<<grid, 128, 0, stream>>>(g.mixedPanels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
-                                                         ws.binCapacity, ws.binOffsets, bin,
-                                                         static_cast<float *>(ws.records), error);
-    } else {
-        const dim3 grid(unsigned(smCount() * 6), B);
-        regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts, ws.binCapacity,
-                                                         ws.binOffsets, bin, static_cast<double *>(ws.records), map,
-                                                         error);
+    // Grid of the grid-stride pair loop in CTAs per SM: each pair is one
+    // independent item, so the choice moves only the load balance and occupancy.
+    static constexpr int kMixedCtas[] = {16, 8, 24, 32};
+    static constexpr int kPlainCtas[] = {6, 3, 12};
+    const int candidates = mixed ? 4 : 3;
+    const auto launch = [&](int c) {
+        if (mixed) {
+            const dim3 grid(unsigned(smCount() * kMixedCtas[c]), B);
+            regularMixedKernel<NP><<<grid, 128, 0, stream>>>(g.mixedPanels, g.bounds, g.T, ks, ws.bins, ws.binCounts,
+                                                             ws.binCapacity, ws.binOffsets, bin,
+                                                             static_cast<float *>(ws.records), error);
+        } else {
+            const dim3 grid(unsigned(smCount() * kPlainCtas[c]), B);
+            regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts,
+                                                             ws.binCapacity, ws.binOffsets, bin,
+                                                             static_cast<double *>(ws.records), map, error);
+        }
+        cudaCheck(cudaGetLastError(), "regular pair assembly launch");
+    };
+    // size class: the form, the rule, the batch and the mesh size to a power of two
+    const std::string key = std::string(mixed ? "regular_mixed" : "regular_fp64") + "_q" + std::to_string(NP) +
+                            "_B" + std::to_string(B) + "_T2^" + std::to_string(31 - __builtin_clz(g.T | 1u)) +
+                            (map.row ? "_near" : "");
+    Autotuner &tuner = Autotuner::instance();
+    int c = tuner.choice(key);
+    // tuned on first use, outside a capture and outside a profiled solve (whose
+    // per-family times would count the candidates' launches)
+    if (c < 0 && tuner.enabled() && !(timer && timer->enabled()) && !capturing(stream)) {
+        tuner.tune(key, candidates, stream, launch);
+        return;
     }
-    cudaCheck(cudaGetLastError(), "regular pair assembly launch");
+    launch(c < 0 ? 0 : c);
 }
 
 }  // namespace

@@ -1,6 +1,7 @@
 // extern "C" entry points of include/hs_bem.h: exceptions of the session
 // layer become hs_status codes plus a thread-local message.
 #include "hs_bem.h"
+#include "autotune.hpp"
 #include "serve.hpp"
 #include "session.hpp"
 
@@ -247,6 +248,45 @@ hs_status hs_bem_session_set_profiling(hs_bem_session *s, int32_t enabled) {
         s->impl->timer().reset();
         s->impl->timer().enable(enabled != 0);
         std::fill(s->impl->work.begin(), s->impl->work.end(), 0);
+    });
+}
+
+hs_status hs_bem_session_set_graphs(hs_bem_session *s, int32_t enabled) {
+    if (!s)
+        return fail(HS_E_INVALID, "Session is null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->setGraphs(enabled != 0);
+    });
+}
+
+hs_status hs_bem_session_graph_launches(const hs_bem_session *s, uint64_t *launches) {
+    if (!s || !launches)
+        return fail(HS_E_INVALID, "Session and output must be non-null.");
+    *launches = s->impl->graphLaunches();
+    return HS_OK;
+}
+
+hs_status hs_autotune_set_enabled(int32_t enabled) {
+    Autotuner::instance().setEnabled(enabled != 0);
+    return HS_OK;
+}
+
+hs_status hs_autotune_clear(void) {
+    Autotuner::instance().clear();
+    return HS_OK;
+}
+
+hs_status hs_autotune_report(char *buffer, size_t size, size_t *needed) {
+    return guarded([&]() {
+        const std::string r = Autotuner::instance().report();
+        if (needed)
+            *needed = r.size() + 1;
+        if (buffer && size) {
+            const size_t n = std::min(size - 1, r.size());
+            std::memcpy(buffer, r.data(), n);
+            buffer[n] = 0;
+        }
     });
 }
 

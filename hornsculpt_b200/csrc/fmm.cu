@@ -841,6 +841,25 @@ struct FmmOperator::Impl {
     std::vector<DevPlan> dm2m, dm2l, dl2l;
     std::vector<DevBuf> dLeaves, dLeafStart;
     std::vector<std::vector<uint32_t>> coaxClassOf;  // per kind*levels: local coax class index -> global
+    // The far-field apply as a CUDA graph per mode (0: operator, 1: right-hand
+    // side). After each prepare() the first apply of a mode runs its launches
+    // directly (and sizes every buffer they use); the second is captured and
+    // every later one replays the graph, the source and the result passing
+    // through fixed staging buffers (the reference captures its M2L chunks the
+    // same way on second contact, support_m2l_graph.hpp:52-78).
+    bool useGraphs = true;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    uint32_t applies[2] = {0, 0};
+    DevBuf stageIn, stageOut;
+    void dropGraphs() {
+        for (auto &g : graph)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        applies[0] = applies[1] = 0;
+    }
+    ~Impl() { dropGraphs(); }
 };
 
 namespace {
@@ -1128,8 +1147,14 @@ FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : 
 
 FmmOperator::~FmmOperator() = default;
 
+void FmmOperator::setGraphs(bool enabled) {
+    impl_->useGraphs = enabled;
+    impl_->dropGraphs();
+}
+
 void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
     Impl &I = *impl_;
+    I.dropGraphs();  // the tables and orders below change what a graph would replay
     k_ = k;
     levelInfo_.clear();
     if (tree_.ppFar.empty())
@@ -1260,6 +1285,41 @@ void FmmOperator::applyFarRhs(const double *q, uint32_t S, double *y, cudaStream
 }
 
 void FmmOperator::run(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer) {
+    Impl &I = *impl_;
+    const int mode = rhs ? 1 : 0;
+    const bool capturable = stream != nullptr && stream != cudaStreamLegacy && stream != cudaStreamPerThread;
+    if (!I.useGraphs || !capturable || tree_.ppFar.empty() || (!I.graph[mode] && I.applies[mode]++ == 0)) {
+        launchApply(src, rhs, y, stream, timer);
+        return;
+    }
+    const size_t inBytes = size_t(rhs ? I.T : I.N) * 16, outBytes = size_t(I.N) * 16;
+    if (!I.graph[mode]) {
+        I.stageIn.ensure(size_t(std::max(I.T, I.N)) * 16);  // allocated before the capture
+        I.stageOut.ensure(outBytes);
+        cudaGraph_t g = nullptr;
+        fmmCheck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed), "far-field graph capture");
+        try {
+            launchApply(I.stageIn.as<double>(), rhs, I.stageOut.as<double>(), stream, nullptr);
+        } catch (...) {
+            cudaStreamEndCapture(stream, &g);
+            if (g)
+                cudaGraphDestroy(g);
+            throw;
+        }
+        fmmCheck(cudaStreamEndCapture(stream, &g), "far-field graph capture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        fmmCheck(e, "far-field graph instantiation");
+        I.graph[mode] = exec;
+    }
+    TimedScope scope(timer, "fmm_far_graph", stream);
+    fmmCheck(cudaMemcpyAsync(I.stageIn.p, src, inBytes, cudaMemcpyDeviceToDevice, stream), "far-field graph input");
+    fmmCheck(cudaGraphLaunch(I.graph[mode], stream), "far-field graph launch");
+    fmmCheck(cudaMemcpyAsync(y, I.stageOut.p, outBytes, cudaMemcpyDeviceToDevice, stream), "far-field graph output");
+}
+
+void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer) {
     Impl &I = *impl_;
     const uint32_t N = I.N;
     const double2 *pv = reinterpret_cast<const double2 *>(src);

@@ -59,6 +59,8 @@ class FmmOperator {
     const std::vector<uint32_t> &nearRowStart() const { return nearRow_; }
     const std::vector<uint32_t> &nearCols() const { return nearCol_; }
     double wavenumber() const { return k_; }
+    // Replay of the far-field apply as a captured CUDA graph (on by default).
+    void setGraphs(bool enabled);
 
   private:
     struct Impl;
@@ -70,6 +72,7 @@ class FmmOperator {
     std::vector<std::pair<uint32_t, uint32_t>> panelPairs_;
     double k_ = 0;
     void run(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer);
+    void launchApply(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer);
 };
 
 // The fast-multipole linear system of one frequency: A = N + R F, with N the

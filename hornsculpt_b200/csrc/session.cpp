@@ -1,6 +1,8 @@
 // Solver session orchestration (cuda_solver.cu:1021-1853, dense form).
 #include "session.hpp"
 
+#include "autotune.hpp"
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -90,7 +92,8 @@ void validateRequest(const hs_request &r) {
     const bool fmm = o.acceleration == HS_FAST_MULTIPOLE;
     const unsigned w = o.fmm_preconditioner_block_width;
     if ((o.acceleration != HS_DENSE && !fmm) ||
-        (fmm && (o.fmm_leaf_support_capacity < 4 || o.fmm_leaf_support_capacity > 256 ||
+        (fmm && ((o.fmm_leaf_support_capacity != 0 && o.fmm_leaf_support_capacity < 4) ||
+                 o.fmm_leaf_support_capacity > 256 ||
                  !std::isfinite(o.fmm_separation_ratio) || o.fmm_separation_ratio < 1.5 || o.fmm_separation_ratio > 10 ||
                  o.fmm_maximum_iterations < 1 || o.fmm_maximum_iterations > 10000 || o.fmm_restart_length < 2 ||
                  o.fmm_restart_length > 300 ||
@@ -156,6 +159,7 @@ Session::Session(const MeshInput &mesh, uint32_t residency) : mesh_(mesh), resid
 }
 
 Session::~Session() {
+    dropGraphs();
     if (own_) {
         cudaStreamSynchronize(own_);
         cudaStreamDestroy(own_);
@@ -240,6 +244,7 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
         return;
     }
     planValid_ = false;
+    dropGraphs();  // captured chains hold the old plan's counts and rules
     const auto start = Clock::now();
     PlanSettings st{o.quadrature_order, o.singular_order, o.near_distance_ratio, o.near_relative_tolerance,
                     o.near_maximum_depth};
@@ -565,7 +570,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     // near-field workspace (no dense records or matrices).
     const uint32_t Bmax = fmmRequest ? 1 : chooseBatch(F, E, O, mixedForm, restart);
     if (fmmRequest)
-        ensureFmmWorkspace(o, E, O);
+        ensureFmmWorkspace(o, E, O, maxK);
     else
         ensureWorkspace(Bmax, E, O, mixedForm, restart);
     if (O)
@@ -612,10 +617,10 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                              T > kExactBinsT ? dBinOffsets_.as<uint64_t>() : nullptr};
         const bool mixed = o.precision == HS_PRECISION_MIXED;
         const bool fmmForm = o.acceleration == HS_FAST_MULTIPOLE;
-        if (!fmmForm)
-            assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws,
-                          dA_.as<double>(), dRhs_.as<double>(), dError_.as<int>(), s, &timer_, mixed);
-        cuda(cudaEventRecord(ev.assembled, s), "phase event");
+        if (!fmmForm)  // assembly, LU and initial solves: launches only, no host waits
+            runDenseChain(geo, ws, B, E, mixed, s);
+        else
+            cuda(cudaEventRecord(ev.assembled, s), "phase event");
         // the assembly error word is checked with the first residual norms
         const auto countWork = [&]() {
             std::vector<uint32_t> counts(size_t(B) * kBins);
@@ -642,7 +647,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             // near part plus expansion far field, block-Jacobi on the leaf
             // blocks and GMRES on near + expansion far field
             // (support_fmm_solve.cu:401-525).
-            FmmOperator &op = fmmOperator(o);
+            FmmOperator &op = fmmOperator(o, maxK, fmmTuneTolerance(o));
             const NearFieldLayout layout{dPanelRow_.as<uint32_t>(), dPanelCol_.as<uint32_t>(), op.nearPanelCol().size(),
                                          dPanelPairs_.as<uint2>(), op.nearPanelPairs().size(),
                                          fmmSystem_->nearRowDevice(), fmmSystem_->nearColDevice()};
@@ -733,39 +738,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             if (timer_.enabled())
                 countWork();
         } else {
-        // LU of every matrix of the batch (FP64, or an FP32 copy in the mixed
-        // form), then the initial solves.
-        const size_t matrixReals = size_t(B) * N * N * 2, vectorReals = size_t(B) * E * N * 2;
-        float *LU32 = dLU_.as<float>(), *work32 = dWork32_.as<float>();
-        if (mixed) {
-            {
-                TimedScope scope(&timer_, "round_fp32", s);
-                roundToFloat(dA_.as<double>(), LU32, matrixReals, s);
-            }
-            luFactorBatch(LU32, N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_, dLuPack_.as<float>());
-        } else {
-            cuda(cudaMemcpyAsync(dLU_.as<void>(), dA_.as<void>(), matrixReals * 8, cudaMemcpyDeviceToDevice, s),
-                 "factorization copy");
-            luFactorBatch(dLU_.as<double>(), N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, &timer_);
-        }
-        cuda(cudaEventRecord(ev.factored, s), "phase event");
-        // the LU status is checked with the first residual norms
-        if (mixed) {
-            {
-                TimedScope scope(&timer_, "round_fp32", s);
-                roundToFloat(dRhs_.as<double>(), work32, vectorReals, s);
-            }
-            luSolveBatch(LU32, dPivots_.as<int>(), N, B, E, work32, dSolveScratch_.as<void>(), s, &timer_);
-            cuda(cudaMemsetAsync(dX_.as<void>(), 0, vectorReals * 8, s), "solution reset");
-            TimedScope scope(&timer_, "add_correction", s);
-            addCorrectionBatch(dX_.as<double>(), work32, vectorReals, s);
-        } else {
-            cuda(cudaMemcpyAsync(dX_.as<void>(), dRhs_.as<void>(), vectorReals * 8, cudaMemcpyDeviceToDevice, s),
-                 "rhs copy");
-            luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), dSolveScratch_.as<void>(), s,
-                         &timer_);
-        }
-        cuda(cudaEventRecord(ev.solved, s), "phase event");
+        const size_t vectorReals = size_t(B) * E * N * 2;
+        float *LU32 = dLU_.as<float>();
         bool refining = false;  // a refinement solve between ev.refine0 and ev.refine1 awaits its time
         // FP64 refinement (cuda_solver.cu:1519-1581), per frequency. The mixed
         // form refines against the FP64 residual to min(tolerance, 1e-10).
@@ -1005,6 +979,126 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     return result;
 }
 
+// Assembly, LU and initial solves of one frequency batch (launches only; the
+// phase events are recorded with `eventFlags`, external inside a capture).
+void Session::denseChain(const AssemblyGeometry &geo, const AssemblyWorkspace &ws, uint32_t B, uint32_t E, bool mixed,
+                         cudaStream_t s, KernelTimer *timer, unsigned eventFlags) {
+    const uint32_t N = geo.N;
+    PhaseEvents &ev = phaseEvents();
+    assembleBatch(geo, dKs_.as<double>(), dGauss_.as<double>(), dFlux_.as<double>(), E, B, ws, dA_.as<double>(),
+                  dRhs_.as<double>(), dError_.as<int>(), s, timer, mixed);
+    cuda(cudaEventRecordWithFlags(ev.assembled, s, eventFlags), "phase event");
+    // LU of every matrix of the batch (FP64, or an FP32 copy in the mixed
+    // form), then the initial solves.
+    const size_t matrixReals = size_t(B) * N * N * 2, vectorReals = size_t(B) * E * N * 2;
+    float *LU32 = dLU_.as<float>(), *work32 = dWork32_.as<float>();
+    if (mixed) {
+        {
+            TimedScope scope(timer, "round_fp32", s);
+            roundToFloat(dA_.as<double>(), LU32, matrixReals, s);
+        }
+        luFactorBatch(LU32, N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, timer, dLuPack_.as<float>());
+    } else {
+        cuda(cudaMemcpyAsync(dLU_.as<void>(), dA_.as<void>(), matrixReals * 8, cudaMemcpyDeviceToDevice, s),
+             "factorization copy");
+        luFactorBatch(dLU_.as<double>(), N, B, dPivots_.as<int>(), dInfo_.as<int>(), s, timer);
+    }
+    cuda(cudaEventRecordWithFlags(ev.factored, s, eventFlags), "phase event");
+    // the LU status is checked with the first residual norms
+    if (mixed) {
+        {
+            TimedScope scope(timer, "round_fp32", s);
+            roundToFloat(dRhs_.as<double>(), work32, vectorReals, s);
+        }
+        luSolveBatch(LU32, dPivots_.as<int>(), N, B, E, work32, dSolveScratch_.as<void>(), s, timer);
+        cuda(cudaMemsetAsync(dX_.as<void>(), 0, vectorReals * 8, s), "solution reset");
+        TimedScope scope(timer, "add_correction", s);
+        addCorrectionBatch(dX_.as<double>(), work32, vectorReals, s);
+    } else {
+        cuda(cudaMemcpyAsync(dX_.as<void>(), dRhs_.as<void>(), vectorReals * 8, cudaMemcpyDeviceToDevice, s),
+             "rhs copy");
+        luSolveBatch(dLU_.as<double>(), dPivots_.as<int>(), N, B, E, dX_.as<double>(), dSolveScratch_.as<void>(), s,
+                     timer);
+    }
+    cuda(cudaEventRecordWithFlags(ev.solved, s, eventFlags), "phase event");
+}
+
+// The dense chain of a batch shape (B, E, form) is captured as a CUDA graph on
+// its second use with the same workspaces and plan, and replayed from then on.
+// With kernel profiling on the chain runs as plain launches, so that every
+// kernel family keeps its own timing.
+void Session::runDenseChain(const AssemblyGeometry &geo, const AssemblyWorkspace &ws, uint32_t B, uint32_t E,
+                            bool mixed, cudaStream_t s) {
+    const bool capturable = s != nullptr && s != cudaStreamLegacy && s != cudaStreamPerThread;
+    if (!graphs_ || timer_.enabled() || !capturable) {
+        denseChain(geo, ws, B, E, mixed, s, &timer_, cudaEventRecordDefault);
+        return;
+    }
+    // a graph is valid while every buffer it captured sits at the same address
+    // (buffers only grow, so the captured extents stay inside them)
+    uint64_t signature = generation_ * 0x9e3779b97f4a7c15ull;
+    for (const DeviceBuffer *b :
+         {&dPanels_, &dBounds_, &dMixedPanels_, &dIncOffsets_, &dIncPanel_, &dIncLocal_, &dRowScale_, &dError_,
+          &dPairCode_, &dTouching_, &dNearPairs_, &dPatches_, &dGauss_, &dSingularTable_, &dRecords_, &dColumns_,
+          &dPanelRhs_, &dBins_, &dBinCounts_, &dBinOffsets_, &dA_, &dLU_, &dRhs_, &dX_, &dPivots_, &dInfo_, &dKs_,
+          &dFlux_, &dWork32_, &dLuPack_, &dSolveScratch_})
+        signature = (signature ^ reinterpret_cast<uintptr_t>(b->as<void>())) * 0x100000001b3ull;
+    DenseGraph *hit = nullptr;
+    for (auto &g : denseGraphs_)
+        if (g.B == B && g.E == E && g.mixed == mixed && g.signature == signature)
+            hit = &g;
+    if (!hit) {
+        // graphs of superseded buffers are released
+        for (auto &g : denseGraphs_)
+            if (g.signature != signature && g.exec) {
+                cudaGraphExecDestroy(g.exec);
+                g.exec = nullptr;
+            }
+        std::erase_if(denseGraphs_, [&](const DenseGraph &g) { return g.signature != signature; });
+        denseGraphs_.push_back({B, E, mixed, signature, 0, nullptr});
+        hit = &denseGraphs_.back();
+    }
+    if (!hit->exec && hit->uses++ == 0) {
+        denseChain(geo, ws, B, E, mixed, s, &timer_, cudaEventRecordDefault);
+        return;
+    }
+    if (!hit->exec) {
+        cudaGraph_t g = nullptr;
+        cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed), "dense chain capture");
+        try {
+            denseChain(geo, ws, B, E, mixed, s, nullptr, cudaEventRecordExternal);
+        } catch (...) {
+            cudaStreamEndCapture(s, &g);
+            if (g)
+                cudaGraphDestroy(g);
+            throw;
+        }
+        cuda(cudaStreamEndCapture(s, &g), "dense chain capture");
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        cuda(e, "dense chain graph instantiation");
+        hit->exec = exec;
+    }
+    cuda(cudaGraphLaunch(hit->exec, s), "dense chain graph launch");
+    ++graphLaunches_;
+}
+
+void Session::dropGraphs() {
+    for (auto &g : denseGraphs_)
+        if (g.exec)
+            cudaGraphExecDestroy(g.exec);
+    denseGraphs_.clear();
+    ++generation_;
+}
+
+void Session::setGraphs(bool enabled) {
+    graphs_ = enabled;
+    dropGraphs();
+    if (fmm_)
+        fmm_->setGraphs(enabled);
+}
+
 void Session::debugAssemble(const hs_numerics &o, double planK, double k, const double *flux, double *matrix,
                             double *rhs) {
     preparePlan(o, planK, nullptr);
@@ -1031,9 +1125,15 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
     cuda(cudaStreamSynchronize(s), "CUDA synchronization");
 }
 
-void Session::ensureFmmWorkspace(const hs_numerics &o, uint32_t E, uint32_t O) {
+// Expansion tolerance the leaf-size tuning measures at: the working tolerance
+// of the solve (1 % of its residual target, as in the batch loop).
+double Session::fmmTuneTolerance(const hs_numerics &o) {
+    return std::clamp(.01 * o.relative_residual_tolerance, 1e-10, 1e-6);
+}
+
+void Session::ensureFmmWorkspace(const hs_numerics &o, uint32_t E, uint32_t O, double maxK) {
     const size_t T = space_.panels.size(), N = space_.vertices.size();
-    FmmOperator &op = fmmOperator(o);
+    FmmOperator &op = fmmOperator(o, maxK, fmmTuneTolerance(o));
     if (!fmmSystem_ || fmmSystemOp_ != &op || fmmBlockWidth_ != o.fmm_preconditioner_block_width) {
         fmmSystem_.reset();
         fmmBlockWidth_ = o.fmm_preconditioner_block_width;
@@ -1074,18 +1174,92 @@ void Session::ensureFmmWorkspace(const hs_numerics &o, uint32_t E, uint32_t O) {
     peakBytes_ = std::max(peakBytes_, bytes);
 }
 
-FmmOperator &Session::fmmOperator(const hs_numerics &o) {
+FmmOperator &Session::fmmOperator(const hs_numerics &o, double tuneK, double tuneTolerance) {
     FmmTreeSettings st;
     st.leafCapacity = o.fmm_leaf_support_capacity ? o.fmm_leaf_support_capacity : 32;
     st.separationRatio = std::isfinite(o.fmm_separation_ratio) && o.fmm_separation_ratio > 1 ? o.fmm_separation_ratio : 1.5;
+    if (o.fmm_leaf_support_capacity == 0 && tuneK > 0)
+        st.leafCapacity = tunedLeafCapacity(st.separationRatio, tuneK, tuneTolerance);
     if (!fmm_ || st.leafCapacity != fmmSettings_.leafCapacity || st.separationRatio != fmmSettings_.separationRatio) {
         fmmSystem_.reset();
         fmmSystemOp_ = nullptr;
         fmm_.reset();
         fmm_ = std::make_unique<FmmOperator>(space_, st);
+        fmm_->setGraphs(graphs_);
         fmmSettings_ = st;
     }
     return *fmm_;
+}
+
+// Leaf support capacity of the fast-multipole tree picked by the autotuner
+// (requests with capacity 0): per mesh size class and electrical size class,
+// each candidate tree is built and its operator apply (far expansions plus the
+// near product) timed at the request's top wavenumber; the fastest is kept for
+// the class. The leaf size moves work between the exact near part and the
+// expansions, so results differ between candidates within the expansion
+// tolerance, as for any explicit capacity.
+uint32_t Session::tunedLeafCapacity(double separation, double k, double tolerance) {
+    static constexpr uint32_t kCandidates[] = {8, 16, 32};
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (const auto &v : space_.vertices)
+        for (int d = 0; d < 3; ++d) {
+            const double x = d == 0 ? v.x : d == 1 ? v.y : v.z;
+            lo[d] = std::min(lo[d], x);
+            hi[d] = std::max(hi[d], x);
+        }
+    const double diameter = std::hypot(hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]);
+    const uint32_t T = uint32_t(space_.panels.size());
+    const int kd = int(std::floor(std::log2(std::max(1.0, k * diameter))));
+    const std::string key = "fmm_leaf_T2^" + std::to_string(31 - __builtin_clz(T | 1u)) + "_kD2^" + std::to_string(kd) +
+                            "_sep" + std::to_string(int(std::lround(separation * 10)));
+    Autotuner &tuner = Autotuner::instance();
+    const int known = tuner.choice(key);
+    if (known >= 0)
+        return kCandidates[known];
+    if (!tuner.enabled() || timer_.enabled())
+        return 16;
+    const cudaStream_t s = stream();
+    const size_t N = space_.vertices.size();
+    DeviceBuffer in, out;
+    in.ensure(N * 16);
+    out.ensure(N * 16);
+    cuda(cudaMemsetAsync(in.as<void>(), 0, N * 16, s), "tuning input");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cuda(cudaEventCreate(&e0), "tuning event");
+    cuda(cudaEventCreate(&e1), "tuning event");
+    std::vector<double> ms;
+    int best = 0;
+    try {
+        for (uint32_t cap : kCandidates) {
+            FmmTreeSettings st;
+            st.leafCapacity = cap;
+            st.separationRatio = separation;
+            FmmOperator op(space_, st);
+            FmmSystem system(op, dRowScale_.as<double>(), dMass_.as<double>(), 32);
+            cuda(cudaMemsetAsync(system.nearValues(), 0, std::max<size_t>(op.nearCols().size(), 1) * 16, s),
+                 "tuning near values");
+            op.setGraphs(false);
+            op.prepare(k, tolerance, s);
+            system.apply(in.as<double>(), 2 * N, 1, out.as<double>(), s, nullptr);  // warm-up
+            cuda(cudaEventRecord(e0, s), "tuning event");
+            system.apply(in.as<double>(), 2 * N, 1, out.as<double>(), s, nullptr);
+            cuda(cudaEventRecord(e1, s), "tuning event");
+            cuda(cudaEventSynchronize(e1), "tuning");
+            float t = 0;
+            cuda(cudaEventElapsedTime(&t, e0, e1), "tuning time");
+            ms.push_back(t);
+            if (t < ms[size_t(best)])
+                best = int(ms.size() - 1);
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    tuner.record(key, best, ms);
+    return kCandidates[best];
 }
 
 void Session::debugFmmFar(const hs_numerics &o, double k, double tolerance, const double *pressure, double *far,

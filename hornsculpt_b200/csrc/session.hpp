@@ -68,6 +68,10 @@ class Session {
                      std::vector<uint32_t> &nearRow, std::vector<uint32_t> &nearCol,
                      std::vector<FmmLevelInfo> &levels);
     KernelTimer &timer() { return timer_; }
+    // Replay of the per-batch dense chain and of the fast-multipole far-field
+    // apply as captured CUDA graphs (on by default); graph launches so far.
+    void setGraphs(bool enabled);
+    uint64_t graphLaunches() const { return graphLaunches_; }
     // Device bytes a solve may hold beyond the resident geometry and plan
     // (0: 60 % of free memory); bounds the frequency batch.
     void setMemoryBudget(size_t bytes) { memoryBudget_ = bytes; }
@@ -96,6 +100,21 @@ class Session {
     PhaseEvents phase_{};
     bool phaseReady_ = false;
     cudaStream_t stream() const { return external_ ? external_ : own_; }
+    void denseChain(const AssemblyGeometry &geo, const AssemblyWorkspace &ws, uint32_t B, uint32_t E, bool mixed,
+                    cudaStream_t s, KernelTimer *timer, unsigned eventFlags);
+    void runDenseChain(const AssemblyGeometry &geo, const AssemblyWorkspace &ws, uint32_t B, uint32_t E, bool mixed,
+                       cudaStream_t s);
+    void dropGraphs();
+    struct DenseGraph {
+        uint32_t B, E;
+        bool mixed;
+        uint64_t signature;
+        uint32_t uses;
+        cudaGraphExec_t exec;
+    };
+    std::vector<DenseGraph> denseGraphs_;
+    uint64_t generation_ = 0, graphLaunches_ = 0;
+    bool graphs_ = true;
 
     MeshInput mesh_;
     V3 origin_{};
@@ -123,14 +142,18 @@ class Session {
     size_t memoryBudget_ = 0;
     // fast-multipole form: operator on the support tree (built on first use
     // for a tree setting) and its workspaces
-    FmmOperator &fmmOperator(const hs_numerics &numerics);
+    // tuneK > 0: a capacity of 0 asks the autotuner (at wavenumber tuneK and
+    // expansion tolerance tuneTolerance) for the leaf size.
+    FmmOperator &fmmOperator(const hs_numerics &numerics, double tuneK = 0, double tuneTolerance = 1e-8);
+    uint32_t tunedLeafCapacity(double separation, double k, double tolerance);
+    static double fmmTuneTolerance(const hs_numerics &numerics);
     std::unique_ptr<FmmOperator> fmm_;
     std::unique_ptr<FmmSystem> fmmSystem_;
     const FmmOperator *fmmSystemOp_ = nullptr;
     uint32_t fmmBlockWidth_ = 0;
     FmmTreeSettings fmmSettings_{};
     DeviceBuffer dFmmIn_, dFmmOut_, dNearWork_, dPanelRow_, dPanelCol_, dPanelPairs_, dAuditWork_, dAuditFine_;
-    void ensureFmmWorkspace(const hs_numerics &numerics, uint32_t E, uint32_t O);
+    void ensureFmmWorkspace(const hs_numerics &numerics, uint32_t E, uint32_t O, double maxK);
 };
 
 // Device bytes of one solve of F frequencies on a mesh with T panels and N

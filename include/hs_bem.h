@@ -63,7 +63,7 @@ typedef struct hs_numerics {
     uint32_t maximum_refinement_steps;    /* <= 10 (default 3) */
     uint32_t acceleration;                /* hs_acceleration */
     uint32_t precision;                   /* hs_precision */
-    uint32_t fmm_leaf_support_capacity;   /* 16 */
+    uint32_t fmm_leaf_support_capacity;   /* 16; 0: chosen by the autotuner (below) */
     double fmm_separation_ratio;          /* 1.5 */
     uint32_t fmm_maximum_iterations;      /* 300 */
     uint32_t fmm_restart_length;          /* 40 */
@@ -192,6 +192,33 @@ hs_status hs_device_description(char *buffer, size_t size);
 hs_status hs_bem_session_set_profiling(hs_bem_session *session, int32_t enabled);
 hs_status hs_bem_session_profile(const hs_bem_session *session, char *names_buffer, size_t names_size,
                                  double *ms, uint64_t *launches, size_t capacity, size_t *count);
+
+/* CUDA graphs (no reference counterpart beyond its captured M2L chunks,
+ * support_m2l_graph.hpp:52-78): a session replays the launch chain of a dense
+ * frequency batch (assembly, LU, initial solves) and the fast-multipole
+ * far-field apply as captured graphs. A chain is captured on its second use
+ * with the same batch shape and buffers (the first use runs its launches
+ * directly) and replayed after that; re-planning or regrown buffers retire
+ * it. With kernel profiling on, the dense chain runs as plain launches so
+ * each kernel family keeps its own time. Results are the same either way (the
+ * graph holds the same launches). On by default; graph_launches counts dense
+ * chain replays of the session. */
+hs_status hs_bem_session_set_graphs(hs_bem_session *session, int32_t enabled);
+hs_status hs_bem_session_graph_launches(const hs_bem_session *session, uint64_t *launches);
+
+/* Launch-shape autotuner (process-wide; the reference has no counterpart).
+ * For each kernel family and size class (form, rule, batch, mesh size to a
+ * power of two) the first solve outside a graph capture and outside a
+ * profiled solve times the candidate launch shapes once with CUDA events and
+ * keeps the fastest. Candidates spread the same independent work items
+ * differently over the grid, so a choice changes speed, never results. A
+ * fast-multipole request with fmm_leaf_support_capacity = 0 has its leaf size
+ * chosen the same way (per mesh size and electrical size class, by timing one
+ * operator apply per candidate tree of 8, 16, 32 supports). The report lists
+ * "class=choice:ms/ms/...;" per tuned class (needed: its size with the NUL). */
+hs_status hs_autotune_set_enabled(int32_t enabled);
+hs_status hs_autotune_clear(void);
+hs_status hs_autotune_report(char *buffer, size_t size, size_t *needed);
 
 /* Work counters of the solves since profiling was last enabled, in this
  * order: regular unordered pairs with the 6/12/16/64-point rules (4 values),

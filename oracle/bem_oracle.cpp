@@ -18,6 +18,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <mutex>
 
 namespace oracle {
 namespace {
@@ -280,8 +281,29 @@ System assemble(const Problem &P, const Plan &plan, const Rules &R, const Numeri
     return S;
 }
 
+// Optional LAPACK (zgetrf / zgetrs, Fortran calling convention) supplied by
+// the caller as function pointers, for the timed CPU baseline: the reference
+// factors with a library LU (cusolverDnCgetrf), so the baseline does too. The
+// row-major matrix is LAPACK's column-major transpose; A x = b is solved as
+// (A^T)^T x = b with trans = 'T'.
+using ZgetrfFn = void (*)(int *, int *, cplx *, int *, int *, int *);
+using ZgetrsFn = void (*)(char *, int *, int *, cplx *, int *, int *, cplx *, int *, int *);
+ZgetrfFn gZgetrf = nullptr;
+ZgetrsFn gZgetrs = nullptr;
+
 // Partial-pivot LU in place (row-major), then forward/back substitution.
 void luFactor(std::vector<cplx> &A, size_t N, std::vector<size_t> &piv) {
+    if (gZgetrf) {
+        int n = int(N), info = 0;
+        std::vector<int> ipiv(N);
+        gZgetrf(&n, &n, A.data(), &n, ipiv.data(), &info);
+        if (info != 0)
+            throw std::runtime_error("singular Burton-Miller matrix");
+        piv.resize(N);
+        for (size_t i = 0; i < N; ++i)
+            piv[i] = size_t(ipiv[i]);  // 1-based LAPACK pivots mark the LAPACK factors
+        return;
+    }
     piv.resize(N);
     for (size_t c = 0; c < N; ++c) {
         size_t best = c;
@@ -308,6 +330,15 @@ void luFactor(std::vector<cplx> &A, size_t N, std::vector<size_t> &piv) {
     }
 }
 void luSolve(const std::vector<cplx> &LU, size_t N, const std::vector<size_t> &piv, std::vector<cplx> &x) {
+    if (gZgetrs) {
+        char trans = 'T';
+        int n = int(N), one = 1, info = 0;
+        std::vector<int> ipiv(piv.begin(), piv.end());
+        gZgetrs(&trans, &n, &one, const_cast<cplx *>(LU.data()), &n, ipiv.data(), x.data(), &n, &info);
+        if (info != 0)
+            throw std::runtime_error("LAPACK zgetrs failed");
+        return;
+    }
     for (size_t c = 0; c < N; ++c)
         if (piv[c] != c)
             std::swap(x[c], x[piv[c]]);
@@ -485,6 +516,13 @@ struct oracle_numerics {
 };
 
 const char *oracle_last_error() { return lastError.c_str(); }
+
+// LAPACK zgetrf / zgetrs for oracle_solve's factorisation (both null: the
+// built-in textbook LU).
+void oracle_set_lapack(void *zgetrf, void *zgetrs) {
+    gZgetrf = reinterpret_cast<ZgetrfFn>(zgetrf);
+    gZgetrs = reinterpret_cast<ZgetrsFn>(zgetrs);
+}
 
 // Builds the interaction plan for a mesh at planning wavenumber maxK.
 int oracle_plan_build(const double *verts, size_t nv, const uint32_t *tris, size_t nt, const oracle_numerics *nm,
@@ -682,7 +720,31 @@ int oracle_solve(const double *verts, size_t nv, const uint32_t *tris, const uin
                 fmax = std::max(fmax, freqs[f]);
         const double maxK = 2 * M_PI * fmax / soundSpeed;
         PlanSettings st{num.quadratureOrder, num.singularOrder, num.nearRatio, num.nearTol, num.nearDepth};
-        const Plan plan = makePlan(sp, st, maxK);
+        // The plan of the last call is reused when mesh, settings and planning
+        // wavenumber repeat (a sweep's later calls, like a solver session's cache).
+        static std::mutex cacheMutex;
+        static std::vector<double> cachedVerts;
+        static std::vector<uint32_t> cachedTris;
+        static std::vector<double> cachedKey;
+        static std::shared_ptr<const Plan> cachedPlan;
+        std::shared_ptr<const Plan> planPtr;
+        {
+            const std::vector<double> key{double(num.quadratureOrder), double(num.singularOrder), num.nearRatio,
+                                          num.nearTol, double(num.nearDepth), maxK};
+            std::lock_guard<std::mutex> lock(cacheMutex);
+            if (cachedPlan && key == cachedKey && cachedVerts.size() == 3 * nv && cachedTris.size() == 3 * nt &&
+                std::equal(cachedVerts.begin(), cachedVerts.end(), verts) &&
+                std::equal(cachedTris.begin(), cachedTris.end(), tris))
+                planPtr = cachedPlan;
+            else {
+                planPtr = std::make_shared<const Plan>(makePlan(sp, st, maxK));
+                cachedVerts.assign(verts, verts + 3 * nv);
+                cachedTris.assign(tris, tris + 3 * nt);
+                cachedKey = key;
+                cachedPlan = planPtr;
+            }
+        }
+        const Plan &plan = *planPtr;
         const Rules R = makeRules(num);
         // Per-panel velocity per excitation.
         std::vector<cplx> vel(ne * T, 0);

@@ -69,6 +69,28 @@ def _load_oracle():
     return _oracle
 
 
+def use_lapack(enabled: bool = True) -> str:
+    """Makes ``solve`` factor with LAPACK zgetrf / zgetrs (scipy's OpenBLAS,
+    through the function pointers scipy.linalg.cython_lapack exports) instead
+    of the built-in textbook LU; returns the provider's description."""
+    lib = _load_oracle()
+    lib.oracle_set_lapack.argtypes = [_P, _P]
+    if not enabled:
+        lib.oracle_set_lapack(None, None)
+        return "textbook LU"
+    import scipy
+    import scipy.linalg.cython_lapack as cl
+    get = C.pythonapi.PyCapsule_GetPointer
+    get.restype = _P
+    get.argtypes = [C.py_object, C.c_char_p]
+    name = C.pythonapi.PyCapsule_GetName
+    name.restype = C.c_char_p
+    name.argtypes = [C.py_object]
+    fns = [get(cl.__pyx_capi__[f], name(cl.__pyx_capi__[f])) for f in ("zgetrf", "zgetrs")]
+    lib.oracle_set_lapack(*fns)
+    return f"LAPACK zgetrf/zgetrs from scipy {scipy.__version__} (OpenBLAS)"
+
+
 def reference_available() -> bool:
     return (HERE / "_ref" / "libhsref.so").exists()
 

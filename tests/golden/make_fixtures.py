@@ -1,9 +1,9 @@
 """Regenerates the golden fixtures of this directory from the reference tree.
 
-Run in a container where the reference is mounted (default /root/reference)
-after `make -C oracle` has compiled oracle/_ref/libhsref.so:
+Run where the reference tree is mounted, after `make -C oracle
+REFERENCE=<reference root>` has compiled oracle/_ref/libhsref.so:
 
-    python tests/golden/make_fixtures.py [reference root]
+    python tests/golden/make_fixtures.py <reference root>
 
 Writes
   beat_sphere_512.json       external BEAT CPU FP64 observer pressures on the
@@ -81,4 +81,6 @@ def main(reference: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py <reference root>")
+    main(sys.argv[1])
