@@ -23,6 +23,7 @@
 #include <stdexcept>
 #include <string>
 #include <tuple>
+#include <type_traits>
 
 namespace hsb {
 namespace {
@@ -97,6 +98,27 @@ __device__ __forceinline__ double2 cmulConj(double2 a, double2 b) {  // conj(a) 
     return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
 }
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+
+// Complex arithmetic of either precision (the translations run in FP64, or in
+// FP32 on scaled coefficients in the mixed form).
+template <class R> struct CxOf;
+template <> struct CxOf<double> {
+    using T = double2;
+};
+template <> struct CxOf<float> {
+    using T = float2;
+};
+template <class R> using C2R = typename CxOf<R>::T;
+template <class R, class A, class B> __device__ __forceinline__ C2R<R> mkc(A x, B y) {
+    C2R<R> v;
+    v.x = R(x);
+    v.y = R(y);
+    return v;
+}
+template <class R> __device__ __forceinline__ C2R<R> cmulT(C2R<R> a, C2R<R> b) {
+    return mkc<R>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <class R> __device__ __forceinline__ C2R<R> caddT(C2R<R> a, C2R<R> b) { return mkc<R>(a.x + b.x, a.y + b.y); }
 
 // Warp table of the regular solid harmonics at d: j_n(k|d|) (n <= P),
 // Theta_n^m(cos t) (triIndex) and exp(i m phi) (m <= P).
@@ -192,7 +214,8 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
                                                  const uint32_t *__restrict__ leaves, const uint32_t *__restrict__ itemStart,
                                                  const FmmItem *__restrict__ items, const double *__restrict__ centers,
                                                  const uint64_t *__restrict__ coefOffset, int p, double k,
-                                                 const double2 *__restrict__ pvec, double2 *M, int rhsMode) {
+                                                 const double2 *__restrict__ pvec, double2 *M, int rhsMode,
+                                                 float2 *M32, const double *__restrict__ sigma) {
     extern __shared__ double smem[];
     const int P = p;
     const int nch = rhsMode ? 1 : 6;
@@ -206,6 +229,7 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
     const uint32_t points = (i1 - i0) * kRulePts;
     const int nc = (P + 1) * (P + 1);
     double2 *out = M + coefOffset[leaf];
+    float2 *out32 = M32 ? M32 + coefOffset[leaf] : nullptr;
     const PointTable mine = tableAt(tables + warp * td, P);
     for (int chunk = 0; chunk * 256 < nc; ++chunk) {
         const int kk = chunk * 256 + threadIdx.x;
@@ -239,9 +263,14 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
                 }
             __syncthreads();
         }
-        if (kk < nc)
-            for (int ch = 0; ch < nch; ++ch)
-                out[size_t(ch) * nc + kk] = acc[ch];
+        if (kk < nc) {
+            if (out32)  // scaled FP32 moments: M sigma_n, sigma_n = (2n+1)!! / (k a)^n of the level
+                for (int ch = 0; ch < nch; ++ch)
+                    out32[size_t(ch) * nc + kk] = make_float2(float(acc[ch].x * sigma[n]), float(acc[ch].y * sigma[n]));
+            else
+                for (int ch = 0; ch < nch; ++ch)
+                    out[size_t(ch) * nc + kk] = acc[ch];
+        }
     }
 }
 
@@ -253,26 +282,26 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
 // The channels [blockIdx.y * CPC, +CPC) of the output node go to one CTA:
 // channels are independent outputs, so spreading them over CTAs multiplies
 // the grid (few output nodes on the coarse levels) with no reduction.
-template <int CPC>
+template <int CPC, class R>
 __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restrict__ outNodes,
                                                        const uint32_t *__restrict__ linkStart,
                                                        const TransLink *__restrict__ links, int pin, int pout,
-                                                       const double2 *__restrict__ inCoef, double2 *outCoef,
+                                                       const C2R<R> *__restrict__ inCoef, C2R<R> *outCoef,
                                                        const uint64_t *__restrict__ coefOffset,
-                                                       const double *__restrict__ wigner,
+                                                       const R *__restrict__ wigner,
                                                        const uint64_t *__restrict__ wignerStart,
-                                                       const double2 *__restrict__ coax,
+                                                       const C2R<R> *__restrict__ coax,
                                                        const uint64_t *__restrict__ coaxStart, int zeroFirst,
-                                                       int nch, int K, double2 *partial) {
+                                                       int nch, int K, C2R<R> *partial) {
     constexpr int chunkCh = CPC;
     extern __shared__ double smem[];
     const int nin = (pin + 1) * (pin + 1), nout = (pout + 1) * (pout + 1);
     const int pmax = pin > pout ? pin : pout;
     const int nmax = nin > nout ? nin : nout;
-    double2 *eph = reinterpret_cast<double2 *>(smem);
-    double2 *a = eph + (pmax + 1);
-    double2 *b = a + size_t(chunkCh) * nmax;
-    double2 *cbuf = b + size_t(chunkCh) * nmax;
+    C2R<R> *eph = reinterpret_cast<C2R<R> *>(smem);
+    C2R<R> *a = eph + (pmax + 1);
+    C2R<R> *b = a + size_t(chunkCh) * nmax;
+    C2R<R> *cbuf = b + size_t(chunkCh) * nmax;
     // K CTAs share an output node's links (contiguous parts); with K > 1 each
     // writes its own partial sum, added in a fixed order by reduceKernel
     const uint32_t oi = blockIdx.x / K, part = blockIdx.x % K;
@@ -280,22 +309,22 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
     const int cFirst = blockIdx.y * CPC, cEnd = min(nch, cFirst + CPC);
     if (cFirst >= nch)
         return;
-    double2 *out = K > 1 ? partial + size_t(blockIdx.x) * 6 * nout : outCoef + coefOffset[node];
+    C2R<R> *out = K > 1 ? partial + size_t(blockIdx.x) * 6 * nout : outCoef + coefOffset[node];
     if (zeroFirst || K > 1)
         for (int i = cFirst * nout + threadIdx.x; i < cEnd * nout; i += blockDim.x)
-            out[i] = make_double2(0, 0);
+            out[i] = mkc<R>(0, 0);
     __syncthreads();
     const uint32_t l0 = linkStart[oi], len = linkStart[oi + 1] - l0;
     const uint32_t lBegin = l0 + uint32_t(uint64_t(len) * part / K), lEnd = l0 + uint32_t(uint64_t(len) * (part + 1) / K);
     for (uint32_t li = lBegin; li < lEnd; ++li) {
         const TransLink L = links[li];
-        const double2 *in = inCoef + coefOffset[L.source];
-        const double *dtab = wigner + wignerStart[L.wclass];
-        const double2 *ctab = coax + coaxStart[L.cclass];
+        const C2R<R> *in = inCoef + coefOffset[L.source];
+        const R *dtab = wigner + wignerStart[L.wclass];
+        const C2R<R> *ctab = coax + coaxStart[L.cclass];
         for (int m = threadIdx.x; m <= pmax; m += blockDim.x) {
             double sn, cs;
             sincos(m * L.phi, &sn, &cs);
-            eph[m] = make_double2(cs, sn);
+            eph[m] = mkc<R>(cs, sn);
         }
         __syncthreads();
         for (int c0 = cFirst; c0 < cEnd; c0 += chunkCh) {
@@ -305,8 +334,8 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 const int ch = i / nin, kk = i - ch * nin;
                 int n, m;
                 decode(kk, n, m);
-                const double2 e = m >= 0 ? eph[m] : make_double2(eph[-m].x, -eph[-m].y);
-                a[ch * nin + kk] = cmul(in[size_t(c0 + ch) * nin + kk], e);
+                const C2R<R> e = m >= 0 ? eph[m] : mkc<R>(eph[-m].x, -eph[-m].y);
+                a[ch * nin + kk] = cmulT<R>(in[size_t(c0 + ch) * nin + kk], e);
             }
             __syncthreads();
             // forward rotation: b[n, m'] = sum_m a[n, m] d^n[m, m']
@@ -314,17 +343,17 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 int n, mp;
                 decode(kk, n, mp);
                 const int w = 2 * n + 1, base = n * n;
-                const double *d = dtab + wignerOffset(n) + (mp + n);
-                double2 acc[CPC];
+                const R *d = dtab + wignerOffset(n) + (mp + n);
+                C2R<R> acc[CPC];
 #pragma unroll
                 for (int ch = 0; ch < CPC; ++ch)
-                    acc[ch] = make_double2(0, 0);
+                    acc[ch] = mkc<R>(0, 0);
                 for (int j = 0; j < w; ++j) {
-                    const double dv = d[size_t(j) * w];
+                    const R dv = d[size_t(j) * w];
 #pragma unroll
                     for (int ch = 0; ch < CPC; ++ch)
                         if (ch < cc) {
-                            const double2 v = a[ch * nin + base + j];
+                            const C2R<R> v = a[ch * nin + base + j];
                             acc[ch].x += v.x * dv;
                             acc[ch].y += v.y * dv;
                         }
@@ -340,23 +369,23 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 int np, m;
                 decode(kk, np, m);
                 const int am = m < 0 ? -m : m;
-                double2 acc[CPC];
+                C2R<R> acc[CPC];
 #pragma unroll
                 for (int ch = 0; ch < CPC; ++ch)
-                    acc[ch] = make_double2(0, 0);
+                    acc[ch] = mkc<R>(0, 0);
                 if (am <= pin) {
                     size_t off = 0;
                     for (int j = 0; j < am; ++j)
                         off += size_t(pin + 1 - j) * (pout + 1 - j);
                     const int wo = pout + 1 - am;
-                    const double2 *C = ctab + off + (np - am);
+                    const C2R<R> *C = ctab + off + (np - am);
                     for (int n = am; n <= pin; ++n) {
-                        const double2 cv = C[size_t(n - am) * wo];
+                        const C2R<R> cv = C[size_t(n - am) * wo];
                         const int src = n * n + n + m;
 #pragma unroll
                         for (int ch = 0; ch < CPC; ++ch)
                             if (ch < cc)
-                                acc[ch] = cadd(acc[ch], cmul(cv, b[ch * nin + src]));
+                                acc[ch] = caddT<R>(acc[ch], cmulT<R>(cv, b[ch * nin + src]));
                     }
                 }
 #pragma unroll
@@ -370,27 +399,27 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
                 int n, m1;
                 decode(kk, n, m1);
                 const int w = 2 * n + 1, base = n * n;
-                const double *d = dtab + wignerOffset(n) + size_t(m1 + n) * w;
-                double2 acc[CPC];
+                const R *d = dtab + wignerOffset(n) + size_t(m1 + n) * w;
+                C2R<R> acc[CPC];
 #pragma unroll
                 for (int ch = 0; ch < CPC; ++ch)
-                    acc[ch] = make_double2(0, 0);
+                    acc[ch] = mkc<R>(0, 0);
                 for (int j = 0; j < w; ++j) {
-                    const double dv = d[j];
+                    const R dv = d[j];
 #pragma unroll
                     for (int ch = 0; ch < CPC; ++ch)
                         if (ch < cc) {
-                            const double2 v = cbuf[ch * nout + base + j];
+                            const C2R<R> v = cbuf[ch * nout + base + j];
                             acc[ch].x += v.x * dv;
                             acc[ch].y += v.y * dv;
                         }
                 }
-                const double2 e = m1 >= 0 ? make_double2(eph[m1].x, -eph[m1].y) : eph[-m1];
+                const C2R<R> e = m1 >= 0 ? mkc<R>(eph[m1].x, -eph[m1].y) : eph[-m1];
 #pragma unroll
                 for (int ch = 0; ch < CPC; ++ch)
                     if (ch < cc) {
                         const size_t o = size_t(c0 + ch) * nout + kk;
-                        out[o] = cadd(out[o], cmul(acc[ch], e));
+                        out[o] = caddT<R>(out[o], cmulT<R>(acc[ch], e));
                     }
             }
             __syncthreads();
@@ -399,15 +428,16 @@ __global__ void __launch_bounds__(256) translateKernel(const uint32_t *__restric
 }
 
 // out[node] (+)= sum over k of the K partial sums of the node, in order of k.
+template <class R>
 __global__ void reduceKernel(const uint32_t *__restrict__ outNodes, const uint64_t *__restrict__ coefOffset,
-                             const double2 *__restrict__ partial, int K, int nout, int nch, int assign,
-                             double2 *outCoef) {
+                             const C2R<R> *__restrict__ partial, int K, int nout, int nch, int assign,
+                             C2R<R> *outCoef) {
     const uint32_t oi = blockIdx.x;
-    double2 *out = outCoef + coefOffset[outNodes[oi]];
+    C2R<R> *out = outCoef + coefOffset[outNodes[oi]];
     for (int e = threadIdx.x; e < nch * nout; e += blockDim.x) {
-        double2 acc = assign ? make_double2(0, 0) : out[e];
+        C2R<R> acc = assign ? mkc<R>(0, 0) : out[e];
         for (int k = 0; k < K; ++k)
-            acc = cadd(acc, partial[(size_t(oi) * K + k) * 6 * nout + e]);
+            acc = caddT<R>(acc, partial[(size_t(oi) * K + k) * 6 * nout + e]);
         out[e] = acc;
     }
 }
@@ -436,6 +466,25 @@ __device__ __forceinline__ double2 coefAt(const double2 *L, int p, int n, int m)
     return L[coefIndex(n, m)];
 }
 
+// A leaf's local coefficients (channels x nc) into shared memory: FP64 as
+// stored, or the mixed form's scaled FP32 locals L^ = L tau_n unscaled to
+// L = L^ sigma_n (tau_n = 1 / sigma_n).
+__device__ void loadLocals(const double2 *L64, const float2 *L32, const double *sigma, uint64_t offset, int channels,
+                           int nc, double2 *Ls) {
+    if (L32) {
+        for (int i = threadIdx.x; i < channels * nc; i += blockDim.x) {
+            int n, m;
+            decode(i % nc, n, m);
+            const float2 v = L32[offset + i];
+            Ls[i] = make_double2(double(v.x) * sigma[n], double(v.y) * sigma[n]);
+        }
+    } else {
+        for (int i = threadIdx.x; i < channels * nc; i += blockDim.x)
+            Ls[i] = L64[offset + i];
+    }
+    __syncthreads();
+}
+
 // L2P of the leaves of one level: forms D = div V (degree p + 1) in shared
 // memory, then one warp per item evaluates V, W, D at its quadrature points
 // and writes the item's incidence contributions
@@ -444,7 +493,8 @@ __global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ pa
                                                  const uint32_t *__restrict__ leaves, const uint32_t *__restrict__ itemStart,
                                                  const FmmItem *__restrict__ items, const double *__restrict__ centers,
                                                  const uint64_t *__restrict__ coefOffset, int p, double k,
-                                                 const double2 *__restrict__ Lcoef, double2 *far) {
+                                                 const double2 *__restrict__ Lcoef, double2 *far,
+                                                 const float2 *__restrict__ L32, const double *__restrict__ sigma) {
     extern __shared__ double smem[];
     const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
     const size_t td = tableDoubles(P);
@@ -453,9 +503,7 @@ __global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ pa
     double2 *Ld = Ls + 6 * nc;                        // [nd]
     double *tables = reinterpret_cast<double *>(Ld + nd);
     const uint32_t leaf = leaves[blockIdx.x];
-    const double2 *L = Lcoef + coefOffset[leaf];
-    for (int i = threadIdx.x; i < 6 * nc; i += blockDim.x)
-        Ls[i] = L[i];
+    loadLocals(Lcoef, L32, sigma, coefOffset[leaf], 6, nc, Ls);
     __syncthreads();
     // D = dx Vx + dy Vy + dz Vz = (d+ U- + d- U+) / 2 + dz Vz, U-+ = Vx -+ i Vy (times k)
     for (int kk = threadIdx.x; kk < nd; kk += blockDim.x) {
@@ -556,7 +604,8 @@ __global__ void __launch_bounds__(256) l2pRhsKernel(const FmmPanel *__restrict__
                                                     const uint32_t *__restrict__ itemStart,
                                                     const FmmItem *__restrict__ items, const double *__restrict__ centers,
                                                     const uint64_t *__restrict__ coefOffset, int p, double k,
-                                                    const double2 *__restrict__ Lcoef, double2 *far) {
+                                                    const double2 *__restrict__ Lcoef, double2 *far,
+                                                    const float2 *__restrict__ L32, const double *__restrict__ sigma) {
     extern __shared__ double smem[];
     const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
     const size_t td = tableDoubles(P);
@@ -565,9 +614,7 @@ __global__ void __launch_bounds__(256) l2pRhsKernel(const FmmPanel *__restrict__
     double2 *Lg = Ls + nc;                            // [3][nd]: d/dx, d/dy, d/dz
     double *tables = reinterpret_cast<double *>(Lg + 3 * nd);
     const uint32_t leaf = leaves[blockIdx.x];
-    const double2 *L = Lcoef + coefOffset[leaf];
-    for (int i = threadIdx.x; i < nc; i += blockDim.x)
-        Ls[i] = L[i];
+    loadLocals(Lcoef, L32, sigma, coefOffset[leaf], 1, nc, Ls);
     __syncthreads();
     for (int kk = threadIdx.x; kk < nd; kk += blockDim.x) {
         int n, m;
@@ -689,6 +736,39 @@ __global__ void coaxKernel(uint32_t classes, const int *__restrict__ pin, const 
             acc.y += sg * g[idx] * f[l].y;
         }
         coax[start[cls] + e] = acc;
+    }
+}
+
+// FP32 coaxial tables of the mixed form: each entry (class, |m|, n, n') of the
+// FP64 table times exp(logRow[class][n'] + logCol[class][n]), the sigma factors
+// that take the scaled input coefficient to its unscaled value and the
+// unscaled output to its scaled value (the exponent split in two so that no
+// FP64 intermediate overflows).
+__global__ void coaxScaleKernel(uint32_t classes, const int *__restrict__ pin, const int *__restrict__ pout,
+                                const uint64_t *__restrict__ start, const double2 *__restrict__ coax,
+                                const double *__restrict__ logRow, const double *__restrict__ logCol, int stride,
+                                float2 *coax32) {
+    const uint32_t cls = blockIdx.y;
+    if (cls >= classes)
+        return;
+    const int a = pin[cls], b = pout[cls];
+    size_t total = 0;
+    for (int j = 0; j <= min(a, b); ++j)
+        total += size_t(a + 1 - j) * (b + 1 - j);
+    for (size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x; e < total; e += size_t(gridDim.x) * blockDim.x) {
+        size_t off = 0;
+        int mm = 0;
+        while (off + size_t(a + 1 - mm) * (b + 1 - mm) <= e) {
+            off += size_t(a + 1 - mm) * (b + 1 - mm);
+            ++mm;
+        }
+        const size_t r = e - off;
+        const int wo = b + 1 - mm;
+        const int n = mm + int(r / wo), np = mm + int(r % wo);
+        const double ex = logRow[size_t(cls) * stride + np] + logCol[size_t(cls) * stride + n];
+        const double half = exp(0.5 * ex);
+        const double2 v = coax[start[cls] + e];
+        coax32[start[cls] + e] = make_float2(float(v.x * half * half), float(v.y * half * half));
     }
 }
 
@@ -847,6 +927,18 @@ struct FmmOperator::Impl {
     // every later one replays the graph, the source and the result passing
     // through fixed staging buffers (the reference captures its M2L chunks the
     // same way on second contact, support_m2l_graph.hpp:52-78).
+    // Mixed form (setFp32): scaled FP32 expansions. With a_l the level's node
+    // radius and sigma_n = (2n+1)!! / (k a_l)^n, moments are stored as
+    // M sigma_n and locals as L / sigma_n, both O(1) where the unscaled
+    // coefficients span many decades (h_n(k t) reaches 1e75 at low k t); the
+    // coaxial tables carry the matching factors, rotations act within a degree
+    // and commute with them. P2M and L2P stay FP64 and convert at the boundary.
+    bool fp32 = false;
+    DevBuf Mc32, Lc32, partial32, coax32, wigner32, sigma, logRow, logCol;
+    std::vector<double> hostWigner;
+    bool wigner32Valid = false;
+    int sigmaStride = 0;
+    const double *levelSigma(int l) const { return fp32 ? sigma.as<double>() + size_t(l) * sigmaStride : nullptr; }
     bool useGraphs = true;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint32_t applies[2] = {0, 0};
@@ -1147,6 +1239,11 @@ FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : 
 
 FmmOperator::~FmmOperator() = default;
 
+void FmmOperator::setFp32(bool enabled) {
+    impl_->fp32 = enabled;
+    impl_->dropGraphs();
+}
+
 void FmmOperator::setGraphs(bool enabled) {
     impl_->useGraphs = enabled;
     impl_->dropGraphs();
@@ -1211,6 +1308,8 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
         }
         uploadVec(I.wigner, tab, stream);
         uploadVec(I.wignerStart, start, stream);
+        I.hostWigner = std::move(tab);
+        I.wigner32Valid = false;
     }
     // coaxial classes of this wavenumber
     int P = 0;
@@ -1239,13 +1338,24 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
         return uint32_t(pin.size() - 1);
     };
     I.coaxClassOf.assign(3 * levels, {});
+    // per class: (level, sign) of the log-sigma factor of its output degree and of its input degree
+    std::vector<std::pair<int, int>> rowScale, colScale;
     for (int l = I.lmin; l < levels; ++l) {
-        for (const auto &u : I.m2l[l].coaxUse)
+        for (const auto &u : I.m2l[l].coaxUse) {  // M = M^ / sigma_l in, L^ = L / sigma_l out
             I.coaxClassOf[l].push_back(addClass(I.order[l], I.order[l], std::get<1>(u), true));
-        for (const auto &u : I.m2m[l].coaxUse)
+            rowScale.push_back({l, -1});
+            colScale.push_back({l, -1});
+        }
+        for (const auto &u : I.m2m[l].coaxUse) {  // child moments M^ / sigma_(l+1) in, M sigma_l out
             I.coaxClassOf[levels + l].push_back(addClass(I.order[l + 1], I.order[l], std::get<1>(u), false));
-        for (const auto &u : I.l2l[l].coaxUse)
+            rowScale.push_back({l, 1});
+            colScale.push_back({l + 1, -1});
+        }
+        for (const auto &u : I.l2l[l].coaxUse) {  // parent locals L^ sigma_(l-1) in, L / sigma_l out
             I.coaxClassOf[2 * levels + l].push_back(addClass(I.order[l - 1], I.order[l], std::get<1>(u), false));
+            rowScale.push_back({l, -1});
+            colScale.push_back({l - 1, 1});
+        }
     }
     uploadVec(I.coaxPin, pin, stream);
     uploadVec(I.coaxPout, pout, stream);
@@ -1256,6 +1366,44 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
         uint32_t(pin.size()), I.coaxPin.as<int>(), I.coaxPout.as<int>(), I.coaxStart.as<uint64_t>(),
         I.fl.as<double2>(), lmaxF, I.gaunt.as<double>(), I.gauntOff.as<uint32_t>(), P, I.coax.as<double2>());
     fmmCheck(cudaGetLastError(), "coaxial table launch");
+    if (I.fp32) {
+        // log sigma_n per level, sigma_n = (2n+1)!! / (k a_l)^n with a_l the level's node radius
+        const int stride = P + 1;
+        std::vector<double> logSigma(size_t(levels) * stride, 0.0), sigma(size_t(levels) * stride, 1.0);
+        for (const auto &info : levelInfo_) {
+            const double lka = std::log(std::max(k * info.radius, 1e-300));
+            double lf = 0;  // log (2n+1)!!
+            for (int n = 0; n <= P; ++n) {
+                if (n)
+                    lf += std::log(2.0 * n + 1);
+                const double v = std::clamp(lf - n * lka, -600.0, 600.0);
+                logSigma[size_t(info.level) * stride + n] = v;
+                sigma[size_t(info.level) * stride + n] = std::exp(v);
+            }
+        }
+        I.sigmaStride = stride;
+        uploadVec(I.sigma, sigma, stream);
+        std::vector<double> lr(pin.size() * stride), lc(pin.size() * stride);
+        for (size_t c = 0; c < pin.size(); ++c)
+            for (int n = 0; n <= P; ++n) {
+                lr[c * stride + n] = rowScale[c].second * logSigma[size_t(rowScale[c].first) * stride + n];
+                lc[c * stride + n] = colScale[c].second * logSigma[size_t(colScale[c].first) * stride + n];
+            }
+        uploadVec(I.logRow, lr, stream);
+        uploadVec(I.logCol, lc, stream);
+        I.coax32.ensure(std::max<uint64_t>(total, 1) * 8);
+        coaxScaleKernel<<<dim3(64, uint32_t(pin.size())), 256, 0, stream>>>(
+            uint32_t(pin.size()), I.coaxPin.as<int>(), I.coaxPout.as<int>(), I.coaxStart.as<uint64_t>(),
+            I.coax.as<double2>(), I.logRow.as<double>(), I.logCol.as<double>(), stride, I.coax32.as<float2>());
+        fmmCheck(cudaGetLastError(), "scaled coaxial table launch");
+        if (!I.wigner32Valid) {
+            std::vector<float> w32(I.hostWigner.begin(), I.hostWigner.end());
+            uploadVec(I.wigner32, w32, stream);
+            I.wigner32Valid = true;
+        }
+        I.Mc32.ensure(std::max<size_t>(at, 1) * 8);
+        I.Lc32.ensure(std::max<size_t>(at, 1) * 8);
+    }
     // local coax class ids -> global ids in the link lists
     for (int l = I.lmin; l < levels; ++l) {
         const auto remap = [&](const Impl::Plan &pl, Impl::DevPlan &d, const std::vector<uint32_t> &cls) {
@@ -1331,47 +1479,62 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
     const int nch = rhs ? 1 : 6;
     const int levels = int(tree_.levels.size());
     fmmCheck(cudaMemsetAsync(I.far.p, 0, 3 * size_t(I.T) * 16, stream), "zero contributions");
-    fmmCheck(cudaMemsetAsync(I.Lc.p, 0, I.coefTotal * 16, stream), "zero locals");
+    if (I.fp32)
+        fmmCheck(cudaMemsetAsync(I.Lc32.p, 0, I.coefTotal * 8, stream), "zero locals");
+    else
+        fmmCheck(cudaMemsetAsync(I.Lc.p, 0, I.coefTotal * 16, stream), "zero locals");
     // channels per CTA: enough CTAs for about four waves of 148 SMs, fewer
     // (more reuse of each Wigner and coaxial entry) when the level has many nodes
-    const auto translate = [&](Impl::DevPlan &d, int pin, int pout, const double2 *in, double2 *out, bool zero) {
+    const auto translate = [&](Impl::DevPlan &d, int pin, int pout, auto *in, auto *out, bool zero) {
+        using CT = std::remove_cv_t<std::remove_pointer_t<decltype(out)>>;
+        using RT = decltype(CT{}.x);
+        constexpr bool f32 = std::is_same_v<RT, float>;
         if (!d.count)
             return;
         const int nmax = std::max((pin + 1) * (pin + 1), (pout + 1) * (pout + 1)), nout = (pout + 1) * (pout + 1);
         // all channels in one CTA where shared memory allows two CTAs per SM (each
         // Wigner and coaxial entry then serves every channel), links split over K
         // CTAs per output node for about eight CTAs per SM
-        const auto bytes = [&](int c) { return (size_t(3) * c * nmax + std::max(pin, pout) + 1) * 16; };
+        const auto bytes = [&](int c) { return (size_t(3) * c * nmax + std::max(pin, pout) + 1) * sizeof(CT); };
         int cpc = nch == 1 ? 1 : 6;
         while (cpc > 1 && bytes(cpc) > 110 * 1024)
             cpc = cpc == 6 ? 3 : cpc == 3 ? 2 : 1;
         const size_t sm = bytes(cpc);
         const unsigned groups = unsigned((nch + cpc - 1) / cpc);
         const int K = int(std::clamp<size_t>((size_t(148) * 8 + d.count * groups - 1) / (d.count * groups), 1, 8));
+        DevBuf &partial = f32 ? I.partial32 : I.partial;
         if (K > 1)
-            I.partial.ensure(size_t(d.count) * K * 6 * nout * 16);
+            partial.ensure(size_t(d.count) * K * 6 * nout * sizeof(CT));
+        const RT *wig;
+        const CT *cx;
+        if constexpr (f32) {
+            wig = I.wigner32.as<float>();
+            cx = I.coax32.as<float2>();
+        } else {
+            wig = I.wigner.as<double>();
+            cx = I.coax.as<double2>();
+        }
         const dim3 grid(d.count * K, groups);
         const auto launch = [&](auto kernel) {
             fmmCheck(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                      "translate smem");
             kernel<<<grid, 256, sm, stream>>>(d.out.as<uint32_t>(), d.start.as<uint32_t>(), d.links.as<TransLink>(),
-                                              pin, pout, in, out, I.coefOffset.as<uint64_t>(), I.wigner.as<double>(),
-                                              I.wignerStart.as<uint64_t>(), I.coax.as<double2>(),
-                                              I.coaxStart.as<uint64_t>(), zero ? 1 : 0, nch, K,
-                                              I.partial.as<double2>());
+                                              pin, pout, in, out, I.coefOffset.as<uint64_t>(), wig,
+                                              I.wignerStart.as<uint64_t>(), cx, I.coaxStart.as<uint64_t>(),
+                                              zero ? 1 : 0, nch, K, partial.as<CT>());
         };
         if (cpc == 6)
-            launch(translateKernel<6>);
+            launch(translateKernel<6, RT>);
         else if (cpc == 3)
-            launch(translateKernel<3>);
+            launch(translateKernel<3, RT>);
         else if (cpc == 2)
-            launch(translateKernel<2>);
+            launch(translateKernel<2, RT>);
         else
-            launch(translateKernel<1>);
+            launch(translateKernel<1, RT>);
         fmmCheck(cudaGetLastError(), "translate launch");
         if (K > 1) {
-            reduceKernel<<<d.count, 256, 0, stream>>>(d.out.as<uint32_t>(), I.coefOffset.as<uint64_t>(),
-                                                      I.partial.as<double2>(), K, nout, nch, zero ? 1 : 0, out);
+            reduceKernel<RT><<<d.count, 256, 0, stream>>>(d.out.as<uint32_t>(), I.coefOffset.as<uint64_t>(),
+                                                          partial.as<CT>(), K, nout, nch, zero ? 1 : 0, out);
             fmmCheck(cudaGetLastError(), "translate reduce launch");
         }
     };
@@ -1391,24 +1554,34 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
             p2mKernel<<<leaves, 256, sm, stream>>>(I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(),
                                                    I.dLeafStart[l].as<uint32_t>(), I.dItems.as<FmmItem>() + I.itemBase[l],
                                                    I.centers.as<double>(), I.coefOffset.as<uint64_t>(), P, k_, pv,
-                                                   I.Mc.as<double2>(), rhs ? 1 : 0);
+                                                   I.Mc.as<double2>(), rhs ? 1 : 0,
+                                                   I.fp32 ? I.Mc32.as<float2>() : nullptr, I.levelSigma(l));
             fmmCheck(cudaGetLastError(), "p2m launch");
         }
     }
     {
         TimedScope scope(timer, "fmm_m2m", stream);
         for (int l = levels - 2; l >= I.lmin; --l)
-            translate(I.dm2m[l], I.order[l + 1], I.order[l], I.Mc.as<double2>(), I.Mc.as<double2>(), true);
+            if (I.fp32)
+                translate(I.dm2m[l], I.order[l + 1], I.order[l], I.Mc32.as<float2>(), I.Mc32.as<float2>(), true);
+            else
+                translate(I.dm2m[l], I.order[l + 1], I.order[l], I.Mc.as<double2>(), I.Mc.as<double2>(), true);
     }
     {
         TimedScope scope(timer, "fmm_m2l", stream);
         for (int l = I.lmin; l < levels; ++l)
-            translate(I.dm2l[l], I.order[l], I.order[l], I.Mc.as<double2>(), I.Lc.as<double2>(), false);
+            if (I.fp32)
+                translate(I.dm2l[l], I.order[l], I.order[l], I.Mc32.as<float2>(), I.Lc32.as<float2>(), false);
+            else
+                translate(I.dm2l[l], I.order[l], I.order[l], I.Mc.as<double2>(), I.Lc.as<double2>(), false);
     }
     {
         TimedScope scope(timer, "fmm_l2l", stream);
         for (int l = I.lmin + 1; l < levels; ++l)
-            translate(I.dl2l[l], I.order[l - 1], I.order[l], I.Lc.as<double2>(), I.Lc.as<double2>(), false);
+            if (I.fp32)
+                translate(I.dl2l[l], I.order[l - 1], I.order[l], I.Lc32.as<float2>(), I.Lc32.as<float2>(), false);
+            else
+                translate(I.dl2l[l], I.order[l - 1], I.order[l], I.Lc.as<double2>(), I.Lc.as<double2>(), false);
     }
     {
         TimedScope scope(timer, "fmm_l2p", stream);
@@ -1428,7 +1601,8 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
                 l2pRhsKernel<<<leaves, 256, sm, stream>>>(
                     I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(), I.dLeafStart[l].as<uint32_t>(),
                     I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(), I.coefOffset.as<uint64_t>(), p, k_,
-                    I.Lc.as<double2>(), I.far.as<double2>());
+                    I.Lc.as<double2>(), I.far.as<double2>(), I.fp32 ? I.Lc32.as<float2>() : nullptr,
+                    I.levelSigma(l));
             } else {
                 fmmCheck(cudaFuncSetAttribute(l2pKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                          "l2p smem");
@@ -1436,7 +1610,8 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
                                                        I.dLeafStart[l].as<uint32_t>(),
                                                        I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(),
                                                        I.coefOffset.as<uint64_t>(), p, k_, I.Lc.as<double2>(),
-                                                       I.far.as<double2>());
+                                                       I.far.as<double2>(), I.fp32 ? I.Lc32.as<float2>() : nullptr,
+                                                       I.levelSigma(l));
             }
             fmmCheck(cudaGetLastError(), "l2p launch");
         }

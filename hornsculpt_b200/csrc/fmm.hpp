@@ -61,6 +61,9 @@ class FmmOperator {
     double wavenumber() const { return k_; }
     // Replay of the far-field apply as a captured CUDA graph (on by default).
     void setGraphs(bool enabled);
+    // Mixed form: translations in FP32 on scaled expansions (P2M and L2P stay
+    // FP64); takes effect at the next prepare().
+    void setFp32(bool enabled);
 
   private:
     struct Impl;
@@ -106,9 +109,16 @@ class FmmSystem {
     void precondition(const double *in, double *out, uint32_t S, cudaStream_t stream);
     // x_s = A^{-1} b_s to mass-weighted relative residual `target` (x starts at 0).
     // relative[s]: final relative residual of the operator; iterations[s]: Arnoldi steps.
+    // With `inner` (an operator on the same tree in FP32 mode, prepared for the
+    // same wavenumber) the solve is GMRES-IR: Krylov cycles on the FP32 operator
+    // and FP32 near values (roundNearValues first), residuals of the FP64 one.
     void solve(const double *b, double *x, uint32_t S, double target, uint32_t restart, uint32_t maxIterations,
                cudaStream_t stream, KernelTimer *timer, std::vector<double> &relative,
-               std::vector<uint32_t> &iterations);
+               std::vector<uint32_t> &iterations, FmmOperator *inner = nullptr);
+    // FP32 copy of the near values for the inner operator of the mixed form.
+    void roundNearValues(cudaStream_t stream);
+    void applyInner(FmmOperator &inner, const double *x, size_t stride, uint32_t S, double *y, cudaStream_t stream,
+                    KernelTimer *timer);
 
   private:
     struct Impl;

@@ -75,6 +75,40 @@ __global__ void spmvKernel(const uint32_t *__restrict__ rowStart, const uint32_t
     }
 }
 
+// The mixed form's near product in FP32: FP32 values and products of the
+// rounded input, FP32 accumulation; the FP64 far part added with the row scale.
+__global__ void spmv32Kernel(const uint32_t *__restrict__ rowStart, const uint32_t *__restrict__ cols,
+                             const float2 *__restrict__ vals, const double2 *__restrict__ x,
+                             const double2 *__restrict__ far, const double *__restrict__ rowScale, uint32_t N,
+                             double2 *y) {
+    const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= N)
+        return;
+    float re = 0, im = 0;
+    for (uint32_t e = rowStart[row] + lane; e < rowStart[row + 1]; e += 32) {
+        const float2 a = vals[e];
+        const double2 xd = x[cols[e]];
+        const float vx = float(xd.x), vy = float(xd.y);
+        re += a.x * vx - a.y * vy;
+        im += a.x * vy + a.y * vx;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_xor_sync(0xffffffffu, re, o);
+        im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) {
+        const double2 f = far[row];
+        const double s = rowScale[row];
+        y[row] = make_double2(double(re) + s * f.x, double(im) + s * f.y);
+    }
+}
+
+__global__ void roundValuesKernel(const double2 *in, float2 *out, size_t count) {
+    const size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i < count)
+        out[i] = make_float2(float(in[i].x), float(in[i].y));
+}
+
 // Inverse of each diagonal block by Gauss-Jordan with partial pivoting in
 // shared memory ([M | I], nb <= 64). A zero pivot leaves the identity for the
 // block and raises the flag.
@@ -236,7 +270,7 @@ struct FmmSystem::Impl {
     uint32_t N = 0, blocks = 0;
     const double *rowScale = nullptr, *mass = nullptr;
     Buf rowStart, cols, vals, blockStart, blockVerts, invStart, inv, flag;
-    Buf far, tmp, r, d, norms, gmres;
+    Buf far, tmp, r, d, norms, gmres, vals32;
     size_t gmresBytes = 0;
     uint32_t gmresS = 0, gmresM = 0;
 };
@@ -362,6 +396,29 @@ void FmmSystem::apply(const double *x, size_t stride, uint32_t S, double *y, cud
     sysCheck(cudaGetLastError(), "near product launch");
 }
 
+void FmmSystem::roundNearValues(cudaStream_t stream) {
+    Impl &I = *impl_;
+    const size_t nnz = std::max<size_t>(op_.nearCols().size(), 1);
+    I.vals32.ensure(nnz * 8);
+    roundValuesKernel<<<unsigned((nnz + 255) / 256), 256, 0, stream>>>(I.vals.as<double2>(), I.vals32.as<float2>(),
+                                                                      op_.nearCols().size());
+    sysCheck(cudaGetLastError(), "near value rounding launch");
+}
+
+void FmmSystem::applyInner(FmmOperator &inner, const double *x, size_t stride, uint32_t S, double *y,
+                           cudaStream_t stream, KernelTimer *timer) {
+    Impl &I = *impl_;
+    I.far.ensure(size_t(S) * I.N * 16);
+    inner.applyFar(x, stride, S, I.far.as<double>(), stream, timer);
+    TimedScope scope(timer, "fmm_near_fp32", stream);
+    for (uint32_t s = 0; s < S; ++s)
+        spmv32Kernel<<<(I.N * 32 + 255) / 256, 256, 0, stream>>>(
+            I.rowStart.as<uint32_t>(), I.cols.as<uint32_t>(), I.vals32.as<float2>(),
+            reinterpret_cast<const double2 *>(x + s * stride), I.far.as<double2>() + size_t(s) * I.N, I.rowScale, I.N,
+            reinterpret_cast<double2 *>(y) + size_t(s) * I.N);
+    sysCheck(cudaGetLastError(), "FP32 near product launch");
+}
+
 void FmmSystem::precondition(const double *in, double *out, uint32_t S, cudaStream_t stream) {
     Impl &I = *impl_;
     blockApplyKernel<<<dim3(I.blocks, S), 64, 0, stream>>>(I.blockStart.as<uint32_t>(), I.blockVerts.as<uint32_t>(),
@@ -373,7 +430,7 @@ void FmmSystem::precondition(const double *in, double *out, uint32_t S, cudaStre
 
 void FmmSystem::solve(const double *b, double *x, uint32_t S, double target, uint32_t restart, uint32_t maxIterations,
                       cudaStream_t stream, KernelTimer *timer, std::vector<double> &relative,
-                      std::vector<uint32_t> &iterations) {
+                      std::vector<uint32_t> &iterations, FmmOperator *inner) {
     Impl &I = *impl_;
     const uint32_t N = I.N;
     const size_t reals = size_t(S) * N * 2;
@@ -391,7 +448,17 @@ void FmmSystem::solve(const double *b, double *x, uint32_t S, double target, uin
     std::vector<double> norms(2 * S);
     int singular = 0;
     sysCheck(cudaMemcpyAsync(&singular, I.flag.p, sizeof(int), cudaMemcpyDeviceToHost, stream), "flag");
-    const auto applyA = [&](const double *in, size_t stride, double *out) { apply(in, stride, S, out, stream, timer); };
+    // GMRES-IR with an inner operator (the mixed form): the Krylov cycles apply the
+    // FP32 operator (scaled FP32 translations, FP32 near values) and each cycle
+    // only needs to win a few digits (the FP32 operator holds about six); the
+    // residual every cycle starts from is the FP64 operator's.
+    const auto applyA = [&](const double *in, size_t stride, double *out) {
+        if (inner)
+            applyInner(*inner, in, stride, S, out, stream, timer);
+        else
+            apply(in, stride, S, out, stream, timer);
+    };
+    const double innerFloor = inner ? 1e-4 : 1e-13;
     const auto pre = [&](const double *in, double *out) { precondition(in, out, S, stream); };
     for (uint32_t total = 0;;) {
         // true residual of the operator
@@ -412,7 +479,7 @@ void FmmSystem::solve(const double *b, double *x, uint32_t S, double target, uin
             if (!std::isfinite(rel))
                 throw NumericError("Fast-multipole residual is not finite.");
             relative[s] = rel;
-            tol[s] = rel > target ? std::clamp(0.1 * target / rel, 1e-13, 0.5) : 1.0;
+            tol[s] = rel > target ? std::clamp(0.1 * target / rel, innerFloor, 0.5) : 1.0;
             done = done && rel <= target;
         }
         if (done)

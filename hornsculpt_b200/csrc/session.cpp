@@ -110,9 +110,6 @@ void validateRequest(const hs_request &r) {
         !std::isfinite(o.relative_residual_tolerance) || o.relative_residual_tolerance < 1e-7 ||
         o.relative_residual_tolerance > .01 || o.maximum_refinement_steps > 10)
         throw InvalidArgument("Invalid BEM medium, frequencies, excitation or Galerkin settings.");
-    if (fmm && o.precision == HS_PRECISION_MIXED)
-        throw Unsupported("The mixed-precision fast-multipole form is not part of this build; use the FP64 fast "
-                          "multipole or the dense mixed form.");
     if (o.precision != HS_PRECISION_FP64 && o.precision != HS_PRECISION_MIXED)
         throw InvalidArgument("Invalid BEM precision form.");
     if (r.excitation_count > 1024 || r.observer_count > 100000)
@@ -158,8 +155,18 @@ Session::Session(const MeshInput &mesh, uint32_t residency) : mesh_(mesh), resid
     uploadGeometry();
 }
 
+void Session::releaseMappedPatches() {
+    if (mappedPatchesHost_) {
+        cudaStreamSynchronize(stream());  // no kernel may still read the mapped range
+        cudaFreeHost(mappedPatchesHost_);
+        mappedPatchesHost_ = nullptr;
+        patches_ = nullptr;
+    }
+}
+
 Session::~Session() {
     dropGraphs();
+    releaseMappedPatches();
     if (own_) {
         cudaStreamSynchronize(own_);
         cudaStreamDestroy(own_);
@@ -295,7 +302,34 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
     upload(dPairCode_, code, s);
     upload(dTouching_, touching, s);
     upload(dNearPairs_, nearPairs, s);
-    upload(dPatches_, plan_.patches, s);
+    // Near-pair quadrature patches: device memory, or mapped pinned host memory
+    // that the kernels read over the bus (CudaCacheResidency, cuda_solver.cu:112-160,
+    // 899-903): always for HS_RESIDENCY_MAPPED_HOST; for AUTOMATIC when the
+    // patches would take more than a quarter of the free device memory.
+    {
+        const size_t patchBytes = plan_.patches.size() * sizeof(Patch);
+        size_t freeBytes = 0, totalBytes = 0;
+        cuda(cudaMemGetInfo(&freeBytes, &totalBytes), "CUDA memory query");
+        const bool mapped = patchBytes && (residency_ == HS_RESIDENCY_MAPPED_HOST ||
+                                           (residency_ == HS_RESIDENCY_AUTOMATIC && patchBytes > freeBytes / 4));
+        releaseMappedPatches();
+        if (mapped) {
+            int device = 0, canMap = 0;
+            cuda(cudaGetDevice(&device), "CUDA device query");
+            cuda(cudaDeviceGetAttribute(&canMap, cudaDevAttrCanMapHostMemory, device), "CUDA host mapping query");
+            if (!canMap)
+                throw CudaError("CUDA device does not support mapped quadrature storage.");
+            cuda(cudaHostAlloc(&mappedPatchesHost_, patchBytes, cudaHostAllocMapped), "CUDA mapped patch allocation");
+            std::memcpy(mappedPatchesHost_, plan_.patches.data(), patchBytes);
+            void *alias = nullptr;
+            cuda(cudaHostGetDevicePointer(&alias, mappedPatchesHost_, 0), "CUDA mapped patch pointer");
+            patches_ = static_cast<const Patch *>(alias);
+            dPatches_.release();
+        } else {
+            upload(dPatches_, plan_.patches, s);
+            patches_ = dPatches_.as<Patch>();
+        }
+    }
     upload(dGauss_, g, s);
     upload(dSingularTable_, buildSingularTable(o.singular_order), s);
     cuda(cudaStreamSynchronize(s), "CUDA synchronization");
@@ -583,7 +617,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     result->E = E;
     result->frequencies.resize(F);
     AssemblyGeometry geo{dPanels_.as<DPanel>(), dBounds_.as<Bounds>(), dPairCode_.as<uint8_t>(),
-                         dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), dPatches_.as<Patch>(),
+                         dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), patches_,
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
                          dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
                          o.near_relative_tolerance,
@@ -640,7 +674,10 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         double assemblyMs = 0, factorMs = 0, triMs = 0, residualMs = 0;
         std::vector<uint32_t> steps(B, 0), krylov(size_t(B) * E, 0), cycle;
         std::vector<double> relative(size_t(B) * E, 0);
-        const double target = mixed ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
+        // the dense mixed form refines to 1e-10; the fast-multipole forms (FP64, or
+        // GMRES-IR over the FP32 operator) solve to the request's tolerance
+        const double target =
+            mixed && !fmmForm ? std::min(o.relative_residual_tolerance, 1e-10) : o.relative_residual_tolerance;
         if (fmmForm) {
             // Fast-multipole form: per frequency the exact near support pairs
             // (records of the near panel pairs only), the right-hand side as
@@ -657,14 +694,21 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             const auto solveStart = Clock::now();
             std::vector<double> rel;
             std::vector<uint32_t> its;
+            // mixed: the inner operator of GMRES-IR, FP32 translations at expansions
+            // for 1e-5 (its cycles win at most four digits each)
+            FmmOperator *inner = mixed ? &fmmInnerOperator(o) : nullptr;
             for (uint32_t b = 0; b < B; ++b) {
                 checkCancel();
                 op.prepare(ks[b], expansionTolerance, s);
+                if (inner)
+                    inner->prepare(ks[b], std::max(expansionTolerance, 1e-5), s);
                 // near support pairs and the near right-hand side from the near panel-pair records
                 double *rhsB = dRhs_.as<double>() + size_t(b) * E * N * 2;
                 const double *fluxB = dFlux_.as<double>() + size_t(b) * E * T * 2;
                 assembleNearField(geo, dKs_.as<double>() + b, dGauss_.as<double>(), fluxB, E, layout,
                                   dNearWork_.as<void>(), fmmSystem_->nearValues(), rhsB, dError_.as<int>(), s, &timer_);
+                if (inner)
+                    fmmSystem_->roundNearValues(s);
                 cuda(cudaEventRecord(ev.assembled, s), "phase event");
                 {
                     TimedScope scope(&timer_, "fmm_rhs_far", s);
@@ -676,7 +720,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 double *xB = dX_.as<double>() + size_t(b) * E * N * 2;
                 // working solve to half the target, leaving the audit its margin
                 fmmSystem_->solve(rhsB, xB, E, .5 * target, o.fmm_restart_length, o.fmm_maximum_iterations, s, &timer_,
-                                  rel, its);
+                                  rel, its, inner);
                 for (uint32_t e = 0; e < E; ++e)
                     krylov[size_t(b) * E + e] = its[e];
                 // Audit against a ten times finer expansion operator and defect-correct
@@ -720,7 +764,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                     tau = std::max(.1 * tau, 1e-12);
                     op.prepare(ks[b], tau, s);
                     fmmSystem_->solve(dAuditFine_.as<double>(), dCorr_.as<double>(), E, .5 * target,
-                                      o.fmm_restart_length, o.fmm_maximum_iterations, s, &timer_, rel, its);
+                                      o.fmm_restart_length, o.fmm_maximum_iterations, s, &timer_, rel, its, inner);
                     fmmSystem_->add(xB, dCorr_.as<double>(), reals, s);
                     for (uint32_t e = 0; e < E; ++e)
                         krylov[size_t(b) * E + e] += its[e];
@@ -1043,6 +1087,7 @@ void Session::runDenseChain(const AssemblyGeometry &geo, const AssemblyWorkspace
           &dPanelRhs_, &dBins_, &dBinCounts_, &dBinOffsets_, &dA_, &dLU_, &dRhs_, &dX_, &dPivots_, &dInfo_, &dKs_,
           &dFlux_, &dWork32_, &dLuPack_, &dSolveScratch_})
         signature = (signature ^ reinterpret_cast<uintptr_t>(b->as<void>())) * 0x100000001b3ull;
+    signature = (signature ^ reinterpret_cast<uintptr_t>(patches_)) * 0x100000001b3ull;
     DenseGraph *hit = nullptr;
     for (auto &g : denseGraphs_)
         if (g.B == B && g.E == E && g.mixed == mixed && g.signature == signature)
@@ -1097,6 +1142,8 @@ void Session::setGraphs(bool enabled) {
     dropGraphs();
     if (fmm_)
         fmm_->setGraphs(enabled);
+    if (fmmInner_)
+        fmmInner_->setGraphs(enabled);
 }
 
 void Session::debugAssemble(const hs_numerics &o, double planK, double k, const double *flux, double *matrix,
@@ -1108,7 +1155,7 @@ void Session::debugAssemble(const hs_numerics &o, double planK, double k, const 
     cuda(cudaMemcpyAsync(dKs_.as<void>(), &k, 8, cudaMemcpyHostToDevice, s), "k upload");
     cuda(cudaMemcpyAsync(dFlux_.as<void>(), flux, size_t(T) * 16, cudaMemcpyHostToDevice, s), "flux upload");
     AssemblyGeometry geo{dPanels_.as<DPanel>(), dBounds_.as<Bounds>(), dPairCode_.as<uint8_t>(),
-                         dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), dPatches_.as<Patch>(),
+                         dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), patches_,
                          dIncOffsets_.as<uint32_t>(), dIncPanel_.as<uint32_t>(), dIncLocal_.as<uint8_t>(),
                          dRowScale_.as<double>(), T, N, touchingCount_, nearPairCount_, projectedPairCount_,
                          o.near_relative_tolerance,
@@ -1191,6 +1238,22 @@ FmmOperator &Session::fmmOperator(const hs_numerics &o, double tuneK, double tun
     return *fmm_;
 }
 
+// The mixed form's inner operator: the same tree and partition as the FP64
+// operator (built from the same settings), translations in FP32 on scaled
+// expansions.
+FmmOperator &Session::fmmInnerOperator(const hs_numerics &o) {
+    if (!fmmInner_ || fmmInnerSettings_.leafCapacity != fmmSettings_.leafCapacity ||
+        fmmInnerSettings_.separationRatio != fmmSettings_.separationRatio) {
+        fmmInner_.reset();
+        fmmInner_ = std::make_unique<FmmOperator>(space_, fmmSettings_);
+        fmmInner_->setFp32(true);
+        fmmInner_->setGraphs(graphs_);
+        fmmInnerSettings_ = fmmSettings_;
+    }
+    (void)o;
+    return *fmmInner_;
+}
+
 // Leaf support capacity of the fast-multipole tree picked by the autotuner
 // (requests with capacity 0): per mesh size class and electrical size class,
 // each candidate tree is built and its operator apply (far expansions plus the
@@ -1265,7 +1328,8 @@ uint32_t Session::tunedLeafCapacity(double separation, double k, double toleranc
 void Session::debugFmmFar(const hs_numerics &o, double k, double tolerance, const double *pressure, double *far,
                           std::vector<uint32_t> &nearRow, std::vector<uint32_t> &nearCol,
                           std::vector<FmmLevelInfo> &levels) {
-    FmmOperator &op = fmmOperator(o);
+    // HS_PRECISION_MIXED: the mixed form's FP32 operator on the same tree
+    FmmOperator &op = o.precision == HS_PRECISION_MIXED ? (fmmOperator(o), fmmInnerOperator(o)) : fmmOperator(o);
     const cudaStream_t s = stream();
     const size_t N = space_.vertices.size();
     op.prepare(k, tolerance, s);

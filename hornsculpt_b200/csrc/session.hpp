@@ -133,6 +133,14 @@ class Session {
     Plan plan_;
     double planMs_ = 0;
     DeviceBuffer dPairCode_, dTouching_, dNearPairs_, dPatches_, dGauss_, dSingularTable_;
+    // patches as the kernels see them: dPatches_, or the device alias of mapped
+    // pinned host memory (residency)
+    const Patch *patches_ = nullptr;
+    void *mappedPatchesHost_ = nullptr;
+    void releaseMappedPatches();
+public:
+    bool patchesMapped() const { return mappedPatchesHost_ != nullptr; }
+private:
     uint32_t touchingCount_ = 0, nearPairCount_ = 0, projectedPairCount_ = 0;
     uint64_t singularSamples_ = 0, nearSamples_ = 0;
     // workspaces (grow only)
@@ -147,7 +155,9 @@ class Session {
     FmmOperator &fmmOperator(const hs_numerics &numerics, double tuneK = 0, double tuneTolerance = 1e-8);
     uint32_t tunedLeafCapacity(double separation, double k, double tolerance);
     static double fmmTuneTolerance(const hs_numerics &numerics);
-    std::unique_ptr<FmmOperator> fmm_;
+    std::unique_ptr<FmmOperator> fmm_, fmmInner_;
+    FmmTreeSettings fmmInnerSettings_{};
+    FmmOperator &fmmInnerOperator(const hs_numerics &numerics);
     std::unique_ptr<FmmSystem> fmmSystem_;
     const FmmOperator *fmmSystemOp_ = nullptr;
     uint32_t fmmBlockWidth_ = 0;

@@ -160,3 +160,56 @@ def test_fast_multipole_on_the_c2_horn_matches_dense():
         assert ed.boundary_residual <= 1e-12
         assert ef.boundary_residual <= 1e-6
         assert trace < 1e-5 and field < 1e-5
+
+
+@pytest.mark.parametrize("case, freq", [("icosphere3", 20.0), ("icosphere3", 500.0), ("icosphere3", 3000.0),
+                                        ("horn", 2000.0)])
+def test_scaled_fp32_far_operator_matches_fp64(case, freq):
+    """The mixed form's far operator (scaled expansions, FP32 translations) against
+    the FP64 one on the same tree. At 20 Hz the unscaled locals of this sphere span
+    far beyond FP32 range (h_n(k t) grows like (2n-1)!!/(k t)^(n+1)); scaled they
+    stay O(1), so the FP32 operator keeps FP32 accuracy there too."""
+    mesh = {"icosphere3": lambda: meshes.icosphere(3),
+            "horn": lambda: meshes.exponential_horn(h=0.0128, seed=5)}[case]()
+    N = mesh.vertex_count
+    k = 2 * np.pi * freq / 343.0
+    rng = np.random.default_rng(5)
+    p = rng.normal(size=N) + 1j * rng.normal(size=N)
+    with hs.CudaBemSolver(mesh) as solver:
+        f64, _, _, levels = solver.debug_fmm_far(FP64, k, 1e-8, p)
+        f32, _, _, _ = solver.debug_fmm_far(hs.BemNumerics(precision="mixed"), k, 1e-8, p)
+    assert len(levels) > 0 and np.all(np.isfinite(f32))
+    rel = np.linalg.norm(f32 - f64) / np.linalg.norm(f64)
+    print(case, freq, "orders", levels[:, 1].tolist(), "FP32 vs FP64 far", rel)
+    assert rel < 2e-5
+
+
+@pytest.mark.parametrize("case, freqs", [("icosphere3", [150.0, 2500.0]), ("horn", [300.0, 2000.0])])
+def test_mixed_fast_multipole_matches_dense(case, freqs):
+    """The precision form of the fast multipole: GMRES-IR whose Krylov cycles run
+    on the FP32 operator (scaled FP32 translations, FP32 near values) and whose
+    residuals come from the FP64 operator. Against the dense FP64 LU solve of the
+    same discretisation: surface pressure within 1e-5 at a 1e-6 residual target."""
+    mesh, face = {"icosphere3": (meshes.icosphere(3), 1),
+                  "horn": (meshes.exponential_horn(h=0.0128, seed=5), meshes.HORN_THROAT)}[case]
+    obs = [(0.0, 0.0, 0.4), (0.5, 0.1, 0.0)]
+
+    def request(acc, precision, tol):
+        return hs.BemRequest(frequencies=freqs, observers=obs,
+                             excitations=[hs.BemExcitation("drive", [hs.FaceVelocity(face, 1.0)])],
+                             numerics=hs.BemNumerics(precision=precision, acceleration=acc,
+                                                     relative_residual_tolerance=tol))
+    with hs.CudaBemSolver(mesh) as solver:
+        dense = solver.solve(request("dense", "fp64", 1e-7))
+        mixed = solver.solve(request("fast_multipole", "mixed", 1e-6))
+    areas = None
+    for fd, fm in zip(dense.frequencies, mixed.frequencies):
+        ed, em = fd.excitations[0], fm.excitations[0]
+        if areas is None:
+            v = mesh.vertices[mesh.triangles]
+            areas = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+        d = em.boundary.surface_pressure - ed.boundary.surface_pressure
+        err = np.sqrt(np.sum(areas * np.abs(d) ** 2) / np.sum(areas * np.abs(ed.boundary.surface_pressure) ** 2))
+        print(case, fm.frequency, "surface error", err, "iterations", em.iterations, "residual", em.boundary_residual)
+        assert em.boundary_residual <= 1e-6
+        assert err < 1e-5

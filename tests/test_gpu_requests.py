@@ -47,11 +47,6 @@ def test_invalid_requests(solver, kw, match):
         solver.solve(req(**kw))
 
 
-def test_mixed_fast_multipole_is_reported_unsupported(solver):
-    with pytest.raises(hs.BemUnsupported):
-        solver.solve(req(numerics=hs.BemNumerics(acceleration="fast_multipole", precision="mixed")))
-
-
 def test_electrically_coarse_mesh_rejected():
     """k*h > 3.25 (regular_qualification.hpp:360-368) stops the observer field
     (tetrahedron: every pair touches, so planning is trivial)."""
@@ -112,3 +107,24 @@ def test_lem_coupled_solve_equals_direct_solve_of_coupled_velocities():
     assert np.linalg.norm(coupled.pressure_trace - d.boundary.pressure_trace) <= 1e-6 * np.linalg.norm(
         d.boundary.pressure_trace)
     assert abs(coupled.observer_pressure[0] - d.observer_pressure[0]) <= 1e-6 * abs(d.observer_pressure[0])
+
+
+def test_mapped_host_patch_residency_equals_device():
+    """CudaStorageOptions.quadrature_patches = mapped_host (cuda_solver.cu:112-160):
+    the near-pair quadrature patches stay in mapped pinned host memory that the
+    kernels read over the bus. The result equals the device-resident one bit for
+    bit, and the session holds the patches' bytes less device memory."""
+    mesh = meshes.octahedral_sphere(3)
+    request = req(frequencies=[400.0, 1700.0], observers=[(0, 0, 0.3)],
+                  numerics=hs.BemNumerics(near_relative_tolerance=1e-6))
+    plan = hs.host_plan(mesh, request.numerics, 2 * np.pi * 1700.0 / 343.0)
+    assert len(plan["patches"]) > 0
+    results = {}
+    for where in ("device", "mapped_host"):
+        with hs.CudaBemSolver(mesh, hs.CudaStorageOptions(quadrature_patches=where)) as solver:
+            results[where] = solver.solve(request)
+    for fd, fm in zip(results["device"].frequencies, results["mapped_host"].frequencies):
+        assert np.array_equal(fd.excitations[0].boundary.pressure_trace, fm.excitations[0].boundary.pressure_trace)
+        assert np.array_equal(fd.excitations[0].observer_pressure, fm.excitations[0].observer_pressure)
+    saved = results["device"].peak_device_bytes - results["mapped_host"].peak_device_bytes
+    assert saved >= len(plan["patches"]) * 22 * 8 * 0.99
