@@ -251,6 +251,10 @@ class CudaBemSolver:
     WORK_KEYS = ("pairs_q6", "pairs_q12", "pairs_q16", "pairs_q64", "regular_samples", "singular_samples",
                  "near_samples", "frequencies")
 
+    def set_plane_wave_threshold(self, threshold: float) -> None:
+        """k x shortest M2L distance from which a fast-multipole level translates in the plane-wave form."""
+        _lib.check(self._lib.hs_bem_session_set_plane_wave_threshold(self._handle, threshold))
+
     def set_graphs(self, enabled: bool) -> None:
         """Replay of the dense batch chain and the fast-multipole far-field apply as captured CUDA graphs."""
         _lib.check(self._lib.hs_bem_session_set_graphs(self._handle, int(enabled)))
@@ -397,7 +401,7 @@ class CudaBemSolver:
     def debug_fmm_far(self, numerics: BemNumerics, k: float, tolerance: float, pressure: np.ndarray):
         """Far part of the fast-multipole operator applied to a P1 vector (row-equilibrated
         like debug_assemble), the near support-pair pattern as CSR (row_start, cols) and
-        the far-field levels as rows (level, order, nodes, M2L links)."""
+        the far-field levels as rows (level, order, nodes, M2L links, plane wave)."""
         N = self._mesh.vertex_count
         p = np.zeros(2 * N)
         p[0::2], p[1::2] = np.real(pressure), np.imag(pressure)
@@ -408,7 +412,7 @@ class CudaBemSolver:
         _lib.check(self._lib.hs_bem_debug_fmm_far(self._handle, C.byref(n), k, tolerance, p.ctypes.data, far.ctypes.data,
                                                   row.ctypes.data, None, 0, C.byref(count), None, 0, C.byref(levels)))
         cols = np.zeros(max(count.value, 1), np.uint32)
-        info = np.zeros((max(levels.value, 1), 4), np.uint32)
+        info = np.zeros((max(levels.value, 1), 5), np.uint32)
         _lib.check(self._lib.hs_bem_debug_fmm_far(self._handle, C.byref(n), k, tolerance, p.ctypes.data, far.ctypes.data,
                                                   row.ctypes.data, cols.ctypes.data, count.value, C.byref(count),
                                                   info.ctypes.data, levels.value, C.byref(levels)))

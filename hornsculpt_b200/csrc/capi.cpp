@@ -441,11 +441,21 @@ hs_status hs_bem_debug_fmm_far(hs_bem_session *s, const hs_numerics *numerics, d
             *level_count = levels.size();
         if (level_info)
             for (size_t i = 0; i < std::min(levels.size(), level_capacity); ++i) {
-                level_info[4 * i] = levels[i].level;
-                level_info[4 * i + 1] = levels[i].order;
-                level_info[4 * i + 2] = levels[i].nodes;
-                level_info[4 * i + 3] = levels[i].m2lLinks;
+                level_info[5 * i] = levels[i].level;
+                level_info[5 * i + 1] = levels[i].order;
+                level_info[5 * i + 2] = levels[i].nodes;
+                level_info[5 * i + 3] = levels[i].m2lLinks;
+                level_info[5 * i + 4] = levels[i].planeWave;
             }
+    });
+}
+
+hs_status hs_bem_session_set_plane_wave_threshold(hs_bem_session *s, double threshold) {
+    if (!s || !(threshold > 0))
+        return fail(HS_E_INVALID, "Plane-wave threshold must be positive.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->setPlaneWaveThreshold(threshold);
     });
 }
 

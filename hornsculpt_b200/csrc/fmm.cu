@@ -14,6 +14,7 @@
 #include "kernel_timer.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <complex>
 #include <map>
@@ -739,6 +740,213 @@ __global__ void coaxKernel(uint32_t classes, const int *__restrict__ pin, const 
     }
 }
 
+// ------------------------------------------------ plane-wave (diagonal) M2L
+// Electrically large levels translate in the plane-wave form instead of
+// rotate-coaxial-rotate (the reference's LF/HF switch,
+// fmm/wideband_transfer.cpp:266-310, and its diagonal product,
+// cuda/support_fmm_operator.cu:36-76). With s on the unit sphere,
+//   sigma(s) = sum_nm i^n M_nm Y_n^m(s)                 (source signature),
+//   psi(s)   = sum over links T_t(s) sigma_source(s),
+//   T_t(s)   = sum_{l<=p} (2l+1) (-i)^l h_l(k|t|) P_l(s.t/|t|),
+//   L_nm    += (-i)^n  int conj(Y_n^m(s)) psi(s) dOmega,
+// for t = target centre - source centre; the sphere rule (Gauss-Legendre in
+// cos(theta) x uniform azimuth) is exact for the degree 3p of the integrand.
+// Conversions are separable: a Legendre stage per (m, theta row) and a Fourier
+// stage per (theta row, azimuth), O(p^3) per node; a link costs O(p^2).
+constexpr int kHfRows = 8;  // theta rows per chunk of the conversion kernels
+
+// sigma of the nodes `ids` (one CTA per node and channel).
+__global__ void __launch_bounds__(256) signatureKernel(const double2 *__restrict__ Mc,
+                                                       const uint64_t *__restrict__ coefOffset,
+                                                       const uint32_t *__restrict__ ids, int p,
+                                                       const double *__restrict__ theta, int nth, int nph, int nch,
+                                                       double2 *sigma) {
+    extern __shared__ double smem[];
+    const int nc = (p + 1) * (p + 1), tri = (p + 1) * (p + 2) / 2, mw = 2 * p + 1;
+    double2 *Mi = reinterpret_cast<double2 *>(smem);  // i^n M_nm
+    double2 *A = Mi + nc;                             // [mw][kHfRows]
+    double2 *root = A + size_t(mw) * kHfRows;         // exp(2 pi i q / nph)
+    const uint32_t node = blockIdx.x, ch = blockIdx.y;
+    const double2 *M = Mc + coefOffset[ids[node]] + size_t(ch) * nc;
+    for (int i = threadIdx.x; i < nc; i += blockDim.x) {
+        int n, m;
+        decode(i, n, m);
+        const double2 v = M[i];
+        // i^n: 1, i, -1, -i
+        const int r = n & 3;
+        Mi[i] = r == 0 ? v : r == 1 ? make_double2(-v.y, v.x) : r == 2 ? make_double2(-v.x, -v.y) : make_double2(v.y, -v.x);
+    }
+    for (int q = threadIdx.x; q < nph; q += blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * q / nph, &sn, &cs);
+        root[q] = make_double2(cs, sn);
+    }
+    __syncthreads();
+    const size_t Q = size_t(nth) * nph;
+    double2 *out = sigma + (size_t(node) * nch + ch) * Q;
+    for (int i0 = 0; i0 < nth; i0 += kHfRows) {
+        for (int e = threadIdx.x; e < mw * kHfRows; e += blockDim.x) {
+            const int m = e % mw - p, ii = e / mw, i = i0 + ii;
+            double2 acc = make_double2(0, 0);
+            if (i < nth) {
+                const int am = m < 0 ? -m : m;
+                const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;  // Theta_n^-m = (-1)^m Theta_n^m
+                const double *th = theta + size_t(i) * tri;
+                for (int n = am; n <= p; ++n) {
+                    const double t = sg * th[triIndex(n, am)];
+                    const double2 v = Mi[coefIndex(n, m)];
+                    acc.x += t * v.x;
+                    acc.y += t * v.y;
+                }
+            }
+            A[size_t(m + p) * kHfRows + ii] = acc;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < kHfRows * nph; e += blockDim.x) {
+            const int ii = e / nph, j = e % nph, i = i0 + ii;
+            if (i >= nth)
+                continue;
+            double2 acc = make_double2(0, 0);
+            for (int m = -p; m <= p; ++m) {
+                const int q = int(((long long)(m + nph) * j) % nph);
+                acc = cadd(acc, cmul(A[size_t(m + p) * kHfRows + ii], root[q]));
+            }
+            out[size_t(i) * nph + j] = acc;
+        }
+        __syncthreads();
+    }
+}
+
+// psi of every target node with links at the level (CTA: target x sample chunk):
+// psi_o(s) = sum over its links T_class(s) sigma_source(s), in link order.
+__global__ void __launch_bounds__(256) diagonalKernel(const uint32_t *__restrict__ linkStart,
+                                                      const uint32_t *__restrict__ linkSource,
+                                                      const uint32_t *__restrict__ linkClass,
+                                                      const double2 *__restrict__ T, const double2 *__restrict__ sigma,
+                                                      size_t Q, int nch, double2 *psi) {
+    const uint32_t o = blockIdx.x;
+    const size_t q = size_t(blockIdx.y) * blockDim.x + threadIdx.x;
+    if (q >= Q)
+        return;
+    double2 acc[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        acc[c] = make_double2(0, 0);
+    for (uint32_t li = linkStart[o]; li < linkStart[o + 1]; ++li) {
+        const double2 t = T[size_t(linkClass[li]) * Q + q];
+        const double2 *src = sigma + size_t(linkSource[li]) * nch * Q + q;
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            if (c < nch)
+                acc[c] = cadd(acc[c], cmul(t, src[size_t(c) * Q]));
+    }
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+        if (c < nch)
+            psi[(size_t(o) * nch + c) * Q + q] = acc[c];
+}
+
+// L_nm += (-i)^n sum_i w_i Theta_n^m(x_i) (2 pi / nph) sum_j exp(-i m phi_j) psi(i, j)
+// for each target node (CTA: target x channel).
+__global__ void __launch_bounds__(256) projectKernel(const double2 *__restrict__ psi,
+                                                     const uint32_t *__restrict__ outNodes,
+                                                     const uint64_t *__restrict__ coefOffset, int p,
+                                                     const double *__restrict__ theta,
+                                                     const double *__restrict__ weights, int nth, int nph, int nch,
+                                                     double2 *Lc) {
+    extern __shared__ double smem[];
+    const int nc = (p + 1) * (p + 1), tri = (p + 1) * (p + 2) / 2, mw = 2 * p + 1;
+    double2 *acc = reinterpret_cast<double2 *>(smem);  // [nc]
+    double2 *B = acc + nc;                             // [mw][kHfRows]
+    double2 *root = B + size_t(mw) * kHfRows;
+    const uint32_t o = blockIdx.x, ch = blockIdx.y;
+    for (int i = threadIdx.x; i < nc; i += blockDim.x)
+        acc[i] = make_double2(0, 0);
+    for (int q = threadIdx.x; q < nph; q += blockDim.x) {
+        double sn, cs;
+        sincospi(2.0 * q / nph, &sn, &cs);
+        root[q] = make_double2(cs, sn);
+    }
+    __syncthreads();
+    const size_t Q = size_t(nth) * nph;
+    const double2 *in = psi + (size_t(o) * nch + ch) * Q;
+    for (int i0 = 0; i0 < nth; i0 += kHfRows) {
+        for (int e = threadIdx.x; e < mw * kHfRows; e += blockDim.x) {
+            const int m = e % mw - p, ii = e / mw, i = i0 + ii;
+            double2 b = make_double2(0, 0);
+            if (i < nth) {
+                const double2 *row = in + size_t(i) * nph;
+                for (int j = 0; j < nph; ++j) {
+                    const double2 r = root[int(((long long)(m + nph) * j) % nph)];
+                    const double2 v = row[j];
+                    b.x += v.x * r.x + v.y * r.y;  // v conj(r)
+                    b.y += v.y * r.x - v.x * r.y;
+                }
+                b.x *= weights[i];
+                b.y *= weights[i];
+            }
+            B[size_t(m + p) * kHfRows + ii] = b;
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+            int n, m;
+            decode(k, n, m);
+            const int am = m < 0 ? -m : m;
+            const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+            double2 a = acc[k];
+            for (int ii = 0; ii < kHfRows && i0 + ii < nth; ++ii) {
+                const double t = sg * theta[size_t(i0 + ii) * tri + triIndex(n, am)];
+                const double2 b = B[size_t(m + p) * kHfRows + ii];
+                a.x += t * b.x;
+                a.y += t * b.y;
+            }
+            acc[k] = a;
+        }
+        __syncthreads();
+    }
+    double2 *L = Lc + coefOffset[outNodes[o]] + size_t(ch) * nc;
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+        int n, m;
+        decode(k, n, m);
+        const double2 v = acc[k];
+        // (-i)^n: 1, -i, -1, i
+        const int r = n & 3;
+        const double2 w = r == 0 ? v : r == 1 ? make_double2(v.y, -v.x) : r == 2 ? make_double2(-v.x, -v.y)
+                                                                        : make_double2(-v.y, v.x);
+        L[k] = cadd(L[k], w);
+    }
+}
+
+// T_class(s_q) = sum_{l<=p} coef[class][l] P_l(s_q . u_class), coef = (2l+1) (-i)^l h_l(k|t|)
+// (one thread per class and sample).
+__global__ void hfTransferKernel(uint32_t classes, const double *__restrict__ dirs, const double2 *__restrict__ coef,
+                                 int p, const double *__restrict__ x, int nth, int nph, double2 *T) {
+    const size_t Q = size_t(nth) * nph;
+    const size_t e = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (e >= Q * classes)
+        return;
+    const uint32_t c = uint32_t(e / Q);
+    const size_t q = e % Q;
+    const int i = int(q / nph), j = int(q % nph);
+    const double ct = x[i], st = sqrt(fmax(0.0, 1.0 - ct * ct));
+    double sp, cp;
+    sincospi(2.0 * j / nph, &sp, &cp);
+    const double u = st * cp * dirs[3 * c] + st * sp * dirs[3 * c + 1] + ct * dirs[3 * c + 2];
+    const double2 *cf = coef + size_t(c) * (p + 1);
+    double p0 = 1.0, p1 = u;
+    double2 acc = make_double2(cf[0].x, cf[0].y);
+    if (p >= 1)
+        acc = make_double2(acc.x + cf[1].x * u, acc.y + cf[1].y * u);
+    for (int l = 2; l <= p; ++l) {
+        const double p2 = ((2 * l - 1) * u * p1 - (l - 1) * p0) / l;
+        acc.x += cf[l].x * p2;
+        acc.y += cf[l].y * p2;
+        p0 = p1;
+        p1 = p2;
+    }
+    T[e] = acc;
+}
+
 // FP32 coaxial tables of the mixed form: each entry (class, |m|, n, n') of the
 // FP64 table times exp(logRow[class][n'] + logCol[class][n]), the sigma factors
 // that take the scaled input coefficient to its unscaled value and the
@@ -939,6 +1147,19 @@ struct FmmOperator::Impl {
     bool wigner32Valid = false;
     int sigmaStride = 0;
     const double *levelSigma(int l) const { return fp32 ? sigma.as<double>() + size_t(l) * sigmaStride : nullptr; }
+    // Plane-wave M2L per level: the offset class of every M2L link (offsets in
+    // units of the level's cell width, so a handful of classes per level), the
+    // link sources as indices into the level's node list, and the tables of the
+    // prepared wavenumber. prepare() turns a level plane-wave when k times its
+    // shortest M2L distance reaches hfThreshold (FP64 operator only).
+    struct HfLevel {
+        bool active = false;
+        int p = 0, nth = 0, nph = 0;
+        std::vector<std::array<int64_t, 3>> offsets;
+        DevBuf ids, linkSource, linkClass, theta, x, weights, coef, dirs, T, sigma, psi;
+    };
+    std::vector<HfLevel> hf;
+    double hfThreshold = 12.0;
     bool useGraphs = true;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint32_t applies[2] = {0, 0};
@@ -1219,6 +1440,35 @@ FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : 
         put(I.dm2l[l], I.m2l[l]);
         put(I.dl2l[l], I.l2l[l]);
     }
+    // plane-wave link classes (offset vectors of the M2L links, per level)
+    I.hf.resize(levels);
+    for (int l = I.lmin; l < levels; ++l) {
+        const Impl::Plan &pl = I.m2l[l];
+        if (pl.links.empty())
+            continue;
+        Impl::HfLevel &h = I.hf[l];
+        std::map<uint32_t, uint32_t> index;
+        for (uint32_t i = 0; i < I.levelNodes[l].size(); ++i)
+            index[I.levelNodes[l][i]] = i;
+        std::map<std::array<int64_t, 3>, uint32_t> cls;
+        std::vector<uint32_t> src, cl;
+        const double w = widthOf(l);
+        for (size_t o = 0; o + 1 < pl.linkStart.size(); ++o)
+            for (uint32_t li = pl.linkStart[o]; li < pl.linkStart[o + 1]; ++li) {
+                const uint32_t sid = pl.links[li].source, tid = pl.outNodes[o];
+                std::array<int64_t, 3> off;
+                for (int d = 0; d < 3; ++d)
+                    off[d] = std::llround((nodes[tid].center[d] - nodes[sid].center[d]) / w);
+                const auto f = cls.emplace(off, uint32_t(h.offsets.size()));
+                if (f.second)
+                    h.offsets.push_back(off);
+                cl.push_back(f.first->second);
+                src.push_back(index.at(sid));
+            }
+        uploadVec(h.ids, I.levelNodes[l], s);
+        uploadVec(h.linkSource, src, s);
+        uploadVec(h.linkClass, cl, s);
+    }
     std::vector<TriPoint> rule = triangleRule(4);
     if (rule.size() != kRulePts)
         throw std::logic_error("fast multipole: unexpected degree-4 rule size");
@@ -1242,6 +1492,79 @@ FmmOperator::~FmmOperator() = default;
 void FmmOperator::setFp32(bool enabled) {
     impl_->fp32 = enabled;
     impl_->dropGraphs();
+}
+
+void FmmOperator::setHfThreshold(double threshold) {
+    impl_->hfThreshold = threshold;
+    impl_->dropGraphs();
+}
+
+// Plane-wave levels of the prepared wavenumber and their tables: the sphere
+// rule (Gauss-Legendre in cos(theta) with ceil((3p+2)/2) nodes, 3p+2 uniform
+// azimuths: exact for the degree 3p of sigma T conj(Y)), Theta_n^m at the rule's
+// rows, and T of every offset class.
+void FmmOperator::prepareHf(cudaStream_t stream) {
+    Impl &I = *impl_;
+    const int levels = int(tree_.levels.size());
+    for (int l = I.lmin; l < levels; ++l) {
+        Impl::HfLevel &h = I.hf[l];
+        h.active = false;
+        if (I.fp32 || h.offsets.empty() || I.order[l] < 8)
+            continue;
+        const double w = 2 * tree_.nodes[tree_.levels[l][0]].half;
+        double tmin = 1e300;
+        for (const auto &o : h.offsets)
+            tmin = std::min(tmin, w * std::sqrt(double(o[0] * o[0] + o[1] * o[1] + o[2] * o[2])));
+        if (k_ * tmin < I.hfThreshold)
+            continue;
+        h.active = true;
+        const int p = I.order[l];
+        h.p = p;
+        h.nth = (3 * p + 3) / 2;
+        h.nph = 3 * p + 2;
+        std::vector<double> gx, gw;
+        gaussLegendre(h.nth, gx, gw);
+        const size_t tri = size_t(p + 1) * (p + 2) / 2;
+        std::vector<double> theta(size_t(h.nth) * tri), weights(h.nth);
+        for (int i = 0; i < h.nth; ++i) {
+            const double st = std::sqrt(std::max(0.0, 1 - gx[i] * gx[i]));
+            for (int m = 0; m <= p; ++m)
+                thetaColumn(m, p, gx[i], st, theta.data() + size_t(i) * tri);
+            weights[i] = gw[i] * 2 * kFmmPi / h.nph;
+        }
+        uploadVec(h.theta, theta, stream);
+        uploadVec(h.x, gx, stream);
+        uploadVec(h.weights, weights, stream);
+        // T coefficients per class: (2l+1) (-i)^l h_l(k |t|), h_l = j_l - i y_l
+        const size_t classes = h.offsets.size();
+        std::vector<double> dirs(3 * classes);
+        std::vector<std::complex<double>> coef(classes * (p + 1));
+        std::vector<double> jb(p + 1), yb(p + 1);
+        for (size_t c = 0; c < classes; ++c) {
+            const auto &o = h.offsets[c];
+            const double len = std::sqrt(double(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]));
+            for (int d = 0; d < 3; ++d)
+                dirs[3 * c + d] = double(o[d]) / len;
+            const double kt = k_ * len * w;
+            besselJ(p, kt, jb.data());
+            besselY(p, kt, yb.data());
+            for (int n = 0; n <= p; ++n) {
+                const std::complex<double> hn(jb[n], -yb[n]);
+                const std::complex<double> mi[4] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}};
+                coef[c * (p + 1) + n] = double(2 * n + 1) * mi[n & 3] * hn;
+            }
+        }
+        uploadVec(h.dirs, dirs, stream);
+        uploadVec(h.coef, coef, stream);
+        const size_t Q = size_t(h.nth) * h.nph;
+        h.T.ensure(classes * Q * 16);
+        hfTransferKernel<<<unsigned((classes * Q + 255) / 256), 256, 0, stream>>>(
+            uint32_t(classes), h.dirs.as<double>(), h.coef.as<double2>(), p, h.x.as<double>(), h.nth, h.nph,
+            h.T.as<double2>());
+        fmmCheck(cudaGetLastError(), "plane-wave transfer launch");
+        h.sigma.ensure(I.levelNodes[l].size() * 6 * Q * 16);
+        h.psi.ensure(I.m2l[l].outNodes.size() * 6 * Q * 16);
+    }
 }
 
 void FmmOperator::setGraphs(bool enabled) {
@@ -1269,7 +1592,7 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
         const int lf = int(std::ceil(1.3 * d0)) + 1;
         I.order[l] = std::min(kFmmMaxOrder, std::max(hf, lf));
         levelInfo_.push_back({uint32_t(l), uint32_t(I.order[l]), uint32_t(I.levelNodes[l].size()),
-                              uint32_t(I.m2l[l].links.size()), r});
+                              uint32_t(I.m2l[l].links.size()), r, 0});
     }
     // coefficient storage: 6 channels per node of every taking part level
     I.hostCoefOffset.assign(nodes.size(), 0);
@@ -1366,6 +1689,9 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
         uint32_t(pin.size()), I.coaxPin.as<int>(), I.coaxPout.as<int>(), I.coaxStart.as<uint64_t>(),
         I.fl.as<double2>(), lmaxF, I.gaunt.as<double>(), I.gauntOff.as<uint32_t>(), P, I.coax.as<double2>());
     fmmCheck(cudaGetLastError(), "coaxial table launch");
+    prepareHf(stream);
+    for (auto &info : levelInfo_)
+        info.planeWave = I.hf[info.level].active ? 1 : 0;
     if (I.fp32) {
         // log sigma_n per level, sigma_n = (2n+1)!! / (k a_l)^n with a_l the level's node radius
         const int stride = P + 1;
@@ -1465,6 +1791,31 @@ void FmmOperator::run(const double *src, bool rhs, double *y, cudaStream_t strea
     fmmCheck(cudaMemcpyAsync(I.stageIn.p, src, inBytes, cudaMemcpyDeviceToDevice, stream), "far-field graph input");
     fmmCheck(cudaGraphLaunch(I.graph[mode], stream), "far-field graph launch");
     fmmCheck(cudaMemcpyAsync(y, I.stageOut.p, outBytes, cudaMemcpyDeviceToDevice, stream), "far-field graph output");
+}
+
+// M2L of one plane-wave level: signatures of the level's nodes, the diagonal
+// products along the links, projection of each target's field onto its locals.
+void FmmOperator::planeWaveM2L(int l, int nch, cudaStream_t stream) {
+    Impl &I = *impl_;
+    Impl::HfLevel &h = I.hf[l];
+    const int p = h.p, nc = (p + 1) * (p + 1), mw = 2 * p + 1;
+    const size_t Q = size_t(h.nth) * h.nph;
+    const size_t sm = (size_t(nc) + size_t(mw) * kHfRows + h.nph) * 16;
+    if (sm > kMaxShared)
+        throw Unsupported("Fast-multipole plane-wave order exceeds the shared-memory tables; refine the tree.");
+    fmmCheck(cudaFuncSetAttribute(signatureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)), "signature smem");
+    fmmCheck(cudaFuncSetAttribute(projectKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)), "project smem");
+    const uint32_t nodes = uint32_t(I.levelNodes[l].size()), outs = I.dm2l[l].count;
+    signatureKernel<<<dim3(nodes, nch), 256, sm, stream>>>(I.Mc.as<double2>(), I.coefOffset.as<uint64_t>(),
+                                                           h.ids.as<uint32_t>(), p, h.theta.as<double>(), h.nth, h.nph,
+                                                           nch, h.sigma.as<double2>());
+    diagonalKernel<<<dim3(outs, unsigned((Q + 255) / 256)), 256, 0, stream>>>(
+        I.dm2l[l].start.as<uint32_t>(), h.linkSource.as<uint32_t>(), h.linkClass.as<uint32_t>(), h.T.as<double2>(),
+        h.sigma.as<double2>(), Q, nch, h.psi.as<double2>());
+    projectKernel<<<dim3(outs, nch), 256, sm, stream>>>(h.psi.as<double2>(), I.dm2l[l].out.as<uint32_t>(),
+                                                        I.coefOffset.as<uint64_t>(), p, h.theta.as<double>(),
+                                                        h.weights.as<double>(), h.nth, h.nph, nch, I.Lc.as<double2>());
+    fmmCheck(cudaGetLastError(), "plane-wave M2L launch");
 }
 
 void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer) {
@@ -1572,6 +1923,8 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
         for (int l = I.lmin; l < levels; ++l)
             if (I.fp32)
                 translate(I.dm2l[l], I.order[l], I.order[l], I.Mc32.as<float2>(), I.Lc32.as<float2>(), false);
+            else if (I.hf[l].active)
+                planeWaveM2L(l, nch, stream);
             else
                 translate(I.dm2l[l], I.order[l], I.order[l], I.Mc.as<double2>(), I.Lc.as<double2>(), false);
     }

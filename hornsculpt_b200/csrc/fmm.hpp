@@ -26,6 +26,7 @@ class KernelTimer;
 struct FmmLevelInfo {
     uint32_t level, order, nodes, m2lLinks;
     double radius;
+    uint32_t planeWave;  // 1: M2L in the plane-wave (diagonal) form at this level
 };
 
 class FmmOperator {
@@ -64,6 +65,9 @@ class FmmOperator {
     // Mixed form: translations in FP32 on scaled expansions (P2M and L2P stay
     // FP64); takes effect at the next prepare().
     void setFp32(bool enabled);
+    // k times the shortest M2L distance from which a level translates in the
+    // plane-wave form (default 12; a large value keeps every level rotational).
+    void setHfThreshold(double threshold);
 
   private:
     struct Impl;
@@ -76,6 +80,8 @@ class FmmOperator {
     double k_ = 0;
     void run(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer);
     void launchApply(const double *src, bool rhs, double *y, cudaStream_t stream, KernelTimer *timer);
+    void prepareHf(cudaStream_t stream);
+    void planeWaveM2L(int level, int nch, cudaStream_t stream);
 };
 
 // The fast-multipole linear system of one frequency: A = N + R F, with N the

@@ -1137,6 +1137,12 @@ void Session::dropGraphs() {
     ++generation_;
 }
 
+void Session::setPlaneWaveThreshold(double threshold) {
+    planeWaveThreshold_ = threshold;
+    if (fmm_)
+        fmm_->setHfThreshold(threshold);
+}
+
 void Session::setGraphs(bool enabled) {
     graphs_ = enabled;
     dropGraphs();
@@ -1233,6 +1239,7 @@ FmmOperator &Session::fmmOperator(const hs_numerics &o, double tuneK, double tun
         fmm_.reset();
         fmm_ = std::make_unique<FmmOperator>(space_, st);
         fmm_->setGraphs(graphs_);
+        fmm_->setHfThreshold(planeWaveThreshold_);
         fmmSettings_ = st;
     }
     return *fmm_;

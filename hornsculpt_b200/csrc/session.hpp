@@ -71,6 +71,7 @@ class Session {
     // Replay of the per-batch dense chain and of the fast-multipole far-field
     // apply as captured CUDA graphs (on by default); graph launches so far.
     void setGraphs(bool enabled);
+    void setPlaneWaveThreshold(double threshold);
     uint64_t graphLaunches() const { return graphLaunches_; }
     // Device bytes a solve may hold beyond the resident geometry and plan
     // (0: 60 % of free memory); bounds the frequency batch.
@@ -115,6 +116,7 @@ class Session {
     std::vector<DenseGraph> denseGraphs_;
     uint64_t generation_ = 0, graphLaunches_ = 0;
     bool graphs_ = true;
+    double planeWaveThreshold_ = 12.0;
 
     MeshInput mesh_;
     V3 origin_{};

@@ -265,8 +265,11 @@ hs_status hs_bem_debug_lu(uint32_t precision, size_t n, size_t batch, const doub
  * tolerance `tolerance`, writing `far` (vertex_count complex); near_row_start
  * (vertex_count + 1) and near_cols (capacity near_capacity, sorted per row)
  * receive the near pattern, near_count its size; level_info receives per
- * far-field level {level, order, nodes, M2L links} (capacity level_capacity
- * rows of 4 u32), level_count their number. Pointers after `far` may be NULL.
+ * far-field level {level, order, nodes, M2L links, plane wave} (capacity
+ * level_capacity rows of 5 u32; plane wave 1 when the level's M2L runs in the
+ * diagonal plane-wave form), level_count their number. Pointers after `far`
+ * may be NULL. With numerics.precision = HS_PRECISION_MIXED the hook applies
+ * the mixed form's operator (scaled expansions, FP32 translations).
  * hs_bem_debug_fmm_selftest checks the expansion primitives (Bessel and
  * Legendre recurrences, Wigner rotations, Gaunt-built coaxial translations)
  * against a direct kernel sum on the host and writes the relative error. */
@@ -275,6 +278,13 @@ hs_status hs_bem_debug_fmm_far(hs_bem_session *session, const hs_numerics *numer
                                size_t near_capacity, size_t *near_count, uint32_t *level_info, size_t level_capacity,
                                size_t *level_count);
 hs_status hs_bem_debug_fmm_selftest(double *error);
+/* Fast-multipole LF/HF switch (wideband_transfer.cpp:266-310): a level's M2L
+ * runs in the diagonal plane-wave form when k times its shortest M2L distance
+ * is at least `threshold` (default 12) and its order is at least 8; below, the
+ * rotate-coaxial-rotate form. A very large threshold keeps every level
+ * rotational. Applies to the FP64 operator; the mixed form's FP32 inner
+ * operator stays rotational. */
+hs_status hs_bem_session_set_plane_wave_threshold(hs_bem_session *session, double threshold);
 /* The support tree of the fast-multipole form (host only): the mesh centred on
  * vertex 0 like a session; sizes = {nodes, levels, pressure-pressure near,
  * pressure-pressure far, pressure-flux near, pressure-flux far} and links the

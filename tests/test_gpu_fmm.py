@@ -213,3 +213,53 @@ def test_mixed_fast_multipole_matches_dense(case, freqs):
         print(case, fm.frequency, "surface error", err, "iterations", em.iterations, "residual", em.boundary_residual)
         assert em.boundary_residual <= 1e-6
         assert err < 1e-5
+
+
+@pytest.mark.parametrize("case, freq, threshold", [("icosphere3", 3000.0, 8.0), ("horn", 6000.0, 12.0),
+                                                   ("horn", 8000.0, 12.0)])
+def test_plane_wave_far_operator_matches_dense_far_part(case, freq, threshold):
+    """Electrically large levels translate in the diagonal plane-wave form (the
+    reference's LF/HF switch, wideband_transfer.cpp:266-310): the far operator with
+    plane-wave levels against the far support pairs of the dense FP64 matrix, and
+    against the all-rotational operator."""
+    mesh = {"icosphere3": lambda: meshes.icosphere(3),
+            "horn": lambda: meshes.exponential_horn(h=0.0128, seed=5)}[case]()
+    N, T = mesh.vertex_count, mesh.triangle_count
+    k = 2 * np.pi * freq / 343.0
+    rng = np.random.default_rng(11)
+    p = rng.normal(size=N) + 1j * rng.normal(size=N)
+    with hs.CudaBemSolver(mesh) as solver:
+        A, _ = solver.debug_assemble(FP64, k, k, np.zeros(T, complex))
+        solver.set_plane_wave_threshold(threshold)
+        far, row, cols, levels = solver.debug_fmm_far(FP64, k, 1e-8, p)
+        solver.set_plane_wave_threshold(1e12)
+        rot, _, _, rlevels = solver.debug_fmm_far(FP64, k, 1e-8, p)
+    assert levels[:, 4].sum() >= 1 and rlevels[:, 4].sum() == 0
+    mask = _far_mask(N, row, cols)
+    expected = (A * mask) @ p
+    full = A @ p
+    full_rel = np.linalg.norm(far - expected) / np.linalg.norm(full)
+    far_rel = np.linalg.norm(far - expected) / np.linalg.norm(expected)
+    vs_rot = np.linalg.norm(far - rot) / np.linalg.norm(rot)
+    print(case, freq, "levels", levels.tolist(), "far rel", far_rel, "of full", full_rel, "vs rotational", vs_rot)
+    assert full_rel < 1e-6 and far_rel < 1e-4 and vs_rot < 1e-5
+
+
+def test_plane_wave_levels_in_a_solve():
+    """A fast-multipole solve of the 4k-triangle horn at 6 kHz with plane-wave
+    levels meets the dense FP64 solve."""
+    mesh = meshes.exponential_horn(h=0.0128, seed=5)
+    req = lambda acc: hs.BemRequest(
+        frequencies=[6000.0], observers=[(0.0, 0.0, 1.0)],
+        excitations=[hs.BemExcitation("throat", [hs.FaceVelocity(meshes.HORN_THROAT, 1.0)])],
+        numerics=hs.BemNumerics(precision="fp64", acceleration=acc, relative_residual_tolerance=1e-6))
+    with hs.CudaBemSolver(mesh) as solver:
+        dense = solver.solve(req("dense"))
+        fmm = solver.solve(req("fast_multipole"))
+        _, _, _, levels = solver.debug_fmm_far(FP64, 2 * np.pi * 6000.0 / 343.0, 1e-8, np.ones(mesh.vertex_count))
+    assert levels[:, 4].sum() >= 1
+    a, b = dense.frequencies[0].excitations[0], fmm.frequencies[0].excitations[0]
+    err = np.linalg.norm(b.boundary.pressure_trace - a.boundary.pressure_trace) / np.linalg.norm(
+        a.boundary.pressure_trace)
+    print("plane-wave solve error", err, "iterations", b.iterations)
+    assert b.boundary_residual <= 1e-6 and err < 1e-5
