@@ -255,6 +255,18 @@ class CudaBemSolver:
         """k x shortest M2L distance from which a fast-multipole level translates in the plane-wave form."""
         _lib.check(self._lib.hs_bem_session_set_plane_wave_threshold(self._handle, threshold))
 
+    def set_fmm_audit(self, mode: str) -> None:
+        """Fast-multipole acceptance audit: "automatic" (the reference's policy), "expansion" (finer
+        expansions and panel-rule promotion) or "direct" (the exact dense system's residual)."""
+        code = {"automatic": 0, "expansion": 1, "direct": 2}[mode]
+        _lib.check(self._lib.hs_bem_session_set_fmm_audit(self._handle, code))
+
+    def fmm_audit_counts(self) -> tuple:
+        """(direct audits, far-field panel-rule promotions) of this session so far."""
+        d, q = C.c_uint64(), C.c_uint64()
+        _lib.check(self._lib.hs_bem_session_fmm_audit_counts(self._handle, C.byref(d), C.byref(q)))
+        return d.value, q.value
+
     def set_graphs(self, enabled: bool) -> None:
         """Replay of the dense batch chain and the fast-multipole far-field apply as captured CUDA graphs."""
         _lib.check(self._lib.hs_bem_session_set_graphs(self._handle, int(enabled)))

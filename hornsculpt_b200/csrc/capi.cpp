@@ -459,6 +459,23 @@ hs_status hs_bem_session_set_plane_wave_threshold(hs_bem_session *s, double thre
     });
 }
 
+hs_status hs_bem_session_set_fmm_audit(hs_bem_session *s, uint32_t mode) {
+    if (!s || mode > 2)
+        return fail(HS_E_INVALID, "Fast-multipole audit mode must be 0, 1 or 2.");
+    std::lock_guard<std::mutex> lock(s->impl->mutex);
+    s->impl->fmmAuditMode_ = mode;
+    return HS_OK;
+}
+
+hs_status hs_bem_session_fmm_audit_counts(const hs_bem_session *s, uint64_t *direct_audits,
+                                          uint64_t *quadrature_promotions) {
+    if (!s || !direct_audits || !quadrature_promotions)
+        return fail(HS_E_INVALID, "Session and outputs must be non-null.");
+    *direct_audits = s->impl->directAudits_;
+    *quadrature_promotions = s->impl->quadraturePromotions_;
+    return HS_OK;
+}
+
 hs_status hs_bem_debug_fmm_selftest(double *error) {
     if (!error)
         return fail(HS_E_INVALID, "Self-test error pointer must be non-null.");

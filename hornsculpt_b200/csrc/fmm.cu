@@ -87,8 +87,8 @@ struct TransLink {
     double phi;
 };
 
-constexpr int kRulePts = 6;
-__constant__ double cFmmRule[kRulePts * 4];  // b0, b1, b2, physical weight fraction (sum 1)
+// Panel rule of the far field: per point b0, b1, b2 and the physical weight
+// fraction (sum 1), in device memory per operator (its degree can be promoted).
 constexpr int kWarps = 8;
 constexpr size_t kMaxShared = 227 * 1024;  // dynamic shared memory per CTA (opt-in)
 
@@ -174,9 +174,10 @@ __device__ __forceinline__ void decode(int k, int &n, int &m) {
 }
 
 // Quadrature point q of an item's panel: position and the six channel strengths.
-__device__ void pointStrengths(const FmmPanel &P, uint32_t mask, int q, const double2 *p, double *x, double2 (&s)[6]) {
-    const double b0 = cFmmRule[4 * q], b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
-    const double w = cFmmRule[4 * q + 3] * P.area;
+__device__ void pointStrengths(const FmmPanel &P, uint32_t mask, const double *rule, int q, const double2 *p,
+                               double *x, double2 (&s)[6]) {
+    const double b0 = rule[4 * q], b1 = rule[4 * q + 1], b2 = rule[4 * q + 2];
+    const double w = rule[4 * q + 3] * P.area;
     for (int d = 0; d < 3; ++d)
         x[d] = P.v0[d] + b1 * P.e1[d] + b2 * P.e2[d];
     const double b[3] = {b0, b1, b2};
@@ -198,10 +199,10 @@ __device__ void pointStrengths(const FmmPanel &P, uint32_t mask, int q, const do
 
 // Right-hand-side source: panel s's flux q_s emitted through the leaf's
 // vertex supports of s, 1/3 per support (channel 0).
-__device__ void fluxStrength(const FmmPanel &P, uint32_t panel, uint32_t mask, int q, const double2 *flux, double *x,
-                             double2 (&s)[6]) {
-    const double b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
-    const double w = cFmmRule[4 * q + 3] * P.area * double(__popc(mask)) / 3.0;
+__device__ void fluxStrength(const FmmPanel &P, uint32_t panel, uint32_t mask, const double *rule, int q,
+                             const double2 *flux, double *x, double2 (&s)[6]) {
+    const double b1 = rule[4 * q + 1], b2 = rule[4 * q + 2];
+    const double w = rule[4 * q + 3] * P.area * double(__popc(mask)) / 3.0;
     for (int d = 0; d < 3; ++d)
         x[d] = P.v0[d] + b1 * P.e1[d] + b2 * P.e2[d];
     const double2 qs = flux[panel];
@@ -216,7 +217,8 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
                                                  const FmmItem *__restrict__ items, const double *__restrict__ centers,
                                                  const uint64_t *__restrict__ coefOffset, int p, double k,
                                                  const double2 *__restrict__ pvec, double2 *M, int rhsMode,
-                                                 float2 *M32, const double *__restrict__ sigma) {
+                                                 float2 *M32, const double *__restrict__ sigma,
+                                                 const double *__restrict__ rule, int rulePts) {
     extern __shared__ double smem[];
     const int P = p;
     const int nch = rhsMode ? 1 : 6;
@@ -227,7 +229,7 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
     const uint32_t leaf = leaves[blockIdx.x];
     const double *c = centers + 3 * size_t(leaf);
     const uint32_t i0 = itemStart[blockIdx.x], i1 = itemStart[blockIdx.x + 1];
-    const uint32_t points = (i1 - i0) * kRulePts;
+    const uint32_t points = (i1 - i0) * rulePts;
     const int nc = (P + 1) * (P + 1);
     double2 *out = M + coefOffset[leaf];
     float2 *out32 = M32 ? M32 + coefOffset[leaf] : nullptr;
@@ -243,13 +245,13 @@ __global__ void __launch_bounds__(256) p2mKernel(const FmmPanel *__restrict__ pa
         for (uint32_t base = 0; base < points; base += kWarps) {
             const uint32_t idx = base + warp;
             if (idx < points) {
-                const FmmItem it = items[i0 + idx / kRulePts];
+                const FmmItem it = items[i0 + idx / rulePts];
                 double x[3];
                 double2 s[6];
                 if (rhsMode)
-                    fluxStrength(panels[it.panel], it.panel, it.mask, idx % kRulePts, pvec, x, s);
+                    fluxStrength(panels[it.panel], it.panel, it.mask, rule, idx % rulePts, pvec, x, s);
                 else
-                    pointStrengths(panels[it.panel], it.mask, idx % kRulePts, pvec, x, s);
+                    pointStrengths(panels[it.panel], it.mask, rule, idx % rulePts, pvec, x, s);
                 fillTable(mine, P, x[0] - c[0], x[1] - c[1], x[2] - c[2], k, lane);
                 if (lane < 6)
                     str[warp * 6 + lane] = s[lane];
@@ -495,7 +497,8 @@ __global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ pa
                                                  const FmmItem *__restrict__ items, const double *__restrict__ centers,
                                                  const uint64_t *__restrict__ coefOffset, int p, double k,
                                                  const double2 *__restrict__ Lcoef, double2 *far,
-                                                 const float2 *__restrict__ L32, const double *__restrict__ sigma) {
+                                                 const float2 *__restrict__ L32, const double *__restrict__ sigma,
+                                                 const double *__restrict__ rule, int rulePts) {
     extern __shared__ double smem[];
     const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
     const size_t td = tableDoubles(P);
@@ -539,8 +542,8 @@ __global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ pa
         const FmmItem item = items[it];
         const FmmPanel &Pn = panels[item.panel];
         double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-        for (int q = 0; q < kRulePts; ++q) {
-            const double b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
+        for (int q = 0; q < rulePts; ++q) {
+            const double b1 = rule[4 * q + 1], b2 = rule[4 * q + 2];
             double x[3];
             for (int d = 0; d < 3; ++d)
                 x[d] = Pn.v0[d] + b1 * Pn.e1[d] + b2 * Pn.e2[d];
@@ -567,8 +570,8 @@ __global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ pa
             double2 F[7];
             for (int ch = 0; ch < 7; ++ch)
                 F[ch] = make_double2(k * f[ch].y, -k * f[ch].x);
-            const double w = cFmmRule[4 * q + 3] * Pn.area;
-            const double bq[3] = {cFmmRule[4 * q], b1, b2};
+            const double w = rule[4 * q + 3] * Pn.area;
+            const double bq[3] = {rule[4 * q], b1, b2};
             // D + i k n.V
             double2 nv = make_double2(0, 0);
             for (int d = 0; d < 3; ++d) {
@@ -606,7 +609,8 @@ __global__ void __launch_bounds__(256) l2pRhsKernel(const FmmPanel *__restrict__
                                                     const FmmItem *__restrict__ items, const double *__restrict__ centers,
                                                     const uint64_t *__restrict__ coefOffset, int p, double k,
                                                     const double2 *__restrict__ Lcoef, double2 *far,
-                                                    const float2 *__restrict__ L32, const double *__restrict__ sigma) {
+                                                    const float2 *__restrict__ L32, const double *__restrict__ sigma,
+                                                    const double *__restrict__ rule, int rulePts) {
     extern __shared__ double smem[];
     const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
     const size_t td = tableDoubles(P);
@@ -642,8 +646,8 @@ __global__ void __launch_bounds__(256) l2pRhsKernel(const FmmPanel *__restrict__
         const FmmItem item = items[it];
         const FmmPanel &Pn = panels[item.panel];
         double2 acc[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-        for (int q = 0; q < kRulePts; ++q) {
-            const double b1 = cFmmRule[4 * q + 1], b2 = cFmmRule[4 * q + 2];
+        for (int q = 0; q < rulePts; ++q) {
+            const double b1 = rule[4 * q + 1], b2 = rule[4 * q + 2];
             double x[3];
             for (int d = 0; d < 3; ++d)
                 x[d] = Pn.v0[d] + b1 * Pn.e1[d] + b2 * Pn.e2[d];
@@ -676,8 +680,8 @@ __global__ void __launch_bounds__(256) l2pRhsKernel(const FmmPanel *__restrict__
             }
             // -S + (i / k) n.grad S
             const double2 v = make_double2(-F[0].x - dn.y / k, -F[0].y + dn.x / k);
-            const double w = cFmmRule[4 * q + 3] * Pn.area;
-            const double bq[3] = {cFmmRule[4 * q], b1, b2};
+            const double w = rule[4 * q + 3] * Pn.area;
+            const double bq[3] = {rule[4 * q], b1, b2};
             for (int a = 0; a < 3; ++a)
                 if ((item.mask >> a) & 1) {
                     acc[a].x += w * bq[a] * v.x;
@@ -1160,6 +1164,9 @@ struct FmmOperator::Impl {
     };
     std::vector<HfLevel> hf;
     double hfThreshold = 12.0;
+    DevBuf rule;
+    int rulePts = 0;
+    unsigned panelDegree = 4;
     bool useGraphs = true;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     uint32_t applies[2] = {0, 0};
@@ -1469,25 +1476,34 @@ FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : 
         uploadVec(h.linkSource, src, s);
         uploadVec(h.linkClass, cl, s);
     }
-    std::vector<TriPoint> rule = triangleRule(4);
-    if (rule.size() != kRulePts)
-        throw std::logic_error("fast multipole: unexpected degree-4 rule size");
-    double ws = 0;
-    for (const auto &r : rule)
-        ws += r.w;
-    double hr[kRulePts * 4];
-    for (int q = 0; q < kRulePts; ++q) {
-        hr[4 * q] = rule[q].b[0];
-        hr[4 * q + 1] = rule[q].b[1];
-        hr[4 * q + 2] = rule[q].b[2];
-        hr[4 * q + 3] = rule[q].w / ws;
-    }
-    fmmCheck(cudaMemcpyToSymbol(cFmmRule, hr, sizeof(hr)), "rule upload");
+    setPanelDegree(4);
     fmmCheck(cudaDeviceSynchronize(), "setup");
     I.far.ensure(3 * size_t(I.T) * 16);
 }
 
 FmmOperator::~FmmOperator() = default;
+
+void FmmOperator::setPanelDegree(unsigned degree) {
+    Impl &I = *impl_;
+    const std::vector<TriPoint> rule = triangleRule(degree);
+    double ws = 0;
+    for (const auto &r : rule)
+        ws += r.w;
+    std::vector<double> hr(4 * rule.size());
+    for (size_t q = 0; q < rule.size(); ++q) {
+        hr[4 * q] = rule[q].b[0];
+        hr[4 * q + 1] = rule[q].b[1];
+        hr[4 * q + 2] = rule[q].b[2];
+        hr[4 * q + 3] = rule[q].w / ws;
+    }
+    uploadVec(I.rule, hr, nullptr);
+    fmmCheck(cudaStreamSynchronize(nullptr), "rule upload");
+    I.rulePts = int(rule.size());
+    I.panelDegree = degree;
+    I.dropGraphs();
+}
+
+unsigned FmmOperator::panelDegree() const { return impl_->panelDegree; }
 
 void FmmOperator::setFp32(bool enabled) {
     impl_->fp32 = enabled;
@@ -1906,7 +1922,8 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
                                                    I.dLeafStart[l].as<uint32_t>(), I.dItems.as<FmmItem>() + I.itemBase[l],
                                                    I.centers.as<double>(), I.coefOffset.as<uint64_t>(), P, k_, pv,
                                                    I.Mc.as<double2>(), rhs ? 1 : 0,
-                                                   I.fp32 ? I.Mc32.as<float2>() : nullptr, I.levelSigma(l));
+                                                   I.fp32 ? I.Mc32.as<float2>() : nullptr, I.levelSigma(l),
+                                                   I.rule.as<double>(), I.rulePts);
             fmmCheck(cudaGetLastError(), "p2m launch");
         }
     }
@@ -1955,7 +1972,7 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
                     I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(), I.dLeafStart[l].as<uint32_t>(),
                     I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(), I.coefOffset.as<uint64_t>(), p, k_,
                     I.Lc.as<double2>(), I.far.as<double2>(), I.fp32 ? I.Lc32.as<float2>() : nullptr,
-                    I.levelSigma(l));
+                    I.levelSigma(l), I.rule.as<double>(), I.rulePts);
             } else {
                 fmmCheck(cudaFuncSetAttribute(l2pKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                          "l2p smem");
@@ -1964,7 +1981,7 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
                                                        I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(),
                                                        I.coefOffset.as<uint64_t>(), p, k_, I.Lc.as<double2>(),
                                                        I.far.as<double2>(), I.fp32 ? I.Lc32.as<float2>() : nullptr,
-                                                       I.levelSigma(l));
+                                                       I.levelSigma(l), I.rule.as<double>(), I.rulePts);
             }
             fmmCheck(cudaGetLastError(), "l2p launch");
         }

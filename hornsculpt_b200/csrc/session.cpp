@@ -705,16 +705,22 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 // near support pairs and the near right-hand side from the near panel-pair records
                 double *rhsB = dRhs_.as<double>() + size_t(b) * E * N * 2;
                 const double *fluxB = dFlux_.as<double>() + size_t(b) * E * T * 2;
+                const size_t reals = size_t(E) * N * 2;
+                double *nearRhs = dNearRhs_.as<double>();
                 assembleNearField(geo, dKs_.as<double>() + b, dGauss_.as<double>(), fluxB, E, layout,
-                                  dNearWork_.as<void>(), fmmSystem_->nearValues(), rhsB, dError_.as<int>(), s, &timer_);
+                                  dNearWork_.as<void>(), fmmSystem_->nearValues(), nearRhs, dError_.as<int>(), s,
+                                  &timer_);
                 if (inner)
                     fmmSystem_->roundNearValues(s);
                 cuda(cudaEventRecord(ev.assembled, s), "phase event");
-                {
+                // right-hand side with the operator's current far-field panel rule
+                const auto buildRhs = [&](double *dst) {
                     TimedScope scope(&timer_, "fmm_rhs_far", s);
+                    cuda(cudaMemcpyAsync(dst, nearRhs, reals * 8, cudaMemcpyDeviceToDevice, s), "near rhs copy");
                     op.applyFarRhs(fluxB, E, dCorr_.as<double>(), s, &timer_);
-                    fmmSystem_->addScaled(rhsB, dCorr_.as<double>(), E, s);
-                }
+                    fmmSystem_->addScaled(dst, dCorr_.as<double>(), E, s);
+                };
+                buildRhs(rhsB);
                 cuda(cudaEventRecord(ev.factored, s), "phase event");
                 fmmSystem_->factorBlocks(s, &timer_);
                 double *xB = dX_.as<double>() + size_t(b) * E * N * 2;
@@ -723,52 +729,144 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                                   rel, its, inner);
                 for (uint32_t e = 0; e < E; ++e)
                     krylov[size_t(b) * E + e] = its[e];
-                // Audit against a ten times finer expansion operator and defect-correct
-                // (SupportFmmLinearSolver::solve / improve, support_fmm_solve.cu:324-343,
-                // 575-634): accept when the audited residual meets the target and the two
-                // operators differ on x by at most a quarter of it; otherwise tighten the
-                // working tolerance and solve for the audited residual's correction.
-                double tau = expansionTolerance;
-                const size_t reals = size_t(E) * N * 2;
-                std::vector<double> relWork, relAudit;
-                std::vector<cplx> rWork(size_t(E) * N), rAudit(size_t(E) * N);
-                for (uint32_t round = 0;; ++round) {
-                    TimedScope scope(&timer_, "fmm_audit", s);
-                    fmmSystem_->residual(rhsB, xB, E, dAuditWork_.as<double>(), relWork, s, &timer_);
-                    op.prepare(ks[b], .1 * tau, s);
-                    fmmSystem_->residual(rhsB, xB, E, dAuditFine_.as<double>(), relAudit, s, &timer_);
-                    cuda(cudaMemcpyAsync(rWork.data(), dAuditWork_.as<void>(), reals * 8, cudaMemcpyDeviceToHost, s),
-                         "audit download");
-                    cuda(cudaMemcpyAsync(rAudit.data(), dAuditFine_.as<void>(), reals * 8, cudaMemcpyDeviceToHost, s),
-                         "audit download");
-                    std::vector<cplx> rhsHost(size_t(E) * N);
-                    cuda(cudaMemcpyAsync(rhsHost.data(), rhsB, reals * 8, cudaMemcpyDeviceToHost, s), "audit download");
-                    cuda(cudaStreamSynchronize(s), "CUDA fast-multipole audit");
-                    bool accept = true;
-                    for (uint32_t e = 0; e < E; ++e) {
-                        double dd = 0, bb = 0;
-                        for (size_t i = 0; i < N; ++i) {
-                            const double m = space_.lumpedMass[i];
-                            dd += m * std::norm(rAudit[size_t(e) * N + i] - rWork[size_t(e) * N + i]);
-                            bb += m * std::norm(rhsHost[size_t(e) * N + i]);
-                        }
-                        const double disc = bb > 0 ? std::sqrt(dd / bb) : 0.0;
-                        relative[size_t(b) * E + e] = relAudit[e];
-                        accept = accept && relAudit[e] <= target && disc <= .25 * target;
-                    }
-                    if (accept)
-                        break;
-                    if (round >= 3)
-                        throw NoConvergence("Fast-multipole audit did not meet the residual tolerance after 4 "
-                                            "expansion refinements.");
-                    tau = std::max(.1 * tau, 1e-12);
-                    op.prepare(ks[b], tau, s);
-                    fmmSystem_->solve(dAuditFine_.as<double>(), dCorr_.as<double>(), E, .5 * target,
-                                      o.fmm_restart_length, o.fmm_maximum_iterations, s, &timer_, rel, its, inner);
+                const auto download = [&](const double *src) {
+                    std::vector<cplx> v(size_t(E) * N);
+                    cuda(cudaMemcpyAsync(v.data(), src, reals * 8, cudaMemcpyDeviceToHost, s), "audit download");
+                    return v;
+                };
+                const auto massNorm = [&](const std::vector<cplx> &v, uint32_t e) {
+                    double acc = 0;
+                    for (size_t i = 0; i < N; ++i)
+                        acc += space_.lumpedMass[i] * std::norm(v[size_t(e) * N + i]);
+                    return std::sqrt(acc);
+                };
+                // defect correction: x += A_work^-1 r with the working expansions
+                const auto correct = [&](const double *r, double workTolerance) {
+                    op.prepare(ks[b], workTolerance, s);
+                    fmmSystem_->solve(r, dCorr_.as<double>(), E, .5 * target, o.fmm_restart_length,
+                                      o.fmm_maximum_iterations, s, &timer_, rel, its, inner);
                     fmmSystem_->add(xB, dCorr_.as<double>(), reals, s);
                     for (uint32_t e = 0; e < E; ++e)
                         krylov[size_t(b) * E + e] += its[e];
-                }
+                };
+                double tau = expansionTolerance;
+                // Direct Galerkin audit (preferSupportDirectAudit, support_fmm_solve.cu:79-114;
+                // directFar, support_direct_audit.cu:26) where assembling the dense
+                // operator costs less than two expansion operators: the residual of
+                // the exact FP64 dense system, defect-corrected with the working
+                // fast-multipole operator.
+                if (preferDirectAudit(op)) {
+                    TimedScope scope(&timer_, "fmm_direct_audit", s);
+                    double *directA = nullptr, *directB = nullptr;
+                    directAuditFrequency_ = b;
+                    directAuditSystem(geo, ks[b], fluxB, E, directA, directB);
+                    for (uint32_t round = 0;; ++round) {
+                        residualBatch(directA, directB, xB, dMass_.as<double>(), N, 1, E, dAuditFine_.as<double>(),
+                                      dNorms_.as<double>(), s, nullptr);
+                        std::vector<double> norms(2 * size_t(E));
+                        cuda(cudaMemcpyAsync(norms.data(), dNorms_.as<void>(), norms.size() * 8, cudaMemcpyDeviceToHost,
+                                             s),
+                             "direct audit norms");
+                        cuda(cudaStreamSynchronize(s), "CUDA direct audit");
+                        bool accept = true;
+                        for (uint32_t e = 0; e < E; ++e) {
+                            const double r = norms[2 * e + 1] > 0 ? norms[2 * e] / norms[2 * e + 1] : 0.0;
+                            relative[size_t(b) * E + e] = r;
+                            accept = accept && r <= target;
+                        }
+                        if (accept)
+                            break;
+                        if (round >= std::max<uint32_t>(o.maximum_refinement_steps, 3))
+                            throw NoConvergence("Direct Galerkin audit residual exceeds the tolerance; bounded "
+                                                "fast-multipole defect corrections did not converge.");
+                        correct(dAuditFine_.as<double>(), tau);
+                    }
+                    directAudits_ += 1;
+                } else
+                    for (unsigned degree = op.panelDegree();;) {
+                        // Audit against a ten times finer expansion operator and defect-correct
+                        // (SupportFmmLinearSolver::solve / improve, support_fmm_solve.cu:324-343,
+                        // 575-634): accept when the audited residual meets the target and the two
+                        // operators differ on x by at most a quarter of it; otherwise tighten the
+                        // working tolerance and solve for the audited residual's correction.
+                        std::vector<double> relWork, relAudit;
+                        for (uint32_t round = 0;; ++round) {
+                            TimedScope scope(&timer_, "fmm_audit", s);
+                            op.prepare(ks[b], tau, s);
+                            fmmSystem_->residual(rhsB, xB, E, dAuditWork_.as<double>(), relWork, s, &timer_);
+                            op.prepare(ks[b], .1 * tau, s);
+                            fmmSystem_->residual(rhsB, xB, E, dAuditFine_.as<double>(), relAudit, s, &timer_);
+                            const auto rWork = download(dAuditWork_.as<double>());
+                            const auto rAudit = download(dAuditFine_.as<double>());
+                            const auto rhsHost = download(rhsB);
+                            cuda(cudaStreamSynchronize(s), "CUDA fast-multipole audit");
+                            bool accept = true;
+                            for (uint32_t e = 0; e < E; ++e) {
+                                double dd = 0, bb = 0;
+                                for (size_t i = 0; i < N; ++i) {
+                                    const double m = space_.lumpedMass[i];
+                                    dd += m * std::norm(rAudit[size_t(e) * N + i] - rWork[size_t(e) * N + i]);
+                                    bb += m * std::norm(rhsHost[size_t(e) * N + i]);
+                                }
+                                const double disc = bb > 0 ? std::sqrt(dd / bb) : 0.0;
+                                relative[size_t(b) * E + e] = relAudit[e];
+                                accept = accept && relAudit[e] <= target && disc <= .25 * target;
+                            }
+                            if (accept)
+                                break;
+                            if (round >= 3)
+                                throw NoConvergence("Fast-multipole audit did not meet the residual tolerance after 4 "
+                                                    "expansion refinements.");
+                            tau = std::max(.1 * tau, 1e-12);
+                            correct(dAuditFine_.as<double>(), tau);
+                        }
+                        // Far-field panel rule (compareQuadrature, support_fmm_solve.cu:525-560):
+                        // at the verification expansions, the operator and right-hand side with
+                        // the next panel rule must differ from the current ones by at most
+                        // 0.025 of the target, and the next rule's residual meet the target;
+                        // otherwise the rule is promoted (4 -> 6 -> 8 -> 12), the solution
+                        // defect-corrected and both audits repeated.
+                        TimedScope scope(&timer_, "fmm_quadrature_audit", s);
+                        const unsigned next = degree < 6 ? 6 : degree < 8 ? 8 : 12;
+                        op.prepare(ks[b], .1 * tau, s);
+                        fmmSystem_->apply(xB, size_t(N) * 2, E, dAuditWork_.as<double>(), s, &timer_);
+                        const auto axNow = download(dAuditWork_.as<double>());
+                        const auto bNow = download(rhsB);
+                        op.setPanelDegree(next);
+                        buildRhs(dAuditB_.as<double>());
+                        fmmSystem_->apply(xB, size_t(N) * 2, E, dAuditWork_.as<double>(), s, &timer_);
+                        const auto axNext = download(dAuditWork_.as<double>());
+                        const auto bNext = download(dAuditB_.as<double>());
+                        cuda(cudaStreamSynchronize(s), "CUDA quadrature audit");
+                        bool accept = true;
+                        for (uint32_t e = 0; e < E; ++e) {
+                            std::vector<cplx> db(size_t(E) * N), da(size_t(E) * N), rn(size_t(E) * N);
+                            for (size_t i = size_t(e) * N; i < size_t(e + 1) * N; ++i) {
+                                db[i] = bNext[i] - bNow[i];
+                                da[i] = axNext[i] - axNow[i];
+                                rn[i] = bNext[i] - axNext[i];
+                            }
+                            const double bn = massNorm(bNext, e);
+                            const double disc = bn > 0 ? (massNorm(db, e) + massNorm(da, e)) / bn : 0.0;
+                            const double res = bn > 0 ? massNorm(rn, e) / bn : 0.0;
+                            accept = accept && disc <= .025 * target && res <= target;
+                        }
+                        if (accept) {
+                            op.setPanelDegree(4);  // the next frequency starts from the base rule again
+                            break;
+                        }
+                        if (degree == 12)
+                            throw NoConvergence("BEM endpoint quadrature 12/14 did not converge: the fast-multipole "
+                                                "far-field panel rules disagree beyond 0.025*residualTolerance; "
+                                                "refine the mesh.");
+                        // promoted: the next rule's right-hand side, then a defect correction
+                        degree = next;
+                        ++quadraturePromotions_;
+                        cuda(cudaMemcpyAsync(rhsB, dAuditB_.as<void>(), reals * 8, cudaMemcpyDeviceToDevice, s),
+                             "promoted rhs");
+                        fmmSystem_->residual(rhsB, xB, E, dAuditFine_.as<double>(), relAudit, s, &timer_);
+                        correct(dAuditFine_.as<double>(), tau);
+                    }
             }
             cuda(cudaEventRecord(ev.solved, s), "phase event");
             cuda(cudaStreamSynchronize(s), "CUDA fast-multipole solve");
@@ -1207,6 +1305,8 @@ void Session::ensureFmmWorkspace(const hs_numerics &o, uint32_t E, uint32_t O, d
     dNearWork_.ensure(nearFieldWorkspaceBytes(op.nearPanelCol().size(), op.nearPanelPairs().size()));
     dAuditWork_.ensure(E * N * 16);
     dAuditFine_.ensure(E * N * 16);
+    dNearRhs_.ensure(E * N * 16);
+    dAuditB_.ensure(E * N * 16);
     dRhs_.ensure(E * N * 16);
     dX_.ensure(E * N * 16);
     dCorr_.ensure(E * N * 16);
@@ -1243,6 +1343,58 @@ FmmOperator &Session::fmmOperator(const hs_numerics &o, double tuneK, double tun
         fmmSettings_ = st;
     }
     return *fmm_;
+}
+
+// Whether the direct Galerkin audit is cheaper than two expansion operators
+// (preferSupportDirectAudit, support_fmm_solve.cu:79-114, restated): dense
+// regular work T^2 (9 + q^2 (13 + 1/r)) with q the panel rule's points and r
+// the FP32:FP64 throughput ratio, against, per far level, the pairs times the
+// rotation-coaxial-rotation work (or the plane-wave samples) plus the O(n^4)
+// coaxial preparation per distance class; at most 20 000 panels.
+bool Session::preferDirectAudit(const FmmOperator &op) const {
+    const size_t T = space_.panels.size(), N = space_.vertices.size();
+    if (fmmAuditMode_ == 2)
+        return true;
+    if (!T || T > 20000 || op.levels().empty() || fmmAuditMode_ == 1)
+        return false;
+    size_t freeBytes = 0, totalBytes = 0;  // the dense system must fit beside the fast-multipole state
+    if (cudaMemGetInfo(&freeBytes, &totalBytes) != cudaSuccess ||
+        recordBytes(uint32_t(T), false) + 2 * N * N * 16 > freeBytes / 2)
+        return false;
+    const long double q = 6, ratio = 2;  // degree-4 Dunavant rule; B200 FP32 : FP64
+    const long double direct = (long double)T * T * (9.L + q * q * (13.L + 1.L / ratio));
+    const FmmTree &tree = op.tree();
+    std::vector<long double> pairs(tree.levels.size(), 0);
+    for (const auto *list : {&tree.ppFar, &tree.pfFar})
+        for (const auto &lk : *list)
+            pairs[tree.nodes[lk.target].level] += 1;
+    long double multipole = 0;
+    for (const auto &lv : op.levels()) {
+        const long double p = lv.order, n = p + 1;
+        if (lv.planeWave)
+            multipole += pairs[lv.level] * 2.L * (1.5L * p + 1) * (3 * p + 2);
+        else {
+            const long double rotation = n * (4 * p * p + 8 * p + 3) / 3, axial = n * n + p * n * (2 * p + 1) / 3;
+            multipole += pairs[lv.level] * (2 * rotation + axial) + n * n * n * n;
+        }
+    }
+    return direct <= 2 * multipole;
+}
+
+// The exact FP64 dense system of one frequency for the direct audit: matrix
+// into dA_, right-hand side into dAuditB_ (the dense assembly of the plain form).
+void Session::directAuditSystem(const AssemblyGeometry &geo, double k, const double *flux, uint32_t E, double *&A,
+                                double *&b) {
+    (void)k;
+    const uint32_t T = geo.T;
+    ensureWorkspace(1, E, 0, false, 2);
+    AssemblyWorkspace ws{dRecords_.as<void>(), dColumns_.as<void>(), dPanelRhs_.as<double>(), dBins_.as<uint2>(),
+                         dBinCounts_.as<uint32_t>(), size_t(T) * (T - 1) / 2,
+                         T > kExactBinsT ? dBinOffsets_.as<uint64_t>() : nullptr};
+    assembleBatch(geo, dKs_.as<double>() + directAuditFrequency_, dGauss_.as<double>(), flux, E, 1, ws,
+                  dA_.as<double>(), dAuditB_.as<double>(), dError_.as<int>(), stream(), nullptr, false);
+    A = dA_.as<double>();
+    b = dAuditB_.as<double>();
 }
 
 // The mixed form's inner operator: the same tree and partition as the FP64

@@ -160,6 +160,18 @@ private:
     std::unique_ptr<FmmOperator> fmm_, fmmInner_;
     FmmTreeSettings fmmInnerSettings_{};
     FmmOperator &fmmInnerOperator(const hs_numerics &numerics);
+    bool preferDirectAudit(const FmmOperator &op) const;
+    void directAuditSystem(const AssemblyGeometry &geo, double k, const double *flux, uint32_t E, double *&A,
+                           double *&b);
+    uint32_t directAuditFrequency_ = 0;
+    DeviceBuffer dNearRhs_, dAuditB_;
+  public:
+    // fast-multipole audit evidence of the session: direct audits, panel-rule promotions
+    uint64_t directAudits_ = 0, quadraturePromotions_ = 0;
+    // 0: the reference's policy (direct audit where cheaper), 1: expansion and
+    // panel-rule audits only, 2: direct audit always
+    uint32_t fmmAuditMode_ = 0;
+  private:
     std::unique_ptr<FmmSystem> fmmSystem_;
     const FmmOperator *fmmSystemOp_ = nullptr;
     uint32_t fmmBlockWidth_ = 0;

@@ -285,6 +285,21 @@ hs_status hs_bem_debug_fmm_selftest(double *error);
  * rotational. Applies to the FP64 operator; the mixed form's FP32 inner
  * operator stays rotational. */
 hs_status hs_bem_session_set_plane_wave_threshold(hs_bem_session *session, double threshold);
+/* Acceptance audit of fast-multipole solves (SupportFmmLinearSolver::solve,
+ * support_fmm_solve.cu:324-634). mode 0 (default), the reference's policy:
+ * where assembling the dense system costs less than two expansion operators
+ * (preferSupportDirectAudit, :79-114; at most 20 000 panels and within half the
+ * free memory) the residual is that of the exact FP64 dense system, with
+ * fast-multipole defect corrections (directFar, support_direct_audit.cu:26);
+ * otherwise a ten times finer expansion operator audits the working one and
+ * the far-field panel rule is compared with the next one and promoted
+ * 4 -> 6 -> 8 -> 12 until they agree to 0.025 of the residual target
+ * (compareQuadrature). mode 1: always the expansion and panel-rule audits;
+ * mode 2: always the direct audit. The counts report the session's direct
+ * audits and panel-rule promotions so far. */
+hs_status hs_bem_session_set_fmm_audit(hs_bem_session *session, uint32_t mode);
+hs_status hs_bem_session_fmm_audit_counts(const hs_bem_session *session, uint64_t *direct_audits,
+                                          uint64_t *quadrature_promotions);
 /* The support tree of the fast-multipole form (host only): the mesh centred on
  * vertex 0 like a session; sizes = {nodes, levels, pressure-pressure near,
  * pressure-pressure far, pressure-flux near, pressure-flux far} and links the

@@ -263,3 +263,48 @@ def test_plane_wave_levels_in_a_solve():
         a.boundary.pressure_trace)
     print("plane-wave solve error", err, "iterations", b.iterations)
     assert b.boundary_residual <= 1e-6 and err < 1e-5
+
+
+def _throat_request(freqs, acc, tol, obs=((0.0, 0.0, 1.0), (0.6, 0.0, 0.3))):
+    return hs.BemRequest(frequencies=freqs, observers=list(obs),
+                         excitations=[hs.BemExcitation("throat", [hs.FaceVelocity(meshes.HORN_THROAT, 1.0)])],
+                         numerics=hs.BemNumerics(precision="fp64", acceleration=acc, relative_residual_tolerance=tol))
+
+
+def test_direct_galerkin_audit():
+    """The direct audit (directFar, support_direct_audit.cu:26): the accepted
+    fast-multipole solution meets the residual target of the exact dense FP64
+    system, which the reported residual is."""
+    mesh = meshes.exponential_horn(h=0.0128, seed=5)
+    with hs.CudaBemSolver(mesh) as solver:
+        dense = solver.solve(_throat_request([2500.0], "dense", 1e-7))
+        solver.set_fmm_audit("direct")
+        fmm = solver.solve(_throat_request([2500.0], "fast_multipole", 1e-6))
+        direct, _ = solver.fmm_audit_counts()
+    assert direct >= 1
+    a, b = dense.frequencies[0].excitations[0], fmm.frequencies[0].excitations[0]
+    assert b.boundary_residual <= 1e-6
+    err = np.linalg.norm(b.boundary.pressure_trace - a.boundary.pressure_trace) / np.linalg.norm(
+        a.boundary.pressure_trace)
+    print("direct audit error", err, "residual", b.boundary_residual)
+    assert err < 1e-5
+
+
+def test_far_field_panel_rule_promotion():
+    """The expansion audit with the far-field panel-rule comparison
+    (compareQuadrature, support_fmm_solve.cu:525-560): at a tight target the
+    degree-4 far-field rule is promoted, and the result approaches the dense
+    solution (whose regular pairs use the plan's higher rules)."""
+    mesh = meshes.exponential_horn(h=0.0128, seed=5)
+    with hs.CudaBemSolver(mesh) as solver:
+        dense = solver.solve(_throat_request([6000.0], "dense", 1e-7))
+        solver.set_fmm_audit("expansion")
+        fmm = solver.solve(_throat_request([6000.0], "fast_multipole", 1e-7))
+        _, promotions = solver.fmm_audit_counts()
+    a, b = dense.frequencies[0].excitations[0], fmm.frequencies[0].excitations[0]
+    trace = np.linalg.norm(b.boundary.pressure_trace - a.boundary.pressure_trace) / np.linalg.norm(
+        a.boundary.pressure_trace)
+    field = np.linalg.norm(b.observer_pressure - a.observer_pressure) / np.linalg.norm(a.observer_pressure)
+    print("promotions", promotions, "trace", trace, "field", field, "residual", b.boundary_residual)
+    assert promotions >= 1
+    assert b.boundary_residual <= 1e-7 and trace < 2e-6 and field < 5e-6
