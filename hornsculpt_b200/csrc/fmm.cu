@@ -1476,14 +1476,14 @@ FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : 
         uploadVec(h.linkSource, src, s);
         uploadVec(h.linkClass, cl, s);
     }
-    setPanelDegree(4);
+    setPanelDegree(4, nullptr);
     fmmCheck(cudaDeviceSynchronize(), "setup");
     I.far.ensure(3 * size_t(I.T) * 16);
 }
 
 FmmOperator::~FmmOperator() = default;
 
-void FmmOperator::setPanelDegree(unsigned degree) {
+void FmmOperator::setPanelDegree(unsigned degree, cudaStream_t stream) {
     Impl &I = *impl_;
     const std::vector<TriPoint> rule = triangleRule(degree);
     double ws = 0;
@@ -1496,8 +1496,9 @@ void FmmOperator::setPanelDegree(unsigned degree) {
         hr[4 * q + 2] = rule[q].b[2];
         hr[4 * q + 3] = rule[q].w / ws;
     }
-    uploadVec(I.rule, hr, nullptr);
-    fmmCheck(cudaStreamSynchronize(nullptr), "rule upload");
+    // ordered after the work already queued on `stream` that reads the old rule
+    uploadVec(I.rule, hr, stream);
+    fmmCheck(cudaStreamSynchronize(stream), "rule upload");
     I.rulePts = int(rule.size());
     I.panelDegree = degree;
     I.dropGraphs();

@@ -70,7 +70,7 @@ class FmmOperator {
     void setHfThreshold(double threshold);
     // Far-field panel rule (Dunavant degree 4 by default; the audit promotes it
     // 4 -> 6 -> 8 -> 12 like the reference's compareQuadrature).
-    void setPanelDegree(unsigned degree);
+    void setPanelDegree(unsigned degree, cudaStream_t stream);
     unsigned panelDegree() const;
 
   private:

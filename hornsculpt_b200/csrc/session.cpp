@@ -699,6 +699,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             FmmOperator *inner = mixed ? &fmmInnerOperator(o) : nullptr;
             for (uint32_t b = 0; b < B; ++b) {
                 checkCancel();
+                if (op.panelDegree() != 4)  // a promotion of an earlier, failed audit
+                    op.setPanelDegree(4, s);
                 op.prepare(ks[b], expansionTolerance, s);
                 if (inner)
                     inner->prepare(ks[b], std::max(expansionTolerance, 1e-5), s);
@@ -832,7 +834,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                         fmmSystem_->apply(xB, size_t(N) * 2, E, dAuditWork_.as<double>(), s, &timer_);
                         const auto axNow = download(dAuditWork_.as<double>());
                         const auto bNow = download(rhsB);
-                        op.setPanelDegree(next);
+                        op.setPanelDegree(next, s);
                         buildRhs(dAuditB_.as<double>());
                         fmmSystem_->apply(xB, size_t(N) * 2, E, dAuditWork_.as<double>(), s, &timer_);
                         const auto axNext = download(dAuditWork_.as<double>());
@@ -852,7 +854,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                             accept = accept && disc <= .025 * target && res <= target;
                         }
                         if (accept) {
-                            op.setPanelDegree(4);  // the next frequency starts from the base rule again
+                            op.setPanelDegree(4, s);  // the next frequency starts from the base rule again
                             break;
                         }
                         if (degree == 12)
