@@ -285,6 +285,7 @@ void Server::worker(int index) {
             }
         }
         const Job &head = *group.front();
+        std::map<double, FrequencyResult> solved;  // results of the call so far, by frequency
         std::unique_ptr<Result> merged;
         std::exception_ptr error;
         std::vector<double> freqs;
@@ -319,8 +320,64 @@ void Server::worker(int index) {
             session->setMemoryBudget(footprint > resident ? footprint - resident : footprint);
             session->setStream(stream);
             const hs_request r = head.request.view(freqs, raster);
+            // Continuous batching. With the server's fixed planning frequency every
+            // request on a mesh shares one interaction plan, so while this call runs,
+            // compatible requests on the mesh that arrive join its next frequency
+            // batch (ahead of the call's remaining frequencies), and every request is
+            // completed as soon as its last frequency is solved, not when the call ends.
+            SolveHooks hooks;
+            std::set<double> scheduled(unique);
+            if (options_.planning_frequency > 0) {
+                hooks.more = [&]() {
+                    std::vector<double> extra;
+                    std::lock_guard<std::mutex> lock(mutex_);
+                    if (stop_)
+                        return extra;
+                    const auto now = Clock::now();
+                    for (auto it = queue_.begin(); it != queue_.end();) {
+                        const auto job = *it;
+                        if (job->meshKey != head.meshKey || !job->request.compatible(head.request)) {
+                            ++it;
+                            continue;
+                        }
+                        job->start = now;
+                        job->footprint = footprint;
+                        for (double f : job->request.frequencies)
+                            if (scheduled.insert(f).second)
+                                extra.push_back(f);
+                        group.push_back(job);
+                        it = queue_.erase(it);
+                    }
+                    return extra;
+                };
+            }
+            hooks.done = [&](const FrequencyResult &fr) {
+                solved.emplace(fr.frequency, fr);
+                std::lock_guard<std::mutex> lock(mutex_);
+                bool any = false;
+                for (auto &job : group) {
+                    if (job->done || !std::all_of(job->request.frequencies.begin(), job->request.frequencies.end(),
+                                                  [&](double f) { return solved.count(f) != 0; }))
+                        continue;
+                    auto result = std::make_unique<Result>();
+                    result->T = head.mesh->faces.size();
+                    result->N = head.mesh->vertices.size();
+                    result->O = job->request.base.observer_count;
+                    result->E = job->request.base.excitation_count;
+                    result->peakDeviceBytes = session->residentBytes();
+                    for (double f : job->request.frequencies)
+                        result->frequencies.push_back(solved.at(f));
+                    job->result = std::move(result);
+                    job->finish = Clock::now();
+                    job->batched = uint32_t(group.size());
+                    job->done = true;
+                    any = true;
+                }
+                if (any)
+                    done_.notify_all();
+            };
             std::lock_guard<std::mutex> solveLock(session->mutex);
-            merged = session->solve(r, nullptr, nullptr, nullptr);
+            merged = session->solve(r, nullptr, nullptr, nullptr, &hooks);
         } catch (...) {
             error = std::current_exception();
         }
@@ -328,7 +385,10 @@ void Server::worker(int index) {
             std::lock_guard<std::mutex> lock(mutex_);
             const auto now = Clock::now();
             for (auto &job : group) {
+                if (job->done)  // completed early by the continuous-batching hook
+                    continue;
                 job->finish = now;
+                job->batched = uint32_t(group.size());
                 if (error) {
                     job->error = error;
                 } else {
@@ -338,10 +398,10 @@ void Server::worker(int index) {
                     result->O = merged->O;
                     result->E = merged->E;
                     result->peakDeviceBytes = merged->peakDeviceBytes;
-                    for (double f : job->request.frequencies) {
-                        const size_t at = size_t(std::lower_bound(freqs.begin(), freqs.end(), f) - freqs.begin());
-                        result->frequencies.push_back(merged->frequencies[at]);
-                    }
+                    for (const auto &fr : merged->frequencies)
+                        solved.emplace(fr.frequency, fr);
+                    for (double f : job->request.frequencies)
+                        result->frequencies.push_back(solved.at(f));
                     job->result = std::move(result);
                 }
                 job->done = true;

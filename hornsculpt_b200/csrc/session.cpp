@@ -521,7 +521,7 @@ void Session::checkDeviceError(const char *where) {
 }
 
 std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32_t *cancel, hs_progress_fn progress,
-                                       void *user) {
+                                       void *user, const SolveHooks *hooks) {
     const auto checkCancel = [&]() {
         if (cancel && *cancel)
             throw Cancelled();
@@ -629,9 +629,20 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     // Device span of the whole sweep (profiling on): from the first upload to
     // the last result download, host-side control included.
     const size_t span = timer_.start("solve_span", s);
-    for (uint32_t f0 = 0; f0 < F; f0 += Bmax) {
+    // frequencies in solve order: the request's, plus those a serving hook adds
+    std::vector<double> freqList(r.frequencies, r.frequencies + F);
+    for (uint32_t f0 = 0, B = 0; f0 < freqList.size(); f0 += B) {
         checkCancel();
-        const uint32_t B = std::min(Bmax, F - f0);
+        if (hooks && hooks->more) {
+            const std::vector<double> extra = hooks->more();
+            for (double f : extra)
+                if (!std::isfinite(f) || f <= 0 || 2 * M_PI * f / r.sound_speed > maxK * (1 + 1e-12))
+                    throw InvalidArgument("A frequency joining a running solve lies outside its interaction plan.");
+            freqList.insert(freqList.begin() + f0, extra.begin(), extra.end());
+            result->frequencies.insert(result->frequencies.begin() + f0, extra.size(), FrequencyResult{});
+        }
+        const uint32_t Ftotal = uint32_t(freqList.size());
+        B = std::min<uint32_t>(Bmax, Ftotal - f0);
         // Phase times come from events on the session stream; the host waits for the
         // device only where it needs data (residual norms, GMRES estimates, fields).
         PhaseEvents &ev = phaseEvents();
@@ -639,7 +650,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         std::vector<double> ks(B);
         std::vector<cplx> flux(size_t(B) * E * T);
         for (uint32_t b = 0; b < B; ++b) {
-            const double omega = 2 * M_PI * r.frequencies[f0 + b];
+            const double omega = 2 * M_PI * freqList[f0 + b];
             ks[b] = omega / r.sound_speed;
             for (size_t i = 0; i < size_t(E) * T; ++i)
                 flux[size_t(b) * E * T + i] = cplx(0, -r.density * omega) * velocity[i];
@@ -935,7 +946,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 if (need && steps[b] >= maxSteps) {
                     std::ostringstream msg;
                     msg << std::setprecision(9) << "Burton-Miller residual " << largest << " exceeds tolerance "
-                        << target << " at " << r.frequencies[f0 + b] << " Hz after " << steps[b]
+                        << target << " at " << freqList[f0 + b] << " Hz after " << steps[b]
                         << " refinement steps.";
                     throw NoConvergence(msg.str());
                 }
@@ -979,7 +990,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         if (O && nonzero) {
             if (progress)
                 for (uint32_t b = 0; b < B; ++b) {
-                    hs_progress p{f0 + b, F, r.frequencies[f0 + b], HS_PHASE_FIELD_EVALUATION};
+                    hs_progress p{f0 + b, Ftotal, freqList[f0 + b], HS_PHASE_FIELD_EVALUATION};
                     progress(&p, user);
                 }
             for (uint32_t b = 0; b < B; ++b) {
@@ -1060,8 +1071,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         cuda(cudaStreamSynchronize(s), "CUDA synchronization");
         for (uint32_t b = 0; b < B; ++b) {
             FrequencyResult &fr = result->frequencies[f0 + b];
-            const double omega = 2 * M_PI * r.frequencies[f0 + b];
-            fr.frequency = r.frequencies[f0 + b];
+            const double omega = 2 * M_PI * freqList[f0 + b];
+            fr.frequency = freqList[f0 + b];
             fr.info.frequency = fr.frequency;
             fr.info.assembly_ms = assemblyMs / B;
             fr.info.factorization_ms = factorMs / B;
@@ -1113,9 +1124,11 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 }
             }
             if (progress) {
-                hs_progress p{f0 + b + 1, F, fr.frequency, HS_PHASE_FREQUENCY_COMPLETE};
+                hs_progress p{f0 + b + 1, Ftotal, fr.frequency, HS_PHASE_FREQUENCY_COMPLETE};
                 progress(&p, user);
             }
+            if (hooks && hooks->done)
+                hooks->done(fr);
         }
     }
     timer_.stop(span, s);

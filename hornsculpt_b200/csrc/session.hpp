@@ -10,6 +10,7 @@
 #include "planner.hpp"
 
 #include <complex>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -52,13 +53,22 @@ struct Result {
     std::vector<FrequencyResult> frequencies;
 };
 
+// Continuous batching hooks of a solve (serving): before each frequency batch
+// `more` may hand in further frequencies (solved next, ahead of the remaining
+// ones; they must lie within the solve's interaction plan), and `done` sees
+// every frequency result as soon as its batch completes.
+struct SolveHooks {
+    std::function<std::vector<double>()> more;
+    std::function<void(const FrequencyResult &)> done;
+};
+
 class Session {
   public:
     Session(const MeshInput &mesh, uint32_t residency);
     ~Session();
     void setStream(cudaStream_t stream);
     std::unique_ptr<Result> solve(const hs_request &request, const volatile int32_t *cancel, hs_progress_fn progress,
-                                  void *user);
+                                  void *user, const SolveHooks *hooks = nullptr);
     const Plan &plan(const hs_numerics &numerics, double maxK, const volatile int32_t *cancel);
     void debugAssemble(const hs_numerics &numerics, double planK, double k, const double *flux, double *matrix,
                        double *rhs);

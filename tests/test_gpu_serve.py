@@ -128,3 +128,32 @@ def test_fast_multipole_request_is_served():
     b = direct.frequencies[0].excitations[0].boundary.pressure_trace
     assert np.linalg.norm(a - b) <= 1e-6 * np.linalg.norm(b)
     assert served.frequencies[0].excitations[0].iterations > 0 and timing.footprint_bytes > 0
+
+
+def test_continuous_batching_joins_a_running_call():
+    """A request that arrives while another request on the same mesh is being
+    solved joins the running call at its next frequency batch (ahead of the
+    call's remaining frequencies) and is completed as soon as its own
+    frequencies are solved, well before the long call ends. Its result equals
+    its solve alone, bit for bit."""
+    import time
+    sphere = meshes.octahedral_sphere(3)
+    long_freqs = [float(f) for f in np.geomspace(150.0, 1900.0, 32)]
+    late = _request([333.0, 1234.0])
+    with hs.BemServer(hs.ServeOptions(workers=1, planning_frequency=PLAN_HZ)) as server:
+        alone, _ = server.wait(server.submit(sphere, late))
+    options = hs.ServeOptions(workers=1, planning_frequency=PLAN_HZ, max_batch_frequencies=2)
+    with hs.BemServer(options) as server:
+        t_long = time.perf_counter()
+        long_ticket = server.submit(sphere, _request(long_freqs))
+        time.sleep(0.05)
+        t_late = time.perf_counter()
+        late_ticket = server.submit(sphere, late)
+        late_result, late_timing = server.wait(late_ticket)
+        long_result, long_timing = server.wait(long_ticket)
+    _same(alone, late_result)
+    assert late_timing.batched_requests >= 2 and long_timing.batched_requests >= 2
+    late_finish = t_late + late_timing.latency_ms / 1e3
+    long_finish = t_long + long_timing.latency_ms / 1e3
+    assert late_finish < long_finish - 0.25 * long_timing.run_ms / 1e3
+    assert [f.frequency for f in long_result.frequencies] == long_freqs
