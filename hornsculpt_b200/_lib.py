@@ -73,6 +73,8 @@ class hs_field_settings(C.Structure):
 
 
 PROGRESS_FN = C.CFUNCTYPE(None, C.POINTER(hs_progress), C.c_void_p)
+NETWORK_FN = C.CFUNCTYPE(C.c_int, C.c_double, C.c_size_t, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                         C.POINTER(C.c_double), C.c_void_p)
 _P = C.c_void_p
 _lib = None
 
@@ -81,7 +83,7 @@ def declared_symbols() -> list[str]:
     """Function names declared by include/hs_bem.h."""
     text = HEADER.read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(hs_[a-z_]+)\s*\(", text)) - {"hs_progress_fn"})
+    return sorted(set(re.findall(r"\b(hs_[a-z_]+)\s*\(", text)) - {"hs_progress_fn", "hs_status"})
 
 
 def load():
@@ -119,6 +121,8 @@ def load():
         "hs_bem_session_profile": (C.c_int, [_P, C.c_char_p, C.c_size_t, _P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
         "hs_bem_session_work": (C.c_int, [_P, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
         "hs_bem_session_set_graphs": (C.c_int, [_P, C.c_int32]),
+        "hs_bem_solve_coupled": (C.c_int, [_P, C.POINTER(hs_request), NETWORK_FN, _P, _P, C.POINTER(_P)]),
+        "hs_result_coupling": (C.c_int, [_P, C.c_size_t, _P, _P, _P, C.POINTER(C.c_size_t)]),
         "hs_autotune_set_enabled": (C.c_int, [C.c_int32]),
         "hs_autotune_clear": (C.c_int, []),
         "hs_autotune_report": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]),

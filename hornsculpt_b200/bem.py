@@ -298,6 +298,53 @@ class CudaBemSolver:
             self._lib.hs_result_free(out)
             del keep
 
+    def solve_coupled(self, request: BemRequest, network: Callable, stop: StopToken | None = None):
+        """LEM-coupled solve in the library (hs_bem_solve_coupled; CudaBemSolver::solve
+        with a coupling, cuda_solver.cu:1584-1667). request.excitations are the unit-flow
+        port basis (coupling.make_coupling_basis); network(frequency, Z) returns the
+        port flows and pressures (two sequences of complex, one per port). Returns the
+        BemResult (one excitation per frequency: the coupled field, named "LEM") and per
+        frequency (Z, flows, pressures)."""
+        req, keep = self._c_request(request)
+        out = C.c_void_p()
+        failure = []
+
+        def bridge(frequency, ports, z, q, p, _user):
+            try:
+                Z = np.ctypeslib.as_array(z, (2 * ports * ports,)).view(np.complex128).reshape(ports, ports)
+                flows, pressures = network(frequency, Z.copy())
+                flows, pressures = np.asarray(flows, np.complex128), np.asarray(pressures, np.complex128)
+                if flows.shape != (ports,) or pressures.shape != (ports,):
+                    raise ValueError("LEM result port count does not match its BEM basis.")
+                np.ctypeslib.as_array(q, (2 * ports,))[:] = flows.view(np.float64)
+                np.ctypeslib.as_array(p, (2 * ports,))[:] = pressures.view(np.float64)
+                return _lib.HS_OK
+            except Exception as e:  # reported after the call
+                failure.append(e)
+                return _lib.HS_E_INVALID
+        cb = _lib.NETWORK_FN(bridge)
+        flag = C.byref(stop._flag) if stop is not None else None
+        status = self._lib.hs_bem_solve_coupled(self._handle, C.byref(req), cb, None, flag, C.byref(out))
+        if failure:
+            raise failure[0]
+        _lib.check(status)
+        try:
+            coupled = dataclasses.replace(request, excitations=[BemExcitation("LEM", [])])
+            result = self._read(out, coupled)
+            ports = C.c_size_t()
+            extra = []
+            for f in range(len(result.frequencies)):
+                _lib.check(self._lib.hs_result_coupling(out, f, None, None, None, C.byref(ports)))
+                n = ports.value
+                Z, q, pr = np.zeros(2 * n * n), np.zeros(2 * n), np.zeros(2 * n)
+                _lib.check(self._lib.hs_result_coupling(out, f, Z.ctypes.data, q.ctypes.data, pr.ctypes.data,
+                                                        C.byref(ports)))
+                extra.append((_cplx(Z).reshape(n, n), _cplx(q), _cplx(pr)))
+            return result, extra
+        finally:
+            self._lib.hs_result_free(out)
+            del keep
+
     def pressure_field(self, frequency: float, solution: BemExcitationResult, points,
                        settings: PressureFieldSettings = PressureFieldSettings(),
                        medium: AcousticMedium = AcousticMedium()) -> list:

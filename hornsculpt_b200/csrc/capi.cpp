@@ -5,6 +5,7 @@
 #include "serve.hpp"
 #include "session.hpp"
 
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -249,6 +250,45 @@ hs_status hs_bem_session_set_profiling(hs_bem_session *s, int32_t enabled) {
         s->impl->timer().enable(enabled != 0);
         std::fill(s->impl->work.begin(), s->impl->work.end(), 0);
     });
+}
+
+hs_status hs_bem_solve_coupled(hs_bem_session *s, const hs_request *request, hs_network_fn network, void *user,
+                               const volatile int32_t *cancel, hs_result **out) {
+    if (!s || !request || !network || !out)
+        return fail(HS_E_INVALID, "Coupled solve: session, request, network and output must be non-null.");
+    *out = nullptr;
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        const CouplingNetwork bridge = [&](double frequency, const std::vector<cplx> &Z, std::vector<cplx> &Q,
+                                           std::vector<cplx> &P) {
+            const size_t ports = size_t(std::sqrt(double(Z.size())) + 0.5);
+            Q.assign(ports, 0.0);
+            P.assign(ports, 0.0);
+            const hs_status st = network(frequency, ports, reinterpret_cast<const double *>(Z.data()),
+                                         reinterpret_cast<double *>(Q.data()), reinterpret_cast<double *>(P.data()),
+                                         user);
+            if (st != HS_OK)
+                throw InvalidArgument("The lumped network failed for the coupled BEM load.");
+        };
+        auto result = s->impl->solve(*request, cancel, nullptr, nullptr, nullptr, &bridge);
+        *out = new hs_result{std::move(result)};
+    });
+}
+
+hs_status hs_result_coupling(const hs_result *r, size_t f, double *impedance, double *volume_velocity,
+                             double *pressure, size_t *ports) {
+    if (!r || !r->impl || f >= r->impl->frequencies.size())
+        return fail(HS_E_INVALID, "Result index out of range.");
+    const FrequencyResult &fr = r->impl->frequencies[f];
+    if (ports)
+        *ports = fr.portFlow.size();
+    if (impedance && !fr.portImpedance.empty())
+        std::memcpy(impedance, fr.portImpedance.data(), fr.portImpedance.size() * sizeof(cplx));
+    if (volume_velocity && !fr.portFlow.empty())
+        std::memcpy(volume_velocity, fr.portFlow.data(), fr.portFlow.size() * sizeof(cplx));
+    if (pressure && !fr.portPressure.empty())
+        std::memcpy(pressure, fr.portPressure.data(), fr.portPressure.size() * sizeof(cplx));
+    return HS_OK;
 }
 
 hs_status hs_bem_session_set_graphs(hs_bem_session *s, int32_t enabled) {

@@ -521,7 +521,7 @@ void Session::checkDeviceError(const char *where) {
 }
 
 std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32_t *cancel, hs_progress_fn progress,
-                                       void *user, const SolveHooks *hooks) {
+                                       void *user, const SolveHooks *hooks, const CouplingNetwork *coupling) {
     const auto checkCancel = [&]() {
         if (cancel && *cancel)
             throw Cancelled();
@@ -589,6 +589,31 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 velocity[size_t(e) * T + t] = it->second;
         }
     }
+    // LEM coupling (cuda_solver.cu:1584-1667): the excitations are the unit-flow
+    // basis, one per port; panel -> port and its velocity per unit flow.
+    std::vector<int32_t> panelPort;
+    std::vector<double> panelUnitVelocity;
+    if (coupling) {
+        if (o.acceleration == HS_FAST_MULTIPOLE)
+            throw Unsupported("LEM-coupled fast-multipole solves are not part of this build; use a dense form.");
+        panelPort.assign(T, -1);
+        panelUnitVelocity.assign(T, 0.0);
+        std::map<uint32_t, std::pair<uint32_t, double>> facePort;
+        for (uint32_t e = 0; e < E; ++e)
+            for (size_t i = r.excitation_face_offsets[e]; i < r.excitation_face_offsets[e + 1]; ++i) {
+                const double vr = r.excitation_velocities[2 * i], vi = r.excitation_velocities[2 * i + 1];
+                if (vi != 0 || !(vr > 0) || !std::isfinite(vr) ||
+                    !facePort.emplace(r.excitation_face_ids[i], std::make_pair(e, vr)).second)
+                    throw InvalidArgument("Coupled ports need positive real unit-flow velocities and disjoint faces.");
+            }
+        for (uint32_t t = 0; t < T; ++t) {
+            const auto it = facePort.find(space_.panels[t].face);
+            if (it != facePort.end()) {
+                panelPort[t] = int32_t(it->second.first);
+                panelUnitVelocity[t] = it->second.second;
+            }
+        }
+    }
     if (progress) {
         hs_progress p{0, F, r.frequencies[0], HS_PHASE_PREPARING};
         progress(&p, user);
@@ -614,7 +639,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     result->T = T;
     result->N = N;
     result->O = O;
-    result->E = E;
+    result->E = coupling ? 1 : E;
     result->frequencies.resize(F);
     AssemblyGeometry geo{dPanels_.as<DPanel>(), dBounds_.as<Bounds>(), dPairCode_.as<uint8_t>(),
                          dTouching_.as<TouchingJob>(), dNearPairs_.as<NearPairJob>(), patches_,
@@ -901,6 +926,10 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
         const uint32_t maxSteps = mixed ? std::max<uint32_t>(o.maximum_refinement_steps, 10) : o.maximum_refinement_steps;
         const auto residualStart = Clock::now();
         std::vector<double> norms(2 * size_t(B) * E);
+        bool statusChecked = false;
+        for (int pass = 0; pass < (coupling ? 2 : 1); ++pass) {
+        if (pass == 1)  // the coupled field: superposed basis, then its own refinement
+            coupleBatch(*coupling, freqList, f0, B, E, r.density, panelPort, panelUnitVelocity, result->frequencies);
         for (;;) {
             checkCancel();
             residualBatch(dA_.as<double>(), dRhs_.as<double>(), dX_.as<double>(), dMass_.as<double>(), N, B, E,
@@ -913,7 +942,8 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                 cuda(cudaEventElapsedTime(&ms, ev.refine0, ev.refine1), "phase time");
                 triMs += ms;
                 refining = false;
-            } else {  // first pass: assembly and factorisation status, phase times
+            } else if (!statusChecked) {  // first residual: assembly and factorisation status, phase times
+                statusChecked = true;
                 checkDeviceError("CUDA Galerkin assembly");
                 int info = 0;
                 cuda(cudaMemcpy(&info, dInfo_.as<int>(), sizeof(int), cudaMemcpyDeviceToHost), "LU info");
@@ -979,6 +1009,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             }
             cuda(cudaEventRecord(ev.refine1, s), "phase event");
             refining = true;
+        }
         }
         residualMs = msSince(residualStart);
         }
@@ -1082,9 +1113,18 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
             fr.info.field_ms = fieldMs / B;
             fr.info.interaction_plan_ms = (f0 + b == 0) ? planMs : 0;
             fr.info.interaction_plan_reused = planMs == 0;
-            fr.excitations.resize(E);
-            for (uint32_t e = 0; e < E; ++e) {
+            const uint32_t Eout = coupling ? 1 : E;  // a coupled solve reports its one coupled field
+            fr.excitations.resize(Eout);
+            // coupled face velocities: each port's unit-flow velocities times its flow
+            std::map<uint32_t, cplx> coupledFaces;
+            if (coupling)
+                for (uint32_t e = 0; e < E; ++e)
+                    for (size_t i = r.excitation_face_offsets[e]; i < r.excitation_face_offsets[e + 1]; ++i)
+                        coupledFaces[r.excitation_face_ids[i]] =
+                            fr.portFlow[e] * cplx(r.excitation_velocities[2 * i], r.excitation_velocities[2 * i + 1]);
+            for (uint32_t e = 0; e < Eout; ++e) {
                 ExcitationResult &er = fr.excitations[e];
+                const std::map<uint32_t, cplx> &velocities = coupling ? coupledFaces : faceVelocity[e];
                 er.trace.assign(x.begin() + (size_t(b) * E + e) * N, x.begin() + (size_t(b) * E + e + 1) * N);
                 er.residual = relative[size_t(b) * E + e];
                 er.refinements = steps[b];
@@ -1102,13 +1142,36 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                     if (!std::isfinite(avg.real()) || !std::isfinite(avg.imag()))
                         throw NumericError("Burton-Miller pressure is not finite.");
                     er.surface[t] = avg;
-                    const auto it = faceVelocity[e].find(p.face);
-                    er.normalDerivative[t] = it == faceVelocity[e].end() ? cplx(0) : cplx(0, -r.density * omega) * it->second;
+                    const auto it = velocities.find(p.face);
+                    er.normalDerivative[t] = it == velocities.end() ? cplx(0) : cplx(0, -r.density * omega) * it->second;
+                }
+                if (coupling) {
+                    // validateCouplingClosure (lem_coupling.cpp:97-120): the coupled field's
+                    // power-dual mean pressure per port against the network's port pressure
+                    std::vector<cplx> means(E, 0.0);
+                    std::vector<double> mags(E, 0.0);
+                    for (uint32_t t = 0; t < T; ++t)
+                        if (panelPort[t] >= 0) {
+                            const double w = space_.panels[t].area * panelUnitVelocity[t];
+                            means[panelPort[t]] += w * er.surface[t];
+                            mags[panelPort[t]] += w * std::abs(er.surface[t]);
+                        }
+                    for (uint32_t i = 0; i < E; ++i) {
+                        const double scale = std::max(mags[i], std::abs(fr.portPressure[i]));
+                        const double diff = std::abs(means[i] - fr.portPressure[i]);
+                        if (!std::isfinite(scale) || !std::isfinite(diff) || diff > 1e-3 * scale)
+                            throw NumericError("BEM and LEM port pressures fail the feedback consistency check.");
+                    }
                 }
                 er.observer.assign(field.begin() + (size_t(b) * E + e) * O, field.begin() + (size_t(b) * E + e + 1) * O);
-                for (size_t i = r.excitation_face_offsets[e]; i < r.excitation_face_offsets[e + 1]; ++i) {
-                    const uint32_t face = r.excitation_face_ids[i];
-                    const cplx v(r.excitation_velocities[2 * i], r.excitation_velocities[2 * i + 1]);
+                std::vector<std::pair<uint32_t, cplx>> drive;
+                if (coupling)
+                    drive.assign(coupledFaces.begin(), coupledFaces.end());
+                else
+                    for (size_t i = r.excitation_face_offsets[e]; i < r.excitation_face_offsets[e + 1]; ++i)
+                        drive.emplace_back(r.excitation_face_ids[i],
+                                           cplx(r.excitation_velocities[2 * i], r.excitation_velocities[2 * i + 1]));
+                for (const auto &[face, v] : drive) {
                     if (std::abs(v) == 0)
                         continue;
                     double area = 0;
@@ -1134,6 +1197,65 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
     timer_.stop(span, s);
     result->peakDeviceBytes = peakBytes_;
     return result;
+}
+
+// LEM coupling of one batch (cuda_solver.cu:1584-1667): per frequency the port
+// impedance Z from the refined unit-flow basis solves (power-dual DP0 mean
+// pressure at port i per unit flow at port j), the network's port flows, and the
+// superposed pressure, right-hand side and flux of the coupled field written to
+// excitation slot 0 (the other slots zeroed), ready for its own refinement with
+// the retained factors.
+void Session::coupleBatch(const CouplingNetwork &network, const std::vector<double> &freqList, uint32_t f0, uint32_t B,
+                          uint32_t E, double density, const std::vector<int32_t> &panelPort,
+                          const std::vector<double> &panelUnitVelocity, std::vector<FrequencyResult> &out) {
+    (void)density;
+    const cudaStream_t s = stream();
+    const size_t N = space_.vertices.size(), T = space_.panels.size();
+    std::vector<cplx> x(size_t(B) * E * N), b(size_t(B) * E * N), q(size_t(B) * E * T);
+    cuda(cudaMemcpyAsync(x.data(), dX_.as<void>(), x.size() * 16, cudaMemcpyDeviceToHost, s), "coupling download");
+    cuda(cudaMemcpyAsync(b.data(), dRhs_.as<void>(), b.size() * 16, cudaMemcpyDeviceToHost, s), "coupling download");
+    cuda(cudaMemcpyAsync(q.data(), dFlux_.as<void>(), q.size() * 16, cudaMemcpyDeviceToHost, s), "coupling download");
+    cuda(cudaStreamSynchronize(s), "CUDA coupling");
+    for (uint32_t bb = 0; bb < B; ++bb) {
+        std::vector<cplx> Z(size_t(E) * E, 0.0), Q, P;
+        for (size_t t = 0; t < T; ++t) {
+            const int port = panelPort[t];
+            if (port < 0)
+                continue;
+            const HostPanel &pn = space_.panels[t];
+            const double w = pn.area * panelUnitVelocity[t];
+            for (uint32_t j = 0; j < E; ++j) {
+                const cplx *xj = x.data() + (size_t(bb) * E + j) * N;
+                Z[size_t(port) * E + j] += (xj[pn.nodes[0]] + xj[pn.nodes[1]] + xj[pn.nodes[2]]) / 3.0 * w;
+            }
+        }
+        network(freqList[f0 + bb], Z, Q, P);
+        if (Q.size() != E || P.size() != E)
+            throw InvalidArgument("LEM result port count does not match its BEM basis.");
+        for (uint32_t j = 0; j < E; ++j)
+            if (!std::isfinite(Q[j].real()) || !std::isfinite(Q[j].imag()) || !std::isfinite(P[j].real()) ||
+                !std::isfinite(P[j].imag()))
+                throw NumericError("LEM port flows or pressures are not finite.");
+        const auto superpose = [&](std::vector<cplx> &v, size_t n) {
+            std::vector<cplx> sum(n, 0.0);
+            for (uint32_t j = 0; j < E; ++j)
+                for (size_t i = 0; i < n; ++i)
+                    sum[i] += Q[j] * v[(size_t(bb) * E + j) * n + i];
+            std::fill(v.begin() + size_t(bb) * E * n, v.begin() + size_t(bb + 1) * E * n, cplx(0));
+            std::copy(sum.begin(), sum.end(), v.begin() + size_t(bb) * E * n);
+        };
+        superpose(x, N);
+        superpose(b, N);
+        superpose(q, T);
+        FrequencyResult &fr = out[f0 + bb];
+        fr.portImpedance = std::move(Z);
+        fr.portFlow = std::move(Q);
+        fr.portPressure = std::move(P);
+    }
+    cuda(cudaMemcpyAsync(dX_.as<void>(), x.data(), x.size() * 16, cudaMemcpyHostToDevice, s), "coupling upload");
+    cuda(cudaMemcpyAsync(dRhs_.as<void>(), b.data(), b.size() * 16, cudaMemcpyHostToDevice, s), "coupling upload");
+    cuda(cudaMemcpyAsync(dFlux_.as<void>(), q.data(), q.size() * 16, cudaMemcpyHostToDevice, s), "coupling upload");
+    cuda(cudaStreamSynchronize(s), "CUDA coupling");
 }
 
 // Assembly, LU and initial solves of one frequency batch (launches only; the

@@ -47,6 +47,9 @@ struct FrequencyResult {
     double frequency{};
     hs_frequency_info info{};
     std::vector<ExcitationResult> excitations;
+    // LEM-coupled solves: port impedance Z (ports x ports, row i col j) and the
+    // network's port flows and pressures
+    std::vector<cplx> portImpedance, portFlow, portPressure;
 };
 struct Result {
     size_t T{}, N{}, O{}, E{}, peakDeviceBytes{};
@@ -62,13 +65,20 @@ struct SolveHooks {
     std::function<void(const FrequencyResult &)> done;
 };
 
+// The lumped network of a coupled solve (lem::solve in the reference): from the
+// frequency and the port impedance matrix Z (ports x ports, row i col j: mean
+// pressure at port i per unit flow at port j) the port flows Q and pressures P.
+using CouplingNetwork = std::function<void(double frequency, const std::vector<cplx> &Z, std::vector<cplx> &Q,
+                                           std::vector<cplx> &P)>;
+
 class Session {
   public:
     Session(const MeshInput &mesh, uint32_t residency);
     ~Session();
     void setStream(cudaStream_t stream);
     std::unique_ptr<Result> solve(const hs_request &request, const volatile int32_t *cancel, hs_progress_fn progress,
-                                  void *user, const SolveHooks *hooks = nullptr);
+                                  void *user, const SolveHooks *hooks = nullptr,
+                                  const CouplingNetwork *coupling = nullptr);
     const Plan &plan(const hs_numerics &numerics, double maxK, const volatile int32_t *cancel);
     void debugAssemble(const hs_numerics &numerics, double planK, double k, const double *flux, double *matrix,
                        double *rhs);
@@ -116,6 +126,9 @@ class Session {
     void runDenseChain(const AssemblyGeometry &geo, const AssemblyWorkspace &ws, uint32_t B, uint32_t E, bool mixed,
                        cudaStream_t s);
     void dropGraphs();
+    void coupleBatch(const CouplingNetwork &network, const std::vector<double> &freqList, uint32_t f0, uint32_t B,
+                     uint32_t E, double density, const std::vector<int32_t> &panelPort,
+                     const std::vector<double> &panelUnitVelocity, std::vector<FrequencyResult> &out);
     struct DenseGraph {
         uint32_t B, E;
         bool mixed;

@@ -162,6 +162,26 @@ hs_status hs_bem_session_set_stream(hs_bem_session *session, void *cuda_stream);
 hs_status hs_bem_solve(hs_bem_session *session, const hs_request *request, const volatile int32_t *cancel,
                        hs_progress_fn progress, void *user, hs_result **out);
 
+/* ---- LEM-coupled solve (CudaBemSolver::solve with request.coupling,
+ * cuda_solver.cu:1584-1667; lem_coupling.cpp:9-120) ----
+ * The request's excitations are the unit-flow basis, one per port: each port's
+ * faces (disjoint between ports) with positive real velocities w_f / S_w whose
+ * flux integrates to one unit of volume velocity (makeCouplingBasis). Per
+ * frequency the library solves the basis, forms the port impedance matrix Z
+ * (ports x ports complex, row-major: the power-dual mean pressure at port i per
+ * unit flow at port j), calls `network` for the port flows and pressures (the
+ * caller's lumped network: lem::solve), superposes the coupled pressure,
+ * right-hand side and flux, refines that combined equation with the retained
+ * factors, checks the port-pressure closure to 1e-3 (validateCouplingClosure)
+ * and evaluates the observers for it. The result has one excitation per
+ * frequency, the coupled field; hs_result_coupling returns Z, the flows and the
+ * pressures. Dense forms only (fast multipole: HS_E_UNSUPPORTED). `network`
+ * returns HS_OK or fails the solve with HS_E_INVALID. */
+typedef hs_status (*hs_network_fn)(double frequency, size_t port_count, const double *impedance,
+                                   double *volume_velocity, double *pressure, void *user);
+hs_status hs_bem_solve_coupled(hs_bem_session *session, const hs_request *request, hs_network_fn network,
+                               void *user, const volatile int32_t *cancel, hs_result **out);
+
 /* ---- results (BemResult, bem.hpp:319-332) ---- */
 size_t hs_result_frequency_count(const hs_result *r);
 size_t hs_result_excitation_count(const hs_result *r);
@@ -178,6 +198,11 @@ hs_status hs_result_surface_pressure(const hs_result *r, size_t f, size_t e, dou
 hs_status hs_result_normal_derivative(const hs_result *r, size_t f, size_t e, double *out);
 hs_status hs_result_observer_pressure(const hs_result *r, size_t f, size_t e, double *out);
 hs_status hs_result_impedances(const hs_result *r, size_t f, size_t e, hs_face_impedance *out);
+/* Coupled solves: Z (ports x ports complex), port flows and pressures (ports
+ * complex each) of frequency f; ports receives the count (0 for uncoupled
+ * results). Any output pointer may be NULL. */
+hs_status hs_result_coupling(const hs_result *r, size_t f, double *impedance, double *volume_velocity,
+                             double *pressure, size_t *ports);
 void hs_result_free(hs_result *r);
 
 /* ---- diagnostics ---- */

@@ -1,5 +1,7 @@
 """Request validation, error classes and cancellation of the CUDA solver,
 matching the reference's behaviour (cuda_solver.cu:1054-1137, 1165-1212)."""
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -128,3 +130,48 @@ def test_mapped_host_patch_residency_equals_device():
         assert np.array_equal(fd.excitations[0].observer_pressure, fm.excitations[0].observer_pressure)
     saved = results["device"].peak_device_bytes - results["mapped_host"].peak_device_bytes
     assert saved >= len(plan["patches"]) * 22 * 8 * 0.99
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_library_coupled_solve(precision):
+    """The coupled solve inside the library (hs_bem_solve_coupled): the port
+    impedance from the basis solves, a network that depends on it (each port a
+    pressure source behind an internal impedance: (Z + Zs) Q = U), the superposed
+    coupled field refined as its own equation, the closure check, and one coupled
+    excitation per frequency. It equals the host-side superposition of the same
+    basis and a direct solve with the coupled face velocities."""
+    m = meshes.icosphere(2)
+    c = m.vertices[m.triangles].mean(axis=1)
+    faces = np.where(c[:, 2] > 0.06, 17, np.where(c[:, 0] < -0.06, 29, 90)).astype(np.uint32)
+    kind = np.where(faces == 90, meshes.WALL, meshes.DRIVEN).astype(np.uint8)
+    mesh = hs.SurfaceMesh(m.vertices, m.triangles, faces, kind)
+    U = np.array([1.0, 0.3j])
+    Zs = np.diag([2e4 + 1e3j, 5e4])
+
+    def flows_of(Z):
+        q = np.linalg.solve(Z + Zs, U)
+        return q, Z @ q
+    numerics = hs.BemNumerics(precision=precision, relative_residual_tolerance=1e-7)
+    ports = [hs.BemPort("front", [17]), hs.BemPort("side", [29])]
+    basis = hs.make_coupling_basis(ports, mesh)
+    request = hs.BemRequest(frequencies=[600.0, 1500.0], excitations=basis.excitations, observers=[(0, 0, 0.5)],
+                            numerics=numerics)
+    with hs.CudaBemSolver(mesh) as solver:
+        lib_result, extra = solver.solve_coupled(request, lambda f, Z: flows_of(Z))
+        host = hs.coupled_solve(solver, mesh, ports, dataclasses.replace(request, excitations=[]),
+                                lambda f, Z: [hs.PortSolution(q, p) for q, p in zip(*flows_of(Z))])
+        for frame, (Z, q, p), h in zip(lib_result.frequencies, extra, host):
+            assert len(frame.excitations) == 1
+            e = frame.excitations[0]
+            assert np.allclose(Z, h.impedance, rtol=1e-9, atol=0)
+            assert np.allclose(q, [s.volume_velocity for s in h.ports], rtol=1e-9, atol=0)
+            assert np.linalg.norm(e.boundary.pressure_trace - h.pressure_trace) <= 1e-6 * np.linalg.norm(
+                h.pressure_trace)
+            assert e.boundary_residual <= (1e-10 if precision == "mixed" else 1e-7)
+            direct = solver.solve(hs.BemRequest(frequencies=[frame.frequency], observers=[(0, 0, 0.5)],
+                                                excitations=[hs.BemExcitation("lem", h.face_velocities)],
+                                                numerics=numerics)).frequencies[0].excitations[0]
+            assert np.linalg.norm(e.boundary.pressure_trace - direct.boundary.pressure_trace) <= 1e-6 * np.linalg.norm(
+                direct.boundary.pressure_trace)
+            assert abs(e.observer_pressure[0] - direct.observer_pressure[0]) <= 1e-6 * abs(direct.observer_pressure[0])
+            assert np.allclose(e.boundary.normal_derivative, direct.boundary.normal_derivative, rtol=1e-12, atol=0)
