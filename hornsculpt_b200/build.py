@@ -57,5 +57,24 @@ def build(verbose_ptxas: bool = False) -> pathlib.Path:
     return LIBRARY
 
 
+ADAPTER = PKG / "adapter"
+ADAPTER_BINARY = ADAPTER / "adapter_solve"
+
+
+def build_adapter(reference: pathlib.Path) -> pathlib.Path:
+    """Compiles the reference-side adapter (adapter/cuda_bem_solver_b200.cpp, the
+    reference's hornsculpt::CudaBemSolver over this library's C ABI) and its driver
+    against the reference's own headers, linked to libhs_bem.so: proof that the
+    drop-in builds against the reference interface as it is declared there."""
+    includes = sorted((reference / "modules").glob("*/include"))
+    if not includes:
+        raise RuntimeError(f"no reference include directories under {reference}")
+    cmd = [shutil.which("g++") or "g++", "-std=c++20", "-O2", "-Wall", *[f"-I{d}" for d in includes], "-I",
+           str(INCLUDE), str(ADAPTER / "cuda_bem_solver_b200.cpp"), str(ADAPTER / "adapter_solve.cpp"), "-L", str(PKG),
+           "-lhs_bem", "-Wl,-rpath,$ORIGIN/..", "-o", str(ADAPTER_BINARY)]
+    subprocess.run(cmd, check=True)
+    return ADAPTER_BINARY
+
+
 if __name__ == "__main__":
     print(build(verbose_ptxas="-v" in sys.argv))
