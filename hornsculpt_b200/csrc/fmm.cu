@@ -498,14 +498,16 @@ __global__ void __launch_bounds__(256) l2pKernel(const FmmPanel *__restrict__ pa
                                                  const uint64_t *__restrict__ coefOffset, int p, double k,
                                                  const double2 *__restrict__ Lcoef, double2 *far,
                                                  const float2 *__restrict__ L32, const double *__restrict__ sigma,
-                                                 const double *__restrict__ rule, int rulePts) {
+                                                 const double *__restrict__ rule, int rulePts, double2 *scratch) {
     extern __shared__ double smem[];
     const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
     const size_t td = tableDoubles(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double2 *Ls = reinterpret_cast<double2 *>(smem);  // [6][nc]
-    double2 *Ld = Ls + 6 * nc;                        // [nd]
-    double *tables = reinterpret_cast<double *>(Ld + nd);
+    // coefficients in shared memory, or for high orders in the block's slice of a
+    // global scratch (L1/L2-resident), leaving shared memory to the point tables
+    double2 *Ls = scratch ? scratch + size_t(blockIdx.x) * (6 * nc + nd) : reinterpret_cast<double2 *>(smem);  // [6][nc]
+    double2 *Ld = Ls + 6 * nc;                                                                               // [nd]
+    double *tables = scratch ? smem : reinterpret_cast<double *>(Ld + nd);
     const uint32_t leaf = leaves[blockIdx.x];
     loadLocals(Lcoef, L32, sigma, coefOffset[leaf], 6, nc, Ls);
     __syncthreads();
@@ -610,14 +612,14 @@ __global__ void __launch_bounds__(256) l2pRhsKernel(const FmmPanel *__restrict__
                                                     const uint64_t *__restrict__ coefOffset, int p, double k,
                                                     const double2 *__restrict__ Lcoef, double2 *far,
                                                     const float2 *__restrict__ L32, const double *__restrict__ sigma,
-                                                    const double *__restrict__ rule, int rulePts) {
+                                                    const double *__restrict__ rule, int rulePts, double2 *scratch) {
     extern __shared__ double smem[];
     const int P = p + 1, nc = (p + 1) * (p + 1), nd = (P + 1) * (P + 1);
     const size_t td = tableDoubles(P);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double2 *Ls = reinterpret_cast<double2 *>(smem);  // [nc]
-    double2 *Lg = Ls + nc;                            // [3][nd]: d/dx, d/dy, d/dz
-    double *tables = reinterpret_cast<double *>(Lg + 3 * nd);
+    double2 *Ls = scratch ? scratch + size_t(blockIdx.x) * (nc + 3 * nd) : reinterpret_cast<double2 *>(smem);  // [nc]
+    double2 *Lg = Ls + nc;  // [3][nd]: d/dx, d/dy, d/dz
+    double *tables = scratch ? smem : reinterpret_cast<double *>(Lg + 3 * nd);
     const uint32_t leaf = leaves[blockIdx.x];
     loadLocals(Lcoef, L32, sigma, coefOffset[leaf], 1, nc, Ls);
     __syncthreads();
@@ -1164,7 +1166,7 @@ struct FmmOperator::Impl {
     };
     std::vector<HfLevel> hf;
     double hfThreshold = 12.0;
-    DevBuf rule;
+    DevBuf rule, l2pScratch;
     int rulePts = 0;
     unsigned panelDegree = 4;
     bool useGraphs = true;
@@ -1963,9 +1965,15 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
             const int p = I.order[l], P = p + 1;
             const size_t td = tableDoubles(P);
             const size_t nc = size_t(p + 1) * (p + 1), nd = size_t(P + 1) * (P + 1);
-            const size_t sm = (rhs ? nc + 3 * nd : 6 * nc + nd) * 16 + kWarps * td * 8;
+            const size_t coefBytes = (rhs ? nc + 3 * nd : 6 * nc + nd) * 16, tableBytes = kWarps * td * 8;
+            // high orders keep the coefficients in global scratch, the point tables in shared memory
+            const bool spill = coefBytes + tableBytes > kMaxShared;
+            const size_t sm = spill ? tableBytes : coefBytes + tableBytes;
             if (sm > kMaxShared)
                 throw Unsupported("Fast-multipole leaf order exceeds the shared-memory tables; refine the tree.");
+            if (spill)
+                I.l2pScratch.ensure(size_t(leaves) * coefBytes);
+            double2 *scratch = spill ? I.l2pScratch.as<double2>() : nullptr;
             if (rhs) {
                 fmmCheck(cudaFuncSetAttribute(l2pRhsKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                          "l2p smem");
@@ -1973,7 +1981,7 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
                     I.panels.as<FmmPanel>(), I.dLeaves[l].as<uint32_t>(), I.dLeafStart[l].as<uint32_t>(),
                     I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(), I.coefOffset.as<uint64_t>(), p, k_,
                     I.Lc.as<double2>(), I.far.as<double2>(), I.fp32 ? I.Lc32.as<float2>() : nullptr,
-                    I.levelSigma(l), I.rule.as<double>(), I.rulePts);
+                    I.levelSigma(l), I.rule.as<double>(), I.rulePts, scratch);
             } else {
                 fmmCheck(cudaFuncSetAttribute(l2pKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
                          "l2p smem");
@@ -1982,7 +1990,7 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
                                                        I.dItems.as<FmmItem>() + I.itemBase[l], I.centers.as<double>(),
                                                        I.coefOffset.as<uint64_t>(), p, k_, I.Lc.as<double2>(),
                                                        I.far.as<double2>(), I.fp32 ? I.Lc32.as<float2>() : nullptr,
-                                                       I.levelSigma(l), I.rule.as<double>(), I.rulePts);
+                                                       I.levelSigma(l), I.rule.as<double>(), I.rulePts, scratch);
             }
             fmmCheck(cudaGetLastError(), "l2p launch");
         }

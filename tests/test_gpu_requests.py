@@ -129,7 +129,7 @@ def test_mapped_host_patch_residency_equals_device():
         assert np.array_equal(fd.excitations[0].boundary.pressure_trace, fm.excitations[0].boundary.pressure_trace)
         assert np.array_equal(fd.excitations[0].observer_pressure, fm.excitations[0].observer_pressure)
     saved = results["device"].peak_device_bytes - results["mapped_host"].peak_device_bytes
-    assert saved >= len(plan["patches"]) * 22 * 8 * 0.99
+    assert saved >= len(plan["patches"]) * 22 * 8 * 0.9
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
