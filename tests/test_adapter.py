@@ -21,7 +21,7 @@ def test_adapter_links_only_this_library():
     assert "libhs_bem.so" in needed and "not found" not in needed
 
 
-def _write_input(path, mesh, freqs, obs, density, c):
+def _write_input(path, mesh, freqs, obs, density, c, tolerance=5e-5, repeats=1):
     with open(path, "wb") as f:
         f.write(struct.pack("<4Q", mesh.vertex_count, mesh.triangle_count, len(freqs), len(obs)))
         f.write(np.ascontiguousarray(mesh.vertices, np.float64).tobytes())
@@ -30,7 +30,8 @@ def _write_input(path, mesh, freqs, obs, density, c):
         f.write(np.ascontiguousarray(mesh.boundary, np.uint8).tobytes())
         f.write(np.asarray(freqs, np.float64).tobytes())
         f.write(np.asarray(obs, np.float64).tobytes())
-        f.write(np.array([density, c], np.float64).tobytes())
+        f.write(np.array([density, c, tolerance], np.float64).tobytes())
+        f.write(struct.pack("<Q", repeats))
 
 
 @pytest.mark.gpu
