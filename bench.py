@@ -416,6 +416,66 @@ def run_c2(args):
     print(json.dumps(line), flush=True)
 
 
+def run_refgpu(args):
+    """C1 through HornSculpt's own GPU CudaBemSolver (compiled from the reference
+    sources into oracle/_ref/reference_solve) and through the adapter over this
+    library (hornsculpt_b200/adapter/adapter_solve): the same driver program and
+    request, default numerics (the reference's FP32 LU with FP64 refinement; the
+    adapter's plain FP64 form), 32 frequencies, one solver object per program.
+    Wall-clock milliseconds of each sweep after the first (plan cached), and the
+    surface-pressure difference of the two. One JSON line."""
+    import numpy as np
+    import struct
+    from hornsculpt_b200 import meshes
+    from hornsculpt_b200.build import ADAPTER_BINARY
+
+    mesh = meshes.icosphere(3)
+    work = pathlib.Path(tempfile.mkdtemp())
+    with open(work / "in.bin", "wb") as f:
+        f.write(struct.pack("<4Q", mesh.vertex_count, mesh.triangle_count, len(FREQUENCIES), len(OBSERVERS)))
+        f.write(np.ascontiguousarray(mesh.vertices, np.float64).tobytes())
+        f.write(np.ascontiguousarray(mesh.triangles, np.uint32).tobytes())
+        f.write(np.ascontiguousarray(mesh.face_ids, np.uint32).tobytes())
+        f.write(np.ascontiguousarray(mesh.boundary, np.uint8).tobytes())
+        f.write(np.asarray(FREQUENCIES, np.float64).tobytes())
+        f.write(np.asarray(OBSERVERS, np.float64).tobytes())
+        f.write(np.array([DENSITY, SOUND_SPEED, 5e-5], np.float64).tobytes())
+        f.write(struct.pack("<Q", args.steps + 1))
+    line = {"workload": "C1 through CudaBemSolver::solve (same driver): the reference's GPU build vs the adapter "
+                        "over this library", "frequencies": len(FREQUENCIES), "sweeps": args.steps}
+    outputs = {}
+    for name, binary in (("reference_gpu", ROOT / "oracle" / "_ref" / "reference_solve"),
+                         ("this_library_adapter", ADAPTER_BINARY)):
+        if not binary.exists():
+            line[name] = {"unavailable": f"{binary.name} not built"}
+            continue
+        run = subprocess.run([str(binary), str(work / "in.bin"), str(work / f"{name}.bin")], capture_output=True,
+                             text=True, timeout=1800)
+        if run.returncode != 0:
+            line[name] = {"failed": run.stderr.strip()[-300:]}
+            continue
+        info = json.loads(run.stdout.strip().splitlines()[-1])
+        wall = info["wall_ms"][1:]
+        line[name] = {"ms_per_sweep_median": statistics.median(wall), "ms_per_sweep": wall,
+                      "first_call_ms": info["wall_ms"][0],
+                      "solves_per_s": 1e3 * len(FREQUENCIES) / statistics.median(wall), "device": info["device"]}
+        outputs[name] = np.fromfile(work / f"{name}.bin", np.float64)
+    if len(outputs) == 2:
+        N, O = mesh.vertex_count, len(OBSERVERS)
+        per = 2 * N + 2 * O + 1
+        v = mesh.vertices[mesh.triangles]
+        area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+        worst = 0.0
+        for i in range(len(FREQUENCIES)):
+            a, b = (outputs[n][i * per:i * per + 2 * N].view(np.complex128)[mesh.triangles].mean(axis=1)
+                    for n in ("reference_gpu", "this_library_adapter"))
+            worst = max(worst, float(np.sqrt(np.sum(area * np.abs(a - b) ** 2) / np.sum(area * np.abs(b) ** 2))))
+        line["max_rel_err_surface_reference_gpu_vs_plain_fp64"] = worst
+        line["speedup_plain_fp64_over_reference_gpu"] = (line["reference_gpu"]["ms_per_sweep_median"] /
+                                                         line["this_library_adapter"]["ms_per_sweep_median"])
+    print(json.dumps(line), flush=True)
+
+
 C4_FREQUENCIES = [float(f) for f in __import__("numpy").geomspace(100.0, 12000.0, 64)]
 
 
@@ -625,7 +685,7 @@ def main():
                     help="solve only n sweep frequencies (small profiling cases)")
     ap.add_argument("--first-frequency", type=int, default=0,
                     help="index of the first sweep frequency solved (small profiling cases)")
-    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4", "serve"],
+    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4", "serve", "refgpu"],
                     help="c1: the headline sweep; c2: the 12.8k-triangle horn sweep (dense forms); "
                          "c3: mixed dense sizes N = 2k-16k (one line per mesh); "
                          "c4: 64-frequency sweeps on icospheres s4/s5; "
@@ -655,6 +715,8 @@ def main():
         return run_c2(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "refgpu":
+        return run_refgpu(args)
 
     import numpy as np
     import torch
