@@ -771,26 +771,35 @@ def main():
             # profiling off (its per-family event records are instrumentation, not work)
             profile, work = solver.profile(), solver.work()
             solver.set_profiling(False)
+            launches0 = solver.graph_launches()
+            plain_s = 0.0
             for _ in range(args.steps):
                 with torch.cuda.stream(stream):
                     flush.zero_()
                 stream.synchronize()
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 t0 = time.perf_counter()
+                start.record(stream)
                 solver.solve(req)
+                end.record(stream)
                 wall_s += time.perf_counter() - t0
                 e2e_ms.append(round(1e3 * (time.perf_counter() - t0), 2))
+                end.synchronize()
+                plain_s += start.elapsed_time(end) / 1e3
+            graph_replays = solver.graph_launches() - launches0
         barrier()
-        times = torch.tensor([device_s, wall_s], dtype=torch.float64, device="cuda")
+        times = torch.tensor([device_s, wall_s, plain_s], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(times, op=dist.ReduceOp.MAX)
-        device_s, wall_s = times.tolist()
+        device_s, wall_s, plain_s = times.tolist()
         span = profile.pop("solve_span", (0.0, 0))[0] / 1e3
         span_t = torch.tensor([span], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(span_t, op=dist.ReduceOp.MAX)
         span = span_t.item()
         return dict(device_s=device_s, wall_s=wall_s, span_s=span, result=result, profile=profile, work=work,
-                    clocks=clocks.summary(), step_ms=step_ms, phase_ms=phase_ms, e2e_ms=e2e_ms)
+                    clocks=clocks.summary(), step_ms=step_ms, phase_ms=phase_ms, e2e_ms=e2e_ms, plain_s=plain_s,
+                    graph_replays=graph_replays)
 
     plain = run_form("fp64")
     mixed = run_form("mixed")
@@ -822,32 +831,38 @@ def main():
         F = len(req.frequencies)
         h2d = F * (T * 16 + 8) + O * 24
         d2h = F * (N * 16 + O * 16 + 32)
-        value = points / mixed["span_s"]
+        # value: CUDA events on the session stream around each sweep with kernel profiling
+        # off (the production configuration: dense chains replayed as graphs)
+        value = points / mixed["plain_s"]
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * mixed["span_s"] / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * mixed["plain_s"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed form)", "data": "synthetic",
             "config": CONFIG,
             "e2e": {"value": points / mixed["wall_s"], "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(sum(v[1] for v in mixed["profile"].values())),
             "forms": {
-                "fp64_plain": {"value": points / plain["span_s"], "e2e": points / plain["wall_s"],
-                               "ms_per_step": 1e3 * plain["span_s"] / args.steps,
+                "fp64_plain": {"value": points / plain["plain_s"], "e2e": points / plain["wall_s"],
+                               "ms_per_step": 1e3 * plain["plain_s"] / args.steps,
+                               "value_profiled": points / plain["span_s"], "graph_replays": plain["graph_replays"],
                                "step_ms": plain["step_ms"], "phase_ms": plain["phase_ms"], "e2e_ms": plain["e2e_ms"],
                                "residual_max": max(e.boundary_residual for f in plain["result"].frequencies
                                                    for e in f.excitations)},
                 "mixed": {"value": value, "e2e": points / mixed["wall_s"],
-                          "ms_per_step": 1e3 * mixed["span_s"] / args.steps,
+                          "ms_per_step": 1e3 * mixed["plain_s"] / args.steps,
+                          "value_profiled": points / mixed["span_s"], "graph_replays": mixed["graph_replays"],
                           "step_ms": mixed["step_ms"], "phase_ms": mixed["phase_ms"], "e2e_ms": mixed["e2e_ms"],
                           "residual_max": max(e.boundary_residual for f in mixed["result"].frequencies
                                               for e in f.excitations),
                           "max_rel_err_surface_vs_fp64": err},
-                "mixed_over_fp64": plain["span_s"] / mixed["span_s"],
-                "timing": "value: CUDA events on the session stream around each sweep inside the library "
-                          "(first upload to last result download, host control included; kernel profiling on "
-                          "for the per-kernel times); e2e: wall clock of the Python API call with host request "
-                          "and result buffers, the same number of steps again with kernel profiling off",
+                "mixed_over_fp64": plain["plain_s"] / mixed["plain_s"],
+                "timing": "value: CUDA events on the session stream around each sweep (first upload to last "
+                          "result download, host control included) with kernel profiling off, so the dense batch "
+                          "chain replays as a CUDA graph; value_profiled: the library's in-sweep span over steps "
+                          "run with per-kernel CUDA-event profiling on (plain launches), the source of kernel_ms "
+                          "and the roofline; e2e: wall clock of the same unprofiled Python API calls with host "
+                          "request and result buffers",
             },
             "roofline": {"kernel": "regularMixedKernel<12> (mixed form, largest launch)", "bound": "fp32",
                          "achieved": m32, "peak": fp32, "unit": "TFLOP/s", "frac": m32 / fp32,
