@@ -405,6 +405,49 @@ def run_c2(args):
                           "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])[:12]},
                           "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations),
                           "gmres_iterations": [f.excitations[0].iterations for f in res.frequencies]}
+    # Far-field apply of the FP64 fast-multipole operator at 2 and 8 kHz: the rotational
+    # M2L against its algorithmic FLOP (per link and channel 2 rotations of
+    # 2 sum_n (2n+1)^2 real x complex products and the coaxial sum_m (p-m+1)^2 complex
+    # products, six channels), and the same apply with the plane-wave levels.
+    if "fmm64" in forms:
+        apply_rows = []
+        rng = np.random.default_rng(3)
+        pvec = rng.normal(size=mesh.vertex_count) + 1j * rng.normal(size=mesh.vertex_count)
+        fp64_peak = fp64_peak_tflops(torch)
+        with hs.CudaBemSolver(mesh) as solver:
+            solver.set_stream(stream.cuda_stream)
+            numerics = hs.BemNumerics(precision="fp64", acceleration="fast_multipole")
+            for freq in (2000.0, 8000.0):
+                k = 2 * np.pi * freq / SOUND_SPEED
+                row = {"frequency": freq}
+                for mode, threshold in (("rotational", 1e12), ("plane_wave", 12.0)):
+                    solver.set_plane_wave_threshold(threshold)
+                    solver.debug_fmm_far(numerics, k, 1e-8, pvec)  # prepare, warm-up
+                    solver.set_profiling(True)
+                    solver.debug_fmm_far(numerics, k, 1e-8, pvec)
+                    prof = solver.profile()
+                    solver.set_profiling(False)
+                    _, _, _, levels = solver.debug_fmm_far(numerics, k, 1e-8, pvec)
+                    m2l_ms = prof.get("fmm_m2l", (0.0, 0))[0]
+                    entry = {"m2l_ms": round(m2l_ms, 3),
+                             "apply_ms": round(sum(v[0] for kk, v in prof.items() if kk.startswith("fmm_")), 3),
+                             "levels": levels.tolist()}
+                    if mode == "rotational":
+                        flop = 0.0
+                        for lv, p_, _nodes, links, _pw in levels.tolist():
+                            rot = 2 * sum((2 * n + 1) ** 2 for n in range(p_ + 1)) * 2
+                            coax = sum((p_ - m + 1) ** 2 for m in range(p_ + 1)) * 8
+                            flop += links * 6 * (2 * rot + coax)
+                        entry["m2l_gflop"] = round(flop / 1e9, 3)
+                        entry["m2l_tflops"] = round(flop / (m2l_ms / 1e3) / 1e12, 3) if m2l_ms else None
+                        entry["frac_of_dgemm"] = (round(flop / (m2l_ms / 1e3) / 1e12 / fp64_peak, 4)
+                                                  if m2l_ms else None)
+                    row[mode] = entry
+                apply_rows.append(row)
+            solver.set_plane_wave_threshold(12.0)
+        line["fmm_far_apply"] = {"rows": apply_rows, "fp64_dgemm_tflops": fp64_peak,
+                                 "note": "one far-field apply (P2M, M2M, M2L, L2L, L2P) at expansion tolerance 1e-8; "
+                                         "CUDA events per kernel family"}
     base = "fp64" if "fp64" in results else "fmm64" if "fmm64" in results else None
     for other in [f for f in forms if f != base and base]:
         err = 0.0
