@@ -1781,7 +1781,10 @@ void FmmOperator::run(const double *src, bool rhs, double *y, cudaStream_t strea
     Impl &I = *impl_;
     const int mode = rhs ? 1 : 0;
     const bool capturable = stream != nullptr && stream != cudaStreamLegacy && stream != cudaStreamPerThread;
-    if (!I.useGraphs || !capturable || tree_.ppFar.empty() || (!I.graph[mode] && I.applies[mode]++ == 0)) {
+    // with kernel profiling on, plain launches keep every family's time
+    const bool profiling = timer && timer->enabled();
+    if (!I.useGraphs || !capturable || profiling || tree_.ppFar.empty() ||
+        (!I.graph[mode] && I.applies[mode]++ == 0)) {
         launchApply(src, rhs, y, stream, timer);
         return;
     }
