@@ -420,7 +420,7 @@ def run_c2(args):
             for freq in (2000.0, 8000.0):
                 k = 2 * np.pi * freq / SOUND_SPEED
                 row = {"frequency": freq}
-                for mode, threshold in (("rotational", 1e12), ("plane_wave", 12.0)):
+                for mode, threshold in (("rotational", 1e12), ("plane_wave", 8.0)):
                     solver.set_plane_wave_threshold(threshold)
                     solver.debug_fmm_far(numerics, k, 1e-8, pvec)  # prepare, warm-up
                     solver.set_profiling(True)
@@ -444,7 +444,7 @@ def run_c2(args):
                                                   if m2l_ms else None)
                     row[mode] = entry
                 apply_rows.append(row)
-            solver.set_plane_wave_threshold(12.0)
+            solver.set_plane_wave_threshold(8.0)
         line["fmm_far_apply"] = {"rows": apply_rows, "fp64_dgemm_tflops": fp64_peak,
                                  "note": "one far-field apply (P2M, M2M, M2L, L2L, L2P) at expansion tolerance 1e-8; "
                                          "CUDA events per kernel family"}

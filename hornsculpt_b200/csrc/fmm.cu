@@ -1165,7 +1165,7 @@ struct FmmOperator::Impl {
         DevBuf ids, linkSource, linkClass, theta, x, weights, coef, dirs, T, sigma, psi;
     };
     std::vector<HfLevel> hf;
-    double hfThreshold = 12.0;
+    double hfThreshold = 8.0;
     DevBuf rule, l2pScratch;
     int rulePts = 0;
     unsigned panelDegree = 4;

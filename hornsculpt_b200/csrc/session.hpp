@@ -139,7 +139,7 @@ class Session {
     std::vector<DenseGraph> denseGraphs_;
     uint64_t generation_ = 0, graphLaunches_ = 0;
     bool graphs_ = true;
-    double planeWaveThreshold_ = 12.0;
+    double planeWaveThreshold_ = 8.0;
 
     MeshInput mesh_;
     V3 origin_{};

@@ -305,7 +305,7 @@ hs_status hs_bem_debug_fmm_far(hs_bem_session *session, const hs_numerics *numer
 hs_status hs_bem_debug_fmm_selftest(double *error);
 /* Fast-multipole LF/HF switch (wideband_transfer.cpp:266-310): a level's M2L
  * runs in the diagonal plane-wave form when k times its shortest M2L distance
- * is at least `threshold` (default 12) and its order is at least 8; below, the
+ * is at least `threshold` (default 8) and its order is at least 8; below, the
  * rotate-coaxial-rotate form. A very large threshold keeps every level
  * rotational. Applies to the FP64 operator; the mixed form's FP32 inner
  * operator stays rotational. */

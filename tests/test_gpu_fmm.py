@@ -220,7 +220,7 @@ def test_mixed_fast_multipole_matches_dense(case, freqs):
 def test_plane_wave_far_operator_matches_dense_far_part(case, freq, threshold):
     """Electrically large levels translate in the diagonal plane-wave form (the
     reference's LF/HF switch, wideband_transfer.cpp:266-310): the far operator with
-    plane-wave levels against the all-rotational operator (to round-off) and against
+    plane-wave levels against the all-rotational operator (inside the expansion tolerance) and against
     the far support pairs of the dense FP64 matrix. At 8 kHz the horn's coarse leaves
     run at orders whose L2P coefficients no longer fit shared memory (global scratch)."""
     mesh = {"icosphere3": lambda: meshes.icosphere(3),
@@ -243,10 +243,11 @@ def test_plane_wave_far_operator_matches_dense_far_part(case, freq, threshold):
     far_rel = np.linalg.norm(far - expected) / np.linalg.norm(expected)
     vs_rot = np.linalg.norm(far - rot) / np.linalg.norm(rot)
     print(case, freq, "levels", levels.tolist(), "far rel", far_rel, "of full", full_rel, "vs rotational", vs_rot)
-    # The plane-wave form reproduces the rotational translations to round-off; against
+    # The plane-wave form reproduces the rotational translations far inside the
+    # expansion tolerance (6e-13 to 1.2e-8 measured, growing as k t_min falls); against
     # the dense far part both carry the far field's degree-4 panel rule, whose error
     # grows with k h (the audit's panel-rule promotion handles it in a solve).
-    assert vs_rot < 1e-9 and full_rel < 3e-5
+    assert vs_rot < 1e-7 and full_rel < 3e-5
 
 
 def test_plane_wave_levels_in_a_solve():

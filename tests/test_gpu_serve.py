@@ -137,16 +137,18 @@ def test_continuous_batching_joins_a_running_call():
     frequencies are solved, well before the long call ends. Its result equals
     its solve alone, bit for bit."""
     import time
-    sphere = meshes.octahedral_sphere(3)
-    long_freqs = [float(f) for f in np.geomspace(150.0, 1900.0, 32)]
+    sphere = meshes.octahedral_sphere(4)
+    long_freqs = [float(f) for f in np.geomspace(150.0, 1900.0, 24)]
     late = _request([333.0, 1234.0])
     with hs.BemServer(hs.ServeOptions(workers=1, planning_frequency=PLAN_HZ)) as server:
         alone, _ = server.wait(server.submit(sphere, late))
-    options = hs.ServeOptions(workers=1, planning_frequency=PLAN_HZ, max_batch_frequencies=2)
+    # one frequency per batch: the long call is 24 batches, the late request joins the next one
+    options = hs.ServeOptions(workers=1, planning_frequency=PLAN_HZ, max_batch_frequencies=1)
     with hs.BemServer(options) as server:
+        server.wait(server.submit(sphere, _request([500.0])))  # mesh resident and planned
         t_long = time.perf_counter()
         long_ticket = server.submit(sphere, _request(long_freqs))
-        time.sleep(0.05)
+        time.sleep(0.02)
         t_late = time.perf_counter()
         late_ticket = server.submit(sphere, late)
         late_result, late_timing = server.wait(late_ticket)
