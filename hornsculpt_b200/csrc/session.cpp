@@ -778,10 +778,15 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                         acc += space_.lumpedMass[i] * std::norm(v[size_t(e) * N + i]);
                     return std::sqrt(acc);
                 };
-                // defect correction: x += A_work^-1 r with the working expansions
-                const auto correct = [&](const double *r, double workTolerance) {
+                // defect correction: x += A_work^-1 r with the working expansions. The
+                // correction solve is relative to r, whose norm is rRel of the
+                // right-hand side's: it aims at half the target relative to the
+                // right-hand side, not to r (which would ask for digits below the
+                // FP64 operator's rounding once r is small).
+                const auto correct = [&](const double *r, double workTolerance, double rRel) {
                     op.prepare(ks[b], workTolerance, s);
-                    fmmSystem_->solve(r, dCorr_.as<double>(), E, .5 * target, o.fmm_restart_length,
+                    const double relTarget = rRel > 0 ? std::clamp(.5 * target / rRel, .5 * target, .5) : .5;
+                    fmmSystem_->solve(r, dCorr_.as<double>(), E, relTarget, o.fmm_restart_length,
                                       o.fmm_maximum_iterations, s, &timer_, rel, its, inner);
                     fmmSystem_->add(xB, dCorr_.as<double>(), reals, s);
                     for (uint32_t e = 0; e < E; ++e)
@@ -807,17 +812,19 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                              "direct audit norms");
                         cuda(cudaStreamSynchronize(s), "CUDA direct audit");
                         bool accept = true;
+                        double worst = 0;
                         for (uint32_t e = 0; e < E; ++e) {
                             const double r = norms[2 * e + 1] > 0 ? norms[2 * e] / norms[2 * e + 1] : 0.0;
                             relative[size_t(b) * E + e] = r;
                             accept = accept && r <= target;
+                            worst = std::max(worst, r);
                         }
                         if (accept)
                             break;
                         if (round >= std::max<uint32_t>(o.maximum_refinement_steps, 3))
                             throw NoConvergence("Direct Galerkin audit residual exceeds the tolerance; bounded "
                                                 "fast-multipole defect corrections did not converge.");
-                        correct(dAuditFine_.as<double>(), tau);
+                        correct(dAuditFine_.as<double>(), tau, worst);
                     }
                     directAudits_ += 1;
                 } else
@@ -856,7 +863,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                                 throw NoConvergence("Fast-multipole audit did not meet the residual tolerance after 4 "
                                                     "expansion refinements.");
                             tau = std::max(.1 * tau, 1e-12);
-                            correct(dAuditFine_.as<double>(), tau);
+                            correct(dAuditFine_.as<double>(), tau, *std::max_element(relAudit.begin(), relAudit.end()));
                         }
                         // Far-field panel rule (compareQuadrature, support_fmm_solve.cu:525-560):
                         // at the verification expansions, the operator and right-hand side with
@@ -903,7 +910,7 @@ std::unique_ptr<Result> Session::solve(const hs_request &r, const volatile int32
                         cuda(cudaMemcpyAsync(rhsB, dAuditB_.as<void>(), reals * 8, cudaMemcpyDeviceToDevice, s),
                              "promoted rhs");
                         fmmSystem_->residual(rhsB, xB, E, dAuditFine_.as<double>(), relAudit, s, &timer_);
-                        correct(dAuditFine_.as<double>(), tau);
+                        correct(dAuditFine_.as<double>(), tau, *std::max_element(relAudit.begin(), relAudit.end()));
                     }
             }
             cuda(cudaEventRecord(ev.solved, s), "phase event");

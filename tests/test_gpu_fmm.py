@@ -246,8 +246,11 @@ def test_plane_wave_far_operator_matches_dense_far_part(case, freq, threshold):
     # The plane-wave form reproduces the rotational translations far inside the
     # expansion tolerance (6e-13 to 1.2e-8 measured, growing as k t_min falls); against
     # the dense far part both carry the far field's degree-4 panel rule, whose error
-    # grows with k h (the audit's panel-rule promotion handles it in a solve).
-    assert vs_rot < 1e-7 and full_rel < 3e-5
+    # grows with k h (the audit's panel-rule promotion handles it in a solve): 5e-8
+    # of the full product at 3 kHz on the sphere, 5.8e-5 at 8 kHz on the horn
+    # (k h = 1.9), the same with every level rotational.
+    panel_rule_bar = 1e-4 if freq >= 8000.0 else 3e-5
+    assert vs_rot < 1e-7 and full_rel < panel_rule_bar
 
 
 def test_plane_wave_levels_in_a_solve():
