@@ -108,7 +108,7 @@ __device__ __forceinline__ void pairRecordValue(int o, const Real *MG, const Rea
 // and sweeps the NP trial points, contracting trial bases on the fly.
 // ---------------------------------------------------------------------------
 template <int NP>
-__global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restrict__ panels, uint32_t T,
+__global__ void __maxnreg__(112) regularPairsKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                           const double *__restrict__ ks,
                                                           const uint2 *__restrict__ bins,
                                                           const uint32_t *__restrict__ binCounts, size_t binCapacity,
@@ -117,37 +117,56 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
     constexpr int PPC = 192 / NP;
     constexpr int RO = ruleOffset<NP>();
     __shared__ double sS[192][18];
-    __shared__ double sL[192][3];
     __shared__ double sM[PPC][54];
+    // per trial point of each pair: its offset from the trial panel's first
+    // vertex and that offset against the trial and test normals
+    __shared__ double sY[192][5];
     const int f = blockIdx.y;
     const double k = ks[f], invk = 1.0 / k;
     const uint32_t count = binCounts[f * kBins + bin];
     const uint2 *list = bins + binStart(binOffsets, binCapacity, f, bin);
     double *rec = records + size_t(f) * map.planeSlots * kRecordDoubles;
     const int l = threadIdx.x / NP, x = threadIdx.x % NP;
+    const double *yRow = &sY[l * NP][0];
     for (uint32_t base = blockIdx.x * PPC; base < count; base += gridDim.x * PPC) {
         const uint32_t p = base + l;
+        uint2 pr = make_uint2(0, 0);
         if (p < count) {
-            const uint2 pr = list[p];
+            // thread x places the pair's trial point x
+            pr = list[p];
+            const DPanel &S = panels[pr.y], &A = panels[pr.x];
+            const double b1 = cRule[4 * (RO + x) + 1], b2 = cRule[4 * (RO + x) + 2];
+            double e[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                e[c] = S.e1[c] * b1 + S.e2[c] * b2;
+            sY[threadIdx.x][0] = e[0];
+            sY[threadIdx.x][1] = e[1];
+            sY[threadIdx.x][2] = e[2];
+            sY[threadIdx.x][3] = e[0] * S.n[0] + e[1] * S.n[1] + e[2] * S.n[2];
+            sY[threadIdx.x][4] = e[0] * A.n[0] + e[1] * A.n[1] + e[2] * A.n[2];
+        }
+        __syncthreads();
+        if (p < count) {
             const DPanel &A = panels[pr.x];
             const DPanel &S = panels[pr.y];
             const double bx1 = cRule[4 * (RO + x) + 1], bx2 = cRule[4 * (RO + x) + 2];
-            const double X0 = A.e1[0] * bx1 + A.e2[0] * bx2, X1 = A.e1[1] * bx1 + A.e2[1] * bx2,
-                         X2 = A.e1[2] * bx1 + A.e2[2] * bx2;
-            const double d0 = A.v0[0] - S.v0[0], d1 = A.v0[1] - S.v0[1], d2 = A.v0[2] - S.v0[2];
+            // test point x relative to the trial panel's first vertex
+            const double P0 = (A.v0[0] - S.v0[0]) + (A.e1[0] * bx1 + A.e2[0] * bx2);
+            const double P1 = (A.v0[1] - S.v0[1]) + (A.e1[1] * bx1 + A.e2[1] * bx2);
+            const double P2 = (A.v0[2] - S.v0[2]) + (A.e1[2] * bx1 + A.e2[2] * bx2);
             const double w0 = cRule[4 * (RO + x) + 3] * 4.0 * A.area * S.area * kInvFourPi;
-            const double nt0 = A.n[0], nt1 = A.n[1], nt2 = A.n[2], ns0 = S.n[0], ns1 = S.n[1], ns2 = S.n[2];
-            const double se10 = S.e1[0], se11 = S.e1[1], se12 = S.e1[2], se20 = S.e2[0], se21 = S.e2[1],
-                         se22 = S.e2[2];
+            // (x - y).n_s = P.n_s - e(y).n_s, (x - y).n_t = P.n_t - e(y).n_t
+            const double psP = P0 * S.n[0] + P1 * S.n[1] + P2 * S.n[2];
+            const double qtP = P0 * A.n[0] + P1 * A.n[1] + P2 * A.n[2];
             double sp[6] = {0, 0, 0, 0, 0, 0}, sq[6] = {0, 0, 0, 0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0};
             bool bad = false;
-#pragma unroll 4
+#pragma unroll(NP == 6 ? 6 : NP == 64 ? 2 : 4)
             for (int y = 0; y < NP; ++y) {
                 const double b0 = cRule[4 * (RO + y)], b1 = cRule[4 * (RO + y) + 1], b2 = cRule[4 * (RO + y) + 2];
                 const double wy = cRule[4 * (RO + y) + 3];
-                const double dx = d0 + (X0 - (se10 * b1 + se20 * b2));
-                const double dy = d1 + (X1 - (se11 * b1 + se21 * b2));
-                const double dz = d2 + (X2 - (se12 * b1 + se22 * b2));
+                const double *Y = yRow + 5 * y;
+                const double dx = P0 - Y[0], dy = P1 - Y[1], dz = P2 - Y[2];
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 bad |= !(r2 > 0) || !isfinite(r2);
                 const double rinv = rsqrt(r2);
@@ -158,8 +177,8 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
                 const double gr = cs * sc, gi = -sn * sc;
                 const double rr = gr - gi * kr, ri = gi + gr * kr;
                 const double rinv2 = rinv * rinv;
-                const double ps = (dx * ns0 + dy * ns1 + dz * ns2) * rinv2;
-                const double qt = -(dx * nt0 + dy * nt1 + dz * nt2) * rinv2;
+                const double ps = (psP - Y[3]) * rinv2;
+                const double qt = (Y[4] - qtP) * rinv2;
                 const double Pr = rr * ps, Pi = ri * ps, Qr = rr * qt, Qi = ri * qt;
                 const double bb[3] = {b0, b1, b2};
 #pragma unroll
@@ -180,9 +199,6 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
                 sS[threadIdx.x][6 + c] = sp[c];
                 sS[threadIdx.x][12 + c] = sq[c];
             }
-            sL[threadIdx.x][0] = cRule[4 * (RO + x)];
-            sL[threadIdx.x][1] = bx1;
-            sL[threadIdx.x][2] = bx2;
         }
         __syncthreads();
         // Test-side contraction: M[kind][i][j] = sum_x bt_i(x) S_kind,j(x).
@@ -193,8 +209,9 @@ __global__ void __launch_bounds__(192) regularPairsKernel(const DPanel *__restri
             double re = 0, im = 0;
             for (int xx = 0; xx < NP; ++xx) {
                 const int th = pl * NP + xx;
-                re += sL[th][i] * sS[th][kind * 6 + 2 * j];
-                im += sL[th][i] * sS[th][kind * 6 + 2 * j + 1];
+                const double bt = cRule[4 * (RO + xx) + i];
+                re += bt * sS[th][kind * 6 + 2 * j];
+                im += bt * sS[th][kind * 6 + 2 * j + 1];
             }
             sM[pl][kind * 18 + 2 * (3 * i + j)] = re;
             sM[pl][kind * 18 + 2 * (3 * i + j) + 1] = im;

@@ -17,6 +17,7 @@
 #include <array>
 #include <cmath>
 #include <complex>
+#include <limits>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -1157,7 +1158,8 @@ struct FmmOperator::Impl {
     // units of the level's cell width, so a handful of classes per level), the
     // link sources as indices into the level's node list, and the tables of the
     // prepared wavenumber. prepare() turns a level plane-wave when k times its
-    // shortest M2L distance reaches hfThreshold (FP64 operator only).
+    // shortest M2L distance reaches hfThreshold and the diagonal form's roundoff
+    // stays inside the expansion tolerance (FP64 operator only).
     struct HfLevel {
         bool active = false;
         int p = 0, nth = 0, nph = 0;
@@ -1166,6 +1168,7 @@ struct FmmOperator::Impl {
     };
     std::vector<HfLevel> hf;
     double hfThreshold = 8.0;
+    double tolerance = 1e-8;  // expansion tolerance of the last prepare()
     DevBuf rule, l2pScratch;
     int rulePts = 0;
     unsigned panelDegree = 4;
@@ -1536,8 +1539,20 @@ void FmmOperator::prepareHf(cudaStream_t stream) {
             tmin = std::min(tmin, w * std::sqrt(double(o[0] * o[0] + o[1] * o[1] + o[2] * o[2])));
         if (k_ * tmin < I.hfThreshold)
             continue;
-        h.active = true;
         const int p = I.order[l];
+        // Diagonal-stability guard: the transfer sum carries terms up to
+        // (2p+1)|h_p(k t)|, which for p > k t grow far beyond the result (about
+        // |h_0(k t)| = 1 / (k t)); their FP64 roundoff, eps (2p+1) |h_p(k t_min)| k t_min
+        // relative, must stay within the expansion tolerance, or the level keeps the
+        // rotational form (measured plane-wave errors sit at or below this estimate).
+        {
+            std::vector<double> yb(p + 1);
+            besselY(p, k_ * tmin, yb.data());
+            const double amplification = double(2 * p + 1) * std::fabs(yb[p]) * k_ * tmin;
+            if (!(std::numeric_limits<double>::epsilon() * amplification <= I.tolerance))
+                continue;
+        }
+        h.active = true;
         h.p = p;
         h.nth = (3 * p + 3) / 2;
         h.nph = 3 * p + 2;
@@ -1601,6 +1616,7 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
     const auto &nodes = tree_.nodes;
     const int levels = int(tree_.levels.size());
     const double d0 = -std::log10(std::clamp(tolerance, 1e-15, 1e-2));
+    I.tolerance = tolerance;
     I.order.assign(levels, 0);
     for (int l = I.lmin; l < levels; ++l) {
         double r = 0;
