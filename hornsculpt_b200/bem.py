@@ -255,6 +255,10 @@ class CudaBemSolver:
         """k x shortest M2L distance from which a fast-multipole level translates in the plane-wave form."""
         _lib.check(self._lib.hs_bem_session_set_plane_wave_threshold(self._handle, threshold))
 
+    def set_fmm_grouped_m2l(self, enabled: bool) -> None:
+        """Rotational M2L grouped by translation class (default) or one CTA per target node."""
+        _lib.check(self._lib.hs_bem_session_set_fmm_grouped_m2l(self._handle, 1 if enabled else 0))
+
     def set_fmm_audit(self, mode: str) -> None:
         """Fast-multipole acceptance audit: "automatic" (the reference's policy), "expansion" (finer
         expansions and panel-rule promotion) or "direct" (the exact dense system's residual)."""

@@ -107,20 +107,25 @@ __device__ __forceinline__ void pairRecordValue(int o, const Real *MG, const Rea
 // Regular pairs: one unordered pair per NP threads, thread x owns test point x
 // and sweeps the NP trial points, contracting trial bases on the fly.
 // ---------------------------------------------------------------------------
+// 128 threads: four CTAs (16 warps) per SM within the 128 registers a thread
+// may use at that occupancy (the register file is split between the four SM
+// sub-partitions, so 192-thread CTAs would stop at two per SM).
+constexpr int kPlainThreads = 128;
+
 template <int NP>
-__global__ void __maxnreg__(112) regularPairsKernel(const DPanel *__restrict__ panels, uint32_t T,
+__global__ void __launch_bounds__(kPlainThreads, 4) regularPairsKernel(const DPanel *__restrict__ panels, uint32_t T,
                                                           const double *__restrict__ ks,
                                                           const uint2 *__restrict__ bins,
                                                           const uint32_t *__restrict__ binCounts, size_t binCapacity,
                                                           const uint64_t *__restrict__ binOffsets, int bin,
                                                           double *__restrict__ records, SlotMap map, int *error) {
-    constexpr int PPC = 192 / NP;
+    constexpr int PPC = kPlainThreads / NP;  // pairs per CTA; the last NP-group of threads may idle
     constexpr int RO = ruleOffset<NP>();
-    __shared__ double sS[192][18];
+    __shared__ double sS[kPlainThreads][18];
     __shared__ double sM[PPC][54];
     // per trial point of each pair: its offset from the trial panel's first
     // vertex and that offset against the trial and test normals
-    __shared__ double sY[192][5];
+    __shared__ double sY[kPlainThreads][5];
     const int f = blockIdx.y;
     const double k = ks[f], invk = 1.0 / k;
     const uint32_t count = binCounts[f * kBins + bin];
@@ -130,8 +135,9 @@ __global__ void __maxnreg__(112) regularPairsKernel(const DPanel *__restrict__ p
     const double *yRow = &sY[l * NP][0];
     for (uint32_t base = blockIdx.x * PPC; base < count; base += gridDim.x * PPC) {
         const uint32_t p = base + l;
+        const bool mine = l < PPC && p < count;
         uint2 pr = make_uint2(0, 0);
-        if (p < count) {
+        if (mine) {
             // thread x places the pair's trial point x
             pr = list[p];
             const DPanel &S = panels[pr.y], &A = panels[pr.x];
@@ -147,7 +153,7 @@ __global__ void __maxnreg__(112) regularPairsKernel(const DPanel *__restrict__ p
             sY[threadIdx.x][4] = e[0] * A.n[0] + e[1] * A.n[1] + e[2] * A.n[2];
         }
         __syncthreads();
-        if (p < count) {
+        if (mine) {
             const DPanel &A = panels[pr.x];
             const DPanel &S = panels[pr.y];
             const double bx1 = cRule[4 * (RO + x) + 1], bx2 = cRule[4 * (RO + x) + 2];
@@ -161,7 +167,7 @@ __global__ void __maxnreg__(112) regularPairsKernel(const DPanel *__restrict__ p
             const double qtP = P0 * A.n[0] + P1 * A.n[1] + P2 * A.n[2];
             double sp[6] = {0, 0, 0, 0, 0, 0}, sq[6] = {0, 0, 0, 0, 0, 0}, sg[6] = {0, 0, 0, 0, 0, 0};
             bool bad = false;
-#pragma unroll(NP == 6 ? 6 : NP == 64 ? 2 : 4)
+#pragma unroll(NP == 6 ? 6 : 4)
             for (int y = 0; y < NP; ++y) {
                 const double b0 = cRule[4 * (RO + y)], b1 = cRule[4 * (RO + y) + 1], b2 = cRule[4 * (RO + y) + 2];
                 const double wy = cRule[4 * (RO + y) + 3];
@@ -202,7 +208,7 @@ __global__ void __maxnreg__(112) regularPairsKernel(const DPanel *__restrict__ p
         }
         __syncthreads();
         // Test-side contraction: M[kind][i][j] = sum_x bt_i(x) S_kind,j(x).
-        for (int item = threadIdx.x; item < PPC * 27; item += 192) {
+        for (int item = threadIdx.x; item < PPC * 27; item += kPlainThreads) {
             const int pl = item / 27, e = item % 27, kind = e / 9, i = (e % 9) / 3, j = e % 3;
             if (base + pl >= count)
                 continue;
@@ -217,7 +223,7 @@ __global__ void __maxnreg__(112) regularPairsKernel(const DPanel *__restrict__ p
             sM[pl][kind * 18 + 2 * (3 * i + j) + 1] = im;
         }
         __syncthreads();
-        for (int item = threadIdx.x; item < PPC * 24; item += 192) {
+        for (int item = threadIdx.x; item < PPC * 24; item += kPlainThreads) {
             const int pl = item / 24, o = item % 24;
             if (base + pl >= count)
                 continue;
@@ -1499,7 +1505,7 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
     // Grid of the grid-stride pair loop in CTAs per SM: each pair is one
     // independent item, so the choice moves only the load balance and occupancy.
     static constexpr int kMixedCtas[] = {16, 8, 24, 32};
-    static constexpr int kPlainCtas[] = {6, 3, 12};
+    static constexpr int kPlainCtas[] = {8, 4, 16};
     const int candidates = mixed ? 4 : 3;
     const auto launch = [&](int c) {
         if (mixed) {
@@ -1509,7 +1515,7 @@ void launchRegular(const AssemblyGeometry &g, const double *ks, uint32_t B, cons
                                                              static_cast<float *>(ws.records), error);
         } else {
             const dim3 grid(unsigned(smCount() * kPlainCtas[c]), B);
-            regularPairsKernel<NP><<<grid, 192, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts,
+            regularPairsKernel<NP><<<grid, kPlainThreads, 0, stream>>>(g.panels, g.T, ks, ws.bins, ws.binCounts,
                                                              ws.binCapacity, ws.binOffsets, bin,
                                                              static_cast<double *>(ws.records), map, error);
         }

@@ -499,6 +499,15 @@ hs_status hs_bem_session_set_plane_wave_threshold(hs_bem_session *s, double thre
     });
 }
 
+hs_status hs_bem_session_set_fmm_grouped_m2l(hs_bem_session *s, int enabled) {
+    if (!s)
+        return fail(HS_E_INVALID, "Session handle is null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->setGroupedM2l(enabled != 0);
+    });
+}
+
 hs_status hs_bem_session_set_fmm_audit(hs_bem_session *s, uint32_t mode) {
     if (!s || mode > 2)
         return fail(HS_E_INVALID, "Fast-multipole audit mode must be 0, 1 or 2.");

@@ -446,6 +446,191 @@ __global__ void reduceKernel(const uint32_t *__restrict__ outNodes, const uint64
     }
 }
 
+// Grouped M2L. The links of a level whose translation vectors share the polar
+// class and the distance (one Wigner block, one coaxial table) are cut into
+// chunks of G links; one CTA takes a chunk with all channels, so every table
+// entry it reads serves 6 G columns, and writes each link's local contribution
+// u (phases applied) to its own slot. m2lSumKernel then adds the slots of each
+// target in link order: the result is independent of the chunking and of the
+// scheduling. Shared memory: two coefficient buffers [nc][cpad] (cpad odd:
+// conflict-free column-strided staging), the links' azimuth phases and the
+// m-major order of the coaxial outputs.
+constexpr int kGroupTile = 6;  // columns per thread item
+
+__host__ __device__ inline size_t groupSmemBytes(int p, int cpad, int g, size_t complexBytes) {
+    const size_t nc = size_t(p + 1) * (p + 1);
+    return 2 * nc * cpad * complexBytes + size_t(g) * (p + 1) * complexBytes + nc * 4 + size_t(p + 2) * 4;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) m2lGroupKernel(const uint2 *__restrict__ chunks,
+                                                      const uint32_t *__restrict__ sorted,
+                                                      const TransLink *__restrict__ links, int p, int nch, int cpad,
+                                                      int gmax, const C2R<R> *__restrict__ inCoef,
+                                                      const uint64_t *__restrict__ coefOffset,
+                                                      const R *__restrict__ wigner,
+                                                      const uint64_t *__restrict__ wignerStart,
+                                                      const C2R<R> *__restrict__ coax,
+                                                      const uint64_t *__restrict__ coaxStart, C2R<R> *__restrict__ u) {
+    using CT = C2R<R>;
+    extern __shared__ double smem[];
+    const int nc = (p + 1) * (p + 1);
+    CT *bufA = reinterpret_cast<CT *>(smem);
+    CT *bufB = bufA + size_t(nc) * cpad;
+    CT *eph = bufB + size_t(nc) * cpad;                        // [gmax][p + 1]
+    int *qmap = reinterpret_cast<int *>(eph + size_t(gmax) * (p + 1));  // m-major position -> kk
+    int *coaxOff = qmap + nc;                                  // [p + 2]: offset of |m| in a coaxial table
+    const uint2 chunk = chunks[blockIdx.x];
+    const int count = int(chunk.y), C = count * nch;
+    const TransLink L0 = links[sorted[chunk.x]];
+    const R *dtab = wigner + wignerStart[L0.wclass];
+    const CT *ctab = coax + coaxStart[L0.cclass];
+    // phases, m-major order and coaxial block offsets
+    for (int e = threadIdx.x; e < count * (p + 1); e += blockDim.x) {
+        const int i = e / (p + 1), m = e - i * (p + 1);
+        double sn, cs;
+        sincos(m * links[sorted[chunk.x + i]].phi, &sn, &cs);
+        eph[e] = mkc<R>(cs, sn);
+    }
+    for (int kk = threadIdx.x; kk < nc; kk += blockDim.x) {
+        int n, m;
+        decode(kk, n, m);
+        const int a = m < 0 ? -m : m;
+        // order m = 0, 1, -1, 2, -2, ...; block |m| = a holds n = a .. p
+        const int before = a == 0 ? 0 : (p + 1) + 2 * ((a - 1) * (p + 1) - a * (a - 1) / 2);
+        const int q = before + (m < 0 ? p + 1 - a : 0) + (n - a);
+        qmap[q] = kk;
+    }
+    if (threadIdx.x == 0) {
+        int off = 0;
+        for (int a = 0; a <= p + 1; ++a) {
+            coaxOff[a] = off;
+            off += (p + 1 - a) * (p + 1 - a);
+        }
+    }
+    __syncthreads();
+    // staged inputs with the azimuth phase: A[kk][col] = M_src[ch][kk] exp(i m phi)
+    for (int e = threadIdx.x; e < C * nc; e += blockDim.x) {
+        const int col = e / nc, kk = e - col * nc;
+        const int i = col / nch, ch = col - i * nch;
+        int n, m;
+        decode(kk, n, m);
+        const uint32_t src = links[sorted[chunk.x + i]].source;
+        const CT ph = eph[i * (p + 1) + (m < 0 ? -m : m)];
+        const CT v = inCoef[coefOffset[src] + size_t(ch) * nc + kk];
+        bufA[size_t(kk) * cpad + col] = cmulT<R>(v, m < 0 ? mkc<R>(ph.x, -ph.y) : ph);
+    }
+    __syncthreads();
+    const int tiles = (C + kGroupTile - 1) / kGroupTile;
+    // forward rotation: B[n, m'] = sum_m A[n, m] d^n[m, m']
+    for (int e = threadIdx.x; e < tiles * nc; e += blockDim.x) {
+        const int tile = e / nc, kk = e - tile * nc, c0 = tile * kGroupTile;
+        int n, mp;
+        decode(kk, n, mp);
+        const int w = 2 * n + 1;
+        const R *d = dtab + wignerOffset(n) + (mp + n);
+        const CT *x = bufA + size_t(n) * n * cpad + c0;
+        CT acc[kGroupTile];
+#pragma unroll
+        for (int c = 0; c < kGroupTile; ++c)
+            acc[c] = mkc<R>(0, 0);
+        for (int j = 0; j < w; ++j) {
+            const R dv = d[size_t(j) * w];
+#pragma unroll
+            for (int c = 0; c < kGroupTile; ++c) {
+                const CT v = x[size_t(j) * cpad + c];
+                acc[c].x += v.x * dv;
+                acc[c].y += v.y * dv;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kGroupTile; ++c)
+            if (c0 + c < C)
+                bufB[size_t(kk) * cpad + c0 + c] = acc[c];
+    }
+    __syncthreads();
+    // coaxial translation per |m| (outputs in m-major order, so a warp reads
+    // consecutive entries of one table block): A[n', m] = sum_n C_|m|[n][n'] B[n, m]
+    for (int e = threadIdx.x; e < tiles * nc; e += blockDim.x) {
+        const int tile = e / nc, q = e - tile * nc, c0 = tile * kGroupTile;
+        const int kk = qmap[q];
+        int np, m;
+        decode(kk, np, m);
+        const int a = m < 0 ? -m : m, wo = p + 1 - a;
+        const CT *Ct = ctab + coaxOff[a] + (np - a);
+        CT acc[kGroupTile];
+#pragma unroll
+        for (int c = 0; c < kGroupTile; ++c)
+            acc[c] = mkc<R>(0, 0);
+        for (int n = a; n <= p; ++n) {
+            const CT cv = Ct[size_t(n - a) * wo];
+            const CT *x = bufB + size_t(n * n + n + m) * cpad + c0;
+#pragma unroll
+            for (int c = 0; c < kGroupTile; ++c)
+                acc[c] = caddT<R>(acc[c], cmulT<R>(cv, x[c]));
+        }
+#pragma unroll
+        for (int c = 0; c < kGroupTile; ++c)
+            if (c0 + c < C)
+                bufA[size_t(kk) * cpad + c0 + c] = acc[c];
+    }
+    __syncthreads();
+    // back rotation: B[n, m1] = sum_m d^n[m1, m] A[n, m]
+    for (int e = threadIdx.x; e < tiles * nc; e += blockDim.x) {
+        const int tile = e / nc, kk = e - tile * nc, c0 = tile * kGroupTile;
+        int n, m1;
+        decode(kk, n, m1);
+        const int w = 2 * n + 1;
+        const R *d = dtab + wignerOffset(n) + size_t(m1 + n) * w;
+        const CT *x = bufA + size_t(n) * n * cpad + c0;
+        CT acc[kGroupTile];
+#pragma unroll
+        for (int c = 0; c < kGroupTile; ++c)
+            acc[c] = mkc<R>(0, 0);
+        for (int j = 0; j < w; ++j) {
+            const R dv = d[j];
+#pragma unroll
+            for (int c = 0; c < kGroupTile; ++c) {
+                const CT v = x[size_t(j) * cpad + c];
+                acc[c].x += v.x * dv;
+                acc[c].y += v.y * dv;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < kGroupTile; ++c)
+            if (c0 + c < C)
+                bufB[size_t(kk) * cpad + c0 + c] = acc[c];
+    }
+    __syncthreads();
+    // each link's contribution with the conjugate phase, into its own slot
+    for (int e = threadIdx.x; e < C * nc; e += blockDim.x) {
+        const int col = e / nc, kk = e - col * nc;
+        const int i = col / nch, ch = col - i * nch;
+        int n, m;
+        decode(kk, n, m);
+        const CT ph = eph[i * (p + 1) + (m < 0 ? -m : m)];
+        const CT v = bufB[size_t(kk) * cpad + col];
+        u[(size_t(sorted[chunk.x + i]) * nch + ch) * nc + kk] = cmulT<R>(v, m < 0 ? ph : mkc<R>(ph.x, -ph.y));
+    }
+}
+
+// out[target] += sum over the target's links, in link order, of their slots.
+template <class R>
+__global__ void __launch_bounds__(256) m2lSumKernel(const uint32_t *__restrict__ outNodes,
+                                                    const uint32_t *__restrict__ linkStart,
+                                                    const uint64_t *__restrict__ coefOffset, int nc, int nch,
+                                                    const C2R<R> *__restrict__ u, C2R<R> *outCoef) {
+    const uint32_t oi = blockIdx.x;
+    const uint32_t l0 = linkStart[oi], l1 = linkStart[oi + 1];
+    C2R<R> *out = outCoef + coefOffset[outNodes[oi]];
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < nch * nc; e += gridDim.y * blockDim.x) {
+        C2R<R> acc = out[e];
+        for (uint32_t l = l0; l < l1; ++l)
+            acc = caddT<R>(acc, u[size_t(l) * nch * nc + e]);
+        out[e] = acc;
+    }
+}
+
 // Coefficient-space derivatives of a regular expansion (k = 1 scaling):
 // dz R_n^m = A(n,m) R_{n-1}^m - A(n+1,m) R_{n+1}^m, d+ = dx + i dy and d- = dx - i dy
 // raise / lower m with the coefficients below.
@@ -1134,6 +1319,21 @@ struct FmmOperator::Impl {
         uint32_t count = 0;
     };
     std::vector<DevPlan> dm2m, dm2l, dl2l;
+    // Grouped M2L per level: links in (polar class, coaxial class) order, the
+    // groups as (first, count) in that order, and per mode (0: six channels,
+    // 1: right-hand side) the chunks of the prepared order and whether the
+    // level uses the grouped kernel (shared memory and slot buffer permitting).
+    struct GroupPlan {
+        DevBuf sorted;
+        std::vector<std::pair<uint32_t, uint32_t>> groups;
+        DevBuf chunks[2];
+        uint32_t chunkCount[2] = {0, 0};
+        int g[2] = {0, 0}, cpad[2] = {0, 0}, p = -1;
+        bool active[2] = {false, false};
+    };
+    std::vector<GroupPlan> gm2l;
+    DevBuf slots;  // per-link M2L contributions (largest grouped level)
+    bool groupedM2l = true;
     std::vector<DevBuf> dLeaves, dLeafStart;
     std::vector<std::vector<uint32_t>> coaxClassOf;  // per kind*levels: local coax class index -> global
     // The far-field apply as a CUDA graph per mode (0: operator, 1: right-hand
@@ -1452,6 +1652,29 @@ FmmOperator::FmmOperator(const Space &space, const FmmTreeSettings &settings) : 
         put(I.dm2l[l], I.m2l[l]);
         put(I.dl2l[l], I.l2l[l]);
     }
+    // grouped M2L: links sorted by (polar class, coaxial class, link index)
+    I.gm2l.resize(levels);
+    for (int l = I.lmin; l < levels; ++l) {
+        const auto &lk = I.m2l[l].links;
+        if (lk.empty())
+            continue;
+        std::vector<uint32_t> order(lk.size());
+        for (uint32_t i = 0; i < order.size(); ++i)
+            order[i] = i;
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+            return lk[a].wclass != lk[b].wclass ? lk[a].wclass < lk[b].wclass : lk[a].cclass < lk[b].cclass;
+        });
+        Impl::GroupPlan &gp = I.gm2l[l];
+        for (uint32_t i = 0; i < order.size();) {
+            uint32_t j = i + 1;
+            while (j < order.size() && lk[order[j]].wclass == lk[order[i]].wclass &&
+                   lk[order[j]].cclass == lk[order[i]].cclass)
+                ++j;
+            gp.groups.emplace_back(i, j - i);
+            i = j;
+        }
+        uploadVec(gp.sorted, order, s);
+    }
     // plane-wave link classes (offset vectors of the M2L links, per level)
     I.hf.resize(levels);
     for (int l = I.lmin; l < levels; ++l) {
@@ -1518,6 +1741,11 @@ void FmmOperator::setFp32(bool enabled) {
 
 void FmmOperator::setHfThreshold(double threshold) {
     impl_->hfThreshold = threshold;
+    impl_->dropGraphs();
+}
+
+void FmmOperator::setGroupedM2l(bool enabled) {
+    impl_->groupedM2l = enabled;
     impl_->dropGraphs();
 }
 
@@ -1779,6 +2007,56 @@ void FmmOperator::prepare(double k, double tolerance, cudaStream_t stream) {
         remap(I.m2m[l], I.dm2m[l], I.coaxClassOf[levels + l]);
         remap(I.l2l[l], I.dl2l[l], I.coaxClassOf[2 * levels + l]);
     }
+    // Grouped M2L of the rotational levels, per mode: the largest chunk whose
+    // buffers fit 110 KB of shared memory (two CTAs per SM), else single links
+    // up to the opt-in limit; the slot buffer of the largest level must stay
+    // within a quarter of the free memory (24 GB at most), else the level runs
+    // the per-target translation kernel.
+    {
+        const size_t cb = I.fp32 ? 8 : 16;
+        size_t freeBytes = 0, totalBytes = 0;
+        if (cudaMemGetInfo(&freeBytes, &totalBytes) != cudaSuccess)
+            freeBytes = 0;
+        const size_t cap = std::min<size_t>(size_t(24) << 30, freeBytes / 4 + I.slots.bytes);
+        size_t slotBytes = 0;
+        for (int l = I.lmin; l < levels; ++l) {
+            Impl::GroupPlan &gp = I.gm2l[l];
+            gp.active[0] = gp.active[1] = false;
+            if (gp.groups.empty() || !I.groupedM2l || I.hf[l].active)
+                continue;
+            const int p = I.order[l];
+            const size_t nc = size_t(p + 1) * (p + 1), links = I.m2l[l].links.size();
+            for (int mode = 0; mode < 2; ++mode) {
+                const int nch = mode == 0 ? 6 : 1;
+                int g = 0, cpad = 0;
+                for (int cand = 16; cand >= 1 && !g; --cand)
+                    if (groupSmemBytes(p, (cand * nch) | 1, cand, cb) <= 110 * 1024) {
+                        g = cand;
+                        cpad = (cand * nch) | 1;
+                    }
+                if (!g && groupSmemBytes(p, nch | 1, 1, cb) <= kMaxShared) {
+                    g = 1;
+                    cpad = nch | 1;
+                }
+                const size_t need = links * nch * nc * cb;
+                if (!g || need > cap)
+                    continue;
+                slotBytes = std::max(slotBytes, need);
+                if (gp.g[mode] != g) {
+                    std::vector<uint2> chunks;
+                    for (const auto &[first, count] : gp.groups)
+                        for (uint32_t o = 0; o < count; o += uint32_t(g))
+                            chunks.push_back(make_uint2(first + o, std::min<uint32_t>(uint32_t(g), count - o)));
+                    uploadVec(gp.chunks[mode], chunks, stream);
+                    gp.chunkCount[mode] = uint32_t(chunks.size());
+                    gp.g[mode] = g;
+                }
+                gp.cpad[mode] = cpad;
+                gp.active[mode] = true;
+            }
+        }
+        I.slots.ensure(slotBytes);
+    }
     fmmCheck(cudaStreamSynchronize(stream), "prepare");
 }
 
@@ -1957,13 +2235,49 @@ void FmmOperator::launchApply(const double *src, bool rhs, double *y, cudaStream
             else
                 translate(I.dm2m[l], I.order[l + 1], I.order[l], I.Mc.as<double2>(), I.Mc.as<double2>(), true);
     }
+    // grouped M2L of level l (chunks into per-link slots, then the link-order sums)
+    const auto grouped = [&](int l, auto *in, auto *out) {
+        using CT = std::remove_cv_t<std::remove_pointer_t<decltype(out)>>;
+        using RT = decltype(CT{}.x);
+        constexpr bool f32 = std::is_same_v<RT, float>;
+        const Impl::GroupPlan &gp = I.gm2l[l];
+        const int mode = rhs ? 1 : 0, p = I.order[l], nc = (p + 1) * (p + 1);
+        const size_t sm = groupSmemBytes(p, gp.cpad[mode], gp.g[mode], sizeof(CT));
+        const RT *wig;
+        const CT *cx;
+        if constexpr (f32) {
+            wig = I.wigner32.as<float>();
+            cx = I.coax32.as<float2>();
+        } else {
+            wig = I.wigner.as<double>();
+            cx = I.coax.as<double2>();
+        }
+        fmmCheck(cudaFuncSetAttribute(m2lGroupKernel<RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm)),
+                 "grouped m2l smem");
+        m2lGroupKernel<RT><<<gp.chunkCount[mode], 256, sm, stream>>>(
+            gp.chunks[mode].as<uint2>(), gp.sorted.as<uint32_t>(), I.dm2l[l].links.as<TransLink>(), p, nch,
+            gp.cpad[mode], gp.g[mode], in, I.coefOffset.as<uint64_t>(), wig, I.wignerStart.as<uint64_t>(), cx,
+            I.coaxStart.as<uint64_t>(), I.slots.as<CT>());
+        fmmCheck(cudaGetLastError(), "grouped m2l launch");
+        const dim3 grid(I.dm2l[l].count, unsigned((nch * nc + 255) / 256));
+        TimedScope sums(timer, "fmm_m2l_sum", stream);  // nested in fmm_m2l
+        m2lSumKernel<RT><<<grid, 256, 0, stream>>>(I.dm2l[l].out.as<uint32_t>(), I.dm2l[l].start.as<uint32_t>(),
+                                                   I.coefOffset.as<uint64_t>(), nc, nch, I.slots.as<CT>(), out);
+        fmmCheck(cudaGetLastError(), "m2l sum launch");
+    };
     {
         TimedScope scope(timer, "fmm_m2l", stream);
+        const int mode = rhs ? 1 : 0;
         for (int l = I.lmin; l < levels; ++l)
-            if (I.fp32)
-                translate(I.dm2l[l], I.order[l], I.order[l], I.Mc32.as<float2>(), I.Lc32.as<float2>(), false);
-            else if (I.hf[l].active)
+            if (I.fp32) {
+                if (I.gm2l[l].active[mode])
+                    grouped(l, I.Mc32.as<float2>(), I.Lc32.as<float2>());
+                else
+                    translate(I.dm2l[l], I.order[l], I.order[l], I.Mc32.as<float2>(), I.Lc32.as<float2>(), false);
+            } else if (I.hf[l].active)
                 planeWaveM2L(l, nch, stream);
+            else if (I.gm2l[l].active[mode])
+                grouped(l, I.Mc.as<double2>(), I.Lc.as<double2>());
             else
                 translate(I.dm2l[l], I.order[l], I.order[l], I.Mc.as<double2>(), I.Lc.as<double2>(), false);
     }

@@ -68,6 +68,9 @@ class FmmOperator {
     // k times the shortest M2L distance from which a level translates in the
     // plane-wave form (default 12; a large value keeps every level rotational).
     void setHfThreshold(double threshold);
+    // Rotational M2L grouped by translation class (default) or per target node;
+    // takes effect at the next prepare().
+    void setGroupedM2l(bool enabled);
     // Far-field panel rule (Dunavant degree 4 by default; the audit promotes it
     // 4 -> 6 -> 8 -> 12 like the reference's compareQuadrature).
     void setPanelDegree(unsigned degree, cudaStream_t stream);

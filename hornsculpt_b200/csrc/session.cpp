@@ -1385,6 +1385,14 @@ void Session::setPlaneWaveThreshold(double threshold) {
         fmm_->setHfThreshold(threshold);
 }
 
+void Session::setGroupedM2l(bool enabled) {
+    groupedM2l_ = enabled;
+    if (fmm_)
+        fmm_->setGroupedM2l(enabled);
+    if (fmmInner_)
+        fmmInner_->setGroupedM2l(enabled);
+}
+
 void Session::setGraphs(bool enabled) {
     graphs_ = enabled;
     dropGraphs();
@@ -1484,6 +1492,7 @@ FmmOperator &Session::fmmOperator(const hs_numerics &o, double tuneK, double tun
         fmm_ = std::make_unique<FmmOperator>(space_, st);
         fmm_->setGraphs(graphs_);
         fmm_->setHfThreshold(planeWaveThreshold_);
+        fmm_->setGroupedM2l(groupedM2l_);
         fmmSettings_ = st;
     }
     return *fmm_;
@@ -1551,6 +1560,7 @@ FmmOperator &Session::fmmInnerOperator(const hs_numerics &o) {
         fmmInner_ = std::make_unique<FmmOperator>(space_, fmmSettings_);
         fmmInner_->setFp32(true);
         fmmInner_->setGraphs(graphs_);
+        fmmInner_->setGroupedM2l(groupedM2l_);
         fmmInnerSettings_ = fmmSettings_;
     }
     (void)o;

@@ -92,6 +92,7 @@ class Session {
     // apply as captured CUDA graphs (on by default); graph launches so far.
     void setGraphs(bool enabled);
     void setPlaneWaveThreshold(double threshold);
+    void setGroupedM2l(bool enabled);
     uint64_t graphLaunches() const { return graphLaunches_; }
     // Device bytes a solve may hold beyond the resident geometry and plan
     // (0: 60 % of free memory); bounds the frequency batch.
@@ -140,6 +141,7 @@ class Session {
     uint64_t generation_ = 0, graphLaunches_ = 0;
     bool graphs_ = true;
     double planeWaveThreshold_ = 8.0;
+    bool groupedM2l_ = true;
 
     MeshInput mesh_;
     V3 origin_{};

@@ -310,6 +310,14 @@ hs_status hs_bem_debug_fmm_selftest(double *error);
  * rotational. Applies to the FP64 operator; the mixed form's FP32 inner
  * operator stays rotational. */
 hs_status hs_bem_session_set_plane_wave_threshold(hs_bem_session *session, double threshold);
+/* Rotational M2L schedule of the fast-multipole operators: grouped by
+ * translation class (enabled != 0, the default: the links sharing a rotation
+ * and a coaxial table are translated together, each into its own slot, and the
+ * slots summed per target in link order) or one CTA per target node walking
+ * its links (enabled == 0). Both give the same operator to rounding; the
+ * switch exists for tests and measurements. The reference's M2L batches its
+ * chunks under graphs (support_m2l_graph.hpp:52-78). */
+hs_status hs_bem_session_set_fmm_grouped_m2l(hs_bem_session *session, int enabled);
 /* Acceptance audit of fast-multipole solves (SupportFmmLinearSolver::solve,
  * support_fmm_solve.cu:324-634). mode 0 (default), the reference's policy:
  * where assembling the dense system costs less than two expansion operators

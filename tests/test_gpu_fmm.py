@@ -184,6 +184,38 @@ def test_scaled_fp32_far_operator_matches_fp64(case, freq):
     assert rel < 2e-5
 
 
+@pytest.mark.parametrize("precision, freq", [("fp64", 2000.0), ("fp64", 6000.0), ("mixed", 2000.0)])
+def test_grouped_m2l_equals_per_target_m2l(precision, freq):
+    """The rotational M2L grouped by translation class (chunks of links sharing a
+    Wigner block and a coaxial table, per-link slots summed per target in link
+    order) against one CTA per target walking its links: the same operator to the
+    rounding of the arithmetic, and a solve through either meets the same result."""
+    mesh = meshes.exponential_horn(h=0.0128, seed=5)
+    k = 2 * np.pi * freq / 343.0
+    rng = np.random.default_rng(7)
+    p = rng.normal(size=mesh.vertex_count) + 1j * rng.normal(size=mesh.vertex_count)
+    numerics = hs.BemNumerics(precision=precision)
+    req = lambda: hs.BemRequest(
+        frequencies=[freq], observers=[(0.0, 0.0, 1.0)],
+        excitations=[hs.BemExcitation("throat", [hs.FaceVelocity(meshes.HORN_THROAT, 1.0)])],
+        numerics=hs.BemNumerics(precision=precision, acceleration="fast_multipole", relative_residual_tolerance=1e-6))
+    with hs.CudaBemSolver(mesh) as solver:
+        solver.set_plane_wave_threshold(1e12)  # every level rotational
+        grouped, _, _, levels = solver.debug_fmm_far(numerics, k, 1e-8, p)
+        g_solve = solver.solve(req())
+        solver.set_fmm_grouped_m2l(False)
+        per_target, _, _, _ = solver.debug_fmm_far(numerics, k, 1e-8, p)
+        t_solve = solver.solve(req())
+    rel = np.linalg.norm(grouped - per_target) / np.linalg.norm(per_target)
+    a, b = g_solve.frequencies[0].excitations[0], t_solve.frequencies[0].excitations[0]
+    sol = np.linalg.norm(a.boundary.pressure_trace - b.boundary.pressure_trace) / np.linalg.norm(
+        b.boundary.pressure_trace)
+    print(precision, freq, "orders", levels[:, 1].tolist(), "grouped vs per-target", rel, "solutions", sol)
+    # FP64: same products, summed in another order; FP32: the same at FP32 rounding
+    assert rel < (1e-13 if precision == "fp64" else 1e-6)
+    assert a.boundary_residual <= 1e-6 and b.boundary_residual <= 1e-6 and sol < 1e-6
+
+
 @pytest.mark.parametrize("case, freqs", [("icosphere3", [150.0, 2500.0]), ("horn", [300.0, 2000.0])])
 def test_mixed_fast_multipole_matches_dense(case, freqs):
     """The precision form of the fast multipole: GMRES-IR whose Krylov cycles run
