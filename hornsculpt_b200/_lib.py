@@ -115,6 +115,8 @@ def load():
         "hs_result_normal_derivative": (C.c_int, [_P, C.c_size_t, C.c_size_t, _P]),
         "hs_result_observer_pressure": (C.c_int, [_P, C.c_size_t, C.c_size_t, _P]),
         "hs_result_impedances": (C.c_int, [_P, C.c_size_t, C.c_size_t, _P]),
+        "hs_result_copy_all": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(hs_excitation_info),
+                                         C.POINTER(hs_frequency_info)]),
         "hs_result_free": (None, [_P]),
         "hs_device_description": (C.c_int, [C.c_char_p, C.c_size_t]),
         "hs_bem_session_set_profiling": (C.c_int, [_P, C.c_int32]),

@@ -418,31 +418,35 @@ class CudaBemSolver:
         T = lib.hs_result_triangle_count(out)
         N = lib.hs_result_pressure_dof_count(out)
         O = lib.hs_result_observer_count(out)
+        # one copy of the whole result; the per-frequency arrays are views of it
+        traces = np.empty((F, E, N), np.complex128)
+        surface = np.empty((F, E, T), np.complex128)
+        normal = np.empty((F, E, T), np.complex128)
+        observers = np.empty((F, E, O), np.complex128)
+        xinfo = (_lib.hs_excitation_info * max(F * E, 1))()
+        finfo = (_lib.hs_frequency_info * max(F, 1))()
+        _lib.check(lib.hs_result_copy_all(out, traces.ctypes.data, surface.ctypes.data, normal.ctypes.data,
+                                          observers.ctypes.data if O else None, xinfo, finfo))
         frames = []
         for f in range(F):
-            fi = _lib.hs_frequency_info()
-            _lib.check(lib.hs_result_frequency_info(out, f, C.byref(fi)))
+            fi = finfo[f]
             excs = []
             for e in range(E):
-                info = _lib.hs_excitation_info()
-                _lib.check(lib.hs_result_excitation_info(out, f, e, C.byref(info)))
-                tr, sp, nd, ob = np.zeros(2 * N), np.zeros(2 * T), np.zeros(2 * T), np.zeros(max(2 * O, 2))
-                _lib.check(lib.hs_result_pressure_trace(out, f, e, tr.ctypes.data))
-                _lib.check(lib.hs_result_surface_pressure(out, f, e, sp.ctypes.data))
-                _lib.check(lib.hs_result_normal_derivative(out, f, e, nd.ctypes.data))
-                _lib.check(lib.hs_result_observer_pressure(out, f, e, ob.ctypes.data))
-                imp = (_lib.hs_face_impedance * max(info.impedance_count, 1))()
-                _lib.check(lib.hs_result_impedances(out, f, e, imp))
-                impedances = [FaceImpedance(x.face_id, x.area, complex(*x.mean_pressure), complex(*x.volume_velocity),
-                                            complex(*x.volume_impedance)) for x in imp[: info.impedance_count]]
+                info = xinfo[f * E + e]
+                impedances = []
+                if info.impedance_count:
+                    imp = (_lib.hs_face_impedance * info.impedance_count)()
+                    _lib.check(lib.hs_result_impedances(out, f, e, imp))
+                    impedances = [FaceImpedance(x.face_id, x.area, complex(*x.mean_pressure),
+                                                complex(*x.volume_velocity), complex(*x.volume_impedance)) for x in imp]
                 excs.append(BemExcitationResult(
-                    name=request.excitations[e].name, observer_pressure=_cplx(ob[: 2 * O]), impedances=impedances,
+                    name=request.excitations[e].name, observer_pressure=observers[f, e], impedances=impedances,
                     refinement_steps=info.refinement_steps, iterations=info.iterations,
                     boundary_residual=info.boundary_residual,
                     field_quadrature_comparison_degree=info.field_comparison_degree,
                     field_quadrature_verification_degree=info.field_verification_degree,
                     field_quadrature_discrepancy=info.field_discrepancy,
-                    boundary=BemBoundaryData(_cplx(sp), _cplx(tr), _cplx(nd))))
+                    boundary=BemBoundaryData(surface[f, e], traces[f, e], normal[f, e])))
             frames.append(BemFrequencyResult(fi.frequency, excs, fi.assembly_ms, fi.solve_ms, fi.factorization_ms,
                                              fi.triangular_solve_ms, fi.field_ms, fi.residual_check_ms,
                                              fi.interaction_plan_ms, bool(fi.interaction_plan_reused)))

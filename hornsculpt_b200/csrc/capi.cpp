@@ -215,6 +215,34 @@ hs_status hs_result_observer_pressure(const hs_result *r, size_t f, size_t e, do
     const ExcitationResult *x = excitation(r, f, e);
     return x ? copyComplex(x->observer, out) : fail(HS_E_INVALID, "Result index out of range.");
 }
+hs_status hs_result_copy_all(const hs_result *r, double *traces, double *surface, double *normal, double *observers,
+                             hs_excitation_info *excitation_infos, hs_frequency_info *frequency_infos) {
+    if (!r || !r->impl)
+        return fail(HS_E_INVALID, "Result handle is null.");
+    const auto &fs = r->impl->frequencies;
+    const size_t E = r->impl->E, N = r->impl->N, T = r->impl->T, O = r->impl->O;
+    for (size_t f = 0; f < fs.size(); ++f) {
+        if (frequency_infos)
+            frequency_infos[f] = fs[f].info;
+        for (size_t e = 0; e < E; ++e) {
+            const ExcitationResult *x = excitation(r, f, e);
+            if (!x)
+                return fail(HS_E_INVALID, "Result index out of range.");
+            const size_t q = f * E + e;
+            if (traces)
+                copyComplex(x->trace, traces + 2 * q * N);
+            if (surface)
+                copyComplex(x->surface, surface + 2 * q * T);
+            if (normal)
+                copyComplex(x->normalDerivative, normal + 2 * q * T);
+            if (observers)
+                copyComplex(x->observer, observers + 2 * q * O);
+            if (excitation_infos)
+                hs_result_excitation_info(r, f, e, excitation_infos + q);
+        }
+    }
+    return HS_OK;
+}
 hs_status hs_result_impedances(const hs_result *r, size_t f, size_t e, hs_face_impedance *out) {
     const ExcitationResult *x = excitation(r, f, e);
     if (!x || (!out && !x->impedances.empty()))

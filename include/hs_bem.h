@@ -198,6 +198,12 @@ hs_status hs_result_surface_pressure(const hs_result *r, size_t f, size_t e, dou
 hs_status hs_result_normal_derivative(const hs_result *r, size_t f, size_t e, double *out);
 hs_status hs_result_observer_pressure(const hs_result *r, size_t f, size_t e, double *out);
 hs_status hs_result_impedances(const hs_result *r, size_t f, size_t e, hs_face_impedance *out);
+/* The whole result in one call, [frequency][excitation] order with interleaved
+ * complex values: traces F*E*N, surface and normal F*E*T, observers F*E*O
+ * complex values, excitation infos F*E, frequency infos F. A null pointer
+ * skips that part. The per-item getters above return the same values. */
+hs_status hs_result_copy_all(const hs_result *r, double *traces, double *surface, double *normal, double *observers,
+                             hs_excitation_info *excitation_infos, hs_frequency_info *frequency_infos);
 /* Coupled solves: Z (ports x ports complex), port flows and pressures (ports
  * complex each) of frequency f; ports receives the count (0 for uncoupled
  * results). Any output pointer may be NULL. */
