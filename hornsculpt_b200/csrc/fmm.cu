@@ -166,7 +166,7 @@ __device__ __forceinline__ double2 solidR(const PointTable &t, int n, int m) {
     return make_double2(sg * a * e.x, -sg * a * e.y);
 }
 __device__ __forceinline__ void decode(int k, int &n, int &m) {
-    n = int(sqrt(double(k)));
+    n = int(sqrtf(float(k)));  // corrected below (k < 2^24)
     while (n * n > k)
         --n;
     while ((n + 1) * (n + 1) <= k)
@@ -522,31 +522,47 @@ __global__ void __launch_bounds__(256) m2lGroupKernel(const uint2 *__restrict__ 
     }
     __syncthreads();
     const int tiles = (C + kGroupTile - 1) / kGroupTile;
+    // Rotations in items of two rows of one degree n (rows n^2 + 2q and + 1; the
+    // odd last row of a degree alone) by kGroupTile columns: each staged value
+    // read serves both rows. Pair q of degree n is item n (n + 1) / 2 + q.
+    const int pairs = (p + 1) * (p + 2) / 2;
     // forward rotation: B[n, m'] = sum_m A[n, m] d^n[m, m']
-    for (int e = threadIdx.x; e < tiles * nc; e += blockDim.x) {
-        const int tile = e / nc, kk = e - tile * nc, c0 = tile * kGroupTile;
-        int n, mp;
-        decode(kk, n, mp);
+    for (int e = threadIdx.x; e < tiles * pairs; e += blockDim.x) {
+        const int tile = e / pairs, pq = e - tile * pairs, c0 = tile * kGroupTile;
+        int n = int((sqrtf(8.f * pq + 1.f) - 1.f) * .5f);
+        while (n * (n + 1) / 2 > pq)
+            --n;
+        while ((n + 1) * (n + 2) / 2 <= pq)
+            ++n;
+        const int r0 = 2 * (pq - n * (n + 1) / 2);  // row m' + n of the first row
+        const bool two = r0 + 1 < 2 * n + 1;
         const int w = 2 * n + 1;
-        const R *d = dtab + wignerOffset(n) + (mp + n);
+        const R *d = dtab + wignerOffset(n) + r0;
         const CT *x = bufA + size_t(n) * n * cpad + c0;
-        CT acc[kGroupTile];
+        CT a0[kGroupTile], a1[kGroupTile];
 #pragma unroll
         for (int c = 0; c < kGroupTile; ++c)
-            acc[c] = mkc<R>(0, 0);
+            a0[c] = a1[c] = mkc<R>(0, 0);
+#pragma unroll 2
         for (int j = 0; j < w; ++j) {
-            const R dv = d[size_t(j) * w];
+            const R d0 = d[size_t(j) * w], d1 = two ? d[size_t(j) * w + 1] : R(0);
 #pragma unroll
             for (int c = 0; c < kGroupTile; ++c) {
                 const CT v = x[size_t(j) * cpad + c];
-                acc[c].x += v.x * dv;
-                acc[c].y += v.y * dv;
+                a0[c].x += v.x * d0;
+                a0[c].y += v.y * d0;
+                a1[c].x += v.x * d1;
+                a1[c].y += v.y * d1;
             }
         }
+        CT *o = bufB + size_t(n * n + r0) * cpad + c0;
 #pragma unroll
         for (int c = 0; c < kGroupTile; ++c)
-            if (c0 + c < C)
-                bufB[size_t(kk) * cpad + c0 + c] = acc[c];
+            if (c0 + c < C) {
+                o[c] = a0[c];
+                if (two)
+                    o[cpad + c] = a1[c];
+            }
     }
     __syncthreads();
     // coaxial translation per |m| (outputs in m-major order, so a warp reads
@@ -576,30 +592,43 @@ __global__ void __launch_bounds__(256) m2lGroupKernel(const uint2 *__restrict__ 
     }
     __syncthreads();
     // back rotation: B[n, m1] = sum_m d^n[m1, m] A[n, m]
-    for (int e = threadIdx.x; e < tiles * nc; e += blockDim.x) {
-        const int tile = e / nc, kk = e - tile * nc, c0 = tile * kGroupTile;
-        int n, m1;
-        decode(kk, n, m1);
+    for (int e = threadIdx.x; e < tiles * pairs; e += blockDim.x) {
+        const int tile = e / pairs, pq = e - tile * pairs, c0 = tile * kGroupTile;
+        int n = int((sqrtf(8.f * pq + 1.f) - 1.f) * .5f);
+        while (n * (n + 1) / 2 > pq)
+            --n;
+        while ((n + 1) * (n + 2) / 2 <= pq)
+            ++n;
+        const int r0 = 2 * (pq - n * (n + 1) / 2);  // row m1 + n of the first row
+        const bool two = r0 + 1 < 2 * n + 1;
         const int w = 2 * n + 1;
-        const R *d = dtab + wignerOffset(n) + size_t(m1 + n) * w;
+        const R *d0p = dtab + wignerOffset(n) + size_t(r0) * w;
+        const R *d1p = two ? d0p + w : d0p;
         const CT *x = bufA + size_t(n) * n * cpad + c0;
-        CT acc[kGroupTile];
+        CT a0[kGroupTile], a1[kGroupTile];
 #pragma unroll
         for (int c = 0; c < kGroupTile; ++c)
-            acc[c] = mkc<R>(0, 0);
+            a0[c] = a1[c] = mkc<R>(0, 0);
+#pragma unroll 2
         for (int j = 0; j < w; ++j) {
-            const R dv = d[j];
+            const R d0 = d0p[j], d1 = d1p[j];
 #pragma unroll
             for (int c = 0; c < kGroupTile; ++c) {
                 const CT v = x[size_t(j) * cpad + c];
-                acc[c].x += v.x * dv;
-                acc[c].y += v.y * dv;
+                a0[c].x += v.x * d0;
+                a0[c].y += v.y * d0;
+                a1[c].x += v.x * d1;
+                a1[c].y += v.y * d1;
             }
         }
+        CT *o = bufB + size_t(n * n + r0) * cpad + c0;
 #pragma unroll
         for (int c = 0; c < kGroupTile; ++c)
-            if (c0 + c < C)
-                bufB[size_t(kk) * cpad + c0 + c] = acc[c];
+            if (c0 + c < C) {
+                o[c] = a0[c];
+                if (two)
+                    o[cpad + c] = a1[c];
+            }
     }
     __syncthreads();
     // each link's contribution with the conjugate phase, into its own slot
