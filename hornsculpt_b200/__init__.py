@@ -7,7 +7,7 @@ from .bem import (AcousticMedium, BemBoundaryData, BemCancelled, BemError, BemEx
                   BemFrequencyResult, BemNumerics, BemRequest, BemResult, BemServer, BemUnsupported, CudaBemSolver,
                   CudaStorageOptions, FaceImpedance, FaceVelocity, FarFieldObservation, FastMultipoleSettings,
                   FieldPointStatus, PressureFieldSample, PressureFieldSettings, ServeOptions, ServeTiming, StopToken,
-                  autotune_clear, autotune_enable, autotune_report, debug_lu_factor, host_plan)
+                  autotune_clear, autotune_enable, autotune_report, debug_lu_factor, device_plan, host_plan)
 from .coupling import BemPort, CouplingBasis, PortSolution, coupled_solve, make_coupling_basis, port_impedance
 from .fixtures import read_fixture, write_fixture
 from .study import StudyRequest, complex_result_document, describe_study_capabilities, parse_study_request
@@ -19,7 +19,7 @@ __all__ = [
     "BemFrequencyResult", "BemNumerics", "BemRequest", "BemResult", "BemServer", "BemUnsupported", "CudaBemSolver",
     "CudaStorageOptions", "FaceImpedance", "FaceVelocity", "FarFieldObservation", "FastMultipoleSettings",
     "FieldPointStatus", "PressureFieldSample", "PressureFieldSettings",
-    "ServeOptions", "ServeTiming", "StopToken", "autotune_clear", "autotune_enable", "autotune_report", "debug_lu_factor", "host_plan", "DRIVEN", "WALL", "SurfaceMesh", "exponential_horn",
+    "ServeOptions", "ServeTiming", "StopToken", "autotune_clear", "autotune_enable", "autotune_report", "debug_lu_factor", "device_plan", "host_plan", "DRIVEN", "WALL", "SurfaceMesh", "exponential_horn",
     "icosphere", "octahedral_sphere", "revolved_sphere", "scalene_tetrahedron", "read_fixture", "write_fixture", "StudyRequest", "parse_study_request",
     "describe_study_capabilities", "complex_result_document", "BemPort", "CouplingBasis", "PortSolution",
     "coupled_solve", "make_coupling_basis", "port_impedance",

@@ -131,6 +131,8 @@ def load():
         "hs_bem_session_graph_launches": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
         "hs_bem_debug_plan": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, C.POINTER(hs_numerics), C.c_double, _P, _P,
                                         _P, _P, _P, _P, _P]),
+        "hs_bem_debug_plan_device": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, C.POINTER(hs_numerics), C.c_double,
+                                               C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P]),
         "hs_bem_observer_field_noalloc": (C.c_int, [_P, C.c_size_t, _P, C.c_size_t, _P, _P, _P, C.c_size_t, C.c_double,
                                                     C.c_uint32, C.c_int32, _P, C.c_double, C.c_double, C.c_uint32,
                                                     _P, _P]),
@@ -141,6 +143,8 @@ def load():
         "hs_bem_debug_fmm_selftest": (C.c_int, [C.POINTER(C.c_double)]),
         "hs_bem_session_set_plane_wave_threshold": (C.c_int, [_P, C.c_double]),
         "hs_bem_session_set_fmm_grouped_m2l": (C.c_int, [_P, C.c_int]),
+        "hs_bem_session_set_planner": (C.c_int, [_P, C.c_uint32]),
+        "hs_bem_session_plan_stats": (C.c_int, [_P, _P]),
         "hs_bem_session_set_fmm_audit": (C.c_int, [_P, C.c_uint32]),
         "hs_bem_session_fmm_audit_counts": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "hs_bem_debug_lu": (C.c_int, [C.c_uint32, C.c_size_t, C.c_size_t, _P, _P, _P, C.POINTER(C.c_int32)]),

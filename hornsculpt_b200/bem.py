@@ -255,6 +255,17 @@ class CudaBemSolver:
         """k x shortest M2L distance from which a fast-multipole level translates in the plane-wave form."""
         _lib.check(self._lib.hs_bem_session_set_plane_wave_threshold(self._handle, threshold))
 
+    def set_planner(self, planner: str) -> None:
+        """Interaction planner: "device" (default; the pair refinement on the GPU) or "host" (host threads,
+        like the reference). Both give the same plan bit for bit."""
+        _lib.check(self._lib.hs_bem_session_set_planner(self._handle, {"device": 0, "host": 1}[planner]))
+
+    def plan_stats(self) -> dict:
+        """Statistics of the session's last device plan (see device_plan)."""
+        stats = (C.c_double * 6)()
+        _lib.check(self._lib.hs_bem_session_plan_stats(self._handle, stats))
+        return dict(zip(PLAN_STATS, list(stats)))
+
     def set_fmm_grouped_m2l(self, enabled: bool) -> None:
         """Rotational M2L grouped by translation class (default) or one CTA per target node."""
         _lib.check(self._lib.hs_bem_session_set_fmm_grouped_m2l(self._handle, 1 if enabled else 0))
@@ -569,6 +580,18 @@ class BemServer:
         self.close()
 
 
+def _plan_arrays(mesh: SurfaceMesh, sizes) -> dict:
+    nt, nn, npch, nw, ntr, depth = list(sizes)
+    return dict(touching=np.zeros((nt, 9), np.uint32), near=np.zeros((nn, 5), np.uint32),
+                patches=np.zeros((npch, 22)), whole=np.zeros(nw, np.uint8),
+                offsets=np.zeros(mesh.triangle_count + 1, np.uint32), trials=np.zeros(ntr, np.uint32), depth=depth)
+
+
+def _plan_pointers(out: dict):
+    return (out["touching"].ctypes.data, out["near"].ctypes.data, out["patches"].ctypes.data,
+            out["whole"].ctypes.data, out["offsets"].ctypes.data, out["trials"].ctypes.data)
+
+
 def host_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float) -> dict:
     """The library's host interaction plan of a mesh (no device needed)."""
     lib = _lib.load()
@@ -577,13 +600,29 @@ def host_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float) -> dict:
     args = (mesh.vertices.ctypes.data, mesh.vertex_count, mesh.triangles.ctypes.data, mesh.triangle_count, C.byref(n),
             max_k, sizes)
     _lib.check(lib.hs_bem_debug_plan(*args, None, None, None, None, None, None))
-    nt, nn, npch, nw, ntr, depth = list(sizes)
-    out = dict(touching=np.zeros((nt, 9), np.uint32), near=np.zeros((nn, 5), np.uint32),
-               patches=np.zeros((npch, 22)), whole=np.zeros(nw, np.uint8),
-               offsets=np.zeros(mesh.triangle_count + 1, np.uint32), trials=np.zeros(ntr, np.uint32), depth=depth)
-    _lib.check(lib.hs_bem_debug_plan(*args, out["touching"].ctypes.data, out["near"].ctypes.data,
-                                     out["patches"].ctypes.data, out["whole"].ctypes.data, out["offsets"].ctypes.data,
-                                     out["trials"].ctypes.data))
+    out = _plan_arrays(mesh, sizes)
+    _lib.check(lib.hs_bem_debug_plan(*args, *_plan_pointers(out)))
+    return out
+
+
+PLAN_STATS = ("device_pairs", "projected_pairs", "flagged_pairs", "whole_panel_pairs", "device_ms", "host_ms")
+
+
+def device_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float, emulate: bool = False) -> dict:
+    """The interaction plan from the device planner (on the current CUDA
+    device, or with emulate=True its algorithm run on the host), with its
+    statistics under "stats". The plan is computed once and read out once;
+    it equals host_plan's bit for bit."""
+    lib = _lib.load()
+    n = numerics.to_c()
+    sizes = (C.c_size_t * 6)()
+    stats = (C.c_double * 6)()
+    args = (mesh.vertices.ctypes.data, mesh.vertex_count, mesh.triangles.ctypes.data, mesh.triangle_count, C.byref(n),
+            max_k, 1 if emulate else 0, stats, sizes)
+    _lib.check(lib.hs_bem_debug_plan_device(*args, None, None, None, None, None, None))
+    out = _plan_arrays(mesh, sizes)
+    _lib.check(lib.hs_bem_debug_plan_device(*args, *_plan_pointers(out)))
+    out["stats"] = dict(zip(PLAN_STATS, list(stats)))
     return out
 
 

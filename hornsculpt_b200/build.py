@@ -19,6 +19,9 @@ INCLUDE = ROOT / "include"
 BUILD = PKG / "_build"
 LIBRARY = PKG / "libhs_bem.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Sources whose floating-point operations must match the host planner's one
+# for one: no multiply-add contraction (explicit fma() only).
+NO_CONTRACTION = {"plan_device.cu"}
 
 
 def _nvcc() -> str:
@@ -42,6 +45,8 @@ def _compile(src: pathlib.Path, verbose_ptxas: bool) -> pathlib.Path:
            str(CSRC), "-c", str(src), "-o", str(obj)]
     if src.suffix == ".cu" and verbose_ptxas:
         cmd += ["-Xptxas", "-v"]
+    if src.name in NO_CONTRACTION:
+        cmd += ["-fmad=false"]
     subprocess.run(cmd, check=True)
     return obj
 

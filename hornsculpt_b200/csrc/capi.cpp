@@ -2,6 +2,7 @@
 // layer become hs_status codes plus a thread-local message.
 #include "hs_bem.h"
 #include "autotune.hpp"
+#include "plan_device.hpp"
 #include "serve.hpp"
 #include "session.hpp"
 
@@ -397,6 +398,70 @@ hs_status hs_bem_session_profile(const hs_bem_session *s, char *names, size_t na
     });
 }
 
+namespace {
+// Writes a plan into hs_bem_debug_plan's output layout.
+void writePlan(const hsb::Plan &p, size_t *sizes, uint32_t *touching, uint32_t *near, double *patches,
+               uint8_t *whole, uint32_t *near_offsets, uint32_t *near_trials) {
+    sizes[0] = p.touching.size();
+    sizes[1] = p.near.size();
+    sizes[2] = p.patches.size();
+    sizes[3] = p.wholePanelDegrees.size();
+    sizes[4] = p.nearTrials.size();
+    sizes[5] = p.maxDepth;
+    if (touching)
+        for (const auto &j : p.touching) {
+            *touching++ = j.test;
+            *touching++ = j.trial;
+            *touching++ = j.perm.topology;
+            for (int i = 0; i < 3; ++i)
+                *touching++ = j.perm.test[i];
+            for (int i = 0; i < 3; ++i)
+                *touching++ = j.perm.trial[i];
+        }
+    if (near)
+        for (const auto &j : p.near) {
+            *near++ = j.test;
+            *near++ = j.trial;
+            *near++ = j.first;
+            *near++ = j.count;
+            *near++ = j.swap;
+        }
+    if (patches)
+        for (const auto &q : p.patches) {
+            for (int i = 0; i < 9; ++i)
+                *patches++ = q.test[i];
+            for (int i = 0; i < 9; ++i)
+                *patches++ = q.trial[i];
+            *patches++ = q.areaFraction;
+            *patches++ = q.degree;
+            *patches++ = q.projection;
+            *patches++ = q.intervals;
+        }
+    if (whole && !p.wholePanelDegrees.empty())
+        std::memcpy(whole, p.wholePanelDegrees.data(), p.wholePanelDegrees.size());
+    if (near_offsets)
+        std::memcpy(near_offsets, p.nearOffsets.data(), p.nearOffsets.size() * 4);
+    if (near_trials && !p.nearTrials.empty())
+        std::memcpy(near_trials, p.nearTrials.data(), p.nearTrials.size() * 4);
+}
+
+hsb::Space debugSpace(const double *vertices, size_t vertex_count, const uint32_t *triangles, size_t triangle_count) {
+    MeshInput mesh;
+    const V3 origin{vertices[0], vertices[1], vertices[2]};
+    for (size_t i = 0; i < vertex_count; ++i)
+        mesh.vertices.push_back(V3{vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]} - origin);
+    mesh.triangles.assign(triangles, triangles + 3 * triangle_count);
+    mesh.faces.assign(triangle_count, 0);
+    mesh.driven.assign(triangle_count, 0);
+    return buildSpace(mesh);
+}
+
+hsb::PlanSettings planSettings(const hs_numerics *n) {
+    return hsb::PlanSettings{n->quadrature_order, n->singular_order, n->near_distance_ratio,
+                             n->near_relative_tolerance, n->near_maximum_depth};
+}
+}  // namespace
+
 hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const uint32_t *triangles,
                             size_t triangle_count, const hs_numerics *numerics, double max_k, size_t *sizes,
                             uint32_t *touching, uint32_t *near, double *patches, uint8_t *whole,
@@ -404,60 +469,37 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
     if (!vertices || !vertex_count || !triangles || !triangle_count || !numerics || !sizes)
         return fail(HS_E_INVALID, "Mesh, numerics and sizes must be non-null.");
     return guarded([&]() {
-        MeshInput mesh;
-        const V3 origin{vertices[0], vertices[1], vertices[2]};
-        for (size_t i = 0; i < vertex_count; ++i)
-            mesh.vertices.push_back(V3{vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2]} - origin);
-        mesh.triangles.assign(triangles, triangles + 3 * triangle_count);
-        mesh.faces.assign(triangle_count, 0);
-        mesh.driven.assign(triangle_count, 0);
-        const Space space = buildSpace(mesh);
-        const Plan p = makePlan(space,
-                                PlanSettings{numerics->quadrature_order, numerics->singular_order,
-                                             numerics->near_distance_ratio, numerics->near_relative_tolerance,
-                                             numerics->near_maximum_depth},
-                                max_k, 0, nullptr);
-        sizes[0] = p.touching.size();
-        sizes[1] = p.near.size();
-        sizes[2] = p.patches.size();
-        sizes[3] = p.wholePanelDegrees.size();
-        sizes[4] = p.nearTrials.size();
-        sizes[5] = p.maxDepth;
-        if (touching)
-            for (const auto &j : p.touching) {
-                *touching++ = j.test;
-                *touching++ = j.trial;
-                *touching++ = j.perm.topology;
-                for (int i = 0; i < 3; ++i)
-                    *touching++ = j.perm.test[i];
-                for (int i = 0; i < 3; ++i)
-                    *touching++ = j.perm.trial[i];
-            }
-        if (near)
-            for (const auto &j : p.near) {
-                *near++ = j.test;
-                *near++ = j.trial;
-                *near++ = j.first;
-                *near++ = j.count;
-                *near++ = j.swap;
-            }
-        if (patches)
-            for (const auto &q : p.patches) {
-                for (int i = 0; i < 9; ++i)
-                    *patches++ = q.test[i];
-                for (int i = 0; i < 9; ++i)
-                    *patches++ = q.trial[i];
-                *patches++ = q.areaFraction;
-                *patches++ = q.degree;
-                *patches++ = q.projection;
-                *patches++ = q.intervals;
-            }
-        if (whole && !p.wholePanelDegrees.empty())
-            std::memcpy(whole, p.wholePanelDegrees.data(), p.wholePanelDegrees.size());
-        if (near_offsets)
-            std::memcpy(near_offsets, p.nearOffsets.data(), p.nearOffsets.size() * 4);
-        if (near_trials && !p.nearTrials.empty())
-            std::memcpy(near_trials, p.nearTrials.data(), p.nearTrials.size() * 4);
+        const Space space = debugSpace(vertices, vertex_count, triangles, triangle_count);
+        const Plan p = makePlan(space, planSettings(numerics), max_k, 0, nullptr);
+        writePlan(p, sizes, touching, near, patches, whole, near_offsets, near_trials);
+    });
+}
+
+hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                   size_t triangle_count, const hs_numerics *numerics, double max_k, uint32_t mode,
+                                   double *stats, size_t *sizes, uint32_t *touching, uint32_t *near,
+                                   double *patches, uint8_t *whole, uint32_t *near_offsets, uint32_t *near_trials) {
+    if (!vertices || !vertex_count || !triangles || !triangle_count || !numerics || !sizes || mode > 1)
+        return fail(HS_E_INVALID, "Mesh, numerics and sizes must be non-null and the mode 0 or 1.");
+    return guarded([&]() {
+        const Space space = debugSpace(vertices, vertex_count, triangles, triangle_count);
+        DevicePlanStats st;
+        const Plan p = makePlanOnDevice(space, planSettings(numerics), max_k, nullptr, nullptr, &st, mode == 1);
+        if (mode == 0)
+        {
+            const cudaError_t e = cudaDeviceSynchronize();
+            if (e != cudaSuccess)
+                throw CudaError(std::string("CUDA synchronization: ") + cudaGetErrorString(e));
+        }
+        if (stats) {
+            stats[0] = double(st.devicePairs);
+            stats[1] = double(st.projectedPairs);
+            stats[2] = double(st.flaggedPairs);
+            stats[3] = double(st.wholePanelPairs);
+            stats[4] = st.deviceMs;
+            stats[5] = st.hostMs;
+        }
+        writePlan(p, sizes, touching, near, patches, whole, near_offsets, near_trials);
     });
 }
 
@@ -524,6 +566,30 @@ hs_status hs_bem_session_set_plane_wave_threshold(hs_bem_session *s, double thre
     return guarded([&]() {
         std::lock_guard<std::mutex> lock(s->impl->mutex);
         s->impl->setPlaneWaveThreshold(threshold);
+    });
+}
+
+hs_status hs_bem_session_set_planner(hs_bem_session *s, uint32_t planner) {
+    if (!s)
+        return fail(HS_E_INVALID, "Session handle is null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        s->impl->setPlanner(planner);
+    });
+}
+
+hs_status hs_bem_session_plan_stats(hs_bem_session *s, double *stats) {
+    if (!s || !stats)
+        return fail(HS_E_INVALID, "Session handle and statistics must be non-null.");
+    return guarded([&]() {
+        std::lock_guard<std::mutex> lock(s->impl->mutex);
+        const DevicePlanStats &st = s->impl->planStats();
+        stats[0] = double(st.devicePairs);
+        stats[1] = double(st.projectedPairs);
+        stats[2] = double(st.flaggedPairs);
+        stats[3] = double(st.wholePanelPairs);
+        stats[4] = st.deviceMs;
+        stats[5] = st.hostMs;
     });
 }
 

@@ -1,0 +1,907 @@
+// Interaction planning on the GPU: pair classification and the adaptive
+// largest-error refinement of tensor-rule near pairs, one warp per pair
+// (interaction_plan.cpp:156-504, pair_quadrature.cpp:143-226, 329-575,
+// 644-683). See plan_device.hpp for how the plan stays bit-identical to the
+// host planner's.
+//
+// This file is compiled with -fmad=false: the geometric decisions
+// (qualification, near and projection tests, diameters, halving) and the
+// sample points repeat the host planner's IEEE operations exactly. Only the
+// moment sums use explicit fma(), and their rounding is covered by the bounds
+// below.
+#include "plan_device.hpp"
+#include "planner_geom.cuh"
+
+#include <math.h>
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+namespace hsb {
+namespace {
+
+constexpr uint32_t kLeafCap = 2048;  // leaves held per warp (pending + at the depth limit + requested)
+constexpr int kRulePoints = 64;      // largest rule (collapsed tensor Gauss degree 14)
+constexpr int kPts = 7;              // per point: barycentrics (3), local point (3), weight
+constexpr double kUnit = 0x1p-53;    // unit roundoff
+// Margin factor on every rounding bound: the bounds below are first-order
+// worst cases; a decision is trusted only when its gap is four times larger.
+constexpr double kSafety = 4;
+
+enum : uint8_t { kSkip = 0, kOnDevice = 1, kProjected = 2 };
+enum : int { kPairRule = 0, kPairWhole = 1, kPairHost = 2 };
+
+struct LeafHdr {
+    Sub a, b;
+    double error, errB, intB, da, db, pad;
+    uint32_t depth, degree;
+};
+
+struct PairRecord {
+    uint32_t first, second, patchFirst, count, maxDepth, pad;
+    double relError;
+};
+
+struct RuleTables {
+    const double *pts[4];  // (b0, b1, b2, w) rows of the degree 6, 8, 12 and 14 rules
+    int n[4];
+};
+
+struct ClassifyParams {
+    const HostPanel *panels;
+    const Bounds *bounds;
+    double k, tol, nearRatio;
+    uint32_t regularOrder;
+};
+
+struct AdaptiveParams {
+    const HostPanel *panels;
+    RuleTables rules;
+    double k, tol;
+    uint32_t maxDepth;
+    int allPairs;
+};
+
+// One warp's memory: leaf arena, pending and depth-limit lists, point tables.
+struct WarpMem {
+    LeafHdr *hdr;
+    double *integ;  // kLeafCap x 72: each leaf's moments (36 complex)
+    uint32_t *pend;
+    double *pendErr;
+    uint32_t *atl;
+    double *pts;  // test and trial point tables, 2 x kRulePoints x kPts
+};
+
+struct PairOutput {
+    Patch *pool;
+    unsigned long long poolCap, *poolUsed;
+    PairRecord *records;
+    unsigned long long *recordCount;
+    uint8_t *whole;  // all-pairs mode: unordered pair index -> whole-panel degree
+};
+
+// ---- warp policies: the same pair code runs with 32 lanes on the device and
+// with one lane on the host (test emulation) ----
+struct LaneWarp {
+    static constexpr int W = 1;
+    HS_HD int lane() const { return 0; }
+    HS_HD double max(double x) const { return x; }
+    HS_HD bool any(bool x) const { return x; }
+    HS_HD double bcast(double x, int) const { return x; }
+    HS_HD void sync() const {}
+    HS_HD bool leader() const { return true; }
+};
+
+#if defined(__CUDACC__)
+struct DeviceWarp {
+    static constexpr int W = 32;
+    __device__ int lane() const { return threadIdx.x & 31; }
+    __device__ double max(double x) const {
+        for (int o = 16; o; o >>= 1)
+            x = fmax(x, __shfl_xor_sync(~0u, x, o));
+        return x;
+    }
+    __device__ bool any(bool x) const { return __any_sync(~0u, x); }
+    __device__ double bcast(double x, int src) const { return __shfl_sync(~0u, x, src); }
+    __device__ void sync() const { __syncwarp(); }
+    __device__ bool leader() const { return lane() == 0; }
+};
+#endif
+
+// Per sample the lanes accumulate 72 moment values (36 complex, index
+// 2 (9c + 3i + j) + re/im) and 4 magnitude sums (values 72..75); padded to
+// 128, a reduce-scatter leaves lane l with values [128/W l, 128/W (l+1)).
+constexpr int kValues = 128;
+
+HS_HD void reduceScatter(const LaneWarp &, double *) {}
+#if defined(__CUDACC__)
+template <int HALF> __device__ __forceinline__ void scatterStep(double *acc, int lane, int off) {
+    const bool up = lane & off;
+#pragma unroll
+    for (int v = 0; v < HALF; ++v) {
+        const double send = up ? acc[v] : acc[v + HALF];
+        const double keep = up ? acc[v + HALF] : acc[v];
+        acc[v] = keep + __shfl_xor_sync(~0u, send, off);
+    }
+}
+__device__ void reduceScatter(const DeviceWarp &w, double *acc) {
+    const int lane = w.lane();
+    scatterStep<64>(acc, lane, 16);
+    scatterStep<32>(acc, lane, 8);
+    scatterStep<16>(acc, lane, 4);
+    scatterStep<8>(acc, lane, 2);
+    scatterStep<4>(acc, lane, 1);
+}
+#endif
+
+// Tensor moments of one rule over sub-triangles a (test) and b (trial)
+// (the host's tensorMoments): lane-strided samples, then the reduce-scatter.
+// `own` receives the lane's values; `bad` is set for a coincident point.
+template <class Wp>
+HS_HD void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, const Sub &a, const Sub &b,
+                         const double *rule, int n, double k, double scale, double *pts, double *own, bool &bad) {
+    constexpr int W = Wp::W;
+    for (int q = w.lane(); q < n; q += W) {
+        const double *x = rule + 4 * q;
+        double bt[3] = {0, 0, 0}, bs[3] = {0, 0, 0};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                bt[i] += x[j] * a.v[j][i];
+                bs[i] += x[j] * b.v[j][i];
+            }
+        const V3 lt = localPoint(t, bt), ls = localPoint(s, bs);
+        double *T = pts + kPts * q, *S = pts + kPts * (kRulePoints + q);
+        T[0] = bt[0], T[1] = bt[1], T[2] = bt[2], T[3] = lt.x, T[4] = lt.y, T[5] = lt.z, T[6] = x[3];
+        S[0] = bs[0], S[1] = bs[1], S[2] = bs[2], S[3] = ls.x, S[4] = ls.y, S[5] = ls.z, S[6] = x[3];
+    }
+    w.sync();
+    const V3 origin = t.v[0] - s.v[0];
+    const double fab = a.fraction * b.fraction;
+    double acc[kValues];
+#pragma unroll
+    for (int v = 0; v < kValues; ++v)
+        acc[v] = 0;
+    for (int smp = w.lane(); smp < n * n; smp += W) {
+        const int xi = smp / n, qi = smp - xi * n;
+        const double *T = pts + kPts * xi, *S = pts + kPts * (kRulePoints + qi);
+        const V3 d{origin.x + (T[3] - S[3]), origin.y + (T[4] - S[4]), origin.z + (T[5] - S[5])};
+        const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+        if (!(r > 0)) {
+            bad = true;
+            continue;
+        }
+        double sn, cs;
+        sincos(-k * r, &sn, &cs);  // exp(-i k r)
+        const double ir = 1 / r, gr = cs * ir, gi = sn * ir, kr = k * r, f = scale * ir * ir;
+        const double dr = (-gr + gi * kr) * f, di = (-gr * kr - gi) * f;
+        const double kre[4] = {gr, dr * d.x, dr * d.y, dr * d.z};
+        const double kim[4] = {gi, di * d.x, di * d.y, di * d.z};
+        const double wgt = T[6] * S[6] * fab;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const double wb = wgt * S[j];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double br = kre[c] * wb, bi = kim[c] * wb;
+#pragma unroll
+                for (int i = 0; i < 3; ++i) {
+                    const int v = 2 * (9 * c + 3 * i + j);
+                    acc[v] = fma(T[i], br, acc[v]);
+                    acc[v + 1] = fma(T[i], bi, acc[v + 1]);
+                }
+            }
+        }
+        // magnitude of each channel's terms: |G| = 1/r, |grad G| <= (1 + kr)/r^2
+        const double m0 = wgt * ir, md = wgt * (1 + kr) * f * ir;
+        acc[72] += m0;
+        acc[73] += md * fabs(d.x);
+        acc[74] += md * fabs(d.y);
+        acc[75] += md * fabs(d.z);
+    }
+    w.sync();  // the point tables are rewritten by the next call
+    reduceScatter(w, acc);
+    constexpr int own_n = kValues / W;
+#pragma unroll
+    for (int v = 0; v < own_n; ++v)
+        own[v] = acc[v];
+}
+
+// Embedded-rule estimate of one leaf (the host's estimate(), tensor form):
+// moments of the lower and higher rule, error = max |hi - lo|. Also the
+// bounds on how far the device values can lie from the host's:
+//   per moment value, |device - host| <= (2 m + 64) u A_c for a rule of m
+//   samples, A_c the sum of |terms| of channel c (both sides' summation
+//   errors, at most m u A_c each, and kernel values within 32 u);
+//   errB bounds |error_device - error_host|, intB a moment value.
+template <class Wp>
+HS_HD void estimateLeaf(const Wp &w, const HostPanel &t, const HostPanel &s, LeafHdr &L, const RuleTables &R,
+                        double k, double scale, double *pts, double *hiOwn, double &mnL, bool &bad) {
+    constexpr int own_n = kValues / Wp::W;
+    const int lo = L.degree == 8 ? 0 : 2, hi = lo + 1;
+    double loOwn[own_n];
+    tensorMoments(w, t, s, L.a, L.b, R.pts[lo], R.n[lo], k, scale, pts, loOwn, bad);
+    tensorMoments(w, t, s, L.a, L.b, R.pts[hi], R.n[hi], k, scale, pts, hiOwn, bad);
+    // magnitude sums live in values 72..75
+    const int magLane = 72 / own_n, magOff = 72 - magLane * own_n;
+    double Elo = 0, Ehi = 0;
+    for (int c = 0; c < 4; ++c) {
+        const double al = w.bcast(loOwn[(magOff + c) % own_n], magLane);
+        const double ah = w.bcast(hiOwn[(magOff + c) % own_n], magLane);
+        const double ml = double(R.n[lo]) * R.n[lo], mh = double(R.n[hi]) * R.n[hi];
+        Elo = fmax(Elo, (2 * ml + 64) * kUnit * al);
+        Ehi = fmax(Ehi, (2 * mh + 64) * kUnit * ah);
+    }
+    double dmax = 0, hmax = 0;
+    bool nonFinite = false;
+    const int base = own_n * w.lane();
+    for (int v = 0; v < own_n; v += 2) {
+        if (base + v >= 72)
+            break;
+        const double dr = hiOwn[v] - loOwn[v], di = hiOwn[v + 1] - loOwn[v + 1];
+        const double dab = hypot(dr, di), hab = hypot(hiOwn[v], hiOwn[v + 1]);
+        nonFinite = nonFinite || !isfinite(dab) || !isfinite(hab);
+        dmax = fmax(dmax, dab);
+        hmax = fmax(hmax, hab);
+    }
+    bad = w.any(bad || nonFinite);
+    L.error = w.max(dmax);
+    mnL = w.max(hmax);
+    L.errB = 1.4142135623730951 * (Ehi + Elo) + 8 * kUnit * L.error;
+    L.intB = Ehi;
+}
+
+HS_HD bool separated(double x, double y, double bound) { return fabs(x - y) > kSafety * bound; }
+
+// Top two pending errors: (largest, its list position, second largest, its position).
+struct Top2 {
+    double e1, e2;
+    uint32_t p1, p2;
+};
+template <class Wp> HS_HD Top2 topTwo(const Wp &w, const double *err, uint32_t n) {
+    Top2 t{-1, -1, 0xffffffffu, 0xffffffffu};
+    for (uint32_t i = w.lane(); i < n; i += Wp::W) {
+        const double e = err[i];
+        if (e > t.e1) {
+            t.e2 = t.e1, t.p2 = t.p1;
+            t.e1 = e, t.p1 = i;
+        } else if (e > t.e2) {
+            t.e2 = e, t.p2 = i;
+        }
+    }
+    if (Wp::W > 1)
+        for (int o = 1; o < Wp::W; o <<= 1) {
+            Top2 u;
+#if defined(__CUDA_ARCH__)
+            u.e1 = __shfl_xor_sync(~0u, t.e1, o);
+            u.e2 = __shfl_xor_sync(~0u, t.e2, o);
+            u.p1 = __shfl_xor_sync(~0u, t.p1, o);
+            u.p2 = __shfl_xor_sync(~0u, t.p2, o);
+#else
+            u = t;
+#endif
+            // merge, ties to the lower position so every lane agrees
+            const bool firstMine = t.e1 > u.e1 || (t.e1 == u.e1 && t.p1 < u.p1);
+            Top2 m;
+            if (firstMine) {
+                m.e1 = t.e1, m.p1 = t.p1;
+                const bool sMine = t.e2 > u.e1 || (t.e2 == u.e1 && t.p2 < u.p1);
+                m.e2 = sMine ? t.e2 : u.e1;
+                m.p2 = sMine ? t.p2 : u.p1;
+            } else {
+                m.e1 = u.e1, m.p1 = u.p1;
+                const bool sMine = t.e1 > u.e2 || (t.e1 == u.e2 && t.p1 < u.p2);
+                m.e2 = sMine ? t.e1 : u.e2;
+                m.p2 = sMine ? t.p1 : u.p2;
+            }
+            t = m;
+        }
+    return t;
+}
+
+HS_HD void writeLeaf(LeafHdr &h, const Sub &a, const Sub &b, const HostPanel &t, const HostPanel &s, uint32_t depth,
+                     uint32_t degree) {
+    h.a = a;
+    h.b = b;
+    h.da = subDiameter(t, a, t.v[0]);
+    h.db = subDiameter(s, b, t.v[0]);
+    h.depth = depth;
+    h.degree = degree;
+    h.error = h.errB = h.intB = h.pad = 0;
+}
+
+// The largest-error refinement of one tensor pair (the host's adaptivePair
+// without projection), with every decision checked against the rounding
+// bounds. Returns kPairRule (patches written to the pool, record appended),
+// kPairWhole (all-pairs mode single whole-panel rule, degree in `whole`) or
+// kPairHost (the host planner must refine this pair).
+template <class Wp>
+HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams &P, const WarpMem &M,
+                     const PairOutput &O) {
+    constexpr int own_n = kValues / Wp::W;
+    const HostPanel &t = P.panels[ti], &s = P.panels[si];
+    const double scale = maxD(t.maxEdge, s.maxEdge);
+    const bool promoteRoot = !isNearPair(t, s, 1.0);
+    const int base = own_n * w.lane();
+    double integral[own_n];
+    for (int v = 0; v < own_n; ++v)
+        integral[v] = 0;
+    double absError = 0, absB = 0, intB = 0;
+    uint32_t nLeaf = 0, nPend = 0, nAtl = 0;
+    uint32_t req[4];
+    int nReq = 0;
+    if (w.leader())
+        writeLeaf(M.hdr[0], wholeSub(), wholeSub(), t, s, 0, 8);
+    w.sync();
+    req[nReq++] = nLeaf++;
+    for (;;) {
+        for (int r = 0; r < nReq; ++r) {
+            LeafHdr L = M.hdr[req[r]];
+            double hiOwn[own_n], mnL = 0;
+            bool bad = false;
+            estimateLeaf(w, t, s, L, P.rules, P.k, scale, M.pts, hiOwn, mnL, bad);
+            if (bad)
+                return kPairHost;
+            for (int v = 0; v < own_n && base + v < 72; ++v)
+                M.integ[size_t(req[r]) * 72 + base + v] = hiOwn[v];
+            w.sync();
+            if (w.leader()) {
+                M.hdr[req[r]].error = L.error;
+                M.hdr[req[r]].errB = L.errB;
+                M.hdr[req[r]].intB = L.intB;
+            }
+            // running sums, in the host's order
+            absError += L.error;
+            absB += L.errB + 2 * kUnit * absError;
+            double mnI = 0;
+            for (int v = 0; v < own_n && base + v < 72; v += 2) {
+                integral[v] += hiOwn[v];
+                integral[v + 1] += hiOwn[v + 1];
+                mnI = fmax(mnI, hypot(integral[v], integral[v + 1]));
+            }
+            mnI = w.max(mnI);
+            intB += L.intB + 2 * kUnit * (mnI + mnL);
+            w.sync();
+            const bool outerLimit = L.depth == P.maxDepth && L.degree == 14;
+            if (outerLimit) {
+                if (w.leader())
+                    M.atl[nAtl] = req[r];
+                ++nAtl;
+            } else {
+                if (w.leader()) {
+                    M.pend[nPend] = req[r];
+                    M.pendErr[nPend] = L.error;
+                }
+                ++nPend;
+            }
+            w.sync();
+        }
+        nReq = 0;
+        double mn = 0;
+        bool nonFinite = false;
+        for (int v = 0; v < own_n && base + v < 72; v += 2) {
+            const double m = hypot(integral[v], integral[v + 1]);
+            nonFinite = nonFinite || !isfinite(m);
+            mn = fmax(mn, m);
+        }
+        if (w.any(nonFinite))
+            return kPairHost;
+        mn = w.max(mn);
+        const double thr = P.tol * .2 * mn;
+        const double mnB = 1.4142135623730951 * intB + 3 * kUnit * mn;
+        const double thrB = P.tol * .2 * mnB + 2 * kUnit * thr;
+        if (!separated(absError, thr, absB + thrB))
+            return kPairHost;
+        if (absError <= thr) {
+            // patches at the depth limit in insertion order, then the pending
+            // leaves by decreasing error (distinct beyond their bounds)
+            if (!(mn > 0))
+                return kPairHost;
+            const double relError = absError / mn;
+            if (!isfinite(relError) || relError > P.tol)
+                return kPairHost;
+            const uint32_t count = nAtl + nPend;
+            for (uint32_t k = 0; k < nPend; ++k) {
+                const Top2 top = topTwo(w, M.pendErr, nPend);
+                if (top.p2 != 0xffffffffu && top.e2 >= 0) {
+                    const double b1 = M.hdr[M.pend[top.p1]].errB, b2 = M.hdr[M.pend[top.p2]].errB;
+                    if (!separated(top.e1, top.e2, b1 + b2))
+                        return kPairHost;
+                }
+                w.sync();
+                if (w.leader()) {
+                    M.atl[nAtl + k] = M.pend[top.p1];
+                    M.pendErr[top.p1] = -1;
+                }
+                w.sync();
+            }
+            uint32_t maxDepth = 0, degree0 = 0;
+            for (uint32_t k = 0; k < count; ++k) {
+                const LeafHdr &h = M.hdr[M.atl[k]];
+                maxDepth = h.depth > maxDepth ? h.depth : maxDepth;
+                degree0 = k == 0 ? h.degree : degree0;
+            }
+            if (P.allPairs && maxDepth == 0 && count == 1) {
+                if (w.leader())
+                    O.whole[unorderedPairIndex(ti, si)] = uint8_t(degree0);
+                return kPairWhole;
+            }
+            unsigned long long first = 0;
+#if defined(__CUDA_ARCH__)
+            if (w.leader())
+                first = atomicAdd(O.poolUsed, (unsigned long long)count);
+            first = __shfl_sync(~0u, first, 0);
+#else
+            first = __atomic_fetch_add(O.poolUsed, (unsigned long long)count, __ATOMIC_RELAXED);
+#endif
+            if (first + count > O.poolCap)
+                return kPairHost;
+            for (uint32_t k = w.lane(); k < count; k += Wp::W) {
+                const LeafHdr &h = M.hdr[M.atl[k]];
+                Patch p;
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) {
+                        p.test[3 * i + j] = h.a.v[i][j];
+                        p.trial[3 * i + j] = h.b.v[i][j];
+                    }
+                p.areaFraction = h.a.fraction * h.b.fraction;
+                p.degree = h.degree;
+                p.projection = 0;
+                p.intervals = 1;
+                p.pad = 0;
+                O.pool[first + k] = p;
+            }
+            if (w.leader()) {
+                unsigned long long slot;
+#if defined(__CUDA_ARCH__)
+                slot = atomicAdd(O.recordCount, 1ull);
+#else
+                slot = __atomic_fetch_add(O.recordCount, 1ull, __ATOMIC_RELAXED);
+#endif
+                O.records[slot] = PairRecord{ti, si, uint32_t(first), count, maxDepth, 0, relError};
+            }
+            return kPairRule;
+        }
+        if (nPend == 0)
+            return kPairHost;
+        const Top2 top = topTwo(w, M.pendErr, nPend);
+        const uint32_t vSlot = M.pend[top.p1];
+        const LeafHdr v = M.hdr[vSlot];
+        if (top.p2 != 0xffffffffu && !separated(top.e1, top.e2, v.errB + M.hdr[M.pend[top.p2]].errB))
+            return kPairHost;
+        w.sync();
+        if (w.leader()) {  // remove v: the last pending entry takes its place
+            M.pend[top.p1] = M.pend[nPend - 1];
+            M.pendErr[top.p1] = M.pendErr[nPend - 1];
+        }
+        --nPend;
+        absError = maxD(0.0, absError - v.error);
+        absB += v.errB + 2 * kUnit * (absError + v.error);
+        double mnI = 0;
+        for (int v2 = 0; v2 < own_n && base + v2 < 72; v2 += 2) {
+            integral[v2] -= M.integ[size_t(vSlot) * 72 + base + v2];
+            integral[v2 + 1] -= M.integ[size_t(vSlot) * 72 + base + v2 + 1];
+            mnI = fmax(mnI, hypot(integral[v2], integral[v2 + 1]));
+        }
+        mnI = w.max(mnI);
+        intB += v.intB + 2 * kUnit * mnI * 2;
+        w.sync();
+        if (v.degree == 8 && (v.depth == P.maxDepth || (promoteRoot && v.depth == 0))) {
+            if (w.leader())
+                writeLeaf(M.hdr[vSlot], v.a, v.b, t, s, v.depth, 14);
+            req[nReq++] = vSlot;
+        } else {
+            if (nPend + nAtl + 4 > 50000 || nLeaf + 3 > kLeafCap)
+                return kPairHost;
+            Sub children[4];
+            const bool splitTest = v.da >= v.db;
+            quarter(splitTest ? v.a : v.b, children);
+            for (int c = 0; c < 4; ++c) {
+                const uint32_t slot = c == 0 ? vSlot : nLeaf++;
+                if (w.leader()) {
+                    if (splitTest)
+                        writeLeaf(M.hdr[slot], children[c], v.b, t, s, v.depth + 1, 8);
+                    else
+                        writeLeaf(M.hdr[slot], v.a, children[c], t, s, v.depth + 1, 8);
+                }
+                req[nReq++] = slot;
+            }
+        }
+        w.sync();
+    }
+}
+
+// Pair classification (the host's processPair test): 0 no adaptive rule,
+// kOnDevice a tensor pair, kProjected a pair on projected patches.
+HS_HD uint8_t classifyPair(const ClassifyParams &P, uint32_t i, uint32_t j) {
+    const HostPanel &a = P.panels[i], &b = P.panels[j];
+    if (!panelsDisjoint(a, b))
+        return kSkip;
+    const unsigned degree = qualifiedDegree(P.bounds[i], P.bounds[j], P.k, P.tol, P.regularOrder);
+    const double h = maxD(a.maxEdge, b.maxEdge);
+    const double limit = P.bounds[i].radius + P.bounds[j].radius + P.nearRatio * h;
+    const double dx = a.centroid.x - b.centroid.x, dy = a.centroid.y - b.centroid.y, dz = a.centroid.z - b.centroid.z;
+    const bool geometricNear =
+        degree && P.nearRatio > 0 && dx * dx + dy * dy + dz * dz < limit * limit && isNearPair(a, b, P.nearRatio);
+    if (degree && !geometricNear)
+        return kSkip;
+    return useProjection(a, b, maxD(a.maxEdge, b.maxEdge)) ? kProjected : kOnDevice;
+}
+
+// Unordered pair index u = j (j - 1) / 2 + i, i < j (interaction_plan.hpp:19-22), inverted.
+HS_HD void pairOfIndex(unsigned long long u, uint32_t &i, uint32_t &j) {
+    unsigned long long jj = (unsigned long long)((1 + sqrt(1 + 8.0 * double(u))) / 2);
+    while (jj * (jj - 1) / 2 > u)
+        --jj;
+    while ((jj + 1) * jj / 2 <= u)
+        ++jj;
+    j = uint32_t(jj);
+    i = uint32_t(u - jj * (jj - 1) / 2);
+}
+
+#if defined(__CUDACC__)
+// Two passes: with null lists only the counts are taken, then the lists are
+// filled (their order is irrelevant: results are keyed by pair). Appends are
+// aggregated per warp.
+__global__ void classifyKernel(ClassifyParams P, const uint2 *candidates, unsigned long long count, int allPairs,
+                               uint2 *deviceList, unsigned long long *deviceCount, uint2 *hostList,
+                               unsigned long long *hostCount) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long warp = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5;
+    const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+    for (unsigned long long b = warp * 32; b < count; b += warps * 32) {
+        const unsigned long long p = b + lane;
+        uint8_t c = kSkip;
+        uint32_t i = 0, j = 0;
+        if (p < count) {
+            if (allPairs) {
+                pairOfIndex(p, i, j);
+            } else {
+                i = candidates[p].x;
+                j = candidates[p].y;
+            }
+            c = classifyPair(P, i, j);
+        }
+        const unsigned md = __ballot_sync(~0u, c == kOnDevice), mh = __ballot_sync(~0u, c == kProjected);
+        unsigned long long bd = 0, bh = 0;
+        if (lane == 0) {
+            if (md)
+                bd = atomicAdd(deviceCount, (unsigned long long)__popc(md));
+            if (mh)
+                bh = atomicAdd(hostCount, (unsigned long long)__popc(mh));
+        }
+        bd = __shfl_sync(~0u, bd, 0);
+        bh = __shfl_sync(~0u, bh, 0);
+        const unsigned below = (1u << lane) - 1;
+        if (c == kOnDevice && deviceList)
+            deviceList[bd + __popc(md & below)] = make_uint2(i, j);
+        if (c == kProjected && hostList)
+            hostList[bh + __popc(mh & below)] = make_uint2(i, j);
+    }
+}
+
+constexpr int kWarpsPerBlock = 4;
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) refineKernel(AdaptiveParams P, const uint2 *list,
+                                                                     unsigned long long count,
+                                                                     unsigned long long *next, WarpMem arena,
+                                                                     PairOutput O, uint2 *flagged,
+                                                                     unsigned long long *flagCount) {
+    __shared__ double pts[kWarpsPerBlock][2 * kRulePoints * kPts];
+    const DeviceWarp w;
+    const int wInBlock = threadIdx.x >> 5;
+    const size_t warpId = size_t(blockIdx.x) * kWarpsPerBlock + wInBlock;
+    WarpMem M;
+    M.hdr = arena.hdr + warpId * kLeafCap;
+    M.integ = arena.integ + warpId * kLeafCap * 72;
+    M.pend = arena.pend + warpId * kLeafCap;
+    M.pendErr = arena.pendErr + warpId * kLeafCap;
+    M.atl = arena.atl + warpId * kLeafCap;
+    M.pts = pts[wInBlock];
+    for (;;) {
+        unsigned long long p = 0;
+        if (w.leader())
+            p = atomicAdd(next, 1ull);
+        p = __shfl_sync(~0u, p, 0);
+        if (p >= count)
+            return;
+        const uint2 pr = list[p];
+        const int r = refinePair(w, pr.x, pr.y, P, M, O);
+        if (r == kPairHost && w.leader())
+            flagged[atomicAdd(flagCount, 1ull)] = pr;
+        __syncwarp();
+    }
+}
+#endif
+
+void check(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation)
+        throw OutOfMemory(std::string(what) + ": " + cudaGetErrorString(e));
+    if (e != cudaSuccess)
+        throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+struct DevMem {
+    void *p = nullptr;
+    DevMem() = default;
+    explicit DevMem(size_t bytes) { alloc(bytes); }
+    void alloc(size_t bytes) { check(cudaMalloc(&p, bytes ? bytes : 16), "planner allocation"); }
+    DevMem(const DevMem &) = delete;
+    DevMem &operator=(const DevMem &) = delete;
+    ~DevMem() {
+        if (p)
+            cudaFree(p);
+    }
+    template <class T> T *as() const { return static_cast<T *>(p); }
+};
+
+std::vector<double> ruleRows(unsigned degree) {
+    const auto rule = triangleRule(degree);
+    std::vector<double> rows;
+    for (const auto &p : rule) {
+        rows.push_back(p.b[0]);
+        rows.push_back(p.b[1]);
+        rows.push_back(p.b[2]);
+        rows.push_back(p.w);
+    }
+    if (rule.size() > size_t(kRulePoints))
+        throw std::logic_error("triangle rule larger than the device planner's point table");
+    return rows;
+}
+
+using Clock = std::chrono::steady_clock;
+double msSince(Clock::time_point t0) { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
+
+}  // namespace
+
+Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cudaStream_t stream,
+                      const volatile int32_t *cancel, DevicePlanStats *stats, bool emulate) {
+    const auto t0 = Clock::now();
+    PlanFrame f = beginPlan(sp, st, maxK);
+    const uint32_t T = uint32_t(sp.panels.size());
+    const unsigned long long units =
+        f.allPairs ? (unsigned long long)T * (T - 1) / 2 : (unsigned long long)f.candidates.size();
+    const std::vector<double> rules[4] = {ruleRows(6), ruleRows(8), ruleRows(12), ruleRows(14)};
+    std::vector<uint2> deviceList, hostList;
+    std::vector<PairRecord> records;
+    std::vector<Patch> pool;
+    std::vector<uint8_t> whole;
+    std::vector<uint2> flagged;
+    size_t devicePairs = 0;
+    if (cancel && *cancel)
+        throw Cancelled();
+    if (emulate) {
+        // The device algorithm on host threads with one-lane warps.
+        ClassifyParams C{sp.panels.data(), f.bounds.data(), maxK, st.tol, st.nearRatio, st.regularOrder};
+        for (unsigned long long p = 0; p < units; ++p) {
+            uint32_t i, j;
+            if (f.allPairs)
+                pairOfIndex(p, i, j);
+            else
+                i = f.candidates[p].first, j = f.candidates[p].second;
+            const uint8_t c = classifyPair(C, i, j);
+            if (c == kOnDevice)
+                deviceList.push_back(make_uint2(i, j));
+            else if (c == kProjected)
+                hostList.push_back(make_uint2(i, j));
+        }
+        AdaptiveParams A{sp.panels.data(), {}, maxK, st.tol, st.maxDepth, f.allPairs ? 1 : 0};
+        for (int r = 0; r < 4; ++r)
+            A.rules.pts[r] = rules[r].data(), A.rules.n[r] = int(rules[r].size() / 4);
+        if (f.allPairs)
+            whole.assign(units, 0);
+        pool.resize(size_t(16) * deviceList.size() + 4096);
+        records.resize(deviceList.size());
+        unsigned long long poolUsed = 0, recordCount = 0;
+        PairOutput O{pool.data(), pool.size(), &poolUsed, records.data(), &recordCount, whole.data()};
+        std::atomic<size_t> next{0};
+        std::mutex flagMutex;
+        const unsigned workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<std::thread> threads;
+        for (unsigned wkr = 0; wkr < workers; ++wkr)
+            threads.emplace_back([&]() {
+                std::vector<LeafHdr> hdr(kLeafCap);
+                std::vector<double> integ(size_t(kLeafCap) * 72), pendErr(kLeafCap), pts(2 * kRulePoints * kPts);
+                std::vector<uint32_t> pend(kLeafCap), atl(kLeafCap);
+                WarpMem M{hdr.data(), integ.data(), pend.data(), pendErr.data(), atl.data(), pts.data()};
+                for (;;) {
+                    const size_t p = next.fetch_add(1);
+                    if (p >= deviceList.size())
+                        return;
+                    if (refinePair(LaneWarp{}, deviceList[p].x, deviceList[p].y, A, M, O) == kPairHost) {
+                        std::lock_guard<std::mutex> lock(flagMutex);
+                        flagged.push_back(deviceList[p]);
+                    }
+                }
+            });
+        for (auto &th : threads)
+            th.join();
+        records.resize(recordCount);
+        pool.resize(std::min<size_t>(poolUsed, pool.size()));
+        devicePairs = deviceList.size();
+    } else {
+#if defined(__CUDACC__)
+        // geometry and rules
+        DevMem dPanels(sizeof(HostPanel) * T), dBounds(sizeof(Bounds) * T);
+        check(cudaMemcpyAsync(dPanels.p, sp.panels.data(), sizeof(HostPanel) * T, cudaMemcpyHostToDevice, stream),
+              "planner upload");
+        check(cudaMemcpyAsync(dBounds.p, f.bounds.data(), sizeof(Bounds) * T, cudaMemcpyHostToDevice, stream),
+              "planner upload");
+        DevMem dRules[4];
+        AdaptiveParams A{dPanels.as<HostPanel>(), {}, maxK, st.tol, st.maxDepth, f.allPairs ? 1 : 0};
+        for (int r = 0; r < 4; ++r) {
+            dRules[r].alloc(rules[r].size() * sizeof(double));
+            check(cudaMemcpyAsync(dRules[r].p, rules[r].data(), rules[r].size() * sizeof(double),
+                                  cudaMemcpyHostToDevice, stream),
+                  "planner upload");
+            A.rules.pts[r] = dRules[r].as<double>();
+            A.rules.n[r] = int(rules[r].size() / 4);
+        }
+        DevMem dCand(f.allPairs ? 16 : sizeof(uint2) * f.candidates.size());
+        if (!f.allPairs && !f.candidates.empty()) {
+            std::vector<uint2> c(f.candidates.size());
+            for (size_t i = 0; i < c.size(); ++i)
+                c[i] = make_uint2(f.candidates[i].first, f.candidates[i].second);
+            check(cudaMemcpyAsync(dCand.p, c.data(), sizeof(uint2) * c.size(), cudaMemcpyHostToDevice, stream),
+                  "planner upload");
+            check(cudaStreamSynchronize(stream), "planner upload");
+        }
+        // classification: counts first, then the lists
+        DevMem dCounters(8 * sizeof(unsigned long long));
+        unsigned long long *counters = dCounters.as<unsigned long long>();
+        check(cudaMemsetAsync(counters, 0, 8 * sizeof(unsigned long long), stream), "planner reset");
+        int device = 0, sms = 0;
+        check(cudaGetDevice(&device), "device query");
+        check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "device query");
+        ClassifyParams C{dPanels.as<HostPanel>(), dBounds.as<Bounds>(), maxK, st.tol, st.nearRatio, st.regularOrder};
+        const unsigned blocks = unsigned(std::max<unsigned long long>(
+            1, std::min<unsigned long long>((units + 255) / 256, 16ull * sms)));
+        unsigned long long n2[2] = {0, 0};
+        if (units) {
+            classifyKernel<<<blocks, 256, 0, stream>>>(C, dCand.as<uint2>(), units, f.allPairs ? 1 : 0, nullptr,
+                                                       counters, nullptr, counters + 1);
+            check(cudaGetLastError(), "planner classification");
+            check(cudaMemcpyAsync(n2, counters, sizeof(n2), cudaMemcpyDeviceToHost, stream), "planner readback");
+            check(cudaStreamSynchronize(stream), "planner classification");
+        }
+        const unsigned long long nDevice = n2[0], nHost = n2[1];
+        DevMem dDeviceList(sizeof(uint2) * nDevice), dHostList(sizeof(uint2) * nHost);
+        if (units) {
+            check(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), stream), "planner reset");
+            classifyKernel<<<blocks, 256, 0, stream>>>(C, dCand.as<uint2>(), units, f.allPairs ? 1 : 0,
+                                                       dDeviceList.as<uint2>(), counters, dHostList.as<uint2>(),
+                                                       counters + 1);
+            check(cudaGetLastError(), "planner classification");
+            check(cudaStreamSynchronize(stream), "planner classification");
+        }
+        hostList.resize(nHost);
+        if (nHost)
+            check(cudaMemcpyAsync(hostList.data(), dHostList.p, sizeof(uint2) * nHost, cudaMemcpyDeviceToHost, stream),
+                  "planner readback");
+        devicePairs = nDevice;
+        // refinement: arenas for the resident warps, the patch pool sized by
+        // the free memory
+        int blocksPerSm = 0;
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, refineKernel, 32 * kWarpsPerBlock, 0),
+              "planner occupancy");
+        blocksPerSm = std::max(1, blocksPerSm);
+        size_t freeBytes = 0, totalBytes = 0;
+        check(cudaMemGetInfo(&freeBytes, &totalBytes), "device memory query");
+        const size_t warpBytes = (sizeof(LeafHdr) + 72 * sizeof(double) + 2 * sizeof(uint32_t) + sizeof(double)) *
+                                 size_t(kLeafCap);
+        size_t grid = size_t(sms) * blocksPerSm;  // resident blocks, fewer when memory is short
+        grid = std::max<size_t>(1, std::min(grid, freeBytes / 4 / (warpBytes * kWarpsPerBlock)));
+        const size_t warps = grid * kWarpsPerBlock;
+        DevMem dHdr(sizeof(LeafHdr) * kLeafCap * warps), dInteg(sizeof(double) * 72 * kLeafCap * warps),
+            dPend(sizeof(uint32_t) * kLeafCap * warps), dPendErr(sizeof(double) * kLeafCap * warps),
+            dAtl(sizeof(uint32_t) * kLeafCap * warps);
+        check(cudaMemGetInfo(&freeBytes, &totalBytes), "device memory query");
+        const size_t poolCap =
+            std::max<size_t>(4096, std::min<size_t>(16 * nDevice + 4096, freeBytes / 4 / sizeof(Patch)));
+        DevMem dPool(sizeof(Patch) * poolCap), dRecords(sizeof(PairRecord) * std::max<unsigned long long>(nDevice, 1)),
+            dFlagged(sizeof(uint2) * std::max<unsigned long long>(nDevice, 1));
+        DevMem dWhole(f.allPairs ? units : 16);
+        if (f.allPairs)
+            check(cudaMemsetAsync(dWhole.p, 0, units, stream), "planner reset");
+        WarpMem arena{dHdr.as<LeafHdr>(), dInteg.as<double>(), dPend.as<uint32_t>(), dPendErr.as<double>(),
+                      dAtl.as<uint32_t>(), nullptr};
+        PairOutput O{dPool.as<Patch>(), poolCap, counters + 2, dRecords.as<PairRecord>(), counters + 3,
+                     dWhole.as<uint8_t>()};
+        // chunks of pairs, so a cancellation is seen between launches
+        const unsigned long long chunk = 1ull << 20;
+        for (unsigned long long begin = 0; begin < nDevice; begin += chunk) {
+            if (cancel && *cancel)
+                throw Cancelled();
+            const unsigned long long n = std::min(chunk, nDevice - begin);
+            check(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), stream), "planner reset");
+            refineKernel<<<unsigned(grid), 32 * kWarpsPerBlock, 0, stream>>>(
+                A, dDeviceList.as<uint2>() + begin, n, counters + 5, arena, O, dFlagged.as<uint2>(), counters + 4);
+            check(cudaGetLastError(), "planner refinement");
+            check(cudaStreamSynchronize(stream), "planner refinement");
+        }
+        unsigned long long n5[5] = {};
+        check(cudaMemcpyAsync(n5, counters, sizeof(n5), cudaMemcpyDeviceToHost, stream), "planner readback");
+        check(cudaStreamSynchronize(stream), "planner readback");
+        const unsigned long long used = std::min<unsigned long long>(n5[2], poolCap), nRec = n5[3], nFlag = n5[4];
+        records.resize(nRec);
+        pool.resize(used);
+        flagged.resize(nFlag);
+        if (nRec)
+            check(cudaMemcpyAsync(records.data(), dRecords.p, sizeof(PairRecord) * nRec, cudaMemcpyDeviceToHost,
+                                  stream),
+                  "planner readback");
+        if (used)
+            check(cudaMemcpyAsync(pool.data(), dPool.p, sizeof(Patch) * used, cudaMemcpyDeviceToHost, stream),
+                  "planner readback");
+        if (nFlag)
+            check(cudaMemcpyAsync(flagged.data(), dFlagged.p, sizeof(uint2) * nFlag, cudaMemcpyDeviceToHost, stream),
+                  "planner readback");
+        if (f.allPairs) {
+            whole.resize(units);
+            check(cudaMemcpyAsync(whole.data(), dWhole.p, units, cudaMemcpyDeviceToHost, stream), "planner readback");
+        }
+        check(cudaStreamSynchronize(stream), "planner readback");
+#else
+        throw Unsupported("device planner unavailable in this build");
+#endif
+    }
+    const double deviceMs = msSince(t0);
+    // the host refines projected and flagged pairs
+    const auto t1 = Clock::now();
+    std::vector<std::pair<uint32_t, uint32_t>> hostPairs;
+    hostPairs.reserve(hostList.size() + flagged.size());
+    for (const auto &p : hostList)
+        hostPairs.emplace_back(p.x, p.y);
+    for (const auto &p : flagged)
+        hostPairs.emplace_back(p.x, p.y);
+    std::sort(hostPairs.begin(), hostPairs.end());
+    const std::vector<PairRule> hostRules = planPairsOnHost(sp, st, maxK, hostPairs, 0, cancel);
+    // flatten in (first, second) order, the host planner's order
+    struct Item {
+        uint64_t key;
+        int32_t host;  // index into hostRules, or -1 - record index
+    };
+    std::vector<Item> items;
+    items.reserve(records.size() + hostRules.size());
+    for (size_t r = 0; r < records.size(); ++r)
+        items.push_back({(uint64_t(records[r].first) << 32) | records[r].second, -1 - int32_t(r)});
+    for (size_t h = 0; h < hostPairs.size(); ++h)
+        items.push_back({(uint64_t(hostPairs[h].first) << 32) | hostPairs[h].second, int32_t(h)});
+    std::sort(items.begin(), items.end(), [](const Item &x, const Item &y) { return x.key < y.key; });
+    if (f.allPairs)
+        for (unsigned long long u = 0; u < units; ++u)
+            if (whole[u])
+                f.plan.wholePanelDegrees[u] = whole[u];
+    for (const auto &it : items) {
+        const uint32_t i = uint32_t(it.key >> 32), j = uint32_t(it.key & 0xffffffffu);
+        if (it.host >= 0) {
+            const PairRule &r = hostRules[size_t(it.host)];
+            appendPairRule(f.plan, f.allPairs, i, j, r.patches.data(), uint32_t(r.patches.size()), r.maxDepth,
+                           r.relError);
+        } else {
+            const PairRecord &r = records[size_t(-1 - it.host)];
+            appendPairRule(f.plan, f.allPairs, i, j, pool.data() + r.patchFirst, r.count, r.maxDepth, r.relError);
+        }
+    }
+    finishPlan(f.plan, T);
+    if (stats) {
+        stats->devicePairs = devicePairs;
+        stats->projectedPairs = hostList.size();
+        stats->flaggedPairs = flagged.size();
+        size_t wholeCount = 0;
+        for (const auto b : whole)
+            wholeCount += b != 0;
+        stats->wholePanelPairs = wholeCount;
+        stats->deviceMs = deviceMs;
+        stats->hostMs = msSince(t1);
+    }
+    return std::move(f.plan);
+}
+
+}  // namespace hsb

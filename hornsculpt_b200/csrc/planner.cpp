@@ -8,6 +8,7 @@
 // flattened in (first, second) order, so the plan is independent of thread
 // count and identical to the reference's.
 #include "planner.hpp"
+#include "planner_geom.cuh"
 
 #include <algorithm>
 #include <array>
@@ -27,80 +28,6 @@ using cplx = std::complex<double>;
 using Moments = std::array<cplx, 36>;
 using Bary = std::array<double, 3>;
 
-struct Sub {
-    std::array<Bary, 3> v{{{1, 0, 0}, {0, 1, 0}, {0, 0, 1}}};
-    double fraction{1};
-};
-
-V3 localPoint(const HostPanel &p, const double *b) { return (p.v[1] - p.v[0]) * b[1] + (p.v[2] - p.v[0]) * b[2]; }
-
-// ---- distances (pair_quadrature.cpp:43-101, 786-807) ----
-double pointTriangleD2(V3 p, const V3 *tr) {
-    const V3 a = tr[0], b = tr[1], c = tr[2], ab = b - a, ac = c - a, ap = p - a;
-    const double d1 = dot(ab, ap), d2 = dot(ac, ap);
-    if (d1 <= 0 && d2 <= 0)
-        return norm2(ap);
-    const V3 bp = p - b;
-    const double d3 = dot(ab, bp), d4 = dot(ac, bp);
-    if (d3 >= 0 && d4 <= d3)
-        return norm2(bp);
-    const double vc = d1 * d4 - d3 * d2;
-    if (vc <= 0 && d1 >= 0 && d3 <= 0)
-        return norm2(p - (a + ab * (d1 / (d1 - d3))));
-    const V3 cp = p - c;
-    const double d5 = dot(ab, cp), d6 = dot(ac, cp);
-    if (d6 >= 0 && d5 <= d6)
-        return norm2(cp);
-    const double vb = d5 * d2 - d1 * d6;
-    if (vb <= 0 && d2 >= 0 && d6 <= 0)
-        return norm2(p - (a + ac * (d2 / (d2 - d6))));
-    const double va = d3 * d6 - d5 * d4;
-    if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
-        const double t = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-        return norm2(p - (b + (c - b) * t));
-    }
-    const double inv = 1 / (va + vb + vc);
-    return norm2(p - (a + (ab * (vb * inv) + ac * (vc * inv))));
-}
-double segmentD2(V3 p, V3 q, V3 a, V3 b) {
-    const V3 u = q - p, v = b - a, w = p - a;
-    const double aa = dot(u, u), bb = dot(u, v), cc = dot(v, v), dd = dot(u, w), ee = dot(v, w);
-    const double det = aa * cc - bb * bb;
-    double s = det > aa * cc * 1e-14 ? std::clamp((bb * ee - cc * dd) / det, 0.0, 1.0) : 0;
-    double t = (bb * s + ee) / cc;
-    if (t < 0) {
-        t = 0;
-        s = std::clamp(-dd / aa, 0.0, 1.0);
-    } else if (t > 1) {
-        t = 1;
-        s = std::clamp((bb - dd) / aa, 0.0, 1.0);
-    }
-    return norm2((w + u * s) - v * t);
-}
-double panelDistance(const HostPanel &t, const HostPanel &s) {
-    V3 a[3], b[3];
-    for (int i = 0; i < 3; ++i) {
-        a[i] = t.v[i] - t.v[0];
-        b[i] = s.v[i] - t.v[0];
-    }
-    double d2 = std::numeric_limits<double>::infinity();
-    for (int i = 0; i < 3; ++i) {
-        d2 = std::min({d2, pointTriangleD2(a[i], b), pointTriangleD2(b[i], a)});
-        for (int j = 0; j < 3; ++j)
-            d2 = std::min(d2, segmentD2(a[i], a[(i + 1) % 3], b[j], b[(j + 1) % 3]));
-    }
-    return std::sqrt(d2);
-}
-bool disjoint(const HostPanel &t, const HostPanel &s) { return classifyNodes(t.nodes, s.nodes).topology == kDisjoint; }
-bool isNearPair(const HostPanel &t, const HostPanel &s, double ratio) {
-    if (ratio == 0 || !disjoint(t, s))
-        return false;
-    const double size = std::max(t.maxEdge, s.maxEdge);
-    const double bound = ratio * size + t.maxEdge + s.maxEdge;
-    if (norm2(t.centroid - s.centroid) >= bound * bound)
-        return false;
-    return panelDistance(t, s) < ratio * size;
-}
 FanPanel fan(const HostPanel &p) { return FanPanel{{p.v[0], p.v[1], p.v[2]}, p.n, p.area}; }
 
 // ---- embedded-rule patch estimate (pair_quadrature.cpp:143-226, 644-683) ----
@@ -307,7 +234,14 @@ std::vector<Sub> projectionPartition(const HostPanel &t, const HostPanel &s) {
             const Bary a = poly[0], b = poly[i], c = poly[i + 1];
             const double f = std::abs((b[1] - a[1]) * (c[2] - a[2]) - (b[2] - a[2]) * (c[1] - a[1]));
             if (f > 0) {
-                out.push_back({{a, b, c}, f});
+                Sub sub{};
+                for (int i = 0; i < 3; ++i) {
+                    sub.v[0][i] = a[i];
+                    sub.v[1][i] = b[i];
+                    sub.v[2][i] = c[i];
+                }
+                sub.fraction = f;
+                out.push_back(sub);
                 area += f;
             }
         }
@@ -317,40 +251,6 @@ std::vector<Sub> projectionPartition(const HostPanel &t, const HostPanel &s) {
         throw NumericError("Projected line partition exceeds its triangle bound.");
     return out;
 }
-bool useProjection(const HostPanel &t, const HostPanel &s, double scale) {
-    if (panelDistance(t, s) >= .025 * scale)
-        return false;
-    const double eps = 128 * std::numeric_limits<double>::epsilon() * scale;
-    double lo = std::numeric_limits<double>::infinity(), hi = -lo;
-    for (int i = 0; i < 3; ++i) {
-        const double h = dot(t.v[i] - s.v[0], s.n);
-        lo = std::min(lo, h);
-        hi = std::max(hi, h);
-    }
-    return (lo >= -eps && hi > eps) || (hi <= eps && lo < -eps);
-}
-std::array<Sub, 4> quarter(const Sub &s) {
-    const auto mid = [](const Bary &a, const Bary &b) {
-        return Bary{(a[0] + b[0]) * .5, (a[1] + b[1]) * .5, (a[2] + b[2]) * .5};
-    };
-    const Bary a = s.v[0], b = s.v[1], c = s.v[2], ab = mid(a, b), bc = mid(b, c), ca = mid(c, a);
-    const double f = s.fraction * .25;
-    return {{{{a, ab, ca}, f}, {{ab, b, bc}, f}, {{ca, bc, c}, f}, {{ab, bc, ca}, f}}};
-}
-double diameter(const HostPanel &p, const Sub &s, V3 origin) {
-    const V3 off = p.v[0] - origin;
-    V3 q[3];
-    for (int i = 0; i < 3; ++i)
-        q[i] = off + localPoint(p, s.v[i].data());
-    return std::sqrt(std::max({norm2(q[0] - q[1]), norm2(q[1] - q[2]), norm2(q[2] - q[0])}));
-}
-
-struct PairRule {
-    std::vector<Patch> patches;
-    unsigned maxDepth{};
-    double relError{};
-};
-
 // Largest-error refinement for one disjoint pair (pair_quadrature.cpp:329-575).
 PairRule adaptivePair(const HostPanel &t, const HostPanel &s, const PlanSettings &st, double k,
                       const volatile int32_t *cancel) {
@@ -363,13 +263,13 @@ PairRule adaptivePair(const HostPanel &t, const HostPanel &s, const PlanSettings
     const auto byError = [](const Leaf &x, const Leaf &y) { return x.error < y.error; };
     const bool projection = useProjection(t, s, std::max(t.maxEdge, s.maxEdge));
     const bool promoteRoot = !projection && !isNearPair(t, s, 1.0);
-    const std::vector<Sub> initial = projection ? projectionPartition(t, s) : std::vector<Sub>{Sub{}};
+    const std::vector<Sub> initial = projection ? projectionPartition(t, s) : std::vector<Sub>{wholeSub()};
     const auto makeLeaf = [&](const Sub &a, const Sub &b, unsigned depth, unsigned degree, unsigned intervals) {
         Leaf l;
         l.a = a;
         l.b = b;
-        l.da = diameter(t, a, t.v[0]);
-        l.db = diameter(s, b, t.v[0]);
+        l.da = subDiameter(t, a, t.v[0]);
+        l.db = subDiameter(s, b, t.v[0]);
         l.depth = depth;
         l.degree = degree;
         l.intervals = intervals;
@@ -394,7 +294,7 @@ PairRule adaptivePair(const HostPanel &t, const HostPanel &s, const PlanSettings
     size_t nextInitial = 0;
     const auto requestInitial = [&]() {
         while (nextInitial < initial.size() && requested.size() < 4)
-            requested.push_back(makeLeaf(initial[nextInitial++], Sub{}, 0, 8, 1));
+            requested.push_back(makeLeaf(initial[nextInitial++], wholeSub(), 0, 8, 1));
     };
     requestInitial();
     for (;;) {
@@ -466,12 +366,16 @@ PairRule adaptivePair(const HostPanel &t, const HostPanel &s, const PlanSettings
         else {
             if (pending.size() + atLimit.size() + 4 > 50000)
                 throw NumericError("Near-pair quadrature exceeds the fifty-thousand-patch safety limit.");
-            if (projection || v.da >= v.db)
-                for (const auto &c : quarter(v.a))
+            Sub children[4];
+            if (projection || v.da >= v.db) {
+                quarter(v.a, children);
+                for (const auto &c : children)
                     requested.push_back(makeLeaf(c, v.b, v.depth + 1, 8, v.intervals));
-            else
-                for (const auto &c : quarter(v.b))
+            } else {
+                quarter(v.b, children);
+                for (const auto &c : children)
                     requested.push_back(makeLeaf(v.a, c, v.depth + 1, 8, 1));
+            }
         }
     }
 }
@@ -525,13 +429,84 @@ std::vector<std::pair<uint32_t, uint32_t>> candidates(const Space &sp, double ra
                         if (std::abs(a.v[0].x - b.v[0].x) > bound || std::abs(a.v[0].y - b.v[0].y) > bound ||
                             std::abs(a.v[0].z - b.v[0].z) > bound)
                             continue;
-                        if (disjoint(a, b))
+                        if (panelsDisjoint(a, b))
                             out.emplace_back(uint32_t(i), j);
                     }
                 }
     }
     std::sort(out.begin(), out.end());
     return out;
+}
+
+// The host planner's per-pair step: regular-rule qualification, the
+// geometric near test, then adaptive refinement of the pairs that need it
+// (interaction_plan.cpp:228-300). Appends (key, rule) to `out`.
+void processPair(const Space &sp, const std::vector<Bounds> &bounds, const PlanSettings &st, double maxK, uint32_t i,
+                 uint32_t j, const volatile int32_t *cancel, std::vector<std::pair<uint64_t, PairRule>> &out,
+                 bool classify) {
+    const HostPanel &a = sp.panels[i], &b = sp.panels[j];
+    if (classify) {
+        if (!panelsDisjoint(a, b))
+            return;
+        const unsigned degree = qualifiedDegree(bounds[i], bounds[j], maxK, st.tol, st.regularOrder);
+        const double h = std::max(a.maxEdge, b.maxEdge);
+        const double limit = bounds[i].radius + bounds[j].radius + st.nearRatio * h;
+        const double dx = a.centroid.x - b.centroid.x, dy = a.centroid.y - b.centroid.y,
+                     dz = a.centroid.z - b.centroid.z;
+        const bool geometricNear = degree && st.nearRatio > 0 && dx * dx + dy * dy + dz * dz < limit * limit &&
+                                   isNearPair(a, b, st.nearRatio);
+        if (degree && !geometricNear)
+            return;
+    }
+    try {
+        out.emplace_back((uint64_t(i) << 32) | j, adaptivePair(a, b, st, maxK, cancel));
+    } catch (const Cancelled &) {
+        throw;
+    } catch (const std::exception &e) {
+        std::ostringstream msg;
+        msg << "Near pair panels " << i << '/' << j << " (faces " << a.face << '/' << b.face << ", k=" << maxK
+            << ", gap=" << panelDistance(a, b) << " m, depth=" << st.maxDepth << "): " << e.what();
+        throw NumericError(msg.str());
+    }
+}
+
+// Runs `work(unit, results[unit])` for units 0..count-1 on up to `threads`
+// host threads (0 = hardware concurrency, at most 64); the first exception
+// stops the workers and is rethrown.
+template <class Work>
+void parallelUnits(size_t count, unsigned threads, const volatile int32_t *cancel,
+                   std::vector<std::vector<std::pair<uint64_t, PairRule>>> &results, Work work) {
+    std::atomic<size_t> next{0};
+    std::atomic<bool> failed{false};
+    std::exception_ptr failure;
+    std::mutex failureMutex;
+    unsigned workers = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
+    workers = unsigned(std::min<size_t>({size_t(workers), size_t(64), std::max<size_t>(count, 1)}));
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < workers; ++w)
+        pool.emplace_back([&]() {
+            try {
+                for (;;) {
+                    if (failed.load(std::memory_order_relaxed))
+                        return;
+                    if (cancel && *cancel)
+                        throw Cancelled();
+                    const size_t u = next.fetch_add(1);
+                    if (u >= count)
+                        return;
+                    work(u, results[u]);
+                }
+            } catch (...) {
+                std::lock_guard<std::mutex> lock(failureMutex);
+                if (!failure)
+                    failure = std::current_exception();
+                failed = true;
+            }
+        });
+    for (auto &th : pool)
+        th.join();
+    if (failure)
+        std::rethrow_exception(failure);
 }
 
 }  // namespace
@@ -556,20 +531,21 @@ Bounds makeBounds(const HostPanel &p) {
     return b;
 }
 
-Plan makePlan(const Space &sp, const PlanSettings &st, double maxK, unsigned threads, const volatile int32_t *cancel) {
+PlanFrame beginPlan(const Space &sp, const PlanSettings &st, double maxK) {
     const size_t T = sp.panels.size();
     if (!T || !std::isfinite(maxK) || maxK < 0 || !std::isfinite(st.nearRatio) || st.nearRatio < 0 ||
         !std::isfinite(st.tol) || st.tol <= 0 || st.maxDepth > 16 || (st.regularOrder != 2 && st.regularOrder != 4) ||
         st.singularOrder < 2 || st.singularOrder > 20)
         throw InvalidArgument("Invalid BEM interaction-plan input or quadrature settings.");
-    Plan plan;
-    std::vector<Bounds> bounds(T);
-    bool allPairs = !((1e-6 + 4 * 3.5e-8) <= .2 * st.tol);
+    PlanFrame f;
+    f.bounds.resize(T);
+    f.allPairs = !((1e-6 + 4 * 3.5e-8) <= .2 * st.tol);
     for (size_t i = 0; i < T; ++i) {
-        bounds[i] = makeBounds(sp.panels[i]);
-        allPairs = allPairs || !bounds[i].qualified || maxK * sp.panels[i].maxEdge > 2;
+        f.bounds[i] = makeBounds(sp.panels[i]);
+        f.allPairs = f.allPairs || !f.bounds[i].qualified || maxK * sp.panels[i].maxEdge > 2;
     }
-    if (allPairs)
+    Plan &plan = f.plan;
+    if (f.allPairs)
         plan.wholePanelDegrees.assign(T * (T - 1) / 2, 0);
     plan.nearOffsets.assign(T + 1, 0);
     for (size_t t = 0; t < T; ++t) {
@@ -584,86 +560,27 @@ Plan makePlan(const Space &sp, const PlanSettings &st, double maxK, unsigned thr
         for (uint32_t s : adj)
             plan.touching.push_back({uint32_t(t), s, classifyNodes(sp.panels[t].nodes, sp.panels[s].nodes)});
     }
-    const auto pairs = allPairs ? std::vector<std::pair<uint32_t, uint32_t>>{}
-                                : candidates(sp, std::max(2.0, st.nearRatio));
-    const size_t units = allPairs ? T : pairs.size();
-    // Results per candidate (or per all-pairs row) keep the flattening order
-    // independent of which worker integrated which pair.
-    std::vector<std::vector<std::pair<uint64_t, PairRule>>> results(units);
-    std::atomic<size_t> next{0};
-    std::atomic<bool> failed{false};
-    std::exception_ptr failure;
-    std::mutex failureMutex;
-    unsigned workers = threads ? threads : std::max(1u, std::thread::hardware_concurrency());
-    workers = unsigned(std::min<size_t>({size_t(workers), size_t(64), std::max<size_t>(units, 1)}));
-    const auto process = [&](uint32_t i, uint32_t j, std::vector<std::pair<uint64_t, PairRule>> &out) {
-        const HostPanel &a = sp.panels[i], &b = sp.panels[j];
-        if (!disjoint(a, b))
-            return;
-        const unsigned degree = qualifiedDegree(bounds[i], bounds[j], maxK, st.tol, st.regularOrder);
-        const double h = std::max(a.maxEdge, b.maxEdge);
-        const double limit = bounds[i].radius + bounds[j].radius + st.nearRatio * h;
-        const double dx = a.centroid.x - b.centroid.x, dy = a.centroid.y - b.centroid.y,
-                     dz = a.centroid.z - b.centroid.z;
-        const bool geometricNear = degree && st.nearRatio > 0 && dx * dx + dy * dy + dz * dz < limit * limit &&
-                                   isNearPair(a, b, st.nearRatio);
-        if (degree && !geometricNear)
-            return;
-        try {
-            out.emplace_back((uint64_t(i) << 32) | j, adaptivePair(a, b, st, maxK, cancel));
-        } catch (const Cancelled &) {
-            throw;
-        } catch (const std::exception &e) {
-            std::ostringstream msg;
-            msg << "Near pair panels " << i << '/' << j << " (faces " << a.face << '/' << b.face << ", k=" << maxK
-                << ", gap=" << panelDistance(a, b) << " m, depth=" << st.maxDepth << "): " << e.what();
-            throw NumericError(msg.str());
-        }
-    };
-    std::vector<std::thread> pool;
-    for (unsigned w = 0; w < workers; ++w)
-        pool.emplace_back([&]() {
-            try {
-                for (;;) {
-                    if (failed.load(std::memory_order_relaxed))
-                        return;
-                    if (cancel && *cancel)
-                        throw Cancelled();
-                    const size_t u = next.fetch_add(1);
-                    if (u >= units)
-                        return;
-                    if (allPairs)
-                        for (uint32_t j = uint32_t(u) + 1; j < T; ++j)
-                            process(uint32_t(u), j, results[u]);
-                    else
-                        process(pairs[u].first, pairs[u].second, results[u]);
-                }
-            } catch (...) {
-                std::lock_guard<std::mutex> lock(failureMutex);
-                if (!failure)
-                    failure = std::current_exception();
-                failed = true;
-            }
-        });
-    for (auto &th : pool)
-        th.join();
-    if (failure)
-        std::rethrow_exception(failure);
-    for (auto &row : results)
-        for (auto &[key, rule] : row) {
-            const uint32_t i = uint32_t(key >> 32), j = uint32_t(key & 0xffffffffu);
-            if (allPairs && rule.maxDepth == 0 && rule.patches.size() == 1 && !rule.patches.front().projection) {
-                plan.wholePanelDegrees[unorderedPairIndex(i, j)] = uint8_t(rule.patches.front().degree);
-                plan.maxRelError = std::max(plan.maxRelError, rule.relError);
-                continue;
-            }
-            const uint32_t first = uint32_t(plan.patches.size()), n = uint32_t(rule.patches.size());
-            plan.patches.insert(plan.patches.end(), rule.patches.begin(), rule.patches.end());
-            plan.near.push_back({i, j, first, n, 0});
-            plan.near.push_back({j, i, first, n, 1});
-            plan.maxDepth = std::max(plan.maxDepth, rule.maxDepth);
-            plan.maxRelError = std::max(plan.maxRelError, rule.relError);
-        }
+    if (!f.allPairs)
+        f.candidates = candidates(sp, std::max(2.0, st.nearRatio));
+    return f;
+}
+
+void appendPairRule(Plan &plan, bool allPairs, uint32_t i, uint32_t j, const Patch *patches, uint32_t count,
+                    unsigned maxDepth, double relError) {
+    if (allPairs && maxDepth == 0 && count == 1 && !patches[0].projection) {
+        plan.wholePanelDegrees[unorderedPairIndex(i, j)] = uint8_t(patches[0].degree);
+        plan.maxRelError = std::max(plan.maxRelError, relError);
+        return;
+    }
+    const uint32_t first = uint32_t(plan.patches.size());
+    plan.patches.insert(plan.patches.end(), patches, patches + count);
+    plan.near.push_back({i, j, first, count, 0});
+    plan.near.push_back({j, i, first, count, 1});
+    plan.maxDepth = std::max(plan.maxDepth, maxDepth);
+    plan.maxRelError = std::max(plan.maxRelError, relError);
+}
+
+void finishPlan(Plan &plan, size_t T) {
     std::sort(plan.near.begin(), plan.near.end(), [](const NearJob &x, const NearJob &y) {
         return x.test != y.test ? x.test < y.test : x.trial < y.trial;
     });
@@ -674,7 +591,42 @@ Plan makePlan(const Space &sp, const PlanSettings &st, double maxK, unsigned thr
     }
     for (size_t r = 1; r <= T; ++r)
         plan.nearOffsets[r] += plan.nearOffsets[r - 1];
-    return plan;
+}
+
+std::vector<PairRule> planPairsOnHost(const Space &sp, const PlanSettings &st, double maxK,
+                                      const std::vector<std::pair<uint32_t, uint32_t>> &pairs, unsigned threads,
+                                      const volatile int32_t *cancel) {
+    std::vector<std::vector<std::pair<uint64_t, PairRule>>> results(pairs.size());
+    const std::vector<Bounds> none;
+    parallelUnits(pairs.size(), threads, cancel, results, [&](size_t u, auto &out) {
+        processPair(sp, none, st, maxK, pairs[u].first, pairs[u].second, cancel, out, false);
+    });
+    std::vector<PairRule> rules(pairs.size());
+    for (size_t u = 0; u < pairs.size(); ++u)
+        rules[u] = std::move(results[u].front().second);
+    return rules;
+}
+
+Plan makePlan(const Space &sp, const PlanSettings &st, double maxK, unsigned threads, const volatile int32_t *cancel) {
+    PlanFrame f = beginPlan(sp, st, maxK);
+    const size_t T = sp.panels.size();
+    const size_t units = f.allPairs ? T : f.candidates.size();
+    // Results per candidate (or per all-pairs row) keep the flattening order
+    // independent of which worker integrated which pair.
+    std::vector<std::vector<std::pair<uint64_t, PairRule>>> results(units);
+    parallelUnits(units, threads, cancel, results, [&](size_t u, auto &out) {
+        if (f.allPairs)
+            for (uint32_t j = uint32_t(u) + 1; j < T; ++j)
+                processPair(sp, f.bounds, st, maxK, uint32_t(u), j, cancel, out, true);
+        else
+            processPair(sp, f.bounds, st, maxK, f.candidates[u].first, f.candidates[u].second, cancel, out, true);
+    });
+    for (auto &row : results)
+        for (auto &[key, rule] : row)
+            appendPairRule(f.plan, f.allPairs, uint32_t(key >> 32), uint32_t(key & 0xffffffffu), rule.patches.data(),
+                           uint32_t(rule.patches.size()), rule.maxDepth, rule.relError);
+    finishPlan(f.plan, T);
+    return std::move(f.plan);
 }
 
 }  // namespace hsb

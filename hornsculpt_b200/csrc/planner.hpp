@@ -32,7 +32,40 @@ struct PlanSettings {
     unsigned maxDepth{6};
 };
 
+// One pair's adaptive rule: patches in the reference's output order (patches
+// at the depth limit first, then the rest by decreasing error estimate).
+struct PairRule {
+    std::vector<Patch> patches;
+    unsigned maxDepth{};
+    double relError{};
+};
+
+// The frequency-independent frame of a plan: validated settings, panel
+// bounds, the all-pairs switch (interaction_plan.cpp:186-196), touching jobs
+// and, outside the all-pairs mode, the grid candidates sorted by (first,
+// second).
+struct PlanFrame {
+    Plan plan;
+    std::vector<Bounds> bounds;
+    bool allPairs{};
+    std::vector<std::pair<uint32_t, uint32_t>> candidates;
+};
+
 Bounds makeBounds(const HostPanel &p);
+PlanFrame beginPlan(const Space &space, const PlanSettings &settings, double maxK);
+// Appends one pair's rule in flattening order: a single depth-0 tensor patch
+// becomes a whole-panel degree in the all-pairs mode, anything else a near job
+// in both orientations.
+void appendPairRule(Plan &plan, bool allPairs, uint32_t first, uint32_t second, const Patch *patches, uint32_t count,
+                    unsigned maxDepth, double relError);
+// Sorts the near jobs by (test, trial) and builds the near CSR.
+void finishPlan(Plan &plan, size_t triangleCount);
+// The host planner's adaptive refinement of the listed pairs (first < second,
+// pairs known to need it), on host threads; errors carry the host planner's
+// messages.
+std::vector<PairRule> planPairsOnHost(const Space &space, const PlanSettings &settings, double maxK,
+                                      const std::vector<std::pair<uint32_t, uint32_t>> &pairs, unsigned threads,
+                                      const volatile int32_t *cancel);
 // Parallel over host threads (at most `threads`, 0 = hardware concurrency).
 // The result does not depend on the thread count.
 Plan makePlan(const Space &space, const PlanSettings &settings, double maxK, unsigned threads,

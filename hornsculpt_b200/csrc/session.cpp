@@ -255,7 +255,9 @@ void Session::preparePlan(const hs_numerics &o, double maxK, const volatile int3
     const auto start = Clock::now();
     PlanSettings st{o.quadrature_order, o.singular_order, o.near_distance_ratio, o.near_relative_tolerance,
                     o.near_maximum_depth};
-    plan_ = makePlan(space_, st, maxK, 0, cancel);
+    planStats_ = DevicePlanStats{};
+    plan_ = planner_ == HS_PLANNER_HOST ? makePlan(space_, st, maxK, 0, cancel)
+                                        : makePlanOnDevice(space_, st, maxK, stream(), cancel, &planStats_);
     const uint32_t T = uint32_t(space_.panels.size());
     const size_t pairs = size_t(T) * (T - 1) / 2;
     std::vector<uint8_t> code(pairs, kPairRegular);
@@ -1383,6 +1385,12 @@ void Session::setPlaneWaveThreshold(double threshold) {
     planeWaveThreshold_ = threshold;
     if (fmm_)
         fmm_->setHfThreshold(threshold);
+}
+
+void Session::setPlanner(uint32_t planner) {
+    if (planner != HS_PLANNER_DEVICE && planner != HS_PLANNER_HOST)
+        throw InvalidArgument("Interaction planner must be HS_PLANNER_DEVICE or HS_PLANNER_HOST.");
+    planner_ = planner;
 }
 
 void Session::setGroupedM2l(bool enabled) {

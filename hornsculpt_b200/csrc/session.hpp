@@ -7,6 +7,7 @@
 #include "fmm.hpp"
 #include "hs_bem.h"
 #include "kernel_timer.hpp"
+#include "plan_device.hpp"
 #include "planner.hpp"
 
 #include <complex>
@@ -93,6 +94,11 @@ class Session {
     void setGraphs(bool enabled);
     void setPlaneWaveThreshold(double threshold);
     void setGroupedM2l(bool enabled);
+    // Interaction planner: on the device (default) or the host's threads;
+    // both give the same plan bit for bit. The statistics are the last device
+    // plan's.
+    void setPlanner(uint32_t planner);
+    const DevicePlanStats &planStats() const { return planStats_; }
     uint64_t graphLaunches() const { return graphLaunches_; }
     // Device bytes a solve may hold beyond the resident geometry and plan
     // (0: 60 % of free memory); bounds the frequency batch.
@@ -159,6 +165,8 @@ class Session {
     double planK_ = -1;
     Plan plan_;
     double planMs_ = 0;
+    uint32_t planner_ = HS_PLANNER_DEVICE;
+    DevicePlanStats planStats_;
     DeviceBuffer dPairCode_, dTouching_, dNearPairs_, dPatches_, dGauss_, dSingularTable_;
     // patches as the kernels see them: dPatches_, or the device alias of mapped
     // pinned host memory (residency)

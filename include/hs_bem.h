@@ -50,6 +50,8 @@ typedef enum hs_precision {
     HS_PRECISION_MIXED = 1  /* FP32 regular/near samples (FP64 displacement and phase), FP64 touching
                                pairs, FP32 LU, FP64 iterative refinement to min(tolerance, 1e-10) */
 } hs_precision;
+/* Interaction planner of a session (hs_bem_session_set_planner). */
+typedef enum hs_planner { HS_PLANNER_DEVICE = 0, HS_PLANNER_HOST = 1 } hs_planner;
 typedef enum hs_residency { HS_RESIDENCY_AUTOMATIC = 0, HS_RESIDENCY_DEVICE = 1, HS_RESIDENCY_MAPPED_HOST = 2 } hs_residency; /* bem.hpp:361-365 */
 
 /* BemNumerics + FastMultipoleSettings (bem.hpp:61-72, 113-123). */
@@ -275,6 +277,19 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
                             size_t triangle_count, const hs_numerics *numerics, double max_k, size_t *sizes,
                             uint32_t *touching, uint32_t *near, double *patches, uint8_t *whole,
                             uint32_t *near_offsets, uint32_t *near_trials);
+/* The same plan from the device planner (mode 0: on the current CUDA device;
+ * mode 1: its algorithm emulated on the host, one lane per warp, no GPU
+ * needed). No reference counterpart beyond makeInteractionPlan itself
+ * (interaction_plan.cpp:156): the result equals hs_bem_debug_plan's bit for
+ * bit. stats (6 doubles, may be NULL): pairs refined on the device, pairs on
+ * projected patches (refined by the host), device pairs handed to the host
+ * because a decision fell within its rounding bound, whole-panel pairs
+ * decided on the device (all-pairs mode), device milliseconds, host
+ * milliseconds. */
+hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, const uint32_t *triangles,
+                                   size_t triangle_count, const hs_numerics *numerics, double max_k, uint32_t mode,
+                                   double *stats, size_t *sizes, uint32_t *touching, uint32_t *near,
+                                   double *patches, uint8_t *whole, uint32_t *near_offsets, uint32_t *near_trials);
 hs_status hs_bem_debug_assemble(hs_bem_session *session, const hs_numerics *numerics, double plan_k, double k,
                                 const double *flux, double *matrix, double *rhs);
 /* LU test hook: factors `batch` complex n x n matrices (host, column-major,
@@ -309,6 +324,16 @@ hs_status hs_bem_debug_fmm_far(hs_bem_session *session, const hs_numerics *numer
                                size_t near_capacity, size_t *near_count, uint32_t *level_info, size_t level_capacity,
                                size_t *level_count);
 hs_status hs_bem_debug_fmm_selftest(double *error);
+/* Interaction planner of a session (makeInteractionPlan,
+ * interaction_plan.cpp:156): HS_PLANNER_DEVICE (default) classifies the
+ * panel pairs and runs the adaptive near-pair refinement on the session's
+ * device, handing the pairs on projected patches and any pair whose decisions
+ * fall within the device's rounding bounds to the host planner's code;
+ * HS_PLANNER_HOST plans on host threads like the reference. Both give the
+ * same plan bit for bit. hs_bem_session_plan_stats writes the last device
+ * plan's statistics (6 doubles, the layout of hs_bem_debug_plan_device). */
+hs_status hs_bem_session_set_planner(hs_bem_session *session, uint32_t planner);
+hs_status hs_bem_session_plan_stats(hs_bem_session *session, double *stats);
 /* Fast-multipole LF/HF switch (wideband_transfer.cpp:266-310): a level's M2L
  * runs in the diagonal plane-wave form when k times its shortest M2L distance
  * is at least `threshold` (default 8) and its order is at least 8; below, the
