@@ -716,6 +716,50 @@ def run_serve(args):
     print(json.dumps(line), flush=True)
 
 
+PLAN_CASES = [
+    ("C1 icosphere s3", lambda hs: hs.meshes.icosphere(3), 5000.0, {}),
+    ("C2 horn h 7.15 mm", lambda hs: hs.meshes.exponential_horn(), 8000.0, {}),
+    ("horn h 12.8 mm (all-pairs mode)", lambda hs: hs.meshes.exponential_horn(h=0.0128), 8000.0, {}),
+    ("short horn h 12.8 mm, tol 1e-5 (all-pairs mode)",
+     lambda hs: hs.meshes.exponential_horn(length=0.1, mouth_radius=0.05, h=0.0128), 1000.0,
+     {"near_relative_tolerance": 1e-5}),
+]
+
+
+def run_plan(args):
+    """Interaction planning (makeInteractionPlan) on the GPU against the host
+    planner on all host threads, same mesh and planning wavenumber; wall
+    clock of each, the device planner's statistics and whether the two plans
+    are equal bit for bit. One JSON line per mesh."""
+    import os
+
+    import numpy as np
+    import torch
+
+    import hornsculpt_b200 as hs
+
+    torch.cuda.set_device(0)
+    cases = [c for i, c in enumerate(PLAN_CASES) if not args.c3_cases or str(i) in args.c3_cases.split(",")]
+    hs.device_plan(hs.meshes.icosphere(2), hs.BemNumerics(), 10.0)  # context and module load
+    for name, make, f, kw in cases:
+        mesh = make(hs)
+        k = 2 * np.pi * f / SOUND_SPEED
+        numerics = hs.BemNumerics(**kw)
+        t0 = time.perf_counter()
+        d = hs.device_plan(mesh, numerics, k)
+        t1 = time.perf_counter()
+        h = hs.host_plan(mesh, numerics, k)
+        t2 = time.perf_counter()
+        equal = all(np.array_equal(d[key], h[key]) for key in ("touching", "near", "patches", "whole", "trials",
+                                                                 "offsets"))
+        line = {"workload": "interaction planning", "mesh": name, "T": mesh.triangle_count, "frequency_hz": f,
+                "numerics": kw, "device_planner_s": round(t1 - t0, 3), "host_planner_s": round(t2 - t1, 3),
+                "speedup": round((t2 - t1) / (t1 - t0), 2), "host_threads": os.cpu_count(),
+                "plans_equal_bit_for_bit": equal, "near_jobs": int(len(h["near"])), "patches": int(len(h["patches"])),
+                "whole_panel_bytes": int(len(h["whole"])), "stats": {k2: round(v, 3) for k2, v in d["stats"].items()}}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -728,11 +772,12 @@ def main():
                     help="solve only n sweep frequencies (small profiling cases)")
     ap.add_argument("--first-frequency", type=int, default=0,
                     help="index of the first sweep frequency solved (small profiling cases)")
-    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4", "serve", "refgpu"],
+    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4", "serve", "refgpu", "plan"],
                     help="c1: the headline sweep; c2: the 12.8k-triangle horn sweep (dense forms); "
                          "c3: mixed dense sizes N = 2k-16k (one line per mesh); "
                          "c4: 64-frequency sweeps on icospheres s4/s5; "
-                         "serve: the serving loop on a seeded Poisson horn stream")
+                         "serve: the serving loop on a seeded Poisson horn stream; "
+                         "plan: interaction planning on the device against the host planner")
     ap.add_argument("--c3-cases", default="", help="c3/c4: comma-separated case indices (default: all)")
     ap.add_argument("--c2-h", type=float, default=0.0,
                     help="C2 edge length in metres (0: 7.15 mm, the spec's lambda(8 kHz)/6)")
@@ -760,6 +805,8 @@ def main():
         return run_serve(args)
     if args.workload == "refgpu":
         return run_refgpu(args)
+    if args.workload == "plan":
+        return run_plan(args)
 
     import numpy as np
     import torch

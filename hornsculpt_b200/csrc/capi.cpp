@@ -475,6 +475,25 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
     });
 }
 
+namespace {
+// The last device plan of this thread, so that the size query and the fill
+// call of hs_bem_debug_plan_device plan once. Keyed by the inputs' bytes.
+struct DevicePlanCache {
+    uint64_t key = 0;
+    bool valid = false;
+    hsb::Plan plan;
+    hsb::DevicePlanStats stats;
+};
+thread_local DevicePlanCache tDevicePlanCache;
+
+uint64_t hashBytes(uint64_t h, const void *data, size_t bytes) {
+    const unsigned char *p = static_cast<const unsigned char *>(data);
+    for (size_t i = 0; i < bytes; ++i)
+        h = (h ^ p[i]) * 1099511628211ull;
+    return h;
+}
+}  // namespace
+
 hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, const uint32_t *triangles,
                                    size_t triangle_count, const hs_numerics *numerics, double max_k, uint32_t mode,
                                    double *stats, size_t *sizes, uint32_t *touching, uint32_t *near,
@@ -482,15 +501,27 @@ hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, 
     if (!vertices || !vertex_count || !triangles || !triangle_count || !numerics || !sizes || mode > 1)
         return fail(HS_E_INVALID, "Mesh, numerics and sizes must be non-null and the mode 0 or 1.");
     return guarded([&]() {
-        const Space space = debugSpace(vertices, vertex_count, triangles, triangle_count);
-        DevicePlanStats st;
-        const Plan p = makePlanOnDevice(space, planSettings(numerics), max_k, nullptr, nullptr, &st, mode == 1);
-        if (mode == 0)
-        {
-            const cudaError_t e = cudaDeviceSynchronize();
-            if (e != cudaSuccess)
-                throw CudaError(std::string("CUDA synchronization: ") + cudaGetErrorString(e));
+        uint64_t key = 1469598103934665603ull;
+        key = hashBytes(key, vertices, vertex_count * 3 * sizeof(double));
+        key = hashBytes(key, triangles, triangle_count * 3 * sizeof(uint32_t));
+        key = hashBytes(key, numerics, sizeof(hs_numerics));
+        key = hashBytes(key, &max_k, sizeof(max_k));
+        key = hashBytes(key, &mode, sizeof(mode));
+        DevicePlanCache &c = tDevicePlanCache;
+        if (!c.valid || c.key != key) {
+            c.valid = false;
+            const Space space = debugSpace(vertices, vertex_count, triangles, triangle_count);
+            c.stats = DevicePlanStats{};
+            c.plan = makePlanOnDevice(space, planSettings(numerics), max_k, nullptr, nullptr, &c.stats, mode == 1);
+            if (mode == 0) {
+                const cudaError_t e = cudaDeviceSynchronize();
+                if (e != cudaSuccess)
+                    throw CudaError(std::string("CUDA synchronization: ") + cudaGetErrorString(e));
+            }
+            c.key = key;
+            c.valid = true;
         }
+        const DevicePlanStats &st = c.stats;
         if (stats) {
             stats[0] = double(st.devicePairs);
             stats[1] = double(st.projectedPairs);
@@ -498,8 +529,11 @@ hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, 
             stats[3] = double(st.wholePanelPairs);
             stats[4] = st.deviceMs;
             stats[5] = st.hostMs;
+            stats[6] = double(st.resolvedPairs);
         }
-        writePlan(p, sizes, touching, near, patches, whole, near_offsets, near_trials);
+        writePlan(c.plan, sizes, touching, near, patches, whole, near_offsets, near_trials);
+        if (touching || near || patches || whole || near_offsets || near_trials)
+            c.valid = false;  // filled: the next call plans again
     });
 }
 
@@ -590,6 +624,7 @@ hs_status hs_bem_session_plan_stats(hs_bem_session *s, double *stats) {
         stats[3] = double(st.wholePanelPairs);
         stats[4] = st.deviceMs;
         stats[5] = st.hostMs;
+        stats[6] = double(st.resolvedPairs);
     });
 }
 

@@ -45,7 +45,7 @@ struct LeafHdr {
 };
 
 struct PairRecord {
-    uint32_t first, second, patchFirst, count, maxDepth, pad;
+    uint32_t first, second, patchFirst, count, maxDepth, uncertain;  // uncertain: runs of unknown order
     double relError;
 };
 
@@ -407,17 +407,23 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
             if (!isfinite(relError) || relError > P.tol)
                 return kPairHost;
             const uint32_t count = nAtl + nPend;
+            // Descending device errors. Each host error lies within kSafety
+            // errB of the device's; where those intervals overlap (a run of
+            // leaves whose order the device cannot know), the leaves after the
+            // first are marked and the host orders the run by its own
+            // estimates. Runs never overlap one another, so the order between
+            // runs is the host's.
+            double runLow = INFINITY;
             for (uint32_t k = 0; k < nPend; ++k) {
                 const Top2 top = topTwo(w, M.pendErr, nPend);
-                if (top.p2 != 0xffffffffu && top.e2 >= 0) {
-                    const double b1 = M.hdr[M.pend[top.p1]].errB, b2 = M.hdr[M.pend[top.p2]].errB;
-                    if (!separated(top.e1, top.e2, b1 + b2))
-                        return kPairHost;
-                }
+                const double B = kSafety * M.hdr[M.pend[top.p1]].errB;
+                const bool joins = top.e1 + B >= runLow;
+                runLow = joins ? fmin(runLow, top.e1 - B) : top.e1 - B;
                 w.sync();
                 if (w.leader()) {
                     M.atl[nAtl + k] = M.pend[top.p1];
-                    M.pendErr[top.p1] = -1;
+                    M.pendErr[top.p1] = -1;  // removed
+                    M.hdr[M.pend[top.p1]].pad = joins ? 1 : 0;
                 }
                 w.sync();
             }
@@ -427,6 +433,9 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
                 maxDepth = h.depth > maxDepth ? h.depth : maxDepth;
                 degree0 = k == 0 ? h.degree : degree0;
             }
+            uint32_t uncertain = 0;
+            for (uint32_t k = nAtl; k < count; ++k)
+                uncertain |= M.hdr[M.atl[k]].pad != 0 ? 1u : 0u;
             if (P.allPairs && maxDepth == 0 && count == 1) {
                 if (w.leader())
                     O.whole[unorderedPairIndex(ti, si)] = uint8_t(degree0);
@@ -454,7 +463,7 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
                 p.degree = h.degree;
                 p.projection = 0;
                 p.intervals = 1;
-                p.pad = 0;
+                p.pad = k >= nAtl && h.pad != 0 ? 1u : 0u;  // joins the run before it (order unknown)
                 O.pool[first + k] = p;
             }
             if (w.leader()) {
@@ -464,7 +473,7 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
 #else
                 slot = __atomic_fetch_add(O.recordCount, 1ull, __ATOMIC_RELAXED);
 #endif
-                O.records[slot] = PairRecord{ti, si, uint32_t(first), count, maxDepth, 0, relError};
+                O.records[slot] = PairRecord{ti, si, uint32_t(first), count, maxDepth, uncertain, relError};
             }
             return kPairRule;
         }
@@ -696,7 +705,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             A.rules.pts[r] = rules[r].data(), A.rules.n[r] = int(rules[r].size() / 4);
         if (f.allPairs)
             whole.assign(units, 0);
-        pool.resize(size_t(16) * deviceList.size() + 4096);
+        pool.resize(size_t(32) * deviceList.size() + 65536);
         records.resize(deviceList.size());
         unsigned long long poolUsed = 0, recordCount = 0;
         PairOutput O{pool.data(), pool.size(), &poolUsed, records.data(), &recordCount, whole.data()};
@@ -852,8 +861,70 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
 #endif
     }
     const double deviceMs = msSince(t0);
-    // the host refines projected and flagged pairs
     const auto t1 = Clock::now();
+    // Runs of leaves whose order the device could not decide: the host
+    // orders each by its own error estimates (pair_quadrature.cpp:644-683 as
+    // the host planner evaluates them); a tie among them leaves the order to
+    // the host planner's heap, so such a pair is refined on the host.
+    size_t resolved = 0;
+    {
+        std::vector<size_t> uncertain;
+        for (size_t r = 0; r < records.size(); ++r)
+            if (records[r].uncertain)
+                uncertain.push_back(r);
+        std::vector<uint8_t> tie(uncertain.size(), 0);
+        std::atomic<size_t> next{0};
+        const unsigned workers = std::max(1u, std::min<unsigned>(64, std::thread::hardware_concurrency()));
+        std::vector<std::thread> threads;
+        for (unsigned wkr = 0; wkr < std::min<size_t>(workers, uncertain.size()); ++wkr)
+            threads.emplace_back([&]() {
+                std::vector<std::pair<double, Patch>> run;
+                for (;;) {
+                    const size_t u = next.fetch_add(1);
+                    if (u >= uncertain.size())
+                        return;
+                    const PairRecord &rec = records[uncertain[u]];
+                    Patch *pp = pool.data() + rec.patchFirst;
+                    const HostPanel &t = sp.panels[rec.first], &s = sp.panels[rec.second];
+                    for (uint32_t k = 0; k < rec.count;) {
+                        uint32_t e = k + 1;
+                        while (e < rec.count && pp[e].pad)
+                            ++e;
+                        if (e - k > 1) {
+                            run.clear();
+                            for (uint32_t q = k; q < e; ++q) {
+                                pp[q].pad = 0;
+                                run.emplace_back(hostPatchError(t, s, pp[q], maxK), pp[q]);
+                            }
+                            std::stable_sort(run.begin(), run.end(),
+                                             [](const auto &x, const auto &y) { return x.first > y.first; });
+                            for (size_t q = 1; q < run.size(); ++q)
+                                tie[u] |= run[q].first == run[q - 1].first ? 1 : 0;
+                            for (size_t q = 0; q < run.size(); ++q)
+                                pp[k + q] = run[q].second;
+                        }
+                        k = e;
+                    }
+                }
+            });
+        for (auto &th : threads)
+            th.join();
+        std::vector<uint8_t> drop(records.size(), 0);
+        for (size_t u = 0; u < uncertain.size(); ++u) {
+            if (tie[u]) {
+                drop[uncertain[u]] = 1;
+                flagged.push_back(make_uint2(records[uncertain[u]].first, records[uncertain[u]].second));
+            } else {
+                ++resolved;
+            }
+        }
+        size_t kept = 0;
+        for (size_t r = 0; r < records.size(); ++r)
+            if (!drop[r])
+                records[kept++] = records[r];
+        records.resize(kept);
+    }
+    // the host refines projected and flagged pairs
     std::vector<std::pair<uint32_t, uint32_t>> hostPairs;
     hostPairs.reserve(hostList.size() + flagged.size());
     for (const auto &p : hostList)
@@ -894,6 +965,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         stats->devicePairs = devicePairs;
         stats->projectedPairs = hostList.size();
         stats->flaggedPairs = flagged.size();
+        stats->resolvedPairs = resolved;
         size_t wholeCount = 0;
         for (const auto b : whole)
             wholeCount += b != 0;

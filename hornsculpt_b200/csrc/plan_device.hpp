@@ -27,6 +27,7 @@ struct DevicePlanStats {
     size_t projectedPairs{};   // pairs with projected patches (host)
     size_t flaggedPairs{};     // device pairs handed back to the host
     size_t wholePanelPairs{};  // all-pairs mode: single whole-panel rules decided on the device
+    size_t resolvedPairs{};    // device pairs whose patch order the host settled by its own estimates
     double deviceMs{}, hostMs{};
 };
 

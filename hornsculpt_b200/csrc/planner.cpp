@@ -607,6 +607,21 @@ std::vector<PairRule> planPairsOnHost(const Space &sp, const PlanSettings &st, d
     return rules;
 }
 
+double hostPatchError(const HostPanel &t, const HostPanel &s, const Patch &p, double k) {
+    // a tensor patch's sub-triangles; fractions are powers of 1/4, so the
+    // product in the sample weight is the same with the whole fraction on the
+    // test side
+    Sub a{}, b{};
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            a.v[i][j] = p.test[3 * i + j];
+            b.v[i][j] = p.trial[3 * i + j];
+        }
+    a.fraction = p.areaFraction;
+    b.fraction = 1;
+    return estimate(t, s, a, b, p.degree, false, 1, k).error;
+}
+
 Plan makePlan(const Space &sp, const PlanSettings &st, double maxK, unsigned threads, const volatile int32_t *cancel) {
     PlanFrame f = beginPlan(sp, st, maxK);
     const size_t T = sp.panels.size();

@@ -66,6 +66,9 @@ void finishPlan(Plan &plan, size_t triangleCount);
 std::vector<PairRule> planPairsOnHost(const Space &space, const PlanSettings &settings, double maxK,
                                       const std::vector<std::pair<uint32_t, uint32_t>> &pairs, unsigned threads,
                                       const volatile int32_t *cancel);
+// The host planner's embedded-rule error estimate of one tensor patch of the
+// pair (t, s), bit for bit the value its refinement compares.
+double hostPatchError(const HostPanel &t, const HostPanel &s, const Patch &patch, double k);
 // Parallel over host threads (at most `threads`, 0 = hardware concurrency).
 // The result does not depend on the thread count.
 Plan makePlan(const Space &space, const PlanSettings &settings, double maxK, unsigned threads,

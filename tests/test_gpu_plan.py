@@ -57,7 +57,8 @@ def test_device_plan_equals_host_plan(name, make, f, kw):
     s = d["stats"]
     print(f"{name}: T={mesh.triangle_count} device plan {1e3 * (t1 - t0):.1f} ms (device {s['device_ms']:.1f}, host "
           f"{s['host_ms']:.1f}), host planner {1e3 * (t2 - t1):.1f} ms; pairs {s['device_pairs']:.0f} on the device, "
-          f"{s['flagged_pairs']:.0f} handed back, {s['projected_pairs']:.0f} projected")
+          f"{s['flagged_pairs']:.0f} handed back, {s['resolved_pairs']:.0f} ordered by the host, "
+          f"{s['projected_pairs']:.0f} projected")
     assert s["device_pairs"] > 0
     assert s["flagged_pairs"] <= 0.01 * s["device_pairs"]
 
