@@ -530,6 +530,8 @@ hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, 
             stats[4] = st.deviceMs;
             stats[5] = st.hostMs;
             stats[6] = double(st.resolvedPairs);
+            for (int i = 0; i < 5; ++i)
+                stats[7 + i] = st.phaseMs[i];
         }
         writePlan(c.plan, sizes, touching, near, patches, whole, near_offsets, near_trials);
         if (touching || near || patches || whole || near_offsets || near_trials)
@@ -625,6 +627,8 @@ hs_status hs_bem_session_plan_stats(hs_bem_session *s, double *stats) {
         stats[4] = st.deviceMs;
         stats[5] = st.hostMs;
         stats[6] = double(st.resolvedPairs);
+        for (int i = 0; i < 5; ++i)
+            stats[7 + i] = st.phaseMs[i];
     });
 }
 

@@ -673,6 +673,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                       const volatile int32_t *cancel, DevicePlanStats *stats, bool emulate) {
     const auto t0 = Clock::now();
     PlanFrame f = beginPlan(sp, st, maxK);
+    double phase[5] = {msSince(t0), 0, 0, 0, 0};  // frame, classification, refinement, readback, flattening
     const uint32_t T = uint32_t(sp.panels.size());
     const unsigned long long units =
         f.allPairs ? (unsigned long long)T * (T - 1) / 2 : (unsigned long long)f.candidates.size();
@@ -700,6 +701,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             else if (c == kProjected)
                 hostList.push_back(make_uint2(i, j));
         }
+        phase[1] = msSince(t0);
         AdaptiveParams A{sp.panels.data(), {}, maxK, st.tol, st.maxDepth, f.allPairs ? 1 : 0};
         for (int r = 0; r < 4; ++r)
             A.rules.pts[r] = rules[r].data(), A.rules.n[r] = int(rules[r].size() / 4);
@@ -731,6 +733,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             });
         for (auto &th : threads)
             th.join();
+        phase[2] = msSince(t0);
         records.resize(recordCount);
         pool.resize(std::min<size_t>(poolUsed, pool.size()));
         devicePairs = deviceList.size();
@@ -780,6 +783,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             check(cudaStreamSynchronize(stream), "planner classification");
         }
         const unsigned long long nDevice = n2[0], nHost = n2[1];
+        phase[1] = msSince(t0);
         DevMem dDeviceList(sizeof(uint2) * nDevice), dHostList(sizeof(uint2) * nHost);
         if (units) {
             check(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), stream), "planner reset");
@@ -835,6 +839,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             check(cudaStreamSynchronize(stream), "planner refinement");
         }
         unsigned long long n5[5] = {};
+        phase[2] = msSince(t0);
         check(cudaMemcpyAsync(n5, counters, sizeof(n5), cudaMemcpyDeviceToHost, stream), "planner readback");
         check(cudaStreamSynchronize(stream), "planner readback");
         const unsigned long long used = std::min<unsigned long long>(n5[2], poolCap), nRec = n5[3], nFlag = n5[4];
@@ -861,6 +866,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
 #endif
     }
     const double deviceMs = msSince(t0);
+    phase[3] = deviceMs;
     const auto t1 = Clock::now();
     // Runs of leaves whose order the device could not decide: the host
     // orders each by its own error estimates (pair_quadrature.cpp:644-683 as
@@ -949,6 +955,13 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         for (unsigned long long u = 0; u < units; ++u)
             if (whole[u])
                 f.plan.wholePanelDegrees[u] = whole[u];
+    {
+        size_t patches = pool.size();
+        for (const auto &r : hostRules)
+            patches += r.patches.size();
+        f.plan.patches.reserve(patches);
+        f.plan.near.reserve(2 * items.size());
+    }
     for (const auto &it : items) {
         const uint32_t i = uint32_t(it.key >> 32), j = uint32_t(it.key & 0xffffffffu);
         if (it.host >= 0) {
@@ -961,6 +974,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         }
     }
     finishPlan(f.plan, T);
+    phase[4] = msSince(t0);
     if (stats) {
         stats->devicePairs = devicePairs;
         stats->projectedPairs = hostList.size();
@@ -971,6 +985,8 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             wholeCount += b != 0;
         stats->wholePanelPairs = wholeCount;
         stats->deviceMs = deviceMs;
+        for (int i = 0; i < 5; ++i)  // phase durations
+            stats->phaseMs[i] = phase[i] - (i ? phase[i - 1] : 0.0);
         stats->hostMs = msSince(t1);
     }
     return std::move(f.plan);

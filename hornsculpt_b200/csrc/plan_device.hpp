@@ -29,6 +29,9 @@ struct DevicePlanStats {
     size_t wholePanelPairs{};  // all-pairs mode: single whole-panel rules decided on the device
     size_t resolvedPairs{};    // device pairs whose patch order the host settled by its own estimates
     double deviceMs{}, hostMs{};
+    // frame (validation, bounds, touching jobs, candidates), classification,
+    // refinement, readback, host part (runs, host pairs, flattening)
+    double phaseMs[5]{};
 };
 
 // The plan of makePlan, with the adaptive pairs refined on the current CUDA
