@@ -10,6 +10,7 @@
 // moment sums use explicit fma(), and their rounding is covered by the bounds
 // below.
 #include "plan_device.hpp"
+#include "device_once.hpp"
 #include "planner_geom.cuh"
 
 #include <math.h>
@@ -38,10 +39,21 @@ constexpr double kSafety = 4;
 enum : uint8_t { kSkip = 0, kOnDevice = 1, kProjected = 2 };
 enum : int { kPairRule = 0, kPairWhole = 1, kPairHost = 2 };
 
+// A leaf: its sub-triangles, also as quadtree paths from the whole panels
+// (2 bits per halving, child order of quarter()), and its estimate.
 struct LeafHdr {
     Sub a, b;
-    double error, errB, intB, da, db, pad;
-    uint32_t depth, degree;
+    double error, errB, intB, da, db;
+    uint32_t depth, degree, pathA, pathB, depthA, depthB, joins, pad;
+};
+
+// A patch as the device writes it: the two quadtree paths, the degree and
+// whether its order against the patch before it is left to the host. The host
+// rebuilds the barycentric vertices by replaying quarter() along the paths,
+// the operations the refinement performed.
+struct PatchCode {
+    uint32_t pathA, pathB;
+    uint8_t depthA, depthB, degree, joins;
 };
 
 struct PairRecord {
@@ -76,11 +88,12 @@ struct WarpMem {
     uint32_t *pend;
     double *pendErr;
     uint32_t *atl;
-    double *pts;  // test and trial point tables, 2 x kRulePoints x kPts
+    double *pts;   // test and trial point tables, 2 x kRulePoints x kPts
+    double *rows;  // row items of a moment computation, kRulePoints x kRowValues
 };
 
 struct PairOutput {
-    Patch *pool;
+    PatchCode *pool;
     unsigned long long poolCap, *poolUsed;
     PairRecord *records;
     unsigned long long *recordCount;
@@ -115,38 +128,23 @@ struct DeviceWarp {
 };
 #endif
 
-// Per sample the lanes accumulate 72 moment values (36 complex, index
-// 2 (9c + 3i + j) + re/im) and 4 magnitude sums (values 72..75); padded to
-// 128, a reduce-scatter leaves lane l with values [128/W l, 128/W (l+1)).
+// Moment values: 72 (36 complex, index 2 (9c + 3i + j) + re/im, channel c,
+// test function i, trial function j) and 4 magnitude sums (values 72..75).
+// After a moment computation lane l holds values [128/W l, 128/W (l+1)).
 constexpr int kValues = 128;
-
-HS_HD void reduceScatter(const LaneWarp &, double *) {}
-#if defined(__CUDACC__)
-template <int HALF> __device__ __forceinline__ void scatterStep(double *acc, int lane, int off) {
-    const bool up = lane & off;
-#pragma unroll
-    for (int v = 0; v < HALF; ++v) {
-        const double send = up ? acc[v] : acc[v + HALF];
-        const double keep = up ? acc[v + HALF] : acc[v];
-        acc[v] = keep + __shfl_xor_sync(~0u, send, off);
-    }
-}
-__device__ void reduceScatter(const DeviceWarp &w, double *acc) {
-    const int lane = w.lane();
-    scatterStep<64>(acc, lane, 16);
-    scatterStep<32>(acc, lane, 8);
-    scatterStep<16>(acc, lane, 4);
-    scatterStep<8>(acc, lane, 2);
-    scatterStep<4>(acc, lane, 1);
-}
-#endif
+constexpr int kRowValues = 28;  // per row item: 12 complex inner sums and 4 magnitude sums
 
 // Tensor moments of one rule over sub-triangles a (test) and b (trial)
-// (the host's tensorMoments): lane-strided samples, then the reduce-scatter.
-// `own` receives the lane's values; `bad` is set for a coincident point.
+// (the host's tensorMoments). The test barycentrics depend on the test point
+// only, so each lane sums one row of trial points (a test point, or a share
+// of its trial points when rows are short) into 12 complex inner sums
+// In[c][j] = sum_q ker_c w bs_j, kept in `rows`; then the owners of the
+// moment values add bt_i In[c][j] over the rows. `own` receives the lane's
+// values; `bad` is set for a coincident point.
 template <class Wp>
 HS_HD void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, const Sub &a, const Sub &b,
-                         const double *rule, int n, double k, double scale, double *pts, double *own, bool &bad) {
+                         const double *rule, int n, double k, double scale, double *pts, double *rows, double *own,
+                         bool &bad) {
     constexpr int W = Wp::W;
     for (int q = w.lane(); q < n; q += W) {
         const double *x = rule + 4 * q;
@@ -164,53 +162,70 @@ HS_HD void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, co
     w.sync();
     const V3 origin = t.v[0] - s.v[0];
     const double fab = a.fraction * b.fraction;
-    double acc[kValues];
+    const int split = n < W ? W / n : 1, items = n * split;  // lanes per test point
+    for (int it = w.lane(); it < items; it += W) {
+        const int xi = it / split, h = it - xi * split;
+        const double *T = pts + kPts * xi;
+        const double tx = T[3], ty = T[4], tz = T[5], tw = T[6] * fab;
+        double in[24], m[4] = {0, 0, 0, 0};
 #pragma unroll
-    for (int v = 0; v < kValues; ++v)
-        acc[v] = 0;
-    for (int smp = w.lane(); smp < n * n; smp += W) {
-        const int xi = smp / n, qi = smp - xi * n;
-        const double *T = pts + kPts * xi, *S = pts + kPts * (kRulePoints + qi);
-        const V3 d{origin.x + (T[3] - S[3]), origin.y + (T[4] - S[4]), origin.z + (T[5] - S[5])};
-        const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
-        if (!(r > 0)) {
-            bad = true;
-            continue;
-        }
-        double sn, cs;
-        sincos(-k * r, &sn, &cs);  // exp(-i k r)
-        const double ir = 1 / r, gr = cs * ir, gi = sn * ir, kr = k * r, f = scale * ir * ir;
-        const double dr = (-gr + gi * kr) * f, di = (-gr * kr - gi) * f;
-        const double kre[4] = {gr, dr * d.x, dr * d.y, dr * d.z};
-        const double kim[4] = {gi, di * d.x, di * d.y, di * d.z};
-        const double wgt = T[6] * S[6] * fab;
+        for (int v = 0; v < 24; ++v)
+            in[v] = 0;
+        for (int qi = h; qi < n; qi += split) {
+            const double *S = pts + kPts * (kRulePoints + qi);
+            const V3 d{origin.x + (tx - S[3]), origin.y + (ty - S[4]), origin.z + (tz - S[5])};
+            const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+            if (!(r > 0)) {
+                bad = true;
+                continue;
+            }
+            double sn, cs;
+            sincos(-k * r, &sn, &cs);  // exp(-i k r)
+            const double ir = 1 / r, gr = cs * ir, gi = sn * ir, kr = k * r, f = scale * ir * ir;
+            const double dr = (-gr + gi * kr) * f, di = (-gr * kr - gi) * f;
+            const double wgt = tw * S[6];
+            const double kre[4] = {gr, dr * d.x, dr * d.y, dr * d.z};
+            const double kim[4] = {gi, di * d.x, di * d.y, di * d.z};
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const double wb = wgt * S[j];
+            for (int j = 0; j < 3; ++j) {
+                const double wb = wgt * S[j];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const double br = kre[c] * wb, bi = kim[c] * wb;
-#pragma unroll
-                for (int i = 0; i < 3; ++i) {
-                    const int v = 2 * (9 * c + 3 * i + j);
-                    acc[v] = fma(T[i], br, acc[v]);
-                    acc[v + 1] = fma(T[i], bi, acc[v + 1]);
+                for (int c = 0; c < 4; ++c) {
+                    in[2 * (3 * c + j)] = fma(kre[c], wb, in[2 * (3 * c + j)]);
+                    in[2 * (3 * c + j) + 1] = fma(kim[c], wb, in[2 * (3 * c + j) + 1]);
                 }
             }
+            // magnitude of each channel's terms: |G| = 1/r, |grad G| <= (1 + kr)/r^2
+            const double md = wgt * (1 + kr) * f * ir;
+            m[0] += wgt * ir;
+            m[1] += md * fabs(d.x);
+            m[2] += md * fabs(d.y);
+            m[3] += md * fabs(d.z);
         }
-        // magnitude of each channel's terms: |G| = 1/r, |grad G| <= (1 + kr)/r^2
-        const double m0 = wgt * ir, md = wgt * (1 + kr) * f * ir;
-        acc[72] += m0;
-        acc[73] += md * fabs(d.x);
-        acc[74] += md * fabs(d.y);
-        acc[75] += md * fabs(d.z);
-    }
-    w.sync();  // the point tables are rewritten by the next call
-    reduceScatter(w, acc);
-    constexpr int own_n = kValues / W;
+        double *R = rows + kRowValues * it;
 #pragma unroll
-    for (int v = 0; v < own_n; ++v)
-        own[v] = acc[v];
+        for (int v = 0; v < 24; ++v)
+            R[v] = in[v];
+        R[24] = m[0], R[25] = m[1], R[26] = m[2], R[27] = m[3];
+    }
+    w.sync();
+    constexpr int own_n = kValues / W;
+    const int base = own_n * w.lane();
+    for (int o = 0; o < own_n; ++o) {
+        const int v = base + o;
+        double acc = 0;
+        if (v < 72) {
+            const int comp = v >> 1, ri = v & 1, c = comp / 9, i = (comp % 9) / 3, j = comp % 3;
+            const int col = 2 * (3 * c + j) + ri;
+            for (int it = 0; it < items; ++it)
+                acc = fma(pts[kPts * (it / split) + i], rows[kRowValues * it + col], acc);
+        } else if (v < 76) {
+            for (int it = 0; it < items; ++it)
+                acc += rows[kRowValues * it + 24 + (v - 72)];
+        }
+        own[o] = acc;
+    }
+    w.sync();  // the point tables and rows are rewritten by the next call
 }
 
 // Embedded-rule estimate of one leaf (the host's estimate(), tensor form):
@@ -221,13 +236,17 @@ HS_HD void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, co
 //   errors, at most m u A_c each, and kernel values within 32 u);
 //   errB bounds |error_device - error_host|, intB a moment value.
 template <class Wp>
-HS_HD void estimateLeaf(const Wp &w, const HostPanel &t, const HostPanel &s, LeafHdr &L, const RuleTables &R,
-                        double k, double scale, double *pts, double *hiOwn, double &mnL, bool &bad) {
+HS_HD void estimateLeaf(const Wp &w, const HostPanel &t, const HostPanel &s, const LeafHdr &L, const RuleTables &R,
+                        double k, double scale, double *pts, double *rows, double *hiOwn, double &error,
+                        double &errB,
+                        double &intB, double &mnL, bool &bad) {
     constexpr int own_n = kValues / Wp::W;
     const int lo = L.degree == 8 ? 0 : 2, hi = lo + 1;
     double loOwn[own_n];
-    tensorMoments(w, t, s, L.a, L.b, R.pts[lo], R.n[lo], k, scale, pts, loOwn, bad);
-    tensorMoments(w, t, s, L.a, L.b, R.pts[hi], R.n[hi], k, scale, pts, hiOwn, bad);
+    // L lives in the warp's arena: its sub-triangles are read where the point
+    // tables are built and hold no registers during the sample loops
+    tensorMoments(w, t, s, L.a, L.b, R.pts[lo], R.n[lo], k, scale, pts, rows, loOwn, bad);
+    tensorMoments(w, t, s, L.a, L.b, R.pts[hi], R.n[hi], k, scale, pts, rows, hiOwn, bad);
     // magnitude sums live in values 72..75
     const int magLane = 72 / own_n, magOff = 72 - magLane * own_n;
     double Elo = 0, Ehi = 0;
@@ -251,10 +270,10 @@ HS_HD void estimateLeaf(const Wp &w, const HostPanel &t, const HostPanel &s, Lea
         hmax = fmax(hmax, hab);
     }
     bad = w.any(bad || nonFinite);
-    L.error = w.max(dmax);
+    error = w.max(dmax);
     mnL = w.max(hmax);
-    L.errB = 1.4142135623730951 * (Ehi + Elo) + 8 * kUnit * L.error;
-    L.intB = Ehi;
+    errB = 1.4142135623730951 * (Ehi + Elo) + 8 * kUnit * error;
+    intB = Ehi;
 }
 
 HS_HD bool separated(double x, double y, double bound) { return fabs(x - y) > kSafety * bound; }
@@ -306,14 +325,19 @@ template <class Wp> HS_HD Top2 topTwo(const Wp &w, const double *err, uint32_t n
 }
 
 HS_HD void writeLeaf(LeafHdr &h, const Sub &a, const Sub &b, const HostPanel &t, const HostPanel &s, uint32_t depth,
-                     uint32_t degree) {
+                     uint32_t degree, uint32_t pathA, uint32_t depthA, uint32_t pathB, uint32_t depthB) {
     h.a = a;
     h.b = b;
     h.da = subDiameter(t, a, t.v[0]);
     h.db = subDiameter(s, b, t.v[0]);
     h.depth = depth;
     h.degree = degree;
-    h.error = h.errB = h.intB = h.pad = 0;
+    h.pathA = pathA;
+    h.pathB = pathB;
+    h.depthA = depthA;
+    h.depthB = depthB;
+    h.error = h.errB = h.intB = 0;
+    h.joins = h.pad = 0;
 }
 
 // The largest-error refinement of one tensor pair (the host's adaptivePair
@@ -337,28 +361,28 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
     uint32_t req[4];
     int nReq = 0;
     if (w.leader())
-        writeLeaf(M.hdr[0], wholeSub(), wholeSub(), t, s, 0, 8);
+        writeLeaf(M.hdr[0], wholeSub(), wholeSub(), t, s, 0, 8, 0, 0, 0, 0);
     w.sync();
     req[nReq++] = nLeaf++;
     for (;;) {
         for (int r = 0; r < nReq; ++r) {
-            LeafHdr L = M.hdr[req[r]];
-            double hiOwn[own_n], mnL = 0;
+            const LeafHdr &L = M.hdr[req[r]];
+            double hiOwn[own_n], error = 0, errB = 0, leafIntB = 0, mnL = 0;
             bool bad = false;
-            estimateLeaf(w, t, s, L, P.rules, P.k, scale, M.pts, hiOwn, mnL, bad);
+            estimateLeaf(w, t, s, L, P.rules, P.k, scale, M.pts, M.rows, hiOwn, error, errB, leafIntB, mnL, bad);
             if (bad)
                 return kPairHost;
             for (int v = 0; v < own_n && base + v < 72; ++v)
                 M.integ[size_t(req[r]) * 72 + base + v] = hiOwn[v];
             w.sync();
             if (w.leader()) {
-                M.hdr[req[r]].error = L.error;
-                M.hdr[req[r]].errB = L.errB;
-                M.hdr[req[r]].intB = L.intB;
+                M.hdr[req[r]].error = error;
+                M.hdr[req[r]].errB = errB;
+                M.hdr[req[r]].intB = leafIntB;
             }
             // running sums, in the host's order
-            absError += L.error;
-            absB += L.errB + 2 * kUnit * absError;
+            absError += error;
+            absB += errB + 2 * kUnit * absError;
             double mnI = 0;
             for (int v = 0; v < own_n && base + v < 72; v += 2) {
                 integral[v] += hiOwn[v];
@@ -366,7 +390,7 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
                 mnI = fmax(mnI, hypot(integral[v], integral[v + 1]));
             }
             mnI = w.max(mnI);
-            intB += L.intB + 2 * kUnit * (mnI + mnL);
+            intB += leafIntB + 2 * kUnit * (mnI + mnL);
             w.sync();
             const bool outerLimit = L.depth == P.maxDepth && L.degree == 14;
             if (outerLimit) {
@@ -376,7 +400,7 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
             } else {
                 if (w.leader()) {
                     M.pend[nPend] = req[r];
-                    M.pendErr[nPend] = L.error;
+                    M.pendErr[nPend] = error;
                 }
                 ++nPend;
             }
@@ -423,7 +447,7 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
                 if (w.leader()) {
                     M.atl[nAtl + k] = M.pend[top.p1];
                     M.pendErr[top.p1] = -1;  // removed
-                    M.hdr[M.pend[top.p1]].pad = joins ? 1 : 0;
+                    M.hdr[M.pend[top.p1]].joins = joins ? 1 : 0;
                 }
                 w.sync();
             }
@@ -435,7 +459,7 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
             }
             uint32_t uncertain = 0;
             for (uint32_t k = nAtl; k < count; ++k)
-                uncertain |= M.hdr[M.atl[k]].pad != 0 ? 1u : 0u;
+                uncertain |= M.hdr[M.atl[k]].joins;
             if (P.allPairs && maxDepth == 0 && count == 1) {
                 if (w.leader())
                     O.whole[unorderedPairIndex(ti, si)] = uint8_t(degree0);
@@ -453,18 +477,9 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
                 return kPairHost;
             for (uint32_t k = w.lane(); k < count; k += Wp::W) {
                 const LeafHdr &h = M.hdr[M.atl[k]];
-                Patch p;
-                for (int i = 0; i < 3; ++i)
-                    for (int j = 0; j < 3; ++j) {
-                        p.test[3 * i + j] = h.a.v[i][j];
-                        p.trial[3 * i + j] = h.b.v[i][j];
-                    }
-                p.areaFraction = h.a.fraction * h.b.fraction;
-                p.degree = h.degree;
-                p.projection = 0;
-                p.intervals = 1;
-                p.pad = k >= nAtl && h.pad != 0 ? 1u : 0u;  // joins the run before it (order unknown)
-                O.pool[first + k] = p;
+                // joins: the order against the patch before it is the host's to settle
+                O.pool[first + k] = PatchCode{h.pathA, h.pathB, uint8_t(h.depthA), uint8_t(h.depthB),
+                                              uint8_t(h.degree), uint8_t(k >= nAtl && h.joins ? 1 : 0)};
             }
             if (w.leader()) {
                 unsigned long long slot;
@@ -503,7 +518,7 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
         w.sync();
         if (v.degree == 8 && (v.depth == P.maxDepth || (promoteRoot && v.depth == 0))) {
             if (w.leader())
-                writeLeaf(M.hdr[vSlot], v.a, v.b, t, s, v.depth, 14);
+                writeLeaf(M.hdr[vSlot], v.a, v.b, t, s, v.depth, 14, v.pathA, v.depthA, v.pathB, v.depthB);
             req[nReq++] = vSlot;
         } else {
             if (nPend + nAtl + 4 > 50000 || nLeaf + 3 > kLeafCap)
@@ -515,9 +530,11 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
                 const uint32_t slot = c == 0 ? vSlot : nLeaf++;
                 if (w.leader()) {
                     if (splitTest)
-                        writeLeaf(M.hdr[slot], children[c], v.b, t, s, v.depth + 1, 8);
+                        writeLeaf(M.hdr[slot], children[c], v.b, t, s, v.depth + 1, 8,
+                                  v.pathA | (uint32_t(c) << (2 * v.depthA)), v.depthA + 1, v.pathB, v.depthB);
                     else
-                        writeLeaf(M.hdr[slot], v.a, children[c], t, s, v.depth + 1, 8);
+                        writeLeaf(M.hdr[slot], v.a, children[c], t, s, v.depth + 1, 8, v.pathA, v.depthA,
+                                  v.pathB | (uint32_t(c) << (2 * v.depthB)), v.depthB + 1);
                 }
                 req[nReq++] = slot;
             }
@@ -597,12 +614,15 @@ __global__ void classifyKernel(ClassifyParams P, const uint2 *candidates, unsign
 
 constexpr int kWarpsPerBlock = 4;
 
+constexpr int kWarpSmemDoubles = 2 * kRulePoints * kPts + kRulePoints * kRowValues;
+constexpr size_t kRefineSmem = sizeof(double) * kWarpSmemDoubles * kWarpsPerBlock;
+
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) refineKernel(AdaptiveParams P, const uint2 *list,
                                                                      unsigned long long count,
                                                                      unsigned long long *next, WarpMem arena,
                                                                      PairOutput O, uint2 *flagged,
                                                                      unsigned long long *flagCount) {
-    __shared__ double pts[kWarpsPerBlock][2 * kRulePoints * kPts];
+    extern __shared__ double smem[];
     const DeviceWarp w;
     const int wInBlock = threadIdx.x >> 5;
     const size_t warpId = size_t(blockIdx.x) * kWarpsPerBlock + wInBlock;
@@ -612,7 +632,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) refineKernel(AdaptivePara
     M.pend = arena.pend + warpId * kLeafCap;
     M.pendErr = arena.pendErr + warpId * kLeafCap;
     M.atl = arena.atl + warpId * kLeafCap;
-    M.pts = pts[wInBlock];
+    M.pts = smem + size_t(kWarpSmemDoubles) * wInBlock;
+    M.rows = M.pts + 2 * kRulePoints * kPts;
     for (;;) {
         unsigned long long p = 0;
         if (w.leader())
@@ -634,6 +655,17 @@ void check(cudaError_t e, const char *what) {
         throw OutOfMemory(std::string(what) + ": " + cudaGetErrorString(e));
     if (e != cudaSuccess)
         throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// The sub-triangle at the end of a quadtree path (2 bits per level, child
+// order of quarter()), by the halvings the refinement performed.
+Sub subOfPath(uint32_t path, uint32_t depth) {
+    Sub cur = wholeSub(), children[4];
+    for (uint32_t l = 0; l < depth; ++l) {
+        quarter(cur, children);
+        cur = children[(path >> (2 * l)) & 3];
+    }
+    return cur;
 }
 
 struct DevMem {
@@ -680,7 +712,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
     const std::vector<double> rules[4] = {ruleRows(6), ruleRows(8), ruleRows(12), ruleRows(14)};
     std::vector<uint2> deviceList, hostList;
     std::vector<PairRecord> records;
-    std::vector<Patch> pool;
+    std::vector<PatchCode> pool;
     std::vector<uint8_t> whole;
     std::vector<uint2> flagged;
     size_t devicePairs = 0;
@@ -707,7 +739,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             A.rules.pts[r] = rules[r].data(), A.rules.n[r] = int(rules[r].size() / 4);
         if (f.allPairs)
             whole.assign(units, 0);
-        pool.resize(size_t(32) * deviceList.size() + 65536);
+        pool.resize(size_t(64) * deviceList.size() + 65536);
         records.resize(deviceList.size());
         unsigned long long poolUsed = 0, recordCount = 0;
         PairOutput O{pool.data(), pool.size(), &poolUsed, records.data(), &recordCount, whole.data()};
@@ -718,9 +750,10 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         for (unsigned wkr = 0; wkr < workers; ++wkr)
             threads.emplace_back([&]() {
                 std::vector<LeafHdr> hdr(kLeafCap);
-                std::vector<double> integ(size_t(kLeafCap) * 72), pendErr(kLeafCap), pts(2 * kRulePoints * kPts);
+                std::vector<double> integ(size_t(kLeafCap) * 72), pendErr(kLeafCap), pts(2 * kRulePoints * kPts),
+                    rows(size_t(kRulePoints) * kRowValues);
                 std::vector<uint32_t> pend(kLeafCap), atl(kLeafCap);
-                WarpMem M{hdr.data(), integ.data(), pend.data(), pendErr.data(), atl.data(), pts.data()};
+                WarpMem M{hdr.data(), integ.data(), pend.data(), pendErr.data(), atl.data(), pts.data(), rows.data()};
                 for (;;) {
                     const size_t p = next.fetch_add(1);
                     if (p >= deviceList.size())
@@ -800,8 +833,14 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         devicePairs = nDevice;
         // refinement: arenas for the resident warps, the patch pool sized by
         // the free memory
+        static PerDeviceOnce attributes;
+        attributes.run([] {
+            check(cudaFuncSetAttribute(refineKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kRefineSmem)),
+                  "planner kernel attribute");
+        });
         int blocksPerSm = 0;
-        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, refineKernel, 32 * kWarpsPerBlock, 0),
+        check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocksPerSm, refineKernel, 32 * kWarpsPerBlock,
+                                                            kRefineSmem),
               "planner occupancy");
         blocksPerSm = std::max(1, blocksPerSm);
         size_t freeBytes = 0, totalBytes = 0;
@@ -816,15 +855,15 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             dAtl(sizeof(uint32_t) * kLeafCap * warps);
         check(cudaMemGetInfo(&freeBytes, &totalBytes), "device memory query");
         const size_t poolCap =
-            std::max<size_t>(4096, std::min<size_t>(16 * nDevice + 4096, freeBytes / 4 / sizeof(Patch)));
-        DevMem dPool(sizeof(Patch) * poolCap), dRecords(sizeof(PairRecord) * std::max<unsigned long long>(nDevice, 1)),
+            std::max<size_t>(4096, std::min<size_t>(64 * nDevice + 4096, freeBytes / 4 / sizeof(PatchCode)));
+        DevMem dPool(sizeof(PatchCode) * poolCap), dRecords(sizeof(PairRecord) * std::max<unsigned long long>(nDevice, 1)),
             dFlagged(sizeof(uint2) * std::max<unsigned long long>(nDevice, 1));
         DevMem dWhole(f.allPairs ? units : 16);
         if (f.allPairs)
             check(cudaMemsetAsync(dWhole.p, 0, units, stream), "planner reset");
         WarpMem arena{dHdr.as<LeafHdr>(), dInteg.as<double>(), dPend.as<uint32_t>(), dPendErr.as<double>(),
-                      dAtl.as<uint32_t>(), nullptr};
-        PairOutput O{dPool.as<Patch>(), poolCap, counters + 2, dRecords.as<PairRecord>(), counters + 3,
+                      dAtl.as<uint32_t>(), nullptr, nullptr};
+        PairOutput O{dPool.as<PatchCode>(), poolCap, counters + 2, dRecords.as<PairRecord>(), counters + 3,
                      dWhole.as<uint8_t>()};
         // chunks of pairs, so a cancellation is seen between launches
         const unsigned long long chunk = 1ull << 20;
@@ -833,7 +872,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                 throw Cancelled();
             const unsigned long long n = std::min(chunk, nDevice - begin);
             check(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), stream), "planner reset");
-            refineKernel<<<unsigned(grid), 32 * kWarpsPerBlock, 0, stream>>>(
+            refineKernel<<<unsigned(grid), 32 * kWarpsPerBlock, kRefineSmem, stream>>>(
                 A, dDeviceList.as<uint2>() + begin, n, counters + 5, arena, O, dFlagged.as<uint2>(), counters + 4);
             check(cudaGetLastError(), "planner refinement");
             check(cudaStreamSynchronize(stream), "planner refinement");
@@ -851,7 +890,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                                   stream),
                   "planner readback");
         if (used)
-            check(cudaMemcpyAsync(pool.data(), dPool.p, sizeof(Patch) * used, cudaMemcpyDeviceToHost, stream),
+            check(cudaMemcpyAsync(pool.data(), dPool.p, sizeof(PatchCode) * used, cudaMemcpyDeviceToHost, stream),
                   "planner readback");
         if (nFlag)
             check(cudaMemcpyAsync(flagged.data(), dFlagged.p, sizeof(uint2) * nFlag, cudaMemcpyDeviceToHost, stream),
@@ -873,6 +912,39 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
     // the host planner evaluates them); a tie among them leaves the order to
     // the host planner's heap, so such a pair is refined on the host.
     size_t resolved = 0;
+    std::vector<Patch> patches(pool.size());
+    std::vector<uint8_t> joins(pool.size());
+    {
+        std::atomic<size_t> next{0};
+        const unsigned workers = std::max(1u, std::min<unsigned>(64, std::thread::hardware_concurrency()));
+        std::vector<std::thread> threads;
+        for (unsigned wkr = 0; wkr < std::min<size_t>(workers, (pool.size() + 4095) / 4096); ++wkr)
+            threads.emplace_back([&]() {
+                for (;;) {
+                    const size_t begin = next.fetch_add(4096);
+                    if (begin >= pool.size())
+                        return;
+                    for (size_t q = begin; q < std::min(pool.size(), begin + 4096); ++q) {
+                        const PatchCode &c = pool[q];
+                        const Sub a = subOfPath(c.pathA, c.depthA), b = subOfPath(c.pathB, c.depthB);
+                        Patch &p = patches[q];
+                        for (int i = 0; i < 3; ++i)
+                            for (int j = 0; j < 3; ++j) {
+                                p.test[3 * i + j] = a.v[i][j];
+                                p.trial[3 * i + j] = b.v[i][j];
+                            }
+                        p.areaFraction = a.fraction * b.fraction;
+                        p.degree = c.degree;
+                        p.projection = 0;
+                        p.intervals = 1;
+                        p.pad = 0;
+                        joins[q] = c.joins;
+                    }
+                }
+            });
+        for (auto &th : threads)
+            th.join();
+    }
     {
         std::vector<size_t> uncertain;
         for (size_t r = 0; r < records.size(); ++r)
@@ -890,18 +962,17 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                     if (u >= uncertain.size())
                         return;
                     const PairRecord &rec = records[uncertain[u]];
-                    Patch *pp = pool.data() + rec.patchFirst;
+                    Patch *pp = patches.data() + rec.patchFirst;
+                    const uint8_t *jn = joins.data() + rec.patchFirst;
                     const HostPanel &t = sp.panels[rec.first], &s = sp.panels[rec.second];
                     for (uint32_t k = 0; k < rec.count;) {
                         uint32_t e = k + 1;
-                        while (e < rec.count && pp[e].pad)
+                        while (e < rec.count && jn[e])
                             ++e;
                         if (e - k > 1) {
                             run.clear();
-                            for (uint32_t q = k; q < e; ++q) {
-                                pp[q].pad = 0;
+                            for (uint32_t q = k; q < e; ++q)
                                 run.emplace_back(hostPatchError(t, s, pp[q], maxK), pp[q]);
-                            }
                             std::stable_sort(run.begin(), run.end(),
                                              [](const auto &x, const auto &y) { return x.first > y.first; });
                             for (size_t q = 1; q < run.size(); ++q)
@@ -956,10 +1027,10 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             if (whole[u])
                 f.plan.wholePanelDegrees[u] = whole[u];
     {
-        size_t patches = pool.size();
+        size_t total = patches.size();
         for (const auto &r : hostRules)
-            patches += r.patches.size();
-        f.plan.patches.reserve(patches);
+            total += r.patches.size();
+        f.plan.patches.reserve(total);
         f.plan.near.reserve(2 * items.size());
     }
     for (const auto &it : items) {
@@ -970,7 +1041,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                            r.relError);
         } else {
             const PairRecord &r = records[size_t(-1 - it.host)];
-            appendPairRule(f.plan, f.allPairs, i, j, pool.data() + r.patchFirst, r.count, r.maxDepth, r.relError);
+            appendPairRule(f.plan, f.allPairs, i, j, patches.data() + r.patchFirst, r.count, r.maxDepth, r.relError);
         }
     }
     finishPlan(f.plan, T);

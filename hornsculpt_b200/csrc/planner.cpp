@@ -412,29 +412,56 @@ std::vector<std::pair<uint32_t, uint32_t>> candidates(const Space &sp, double ra
         where[i] = cell(sp.panels[i].v[0]);
         grid[where[i]].push_back(uint32_t(i));
     }
-    std::vector<std::pair<uint32_t, uint32_t>> out;
-    for (size_t i = 0; i < sp.panels.size(); ++i) {
-        const auto &a = sp.panels[i];
-        for (int dx = -1; dx <= 1; ++dx)
-            for (int dy = -1; dy <= 1; ++dy)
-                for (int dz = -1; dz <= 1; ++dz) {
-                    const auto it = grid.find(Key{where[i].x + dx, where[i].y + dy, where[i].z + dz});
-                    if (it == grid.end())
-                        continue;
-                    for (uint32_t j : it->second) {
-                        if (j <= i)
-                            continue;
-                        const auto &b = sp.panels[j];
-                        const double bound = ratio * std::max(a.maxEdge, b.maxEdge) + a.maxEdge + b.maxEdge;
-                        if (std::abs(a.v[0].x - b.v[0].x) > bound || std::abs(a.v[0].y - b.v[0].y) > bound ||
-                            std::abs(a.v[0].z - b.v[0].z) > bound)
-                            continue;
-                        if (panelsDisjoint(a, b))
-                            out.emplace_back(uint32_t(i), j);
-                    }
+    // Each panel's partners j > i, sorted, on host threads; concatenated in
+    // panel order this is the sorted pair list.
+    const size_t T = sp.panels.size();
+    std::vector<std::vector<uint32_t>> partners(T);
+    std::atomic<size_t> next{0};
+    const unsigned workers = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < std::min<size_t>(workers, (T + 255) / 256); ++w)
+        pool.emplace_back([&]() {
+            for (;;) {
+                const size_t begin = next.fetch_add(256);
+                if (begin >= T)
+                    return;
+                for (size_t i = begin; i < std::min(T, begin + 256); ++i) {
+                    const auto &a = sp.panels[i];
+                    auto &mine = partners[i];
+                    for (int dx = -1; dx <= 1; ++dx)
+                        for (int dy = -1; dy <= 1; ++dy)
+                            for (int dz = -1; dz <= 1; ++dz) {
+                                const auto it = grid.find(Key{where[i].x + dx, where[i].y + dy, where[i].z + dz});
+                                if (it == grid.end())
+                                    continue;
+                                for (uint32_t j : it->second) {
+                                    if (j <= i)
+                                        continue;
+                                    const auto &b = sp.panels[j];
+                                    const double bound =
+                                        ratio * std::max(a.maxEdge, b.maxEdge) + a.maxEdge + b.maxEdge;
+                                    if (std::abs(a.v[0].x - b.v[0].x) > bound ||
+                                        std::abs(a.v[0].y - b.v[0].y) > bound ||
+                                        std::abs(a.v[0].z - b.v[0].z) > bound)
+                                        continue;
+                                    if (panelsDisjoint(a, b))
+                                        mine.push_back(j);
+                                }
+                            }
+                    std::sort(mine.begin(), mine.end());
                 }
-    }
-    std::sort(out.begin(), out.end());
+            }
+        });
+    for (auto &th : pool)
+        th.join();
+    size_t total = 0;
+    for (const auto &m : partners)
+        total += m.size();
+    std::vector<std::pair<uint32_t, uint32_t>> out;
+    out.reserve(total);
+    for (size_t i = 0; i < T; ++i)
+        for (uint32_t j : partners[i])
+            out.emplace_back(uint32_t(i), j);
     return out;
 }
 
@@ -581,16 +608,25 @@ void appendPairRule(Plan &plan, bool allPairs, uint32_t i, uint32_t j, const Pat
 }
 
 void finishPlan(Plan &plan, size_t T) {
-    std::sort(plan.near.begin(), plan.near.end(), [](const NearJob &x, const NearJob &y) {
-        return x.test != y.test ? x.test < y.test : x.trial < y.trial;
-    });
-    plan.nearTrials.reserve(plan.near.size());
-    for (const auto &j : plan.near) {
-        ++plan.nearOffsets[j.test + 1];
-        plan.nearTrials.push_back(j.trial);
-    }
+    // jobs by (test, trial): a counting sort by test, then each test's jobs by
+    // trial (keys are unique, so this is the order of a full sort)
+    std::vector<uint32_t> start(T + 1, 0);
+    for (const auto &j : plan.near)
+        ++start[j.test + 1];
     for (size_t r = 1; r <= T; ++r)
-        plan.nearOffsets[r] += plan.nearOffsets[r - 1];
+        start[r] += start[r - 1];
+    std::vector<NearJob> sorted(plan.near.size());
+    std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+    for (const auto &j : plan.near)
+        sorted[fill[j.test]++] = j;
+    for (size_t r = 0; r < T; ++r)
+        std::sort(sorted.begin() + start[r], sorted.begin() + start[r + 1],
+                  [](const NearJob &x, const NearJob &y) { return x.trial < y.trial; });
+    plan.near = std::move(sorted);
+    plan.nearTrials.reserve(plan.near.size());
+    for (const auto &j : plan.near)
+        plan.nearTrials.push_back(j.trial);
+    plan.nearOffsets.assign(start.begin(), start.end());
 }
 
 std::vector<PairRule> planPairsOnHost(const Space &sp, const PlanSettings &st, double maxK,
