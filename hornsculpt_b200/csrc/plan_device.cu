@@ -853,10 +853,13 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         DevMem dHdr(sizeof(LeafHdr) * kLeafCap * warps), dInteg(sizeof(double) * 72 * kLeafCap * warps),
             dPend(sizeof(uint32_t) * kLeafCap * warps), dPendErr(sizeof(double) * kLeafCap * warps),
             dAtl(sizeof(uint32_t) * kLeafCap * warps);
+        // Patch codes and records of one launch chunk; read back after each
+        // chunk, so the pool is bounded by the chunk's pairs.
+        const unsigned long long chunk = std::min<unsigned long long>(1ull << 20, std::max(nDevice, 1ull));
         check(cudaMemGetInfo(&freeBytes, &totalBytes), "device memory query");
         const size_t poolCap =
-            std::max<size_t>(4096, std::min<size_t>(64 * nDevice + 4096, freeBytes / 4 / sizeof(PatchCode)));
-        DevMem dPool(sizeof(PatchCode) * poolCap), dRecords(sizeof(PairRecord) * std::max<unsigned long long>(nDevice, 1)),
+            std::max<size_t>(4096, std::min<size_t>(64 * chunk + 4096, freeBytes / 4 / sizeof(PatchCode)));
+        DevMem dPool(sizeof(PatchCode) * poolCap), dRecords(sizeof(PairRecord) * chunk),
             dFlagged(sizeof(uint2) * std::max<unsigned long long>(nDevice, 1));
         DevMem dWhole(f.allPairs ? units : 16);
         if (f.allPairs)
@@ -865,33 +868,42 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                       dAtl.as<uint32_t>(), nullptr, nullptr};
         PairOutput O{dPool.as<PatchCode>(), poolCap, counters + 2, dRecords.as<PairRecord>(), counters + 3,
                      dWhole.as<uint8_t>()};
-        // chunks of pairs, so a cancellation is seen between launches
-        const unsigned long long chunk = 1ull << 20;
         for (unsigned long long begin = 0; begin < nDevice; begin += chunk) {
             if (cancel && *cancel)
                 throw Cancelled();
             const unsigned long long n = std::min(chunk, nDevice - begin);
+            check(cudaMemsetAsync(counters + 2, 0, 2 * sizeof(unsigned long long), stream), "planner reset");
             check(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), stream), "planner reset");
             refineKernel<<<unsigned(grid), 32 * kWarpsPerBlock, kRefineSmem, stream>>>(
                 A, dDeviceList.as<uint2>() + begin, n, counters + 5, arena, O, dFlagged.as<uint2>(), counters + 4);
             check(cudaGetLastError(), "planner refinement");
+            unsigned long long n2c[2] = {};
+            check(cudaMemcpyAsync(n2c, counters + 2, sizeof(n2c), cudaMemcpyDeviceToHost, stream), "planner readback");
             check(cudaStreamSynchronize(stream), "planner refinement");
+            const unsigned long long used = std::min<unsigned long long>(n2c[0], poolCap), nRec = n2c[1];
+            const size_t r0 = records.size(), p0 = pool.size();
+            records.resize(r0 + nRec);
+            pool.resize(p0 + used);
+            if (nRec)
+                check(cudaMemcpyAsync(records.data() + r0, dRecords.p, sizeof(PairRecord) * nRec,
+                                      cudaMemcpyDeviceToHost, stream),
+                      "planner readback");
+            if (used)
+                check(cudaMemcpyAsync(pool.data() + p0, dPool.p, sizeof(PatchCode) * used, cudaMemcpyDeviceToHost,
+                                      stream),
+                      "planner readback");
+            check(cudaStreamSynchronize(stream), "planner readback");
+            if (pool.size() > 0xffffffffull)
+                throw OutOfMemory("Interaction plan exceeds 2^32 quadrature patches.");
+            for (size_t r = r0; r < records.size(); ++r)
+                records[r].patchFirst += uint32_t(p0);
         }
         unsigned long long n5[5] = {};
         phase[2] = msSince(t0);
         check(cudaMemcpyAsync(n5, counters, sizeof(n5), cudaMemcpyDeviceToHost, stream), "planner readback");
         check(cudaStreamSynchronize(stream), "planner readback");
-        const unsigned long long used = std::min<unsigned long long>(n5[2], poolCap), nRec = n5[3], nFlag = n5[4];
-        records.resize(nRec);
-        pool.resize(used);
+        const unsigned long long nFlag = n5[4];
         flagged.resize(nFlag);
-        if (nRec)
-            check(cudaMemcpyAsync(records.data(), dRecords.p, sizeof(PairRecord) * nRec, cudaMemcpyDeviceToHost,
-                                  stream),
-                  "planner readback");
-        if (used)
-            check(cudaMemcpyAsync(pool.data(), dPool.p, sizeof(PatchCode) * used, cudaMemcpyDeviceToHost, stream),
-                  "planner readback");
         if (nFlag)
             check(cudaMemcpyAsync(flagged.data(), dFlagged.p, sizeof(uint2) * nFlag, cudaMemcpyDeviceToHost, stream),
                   "planner readback");
@@ -907,99 +919,95 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
     const double deviceMs = msSince(t0);
     phase[3] = deviceMs;
     const auto t1 = Clock::now();
+    const unsigned workers = std::max(1u, std::min<unsigned>(64, std::thread::hardware_concurrency()));
+    const auto parallel = [&](size_t count, size_t grain, auto &&body) {
+        std::atomic<size_t> next{0};
+        std::vector<std::thread> threads;
+        for (unsigned wkr = 0; wkr < std::min<size_t>(workers, (count + grain - 1) / grain); ++wkr)
+            threads.emplace_back([&]() {
+                for (;;) {
+                    const size_t begin = next.fetch_add(grain);
+                    if (begin >= count)
+                        return;
+                    for (size_t q = begin; q < std::min(count, begin + grain); ++q)
+                        body(q);
+                }
+            });
+        for (auto &th : threads)
+            th.join();
+    };
+    const auto decode = [&](const PatchCode &c, Patch &p) {
+        const Sub a = subOfPath(c.pathA, c.depthA), b = subOfPath(c.pathB, c.depthB);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                p.test[3 * i + j] = a.v[i][j];
+                p.trial[3 * i + j] = b.v[i][j];
+            }
+        p.areaFraction = a.fraction * b.fraction;
+        p.degree = c.degree;
+        p.projection = 0;
+        p.intervals = 1;
+        p.pad = 0;
+    };
     // Runs of leaves whose order the device could not decide: the host
     // orders each by its own error estimates (pair_quadrature.cpp:644-683 as
     // the host planner evaluates them); a tie among them leaves the order to
     // the host planner's heap, so such a pair is refined on the host.
     size_t resolved = 0;
-    std::vector<Patch> patches(pool.size());
-    std::vector<uint8_t> joins(pool.size());
-    {
-        std::atomic<size_t> next{0};
-        const unsigned workers = std::max(1u, std::min<unsigned>(64, std::thread::hardware_concurrency()));
-        std::vector<std::thread> threads;
-        for (unsigned wkr = 0; wkr < std::min<size_t>(workers, (pool.size() + 4095) / 4096); ++wkr)
-            threads.emplace_back([&]() {
-                for (;;) {
-                    const size_t begin = next.fetch_add(4096);
-                    if (begin >= pool.size())
-                        return;
-                    for (size_t q = begin; q < std::min(pool.size(), begin + 4096); ++q) {
-                        const PatchCode &c = pool[q];
-                        const Sub a = subOfPath(c.pathA, c.depthA), b = subOfPath(c.pathB, c.depthB);
-                        Patch &p = patches[q];
-                        for (int i = 0; i < 3; ++i)
-                            for (int j = 0; j < 3; ++j) {
-                                p.test[3 * i + j] = a.v[i][j];
-                                p.trial[3 * i + j] = b.v[i][j];
-                            }
-                        p.areaFraction = a.fraction * b.fraction;
-                        p.degree = c.degree;
-                        p.projection = 0;
-                        p.intervals = 1;
-                        p.pad = 0;
-                        joins[q] = c.joins;
-                    }
-                }
-            });
-        for (auto &th : threads)
-            th.join();
-    }
+    std::vector<int32_t> settled(records.size(), -1);  // record -> its resolved patches
+    std::vector<std::vector<Patch>> settledPatches;
     {
         std::vector<size_t> uncertain;
         for (size_t r = 0; r < records.size(); ++r)
             if (records[r].uncertain)
                 uncertain.push_back(r);
         std::vector<uint8_t> tie(uncertain.size(), 0);
-        std::atomic<size_t> next{0};
-        const unsigned workers = std::max(1u, std::min<unsigned>(64, std::thread::hardware_concurrency()));
-        std::vector<std::thread> threads;
-        for (unsigned wkr = 0; wkr < std::min<size_t>(workers, uncertain.size()); ++wkr)
-            threads.emplace_back([&]() {
-                std::vector<std::pair<double, Patch>> run;
-                for (;;) {
-                    const size_t u = next.fetch_add(1);
-                    if (u >= uncertain.size())
-                        return;
-                    const PairRecord &rec = records[uncertain[u]];
-                    Patch *pp = patches.data() + rec.patchFirst;
-                    const uint8_t *jn = joins.data() + rec.patchFirst;
-                    const HostPanel &t = sp.panels[rec.first], &s = sp.panels[rec.second];
-                    for (uint32_t k = 0; k < rec.count;) {
-                        uint32_t e = k + 1;
-                        while (e < rec.count && jn[e])
-                            ++e;
-                        if (e - k > 1) {
-                            run.clear();
-                            for (uint32_t q = k; q < e; ++q)
-                                run.emplace_back(hostPatchError(t, s, pp[q], maxK), pp[q]);
-                            std::stable_sort(run.begin(), run.end(),
-                                             [](const auto &x, const auto &y) { return x.first > y.first; });
-                            for (size_t q = 1; q < run.size(); ++q)
-                                tie[u] |= run[q].first == run[q - 1].first ? 1 : 0;
-                            for (size_t q = 0; q < run.size(); ++q)
-                                pp[k + q] = run[q].second;
-                        }
-                        k = e;
-                    }
+        settledPatches.resize(uncertain.size());
+        parallel(uncertain.size(), 1, [&](size_t u) {
+            const PairRecord &rec = records[uncertain[u]];
+            const PatchCode *codes = pool.data() + rec.patchFirst;
+            std::vector<Patch> &pp = settledPatches[u];
+            pp.resize(rec.count);
+            for (uint32_t q = 0; q < rec.count; ++q)
+                decode(codes[q], pp[q]);
+            const HostPanel &t = sp.panels[rec.first], &s = sp.panels[rec.second];
+            std::vector<std::pair<double, Patch>> run;
+            for (uint32_t k = 0; k < rec.count;) {
+                uint32_t e = k + 1;
+                while (e < rec.count && codes[e].joins)
+                    ++e;
+                if (e - k > 1) {
+                    run.clear();
+                    for (uint32_t q = k; q < e; ++q)
+                        run.emplace_back(hostPatchError(t, s, pp[q], maxK), pp[q]);
+                    std::stable_sort(run.begin(), run.end(),
+                                     [](const auto &x, const auto &y) { return x.first > y.first; });
+                    for (size_t q = 1; q < run.size(); ++q)
+                        tie[u] |= run[q].first == run[q - 1].first ? 1 : 0;
+                    for (size_t q = 0; q < run.size(); ++q)
+                        pp[k + q] = run[q].second;
                 }
-            });
-        for (auto &th : threads)
-            th.join();
+                k = e;
+            }
+        });
         std::vector<uint8_t> drop(records.size(), 0);
         for (size_t u = 0; u < uncertain.size(); ++u) {
             if (tie[u]) {
                 drop[uncertain[u]] = 1;
                 flagged.push_back(make_uint2(records[uncertain[u]].first, records[uncertain[u]].second));
             } else {
+                settled[uncertain[u]] = int32_t(u);
                 ++resolved;
             }
         }
         size_t kept = 0;
         for (size_t r = 0; r < records.size(); ++r)
-            if (!drop[r])
+            if (!drop[r]) {
+                settled[kept] = settled[r];
                 records[kept++] = records[r];
+            }
         records.resize(kept);
+        settled.resize(kept);
     }
     // the host refines projected and flagged pairs
     std::vector<std::pair<uint32_t, uint32_t>> hostPairs;
@@ -1010,40 +1018,75 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         hostPairs.emplace_back(p.x, p.y);
     std::sort(hostPairs.begin(), hostPairs.end());
     const std::vector<PairRule> hostRules = planPairsOnHost(sp, st, maxK, hostPairs, 0, cancel);
-    // flatten in (first, second) order, the host planner's order
+    // Flatten in (first, second) order, the host planner's order
+    // (appendPairRule's rules): offsets first, then every pair's patches are
+    // decoded or copied straight to their place.
     struct Item {
         uint64_t key;
         int32_t host;  // index into hostRules, or -1 - record index
+        uint64_t offset;
     };
     std::vector<Item> items;
     items.reserve(records.size() + hostRules.size());
     for (size_t r = 0; r < records.size(); ++r)
-        items.push_back({(uint64_t(records[r].first) << 32) | records[r].second, -1 - int32_t(r)});
+        items.push_back({(uint64_t(records[r].first) << 32) | records[r].second, -1 - int32_t(r), 0});
     for (size_t h = 0; h < hostPairs.size(); ++h)
-        items.push_back({(uint64_t(hostPairs[h].first) << 32) | hostPairs[h].second, int32_t(h)});
+        items.push_back({(uint64_t(hostPairs[h].first) << 32) | hostPairs[h].second, int32_t(h), 0});
     std::sort(items.begin(), items.end(), [](const Item &x, const Item &y) { return x.key < y.key; });
     if (f.allPairs)
         for (unsigned long long u = 0; u < units; ++u)
             if (whole[u])
                 f.plan.wholePanelDegrees[u] = whole[u];
-    {
-        size_t total = patches.size();
-        for (const auto &r : hostRules)
-            total += r.patches.size();
-        f.plan.patches.reserve(total);
-        f.plan.near.reserve(2 * items.size());
-    }
-    for (const auto &it : items) {
+    Plan &plan = f.plan;
+    uint64_t total = 0;
+    plan.near.reserve(2 * items.size());
+    for (auto &it : items) {
         const uint32_t i = uint32_t(it.key >> 32), j = uint32_t(it.key & 0xffffffffu);
+        uint32_t count, maxDepth;
+        double relError;
         if (it.host >= 0) {
             const PairRule &r = hostRules[size_t(it.host)];
-            appendPairRule(f.plan, f.allPairs, i, j, r.patches.data(), uint32_t(r.patches.size()), r.maxDepth,
-                           r.relError);
+            count = uint32_t(r.patches.size()), maxDepth = r.maxDepth, relError = r.relError;
+            if (f.allPairs && maxDepth == 0 && count == 1 && !r.patches[0].projection) {
+                plan.wholePanelDegrees[unorderedPairIndex(i, j)] = uint8_t(r.patches[0].degree);
+                plan.maxRelError = std::max(plan.maxRelError, relError);
+                it.offset = ~0ull;
+                continue;
+            }
         } else {
             const PairRecord &r = records[size_t(-1 - it.host)];
-            appendPairRule(f.plan, f.allPairs, i, j, patches.data() + r.patchFirst, r.count, r.maxDepth, r.relError);
+            count = r.count, maxDepth = r.maxDepth, relError = r.relError;
         }
+        it.offset = total;
+        plan.near.push_back({i, j, uint32_t(total), count, 0});
+        plan.near.push_back({j, i, uint32_t(total), count, 1});
+        plan.maxDepth = std::max(plan.maxDepth, maxDepth);
+        plan.maxRelError = std::max(plan.maxRelError, relError);
+        total += count;
     }
+    if (total > 0xffffffffull)
+        throw OutOfMemory("Interaction plan exceeds 2^32 quadrature patches.");
+    plan.patches.resize(total);
+    parallel(items.size(), 256, [&](size_t q) {
+        const Item &it = items[q];
+        if (it.offset == ~0ull)
+            return;
+        Patch *out = plan.patches.data() + it.offset;
+        if (it.host >= 0) {
+            const PairRule &r = hostRules[size_t(it.host)];
+            std::copy(r.patches.begin(), r.patches.end(), out);
+            return;
+        }
+        const size_t rec = size_t(-1 - it.host);
+        const PairRecord &r = records[rec];
+        if (settled[rec] >= 0) {
+            const auto &pp = settledPatches[size_t(settled[rec])];
+            std::copy(pp.begin(), pp.end(), out);
+        } else {
+            for (uint32_t k = 0; k < r.count; ++k)
+                decode(pool[r.patchFirst + k], out[k]);
+        }
+    });
     finishPlan(f.plan, T);
     phase[4] = msSince(t0);
     if (stats) {
