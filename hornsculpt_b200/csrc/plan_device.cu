@@ -28,6 +28,17 @@
 namespace hsb {
 namespace {
 
+// The pair code is large; letting the compiler decide what to inline keeps the
+// kernel's instruction footprint small (a force-inlined build stalled on
+// instruction fetch).
+#if defined(__CUDACC__)
+#define PD_HD __host__ __device__
+#define PD_NOINLINE __noinline__
+#else
+#define PD_HD
+#define PD_NOINLINE
+#endif
+
 constexpr uint32_t kLeafCap = 2048;  // leaves held per warp (pending + at the depth limit + requested)
 constexpr int kRulePoints = 64;      // largest rule (collapsed tensor Gauss degree 14)
 constexpr int kPts = 7;              // per point: barycentrics (3), local point (3), weight
@@ -142,7 +153,7 @@ constexpr int kRowValues = 28;  // per row item: 12 complex inner sums and 4 mag
 // moment values add bt_i In[c][j] over the rows. `own` receives the lane's
 // values; `bad` is set for a coincident point.
 template <class Wp>
-HS_HD void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, const Sub &a, const Sub &b,
+PD_HD PD_NOINLINE void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, const Sub &a, const Sub &b,
                          const double *rule, int n, double k, double scale, double *pts, double *rows, double *own,
                          bool &bad) {
     constexpr int W = Wp::W;
@@ -236,7 +247,7 @@ HS_HD void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, co
 //   errors, at most m u A_c each, and kernel values within 32 u);
 //   errB bounds |error_device - error_host|, intB a moment value.
 template <class Wp>
-HS_HD void estimateLeaf(const Wp &w, const HostPanel &t, const HostPanel &s, const LeafHdr &L, const RuleTables &R,
+PD_HD void estimateLeaf(const Wp &w, const HostPanel &t, const HostPanel &s, const LeafHdr &L, const RuleTables &R,
                         double k, double scale, double *pts, double *rows, double *hiOwn, double &error,
                         double &errB,
                         double &intB, double &mnL, bool &bad) {
@@ -283,7 +294,7 @@ struct Top2 {
     double e1, e2;
     uint32_t p1, p2;
 };
-template <class Wp> HS_HD Top2 topTwo(const Wp &w, const double *err, uint32_t n) {
+template <class Wp> PD_HD Top2 topTwo(const Wp &w, const double *err, uint32_t n) {
     Top2 t{-1, -1, 0xffffffffu, 0xffffffffu};
     for (uint32_t i = w.lane(); i < n; i += Wp::W) {
         const double e = err[i];
@@ -324,7 +335,7 @@ template <class Wp> HS_HD Top2 topTwo(const Wp &w, const double *err, uint32_t n
     return t;
 }
 
-HS_HD void writeLeaf(LeafHdr &h, const Sub &a, const Sub &b, const HostPanel &t, const HostPanel &s, uint32_t depth,
+PD_HD PD_NOINLINE void writeLeaf(LeafHdr &h, const Sub &a, const Sub &b, const HostPanel &t, const HostPanel &s, uint32_t depth,
                      uint32_t degree, uint32_t pathA, uint32_t depthA, uint32_t pathB, uint32_t depthB) {
     h.a = a;
     h.b = b;
@@ -340,13 +351,34 @@ HS_HD void writeLeaf(LeafHdr &h, const Sub &a, const Sub &b, const HostPanel &t,
     h.joins = h.pad = 0;
 }
 
+// The four children of leaf slots[0] (halving its test side when splitTest,
+// else its trial side), written to slots[3], slots[2], slots[1] and last
+// slots[0], the parent's own slot. One lane.
+PD_HD PD_NOINLINE void spawnChildren(LeafHdr *hdr, const uint32_t *slots, const HostPanel &t, const HostPanel &s,
+                                     bool splitTest) {
+    const LeafHdr &v = hdr[slots[0]];
+    const Sub parent = splitTest ? v.a : v.b;
+    const uint32_t depth = v.depth, pathA = v.pathA, pathB = v.pathB, depthA = v.depthA, depthB = v.depthB;
+    for (int c = 3; c >= 0; --c) {
+        Sub child;
+        quarterChild(parent, c, child);
+        LeafHdr &h = hdr[slots[c]];
+        if (splitTest)
+            writeLeaf(h, child, v.b, t, s, depth + 1, 8, pathA | (uint32_t(c) << (2 * depthA)), depthA + 1, pathB,
+                      depthB);
+        else
+            writeLeaf(h, v.a, child, t, s, depth + 1, 8, pathA, depthA, pathB | (uint32_t(c) << (2 * depthB)),
+                      depthB + 1);
+    }
+}
+
 // The largest-error refinement of one tensor pair (the host's adaptivePair
 // without projection), with every decision checked against the rounding
 // bounds. Returns kPairRule (patches written to the pool, record appended),
 // kPairWhole (all-pairs mode single whole-panel rule, degree in `whole`) or
 // kPairHost (the host planner must refine this pair).
 template <class Wp>
-HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams &P, const WarpMem &M,
+PD_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams &P, const WarpMem &M,
                      const PairOutput &O) {
     constexpr int own_n = kValues / Wp::W;
     const HostPanel &t = P.panels[ti], &s = P.panels[si];
@@ -496,8 +528,11 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
             return kPairHost;
         const Top2 top = topTwo(w, M.pendErr, nPend);
         const uint32_t vSlot = M.pend[top.p1];
-        const LeafHdr v = M.hdr[vSlot];
-        if (top.p2 != 0xffffffffu && !separated(top.e1, top.e2, v.errB + M.hdr[M.pend[top.p2]].errB))
+        const LeafHdr &vh = M.hdr[vSlot];  // v stays in the arena; its slot goes to its first child
+        const double vError = vh.error, vErrB = vh.errB, vIntB = vh.intB;
+        const uint32_t vDepth = vh.depth, vDegree = vh.degree;
+        const bool splitTest = vh.da >= vh.db;
+        if (top.p2 != 0xffffffffu && !separated(top.e1, top.e2, vErrB + M.hdr[M.pend[top.p2]].errB))
             return kPairHost;
         w.sync();
         if (w.leader()) {  // remove v: the last pending entry takes its place
@@ -505,8 +540,8 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
             M.pendErr[top.p1] = M.pendErr[nPend - 1];
         }
         --nPend;
-        absError = maxD(0.0, absError - v.error);
-        absB += v.errB + 2 * kUnit * (absError + v.error);
+        absError = maxD(0.0, absError - vError);
+        absB += vErrB + 2 * kUnit * (absError + vError);
         double mnI = 0;
         for (int v2 = 0; v2 < own_n && base + v2 < 72; v2 += 2) {
             integral[v2] -= M.integ[size_t(vSlot) * 72 + base + v2];
@@ -514,30 +549,21 @@ HS_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
             mnI = fmax(mnI, hypot(integral[v2], integral[v2 + 1]));
         }
         mnI = w.max(mnI);
-        intB += v.intB + 2 * kUnit * mnI * 2;
+        intB += vIntB + 2 * kUnit * mnI * 2;
         w.sync();
-        if (v.degree == 8 && (v.depth == P.maxDepth || (promoteRoot && v.depth == 0))) {
+        if (vDegree == 8 && (vDepth == P.maxDepth || (promoteRoot && vDepth == 0))) {
             if (w.leader())
-                writeLeaf(M.hdr[vSlot], v.a, v.b, t, s, v.depth, 14, v.pathA, v.depthA, v.pathB, v.depthB);
+                M.hdr[vSlot].degree = 14;  // same patch, the degree 12/14 pair of rules
             req[nReq++] = vSlot;
         } else {
             if (nPend + nAtl + 4 > 50000 || nLeaf + 3 > kLeafCap)
                 return kPairHost;
-            Sub children[4];
-            const bool splitTest = v.da >= v.db;
-            quarter(splitTest ? v.a : v.b, children);
-            for (int c = 0; c < 4; ++c) {
-                const uint32_t slot = c == 0 ? vSlot : nLeaf++;
-                if (w.leader()) {
-                    if (splitTest)
-                        writeLeaf(M.hdr[slot], children[c], v.b, t, s, v.depth + 1, 8,
-                                  v.pathA | (uint32_t(c) << (2 * v.depthA)), v.depthA + 1, v.pathB, v.depthB);
-                    else
-                        writeLeaf(M.hdr[slot], v.a, children[c], t, s, v.depth + 1, 8, v.pathA, v.depthA,
-                                  v.pathB | (uint32_t(c) << (2 * v.depthB)), v.depthB + 1);
-                }
-                req[nReq++] = slot;
-            }
+            const uint32_t slots[4] = {vSlot, nLeaf, nLeaf + 1, nLeaf + 2};
+            nLeaf += 3;
+            if (w.leader())
+                spawnChildren(M.hdr, slots, t, s, splitTest);
+            for (int c = 0; c < 4; ++c)
+                req[nReq++] = slots[c];
         }
         w.sync();
     }

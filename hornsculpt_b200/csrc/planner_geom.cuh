@@ -125,22 +125,40 @@ HS_HD bool useProjection(const HostPanel &t, const HostPanel &s, double scale) {
     return (lo >= -eps && hi > eps) || (hi <= eps && lo < -eps);
 }
 
-HS_HD void quarter(const Sub &s, Sub *out) {
-    double mid[3][3];  // ab, bc, ca
-    for (int e = 0; e < 3; ++e)
+// Child c of a sub-triangle's halving (0..2 at its corners, 3 the middle),
+// vertices as midpoints of the parent's edges ab, bc, ca.
+HS_HD void quarterChild(const Sub &s, int c, Sub &out) {
+    const auto mid = [&](int e, double *m) {  // midpoint of edge e (v_e, v_e+1)
+        const int f = e == 2 ? 0 : e + 1;
         for (int i = 0; i < 3; ++i)
-            mid[e][i] = (s.v[e][i] + s.v[(e + 1) % 3][i]) * .5;
-    const double f = s.fraction * .25;
-    const double *corner[4][3] = {{s.v[0], mid[0], mid[2]},
-                                  {mid[0], s.v[1], mid[1]},
-                                  {mid[2], mid[1], s.v[2]},
-                                  {mid[0], mid[1], mid[2]}};
-    for (int c = 0; c < 4; ++c) {
-        for (int k = 0; k < 3; ++k)
-            for (int i = 0; i < 3; ++i)
-                out[c].v[k][i] = corner[c][k][i];
-        out[c].fraction = f;
+            m[i] = (s.v[e][i] + s.v[f][i]) * .5;
+    };
+    if (c == 0) {
+        for (int i = 0; i < 3; ++i)
+            out.v[0][i] = s.v[0][i];
+        mid(0, out.v[1]);
+        mid(2, out.v[2]);
+    } else if (c == 1) {
+        mid(0, out.v[0]);
+        for (int i = 0; i < 3; ++i)
+            out.v[1][i] = s.v[1][i];
+        mid(1, out.v[2]);
+    } else if (c == 2) {
+        mid(2, out.v[0]);
+        mid(1, out.v[1]);
+        for (int i = 0; i < 3; ++i)
+            out.v[2][i] = s.v[2][i];
+    } else {
+        mid(0, out.v[0]);
+        mid(1, out.v[1]);
+        mid(2, out.v[2]);
     }
+    out.fraction = s.fraction * .25;
+}
+
+HS_HD void quarter(const Sub &s, Sub *out) {
+    for (int c = 0; c < 4; ++c)
+        quarterChild(s, c, out[c]);
 }
 
 HS_HD double subDiameter(const HostPanel &p, const Sub &s, V3 origin) {
