@@ -881,7 +881,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             dAtl(sizeof(uint32_t) * kLeafCap * warps);
         // Patch codes and records of one launch chunk; read back after each
         // chunk, so the pool is bounded by the chunk's pairs.
-        const unsigned long long chunk = std::min<unsigned long long>(1ull << 20, std::max(nDevice, 1ull));
+        const unsigned long long chunk = std::min<unsigned long long>(1ull << 18, std::max(nDevice, 1ull));
         check(cudaMemGetInfo(&freeBytes, &totalBytes), "device memory query");
         const size_t poolCap =
             std::max<size_t>(4096, std::min<size_t>(64 * chunk + 4096, freeBytes / 4 / sizeof(PatchCode)));
