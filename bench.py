@@ -589,15 +589,15 @@ def run_c4(args):
         torch.cuda.empty_cache()
 
 
-def serve_stream(hs, count: int, seed: int, rate: float, distinct: int = 0):
+def serve_stream(hs, count: int, seed: int, rate: float, distinct: int = 0, triangles=(2000, 4000), kh=1.9):
     """Seeded Poisson stream of horn requests: throat U[15, 50] mm, mouth
     U[80, 300] mm, length U[100, 600] mm, flare exponent U[1, 4], triangle
-    count log-uniform in [2k, 4k] (the dense form's range at interactive
-    planning cost; larger meshes need the FMM form), wall max(3 mm, 1.2 h) so
-    the mouth rim meshes with angles >= 20 degrees, 1-16 frequencies
-    log-uniform in 200 Hz-20 kHz kept where k * (longest edge) <= 1.9 (below
-    the plan's all-pairs switch at 2). Returns [(arrival_s, mesh, frequencies)]
-    and the number of rejected frequencies."""
+    count log-uniform in `triangles` (default [2k, 4k]), wall max(3 mm, 1.2 h)
+    so the mouth rim meshes with angles >= 20 degrees, 1-16 frequencies
+    log-uniform in 200 Hz-20 kHz kept where k * (longest edge) <= kh (default
+    1.9, below the plan's all-pairs switch at 2; the reference's limit is
+    3.25). Returns [(arrival_s, mesh, frequencies)] and the number of rejected
+    frequencies."""
     import numpy as np
 
     rng = np.random.default_rng(seed)
@@ -605,10 +605,10 @@ def serve_stream(hs, count: int, seed: int, rate: float, distinct: int = 0):
     if distinct:
         # a design-iteration stream: `distinct` horns, each request a random subset of
         # its mesh's 16-point raster (passed as the planning raster, so plans are reused)
-        designs, _ = serve_stream(hs, distinct, seed + 1, rate)
+        designs, _ = serve_stream(hs, distinct, seed + 1, rate, 0, triangles, kh)
         rasters = []
         for _, mesh, _, _ in designs:
-            fmax = min(20000.0, 1.9 / mesh.max_edge() * SOUND_SPEED / (2 * math.pi))
+            fmax = min(20000.0, kh / mesh.max_edge() * SOUND_SPEED / (2 * math.pi))
             rasters.append([float(f) for f in np.round(np.geomspace(200.0, fmax, 16), 3)])
         while len(stream) < count:
             d = int(rng.integers(distinct))
@@ -620,7 +620,7 @@ def serve_stream(hs, count: int, seed: int, rate: float, distinct: int = 0):
     while len(stream) < count:
         throat, mouth = rng.uniform(0.015, 0.050), rng.uniform(0.080, 0.300)
         length, flare = rng.uniform(0.100, 0.600), rng.uniform(1.0, 4.0)
-        target = math.exp(rng.uniform(math.log(2000), math.log(4000)))
+        target = math.exp(rng.uniform(math.log(triangles[0]), math.log(triangles[1])))
         z = np.linspace(0, length, 400)
         r = throat * np.exp(math.log(mouth / throat) * (z / length) ** flare)
         lateral = float(np.sum(np.pi * (r[1:] + r[:-1]) * np.hypot(np.diff(z), np.diff(r))))
@@ -628,7 +628,7 @@ def serve_stream(hs, count: int, seed: int, rate: float, distinct: int = 0):
         wall = max(0.003, 1.2 * h)
         mesh = hs.meshes.exponential_horn(throat, mouth, length, wall=wall, rear=wall, h=h,
                                           seed=int(rng.integers(1 << 31)), flare=flare)
-        kmax = 1.9 / mesh.max_edge()
+        kmax = kh / mesh.max_edge()
         freqs = sorted(set(np.round(np.exp(rng.uniform(math.log(200), math.log(20000), int(rng.integers(1, 17)))), 3)))
         kept = [float(f) for f in freqs if 2 * math.pi * f / SOUND_SPEED <= kmax]
         rejected += len(freqs) - len(kept)
@@ -648,11 +648,13 @@ def run_serve(args):
 
     import hornsculpt_b200 as hs
 
-    stream, rejected = serve_stream(hs, args.serve_requests, args.serve_seed, args.serve_rate, args.serve_distinct)
+    stream, rejected = serve_stream(hs, args.serve_requests, args.serve_seed, args.serve_rate, args.serve_distinct,
+                                    (args.serve_min_triangles, args.serve_max_triangles), args.serve_kh)
     line = {"workload": "C5 serving loop (seeded Poisson horn stream" +
                         (f", {args.serve_distinct} designs revisited" if args.serve_distinct else ", every mesh new") + ")",
             "requests": len(stream),
             "rate_per_s": args.serve_rate, "seed": args.serve_seed, "rejected_frequencies": rejected,
+            "kh_limit": args.serve_kh,
             "frequency_points": sum(len(f) for _, _, f, _ in stream),
             "triangles": [min(m.triangle_count for _, m, _, _ in stream), max(m.triangle_count for _, m, _, _ in stream)]}
     for form in ("mixed", "fp64"):
@@ -789,6 +791,10 @@ def main():
     ap.add_argument("--serve-timeout", type=float, default=400.0, help="seconds to wait for a stream to drain")
     ap.add_argument("--serve-seed", type=int, default=2026)
     ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--serve-min-triangles", type=int, default=2000)
+    ap.add_argument("--serve-max-triangles", type=int, default=4000)
+    ap.add_argument("--serve-kh", type=float, default=1.9,
+                    help="frequencies kept where k x longest edge <= this (the reference's limit is 3.25)")
     ap.add_argument("--serve-distinct", type=int, default=0,
                     help="> 0: requests revisit this many horn designs (planning rasters reused)")
     args = ap.parse_args()
