@@ -527,7 +527,10 @@ def run_c4(args):
     64 log frequencies 100 Hz-12 kHz, one interaction plan per mesh (the raster's
     planning frequency). The mixed form solves all 64 frequencies; the plain FP64
     form solves every 8th of them (8 points, the comparison set). One JSON line per
-    mesh; the third mesh is the C2 horn (12.8k triangles), driven at its throat."""
+    mesh; the third mesh is the C2 horn (12.8k triangles), driven at its throat;
+    the fourth the same horn at h = 4 mm (39 776 triangles), where the dense
+    forms do not fit and the fast-multipole forms run (FP64 every 8th point,
+    FP32 + FP64 GMRES-IR all 64; restart 50, tolerance 1e-6)."""
     import numpy as np
     import torch
 
@@ -541,7 +544,8 @@ def run_c4(args):
     only = [int(c) for c in args.c3_cases.split(",")] if args.c3_cases else None
     cases = (("icosphere-4 r=0.1 m", lambda: hs.meshes.icosphere(4), sphere),
              ("icosphere-5 r=0.1 m", lambda: hs.meshes.icosphere(5), sphere),
-             ("C2 horn h=7.15 mm seed 0", lambda: hs.meshes.exponential_horn(), throat))
+             ("C2 horn h=7.15 mm seed 0", lambda: hs.meshes.exponential_horn(), throat),
+             ("C2 horn h=4 mm seed 0 (fast multipole)", lambda: hs.meshes.exponential_horn(h=0.004), throat))
     for c, (name, make, exc) in enumerate(cases):
         if only is not None and c not in only:
             continue
@@ -551,6 +555,7 @@ def run_c4(args):
         line = {"workload": "C4 batched sweep", "mesh": name, "N": mesh.vertex_count, "T": mesh.triangle_count,
                 "frequencies": {"mixed": len(C4_FREQUENCIES), "fp64": len(plain_freqs), "range_hz": [100.0, 12000.0]}}
         results = {}
+        fmm = c == 3
         for form, freqs in (("fp64", plain_freqs), ("mixed", C4_FREQUENCIES)):
             # one session per form: at s5 each form's workspace alone takes over half the device
             torch.cuda.synchronize()
@@ -559,11 +564,17 @@ def run_c4(args):
                 solver.set_stream(stream.cuda_stream)
 
                 def request(fs):
+                    numerics = (hs.BemNumerics(precision=form, acceleration="fast_multipole",
+                                               relative_residual_tolerance=1e-6,
+                                               fast_multipole=hs.FastMultipoleSettings(restart_length=50))
+                                if fmm else hs.BemNumerics(precision=form))
                     return hs.BemRequest(frequencies=fs, observers=OBSERVERS, excitations=exc,
-                                         medium=hs.AcousticMedium(DENSITY, SOUND_SPEED),
-                                         numerics=hs.BemNumerics(precision=form),
+                                         medium=hs.AcousticMedium(DENSITY, SOUND_SPEED), numerics=numerics,
                                          interaction_plan_frequencies=C4_FREQUENCIES)
+                t0 = time.perf_counter()
                 solver.solve(request(freqs[-1:]))  # plan, workspace and warm-up
+                first = time.perf_counter() - t0
+                plan_stats = solver.plan_stats()
                 solver.set_profiling(True)
                 t0 = time.perf_counter()
                 res = solver.solve(request(freqs))
@@ -574,8 +585,12 @@ def run_c4(args):
                 results[form] = res
                 line[form] = {"ms_per_frequency": span / len(freqs), "wall_ms_per_frequency": 1e3 * wall / len(freqs),
                               "solves_per_s": 1e3 * len(freqs) / span if span else None,
+                              "first_call_s_with_planning": round(first, 2),
+                              "plan_device_ms": round(plan_stats["device_ms"] + plan_stats["host_ms"], 1),
                               "kernel_ms": {k: round(v[0], 3) for k, v in sorted(prof.items(), key=lambda t: -t[1][0])[:8]},
                               "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations)}
+                if fmm:
+                    line[form]["gmres_iterations"] = [f.excitations[0].iterations for f in res.frequencies]
         err = 0.0
         mixed_at = {f.frequency: f for f in results["mixed"].frequencies}
         for fp in results["fp64"].frequencies:
