@@ -459,6 +459,42 @@ def run_c2(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fmm_apply(args):
+    """Far-field applies of the FP64 fast-multipole operator on the C2 horn
+    (the kernel-profiling case): expansion tolerance 1e-8, every level
+    rotational, grouped M2L; a preparing apply, then two timed applies with
+    per-kernel CUDA events. One JSON line with the levels (level, order,
+    nodes, M2L links, plane wave) and the M2L milliseconds."""
+    import numpy as np
+    import torch
+
+    import hornsculpt_b200 as hs
+
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    mesh = hs.meshes.exponential_horn(h=args.c2_h) if args.c2_h else hs.meshes.exponential_horn()
+    freq = args.apply_frequency
+    k = 2 * np.pi * freq / SOUND_SPEED
+    rng = np.random.default_rng(3)
+    pvec = rng.normal(size=mesh.vertex_count) + 1j * rng.normal(size=mesh.vertex_count)
+    numerics = hs.BemNumerics(precision="fp64", acceleration="fast_multipole")
+    with hs.CudaBemSolver(mesh) as solver:
+        solver.set_stream(stream.cuda_stream)
+        solver.set_plane_wave_threshold(1e12)
+        solver.set_fmm_grouped_m2l(True)
+        _, _, _, levels = solver.debug_fmm_far(numerics, k, 1e-8, pvec)  # prepare
+        solver.set_profiling(True)
+        for _ in range(2):
+            solver.debug_fmm_far(numerics, k, 1e-8, pvec)
+        prof = solver.profile()
+        solver.set_profiling(False)
+    print(json.dumps({"workload": "fast-multipole far-field apply (C2 horn, all levels rotational, grouped M2L)",
+                      "T": mesh.triangle_count, "frequency_hz": freq, "levels": levels.tolist(),
+                      "m2l_ms_two_applies": round(prof.get("fmm_m2l", (0.0, 0))[0], 3),
+                      "kernel_ms_two_applies": {kk: round(v[0], 3) for kk, v in prof.items() if kk.startswith("fmm_")}}),
+          flush=True)
+
+
 def run_refgpu(args):
     """C1 through HornSculpt's own GPU CudaBemSolver (compiled from the reference
     sources into oracle/_ref/reference_solve) and through the adapter over this
@@ -789,12 +825,15 @@ def main():
                     help="solve only n sweep frequencies (small profiling cases)")
     ap.add_argument("--first-frequency", type=int, default=0,
                     help="index of the first sweep frequency solved (small profiling cases)")
-    ap.add_argument("--workload", default="c1", choices=["c1", "c2", "c3", "c4", "serve", "refgpu", "plan"],
+    ap.add_argument("--workload", default="c1",
+                    choices=["c1", "c2", "c3", "c4", "serve", "refgpu", "plan", "fmm-apply"],
                     help="c1: the headline sweep; c2: the 12.8k-triangle horn sweep (dense forms); "
                          "c3: mixed dense sizes N = 2k-16k (one line per mesh); "
                          "c4: 64-frequency sweeps on icospheres s4/s5; "
                          "serve: the serving loop on a seeded Poisson horn stream; "
-                         "plan: interaction planning on the device against the host planner")
+                         "plan: interaction planning on the device against the host planner; "
+                         "fmm-apply: far-field applies of the fast-multipole operator (kernel profiling)")
+    ap.add_argument("--apply-frequency", type=float, default=2000.0, help="fmm-apply: frequency in Hz")
     ap.add_argument("--c3-cases", default="", help="c3/c4: comma-separated case indices (default: all)")
     ap.add_argument("--c2-h", type=float, default=0.0,
                     help="C2 edge length in metres (0: 7.15 mm, the spec's lambda(8 kHz)/6)")
@@ -828,6 +867,8 @@ def main():
         return run_refgpu(args)
     if args.workload == "plan":
         return run_plan(args)
+    if args.workload == "fmm-apply":
+        return run_fmm_apply(args)
 
     import numpy as np
     import torch
