@@ -55,6 +55,9 @@ MIXED_FP32_FLOPS_PER_TEST_POINT = 114
 # regularMixedKernel<12> (ncu summary in profiles/); scaled by the pairs of a
 # launch for the roofline's traffic figure.
 REGULAR_Q12_DRAM_BYTES_PER_PAIR = 325
+# Column gather: per ordered panel pair the three FP32 record entries of a
+# column (72 B), per matrix entry the FP64 complex write (16 B).
+GATHER_BYTES_PER_ORDERED_PAIR = 72
 CONFIG = {"workload": "C1 icosphere s3 (642 v / 1280 t), 32 log freqs 100 Hz-5 kHz, 3 observers, dense; "
                       "mixed form timed, plain FP64 form timed beside it",
           "mesh": "icosphere-3 r=0.1 m", "frequencies": 32, "observers": 3, "excitations": 1,
@@ -813,6 +816,50 @@ def run_plan(args):
         print(json.dumps(line), flush=True)
 
 
+def roofline_components(form, mesh, frequencies, steps, fp32_tflops, hbm_gbs):
+    """Per kernel family of the mixed C1 sweep: share of device time, bound,
+    algorithmic work per sweep, achieved rate and fraction of its peak, and the
+    time-weighted sum of the fractions (families without a roofline, the
+    latency-bound ones, count with fraction 0). Work per sweep: regular pairs
+    from the library's pair counters (samples x 81 + test points x 114 FP32
+    FLOP), touching and near pairs from its sample counters at the regular
+    sample's 85 FLOP (the same integrand), the column gather 72 B per ordered
+    panel pair and 16 B per matrix entry written, the LU 8 N^3 / 3 real FLOP
+    per matrix, the FP64 residual 16 B per matrix entry per evaluation."""
+    prof, work = form["profile"], form["work"]
+    T, N, F = mesh.triangle_count, mesh.vertex_count, frequencies
+    total = sum(v[0] for v in prof.values()) / steps
+    ms = lambda *keys: sum(prof[k][0] for k in prof if any(k.startswith(p) for p in keys)) / steps  # noqa: E731
+    launches = lambda key: prof.get(key, (0.0, 0))[1] / steps  # noqa: E731
+    reg_flop = sum(work.get(f"pairs_q{n}", 0) * (n * n * MIXED_FP32_FLOPS_PER_SAMPLE + n * MIXED_FP32_FLOPS_PER_TEST_POINT)
+                   for n in (6, 12, 16, 64)) / steps
+    rows = [
+        ("regular pairs", ms("regular_mixed_q"), "fp32", reg_flop, "FLOP"),
+        ("touching pairs", ms("singular_mixed"), "fp32", work.get("singular_samples", 0) / steps * 85, "FLOP"),
+        ("near pairs", ms("near"), "fp32", work.get("near_samples", 0) / steps * 85, "FLOP"),
+        ("column gather", ms("gather_column"), "hbm", F * (T * T * GATHER_BYTES_PER_ORDERED_PAIR + N * N * 16), "B"),
+        ("LU factorisation", ms("lu_panel", "lu_gemm", "lu_pack", "lu_swap", "lu_trsm"), "fp32", F * 8 * N ** 3 / 3,
+         "FLOP"),
+        ("FP64 residual", ms("residual"), "hbm", launches("residual") * F * N * N * 16, "B"),
+    ]
+    comps, weighted, covered = [], 0.0, 0.0
+    for name, t_ms, bound, amount, unit in rows:
+        if t_ms <= 0:
+            continue
+        rate = amount / (t_ms / 1e3)
+        peak = fp32_tflops * 1e12 if bound == "fp32" else (hbm_gbs or 0) * 1e9
+        frac = rate / peak if peak else None
+        share = t_ms / total
+        comps.append({"family": name, "ms_per_sweep": round(t_ms, 4), "share": round(share, 4), "bound": bound,
+                      "work_per_sweep": amount, "unit": unit, "achieved": rate, "frac": frac})
+        weighted += share * (frac or 0.0)
+        covered += share
+    return {"components": comps, "time_weighted_frac": weighted, "share_with_roofline": covered,
+            "peaks": {"fp32_tflops_sgemm": fp32_tflops, "hbm_gbs": hbm_gbs},
+            "note": "kernels outside these families (pair classification, right-hand sides, triangular solves, "
+                    "GMRES-IR orthogonalisation, fields) are latency-bound and count with fraction 0"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1036,6 +1083,8 @@ def main():
             "clocks": mixed["clocks"], "clocks_fp64_plain": plain["clocks"],
             "peaks": {"hbm_gbs": peaks.get("hbm_gbs"), "fp64_tflops_dgemm": fp64, "fp32_tflops_sgemm": fp32},
         }
+        line["roofline_components"] = roofline_components(mixed, mesh, len(req.frequencies), args.steps, fp32,
+                                                          peaks.get("hbm_gbs"))
         if world == 1 and not args.no_cpu_baseline:
             times_cpu, picks, info = cpu_reference(2, 4)
             line["cpu_baseline"] = {"value": len(picks) * len(times_cpu) / sum(times_cpu), "unit": "solves/s",
