@@ -281,8 +281,9 @@ def c3_cases(hs):
             ("horn", "exponential horn h=12.8 mm seed 0", lambda: m.exponential_horn(h=0.0128)),
             ("horn", "exponential horn h=9.0 mm seed 0", lambda: m.exponential_horn(h=0.0090)),
             ("horn", "exponential horn h=6.4 mm seed 0", lambda: m.exponential_horn(h=0.0064)),
-            # N = 16k: mixed form only (the plain form's FP64 pair records alone would be 206 GB)
-            ("sphere", "octahedral-6 r=0.1 m", lambda: m.octahedral_sphere(6), ("mixed",))]
+            # N = 16k: the plain form's FP64 pair records alone would be 206 GB; the FP64
+            # fast-multipole form at tolerance 1e-9 is the FP64 comparison
+            ("sphere", "octahedral-6 r=0.1 m", lambda: m.octahedral_sphere(6), ("mixed", "fmm64"))]
 
 
 def run_c3(args):
@@ -301,8 +302,12 @@ def run_c3(args):
     chosen = [int(c) for c in args.c3_cases.split(",")] if args.c3_cases else range(len(cases))
     forms = tuple(args.c3_forms.split(","))
     for case in (cases[c] for c in chosen):
+        if len(case) >= 4:
+            forms_here = case[3]
+        else:
+            forms_here = forms
         family, name, make = case[:3]
-        case_forms = tuple(f for f in forms if len(case) < 4 or f in case[3])
+        case_forms = tuple(forms_here)
         mesh = make()
         if family == "horn":
             exc = [hs.BemExcitation("throat", [hs.FaceVelocity(hs.meshes.HORN_THROAT, 1.0)])]
@@ -318,9 +323,12 @@ def run_c3(args):
         with hs.CudaBemSolver(mesh) as solver:
             solver.set_stream(stream.cuda_stream)
             for form in case_forms:
+                numerics = (hs.BemNumerics(precision="fp64", acceleration="fast_multipole",
+                                           relative_residual_tolerance=1e-9,
+                                           fast_multipole=hs.FastMultipoleSettings(restart_length=50))
+                            if form == "fmm64" else hs.BemNumerics(precision=form))
                 req = hs.BemRequest(frequencies=C3_FREQUENCIES, observers=obs, excitations=exc,
-                                    medium=hs.AcousticMedium(DENSITY, SOUND_SPEED),
-                                    numerics=hs.BemNumerics(precision=form))
+                                    medium=hs.AcousticMedium(DENSITY, SOUND_SPEED), numerics=numerics)
                 solver.solve(req)  # plan, workspace and warm-up
                 solver.set_profiling(True)
                 t0 = time.perf_counter()
@@ -337,13 +345,14 @@ def run_c3(args):
                               "residual_max": max(e.boundary_residual for f in res.frequencies for e in f.excitations)}
                 if form == "mixed":
                     line[form]["gmres_iterations"] = [e.iterations for f in res.frequencies for e in f.excitations]
-        if len(results) == 2:
+        base = "fp64" if "fp64" in results else "fmm64" if "fmm64" in results else None
+        if base and "mixed" in results:
             err = 0.0
-            for fp, fm in zip(results["fp64"].frequencies, results["mixed"].frequencies):
+            for fp, fm in zip(results[base].frequencies, results["mixed"].frequencies):
                 a, b = fp.excitations[0].boundary.surface_pressure, fm.excitations[0].boundary.surface_pressure
                 err = max(err, float(np.sqrt((area * np.abs(b - a) ** 2).sum() / (area * np.abs(a) ** 2).sum())))
-            line["max_rel_err_surface_mixed_vs_fp64"] = err
-            line["mixed_over_fp64"] = line["fp64"]["ms_per_frequency"] / line["mixed"]["ms_per_frequency"]
+            line[f"max_rel_err_surface_mixed_vs_{base}"] = err
+            line[f"mixed_over_{base}"] = line[base]["ms_per_frequency"] / line["mixed"]["ms_per_frequency"]
         print(json.dumps(line), flush=True)
         del results
         torch.cuda.empty_cache()
