@@ -722,6 +722,7 @@ def run_serve(args):
             "triangles": [min(m.triangle_count for _, m, _, _ in stream), max(m.triangle_count for _, m, _, _ in stream)]}
     for form in ("mixed", "fp64"):
         latencies, errors = [None] * len(stream), []
+        runs, plans = [None] * len(stream), [None] * len(stream)
         with hs.BemServer(hs.ServeOptions(workers=args.serve_workers)) as server:
             # warm the library (CUDA context, rule tables) outside the timed stream
             warm = stream[0]
@@ -742,8 +743,10 @@ def run_serve(args):
                     if tickets[i] < 0:
                         continue
                     try:
-                        _, timing = server.wait(tickets[i])
+                        result, timing = server.wait(tickets[i])
                         latencies[i] = timing.latency_ms
+                        runs[i] = timing.run_ms
+                        plans[i] = sum(f.interaction_plan_milliseconds for f in result.frequencies)
                     except Exception as e:  # recorded, not fatal
                         errors.append(f"{type(e).__name__}: {e}")
                 done.set()
@@ -773,9 +776,13 @@ def run_serve(args):
             makespan = time.perf_counter() - t0
         ok = [x for x in latencies if x is not None]
         points = sum(len(f) for (_, _, f, _), x in zip(stream, latencies) if x is not None)
+        run_ok = [x for x in runs if x is not None]
+        plan_ok = [x for x in plans if x is not None]
         line[form] = {"solves_per_s": points / makespan, "makespan_s": makespan,
                       "p50_ms": float(np.percentile(ok, 50)) if ok else None,
                       "p99_ms": float(np.percentile(ok, 99)) if ok else None,
+                      "run_ms_mean": float(np.mean(run_ok)) if run_ok else None,
+                      "plan_ms_mean": float(np.mean(plan_ok)) if plan_ok else None,
                       "completed": len(ok), "errors": errors[:5]}
     line["mixed_over_fp64_solves_per_s"] = line["mixed"]["solves_per_s"] / line["fp64"]["solves_per_s"]
     print(json.dumps(line), flush=True)
