@@ -282,7 +282,7 @@ def c3_cases(hs):
             ("horn", "exponential horn h=9.0 mm seed 0", lambda: m.exponential_horn(h=0.0090)),
             ("horn", "exponential horn h=6.4 mm seed 0", lambda: m.exponential_horn(h=0.0064)),
             # N = 16k: the plain form's FP64 pair records alone would be 206 GB; the FP64
-            # fast-multipole form at tolerance 1e-9 is the FP64 comparison
+            # fast-multipole form at tolerance 1e-7 (the reference's tightest) is the FP64 comparison
             ("sphere", "octahedral-6 r=0.1 m", lambda: m.octahedral_sphere(6), ("mixed", "fmm64"))]
 
 
@@ -324,7 +324,7 @@ def run_c3(args):
             solver.set_stream(stream.cuda_stream)
             for form in case_forms:
                 numerics = (hs.BemNumerics(precision="fp64", acceleration="fast_multipole",
-                                           relative_residual_tolerance=1e-9,
+                                           relative_residual_tolerance=1e-7,
                                            fast_multipole=hs.FastMultipoleSettings(restart_length=50))
                             if form == "fmm64" else hs.BemNumerics(precision=form))
                 req = hs.BemRequest(frequencies=C3_FREQUENCIES, observers=obs, excitations=exc,

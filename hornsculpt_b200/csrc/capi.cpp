@@ -530,8 +530,10 @@ hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, 
             stats[4] = st.deviceMs;
             stats[5] = st.hostMs;
             stats[6] = double(st.resolvedPairs);
-            for (int i = 0; i < 5; ++i)
+            for (int i = 0; i < 5; ++i) {
                 stats[7 + i] = st.phaseMs[i];
+                stats[12 + i] = st.hostPhaseMs[i];
+            }
         }
         writePlan(c.plan, sizes, touching, near, patches, whole, near_offsets, near_trials);
         if (touching || near || patches || whole || near_offsets || near_trials)
@@ -627,8 +629,10 @@ hs_status hs_bem_session_plan_stats(hs_bem_session *s, double *stats) {
         stats[4] = st.deviceMs;
         stats[5] = st.hostMs;
         stats[6] = double(st.resolvedPairs);
-        for (int i = 0; i < 5; ++i)
+        for (int i = 0; i < 5; ++i) {
             stats[7 + i] = st.phaseMs[i];
+            stats[12 + i] = st.hostPhaseMs[i];
+        }
     });
 }
 

@@ -32,6 +32,8 @@ struct DevicePlanStats {
     // frame (validation, bounds, touching jobs, candidates), classification,
     // refinement, readback, host part (runs, host pairs, flattening)
     double phaseMs[5]{};
+    // the host part: ordering runs, host pairs, flattening, patch fill, near CSR
+    double hostPhaseMs[5]{};
 };
 
 // The plan of makePlan, with the adaptive pairs refined on the current CUDA
