@@ -34,11 +34,9 @@ namespace {
 #if defined(__CUDACC__)
 #define PD_HD __host__ __device__
 #define PD_NOINLINE __noinline__
-#define PD_INLINE __forceinline__
 #else
 #define PD_HD
 #define PD_NOINLINE
-#define PD_INLINE inline
 #endif
 
 constexpr uint32_t kLeafCap = 2048;  // leaves held per warp (pending + at the depth limit + requested)
@@ -103,7 +101,6 @@ struct WarpMem {
     uint32_t *atl;
     double *pts;   // test and trial point tables, 2 x kRulePoints x kPts
     double *rows;  // row items of a moment computation, kRulePoints x kRowValues
-    double *park;  // the two rules' moment values, 2 x kValues
 };
 
 struct PairOutput {
@@ -156,7 +153,7 @@ constexpr int kRowValues = 28;  // per row item: 12 complex inner sums and 4 mag
 // moment values add bt_i In[c][j] over the rows. `own` receives the lane's
 // values; `bad` is set for a coincident point.
 template <class Wp>
-PD_HD PD_INLINE void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, const Sub &a, const Sub &b,
+PD_HD PD_NOINLINE void tensorMoments(const Wp &w, const HostPanel &t, const HostPanel &s, const Sub &a, const Sub &b,
                          const double *rule, int n, double k, double scale, double *pts, double *rows, double *own,
                          bool &bad) {
     constexpr int W = Wp::W;
@@ -230,12 +227,9 @@ PD_HD PD_INLINE void tensorMoments(const Wp &w, const HostPanel &t, const HostPa
         double acc = 0;
         if (v < 72) {
             const int comp = v >> 1, ri = v & 1, c = comp / 9, i = (comp % 9) / 3, j = comp % 3;
-            const double *R = rows + 2 * (3 * c + j) + ri;
-            for (int xi = 0; xi < n; ++xi) {
-                const double bt = pts[kPts * xi + i];
-                for (int h = 0; h < split; ++h, R += kRowValues)
-                    acc = fma(bt, *R, acc);
-            }
+            const int col = 2 * (3 * c + j) + ri;
+            for (int it = 0; it < items; ++it)
+                acc = fma(pts[kPts * (it / split) + i], rows[kRowValues * it + col], acc);
         } else if (v < 76) {
             for (int it = 0; it < items; ++it)
                 acc += rows[kRowValues * it + 24 + (v - 72)];
@@ -254,29 +248,16 @@ PD_HD PD_INLINE void tensorMoments(const Wp &w, const HostPanel &t, const HostPa
 //   errB bounds |error_device - error_host|, intB a moment value.
 template <class Wp>
 PD_HD void estimateLeaf(const Wp &w, const HostPanel &t, const HostPanel &s, const LeafHdr &L, const RuleTables &R,
-                        double k, double scale, double *pts, double *rows, double *park, double *hiOwn,
-                        double &error, double &errB,
+                        double k, double scale, double *pts, double *rows, double *hiOwn, double &error,
+                        double &errB,
                         double &intB, double &mnL, bool &bad) {
     constexpr int own_n = kValues / Wp::W;
     const int lo = L.degree == 8 ? 0 : 2, hi = lo + 1;
-    // L lives in the warp's arena: its sub-triangles are read where the point
-    // tables are built and hold no registers during the sample loops. One copy
-    // of the moment code serves both rules; each rule's lane values are parked
-    // in `park` (2 x 128 per warp).
-    for (int rr = 0; rr < 2; ++rr) {
-        double own[own_n];
-        const int rule = rr == 0 ? lo : hi;
-        tensorMoments(w, t, s, L.a, L.b, R.pts[rule], R.n[rule], k, scale, pts, rows, own, bad);
-        for (int o = 0; o < own_n; ++o)
-            park[kValues * rr + own_n * w.lane() + o] = own[o];
-    }
-    w.sync();
     double loOwn[own_n];
-    for (int o = 0; o < own_n; ++o) {
-        loOwn[o] = park[own_n * w.lane() + o];
-        hiOwn[o] = park[kValues + own_n * w.lane() + o];
-    }
-    w.sync();
+    // L lives in the warp's arena: its sub-triangles are read where the point
+    // tables are built and hold no registers during the sample loops
+    tensorMoments(w, t, s, L.a, L.b, R.pts[lo], R.n[lo], k, scale, pts, rows, loOwn, bad);
+    tensorMoments(w, t, s, L.a, L.b, R.pts[hi], R.n[hi], k, scale, pts, rows, hiOwn, bad);
     // magnitude sums live in values 72..75
     const int magLane = 72 / own_n, magOff = 72 - magLane * own_n;
     double Elo = 0, Ehi = 0;
@@ -420,8 +401,7 @@ PD_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
             const LeafHdr &L = M.hdr[req[r]];
             double hiOwn[own_n], error = 0, errB = 0, leafIntB = 0, mnL = 0;
             bool bad = false;
-            estimateLeaf(w, t, s, L, P.rules, P.k, scale, M.pts, M.rows, M.park, hiOwn, error, errB, leafIntB, mnL,
-                         bad);
+            estimateLeaf(w, t, s, L, P.rules, P.k, scale, M.pts, M.rows, hiOwn, error, errB, leafIntB, mnL, bad);
             if (bad)
                 return kPairHost;
             for (int v = 0; v < own_n && base + v < 72; ++v)
@@ -660,7 +640,7 @@ __global__ void classifyKernel(ClassifyParams P, const uint2 *candidates, unsign
 
 constexpr int kWarpsPerBlock = 4;
 
-constexpr int kWarpSmemDoubles = 2 * kRulePoints * kPts + kRulePoints * kRowValues + 2 * kValues;
+constexpr int kWarpSmemDoubles = 2 * kRulePoints * kPts + kRulePoints * kRowValues;
 constexpr size_t kRefineSmem = sizeof(double) * kWarpSmemDoubles * kWarpsPerBlock;
 
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) refineKernel(AdaptiveParams P, const uint2 *list,
@@ -680,7 +660,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) refineKernel(AdaptivePara
     M.atl = arena.atl + warpId * kLeafCap;
     M.pts = smem + size_t(kWarpSmemDoubles) * wInBlock;
     M.rows = M.pts + 2 * kRulePoints * kPts;
-    M.park = M.rows + kRulePoints * kRowValues;
     for (;;) {
         unsigned long long p = 0;
         if (w.leader())
@@ -798,10 +777,9 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             threads.emplace_back([&]() {
                 std::vector<LeafHdr> hdr(kLeafCap);
                 std::vector<double> integ(size_t(kLeafCap) * 72), pendErr(kLeafCap), pts(2 * kRulePoints * kPts),
-                    rows(size_t(kRulePoints) * kRowValues), park(2 * kValues);
+                    rows(size_t(kRulePoints) * kRowValues);
                 std::vector<uint32_t> pend(kLeafCap), atl(kLeafCap);
-                WarpMem M{hdr.data(), integ.data(), pend.data(), pendErr.data(), atl.data(), pts.data(), rows.data(),
-                          park.data()};
+                WarpMem M{hdr.data(), integ.data(), pend.data(), pendErr.data(), atl.data(), pts.data(), rows.data()};
                 for (;;) {
                     const size_t p = next.fetch_add(1);
                     if (p >= deviceList.size())
@@ -913,7 +891,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         if (f.allPairs)
             check(cudaMemsetAsync(dWhole.p, 0, units, stream), "planner reset");
         WarpMem arena{dHdr.as<LeafHdr>(), dInteg.as<double>(), dPend.as<uint32_t>(), dPendErr.as<double>(),
-                      dAtl.as<uint32_t>(), nullptr, nullptr, nullptr};
+                      dAtl.as<uint32_t>(), nullptr, nullptr};
         PairOutput O{dPool.as<PatchCode>(), poolCap, counters + 2, dRecords.as<PairRecord>(), counters + 3,
                      dWhole.as<uint8_t>()};
         for (unsigned long long begin = 0; begin < nDevice; begin += chunk) {
