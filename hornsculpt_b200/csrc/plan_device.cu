@@ -686,10 +686,10 @@ void check(cudaError_t e, const char *what) {
 // The sub-triangle at the end of a quadtree path (2 bits per level, child
 // order of quarter()), by the halvings the refinement performed.
 Sub subOfPath(uint32_t path, uint32_t depth) {
-    Sub cur = wholeSub(), children[4];
+    Sub cur = wholeSub(), next;
     for (uint32_t l = 0; l < depth; ++l) {
-        quarter(cur, children);
-        cur = children[(path >> (2 * l)) & 3];
+        quarterChild(cur, int((path >> (2 * l)) & 3), next);
+        cur = next;
     }
     return cur;
 }
