@@ -824,11 +824,22 @@ def run_plan(args):
         t2 = time.perf_counter()
         equal = all(np.array_equal(d[key], h[key]) for key in ("touching", "near", "patches", "whole", "trials",
                                                                  "offsets"))
+        st = d["stats"]
+        # refinement kernel against the FP64 roofline: 97 FLOP per kernel sample (displacement 6,
+        # distance 5 + sqrt, phase 2 + sincos, 1/r and factors 5, derivative kernel 12, weight 1,
+        # 12 complex multiply-adds into the row sums 51, magnitude sums 12; sqrt, division and
+        # sincos counted as 1)
+        fp64 = fp64_peak_tflops(torch)
+        achieved = st["samples"] * 97 / (st["refine_kernel_ms"] / 1e3) / 1e12 if st["refine_kernel_ms"] else None
         line = {"workload": "interaction planning", "mesh": name, "T": mesh.triangle_count, "frequency_hz": f,
                 "numerics": kw, "device_planner_s": round(t1 - t0, 3), "host_planner_s": round(t2 - t1, 3),
                 "speedup": round((t2 - t1) / (t1 - t0), 2), "host_threads": os.cpu_count(),
                 "plans_equal_bit_for_bit": equal, "near_jobs": int(len(h["near"])), "patches": int(len(h["patches"])),
-                "whole_panel_bytes": int(len(h["whole"])), "stats": {k2: round(v, 3) for k2, v in d["stats"].items()}}
+                "whole_panel_bytes": int(len(h["whole"])), "stats": {k2: round(v, 3) for k2, v in d["stats"].items()},
+                "roofline_refine": {"bound": "fp64", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                                    "frac": achieved / fp64 if achieved else None,
+                                    "algorithmic": f"{st['samples']:.0f} kernel samples x 97 FP64 FLOP",
+                                    "peak_source": "cuBLAS DGEMM measured in this run"}}
         print(json.dumps(line), flush=True)
 
 

@@ -534,6 +534,8 @@ hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, 
                 stats[7 + i] = st.phaseMs[i];
                 stats[12 + i] = st.hostPhaseMs[i];
             }
+            stats[17] = double(st.samples);
+            stats[18] = st.refineKernelMs;
         }
         writePlan(c.plan, sizes, touching, near, patches, whole, near_offsets, near_trials);
         if (touching || near || patches || whole || near_offsets || near_trials)
@@ -633,6 +635,8 @@ hs_status hs_bem_session_plan_stats(hs_bem_session *s, double *stats) {
             stats[7 + i] = st.phaseMs[i];
             stats[12 + i] = st.hostPhaseMs[i];
         }
+        stats[17] = double(st.samples);
+        stats[18] = st.refineKernelMs;
     });
 }
 

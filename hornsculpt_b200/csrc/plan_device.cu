@@ -109,6 +109,7 @@ struct PairOutput {
     PairRecord *records;
     unsigned long long *recordCount;
     uint8_t *whole;  // all-pairs mode: unordered pair index -> whole-panel degree
+    unsigned long long *samples;  // kernel samples evaluated (both rules of every estimate)
 };
 
 // ---- warp policies: the same pair code runs with 32 lanes on the device and
@@ -379,7 +380,7 @@ PD_HD PD_NOINLINE void spawnChildren(LeafHdr *hdr, const uint32_t *slots, const 
 // kPairHost (the host planner must refine this pair).
 template <class Wp>
 PD_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams &P, const WarpMem &M,
-                     const PairOutput &O) {
+                     const PairOutput &O, unsigned long long &samples) {
     constexpr int own_n = kValues / Wp::W;
     const HostPanel &t = P.panels[ti], &s = P.panels[si];
     const double scale = maxD(t.maxEdge, s.maxEdge);
@@ -399,6 +400,11 @@ PD_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
     for (;;) {
         for (int r = 0; r < nReq; ++r) {
             const LeafHdr &L = M.hdr[req[r]];
+            {
+                const int lo = L.degree == 8 ? 0 : 2;
+                samples += (unsigned long long)(P.rules.n[lo]) * P.rules.n[lo] +
+                           (unsigned long long)(P.rules.n[lo + 1]) * P.rules.n[lo + 1];
+            }
             double hiOwn[own_n], error = 0, errB = 0, leafIntB = 0, mnL = 0;
             bool bad = false;
             estimateLeaf(w, t, s, L, P.rules, P.k, scale, M.pts, M.rows, hiOwn, error, errB, leafIntB, mnL, bad);
@@ -660,19 +666,22 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) refineKernel(AdaptivePara
     M.atl = arena.atl + warpId * kLeafCap;
     M.pts = smem + size_t(kWarpSmemDoubles) * wInBlock;
     M.rows = M.pts + 2 * kRulePoints * kPts;
+    unsigned long long samples = 0;
     for (;;) {
         unsigned long long p = 0;
         if (w.leader())
             p = atomicAdd(next, 1ull);
         p = __shfl_sync(~0u, p, 0);
         if (p >= count)
-            return;
+            break;
         const uint2 pr = list[p];
-        const int r = refinePair(w, pr.x, pr.y, P, M, O);
+        const int r = refinePair(w, pr.x, pr.y, P, M, O, samples);
         if (r == kPairHost && w.leader())
             flagged[atomicAdd(flagCount, 1ull)] = pr;
         __syncwarp();
     }
+    if (w.leader())
+        atomicAdd(O.samples, samples);
 }
 #endif
 
@@ -742,6 +751,8 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
     std::vector<uint8_t> whole;
     std::vector<uint2> flagged;
     size_t devicePairs = 0;
+    unsigned long long sampleTotal = 0;
+    double refineKernelMs = 0;
     if (cancel && *cancel)
         throw Cancelled();
     if (emulate) {
@@ -768,7 +779,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         pool.resize(size_t(64) * deviceList.size() + 65536);
         records.resize(deviceList.size());
         unsigned long long poolUsed = 0, recordCount = 0;
-        PairOutput O{pool.data(), pool.size(), &poolUsed, records.data(), &recordCount, whole.data()};
+        PairOutput O{pool.data(), pool.size(), &poolUsed, records.data(), &recordCount, whole.data(), &sampleTotal};
         std::atomic<size_t> next{0};
         std::mutex flagMutex;
         const unsigned workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
@@ -780,15 +791,17 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                     rows(size_t(kRulePoints) * kRowValues);
                 std::vector<uint32_t> pend(kLeafCap), atl(kLeafCap);
                 WarpMem M{hdr.data(), integ.data(), pend.data(), pendErr.data(), atl.data(), pts.data(), rows.data()};
+                unsigned long long samples = 0;
                 for (;;) {
                     const size_t p = next.fetch_add(1);
                     if (p >= deviceList.size())
-                        return;
-                    if (refinePair(LaneWarp{}, deviceList[p].x, deviceList[p].y, A, M, O) == kPairHost) {
+                        break;
+                    if (refinePair(LaneWarp{}, deviceList[p].x, deviceList[p].y, A, M, O, samples) == kPairHost) {
                         std::lock_guard<std::mutex> lock(flagMutex);
                         flagged.push_back(deviceList[p]);
                     }
                 }
+                __atomic_fetch_add(&sampleTotal, samples, __ATOMIC_RELAXED);
             });
         for (auto &th : threads)
             th.join();
@@ -893,19 +906,36 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         WarpMem arena{dHdr.as<LeafHdr>(), dInteg.as<double>(), dPend.as<uint32_t>(), dPendErr.as<double>(),
                       dAtl.as<uint32_t>(), nullptr, nullptr};
         PairOutput O{dPool.as<PatchCode>(), poolCap, counters + 2, dRecords.as<PairRecord>(), counters + 3,
-                     dWhole.as<uint8_t>()};
+                     dWhole.as<uint8_t>(), counters + 6};
+        struct Events {  // kernel time of the refinement launches
+            cudaEvent_t a = nullptr, b = nullptr;
+            ~Events() {
+                if (a)
+                    cudaEventDestroy(a);
+                if (b)
+                    cudaEventDestroy(b);
+            }
+        } events;
+        check(cudaEventCreate(&events.a), "planner event");
+        check(cudaEventCreate(&events.b), "planner event");
+        const cudaEvent_t evStart = events.a, evStop = events.b;
         for (unsigned long long begin = 0; begin < nDevice; begin += chunk) {
             if (cancel && *cancel)
                 throw Cancelled();
             const unsigned long long n = std::min(chunk, nDevice - begin);
             check(cudaMemsetAsync(counters + 2, 0, 2 * sizeof(unsigned long long), stream), "planner reset");
             check(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), stream), "planner reset");
+            check(cudaEventRecord(evStart, stream), "planner event");
             refineKernel<<<unsigned(grid), 32 * kWarpsPerBlock, kRefineSmem, stream>>>(
                 A, dDeviceList.as<uint2>() + begin, n, counters + 5, arena, O, dFlagged.as<uint2>(), counters + 4);
             check(cudaGetLastError(), "planner refinement");
+            check(cudaEventRecord(evStop, stream), "planner event");
             unsigned long long n2c[2] = {};
             check(cudaMemcpyAsync(n2c, counters + 2, sizeof(n2c), cudaMemcpyDeviceToHost, stream), "planner readback");
             check(cudaStreamSynchronize(stream), "planner refinement");
+            float chunkMs = 0;
+            check(cudaEventElapsedTime(&chunkMs, evStart, evStop), "planner event");
+            refineKernelMs += chunkMs;
             const unsigned long long used = std::min<unsigned long long>(n2c[0], poolCap), nRec = n2c[1];
             const size_t r0 = records.size(), p0 = pool.size();
             records.resize(r0 + nRec);
@@ -924,10 +954,11 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
             for (size_t r = r0; r < records.size(); ++r)
                 records[r].patchFirst += uint32_t(p0);
         }
-        unsigned long long n5[5] = {};
+        unsigned long long n5[7] = {};
         phase[2] = msSince(t0);
         check(cudaMemcpyAsync(n5, counters, sizeof(n5), cudaMemcpyDeviceToHost, stream), "planner readback");
         check(cudaStreamSynchronize(stream), "planner readback");
+        sampleTotal = n5[6];
         const unsigned long long nFlag = n5[4];
         flagged.resize(nFlag);
         if (nFlag)
@@ -1124,6 +1155,8 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         stats->projectedPairs = hostList.size();
         stats->flaggedPairs = flagged.size();
         stats->resolvedPairs = resolved;
+        stats->samples = sampleTotal;
+        stats->refineKernelMs = refineKernelMs;
         size_t wholeCount = 0;
         for (const auto b : whole)
             wholeCount += b != 0;
