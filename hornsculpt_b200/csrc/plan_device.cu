@@ -144,7 +144,7 @@ struct DeviceWarp {
 // test function i, trial function j) and 4 magnitude sums (values 72..75).
 // After a moment computation lane l holds values [128/W l, 128/W (l+1)).
 constexpr int kValues = 128;
-constexpr int kRowValues = 28;  // per row item: 12 complex inner sums and 4 magnitude sums
+constexpr int kRowValues = 32;  // per row item: 12 complex inner sums, 4 magnitude sums, its test barycentrics, pad
 
 // Tensor moments of one rule over sub-triangles a (test) and b (trial)
 // (the host's tensorMoments). The test barycentrics depend on the test point
@@ -219,6 +219,7 @@ PD_HD PD_NOINLINE void tensorMoments(const Wp &w, const HostPanel &t, const Host
         for (int v = 0; v < 24; ++v)
             R[v] = in[v];
         R[24] = m[0], R[25] = m[1], R[26] = m[2], R[27] = m[3];
+        R[28] = T[0], R[29] = T[1], R[30] = T[2];
     }
     w.sync();
     constexpr int own_n = kValues / W;
@@ -230,7 +231,7 @@ PD_HD PD_NOINLINE void tensorMoments(const Wp &w, const HostPanel &t, const Host
             const int comp = v >> 1, ri = v & 1, c = comp / 9, i = (comp % 9) / 3, j = comp % 3;
             const int col = 2 * (3 * c + j) + ri;
             for (int it = 0; it < items; ++it)
-                acc = fma(pts[kPts * (it / split) + i], rows[kRowValues * it + col], acc);
+                acc = fma(rows[kRowValues * it + 28 + i], rows[kRowValues * it + col], acc);
         } else if (v < 76) {
             for (int it = 0; it < items; ++it)
                 acc += rows[kRowValues * it + 24 + (v - 72)];
