@@ -113,6 +113,42 @@ def scalene_tetrahedron() -> SurfaceMesh:
     return SurfaceMesh(v, t, [50, 51, 52, 53], [DRIVEN, DRIVEN, WALL, WALL])
 
 
+def thin_box(lx: float, ly: float, lz: float, n: int, face_id: int = 1) -> SurfaceMesh:
+    """Closed outward cuboid [0, lx] x [0, ly] x [0, lz]: n x n squares (two triangles
+    each) on the top and bottom faces, one layer of n squares on each side. With lz much
+    smaller than lx / n the top and bottom panels face each other across a gap the
+    interaction plan integrates on projected patches (like the reference's thin closed
+    box, ``docs/BURTON-MILLER.md:277-283``). All faces driven."""
+    index, verts, tris = {}, [], []
+
+    def vid(p):
+        key = tuple(round(c, 12) for c in p)
+        if key not in index:
+            index[key] = len(verts)
+            verts.append(p)
+        return index[key]
+
+    def quad(a, b, c, d):  # counter-clockwise seen from outside
+        tris.append((vid(a), vid(b), vid(c)))
+        tris.append((vid(a), vid(c), vid(d)))
+
+    xs, ys = np.linspace(0, lx, n + 1), np.linspace(0, ly, n + 1)
+    for i in range(n):
+        for j in range(n):
+            x0, x1, y0, y1 = xs[i], xs[i + 1], ys[j], ys[j + 1]
+            quad((x0, y0, lz), (x1, y0, lz), (x1, y1, lz), (x0, y1, lz))
+            quad((x0, y0, 0), (x0, y1, 0), (x1, y1, 0), (x1, y0, 0))
+    for i in range(n):
+        x0, x1, y0, y1 = xs[i], xs[i + 1], ys[i], ys[i + 1]
+        quad((x0, 0, 0), (x1, 0, 0), (x1, 0, lz), (x0, 0, lz))
+        quad((x0, ly, 0), (x0, ly, lz), (x1, ly, lz), (x1, ly, 0))
+        quad((0, y0, 0), (0, y0, lz), (0, y1, lz), (0, y1, 0))
+        quad((lx, y0, 0), (lx, y1, 0), (lx, y1, lz), (lx, y0, lz))
+    T = len(tris)
+    return SurfaceMesh(np.array(verts, float), np.array(tris, np.uint32), np.full(T, face_id, np.uint32),
+                       np.full(T, DRIVEN, np.uint8))
+
+
 def signed_volume(mesh: SurfaceMesh) -> float:
     v = mesh.vertices[mesh.triangles] - mesh.vertices.min(0)
     return float(np.einsum("ij,ij->i", v[:, 0], np.cross(v[:, 1], v[:, 2])).sum() / 6)

@@ -40,6 +40,8 @@ CASES = [
     ("short_horn", lambda: meshes.exponential_horn(length=0.1, mouth_radius=0.05, h=0.0128), 3000.0, {}),
     ("short_horn_tight", lambda: meshes.exponential_horn(length=0.1, mouth_radius=0.05, h=0.0128), 1000.0,
      {"near_relative_tolerance": 1e-5}),
+    # 0.2 mm thin box: pairs across the gap on projected patches (refined by the host's code)
+    ("thin_box", lambda: meshes.thin_box(0.02, 0.02, 0.0002, 2), 1000.0, {}),
 ]
 
 
@@ -60,7 +62,10 @@ def test_device_plan_equals_host_plan(name, make, f, kw):
           f"{s['flagged_pairs']:.0f} handed back, {s['resolved_pairs']:.0f} ordered by the host, "
           f"{s['projected_pairs']:.0f} projected")
     assert s["device_pairs"] > 0
-    assert s["flagged_pairs"] <= 0.01 * s["device_pairs"]
+    if name == "thin_box":
+        assert s["projected_pairs"] > 0
+    else:
+        assert s["flagged_pairs"] <= 0.01 * s["device_pairs"]
 
 
 def test_session_planned_on_the_device_solves_like_the_host_planner():

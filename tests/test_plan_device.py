@@ -44,3 +44,15 @@ def test_device_plan_validates_like_the_host_plan():
     mesh = meshes.octahedral_sphere(1)
     with pytest.raises(ValueError, match="interaction-plan input"):
         hs.device_plan(mesh, hs.BemNumerics(near_maximum_depth=17), 10.0, emulate=True)
+
+
+def test_emulated_device_plan_hands_projected_pairs_to_the_host():
+    """A 0.2 mm thin box: panels facing each other across the gap are integrated on
+    projected patches by the host planner's code; the merged plan is the host's."""
+    mesh = meshes.thin_box(0.02, 0.02, 0.0002, 2)
+    k = 2 * np.pi * 1000 / 343
+    d = hs.device_plan(mesh, hs.BemNumerics(), k, emulate=True)
+    h = hs.host_plan(mesh, hs.BemNumerics(), k)
+    for key in KEYS:
+        assert np.array_equal(d[key], h[key]), key
+    assert d["stats"]["projected_pairs"] > 0 and (h["patches"][:, 20] == 1).any()
