@@ -262,7 +262,7 @@ class CudaBemSolver:
 
     def plan_stats(self) -> dict:
         """Statistics of the session's last device plan (see device_plan)."""
-        stats = (C.c_double * 19)()
+        stats = (C.c_double * 20)()
         _lib.check(self._lib.hs_bem_session_plan_stats(self._handle, stats))
         return dict(zip(PLAN_STATS, list(stats)))
 
@@ -608,7 +608,7 @@ def host_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float) -> dict:
 PLAN_STATS = ("device_pairs", "projected_pairs", "flagged_pairs", "whole_panel_pairs", "device_ms", "host_ms",
               "resolved_pairs", "frame_ms", "classify_ms", "refine_ms", "readback_ms", "host_part_ms",
               "host_runs_ms", "host_pairs_ms", "host_flatten_ms", "host_fill_ms", "host_csr_ms", "samples",
-              "refine_kernel_ms")
+              "refine_kernel_ms", "root_settled_pairs")
 
 
 def device_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float, emulate: bool = False) -> dict:
@@ -619,7 +619,7 @@ def device_plan(mesh: SurfaceMesh, numerics: BemNumerics, max_k: float, emulate:
     lib = _lib.load()
     n = numerics.to_c()
     sizes = (C.c_size_t * 6)()
-    stats = (C.c_double * 19)()
+    stats = (C.c_double * 20)()
     args = (mesh.vertices.ctypes.data, mesh.vertex_count, mesh.triangles.ctypes.data, mesh.triangle_count, C.byref(n),
             max_k, 1 if emulate else 0, stats, sizes)
     _lib.check(lib.hs_bem_debug_plan_device(*args, None, None, None, None, None, None))

@@ -536,6 +536,7 @@ hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, 
             }
             stats[17] = double(st.samples);
             stats[18] = st.refineKernelMs;
+            stats[19] = double(st.rootSettledPairs);
         }
         writePlan(c.plan, sizes, touching, near, patches, whole, near_offsets, near_trials);
         if (touching || near || patches || whole || near_offsets || near_trials)
@@ -637,6 +638,7 @@ hs_status hs_bem_session_plan_stats(hs_bem_session *s, double *stats) {
         }
         stats[17] = double(st.samples);
         stats[18] = st.refineKernelMs;
+        stats[19] = double(st.rootSettledPairs);
     });
 }
 

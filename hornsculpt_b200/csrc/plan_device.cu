@@ -576,6 +576,101 @@ PD_HD int refinePair(const Wp &w, uint32_t ti, uint32_t si, const AdaptiveParams
     }
 }
 
+// ---- root pre-pass (all-pairs mode) ----
+// Most pairs of the all-pairs table end at their root estimate (the whole-panel
+// degree-8 rule). Four lanes take one pair, lane c summing kernel channel c of
+// both rules in registers; the first decision of the refinement, with the same
+// bounds as refinePair, settles the pair when it clearly converges at the root.
+// Every other pair goes on to refineKernel.
+struct RootChannel {
+    double dmax, hmax, Elo, Ehi;
+    bool bad;
+};
+
+// Channel c (0: G, 1..3: the gradient components) of the root leaf's two rules.
+PD_HD RootChannel rootChannel(const HostPanel &t, const HostPanel &s, int c, const RuleTables &R, double k,
+                              double scale) {
+    const V3 origin = t.v[0] - s.v[0];
+    double hi[18], lo[18], A[2] = {0, 0};
+    bool bad = false;
+    for (int rr = 1; rr >= 0; --rr) {  // the degree 8 rule, then the degree 6 rule
+        const double *rule = R.pts[rr];
+        const int n = R.n[rr];
+        double *m = rr == 1 ? hi : lo;
+        for (int v = 0; v < 18; ++v)
+            m[v] = 0;
+        for (int x = 0; x < n; ++x) {
+            // whole test panel: the rule's barycentrics are the point's
+            const double bt[3] = {rule[4 * x], rule[4 * x + 1], rule[4 * x + 2]}, wx = rule[4 * x + 3];
+            const V3 lt = localPoint(t, bt);
+            double in[6] = {0, 0, 0, 0, 0, 0};
+            for (int q = 0; q < n; ++q) {
+                const double bs[3] = {rule[4 * q], rule[4 * q + 1], rule[4 * q + 2]};
+                const V3 ls = localPoint(s, bs);
+                const V3 d{origin.x + (lt.x - ls.x), origin.y + (lt.y - ls.y), origin.z + (lt.z - ls.z)};
+                const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+                if (!(r > 0)) {
+                    bad = true;
+                    continue;
+                }
+                double sn, cs;
+                sincos(-k * r, &sn, &cs);
+                const double ir = 1 / r, gr = cs * ir, gi = sn * ir, kr = k * r, f = scale * ir * ir;
+                const double wgt = wx * rule[4 * q + 3];
+                double vr, vi, mag;
+                if (c == 0) {
+                    vr = gr, vi = gi, mag = ir;
+                } else {
+                    const double dc = c == 1 ? d.x : c == 2 ? d.y : d.z;
+                    vr = (-gr + gi * kr) * f * dc;
+                    vi = (-gr * kr - gi) * f * dc;
+                    mag = (1 + kr) * f * ir * fabs(dc);
+                }
+                A[rr] += wgt * mag;
+                for (int j = 0; j < 3; ++j) {
+                    in[2 * j] = fma(vr * wgt, bs[j], in[2 * j]);
+                    in[2 * j + 1] = fma(vi * wgt, bs[j], in[2 * j + 1]);
+                }
+            }
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    m[2 * (3 * i + j)] = fma(bt[i], in[2 * j], m[2 * (3 * i + j)]);
+                    m[2 * (3 * i + j) + 1] = fma(bt[i], in[2 * j + 1], m[2 * (3 * i + j) + 1]);
+                }
+        }
+    }
+    RootChannel out{0, 0, 0, 0, bad};
+    for (int v = 0; v < 18; v += 2) {
+        const double dab = hypot(hi[v] - lo[v], hi[v + 1] - lo[v + 1]), hab = hypot(hi[v], hi[v + 1]);
+        out.bad = out.bad || !isfinite(dab) || !isfinite(hab);
+        out.dmax = fmax(out.dmax, dab);
+        out.hmax = fmax(out.hmax, hab);
+    }
+    const double ml = double(R.n[0]) * R.n[0], mh = double(R.n[1]) * R.n[1];
+    out.Elo = (2 * ml + 64) * kUnit * A[0];
+    out.Ehi = (2 * mh + 64) * kUnit * A[1];
+    return out;
+}
+
+// The refinement's first decision from the channels' maxima (refinePair's
+// formulas for a single root leaf): 8 when the root clearly converges (the
+// pair's rule is the whole-panel degree-8 patch), 0 when the pair must be
+// refined further or its decision is too close to call.
+PD_HD uint8_t rootDecision(double error, double mn, double Elo, double Ehi, bool bad, double tol) {
+    if (bad)
+        return 0;
+    const double errB = 1.4142135623730951 * (Ehi + Elo) + 8 * kUnit * error;
+    const double absError = error, absB = errB + 2 * kUnit * absError;
+    const double intB = Ehi + 2 * kUnit * (mn + mn);
+    const double thr = tol * .2 * mn;
+    const double mnB = 1.4142135623730951 * intB + 3 * kUnit * mn;
+    const double thrB = tol * .2 * mnB + 2 * kUnit * thr;
+    if (!separated(absError, thr, absB + thrB) || !(absError <= thr) || !(mn > 0))
+        return 0;
+    const double relError = absError / mn;
+    return isfinite(relError) && relError <= tol ? 8 : 0;
+}
+
 // Pair classification (the host's processPair test): 0 no adaptive rule,
 // kOnDevice a tensor pair, kProjected a pair on projected patches.
 HS_HD uint8_t classifyPair(const ClassifyParams &P, uint32_t i, uint32_t j) {
@@ -643,6 +738,40 @@ __global__ void classifyKernel(ClassifyParams P, const uint2 *candidates, unsign
         if (c == kProjected && hostList)
             hostList[bh + __popc(mh & below)] = make_uint2(i, j);
     }
+}
+
+constexpr int kRootThreads = 128;
+
+// Four lanes per pair; lane c sums channel c. A settled pair writes its
+// whole-panel degree, the others are appended to `rest` for refineKernel.
+__global__ void __launch_bounds__(kRootThreads) rootKernel(AdaptiveParams P, const uint2 *list,
+                                                           unsigned long long count, uint8_t *whole, uint2 *rest,
+                                                           unsigned long long *restCount) {
+    const unsigned long long g = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+    const unsigned long long p = g >> 2;
+    const int c = int(g & 3);
+    const bool active = p < count;
+    uint2 pr = make_uint2(0, 0);
+    RootChannel ch{0, 0, 0, 0, false};
+    if (active) {
+        pr = list[p];
+        const HostPanel &t = P.panels[pr.x], &s = P.panels[pr.y];
+        ch = rootChannel(t, s, c, P.rules, P.k, maxD(t.maxEdge, s.maxEdge));
+    }
+    for (int o = 1; o <= 2; o <<= 1) {  // maxima over the pair's four lanes
+        ch.dmax = fmax(ch.dmax, __shfl_xor_sync(~0u, ch.dmax, o));
+        ch.hmax = fmax(ch.hmax, __shfl_xor_sync(~0u, ch.hmax, o));
+        ch.Elo = fmax(ch.Elo, __shfl_xor_sync(~0u, ch.Elo, o));
+        ch.Ehi = fmax(ch.Ehi, __shfl_xor_sync(~0u, ch.Ehi, o));
+        ch.bad = ch.bad || __shfl_xor_sync(~0u, int(ch.bad), o) != 0;
+    }
+    if (!active || c != 0)
+        return;
+    const uint8_t degree = rootDecision(ch.dmax, ch.hmax, ch.Elo, ch.Ehi, ch.bad, P.tol);
+    if (degree)
+        whole[unorderedPairIndex(pr.x, pr.y)] = degree;
+    else
+        rest[atomicAdd(restCount, 1ull)] = pr;
 }
 
 constexpr int kWarpsPerBlock = 4;
@@ -752,7 +881,8 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
     std::vector<uint8_t> whole;
     std::vector<uint2> flagged;
     size_t devicePairs = 0;
-    unsigned long long sampleTotal = 0;
+    unsigned long long sampleTotal = 0, rootSamples = 0;
+    size_t rootSettled = 0;
     double refineKernelMs = 0;
     if (cancel && *cancel)
         throw Cancelled();
@@ -781,9 +911,47 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         records.resize(deviceList.size());
         unsigned long long poolUsed = 0, recordCount = 0;
         PairOutput O{pool.data(), pool.size(), &poolUsed, records.data(), &recordCount, whole.data(), &sampleTotal};
+        const unsigned workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+        std::vector<uint2> refineList;  // all-pairs mode: the pairs the root pre-pass leaves
+        if (f.allPairs) {
+            std::vector<uint8_t> settled(deviceList.size(), 0);
+            std::atomic<size_t> nextRoot{0};
+            std::vector<std::thread> rootThreads;
+            for (unsigned wkr = 0; wkr < workers; ++wkr)
+                rootThreads.emplace_back([&]() {
+                    for (;;) {
+                        const size_t p = nextRoot.fetch_add(1);
+                        if (p >= deviceList.size())
+                            return;
+                        const HostPanel &t = sp.panels[deviceList[p].x], &s = sp.panels[deviceList[p].y];
+                        RootChannel m{0, 0, 0, 0, false};
+                        for (int c = 0; c < 4; ++c) {
+                            const RootChannel ch = rootChannel(t, s, c, A.rules, maxK, maxD(t.maxEdge, s.maxEdge));
+                            m.dmax = fmax(m.dmax, ch.dmax);
+                            m.hmax = fmax(m.hmax, ch.hmax);
+                            m.Elo = fmax(m.Elo, ch.Elo);
+                            m.Ehi = fmax(m.Ehi, ch.Ehi);
+                            m.bad = m.bad || ch.bad;
+                        }
+                        const uint8_t degree = rootDecision(m.dmax, m.hmax, m.Elo, m.Ehi, m.bad, A.tol);
+                        if (degree) {
+                            whole[unorderedPairIndex(deviceList[p].x, deviceList[p].y)] = degree;
+                            settled[p] = 1;
+                        }
+                    }
+                });
+            for (auto &th : rootThreads)
+                th.join();
+            for (size_t p = 0; p < deviceList.size(); ++p)
+                if (!settled[p])
+                    refineList.push_back(deviceList[p]);
+            rootSettled = deviceList.size() - refineList.size();
+            rootSamples = deviceList.size() * (unsigned long long)(A.rules.n[0] * A.rules.n[0] + A.rules.n[1] * A.rules.n[1]);
+        } else {
+            refineList = deviceList;
+        }
         std::atomic<size_t> next{0};
         std::mutex flagMutex;
-        const unsigned workers = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
         std::vector<std::thread> threads;
         for (unsigned wkr = 0; wkr < workers; ++wkr)
             threads.emplace_back([&]() {
@@ -795,11 +963,11 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
                 unsigned long long samples = 0;
                 for (;;) {
                     const size_t p = next.fetch_add(1);
-                    if (p >= deviceList.size())
+                    if (p >= refineList.size())
                         break;
-                    if (refinePair(LaneWarp{}, deviceList[p].x, deviceList[p].y, A, M, O, samples) == kPairHost) {
+                    if (refinePair(LaneWarp{}, refineList[p].x, refineList[p].y, A, M, O, samples) == kPairHost) {
                         std::lock_guard<std::mutex> lock(flagMutex);
-                        flagged.push_back(deviceList[p]);
+                        flagged.push_back(refineList[p]);
                     }
                 }
                 __atomic_fetch_add(&sampleTotal, samples, __ATOMIC_RELAXED);
@@ -807,6 +975,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         for (auto &th : threads)
             th.join();
         phase[2] = msSince(t0);
+        sampleTotal += rootSamples;
         records.resize(recordCount);
         pool.resize(std::min<size_t>(poolUsed, pool.size()));
         devicePairs = deviceList.size();
@@ -920,15 +1089,39 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         check(cudaEventCreate(&events.a), "planner event");
         check(cudaEventCreate(&events.b), "planner event");
         const cudaEvent_t evStart = events.a, evStop = events.b;
-        for (unsigned long long begin = 0; begin < nDevice; begin += chunk) {
+        // all-pairs mode: the root pre-pass settles the pairs that end at their
+        // root estimate; the rest go to the refinement
+        const uint2 *refineList = dDeviceList.as<uint2>();
+        unsigned long long nRefine = nDevice;
+        DevMem dRest(f.allPairs ? sizeof(uint2) * std::max(nDevice, 1ull) : 16);
+        if (f.allPairs && nDevice) {
+            check(cudaMemsetAsync(counters + 7, 0, sizeof(unsigned long long), stream), "planner reset");
+            check(cudaEventRecord(evStart, stream), "planner event");
+            rootKernel<<<unsigned((nDevice * 4 + kRootThreads - 1) / kRootThreads), kRootThreads, 0, stream>>>(
+                A, dDeviceList.as<uint2>(), nDevice, dWhole.as<uint8_t>(), dRest.as<uint2>(), counters + 7);
+            check(cudaGetLastError(), "planner root pre-pass");
+            check(cudaEventRecord(evStop, stream), "planner event");
+            unsigned long long nRest = 0;
+            check(cudaMemcpyAsync(&nRest, counters + 7, sizeof(nRest), cudaMemcpyDeviceToHost, stream),
+                  "planner readback");
+            check(cudaStreamSynchronize(stream), "planner root pre-pass");
+            float rootMs = 0;
+            check(cudaEventElapsedTime(&rootMs, evStart, evStop), "planner event");
+            refineKernelMs += rootMs;
+            rootSamples = nDevice * (unsigned long long)(A.rules.n[0] * A.rules.n[0] + A.rules.n[1] * A.rules.n[1]);
+            rootSettled = nDevice - nRest;
+            refineList = dRest.as<uint2>();
+            nRefine = nRest;
+        }
+        for (unsigned long long begin = 0; begin < nRefine; begin += chunk) {
             if (cancel && *cancel)
                 throw Cancelled();
-            const unsigned long long n = std::min(chunk, nDevice - begin);
+            const unsigned long long n = std::min(chunk, nRefine - begin);
             check(cudaMemsetAsync(counters + 2, 0, 2 * sizeof(unsigned long long), stream), "planner reset");
             check(cudaMemsetAsync(counters + 5, 0, sizeof(unsigned long long), stream), "planner reset");
             check(cudaEventRecord(evStart, stream), "planner event");
             refineKernel<<<unsigned(grid), 32 * kWarpsPerBlock, kRefineSmem, stream>>>(
-                A, dDeviceList.as<uint2>() + begin, n, counters + 5, arena, O, dFlagged.as<uint2>(), counters + 4);
+                A, refineList + begin, n, counters + 5, arena, O, dFlagged.as<uint2>(), counters + 4);
             check(cudaGetLastError(), "planner refinement");
             check(cudaEventRecord(evStop, stream), "planner event");
             unsigned long long n2c[2] = {};
@@ -959,7 +1152,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         phase[2] = msSince(t0);
         check(cudaMemcpyAsync(n5, counters, sizeof(n5), cudaMemcpyDeviceToHost, stream), "planner readback");
         check(cudaStreamSynchronize(stream), "planner readback");
-        sampleTotal = n5[6];
+        sampleTotal = n5[6] + rootSamples;
         const unsigned long long nFlag = n5[4];
         flagged.resize(nFlag);
         if (nFlag)
@@ -1157,6 +1350,7 @@ Plan makePlanOnDevice(const Space &sp, const PlanSettings &st, double maxK, cuda
         stats->flaggedPairs = flagged.size();
         stats->resolvedPairs = resolved;
         stats->samples = sampleTotal;
+        stats->rootSettledPairs = rootSettled;
         stats->refineKernelMs = refineKernelMs;
         size_t wholeCount = 0;
         for (const auto b : whole)

@@ -29,7 +29,8 @@ struct DevicePlanStats {
     size_t wholePanelPairs{};  // all-pairs mode: single whole-panel rules decided on the device
     size_t resolvedPairs{};    // device pairs whose patch order the host settled by its own estimates
     unsigned long long samples{};  // kernel samples the refinement evaluated (both rules of every estimate)
-    double refineKernelMs{};       // CUDA-event time of the refinement launches
+    double refineKernelMs{};       // CUDA-event time of the refinement launches (root pre-pass included)
+    size_t rootSettledPairs{};     // all-pairs mode: pairs the root pre-pass settled
     double deviceMs{}, hostMs{};
     // frame (validation, bounds, touching jobs, candidates), classification,
     // refinement, readback, host part (runs, host pairs, flattening)

@@ -281,7 +281,7 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
  * mode 1: its algorithm emulated on the host, one lane per warp, no GPU
  * needed). No reference counterpart beyond makeInteractionPlan itself
  * (interaction_plan.cpp:156): the result equals hs_bem_debug_plan's bit for
- * bit. stats (19 doubles, may be NULL): pairs refined on the device, pairs on
+ * bit. stats (20 doubles, may be NULL): pairs refined on the device, pairs on
  * projected patches (refined by the host), device pairs handed to the host
  * because a decision fell within its rounding bound, whole-panel pairs
  * decided on the device (all-pairs mode), device milliseconds, host
@@ -290,7 +290,8 @@ hs_status hs_bem_debug_plan(const double *vertices, size_t vertex_count, const u
  * frame (validation, bounds, touching jobs, grid candidates), classification,
  * refinement, readback, host part; then the host part's own phases: ordering
  * runs, host pairs, flattening, patch fill, near CSR; then the kernel samples
- * the refinement evaluated and the CUDA-event time of its launches. */
+ * the refinement evaluated, the CUDA-event time of its launches and, in the
+ * all-pairs mode, the pairs settled by their root estimate alone. */
 hs_status hs_bem_debug_plan_device(const double *vertices, size_t vertex_count, const uint32_t *triangles,
                                    size_t triangle_count, const hs_numerics *numerics, double max_k, uint32_t mode,
                                    double *stats, size_t *sizes, uint32_t *touching, uint32_t *near,
@@ -336,7 +337,7 @@ hs_status hs_bem_debug_fmm_selftest(double *error);
  * fall within the device's rounding bounds to the host planner's code;
  * HS_PLANNER_HOST plans on host threads like the reference. Both give the
  * same plan bit for bit. hs_bem_session_plan_stats writes the last device
- * plan's statistics (19 doubles, the layout of hs_bem_debug_plan_device). */
+ * plan's statistics (20 doubles, the layout of hs_bem_debug_plan_device). */
 hs_status hs_bem_session_set_planner(hs_bem_session *session, uint32_t planner);
 hs_status hs_bem_session_plan_stats(hs_bem_session *session, double *stats);
 /* Fast-multipole LF/HF switch (wideband_transfer.cpp:266-310): a level's M2L
