@@ -18,11 +18,9 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
-#include <cstring>
 #include <mutex>
 #include <string>
 #include <thread>
-#include <unordered_map>
 #include <vector>
 
 namespace hsb {
@@ -652,6 +650,93 @@ PD_HD RootChannel rootChannel(const HostPanel &t, const HostPanel &s, int c, con
     return out;
 }
 
+#if defined(__CUDACC__)
+// rootChannel with the kernel evaluations shared by the pair's four lanes:
+// lane c evaluates every fourth trial point for all four channels, and a 4 x 4
+// shuffle transpose hands each lane its own channel of the four points.
+__device__ RootChannel rootChannelQuad(const HostPanel &t, const HostPanel &s, int c, bool active,
+                                       const RuleTables &R, double k, double scale) {
+    const V3 origin = t.v[0] - s.v[0];
+    double hi[18], lo[18], A[2] = {0, 0};
+    bool bad = false;
+    for (int rr = 1; rr >= 0; --rr) {
+        const double *rule = R.pts[rr];
+        const int n = R.n[rr];
+        double *m = rr == 1 ? hi : lo;
+        for (int v = 0; v < 18; ++v)
+            m[v] = 0;
+        for (int x = 0; x < n; ++x) {
+            const double bt[3] = {rule[4 * x], rule[4 * x + 1], rule[4 * x + 2]}, wx = rule[4 * x + 3];
+            const V3 lt = localPoint(t, bt);
+            double in[6] = {0, 0, 0, 0, 0, 0};
+            for (int q0 = 0; q0 < n; q0 += 4) {
+                // this lane's point: all four channels (value times weight, magnitude times weight)
+                const int q = q0 + c;
+                double vr[4] = {0, 0, 0, 0}, vi[4] = {0, 0, 0, 0}, mg[4] = {0, 0, 0, 0};
+                if (active && q < n) {
+                    const double bs[3] = {rule[4 * q], rule[4 * q + 1], rule[4 * q + 2]};
+                    const V3 ls = localPoint(s, bs);
+                    const V3 d{origin.x + (lt.x - ls.x), origin.y + (lt.y - ls.y), origin.z + (lt.z - ls.z)};
+                    const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+                    if (!(r > 0)) {
+                        bad = true;
+                    } else {
+                        double sn, cs;
+                        sincos(-k * r, &sn, &cs);
+                        const double ir = 1 / r, gr = cs * ir, gi = sn * ir, kr = k * r, f = scale * ir * ir;
+                        const double wgt = wx * rule[4 * q + 3];
+                        const double dr = (-gr + gi * kr) * f, di = (-gr * kr - gi) * f, md = (1 + kr) * f * ir;
+                        vr[0] = gr * wgt, vi[0] = gi * wgt, mg[0] = ir * wgt;
+                        const double dd[3] = {d.x, d.y, d.z};
+#pragma unroll
+                        for (int ch = 1; ch < 4; ++ch) {
+                            vr[ch] = dr * dd[ch - 1] * wgt;
+                            vi[ch] = di * dd[ch - 1] * wgt;
+                            mg[ch] = md * fabs(dd[ch - 1]) * wgt;
+                        }
+                    }
+                }
+                // transpose: in round o, lane c receives point q0 + (c ^ o)'s channel c
+#pragma unroll
+                for (int o = 0; o < 4; ++o) {
+                    const int send = c ^ o;  // the channel the partner lane needs
+                    const double sr = send == 0 ? vr[0] : send == 1 ? vr[1] : send == 2 ? vr[2] : vr[3];
+                    const double si = send == 0 ? vi[0] : send == 1 ? vi[1] : send == 2 ? vi[2] : vi[3];
+                    const double sm = send == 0 ? mg[0] : send == 1 ? mg[1] : send == 2 ? mg[2] : mg[3];
+                    const double gotr = __shfl_xor_sync(~0u, sr, o), goti = __shfl_xor_sync(~0u, si, o),
+                                 gotm = __shfl_xor_sync(~0u, sm, o);
+                    const int qq = q0 + (c ^ o);
+                    if (qq < n) {
+                        const double bs[3] = {rule[4 * qq], rule[4 * qq + 1], rule[4 * qq + 2]};
+                        A[rr] += gotm;
+                        for (int j = 0; j < 3; ++j) {
+                            in[2 * j] = fma(gotr, bs[j], in[2 * j]);
+                            in[2 * j + 1] = fma(goti, bs[j], in[2 * j + 1]);
+                        }
+                    }
+                }
+            }
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    m[2 * (3 * i + j)] = fma(bt[i], in[2 * j], m[2 * (3 * i + j)]);
+                    m[2 * (3 * i + j) + 1] = fma(bt[i], in[2 * j + 1], m[2 * (3 * i + j) + 1]);
+                }
+        }
+    }
+    RootChannel out{0, 0, 0, 0, bad};
+    for (int v = 0; v < 18; v += 2) {
+        const double dab = hypot(hi[v] - lo[v], hi[v + 1] - lo[v + 1]), hab = hypot(hi[v], hi[v + 1]);
+        out.bad = out.bad || !isfinite(dab) || !isfinite(hab);
+        out.dmax = fmax(out.dmax, dab);
+        out.hmax = fmax(out.hmax, hab);
+    }
+    const double ml = double(R.n[0]) * R.n[0], mh = double(R.n[1]) * R.n[1];
+    out.Elo = (2 * ml + 64) * kUnit * A[0];
+    out.Ehi = (2 * mh + 64) * kUnit * A[1];
+    return out;
+}
+#endif
+
 // The refinement's first decision from the channels' maxima (refinePair's
 // formulas for a single root leaf): 8 when the root clearly converges (the
 // pair's rule is the whole-panel degree-8 patch), 0 when the pair must be
@@ -751,13 +836,12 @@ __global__ void __launch_bounds__(kRootThreads) rootKernel(AdaptiveParams P, con
     const unsigned long long p = g >> 2;
     const int c = int(g & 3);
     const bool active = p < count;
-    uint2 pr = make_uint2(0, 0);
-    RootChannel ch{0, 0, 0, 0, false};
-    if (active) {
-        pr = list[p];
-        const HostPanel &t = P.panels[pr.x], &s = P.panels[pr.y];
-        ch = rootChannel(t, s, c, P.rules, P.k, maxD(t.maxEdge, s.maxEdge));
-    }
+    // pairs beyond the list run pair 0's geometry inactive, so every lane joins the shuffles
+    const uint2 pr = list[active ? p : 0];
+    const HostPanel &t = P.panels[pr.x], &s = P.panels[pr.y];
+    RootChannel ch = rootChannelQuad(t, s, c, active, P.rules, P.k, maxD(t.maxEdge, s.maxEdge));
+    if (!active)
+        ch = RootChannel{0, 0, 0, 0, false};
     for (int o = 1; o <= 2; o <<= 1) {  // maxima over the pair's four lanes
         ch.dmax = fmax(ch.dmax, __shfl_xor_sync(~0u, ch.dmax, o));
         ch.hmax = fmax(ch.hmax, __shfl_xor_sync(~0u, ch.hmax, o));
