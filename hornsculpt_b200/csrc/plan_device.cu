@@ -98,7 +98,7 @@ struct WarpMem {
     double *pendErr;
     uint32_t *atl;
     double *pts;   // test and trial point tables, 2 x kRulePoints x kPts
-    double *rows;  // row items of a moment computation, kRulePoints x kRowValues
+    double *rows;  // one chunk of row items of a moment computation, W x kRowValues
 };
 
 struct PairOutput {
@@ -173,69 +173,79 @@ PD_HD PD_NOINLINE void tensorMoments(const Wp &w, const HostPanel &t, const Host
     const V3 origin = t.v[0] - s.v[0];
     const double fab = a.fraction * b.fraction;
     const int split = n < W ? W / n : 1, items = n * split;  // lanes per test point
-    for (int it = w.lane(); it < items; it += W) {
-        const int xi = it / split, h = it - xi * split;
-        const double *T = pts + kPts * xi;
-        const double tx = T[3], ty = T[4], tz = T[5], tw = T[6] * fab;
-        double in[24], m[4] = {0, 0, 0, 0};
-#pragma unroll
-        for (int v = 0; v < 24; ++v)
-            in[v] = 0;
-        for (int qi = h; qi < n; qi += split) {
-            const double *S = pts + kPts * (kRulePoints + qi);
-            const V3 d{origin.x + (tx - S[3]), origin.y + (ty - S[4]), origin.z + (tz - S[5])};
-            const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
-            if (!(r > 0)) {
-                bad = true;
-                continue;
-            }
-            double sn, cs;
-            sincos(-k * r, &sn, &cs);  // exp(-i k r)
-            const double ir = 1 / r, gr = cs * ir, gi = sn * ir, kr = k * r, f = scale * ir * ir;
-            const double dr = (-gr + gi * kr) * f, di = (-gr * kr - gi) * f;
-            const double wgt = tw * S[6];
-            const double kre[4] = {gr, dr * d.x, dr * d.y, dr * d.z};
-            const double kim[4] = {gi, di * d.x, di * d.y, di * d.z};
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const double wb = wgt * S[j];
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    in[2 * (3 * c + j)] = fma(kre[c], wb, in[2 * (3 * c + j)]);
-                    in[2 * (3 * c + j) + 1] = fma(kim[c], wb, in[2 * (3 * c + j) + 1]);
-                }
-            }
-            // magnitude of each channel's terms: |G| = 1/r, |grad G| <= (1 + kr)/r^2
-            const double md = wgt * (1 + kr) * f * ir;
-            m[0] += wgt * ir;
-            m[1] += md * fabs(d.x);
-            m[2] += md * fabs(d.y);
-            m[3] += md * fabs(d.z);
-        }
-        double *R = rows + kRowValues * it;
-#pragma unroll
-        for (int v = 0; v < 24; ++v)
-            R[v] = in[v];
-        R[24] = m[0], R[25] = m[1], R[26] = m[2], R[27] = m[3];
-        R[28] = T[0], R[29] = T[1], R[30] = T[2];
-    }
-    w.sync();
+    // Row items in chunks of W (one per lane), so `rows` holds W records; the
+    // owners of the moment values add each chunk's records in item order.
     constexpr int own_n = kValues / W;
     const int base = own_n * w.lane();
-    for (int o = 0; o < own_n; ++o) {
-        const int v = base + o;
-        double acc = 0;
-        if (v < 72) {
-            const int comp = v >> 1, ri = v & 1, c = comp / 9, i = (comp % 9) / 3, j = comp % 3;
-            const int col = 2 * (3 * c + j) + ri;
-            for (int it = 0; it < items; ++it)
-                acc = fma(rows[kRowValues * it + 28 + i], rows[kRowValues * it + col], acc);
-        } else if (v < 76) {
-            for (int it = 0; it < items; ++it)
-                acc += rows[kRowValues * it + 24 + (v - 72)];
+    double acc[own_n];
+    for (int o = 0; o < own_n; ++o)
+        acc[o] = 0;
+    for (int c0 = 0; c0 < items; c0 += W) {
+        const int it = c0 + w.lane();
+        if (it < items) {
+            const int xi = it / split, h = it - xi * split;
+            const double *T = pts + kPts * xi;
+            const double tx = T[3], ty = T[4], tz = T[5], tw = T[6] * fab;
+            double in[24], m[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int v = 0; v < 24; ++v)
+                in[v] = 0;
+            for (int qi = h; qi < n; qi += split) {
+                const double *S = pts + kPts * (kRulePoints + qi);
+                const V3 d{origin.x + (tx - S[3]), origin.y + (ty - S[4]), origin.z + (tz - S[5])};
+                const double r = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+                if (!(r > 0)) {
+                    bad = true;
+                    continue;
+                }
+                double sn, cs;
+                sincos(-k * r, &sn, &cs);  // exp(-i k r)
+                const double ir = 1 / r, gr = cs * ir, gi = sn * ir, kr = k * r, f = scale * ir * ir;
+                const double dr = (-gr + gi * kr) * f, di = (-gr * kr - gi) * f;
+                const double wgt = tw * S[6];
+                const double kre[4] = {gr, dr * d.x, dr * d.y, dr * d.z};
+                const double kim[4] = {gi, di * d.x, di * d.y, di * d.z};
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double wb = wgt * S[j];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) {
+                        in[2 * (3 * c + j)] = fma(kre[c], wb, in[2 * (3 * c + j)]);
+                        in[2 * (3 * c + j) + 1] = fma(kim[c], wb, in[2 * (3 * c + j) + 1]);
+                    }
+                }
+                // magnitude of each channel's terms: |G| = 1/r, |grad G| <= (1 + kr)/r^2
+                const double md = wgt * (1 + kr) * f * ir;
+                m[0] += wgt * ir;
+                m[1] += md * fabs(d.x);
+                m[2] += md * fabs(d.y);
+                m[3] += md * fabs(d.z);
+            }
+            double *R = rows + kRowValues * (it - c0);
+#pragma unroll
+            for (int v = 0; v < 24; ++v)
+                R[v] = in[v];
+            R[24] = m[0], R[25] = m[1], R[26] = m[2], R[27] = m[3];
+            R[28] = T[0], R[29] = T[1], R[30] = T[2];
         }
-        own[o] = acc;
+        w.sync();
+        const int chunk = items - c0 < W ? items - c0 : W;
+        for (int o = 0; o < own_n; ++o) {
+            const int v = base + o;
+            if (v < 72) {
+                const int comp = v >> 1, ri = v & 1, c = comp / 9, i = (comp % 9) / 3, j = comp % 3;
+                const int col = 2 * (3 * c + j) + ri;
+                for (int q = 0; q < chunk; ++q)
+                    acc[o] = fma(rows[kRowValues * q + 28 + i], rows[kRowValues * q + col], acc[o]);
+            } else if (v < 76) {
+                for (int q = 0; q < chunk; ++q)
+                    acc[o] += rows[kRowValues * q + 24 + (v - 72)];
+            }
+        }
+        w.sync();
     }
+    for (int o = 0; o < own_n; ++o)
+        own[o] = acc[o];
     w.sync();  // the point tables and rows are rewritten by the next call
 }
 
@@ -860,10 +870,10 @@ __global__ void __launch_bounds__(kRootThreads) rootKernel(AdaptiveParams P, con
 
 constexpr int kWarpsPerBlock = 4;
 
-constexpr int kWarpSmemDoubles = 2 * kRulePoints * kPts + kRulePoints * kRowValues;
+constexpr int kWarpSmemDoubles = 2 * kRulePoints * kPts + 32 * kRowValues;
 constexpr size_t kRefineSmem = sizeof(double) * kWarpSmemDoubles * kWarpsPerBlock;
 
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) refineKernel(AdaptiveParams P, const uint2 *list,
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 3) refineKernel(AdaptiveParams P, const uint2 *list,
                                                                      unsigned long long count,
                                                                      unsigned long long *next, WarpMem arena,
                                                                      PairOutput O, uint2 *flagged,
