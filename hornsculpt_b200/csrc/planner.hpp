@@ -5,9 +5,34 @@
 
 #include "host_mesh.hpp"
 
+#include <memory>
+#include <new>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace hsb {
+
+// Allocator that leaves elements default-initialised (for Patch: uninitialised)
+// when a vector grows by resize: a plan's patch array is sized once and then
+// filled in parallel, so zeroing hundreds of megabytes on one thread first
+// would only cost time.
+template <class T> struct UninitAllocator : std::allocator<T> {
+    using value_type = T;
+    template <class U> struct rebind {
+        using other = UninitAllocator<U>;
+    };
+    UninitAllocator() noexcept = default;
+    template <class U> UninitAllocator(const UninitAllocator<U> &) noexcept {}
+    template <class U> void construct(U *p) noexcept(std::is_nothrow_default_constructible_v<U>) {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <class U, class... Args> void construct(U *p, Args &&...args) {
+        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <class T, class U> bool operator==(const UninitAllocator<T> &, const UninitAllocator<U> &) { return true; }
+template <class T, class U> bool operator!=(const UninitAllocator<T> &, const UninitAllocator<U> &) { return false; }
 
 struct TouchJob {
     uint32_t test, trial;
@@ -19,7 +44,7 @@ struct NearJob {
 struct Plan {
     std::vector<TouchJob> touching;           // ordered (test, trial), self and both directions
     std::vector<NearJob> near;                // ordered near jobs sorted by (test, trial)
-    std::vector<Patch> patches;
+    std::vector<Patch, UninitAllocator<Patch>> patches;
     std::vector<uint8_t> wholePanelDegrees;   // all-pairs mode only: unordered pair -> 8/14
     std::vector<uint32_t> nearOffsets, nearTrials;
     unsigned maxDepth{};

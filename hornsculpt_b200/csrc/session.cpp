@@ -26,7 +26,7 @@ void cuda(cudaError_t e, const char *what) {
         throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-template <class T> void upload(DeviceBuffer &buf, const std::vector<T> &v, cudaStream_t s) {
+template <class T, class A> void upload(DeviceBuffer &buf, const std::vector<T, A> &v, cudaStream_t s) {
     buf.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
     if (!v.empty())
         cuda(cudaMemcpyAsync(buf.as<void>(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
