@@ -68,6 +68,15 @@ def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(values, world, dist, torch, device):
+    """Each value's maximum over the ranks (one collective of all values; the
+    job's time is its slowest rank's). Identity for one rank."""
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def request(hs):
     return hs.BemRequest(frequencies=FREQUENCIES, observers=OBSERVERS,
                          excitations=[hs.BemExcitation("uniform", [hs.FaceVelocity(1, 1.0)])],
@@ -1014,15 +1023,8 @@ def main():
                 plain_s += start.elapsed_time(end) / 1e3
             graph_replays = solver.graph_launches() - launches0
         barrier()
-        times = torch.tensor([device_s, wall_s, plain_s], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(times, op=dist.ReduceOp.MAX)
-        device_s, wall_s, plain_s = times.tolist()
         span = profile.pop("solve_span", (0.0, 0))[0] / 1e3
-        span_t = torch.tensor([span], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(span_t, op=dist.ReduceOp.MAX)
-        span = span_t.item()
+        device_s, wall_s, plain_s, span = max_over_ranks([device_s, wall_s, plain_s, span], world, dist, torch, "cuda")
         return dict(device_s=device_s, wall_s=wall_s, span_s=span, result=result, profile=profile, work=work,
                     clocks=clocks.summary(), step_ms=step_ms, phase_ms=phase_ms, e2e_ms=e2e_ms, plain_s=plain_s,
                     graph_replays=graph_replays)
