@@ -598,6 +598,182 @@ template <class R> size_t panelSmemBytes(uint32_t rows, uint32_t jb) {
 }
 constexpr size_t kPanelSmemLimit = 220 * 1024;
 
+// FP32 panel factorisation with the panel in registers, for full 32-column
+// panels of at most kRegPanelRows rows: thread t owns panel rows
+// t + r * blockDim.x (r < kRegRowsPerThread), 32 complex values each, so the
+// elimination reads nothing but the pivot row. Pivot rule, tie rule and
+// interchange sequence are those of panelSmemKernel, and every entry of a
+// row that is not yet a pivot row is updated by the same operations in the
+// same order (a pivot row's multiplier is zero, which leaves finite values
+// unchanged). Per column, each warp
+// reduces its candidates by shuffles and the lane that holds the warp's best
+// row writes that row's remaining columns to the warp's slot in shared
+// memory; after the column's one barrier every warp reduces the warp
+// candidates, reads the pivot row from the winning warp's slot and
+// eliminates its own rows. Slots and candidates alternate with the column's
+// parity: a warp writes the slot of column j + 2 only after the barrier of
+// column j + 1, which every reader of column j has passed.
+// Eight warps, so that each SM sub-partition holds two and a thread may use
+// 255 registers: 128 hold its two rows.
+constexpr int kRegRowsPerThread = 2;
+constexpr uint32_t kRegPanelThreads = 256;
+constexpr uint32_t kRegPanelRows = kRegRowsPerThread * kRegPanelThreads;
+constexpr int kRegPanelWarps = int(kRegPanelThreads / 32);
+
+__global__ void __launch_bounds__(kRegPanelThreads, 1) panelRegKernel(float *LU, uint32_t N, uint32_t k0, int *pivots,
+                                                                      int *info) {
+    constexpr int RT = kRegRowsPerThread;
+    __shared__ __align__(16) float2 sCand[2][kRegPanelWarps][kPanel];
+    __shared__ float sBest[2][kRegPanelWarps];
+    __shared__ int sRow[2][kRegPanelWarps];
+    __shared__ int sSel[kPanel];
+    __shared__ int arrangement[kRegPanelRows], where[kRegPanelRows];
+    const uint32_t rows = N - k0, T = blockDim.x;
+    float *M = LU + size_t(blockIdx.x) * N * N * 2;
+    int *piv = pivots + size_t(blockIdx.x) * N;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = int(T >> 5);
+    int row[RT];
+    bool have[RT], taken[RT];
+    float2 a[RT][kPanel];
+#pragma unroll
+    for (int r = 0; r < RT; ++r) {
+        row[r] = int(threadIdx.x + r * T);
+        have[r] = uint32_t(row[r]) < rows;
+        taken[r] = !have[r];
+    }
+#pragma unroll
+    for (int q = 0; q < kPanel; ++q) {
+        const float *col = M + 2 * (size_t(k0 + q) * N + k0);
+#pragma unroll
+        for (int r = 0; r < RT; ++r)
+            a[r][q] = have[r] ? ld2<float>(col + 2 * row[r]) : make_float2(0.f, 0.f);
+    }
+    for (uint32_t i = threadIdx.x; i < rows; i += T) {
+        arrangement[i] = int(i);
+        where[i] = int(i);
+    }
+    const auto magnitude = [](float2 z) {
+        const float m = fabsf(z.x) + fabsf(z.y);
+        return m >= 0.f ? m : 0.f;  // a NaN row competes as zero, so a pivot row always exists
+    };
+    // Loops over columns inside the column loop run over all 32 with the
+    // columns before j skipped: a constant trip count lets them unroll first,
+    // so that every index into a[][] is a constant once the column loop is.
+#pragma unroll 32
+    for (int j = 0; j < kPanel; ++j) {
+        const int buf = j & 1;
+        float best = -1.f;
+        int bestRow = int(rows), bestSlot = -1;
+#pragma unroll
+        for (int r = 0; r < RT; ++r)
+            if (!taken[r]) {
+                const float m = magnitude(a[r][j]);
+                if (m > best) {  // rows ascend with r: ties keep the lower row
+                    best = m;
+                    bestRow = row[r];
+                    bestSlot = r;
+                }
+            }
+        const int myRow = bestRow;
+        for (int off = 16; off > 0; off >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bestRow, off);
+            if (ob > best || (ob == best && oi < bestRow)) {
+                best = ob;
+                bestRow = oi;
+            }
+        }
+        // the warp's candidate row, columns from the even column at or below j
+        if (bestSlot >= 0 && myRow == bestRow) {
+            float4 *dst = reinterpret_cast<float4 *>(&sCand[buf][warp][0]);
+#pragma unroll
+            for (int q = 0; q < kPanel; q += 2) {
+                if (q < (j & ~1))
+                    continue;
+                float2 u = a[0][q], v = a[0][q + 1];
+#pragma unroll
+                for (int r = 1; r < RT; ++r)
+                    if (bestSlot == r) {
+                        u = a[r][q];
+                        v = a[r][q + 1];
+                    }
+                dst[q / 2] = make_float4(u.x, u.y, v.x, v.y);
+            }
+        }
+        if (lane == 0) {
+            sBest[buf][warp] = best;
+            sRow[buf][warp] = bestRow;
+        }
+        __syncthreads();
+        // every warp reduces the warp candidates by shuffles (same result in every warp)
+        float pb = lane < warps ? sBest[buf][lane] : -1.f;
+        int p = lane < warps ? sRow[buf][lane] : int(rows), pw = lane;
+        for (int off = 16; off > 0; off >>= 1) {
+            const float ob = __shfl_xor_sync(0xffffffffu, pb, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, p, off), ow = __shfl_xor_sync(0xffffffffu, pw, off);
+            if (ob > pb || (ob == pb && oi < p)) {
+                pb = ob;
+                p = oi;
+                pw = ow;
+            }
+        }
+        if (threadIdx.x == 0) {
+            sSel[j] = p;
+            if (!(pb > 0.f) && *info == 0)
+                atomicCAS(info, 0, int(k0) + j + 1);
+        }
+        const float2 *prow = sCand[buf][pw];
+        const float2 d = prow[j];
+        const float den = d.x * d.x + d.y * d.y;
+        const float rden = den > 0.f ? 1.f / den : 0.f;
+        const float2 inv = make_float2(d.x * rden, -d.y * rden);
+        // a row already chosen as a pivot row keeps its values: its multiplier is zero
+        float2 l[RT];
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+            taken[r] |= p == row[r];
+            const float2 m = cmul<float>(a[r][j], inv);
+            l[r] = taken[r] ? make_float2(0.f, 0.f) : m;
+            a[r][j] = taken[r] ? a[r][j] : m;
+        }
+#pragma unroll
+        for (int q = 1; q < kPanel; ++q) {
+            if (q <= j)
+                continue;
+            const float2 pv = prow[q];
+#pragma unroll
+            for (int r = 0; r < RT; ++r)
+                csub<float>(a[r][q], l[r], pv);
+        }
+    }
+    __syncthreads();
+    // selection order -> interchange sequence (row k0+j swapped with row piv[k0+j])
+    if (threadIdx.x == 0)
+        for (int j = 0; j < kPanel; ++j) {
+            const int r = sSel[j], pj = where[r], rj = arrangement[j];
+            piv[k0 + j] = int(k0) + pj;
+            arrangement[j] = r;
+            arrangement[pj] = rj;
+            where[r] = j;
+            where[rj] = pj;
+        }
+    __syncthreads();
+    // row r of this thread goes to position where[row]; one running pointer per row
+    float *out[RT];
+#pragma unroll
+    for (int r = 0; r < RT; ++r)
+        out[r] = M + 2 * (size_t(k0) * N + k0 + (have[r] ? where[row[r]] : 0));
+    const size_t stride = size_t(N) * 2;
+#pragma unroll
+    for (int q = 0; q < kPanel; ++q)
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+            if (have[r])
+                st2<float>(out[r], a[r][q]);
+            out[r] += stride;
+        }
+}
+
 // Row interchanges of the panel applied to columns outside it.
 template <class R> __global__ void swapKernel(R *LU, uint32_t N, uint32_t k0, uint32_t jb, const int *pivots) {
     const uint32_t col = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1054,20 +1230,12 @@ __global__ void __launch_bounds__(sizeof(R) == 8 ? 256 : 512) solveKernel(const 
     C2<R> *x = reinterpret_cast<C2<R> *>(rawSmem);
     const uint32_t e = blockIdx.x, f = blockIdx.y;
     const R *M = LU + size_t(f) * N * N * 2;
-    const int *piv = pivots + size_t(f) * N;
+    // the factorisation's row interchanges, composed into one permutation
+    // (stored after the batch's interchange sequences): a parallel gather
+    const int *perm = pivots + (size_t(gridDim.y) + f) * N;
     R *out = X + (size_t(f) * E + e) * N * 2;
     for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
-        x[i] = ld2(out + 2 * i);
-    __syncthreads();
-    if (threadIdx.x == 0)
-        for (uint32_t c = 0; c < N; ++c) {
-            const int p = piv[c];
-            if (p != int(c)) {
-                const C2<R> t = x[c];
-                x[c] = x[p];
-                x[p] = t;
-            }
-        }
+        x[i] = ld2(out + 2 * perm[i]);
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const C2<R> zero = mk<R>(0, 0);
@@ -1161,10 +1329,12 @@ constexpr uint32_t kTriBlock = 128, kTriRows = 64;
 constexpr uint32_t kSmallSolve = 1024;  // up to this N the one-CTA-per-system kernel is faster
 
 __global__ void permutationKernel(const int *pivots, uint32_t N, int *perm) {
-    extern __shared__ int p[];
-    const int *piv = pivots + size_t(blockIdx.x) * N;
-    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x)
+    extern __shared__ int p[];  // [N] the permutation, [N] the interchange sequence
+    int *piv = p + N;
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
         p[i] = int(i);
+        piv[i] = pivots[size_t(blockIdx.x) * N + i];
+    }
     __syncthreads();
     if (threadIdx.x == 0)
         for (uint32_t c = 0; c < N; ++c) {
@@ -1492,7 +1662,11 @@ template <class R> void factor(R *LU, uint32_t N, uint32_t B, int *pivots, int *
                 const size_t bytes = panelSmemBytes<R>(N - k0, jb);
                 const uint32_t rows = N - k0;
                 const uint32_t limit = clusterLimit<R>();
-                if (bytes > kPanelSmemLimit && rows <= limit * (kClusterRows<R> + kGlobalSlots * 1024u)) {
+                if (sizeof(R) == 4 && jb == uint32_t(kPanel) && rows <= kRegPanelRows) {
+                    const uint32_t threads =
+                        std::max(32u, ((rows + kRegRowsPerThread - 1) / kRegRowsPerThread + 31) / 32 * 32);
+                    panelRegKernel<<<B, threads, 0, stream>>>(reinterpret_cast<float *>(LU), N, k0, pivots, info);
+                } else if (bytes > kPanelSmemLimit && rows <= limit * (kClusterRows<R> + kGlobalSlots * 1024u)) {
                     // as few CTAs as hold the panel in shared memory, else the whole cluster with the
                     // rows beyond kClusterRows per CTA kept in global memory
                     const uint32_t C = std::min(limit, (rows + kClusterRows<R> - 1) / kClusterRows<R>);
@@ -1601,7 +1775,7 @@ template <class R> void solve(const R *LU, const int *pivots, uint32_t N, uint32
 }
 
 template <class R> void permutation(const int *pivots, uint32_t N, uint32_t B, cudaStream_t stream) {
-    const size_t smem = size_t(N) * sizeof(int);
+    const size_t smem = 2 * size_t(N) * sizeof(int);
     static PerDeviceHighWater attr;
     if (smem > 48 * 1024 && attr.raise(smem))
         check(cudaFuncSetAttribute(permutationKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),

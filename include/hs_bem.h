@@ -396,11 +396,11 @@ hs_status hs_bem_debug_fmm_tree(const double *vertices, size_t vertex_count, con
  * triangle_count * 200 + observer_count * 24 +
  * observer_count * ceil(triangle_count / 256) * 16 + 256 bytes to 4 MiB (larger
  * requests return HS_E_INVALID). The first call on a device looks up that
- * array's device address, so make it before any stream capture on that device;
- * the address is kept until the process exits, so do not reset the device
- * between calls. All calls share the array: calls that overlap on the GPU race
- * and must be serialised. The call reads status words back and waits for
- * `cuda_stream`; it returns after the work on that stream has finished. A
+ * array's device address and keeps it until the process exits, so do not
+ * reset the device between calls. All calls share the array: calls that
+ * overlap on the GPU race and must be serialised. The call reads status words
+ * back and waits for `cuda_stream`, so it returns after the work on that
+ * stream has finished and cannot be captured in a CUDA graph. A
  * degenerate triangle returns HS_E_INVALID, as at session creation. */
 hs_status hs_bem_observer_field_noalloc(const double *vertices, size_t vertex_count, const uint32_t *triangles,
                                         size_t triangle_count, const double *pressure_trace, const double *flux,
