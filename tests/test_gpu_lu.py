@@ -124,3 +124,6 @@ def test_lu_reports_a_zero_pivot():
     a[0, :, 40] = 0
     _, _, info = hs.debug_lu_factor(a)
     assert info == 41
+    # the FP32 factorisation (its panels of at most 512 rows are factored in registers)
+    _, _, info32 = hs.debug_lu_factor(a, fp32=True)
+    assert info32 == 41
