@@ -605,24 +605,36 @@ constexpr size_t kPanelSmemLimit = 220 * 1024;
 // interchange sequence are those of panelSmemKernel, and every entry of a
 // row that is not yet a pivot row is updated by the same operations in the
 // same order (a pivot row's multiplier is zero, which leaves finite values
-// unchanged). Per column, each warp
-// reduces its candidates by shuffles and the lane that holds the warp's best
-// row writes that row's remaining columns to the warp's slot in shared
-// memory; after the column's one barrier every warp reduces the warp
-// candidates, reads the pivot row from the winning warp's slot and
-// eliminates its own rows. Slots and candidates alternate with the column's
-// parity: a warp writes the slot of column j + 2 only after the barrier of
-// column j + 1, which every reader of column j has passed.
+// unchanged).
+//
+// Per column, each warp reduces its candidates by shuffles and the lane that
+// holds the warp's best row writes that row's remaining columns to the
+// warp's slot in shared memory; after the column's one barrier every warp
+// reduces the warp candidates, reads the pivot row from the winning warp's
+// slot and eliminates its own rows. Slots and candidates alternate with the
+// column's parity: a warp writes the slot of column j + 2 only after the
+// barrier of column j + 1, which every reader of column j has passed.
+//
+// Register indices must be constants, and a fully unrolled 32-column body is
+// too long for the instruction cache (an earlier build stalled on
+// instruction fetch for most of its cycles). So each row is rotated instead:
+// at column j, a[r][c] holds column j + c for c < 32 - j and the finished
+// columns j + c - 32 after them. The loop body handles kRegUnroll columns
+// with constant indices (updates of the entries c >= 32 - j are predicated
+// off) and rotates the rows by kRegUnroll at its end; after the 32 columns
+// every row is back in column order.
 // Eight warps, so that each SM sub-partition holds two and a thread may use
-// 255 registers: 128 hold its two rows.
-constexpr int kRegRowsPerThread = 2;
+// 255 registers: 64 per row.
+constexpr int kRegRowsPerThread = 3;
+constexpr int kRegUnroll = 2;
 constexpr uint32_t kRegPanelThreads = 256;
 constexpr uint32_t kRegPanelRows = kRegRowsPerThread * kRegPanelThreads;
 constexpr int kRegPanelWarps = int(kRegPanelThreads / 32);
 
 __global__ void __launch_bounds__(kRegPanelThreads, 1) panelRegKernel(float *LU, uint32_t N, uint32_t k0, int *pivots,
                                                                       int *info) {
-    constexpr int RT = kRegRowsPerThread;
+    constexpr int RT = kRegRowsPerThread, U = kRegUnroll;
+    static_assert(kPanel % U == 0, "the column groups must tile the panel");
     __shared__ __align__(16) float2 sCand[2][kRegPanelWarps][kPanel];
     __shared__ float sBest[2][kRegPanelWarps];
     __shared__ int sRow[2][kRegPanelWarps];
@@ -656,94 +668,109 @@ __global__ void __launch_bounds__(kRegPanelThreads, 1) panelRegKernel(float *LU,
         const float m = fabsf(z.x) + fabsf(z.y);
         return m >= 0.f ? m : 0.f;  // a NaN row competes as zero, so a pivot row always exists
     };
-    // Loops over columns inside the column loop run over all 32 with the
-    // columns before j skipped: a constant trip count lets them unroll first,
-    // so that every index into a[][] is a constant once the column loop is.
-#pragma unroll 32
-    for (int j = 0; j < kPanel; ++j) {
-        const int buf = j & 1;
-        float best = -1.f;
-        int bestRow = int(rows), bestSlot = -1;
+#pragma unroll 1
+    for (int j0 = 0; j0 < kPanel; j0 += U) {
 #pragma unroll
-        for (int r = 0; r < RT; ++r)
-            if (!taken[r]) {
-                const float m = magnitude(a[r][j]);
-                if (m > best) {  // rows ascend with r: ties keep the lower row
-                    best = m;
-                    bestRow = row[r];
-                    bestSlot = r;
-                }
-            }
-        const int myRow = bestRow;
-        for (int off = 16; off > 0; off >>= 1) {
-            const float ob = __shfl_xor_sync(0xffffffffu, best, off);
-            const int oi = __shfl_xor_sync(0xffffffffu, bestRow, off);
-            if (ob > best || (ob == best && oi < bestRow)) {
-                best = ob;
-                bestRow = oi;
-            }
-        }
-        // the warp's candidate row, columns from the even column at or below j
-        if (bestSlot >= 0 && myRow == bestRow) {
-            float4 *dst = reinterpret_cast<float4 *>(&sCand[buf][warp][0]);
-#pragma unroll
-            for (int q = 0; q < kPanel; q += 2) {
-                if (q < (j & ~1))
-                    continue;
-                float2 u = a[0][q], v = a[0][q + 1];
-#pragma unroll
-                for (int r = 1; r < RT; ++r)
-                    if (bestSlot == r) {
-                        u = a[r][q];
-                        v = a[r][q + 1];
-                    }
-                dst[q / 2] = make_float4(u.x, u.y, v.x, v.y);
-            }
-        }
-        if (lane == 0) {
-            sBest[buf][warp] = best;
-            sRow[buf][warp] = bestRow;
-        }
-        __syncthreads();
-        // every warp reduces the warp candidates by shuffles (same result in every warp)
-        float pb = lane < warps ? sBest[buf][lane] : -1.f;
-        int p = lane < warps ? sRow[buf][lane] : int(rows), pw = lane;
-        for (int off = 16; off > 0; off >>= 1) {
-            const float ob = __shfl_xor_sync(0xffffffffu, pb, off);
-            const int oi = __shfl_xor_sync(0xffffffffu, p, off), ow = __shfl_xor_sync(0xffffffffu, pw, off);
-            if (ob > pb || (ob == pb && oi < p)) {
-                pb = ob;
-                p = oi;
-                pw = ow;
-            }
-        }
-        if (threadIdx.x == 0) {
-            sSel[j] = p;
-            if (!(pb > 0.f) && *info == 0)
-                atomicCAS(info, 0, int(k0) + j + 1);
-        }
-        const float2 *prow = sCand[buf][pw];
-        const float2 d = prow[j];
-        const float den = d.x * d.x + d.y * d.y;
-        const float rden = den > 0.f ? 1.f / den : 0.f;
-        const float2 inv = make_float2(d.x * rden, -d.y * rden);
-        // a row already chosen as a pivot row keeps its values: its multiplier is zero
-        float2 l[RT];
-#pragma unroll
-        for (int r = 0; r < RT; ++r) {
-            taken[r] |= p == row[r];
-            const float2 m = cmul<float>(a[r][j], inv);
-            l[r] = taken[r] ? make_float2(0.f, 0.f) : m;
-            a[r][j] = taken[r] ? a[r][j] : m;
-        }
-#pragma unroll
-        for (int q = 1; q < kPanel; ++q) {
-            if (q <= j)
-                continue;
-            const float2 pv = prow[q];
+        for (int u = 0; u < U; ++u) {
+            // column j = j0 + u sits at index u of the rotated rows; its remaining
+            // columns at indices u .. u + left - 1
+            const int j = j0 + u, buf = j & 1, left = kPanel - j;
+            float best = -1.f;
+            int bestRow = int(rows), bestSlot = -1;
 #pragma unroll
             for (int r = 0; r < RT; ++r)
-                csub<float>(a[r][q], l[r], pv);
+                if (!taken[r]) {
+                    const float m = magnitude(a[r][u]);
+                    if (m > best) {  // rows ascend with r: ties keep the lower row
+                        best = m;
+                        bestRow = row[r];
+                        bestSlot = r;
+                    }
+                }
+            const int myRow = bestRow;
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bestRow, off);
+                if (ob > best || (ob == best && oi < bestRow)) {
+                    best = ob;
+                    bestRow = oi;
+                }
+            }
+            // the warp's candidate row (slot entry c = column j + c; entries past the
+            // panel's end are never read)
+            if (bestSlot >= 0 && myRow == bestRow) {
+                float4 *dst = reinterpret_cast<float4 *>(&sCand[buf][warp][0]);
+#pragma unroll
+                for (int c = 0; c < kPanel; c += 2) {
+                    float2 x0 = a[0][(u + c) % kPanel], x1 = a[0][(u + c + 1) % kPanel];
+#pragma unroll
+                    for (int r = 1; r < RT; ++r)
+                        if (bestSlot == r) {
+                            x0 = a[r][(u + c) % kPanel];
+                            x1 = a[r][(u + c + 1) % kPanel];
+                        }
+                    dst[c / 2] = make_float4(x0.x, x0.y, x1.x, x1.y);
+                }
+            }
+            if (lane == 0) {
+                sBest[buf][warp] = best;
+                sRow[buf][warp] = bestRow;
+            }
+            __syncthreads();
+            // every warp reduces the warp candidates by shuffles (same result in every warp)
+            float pb = lane < warps ? sBest[buf][lane] : -1.f;
+            int p = lane < warps ? sRow[buf][lane] : int(rows), pw = lane;
+            for (int off = 16; off > 0; off >>= 1) {
+                const float ob = __shfl_xor_sync(0xffffffffu, pb, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, p, off), ow = __shfl_xor_sync(0xffffffffu, pw, off);
+                if (ob > pb || (ob == pb && oi < p)) {
+                    pb = ob;
+                    p = oi;
+                    pw = ow;
+                }
+            }
+            if (threadIdx.x == 0) {
+                sSel[j] = p;
+                if (!(pb > 0.f) && *info == 0)
+                    atomicCAS(info, 0, int(k0) + j + 1);
+            }
+            const float2 *prow = sCand[buf][pw];
+            const float2 d = prow[0];
+            const float den = d.x * d.x + d.y * d.y;
+            const float rden = den > 0.f ? 1.f / den : 0.f;
+            const float2 inv = make_float2(d.x * rden, -d.y * rden);
+            // a row already chosen as a pivot row keeps its values: its multiplier is zero
+            float2 l[RT];
+#pragma unroll
+            for (int r = 0; r < RT; ++r) {
+                taken[r] |= p == row[r];
+                const float2 m = cmul<float>(a[r][u], inv);
+                l[r] = taken[r] ? make_float2(0.f, 0.f) : m;
+                a[r][u] = taken[r] ? a[r][u] : m;
+            }
+#pragma unroll
+            for (int c = 1; c < kPanel; ++c) {
+                if (c >= left)  // finished columns
+                    break;
+                const float2 pv = prow[c];
+#pragma unroll
+                for (int r = 0; r < RT; ++r)
+                    csub<float>(a[r][(u + c) % kPanel], l[r], pv);
+            }
+        }
+        // rotate every row left by U: index c takes column j0 + U + c
+        float2 t[RT][U];
+#pragma unroll
+        for (int r = 0; r < RT; ++r) {
+#pragma unroll
+            for (int c = 0; c < U; ++c)
+                t[r][c] = a[r][c];
+#pragma unroll
+            for (int c = 0; c + U < kPanel; ++c)
+                a[r][c] = a[r][c + U];
+#pragma unroll
+            for (int c = 0; c < U; ++c)
+                a[r][kPanel - U + c] = t[r][c];
         }
     }
     __syncthreads();
