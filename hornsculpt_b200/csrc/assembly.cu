@@ -1048,6 +1048,7 @@ __global__ void __launch_bounds__(64, Mixed ? 10 : 1) nearWarpKernel(const DPane
     __shared__ Acc sS[2][64][18];     // per warp: trial-contracted values S(x)
     __shared__ double sB[2][64][3];   // per warp: mapped test barycentrics
     __shared__ double sY[2][64][3];   // per warp: mapped trial barycentrics
+    __shared__ double sE[2][64][3];   // per warp: trial points' offsets from the trial panel's first vertex
     __shared__ double sM[2][54];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t pairIndex = blockIdx.x * 2 + warp;
@@ -1068,13 +1069,19 @@ __global__ void __launch_bounds__(64, Mixed ? 10 : 1) nearWarpKernel(const DPane
         const int ro = patch.degree == 14 ? 34 : 18;  // rule offsets of the 16- and 64-point bins
         // mapped rule points of this patch (test from patch.test, trial from patch.trial)
         for (int idx = lane; idx < n; idx += 32) {
+            double by[3];
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
                 sB[warp][idx][i] = cRule[4 * (ro + idx)] * patch.test[i] + cRule[4 * (ro + idx) + 1] * patch.test[3 + i] +
                                    cRule[4 * (ro + idx) + 2] * patch.test[6 + i];
-                sY[warp][idx][i] = cRule[4 * (ro + idx)] * patch.trial[i] + cRule[4 * (ro + idx) + 1] * patch.trial[3 + i] +
-                                   cRule[4 * (ro + idx) + 2] * patch.trial[6 + i];
+                by[i] = cRule[4 * (ro + idx)] * patch.trial[i] + cRule[4 * (ro + idx) + 1] * patch.trial[3 + i] +
+                        cRule[4 * (ro + idx) + 2] * patch.trial[6 + i];
+                sY[warp][idx][i] = by[i];
             }
+            // the trial point's offset from the trial panel's first vertex, once per patch point
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                sE[warp][idx][c] = s.e1[c] * by[1] + s.e2[c] * by[2];
         }
         __syncwarp();
         const double wpatch = patch.areaFraction * w4;
@@ -1093,10 +1100,10 @@ __global__ void __launch_bounds__(64, Mixed ? 10 : 1) nearWarpKernel(const DPane
             for (int c = 0; c < 18; ++c)
                 S[c] = 0;
             for (int y = y0; y < y1; ++y) {
-                const double *bs = sY[warp][y];
-                const double dx = Dx - (s.e1[0] * bs[1] + s.e2[0] * bs[2]);
-                const double dy = Dy - (s.e1[1] * bs[1] + s.e2[1] * bs[2]);
-                const double dz = Dz - (s.e1[2] * bs[1] + s.e2[2] * bs[2]);
+                const double *bs = sY[warp][y], *ey = sE[warp][y];
+                const double dx = Dx - ey[0];
+                const double dy = Dy - ey[1];
+                const double dz = Dz - ey[2];
                 const double w = wx * cRule[4 * (ro + y) + 3];
                 Acc val[6];
                 if constexpr (Mixed) {
