@@ -899,7 +899,11 @@ __global__ void __launch_bounds__(128, 6) singularMixedKernel(const DPanel *__re
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0)
         flagError(error, kErrDistance);
-    float v[26];
+    // Warp sums of the 26 moment values as a reduce-scatter: after the pass at
+    // distance h a lane keeps the h partial sums of the half its lane bit h
+    // selects, so after five passes (31 shuffles instead of 26 x 5) lane l holds
+    // the sum of value l.
+    float v[32];
 #pragma unroll
     for (int c = 0; c < 18; ++c)
         v[c] = m[c];
@@ -909,36 +913,37 @@ __global__ void __launch_bounds__(128, 6) singularMixedKernel(const DPanel *__re
     v[24] = g[0];
     v[25] = g[1];
 #pragma unroll
-    for (int c = 0; c < 26; ++c)
+    for (int c = 26; c < 32; ++c)
+        v[c] = 0.f;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
-            v[c] += __shfl_xor_sync(0xffffffffu, v[c], off);
+    for (int h = 16; h >= 1; h >>= 1) {
+        const bool upper = (lane & unsigned(h)) != 0;
+#pragma unroll
+        for (int c = 0; c < h; ++c) {
+            const float send = upper ? v[c] : v[c + h], keep = upper ? v[c + h] : v[c];
+            v[c] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+        }
+    }
+    const float sum = v[0];  // value `lane`
+    // lanes 0..11 write record entry `lane`: canonical index of each local vertex
+    int invT[3], invS[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        invT[job.permTest[c]] = c;
+        invS[job.permTrial[c]] = c;
+    }
+    const int o = lane < 12 ? int(lane) : 0;
+    const int i = o < 9 ? o / 3 : o - 9, j = o % 3;
+    const int src = o < 9 ? 2 * (3 * invT[i] + invS[j]) : 18 + 2 * invT[i];
+    const float vre = __shfl_sync(0xffffffffu, sum, src), vim = __shfl_sync(0xffffffffu, sum, src + 1);
+    const float g0 = __shfl_sync(0xffffffffu, sum, 24), g1 = __shfl_sync(0xffffffffu, sum, 25);
     if (lane < 12) {
-        const int o = lane;
-        // canonical index of each local vertex
-        int invT[3], invS[3];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            invT[job.permTest[c]] = c;
-            invS[job.permTrial[c]] = c;
-        }
-        const int i = o < 9 ? o / 3 : o - 9, j = o % 3;
-        const int src = o < 9 ? 2 * (3 * invT[i] + invS[j]) : 18 + 2 * invT[i];
-        float vre = 0.f, vim = 0.f;
-#pragma unroll
-        for (int c = 0; c < 12; ++c) {
-            const int cand = c < 9 ? 2 * c : 18 + 2 * (c - 9);
-            if (cand == src) {
-                vre = v[cand];
-                vim = v[cand + 1];
-            }
-        }
         double re, im;
         if (o < 9) {
             const double curl = t.curl[3 * i] * s.curl[3 * j] + t.curl[3 * i + 1] * s.curl[3 * j + 1] +
                                 t.curl[3 * i + 2] * s.curl[3 * j + 2];
-            re = double(vre) + double(v[25]) * curl * invk;
-            im = double(vim) - double(v[24]) * curl * invk;
+            re = double(vre) + double(g1) * curl * invk;
+            im = double(vim) - double(g0) * curl * invk;
         } else {
             re = vre;
             im = double(vim) + (coincident ? t.area / (6.0 * k) : 0.0);
