@@ -671,24 +671,41 @@ __device__ __forceinline__ void sampleFp64(Moments13 &acc, const DPanel &t, cons
     }
 }
 
+// Block sums of N values, left in smem[0][0..N). Within a warp a
+// reduce-scatter per group of 32 values: after the pass at distance h a lane
+// keeps the h partial sums of the half its lane bit h selects, so after five
+// passes (31 shuffles per group instead of 32 x 5) lane l holds the sum of
+// value l of the group. The warps' sums are then added in warp order by the
+// thread that owns each value.
 template <int N>
 __device__ __forceinline__ void blockReduce(double (&v)[N], double (*smem)[N]) {
-#pragma unroll
-    for (int c = 0; c < N; ++c)
-        for (int off = 16; off > 0; off >>= 1)
-            v[c] += __shfl_down_sync(0xffffffffu, v[c], off);
+    constexpr int G = (N + 31) / 32;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0)
 #pragma unroll
-        for (int c = 0; c < N; ++c)
-            smem[warp][c] = v[c];
+    for (int gi = 0; gi < G; ++gi) {
+        double x[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+            x[c] = 32 * gi + c < N ? v[32 * gi + c] : 0.0;
+#pragma unroll
+        for (int h = 16; h >= 1; h >>= 1) {
+            const bool upper = (lane & h) != 0;
+#pragma unroll
+            for (int c = 0; c < h; ++c) {
+                const double send = upper ? x[c] : x[c + h], keep = upper ? x[c + h] : x[c];
+                x[c] = keep + __shfl_xor_sync(0xffffffffu, send, h);
+            }
+        }
+        if (32 * gi + lane < N)
+            smem[warp][32 * gi + lane] = x[0];
+    }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const int warps = blockDim.x >> 5;
+    const int warps = blockDim.x >> 5;
+    for (int c = threadIdx.x; c < N; c += blockDim.x) {
+        double sum = smem[0][c];
         for (int w = 1; w < warps; ++w)
-#pragma unroll
-            for (int c = 0; c < N; ++c)
-                smem[0][c] += smem[w][c];
+            sum += smem[w][c];
+        smem[0][c] = sum;
     }
     __syncthreads();
 }
