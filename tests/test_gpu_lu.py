@@ -127,3 +127,18 @@ def test_lu_reports_a_zero_pivot():
     # the FP32 factorisation (its panels of at most 512 rows are factored in registers)
     _, _, info32 = hs.debug_lu_factor(a, fp32=True)
     assert info32 == 41
+
+
+@pytest.mark.parametrize("n", [96, 642])
+def test_pivot_ties_take_the_lowest_row(n):
+    """Entries of equal |re| + |im| in the first column: both factorisations choose the
+    lowest row, as zgetrf (izamax) does, in the register, shared-memory and cluster panels."""
+    rng = np.random.default_rng(n + 7)
+    a = rng.standard_normal((1, n, n)) + 1j * rng.standard_normal((1, n, n))
+    a[0, :, 0] = rng.choice([1 + 1j, 1 - 1j, -1 + 1j, -1 - 1j, 2, -2j], n)  # |re| + |im| = 2 throughout
+    for fp32 in (False, True):
+        factors, piv, info = hs.debug_lu_factor(a, fp32=fp32)
+        assert info == 0
+        assert piv[0][0] == 0, (fp32, piv[0][:4])
+    _, ref_piv = _lapack(a[0], fp32=False)
+    assert ref_piv[0] == 0
